@@ -1,0 +1,401 @@
+// ORACLE — test infrastructure, not product code.
+//
+// A CPU restatement of the reference's bidiagonal-SVD and data-mask
+// algorithms (Excalibur `src/bbtsvd.cpp`), used only by tests/, by
+// __graft_entry__.smoke() and by bench.py's cpu_baseline leg to check the
+// CUDA path.  The product never links or calls this library.
+//
+// Parity is pinned: tests/test_oracle_golden.py checks every function here
+// against golden vectors produced by the reference's own sources compiled
+// in this repository's checker build (oracle/Makefile, target `ref`).
+//
+// Arithmetic follows the reference operation by operation and is compiled
+// with -ffp-contract=off (no fused multiply-add), matching the reference's
+// `-O3 -mavx2` build in which pow(x, 2) is folded to x*x and AVX2 without
+// FMA rounds every product and every sum.
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdlib>
+#include <cstring>
+#include <random>
+#include <vector>
+
+namespace {
+
+// Stationary-qd Sturm count of B^T B - mu^2 I.  bbtsvd.cpp:7-17.
+int sturm_count(int n, const double* a, const double* b, double mu) {
+  const double mu2 = mu * mu;
+  int neg = 0;
+  double piv = 1.0, t = 0.0;
+  for (int i = 0; i < n; ++i) {
+    if (i == 0) {
+      t = -mu2;
+    } else {
+      const double q = (b[i - 1] * b[i - 1]) / piv;
+      t = t * q;
+      t = t - mu2;
+    }
+    piv = a[i] * a[i] + t;
+    if (piv < 0.0) ++neg;
+  }
+  return neg;
+}
+
+// Plain 2-norm, stride inc.  Stands in for cblas_dnrm2 (bbtsvd.cpp:69);
+// agrees with BLAS to rounding, not bitwise.
+double norm2(int n, const double* x, int inc) {
+  double scale = 0.0, ssq = 1.0;
+  for (int i = 0; i < n; ++i) {
+    const double v = std::fabs(x[(size_t)i * inc]);
+    if (v != 0.0) {
+      if (scale < v) {
+        ssq = 1.0 + ssq * (scale / v) * (scale / v);
+        scale = v;
+      } else {
+        ssq += (v / scale) * (v / scale);
+      }
+    }
+  }
+  return scale * std::sqrt(ssq);
+}
+
+// First index of the smallest |x_i| (cblas_idamin semantics).
+int argmin_abs(int n, const double* x) {
+  int best = 0;
+  double bv = std::fabs(x[0]);
+  for (int i = 1; i < n; ++i) {
+    const double v = std::fabs(x[i]);
+    if (v < bv) { bv = v; best = i; }
+  }
+  return best;
+}
+
+// First index of the largest |x_i| (cblas_idamax semantics).
+int argmax_abs(int n, const double* x, int inc) {
+  int best = 0;
+  double bv = std::fabs(x[0]);
+  for (int i = 1; i < n; ++i) {
+    const double v = std::fabs(x[(size_t)i * inc]);
+    if (v > bv) { bv = v; best = i; }
+  }
+  return best;
+}
+
+// Twisted inverse-iteration solve: x[k] = 1, backward with lower factor,
+// forward with upper factor, then normalise.  bbtsvd.cpp:65-71.
+void twisted_solve(int n, int k, const double* lo, const double* up, double* x, int inc) {
+  x[(size_t)k * inc] = 1.0;
+  for (int i = k - 1; i >= 0; --i) x[(size_t)i * inc] = -lo[i] * x[(size_t)(i + 1) * inc];
+  for (int i = k + 1; i < n; ++i) x[(size_t)i * inc] = -up[i - 1] * x[(size_t)(i - 1) * inc];
+  const double r = 1.0 / norm2(n, x, inc);
+  for (int i = 0; i < n; ++i) x[(size_t)i * inc] *= r;
+}
+
+// One singular triplet's vectors by twisted factorisations of B^T B - w^2 I
+// and the coupled B B^T - w^2 I.  bbtsvd.cpp:73-135.
+void one_triplet(int n, int ldu, double w, const double* L, const double* D,
+                 const double* a, const double* b, double* v, double* u) {
+  const double w2 = w * w;
+  std::vector<double> lp(n > 1 ? n - 1 : 1), dp(n), s(n + 1), up(n > 1 ? n - 1 : 1),
+      rp(n + 1), p(n + 1), g(n);
+  // stationary qd (dstqds), bbtsvd.cpp:73-81
+  s[0] = -w2;
+  for (int i = 0; i + 1 < n; ++i) {
+    dp[i] = D[i] + s[i];
+    lp[i] = D[i] * L[i] / dp[i];
+    s[i + 1] = lp[i] * L[i] * s[i] - w2;
+  }
+  dp[n - 1] = D[n - 1] + s[n - 1];
+  // progressive qd (dpqds), bbtsvd.cpp:83-91
+  p[n - 1] = D[n - 1] - w2;
+  for (int i = n - 2; i >= 0; --i) {
+    rp[i + 1] = D[i] * (L[i] * L[i]) + p[i + 1];
+    up[i] = L[i] * D[i] / rp[i + 1];
+    p[i] = p[i + 1] * D[i] / rp[i + 1] - w2;
+  }
+  rp[0] = p[0];
+  for (int i = 0; i < n; ++i) g[i] = s[i] + p[i] + w2;
+  int k = argmin_abs(n, g.data());
+  twisted_solve(n, k, lp.data(), up.data(), v, 1);
+  // coupling to the left factor, bbtsvd.cpp:114-126
+  s[n] = -w2; p[n] = 1.0; rp[n] = 1.0;
+  for (int i = 0; i < n; ++i) {
+    dp[i] = s[i + 1] / s[i] * dp[i];
+    g[i] = -w2 * g[i] * rp[i + 1] / (s[i] * p[i + 1]);
+  }
+  k = argmin_abs(n, g.data());
+  for (int i = 0; i < n; ++i) rp[i] = p[i] / p[i + 1] * rp[i + 1];
+  for (int i = 0; i + 1 < n; ++i) {
+    lp[i] = a[i + 1] / dp[i] * b[i];
+    up[i] = a[i + 1] / rp[i + 1] * b[i];
+  }
+  twisted_solve(n, k, lp.data(), up.data(), u, ldu);
+}
+
+}  // namespace
+
+extern "C" {
+
+int orc_negative_count(int n, const double* a, const double* b, double mu) {
+  return sturm_count(n, a, b, mu);
+}
+
+// Depth-first bisection over [lo, hi], upper half first, until the midpoint
+// no longer splits the interval (or the width is <= tol).  One value per
+// converged interval, descending, at most top_k.  bbtsvd.cpp:19-52.
+void orc_bisection(int n, const double* a, const double* b, double lo, double hi, double tol,
+                   int top_k, double* sigma, int* count) {
+  struct Node { double lo; int clo; double hi; int chi; };
+  const int clo = sturm_count(n, a, b, lo), chi = sturm_count(n, a, b, hi);
+  *count = 0;
+  if (!(clo <= chi && top_k > 0)) return;
+  std::vector<Node> st;
+  st.push_back({lo, clo, hi, chi});
+  while (!st.empty()) {
+    Node nd = st.back();
+    st.pop_back();
+    const double mid = (nd.lo + nd.hi) / 2;
+    if ((nd.hi - nd.lo) <= tol || mid == nd.lo || mid == nd.hi) {
+      sigma[(*count)++] = mid;
+      if (*count >= top_k) break;
+      continue;
+    }
+    const int cm = sturm_count(n, a, b, mid);
+    if (cm > nd.clo) st.push_back({nd.lo, nd.clo, mid, cm});
+    if (nd.chi > cm) st.push_back({mid, cm, nd.hi, nd.chi});
+  }
+}
+
+// LDL^T of B^T B.  bbtsvd.cpp:54-63.
+void orc_ldl(int n, const double* a, const double* b, double* L, double* D) {
+  D[0] = a[0] * a[0];
+  for (int i = 1; i < n; ++i) {
+    const double ab = a[i - 1] * b[i - 1];
+    L[i - 1] = ab / D[i - 1];
+    D[i] = a[i] * a[i] + b[i - 1] * b[i - 1] - (ab * ab) / D[i - 1];
+  }
+}
+
+// Vectors for `cnt` singular values: v_i in row i of V (cnt x n), u_i in
+// column i of U (n x cnt).  bbtsvd.cpp:138-147.
+void orc_twisted_vectors(int n, int cnt, const double* sigma, const double* a, const double* b,
+                         double* U, double* V) {
+  std::vector<double> L(n > 1 ? n - 1 : 1), D(n);
+  orc_ldl(n, a, b, L.data(), D.data());
+  for (int i = 0; i < cnt; ++i)
+    one_triplet(n, cnt, sigma[i], L.data(), D.data(), a, b, V + (size_t)i * n, U + i);
+}
+
+// Top-k bisection + twisted vectors + sign fixes.  bbtsvd.cpp:932-968.
+// Returns 0, or -1 where the reference asserts (fewer values than top_k).
+int orc_bidiagonal_svd(int k, const double* a, const double* b, double* U, double* V,
+                       double* sigma, int top_k) {
+  const double na = norm2(k, a, 1), nb = (k > 1) ? norm2(k - 1, b, 1) : 0.0;
+  const double bound = na * na + nb * nb;
+  int cnt = 0;
+  orc_bisection(k, a, b, 0.0, bound, 1e-20, top_k, sigma, &cnt);
+  if (cnt < top_k) return -1;
+  orc_twisted_vectors(k, top_k, sigma, a, b, U, V);
+  for (int i = 0; i < top_k; ++i) {
+    double* vi = V + (size_t)i * k;
+    const int p = argmax_abs(k, vi, 1);
+    double sg;
+    if (p == 0) sg = U[i] * a[0] / sigma[i];
+    else sg = (U[(size_t)(p - 1) * top_k + i] * b[p - 1] + U[(size_t)p * top_k + i] * a[p]) / sigma[i];
+    if (sg * vi[p] < 0)
+      for (int j = 0; j < k; ++j) vi[j] = -vi[j];
+  }
+  for (int i = 0; i < top_k; ++i) {
+    if (std::fabs(sigma[i] - a[i]) < 1e-15) {
+      U[(size_t)i + (size_t)i * top_k] = 1.0;
+      for (int j = i + 1; j < top_k; ++j) U[(size_t)i * top_k + j] = 0.0;
+      for (int j = i + 1; j < k; ++j) U[(size_t)j * top_k + i] = 0.0;
+      for (int j = 0; j < k; ++j) V[(size_t)i * k + j] = (j == i) ? 1.0 : 0.0;
+    }
+  }
+  return 0;
+}
+
+// Random Givens tables exactly as the reference draws them
+// (bbtsvd.cpp:729-779): per pass a std::shuffle of 0..k-1 with
+// std::default_random_engine(seed), an extra rand() partner when k is odd,
+// reversal for the inverse, pairs ordered (smaller, larger); then per pass
+// c, s = random_value(-1, 1) normalised.  Output per pass: `ops` index pairs
+// in application order and their c, s (s already signed for this
+// direction: x1' = c x1 + s x2, x2' = -s x1 + c x2).
+void orc_givens_tables(size_t k, size_t passes, int mask, unsigned seed, int32_t* pairs,
+                       double* c, double* s) {
+  srand(seed);
+  std::default_random_engine eng(seed);
+  const size_t ops = (k + (k & 1)) / 2;
+  std::vector<std::vector<size_t>> perm(passes);
+  for (size_t t = 0; t < passes; ++t) {
+    std::vector<size_t> idx(k);
+    for (size_t j = 0; j < k; ++j) idx[j] = j;
+    std::shuffle(idx.begin(), idx.end(), eng);
+    if (k & 1) {
+      idx.push_back(rand() % k);
+      while (idx[k] == idx[k - 1]) idx[k] = rand() % k;
+    }
+    if (!mask) std::reverse(idx.begin(), idx.end());
+    for (size_t j = 0; j < 2 * ops; j += 2)
+      if (idx[j] > idx[j + 1]) std::swap(idx[j], idx[j + 1]);
+    perm[t] = idx;
+  }
+  if (!mask) std::reverse(perm.begin(), perm.end());
+  std::vector<std::vector<double>> cc(passes), ss(passes);
+  for (size_t t = 0; t < passes; ++t) {
+    cc[t].assign(ops, 0.0);
+    ss[t].assign(ops, 0.0);
+    for (size_t j = 0; j < ops; ++j) {
+      cc[t][j] = (rand() / (double)RAND_MAX) * 2.0 + -1.0;
+      ss[t][j] = (rand() / (double)RAND_MAX) * 2.0 + -1.0;
+      const double r = pow(cc[t][j] * cc[t][j] + ss[t][j] * ss[t][j], 0.5);
+      cc[t][j] /= r;
+      ss[t][j] /= r;
+    }
+    if (!mask) {
+      std::reverse(cc[t].begin(), cc[t].end());
+      std::reverse(ss[t].begin(), ss[t].end());
+    }
+  }
+  if (!mask) {
+    std::reverse(cc.begin(), cc.end());
+    std::reverse(ss.begin(), ss.end());
+  }
+  for (size_t t = 0; t < passes; ++t)
+    for (size_t j = 0; j < ops; ++j) {
+      pairs[(t * ops + j) * 2] = (int32_t)perm[t][2 * j];
+      pairs[(t * ops + j) * 2 + 1] = (int32_t)perm[t][2 * j + 1];
+      c[t * ops + j] = cc[t][j];
+      s[t * ops + j] = (mask ? 1.0 : -1.0) * ss[t][j];
+    }
+}
+
+// Direct Givens mask of a row-major m x n matrix: rotates rows (is_left)
+// or columns.  bbtsvd.cpp:727-876.
+void orc_givens_mask(size_t m, size_t n, size_t passes, double* x, int mask, int is_left,
+                     unsigned seed) {
+  const size_t k = is_left ? m : n;
+  if (k <= 1) return;
+  const size_t ops = (k + (k & 1)) / 2;
+  std::vector<int32_t> pr(passes * ops * 2);
+  std::vector<double> c(passes * ops), s(passes * ops);
+  orc_givens_tables(k, passes, mask, seed, pr.data(), c.data(), s.data());
+  const size_t other = is_left ? n : m;
+  std::vector<double> vec(k);
+  for (size_t col = 0; col < other; ++col) {
+    for (size_t i = 0; i < k; ++i) vec[i] = is_left ? x[i * n + col] : x[col * n + i];
+    for (size_t t = 0; t < passes; ++t)
+      for (size_t j = 0; j < ops; ++j) {
+        const size_t q = t * ops + j;
+        const double x1 = vec[pr[2 * q]], x2 = vec[pr[2 * q + 1]];
+        const double cq = c[q], sq = s[q];
+        const double n1 = x1 * cq + x2 * sq;
+        const double n2 = x1 * (-sq) + x2 * cq;
+        vec[pr[2 * q]] = n1;
+        vec[pr[2 * q + 1]] = n2;
+      }
+    for (size_t i = 0; i < k; ++i) {
+      if (is_left) x[i * n + col] = vec[i];
+      else x[col * n + i] = vec[i];
+    }
+  }
+}
+
+// Near-square factorisation k - remain = rows * cols used by the large-k
+// mask path.  bbtsvd.cpp:166-188 (limit 10000, aspect ratio < 2).
+void orc_square_convert(size_t k, size_t* rows, size_t* cols, size_t* remain) {
+  const size_t lim = 10000;
+  size_t rem = 0;
+  for (;;) {
+    const size_t kk = k - rem;
+    size_t bm = kk, bn = 1;
+    for (size_t i = lim; i > 1; --i) {
+      if (kk % i) continue;
+      const size_t q = kk / i;
+      if (i > q && q < lim && q > 1 && (i - q) < (bm - bn) && ((double)i / (double)q) < 2) {
+        bm = i;
+        bn = q;
+      }
+    }
+    if (bm < lim) { *rows = bm; *cols = bn; *remain = rem; return; }
+    ++rem;
+  }
+}
+
+// Block-shift mask: direct Givens mask when the rotated dimension k <= 10000,
+// otherwise each vector is folded into a near-square virtual matrix
+// (Givens mask on both sides, cyclic row shift, remainder pass).
+// bbtsvd.cpp:533-669.
+void orc_block_shift_mask(size_t m, size_t n, size_t passes, double* x, int mask, int is_left,
+                          unsigned seed) {
+  srand(seed);
+  const size_t k = is_left ? m : n;
+  if (k <= 10000) {
+    orc_givens_mask(m, n, passes, x, mask, is_left, seed);
+    return;
+  }
+  size_t vm, vn, rem;
+  orc_square_convert(k, &vm, &vn, &rem);
+  const size_t body = k - rem;
+  const size_t nvec = is_left ? n : m;
+  const size_t stride = is_left ? n : 1;  // step between elements of one vector
+  std::vector<double> blk(body), sh(body), rb(rem + vm);
+  auto at = [&](size_t v, size_t i) -> double& { return x[v * (is_left ? 1 : n) + i * stride]; };
+  for (size_t v = 0; v < nvec; ++v) {
+    if (mask) {
+      for (size_t i = 0; i < body; ++i) blk[i] = at(v, i);
+      if (rem) {
+        for (size_t r = 0; r < vm; ++r) rb[r] = blk[r * vn];
+        for (size_t r = 0; r < rem; ++r) rb[vm + r] = at(v, body + r);
+        orc_givens_mask(1, rem + vm, passes, rb.data(), 1, 0, seed + 1000);
+        for (size_t r = 0; r < vm; ++r) blk[r * vn] = rb[r];
+      }
+      orc_givens_mask(vm, vn, passes, blk.data(), 1, 1, seed + 2000);
+      for (size_t r = 0; r < vm; ++r)
+        for (size_t q = 0; q < vn; ++q) {
+          long sft = ((long)q - (long)r) % (long)vn;
+          if (sft < 0) sft += (long)vn;
+          sh[r * vn + q] = blk[r * vn + (size_t)sft];
+        }
+      orc_givens_mask(vm, vn, passes, sh.data(), 1, 1, seed + 3000);
+      orc_givens_mask(vm, vn, passes, sh.data(), 1, 0, seed + 4000);
+      if (rem) {
+        for (size_t r = 0; r < vm; ++r) rb[r] = sh[r * vn];
+        orc_givens_mask(1, rem + vm, passes, rb.data(), 1, 0, seed + 5000);
+        for (size_t r = 0; r < vm; ++r) sh[r * vn] = rb[r];
+        for (size_t r = 0; r < rem; ++r) at(v, body + r) = rb[vm + r];
+      }
+      for (size_t i = 0; i < body; ++i) at(v, i) = sh[i];
+    } else {
+      for (size_t i = 0; i < body; ++i) sh[i] = at(v, i);
+      if (rem) {
+        for (size_t r = 0; r < rem; ++r) rb[vm + r] = at(v, body + r);
+        for (size_t r = 0; r < vm; ++r) rb[r] = sh[r * vn];
+        orc_givens_mask(1, rem + vm, passes, rb.data(), 0, 0, seed + 5000);
+        for (size_t r = 0; r < vm; ++r) sh[r * vn] = rb[r];
+      }
+      orc_givens_mask(vm, vn, passes, sh.data(), 0, 1, seed + 3000);
+      orc_givens_mask(vm, vn, passes, sh.data(), 0, 0, seed + 4000);
+      for (size_t r = 0; r < vm; ++r)
+        for (size_t q = 0; q < vn; ++q) blk[r * vn + q] = sh[r * vn + (q + r) % vn];
+      orc_givens_mask(vm, vn, passes, blk.data(), 0, 1, seed + 2000);
+      if (rem) {
+        for (size_t r = 0; r < vm; ++r) rb[r] = blk[r * vn];
+        orc_givens_mask(1, rem + vm, passes, rb.data(), 0, 0, seed + 1000);
+        for (size_t r = 0; r < vm; ++r) blk[r * vn] = rb[r];
+        for (size_t r = 0; r < rem; ++r) at(v, body + r) = rb[vm + r];
+      }
+      for (size_t i = 0; i < body; ++i) at(v, i) = blk[i];
+    }
+  }
+}
+
+// glibc srand/rand passthrough so tests can derive seeds the way the
+// reference's participants do (client.cpp:196, 498, 531).
+void orc_srand(unsigned s) { srand(s); }
+int orc_rand(void) { return rand(); }
+
+}  // extern "C"

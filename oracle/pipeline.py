@@ -1,0 +1,231 @@
+"""ORACLE — test infrastructure, not product code.
+
+numpy restatement of Excalibur's ``DecentralizedClient::run()`` for the
+short-and-wide branch (m <= global_n, ``src/client.cpp:570-606, 680-1199``),
+with all P participants held in one process.  The reference's socket
+collectives become plain array operations; its ``ring_all_reduce_sum``
+becomes a sum over participants in index order.
+
+Conventions (as in the reference): participant c holds X_c, a row-major
+m x local_n[c] float64 block; the global matrix is X = [X_0 | X_1 | ...].
+Outputs: sigma (descending), FinalU (m x k, row-major, every participant
+holds the same), FinalVT_c (k x local_n[c]) per participant, with
+X ~= FinalU diag(sigma) [FinalVT_0 | FinalVT_1 | ...].
+"""
+import numpy as np
+import scipy.linalg.lapack as lapack
+
+from . import bidiagonal_svd, block_shift_mask, negative_count
+
+LOCAL_QR_THRESHOLD = 5.0   # client.cpp:482
+MASK_PASSES = 32           # client.cpp:536
+
+
+def row_split(m, P):
+    """m_part / m_part_pos (client.cpp:613-624)."""
+    part = [m // P + (1 if i < m % P else 0) for i in range(P)]
+    pos = [0]
+    for p in part:
+        pos.append(pos[-1] + p)
+    return part, pos
+
+
+def reduced_width(m, local_n):
+    """Columns kept after the local QR: min(m, local_n) when the integer
+    ratio local_n/m exceeds 5 (client.cpp:505,510,517)."""
+    return min(m, local_n) if (local_n // m) > LOCAL_QR_THRESHOLD else local_n
+
+
+def local_qr(x):
+    """local_qr_reduction(local_n, m, ...) with compute_q (client.cpp:417-445):
+    dgeqrf of A = X_c^T (local_n x m, column-major = X_c row-major), Q by
+    dorgqr.  Returns (R^T as the new m x m block, Q^T as m x local_n)."""
+    A = np.asfortranarray(x.T)
+    qr, tau, _, info = lapack.dgeqrf(A)
+    assert info == 0
+    R = np.triu(qr[: x.shape[0], :])
+    Q, _, info = lapack.dorgqr(qr, tau)
+    assert info == 0
+    return R.T.copy(), np.ascontiguousarray(Q.T)
+
+
+def householder(alpha, x):
+    """dlarfg: H (alpha; x) = (beta; 0), H = I - tau (1; v)(1; v)^T."""
+    xn = np.linalg.norm(x)
+    if xn == 0.0:
+        return alpha, np.zeros_like(x), 0.0
+    beta = -np.copysign(np.hypot(alpha, xn), alpha)
+    tau = (beta - alpha) / beta
+    return beta, x / (alpha - beta), tau
+
+
+def drotg(a, b):
+    """Reference-BLAS drotg: returns (r, c, s) with r carrying the sign of
+    the larger-magnitude input."""
+    roe = b if abs(b) > abs(a) else a
+    scale = abs(a) + abs(b)
+    if scale == 0.0:
+        return 0.0, 1.0, 0.0
+    r = scale * np.sqrt((a / scale) ** 2 + (b / scale) ** 2)
+    r = np.copysign(1.0, roe) * r
+    return r, a / r, b / r
+
+
+def ralha(slabs):
+    """One-sided (Ralha) bidiagonalisation, overlapped variant
+    (client.cpp:829-910), of the m x m matrix whose column slabs are
+    ``slabs`` (participant c holds m x m_part[c]).  Returns lower-bidiagonal
+    alpha, beta, the Householder store (m x m, reflector j in column j from
+    row j, unit diagonal), tau (m), and the left vectors as per-participant
+    slabs (m x m_part[c])."""
+    W = [s.copy() for s in slabs]
+    m = W[0].shape[0]
+    house = np.zeros((m, m))
+    house[0, 0] = 1.0
+    tau = np.zeros(m)
+    alpha = np.zeros(m)
+    beta = np.zeros(max(m - 1, 1))
+    V = [np.zeros_like(w) for w in W]
+    alpha[0] = np.sqrt(sum(float(w[0] @ w[0]) for w in W))
+    for c in range(len(W)):
+        V[c][0] = W[c][0] / alpha[0]
+    for i in range(m - 2):
+        msg = np.zeros(m + 3 - i)
+        for w, v in zip(W, V):               # fixed-order in-process all-reduce
+            part = np.zeros(m + 3 - i)
+            part[: m - 1 - i] = w[i + 1:] @ w[i]
+            if i > 0:
+                part[m - i - 1] = w[i] @ v[i - 1]
+                part[m - i] = v[i - 1] @ v[i - 1]
+                part[m - i + 1] = w[i] @ w[i]
+                part[m - i + 2] = v[i - 1] @ w[i]
+            msg += part
+        g = msg[: m - 1 - i]
+        if i > 0:
+            beta[i - 1] = msg[m - i - 1]
+        _, vec, t = householder(g[0], g[1:])
+        house[i + 1, i + 1] = 1.0
+        house[i + 2:, i + 1] = vec
+        tau[i + 1] = t
+        h = house[i + 1:, i + 1]
+        for c in range(len(W)):
+            blk = W[c][i + 1:]
+            W[c][i + 1:] = blk - t * np.outer(h, h @ blk)
+        if i > 0:
+            b = beta[i - 1]
+            for c in range(len(W)):
+                W[c][i] = W[c][i] - b * V[c][i - 1]
+            alpha[i] = np.sqrt(msg[m - i] * b * b + msg[m - i + 1] - 2 * b * msg[m - i + 2])
+            for c in range(len(W)):
+                V[c][i] = W[c][i] / alpha[i]
+    for i in range(max(m - 2, 1), m):        # tail steps (client.cpp:897-905)
+        if i < 1:
+            continue
+        b = sum(float(w[i] @ v[i - 1]) for w, v in zip(W, V))
+        beta[i - 1] = b
+        for c in range(len(W)):
+            W[c][i] = W[c][i] - b * V[c][i - 1]
+        alpha[i] = np.sqrt(sum(float(w[i] @ w[i]) for w in W))
+        for c in range(len(W)):
+            V[c][i] = W[c][i] / alpha[i]
+    return alpha, beta[: m - 1], house, tau, V
+
+
+def lower_to_upper(alpha, beta):
+    """drotg sweep turning the lower bidiagonal upper (client.cpp:947-954)."""
+    a, b = alpha.copy(), beta.copy()
+    cs = np.zeros((len(a), 2))
+    for i in range(len(a) - 1):
+        r, c, s = drotg(a[i], b[i])
+        a[i] = r
+        cs[i] = (c, s)
+        b[i] = s * a[i + 1]
+        a[i + 1] = c * a[i + 1]
+    return a, b, cs
+
+
+def apply_house(house, tau, C):
+    """dormqr('L','N'): C <- H_0 H_1 ... H_{m-1} C with reflector j stored in
+    column j of ``house`` (unit diagonal)."""
+    m = house.shape[0]
+    C = C.copy()
+    for j in range(m - 1, -1, -1):
+        if tau[j] == 0.0:
+            continue
+        v = house[j:, j].copy()
+        v[0] = 1.0
+        C[j:] -= tau[j] * np.outer(v, v @ C[j:])
+    return C
+
+
+def run(blocks, public_seed, private_seeds, top_k=-1, return_stages=False):
+    """DecentralizedClient::run(), svd_mode 1 (two-sided), opt_control 3."""
+    P = len(blocks)
+    m = blocks[0].shape[0]
+    local_n = [b.shape[1] for b in blocks]
+    global_n = sum(local_n)
+    if m > global_n:
+        raise NotImplementedError("tall-and-skinny branch (m > global_n)")
+    red = [reduced_width(m, n) for n in local_n]
+    rg = sum(red)
+    if rg <= m:
+        raise ValueError("the V back-transform needs reduced_global_n > m (client.cpp:1179)")
+    stages = {}
+    masked, local_q = [], []
+    for c in range(P):                                            # client.cpp:572-605
+        x = np.ascontiguousarray(blocks[c], dtype=np.float64)
+        if m < local_n[c] and (local_n[c] // m) > LOCAL_QR_THRESHOLD:
+            r, q = local_qr(x)
+        else:
+            r, q = x.copy(), None
+        stages.setdefault("local_r", []).append(r.copy())
+        r = block_shift_mask(r, MASK_PASSES, True, True, public_seed)
+        r = block_shift_mask(r, MASK_PASSES, True, False, private_seeds[c])
+        masked.append(r)
+        local_q.append(q)
+    stages["masked"] = [x.copy() for x in masked]
+    M = np.concatenate(masked, axis=1)                            # m x rg, repartition :681-703
+    part, pos = row_split(m, P)
+    # global Householder QR of M^T (client.cpp:705-794), panel by panel in
+    # the reference; one dgeqrf here (same reflectors, up to rounding)
+    qr, tau_g, _, info = lapack.dgeqrf(np.asfortranarray(M.T))
+    assert info == 0
+    Rg = np.triu(qr[:m, :])
+    Qg, _, info = lapack.dorgqr(qr, tau_g)
+    assert info == 0
+    stages["global_r"] = Rg.copy()
+    slabs = [Rg[:, pos[c]:pos[c + 1]].copy() for c in range(P)]
+    alpha, beta, house, tau, Vr = ralha(slabs)                    # :801-945
+    stages["ralha_lower"] = (alpha.copy(), beta.copy())
+    a, b, cs = lower_to_upper(alpha, beta)                        # :947-954
+    stages["bidiagonal"] = (a.copy(), b.copy())
+    bound = np.linalg.norm(a) ** 2 + np.linalg.norm(b) ** 2       # :966-971
+    k = negative_count(a, b, bound) - negative_count(a, b, 0.0)
+    if top_k > 0:
+        k = min(k, top_k)
+    sigma, Ub, Vb = bidiagonal_svd(a, b, k)                       # :984
+    for i in range(k):                                            # :988-995
+        p = int(np.argmax(np.abs(Ub[:, i])))
+        if Ub[p, i] < 0:
+            Ub[:, i] = -Ub[:, i]
+            Vb[i] = -Vb[i]
+    stages["bsvd"] = (sigma.copy(), Ub.copy(), Vb.copy())
+    FinalU = np.zeros((m, k))                                     # :1007-1115
+    for c in range(P):
+        FinalU[pos[c]:pos[c + 1]] = (Vb @ Vr[c]).T
+    FinalU = block_shift_mask(FinalU, MASK_PASSES, False, True, public_seed)
+    U2 = Ub.copy()                                                # :1127-1128
+    for i in range(m - 2, -1, -1):
+        c_, s_ = cs[i]
+        x, y = U2[i].copy(), U2[i + 1].copy()
+        U2[i] = c_ * x - s_ * y
+        U2[i + 1] = c_ * y + s_ * x
+    U2 = apply_house(house, tau, U2)                              # :1176
+    rpos = np.concatenate([[0], np.cumsum(red)])
+    FinalVT = []
+    for c in range(P):
+        t = U2.T @ Qg[rpos[c]:rpos[c + 1], :].T                   # :1179
+        t = block_shift_mask(t, MASK_PASSES, False, False, private_seeds[c])
+        FinalVT.append(t @ local_q[c] if local_q[c] is not None else t)   # :1188-1195
+    out = (sigma, FinalU, FinalVT)
+    return (out + (stages,)) if return_stages else out

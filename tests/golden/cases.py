@@ -1,0 +1,77 @@
+"""Seeded inputs of the golden fixtures (shared by make_golden.py and the
+tests).  Shapes follow the reference's own conventions: a participant's block
+is row-major m x local_n (Excalibur client.hpp:39-44, generate_data.cpp)."""
+import numpy as np
+
+
+def bidiagonal_cases():
+    """name -> (alpha, beta, top_k)."""
+    out = {}
+    rng = np.random.default_rng(20240601)
+    for k in (1, 2, 3, 5, 31, 33, 100, 257):
+        a = rng.uniform(0.5, 2.0, k)
+        b = rng.uniform(-1.0, 1.0, k - 1)
+        out[f"rand_k{k}"] = (a, b, k)
+    a = rng.uniform(0.5, 2.0, 100)
+    b = rng.uniform(-1.0, 1.0, 99)
+    out["topk_k100_t10"] = (a, b, 10)
+    k = 64
+    a = np.geomspace(1.0, 1e-6, k) * rng.choice([-1.0, 1.0], k)
+    b = 0.3 * np.geomspace(1.0, 1e-6, k)[1:] * rng.choice([-1.0, 1.0], k - 1)
+    out["graded_signed_k64"] = (a, b, k)
+    centres = np.geomspace(1.0, 1e-3, 4)
+    a = np.concatenate([c * (1.0 + 1e-10 * np.arange(16)) for c in centres])
+    b = 1e-13 * rng.uniform(-1.0, 1.0, 63)
+    out["cluster_k64"] = (a, b, 64)
+    return out
+
+
+def sturm_shifts(a, b):
+    k = len(a)
+    B = np.diag(a) + (np.diag(b, 1) if k > 1 else 0)
+    s = np.linalg.svd(np.atleast_2d(B), compute_uv=False)
+    bound = np.linalg.norm(a) ** 2 + (np.linalg.norm(b) ** 2 if k > 1 else 0.0)
+    rng = np.random.default_rng(k)
+    mus = np.concatenate([[0.0, bound, s.max() * 1.5], s, rng.uniform(0, s.max(), 16)])
+    return mus.astype(np.float64)
+
+
+def mask_cases():
+    """name -> (x, passes, mask, is_left, seed, fn)."""
+    out = {}
+    rng = np.random.default_rng(7)
+    shapes = [
+        ("sq100_left", (100, 100), 1, 1, 11, "givens"),
+        ("sq100_right", (100, 100), 1, 0, 12, "givens"),
+        ("sq100_left_unmask", (100, 100), 0, 1, 11, "givens"),
+        ("wide_right", (37, 1000), 1, 0, 13, "givens"),
+        ("tall_left", (1000, 37), 1, 1, 14, "givens"),
+        ("odd_left", (33, 17), 1, 1, 15, "givens"),
+        ("odd_right", (17, 33), 1, 0, 16, "givens"),
+        ("odd_left_unmask", (33, 17), 0, 1, 15, "givens"),
+        ("odd_right_unmask", (17, 33), 0, 0, 16, "givens"),
+        ("k2_left", (2, 9), 1, 1, 17, "givens"),
+        ("k3_right", (6, 3), 1, 0, 18, "givens"),
+        ("tail_left", (5, 7), 1, 1, 19, "givens"),
+        ("bsm_direct", (64, 48), 1, 1, 20, "block_shift"),
+        ("bsm_virtual_rem", (1, 10007), 1, 0, 21, "block_shift"),
+        ("bsm_virtual_rem_unmask", (1, 10007), 0, 0, 21, "block_shift"),
+        ("bsm_virtual_exact", (2, 10240), 1, 0, 22, "block_shift"),
+        ("bsm_virtual_left", (10009, 2), 1, 1, 23, "block_shift"),
+    ]
+    for name, shp, mask, left, seed, fn in shapes:
+        out[name] = (rng.standard_normal(shp), 32, mask, left, seed, fn)
+    return out
+
+
+def pipeline_cases():
+    """name -> (blocks, seed).  ``c1`` is the 2 x (1000 x 100) N(0,1) case
+    (row-stacked 2000 x 100), held as the reference's m=100 x local_n=1000."""
+    out = {}
+    rng = np.random.default_rng(0)
+    out["c1"] = ([rng.standard_normal((1000, 100)).T.copy() for _ in range(2)], 0)
+    rng = np.random.default_rng(5)
+    out["p3_uneven"] = ([rng.standard_normal((48, n)) for n in (400, 290, 150)], 5)
+    rng = np.random.default_rng(9)
+    out["noqr"] = ([rng.standard_normal((40, n)) for n in (160, 200)], 9)
+    return out

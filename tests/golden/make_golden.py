@@ -1,0 +1,161 @@
+"""Generate the golden fixtures in tests/golden/ from the REFERENCE itself.
+
+Runs the reference's own sources, compiled by ``make -C oracle ref`` from
+the Excalibur checkout (default /root/reference; override with
+EXCALIBUR_REF), never the oracle restatement:
+
+* ``oracle/_ref/libref_capi.so``: the reference's bbtsvd.hpp functions
+  (negative_count, bisection_singular_values,
+  bidiagonal_bisection_twisted_svd, givens_mask_..._with_simd,
+  block_shift_mask) called through extern "C" wrappers;
+* ``oracle/_ref/ref_pipeline``: one reference participant
+  (DecentralizedClient::run(), svd_mode 1, opt 3) per process over
+  loopback TCP, P processes per case.
+
+Inputs are regenerated from numpy seeds; each fixture stores a SHA-256 of
+its inputs so a test can tell a changed generator from a changed result.
+
+Usage:  python tests/golden/make_golden.py   (needs the reference checkout)
+"""
+import ctypes as C
+import hashlib
+import os
+import random
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+REF = os.environ.get("EXCALIBUR_REF", "/root/reference")
+REFDIR = os.path.join(ROOT, "oracle", "_ref")
+
+
+def sha(*arrays):
+    h = hashlib.sha256()
+    for a in arrays:
+        h.update(np.ascontiguousarray(a).tobytes())
+    return h.hexdigest()
+
+
+def p(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+# ---------------------------------------------------------------------------
+# inputs (shared with the tests through tests/golden/cases.py)
+sys.path.insert(0, HERE)
+import cases  # noqa: E402
+
+
+def blas_bound(a, b):
+    """The bisection bound exactly as the reference forms it
+    (bbtsvd.cpp:936): ||alpha||^2 + ||beta||^2 with the BLAS dnrm2 it links
+    (here scipy's OpenBLAS, the library oracle/_ref links)."""
+    import glob
+    import scipy
+    lib = glob.glob(os.path.join(os.path.dirname(os.path.dirname(scipy.__file__)), "scipy.libs",
+                                 "libscipy_openblas-*.so"))[0]
+    B = C.CDLL(lib)
+    B.scipy_cblas_dnrm2.restype = C.c_double
+    B.scipy_cblas_dnrm2.argtypes = [C.c_int, C.c_void_p, C.c_int]
+    a = np.ascontiguousarray(a)
+    b = np.ascontiguousarray(b if len(b) else np.zeros(1))
+    na = B.scipy_cblas_dnrm2(len(a), p(a), 1)
+    nb = B.scipy_cblas_dnrm2(len(a) - 1, p(b), 1)
+    return na * na + nb * nb
+
+
+def bidiagonal_fixtures(R):
+    out = {}
+    for name, (a, b, top_k) in cases.bidiagonal_cases().items():
+        k = len(a)
+        U = np.zeros(k * top_k)
+        V = np.zeros(top_k * k)
+        s = np.zeros(k)
+        aa, bb = a.copy(), (b.copy() if k > 1 else np.zeros(1))
+        R.ref_bidiagonal_svd(C.c_int(k), p(aa), p(bb), p(U), p(V), p(s), C.c_int(top_k))
+        mus = cases.sturm_shifts(a, b)
+        counts = np.array([R.ref_negative_count(C.c_int(k), p(aa), p(bb), C.c_double(mu)) for mu in mus],
+                          dtype=np.int32)
+        out[name] = dict(alpha=a, beta=b, top_k=np.int32(top_k), sigma=s[:top_k],
+                         bound=np.float64(blas_bound(a, b)),
+                         U=U.reshape(k, top_k), V=V.reshape(top_k, k), mus=mus, counts=counts)
+    return out
+
+
+def mask_fixtures(R):
+    out = {}
+    for name, (x, passes, mask, is_left, seed, fn) in cases.mask_cases().items():
+        y = np.ascontiguousarray(x.copy())
+        m, n = y.shape
+        f = R.ref_givens_mask if fn == "givens" else R.ref_block_shift_mask
+        f(C.c_size_t(m), C.c_size_t(n), C.c_size_t(passes), p(y), C.c_int(mask), C.c_int(is_left),
+          C.c_uint(seed))
+        out[name] = dict(x_sha=sha(x), shape=np.array(x.shape), passes=np.int32(passes),
+                         mask=np.int32(mask), is_left=np.int32(is_left), seed=np.uint32(seed),
+                         fn=np.array(fn), y=y)
+    return out
+
+
+def run_reference_pipeline(blocks, seed, mode=1, topk=-1):
+    """P reference processes over loopback; returns (sigma, FinalU, [FinalVT_c],
+    alpha_beta_c0, run_seconds_per_participant)."""
+    P = len(blocks)
+    m = blocks[0].shape[0]
+    with tempfile.TemporaryDirectory() as td:
+        port = random.randint(20000, 40000)
+        procs = []
+        for c, x in enumerate(blocks):
+            np.ascontiguousarray(x, dtype=np.float64).tofile(os.path.join(td, f"Client{c}.mat"))
+        env = dict(os.environ, OMP_NUM_THREADS=str(max(1, (os.cpu_count() or 2) // P)))
+        for c, x in enumerate(blocks):
+            od = os.path.join(td, f"out{c}")
+            os.makedirs(od)
+            procs.append(subprocess.Popen(
+                [os.path.join(REFDIR, "ref_pipeline"), str(c), str(P), str(m), str(x.shape[1]),
+                 str(port), td, td, str(seed), str(mode), str(topk), od],
+                stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL, env=env, cwd=td))
+        for pr in procs:
+            if pr.wait(timeout=600) != 0:
+                raise RuntimeError("reference participant failed")
+        sig = np.fromfile(os.path.join(td, "out0", "sigma.bin"))
+        k = len(sig)
+        U = np.fromfile(os.path.join(td, "out0", "U.bin")).reshape(m, k)
+        VT = [np.fromfile(os.path.join(td, f"out{c}", "VT.bin")).reshape(k, blocks[c].shape[1])
+              for c in range(P)]
+        ab = np.fromfile(os.path.join(td, "out0", "ab.bin"))
+        secs = [float(open(os.path.join(td, f"out{c}", "time.txt")).read().split()[0]) for c in range(P)]
+    return sig, U, VT, ab, secs
+
+
+def pipeline_fixtures():
+    out = {}
+    for name, (blocks, seed) in cases.pipeline_cases().items():
+        sig, U, VT, ab, secs = run_reference_pipeline(blocks, seed)
+        d = dict(x_sha=sha(*blocks), seed=np.uint32(seed), sigma=sig, U=U, ab=ab)
+        for c, v in enumerate(VT):
+            d[f"VT{c}"] = v
+        out[name] = d
+    return out
+
+
+def main():
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref", f"REF={REF}"], check=True)
+    R = C.CDLL(os.path.join(REFDIR, "libref_capi.so"))
+    R.ref_negative_count.restype = C.c_int
+    R.ref_set_threads(1)
+    fx = {}
+    for grp, d in (("bidiag", bidiagonal_fixtures(R)), ("mask", mask_fixtures(R)),
+                   ("pipe", pipeline_fixtures())):
+        for name, arrs in d.items():
+            fx[f"{grp}__{name}"] = arrs
+    for key, arrs in fx.items():
+        np.savez_compressed(os.path.join(HERE, f"{key}.npz"), **arrs)
+    print(f"wrote {len(fx)} fixtures to {HERE}")
+
+
+if __name__ == "__main__":
+    main()
