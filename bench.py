@@ -1,0 +1,366 @@
+"""Benchmark: decentralized SVD wall time on one B200 (per replica).
+
+Workload (default): 2 participants, each holding a 500,000 x 1,000 FP64
+block of X = U diag(s) V^T (U 10^6 x 1000 and V 1000 x 1000 Haar-random,
+seeded; s geometric from 1 to 1e-6) — the reference's short-and-wide branch
+with m = 1000 and local_n = 500,000.  One step is the whole pipeline
+(local QR, masks, global QR, Ralha bidiagonalisation, bisection + twisted
+vectors, back-transforms) on inputs resident in HBM; the 8 GB inputs are
+larger than L2, and are restored from a pristine device copy before every
+step (outside the timed events).
+
+Prints one JSON line (rank 0).  --impl reference times the reference's own
+CPU implementation (oracle/_ref, built from the reference's sources) on a
+bounded sample of the same workload.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+CONFIGS = {
+    # name: (participants, m, local_n, spectrum)
+    "c2": (2, 1000, 500_000, "geometric"),
+    "c1": (2, 100, 1000, "gaussian"),
+}
+METRIC = "SVD wall-s at rel err <=1e-10 vs FP64 oracle"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--config", default="c2", choices=sorted(CONFIGS))
+    p.add_argument("--rows", type=int, default=0, help="override local_n (smaller runs)")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--cpu-sample-rows", type=int, default=50_000)
+    return p.parse_args()
+
+
+# ---------------------------------------------------------------- clocks
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, gpu):
+        self.gpu, self.samples, self.stop = gpu, [], threading.Event()
+
+    def _run(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        while not self.stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                self.samples.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self.stop.wait(0.2)
+
+    def __enter__(self):
+        self.t = threading.Thread(target=self._run, daemon=True)
+        self.t.start()
+        return self
+
+    def __exit__(self, *a):
+        self.stop.set()
+        self.t.join(timeout=10)
+
+    def summary(self):
+        sm = [float(s[0]) for s in self.samples if s and s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if len(s) > 1 and s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4)
+                          if len(s) > 3 + i and s[3 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+# ---------------------------------------------------------------- data
+def make_blocks(torch, dev, P, m, n, spectrum, seed=0):
+    """Participant blocks X_c (m x n row-major), X = [X_0 | X_1 | ...]."""
+    g = torch.Generator(device=dev).manual_seed(seed)
+    if spectrum == "gaussian":
+        return [torch.randn(m, n, generator=g, device=dev, dtype=torch.float64) for _ in range(P)], None
+    G = torch.randn(P * n, m, generator=g, device=dev, dtype=torch.float64)
+    Q, R = torch.linalg.qr(G)
+    Q *= torch.sign(torch.diagonal(R))
+    del G, R
+    H = torch.randn(m, m, generator=g, device=dev, dtype=torch.float64)
+    V, R = torch.linalg.qr(H)
+    V *= torch.sign(torch.diagonal(R))
+    s = torch.logspace(0, -6, m, dtype=torch.float64, device=dev)
+    # row-stacked X_s = Q diag(s) V^T; participant c holds (rows of c)^T = V diag(s) Q_c^T
+    blocks = [(V * s) @ Q[c * n:(c + 1) * n].T for c in range(P)]
+    del Q
+    return [b.contiguous() for b in blocks], s
+
+
+def fp64_oracle(torch, blocks):
+    """FP64 SVD of the stored X on the GPU (cuSOLVER QR + SVD): the
+    measurement's accuracy oracle, not part of the timed path."""
+    X = torch.cat(blocks, dim=1)                 # m x global_n
+    R = torch.linalg.qr(X.T, mode="r")[1]        # X^T = Q R  ->  X = R^T Q^T
+    Ur, s, Vh = torch.linalg.svd(R.T)
+    return s, Ur
+
+
+def accuracy(torch, s_ref, U_ref, s, U):
+    k = min(len(s), len(s_ref))
+    rel = (s[:k] - s_ref[:k]).abs() / s_ref[:k]
+    # gap-aware per-vector angles of the left singular vectors, sine form:
+    # sin(angle) = || u - (u_ref . u) u_ref || (arccos of the cosine bottoms
+    # out near 1.5e-8 in FP64)
+    d = (U_ref[:, :k] * U[:, :k]).sum(dim=0)
+    ang = torch.linalg.vector_norm(U[:, :k] - U_ref[:, :k] * d, dim=0).clamp(max=1.0).arcsin()
+    gap = torch.full_like(s_ref[:k], float("inf"))
+    gap[1:] = torch.minimum(gap[1:], s_ref[:k - 1] - s_ref[1:k])
+    gap[:-1] = torch.minimum(gap[:-1], s_ref[:k - 1] - s_ref[1:k])
+    well = (2.2e-16 * s_ref[0] / gap) <= 1e-10
+    return {"sigma_rel_err_max": float(rel.max()), "sigma_count": int(len(s)),
+            "u_angle_max_well_posed": float(ang[well].max()) if bool(well.any()) else None,
+            "u_angle_max_all": float(ang.max())}
+
+
+# ---------------------------------------------------------------- reference arm
+def reference_run(P, m, n, seed=0, threads=None, workdir=None):
+    """One run of the reference's own pipeline (oracle/_ref/ref_pipeline, P
+    processes over loopback TCP).  Returns (max run seconds over participants,
+    per-phase seconds of participant 0)."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_pipeline")
+    if not os.path.exists(exe):
+        raise FileNotFoundError(exe)
+    cores = os.cpu_count() or 1
+    threads = threads or max(1, cores // P)
+    rng = np.random.default_rng(seed)
+    with tempfile.TemporaryDirectory(dir=workdir) as td:
+        for c in range(P):
+            rng.standard_normal((m, n)).tofile(os.path.join(td, f"Client{c}.mat"))
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads), OPENBLAS_NUM_THREADS=str(threads))
+        port = 20000 + (os.getpid() * 7 + int(time.time())) % 20000
+        procs = []
+        for c in range(P):
+            od = os.path.join(td, f"o{c}")
+            os.makedirs(od)
+            procs.append(subprocess.Popen([exe, str(c), str(P), str(m), str(n), str(port), td, td, "0", "1", "-1", od],
+                                          stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL, env=env, cwd=td))
+        for pr in procs:
+            if pr.wait(timeout=1800) != 0:
+                raise RuntimeError("reference participant failed")
+        times = [list(map(float, open(os.path.join(td, f"o{c}", "time.txt")).read().split())) for c in range(P)]
+    total = max(t[0] for t in times)
+    ph = times[0]
+    phases = dict(zip(("total", "local_qr", "global_qr", "apply_mask", "exchange", "bi_diag", "bsvd", "combine",
+                       "comm"), ph))
+    return total, phases, threads * P
+
+
+def reference_extrapolated(P, m, n_full, n_sample, steps=1, seed=0):
+    """Reference time on a bounded sample (local_n = n_sample), extrapolated to
+    local_n = n_full: the phases whose work grows with local_n (local QR, the
+    V back-transform in combine) scale by n_full/n_sample, the m-sized
+    phases (masks, global QR, Ralha, bisection) are kept."""
+    vals = []
+    for i in range(steps):
+        total, ph, cores = reference_run(P, m, n_sample, seed=seed + i)
+        scale = n_full / n_sample
+        grow = ph["local_qr"] + ph["combine"]
+        vals.append(total + grow * (scale - 1.0))
+    return statistics.median(vals), cores, ph
+
+
+# ---------------------------------------------------------------- our arm
+def cublas_dgemm_peak(torch, dev):
+    a = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
+    b = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
+    for _ in range(2):
+        a @ b
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        a @ b
+        e1.record()
+        torch.cuda.synchronize()
+        best = max(best, 2 * 8192 ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    return best
+
+
+def run_ours(args, rank, world):
+    import torch
+    import excalibur_b200 as eb
+    P, m, n, spectrum = CONFIGS[args.config]
+    if args.rows:
+        n = args.rows
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    ctx = eb.Context(dev.index)
+    blocks, s_gen = make_blocks(torch, dev, P, m, n, spectrum, seed=0)
+    pristine = [b.clone() for b in blocks]
+    s_ref, U_ref = fp64_oracle(torch, pristine)
+    pub, priv = eb.reference_seeds(0, P)
+
+    def step():
+        for b, p0 in zip(blocks, pristine):
+            b.copy_(p0)
+        torch.cuda.synchronize()
+        return ctx.fedsvd(blocks, pub, priv)
+
+    for _ in range(args.warmup):
+        out = step()
+    acc = accuracy(torch, s_ref, U_ref, out[0], out[1])
+    del out
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    l0 = ctx.launches()
+    times = []
+    stage = {}
+    ctx.profile(True)
+    with Clocks(dev.index) as clk:
+        for _ in range(args.steps):
+            for b, p0 in zip(blocks, pristine):
+                b.copy_(p0)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            out = ctx.fedsvd(blocks, pub, priv)      # synchronises before returning
+            times.append(time.perf_counter() - t0)
+            for kk, v in ctx.stage_ms().items():
+                stage[kk] = stage.get(kk, 0.0) + v / args.steps
+            del out
+    prof = ctx.profile_get()
+    ctx.profile(False)
+    launches = (ctx.launches() - l0) // args.steps
+    torch.cuda.synchronize()
+    # device time of a step = sum of its stage events (CUDA events on the stream)
+    dev_ms = sum(stage.values())
+    sec = dev_ms / 1e3
+    if world > 1:
+        t = torch.tensor([sec], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        sec = float(t)
+    res = {"sec": sec, "host_sec": statistics.median(times), "stage_ms": stage, "acc": acc,
+           "launches": launches, "prof": prof, "clocks": clk.summary()}
+    if rank == 0:
+        res["dgemm_peak"] = cublas_dgemm_peak(torch, dev)
+    if not args.no_e2e:
+        # end to end through the host-pointer C-ABI entry: pinned host inputs,
+        # H2D + pipeline + D2H inside the timed call
+        hb = [p0.cpu().pin_memory().numpy() for p0 in pristine]
+        del blocks
+        torch.cuda.empty_cache()
+        outbuf = (torch.empty(m, dtype=torch.float64).pin_memory().numpy(),
+                  torch.empty(m * m, dtype=torch.float64).pin_memory().numpy(),
+                  [torch.empty(m * nn, dtype=torch.float64).pin_memory().numpy() for nn in [n] * P])
+        ctx.fedsvd_host(hb, pub, priv, out=outbuf)     # warm
+        et = []
+        for _ in range(max(1, min(args.steps, 3))):
+            t0 = time.perf_counter()
+            sg, Ug, VTg = ctx.fedsvd_host(hb, pub, priv, out=outbuf)
+            et.append(time.perf_counter() - t0)
+        k = len(sg)
+        res["e2e"] = {"value": statistics.median(et), "unit": "s", "h2d_bytes_per_step": int(sum(h.nbytes for h in hb)),
+                      "d2h_bytes_per_step": int(8 * (k + m * k + k * n * P))}
+    return res
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    P, m, n, spectrum = CONFIGS[args.config]
+    if args.rows:
+        n = args.rows
+    workload = f"{args.config}: {P} participants x {n} x {m} FP64 (reference m={m}, local_n={n})"
+    cfg = {"workload": workload, "participants": P, "m": m, "local_n": n, "spectrum": spectrum,
+           "mode": "svd_mode 1 (two-sided), opt_control 3, full spectrum",
+           "l2": "inputs (%.1f GB) larger than L2; restored from a device copy before each step" % (P * m * n * 8 / 1e9),
+           "parallelism": "replicas only" if args.gpus > 1 else "1 GPU"}
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        ns = min(args.cpu_sample_rows, n)
+        vals = []
+        for i in range(args.warmup + args.steps):
+            v, cores, ph = reference_extrapolated(P, m, n, ns, steps=1, seed=i)
+            if i >= args.warmup:
+                vals.append(v)
+        val = statistics.median(vals)
+        sample = (f"reference pipeline (oracle/_ref, its own sources) at local_n={ns}; local QR and "
+                  f"back-transform phases scaled by {n}/{ns}")
+        print(json.dumps({"impl": "reference", "metric": METRIC, "value": val, "unit": "s", "n_gpus": args.gpus,
+                          "steps": args.steps, "warmup": args.warmup, "ms_per_step": val * 1e3,
+                          "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                          "data": "synthetic", "config": cfg,
+                          "cpu_baseline": {"value": val, "unit": "s", "cores": cores, "kind": "reference",
+                                           "sample": sample},
+                          "e2e": {"value": val, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        return
+    if world > 1:
+        import torch
+        torch.distributed.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    res = run_ours(args, rank, world)
+    if world > 1:
+        import torch
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank != 0:
+        return
+    # dominant kernel class by event time
+    prof = res["prof"]
+    dom = max(prof, key=lambda k: prof[k][0])
+    ms, nl, work = prof[dom]
+    if dom in ("dgemm",):
+        achieved = work / (ms * 1e-3) / 1e12
+        peak = res["dgemm_peak"]
+        roof = {"kernel": "dgemm_kernel (DMMA m8n8k4 FP64)", "bound": "tensor", "achieved": achieved, "peak": peak,
+                "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 figure)",
+                "launches": nl, "share": ms / sum(v[0] for v in prof.values())}
+    else:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+            os.path.join(ROOT, "MEASURED_PEAKS.json")) else {"hbm_gbs": 6650.0}
+        achieved = work / (ms * 1e-3) / 1e9 if work else 0.0
+        roof = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": achieved / peaks["hbm_gbs"], "traffic": None, "launches": nl,
+                "share": ms / sum(v[0] for v in prof.values())}
+    line = {"metric": METRIC, "value": res["sec"], "unit": "s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": res["sec"] * 1e3, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
+            "accuracy": res["acc"], "stage_ms": res["stage_ms"], "host_s_per_step": res["host_sec"],
+            "gpu_launches": res["launches"], "roofline": roof,
+            "kernel_classes": {k: {"ms": v[0], "launches": v[1]} for k, v in prof.items()},
+            "clocks": res["clocks"]}
+    if "e2e" in res:
+        line["e2e"] = res["e2e"]
+    if not args.no_cpu_baseline:
+        ns = min(args.cpu_sample_rows, n)
+        try:
+            v, cores, ph = reference_extrapolated(P, m, n, ns, steps=1)
+            line["cpu_baseline"] = {"value": v, "unit": "s", "cores": cores, "kind": "reference",
+                                    "sample": f"reference pipeline at local_n={ns}, local QR and back-transform "
+                                              f"phases scaled by {n}/{ns}", "sample_phases_s": ph}
+        except Exception as e:   # the checker build is missing on this machine
+            line["cpu_baseline"] = {"value": None, "unit": "s", "cores": os.cpu_count(), "kind": "reference",
+                                    "sample": f"unavailable: {e}"}
+    print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

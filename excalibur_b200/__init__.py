@@ -1,0 +1,270 @@
+"""excalibur_b200 — Excalibur's matrix-factorisation hot path on B200 (sm_100a).
+
+Python mirror of the reference's API (Excalibur include/bbtsvd.hpp and the
+math inline in DecentralizedClient::run()), calling the CUDA kernels of
+libexcalibur_b200.so through its C ABI (include/bbtsvd_b200.h).  Device
+arrays are torch CUDA tensors (float64, contiguous); numpy arrays are copied
+to the device and results copied back.  There is no CPU path: every method
+raises if the library or a GPU is missing.
+
+    ctx = Context(0)
+    sigma, U, V = ctx.bidiagonal_bisection_twisted_svd(alpha, beta, top_k)
+    ctx.block_shift_mask(x, 32, mask=True, is_left=True, seed=s)
+    sigma, U, VT = ctx.fedsvd(blocks, public_seed, private_seeds)
+"""
+import ctypes as C
+
+import numpy as np
+
+from ._lib import BBT_OK, STATUS, FedSVDConfig, load
+
+__all__ = ["Context", "BBTError", "load", "reference_seeds"]
+
+
+class BBTError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        raise RuntimeError("excalibur_b200 needs a CUDA GPU (no CPU fallback)")
+    return torch
+
+
+def reference_seeds(seed, participants):
+    """(public_seed, [private_seed]) as the reference's participants derive
+    them from a shared --seed with glibc rand() (client.cpp:196, 498, 531):
+    participant 0 draws the public seed then its private seed; every other
+    participant's first draw is its private seed."""
+    libc = C.CDLL("libc.so.6")
+    libc.srand(C.c_uint(seed))
+    r1 = libc.rand() & 0xFFFFFFFF
+    r2 = libc.rand() & 0xFFFFFFFF
+    return r1, [r2] + [r1] * (participants - 1)
+
+
+class Context:
+    """A bbt_ctx: one CUDA stream, a device workspace, error text."""
+
+    def __init__(self, device=0):
+        self.torch = _torch()
+        self.L = load()
+        self.device = device
+        self.torch.cuda.set_device(device)
+        h = C.c_void_p()
+        self._check(self.L.bbt_create(C.byref(h), device), "bbt_create")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.bbt_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- helpers -----------------------------------------------------------
+    def _check(self, st, what):
+        if st != BBT_OK:
+            msg = self.L.bbt_last_error(self.h).decode() if getattr(self, "h", None) else what
+            raise BBTError(st, f"{what}: {msg}")
+
+    def _dev(self, x, dtype=None):
+        """torch CUDA float64 contiguous tensor (copy of numpy input)."""
+        t = self.torch
+        dtype = dtype or t.float64
+        if isinstance(x, t.Tensor):
+            assert x.is_cuda and x.dtype == dtype and x.is_contiguous(), "need a contiguous CUDA tensor"
+            return x
+        return t.as_tensor(np.ascontiguousarray(x), dtype=dtype, device=f"cuda:{self.device}")
+
+    def _empty(self, *shape, dtype=None):
+        t = self.torch
+        return t.empty(*shape, dtype=dtype or t.float64, device=f"cuda:{self.device}")
+
+    def sync(self):
+        self._check(self.L.bbt_synchronize(self.h), "synchronize")
+
+    def launches(self):
+        return int(self.L.bbt_kernel_launches(self.h))
+
+    @staticmethod
+    def _p(t):
+        return C.c_void_p(t.data_ptr())
+
+    def _pre(self):
+        self.torch.cuda.synchronize(self.device)   # inputs written by torch are complete
+
+    # -- bbtsvd.hpp ---------------------------------------------------------
+    def negative_count(self, alpha, beta, mu):
+        """Sturm counts at every shift in mu (bbtsvd.cpp:7-17)."""
+        a, b = self._dev(alpha), self._dev(beta if len(beta) else np.zeros(1))
+        mus = self._dev(np.atleast_1d(np.asarray(mu, dtype=np.float64)))
+        out = self._empty(mus.numel(), dtype=self.torch.int32)
+        self._pre()
+        self._check(self.L.bbt_negative_count(self.h, a.numel(), self._p(a), self._p(b), self._p(mus),
+                                              mus.numel(), self._p(out)), "negative_count")
+        self.sync()
+        return out.cpu().numpy()
+
+    def bisection_singular_values(self, alpha, beta, lo, hi, tol=1e-20, top_k=None):
+        """Singular values by the reference's bisection tree (bbtsvd.cpp:19-52)."""
+        a, b = self._dev(alpha), self._dev(beta if len(beta) else np.zeros(1))
+        n = a.numel()
+        top_k = n if top_k is None else top_k
+        s = self._empty(max(n, 1))
+        cnt = C.c_int(0)
+        self._pre()
+        self._check(self.L.bbt_bisection(self.h, n, self._p(a), self._p(b), lo, hi, tol, top_k, self._p(s),
+                                         C.byref(cnt)), "bisection")
+        self.sync()
+        return s[: cnt.value]
+
+    def two_side_singular_vectors_twisted_factorization(self, alpha, beta, sigma):
+        """(U n x cnt, V cnt x n) for given singular values (bbtsvd.cpp:138-147)."""
+        a, b = self._dev(alpha), self._dev(beta if len(beta) else np.zeros(1))
+        s = self._dev(sigma)
+        n, c = a.numel(), s.numel()
+        U = self._empty(n, c)
+        V = self._empty(c, n)
+        self._pre()
+        self._check(self.L.bbt_twisted_vectors(self.h, n, c, self._p(s), self._p(a), self._p(b), self._p(U),
+                                               self._p(V)), "twisted_vectors")
+        self.sync()
+        return U, V
+
+    def bidiagonal_bisection_twisted_svd(self, alpha, beta, top_k=None):
+        """(sigma, U k x top_k, V top_k x k) (bbtsvd.cpp:932-968)."""
+        a, b = self._dev(alpha), self._dev(beta if len(beta) else np.zeros(1))
+        k = a.numel()
+        top_k = k if top_k is None else top_k
+        U = self._empty(k, top_k)
+        V = self._empty(top_k, k)
+        s = self._empty(top_k)
+        self._pre()
+        self._check(self.L.bbt_bidiagonal_svd(self.h, k, self._p(a), self._p(b), self._p(U), self._p(V),
+                                              self._p(s), top_k), "bidiagonal_svd")
+        self.sync()
+        return s, U, V
+
+    def givens_mask_cache_optimized_parallel_with_simd(self, x, mask_times, mask, is_left, seed):
+        """In place on x (m x n row-major CUDA tensor) (bbtsvd.cpp:727-876)."""
+        x = self._dev(x) if not isinstance(x, self.torch.Tensor) else x
+        m, n = x.shape
+        self._pre()
+        self._check(self.L.bbt_givens_mask(self.h, m, n, mask_times, self._p(x), int(bool(mask)),
+                                           int(bool(is_left)), seed), "givens_mask")
+        self.sync()
+        return x
+
+    def block_shift_mask(self, x, mask_times, mask, is_left, seed):
+        """In place on x (m x n row-major CUDA tensor) (bbtsvd.cpp:533-669)."""
+        x = self._dev(x) if not isinstance(x, self.torch.Tensor) else x
+        m, n = x.shape
+        self._pre()
+        self._check(self.L.bbt_block_shift_mask(self.h, m, n, mask_times, self._p(x), int(bool(mask)),
+                                                int(bool(is_left)), seed), "block_shift_mask")
+        self.sync()
+        return x
+
+    # -- client.cpp -----------------------------------------------------------
+    def local_qr_reduction(self, x, compute_q=True):
+        """Householder QR of X^T for X (m x local_n row-major, CUDA tensor,
+        overwritten by Q^T when compute_q).  Returns R^T (m x m)
+        (client.cpp:417-445)."""
+        m, n = x.shape
+        rt = self._empty(m, m)
+        self._pre()
+        self._check(self.L.bbt_local_qr(self.h, m, n, self._p(x), self._p(rt), int(bool(compute_q))), "local_qr")
+        self.sync()
+        return rt
+
+    def _config(self, m, local_n, public_seed, private_seeds, top_k, precision):
+        P = len(local_n)
+        self._ln = (C.c_size_t * P)(*local_n)
+        self._ps = (C.c_uint * P)(*[s & 0xFFFFFFFF for s in private_seeds])
+        return FedSVDConfig(P, m, self._ln, public_seed & 0xFFFFFFFF, self._ps, top_k, precision)
+
+    def fedsvd(self, blocks, public_seed, private_seeds, top_k=-1, precision=0):
+        """DecentralizedClient::run() for P participants on this GPU
+        (client.cpp:447-1200).  blocks: list of m x local_n CUDA tensors,
+        overwritten.  Returns (sigma k, FinalU m x k, [FinalVT_c k x local_n])."""
+        P = len(blocks)
+        m = blocks[0].shape[0]
+        ln = [b.shape[1] for b in blocks]
+        cfg = self._config(m, ln, public_seed, private_seeds, top_k, precision)
+        sig = self._empty(m)
+        U = self._empty(m * m)
+        VT = [self._empty(m * n) for n in ln]
+        bp = (C.c_void_p * P)(*[b.data_ptr() for b in blocks])
+        vp = (C.c_void_p * P)(*[v.data_ptr() for v in VT])
+        k = C.c_int(0)
+        self._pre()
+        self._check(self.L.bbt_fedsvd_run(self.h, C.byref(cfg), bp, self._p(sig), self._p(U), vp, C.byref(k)),
+                    "fedsvd")
+        self.sync()
+        k = k.value
+        return sig[:k], U[: m * k].view(m, k), [v[: k * n].view(k, n) for v, n in zip(VT, ln)]
+
+    def fedsvd_host(self, blocks, public_seed, private_seeds, top_k=-1, precision=0, out=None):
+        """Same through the host-pointer entry (bbt_fedsvd_run_host): numpy
+        blocks in, numpy results out (copies timed inside the call)."""
+        P = len(blocks)
+        m = blocks[0].shape[0]
+        ln = [b.shape[1] for b in blocks]
+        cfg = self._config(m, ln, public_seed, private_seeds, top_k, precision)
+        blocks = [np.ascontiguousarray(b, dtype=np.float64) for b in blocks]
+        if out is None:
+            out = (np.empty(m), np.empty(m * m), [np.empty(m * n) for n in ln])
+        sig, U, VT = out
+        bp = (C.c_void_p * P)(*[b.ctypes.data for b in blocks])
+        vp = (C.c_void_p * P)(*[v.ctypes.data for v in VT])
+        k = C.c_int(0)
+        self._check(self.L.bbt_fedsvd_run_host(self.h, C.byref(cfg), bp, C.c_void_p(sig.ctypes.data),
+                                               C.c_void_p(U.ctypes.data), vp, C.byref(k)), "fedsvd_host")
+        k = k.value
+        return sig[:k], U[: m * k].reshape(m, k), [v[: k * n].reshape(k, n) for v, n in zip(VT, ln)]
+
+    def dgemm(self, transa, transb, A, B, alpha=1.0, beta=0.0, C=None):
+        """C = alpha op(A) op(B) + beta C on column-major data.  A, B, C are
+        CUDA tensors holding column-major matrices as their transposes
+        (a column-major M x K matrix is a row-major K x M tensor)."""
+        M = A.shape[0] if transa else A.shape[1]
+        K = A.shape[1] if transa else A.shape[0]
+        N = B.shape[0] if not transb else B.shape[1]
+        K2 = B.shape[1] if not transb else B.shape[0]
+        assert K == K2, (K, K2)
+        if C is None:
+            C = self._empty(N, M)
+        self._pre()
+        self._check(self.L.bbt_dgemm(self.h, int(transa), int(transb), M, N, K, alpha, self._p(A), A.shape[1],
+                                     self._p(B), B.shape[1], beta, self._p(C), C.shape[1]), "dgemm")
+        self.sync()
+        return C
+
+    def profile(self, enable=True):
+        self._check(self.L.bbt_profile(self.h, int(bool(enable))), "profile")
+
+    def profile_get(self):
+        """{class: (ms, launches, work)} since profiling was switched on."""
+        from ._lib import PROF_CLASSES
+        out = {}
+        for i, name in enumerate(PROF_CLASSES):
+            ms, n, w = C.c_double(), C.c_uint64(), C.c_double()
+            self._check(self.L.bbt_profile_get(self.h, i, C.byref(ms), C.byref(n), C.byref(w)), "profile_get")
+            out[name] = (ms.value, n.value, w.value)
+        return out
+
+    def stage_ms(self):
+        """Per-phase ms of the last fedsvd: local_qr, apply_mask, global_qr,
+        bi_diag, bsvd, combine_svd_remove_mask (the reference's timers)."""
+        buf = (C.c_double * 6)()
+        self._check(self.L.bbt_fedsvd_stage_ms(self.h, buf, 6), "stage_ms")
+        return dict(zip(("local_qr", "apply_mask", "global_qr", "bi_diag", "bsvd", "combine_svd_remove_mask"),
+                        list(buf)))

@@ -1,0 +1,303 @@
+// extern "C" entry points (include/bbtsvd_b200.h): argument checks, context
+// and workspace management, host<->device staging for the host-pointer
+// pipeline entry.  All arithmetic is in the kernels of the other sources.
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "internal.h"
+
+namespace bbt {
+
+cudaError_t Arena::reserve(size_t bytes) {
+  if (bytes <= cap) return cudaSuccess;
+  if (base) {
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return e;
+    cudaFree(base);
+    base = nullptr;
+    cap = 0;
+  }
+  cudaError_t e = cudaMalloc(&base, bytes);
+  if (e != cudaSuccess) {
+    base = nullptr;
+    return e;
+  }
+  cap = bytes;
+  top = 0;
+  return cudaSuccess;
+}
+
+bbt_status fail(bbt_ctx* ctx, bbt_status s, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  if (ctx) ctx->err = buf;
+  return s;
+}
+
+bbt_status cuda_fail(bbt_ctx* ctx, cudaError_t e, const char* what) {
+  return fail(ctx, e == cudaErrorMemoryAllocation ? BBT_ERR_NOMEM : BBT_ERR_CUDA, "%s: %s", what,
+              cudaGetErrorString(e));
+}
+
+namespace {
+
+// Scratch for the single-call entries: grow the arena to at least `bytes`.
+bbt_status ensure(bbt_ctx* ctx, size_t bytes) {
+  ctx->ws.reset();
+  if (ctx->ws.cap < bytes) BBT_CUDA(ctx, ctx->ws.reserve(bytes));
+  return BBT_OK;
+}
+
+bool bad(const void* p) { return p == nullptr || (reinterpret_cast<uintptr_t>(p) & 7) != 0; }
+
+}  // namespace
+}  // namespace bbt
+
+using namespace bbt;
+
+extern "C" {
+
+const char* bbt_status_string(bbt_status s) {
+  switch (s) {
+    case BBT_OK: return "ok";
+    case BBT_ERR_ARG: return "invalid argument";
+    case BBT_ERR_CUDA: return "CUDA error";
+    case BBT_ERR_COUNT: return "fewer singular values than requested";
+    case BBT_ERR_NOMEM: return "out of device memory";
+    case BBT_ERR_TIMEOUT: return "device-side wait timed out";
+    case BBT_ERR_UNSUPPORTED: return "unsupported shape or mode";
+  }
+  return "unknown status";
+}
+
+bbt_status bbt_create(bbt_ctx** out, int device) {
+  if (!out) return BBT_ERR_ARG;
+  *out = nullptr;
+  bbt_ctx* ctx = new bbt_ctx();
+  ctx->device = device;
+  cudaError_t e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->own, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaMalloc(&ctx->d_flag, 64);
+  if (e == cudaSuccess) e = cudaMalloc(&ctx->d_barrier, 64);
+  if (e == cudaSuccess) e = cudaMemset(ctx->d_flag, 0, 64);
+  if (e == cudaSuccess) e = cudaMemset(ctx->d_barrier, 0, 64);
+  if (e != cudaSuccess) {
+    fprintf(stderr, "bbt_create: %s\n", cudaGetErrorString(e));
+    if (ctx->own) cudaStreamDestroy(ctx->own);
+    delete ctx;
+    return e == cudaErrorMemoryAllocation ? BBT_ERR_NOMEM : BBT_ERR_CUDA;
+  }
+  ctx->stream = ctx->own;
+  *out = ctx;
+  return BBT_OK;
+}
+
+bbt_status bbt_destroy(bbt_ctx* ctx) {
+  if (!ctx) return BBT_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  if (ctx->ws.base) cudaFree(ctx->ws.base);
+  if (ctx->d_flag) cudaFree(ctx->d_flag);
+  if (ctx->d_barrier) cudaFree(ctx->d_barrier);
+  if (ctx->own) cudaStreamDestroy(ctx->own);
+  delete ctx;
+  return BBT_OK;
+}
+
+bbt_status bbt_set_stream(bbt_ctx* ctx, void* stream) {
+  if (!ctx) return BBT_ERR_ARG;
+  ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own;
+  return BBT_OK;
+}
+
+bbt_status bbt_synchronize(bbt_ctx* ctx) {
+  if (!ctx) return BBT_ERR_ARG;
+  BBT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return BBT_OK;
+}
+
+const char* bbt_last_error(const bbt_ctx* ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+uint64_t bbt_kernel_launches(const bbt_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+bbt_status bbt_negative_count(bbt_ctx* ctx, int n, const double* a, const double* b, const double* mu,
+                              int nmu, int* counts) {
+  if (!ctx) return BBT_ERR_ARG;
+  if (n < 1 || nmu < 0 || bad(a) || (n > 1 && bad(b)) || (nmu > 0 && (bad(mu) || !counts)))
+    return fail(ctx, BBT_ERR_ARG, "negative_count: bad arguments");
+  BBT_TRY(ensure(ctx, (size_t)n * 16 + (1 << 20)));
+  return sturm_counts(ctx, n, a, b, mu, nmu, counts);
+}
+
+bbt_status bbt_bisection(bbt_ctx* ctx, int n, const double* a, const double* b, double lo, double hi,
+                         double tol, int top_k, double* sigma, int* count) {
+  if (!ctx) return BBT_ERR_ARG;
+  if (!count) return fail(ctx, BBT_ERR_ARG, "bisection: count is NULL");
+  *count = 0;
+  if (n < 1 || bad(a) || (n > 1 && bad(b)) || (top_k > 0 && bad(sigma)))
+    return fail(ctx, BBT_ERR_ARG, "bisection: bad arguments");
+  BBT_TRY(ensure(ctx, (size_t)(n + 2) * 48 * 18 + (1 << 20)));
+  return bisect(ctx, n, a, b, lo, hi, tol, top_k, sigma, count);
+}
+
+bbt_status bbt_twisted_vectors(bbt_ctx* ctx, int n, int cnt, const double* sigma, const double* a,
+                               const double* b, double* U, double* V) {
+  if (!ctx) return BBT_ERR_ARG;
+  if (n < 1 || cnt < 0 || cnt > n || bad(a) || (n > 1 && bad(b)) || (cnt > 0 && (bad(sigma) || bad(U) || bad(V))))
+    return fail(ctx, BBT_ERR_ARG, "twisted_vectors: bad arguments");
+  BBT_TRY(ensure(ctx, (size_t)(n + 1) * cnt * 8 * 8 + (size_t)n * 32 + (1 << 20)));
+  return twisted(ctx, n, cnt, sigma, a, b, U, cnt, V, false);
+}
+
+bbt_status bbt_bidiagonal_svd(bbt_ctx* ctx, int k, const double* a, const double* b, double* U,
+                              double* V, double* sigma, int top_k) {
+  if (!ctx) return BBT_ERR_ARG;
+  if (k < 1 || top_k < 1 || top_k > k || bad(a) || (k > 1 && bad(b)) || bad(U) || bad(V) || bad(sigma))
+    return fail(ctx, BBT_ERR_ARG, "bidiagonal_svd: bad arguments (k=%d top_k=%d)", k, top_k);
+  BBT_TRY(ensure(ctx, (size_t)(k + 1) * top_k * 8 * 8 + (size_t)(k + 2) * 48 * 18 + (2 << 20)));
+  return bidiag_svd(ctx, k, a, b, U, V, sigma, top_k, false);
+}
+
+bbt_status bbt_givens_mask(bbt_ctx* ctx, size_t m, size_t n, size_t t, double* x, int mask, int is_left,
+                           unsigned seed) {
+  if (!ctx) return BBT_ERR_ARG;
+  if ((m * n > 0 && bad(x)) || t > 4096) return fail(ctx, BBT_ERR_ARG, "givens_mask: bad arguments");
+  const size_t k = is_left ? m : n;
+  BBT_TRY(ensure(ctx, t * (k + 2) * 24 + (1 << 20)));
+  return givens_mask(ctx, m, n, t, x, mask != 0, is_left != 0, seed);
+}
+
+bbt_status bbt_block_shift_mask(bbt_ctx* ctx, size_t m, size_t n, size_t t, double* x, int mask,
+                                int is_left, unsigned seed) {
+  if (!ctx) return BBT_ERR_ARG;
+  if ((m * n > 0 && bad(x)) || t > 4096) return fail(ctx, BBT_ERR_ARG, "block_shift_mask: bad arguments");
+  const size_t k = is_left ? m : n;
+  BBT_TRY(ensure(ctx, 2 * m * n * 8 + 2 * t * (k + 2) * 24 + 2 * (m + n + 20000) * 8 + (4 << 20)));
+  return block_shift_mask(ctx, m, n, t, x, mask != 0, is_left != 0, seed);
+}
+
+bbt_status bbt_local_qr(bbt_ctx* ctx, size_t m, size_t local_n, double* x, double* rt, int compute_q) {
+  if (!ctx) return BBT_ERR_ARG;
+  if (m < 1 || local_n <= m || bad(x) || bad(rt) || local_n > (size_t)1 << 31)
+    return fail(ctx, BBT_ERR_ARG, "local_qr: needs local_n > m (client.cpp:419)");
+  QrPlan qp;
+  const size_t tq = ((m + qp.nb - 1) / qp.nb) * qp.nb * qp.nb;
+  BBT_TRY(ensure(ctx, qr_workspace_bytes((long)local_n, (int)m, (int)m, qp) + (tq + m) * 8 + (4 << 20)));
+  double* tau = ctx->ws.take<double>(m);
+  double* T = ctx->ws.take<double>(tq);
+  const long n = (long)local_n;
+  BBT_TRY(geqrf(ctx, n, (int)m, x, n, tau, T, qp));
+  BBT_TRY(r_transpose(ctx, (int)m, x, n, rt));   // the reference's shrinked_x (client.cpp:437-442)
+  if (compute_q) BBT_TRY(orgqr(ctx, n, (int)m, x, n, tau, T, qp));
+  return BBT_OK;
+}
+
+bbt_status bbt_fedsvd_run(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* blocks,
+                          double* sigma, double* U, double* const* VT, int* k) {
+  if (!ctx) return BBT_ERR_ARG;
+  if (!cfg || !blocks || !VT || !k || bad(sigma) || bad(U)) return fail(ctx, BBT_ERR_ARG, "fedsvd: NULL argument");
+  for (int c = 0; c < cfg->participants; ++c)
+    if (bad(blocks[c]) || bad(VT[c])) return fail(ctx, BBT_ERR_ARG, "fedsvd: participant %d buffer", c);
+  return fedsvd(ctx, cfg, blocks, sigma, U, VT, k);
+}
+
+bbt_status bbt_fedsvd_run_host(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, const double* const* hX,
+                               double* hsigma, double* hU, double* const* hVT, int* k) {
+  if (!ctx) return BBT_ERR_ARG;
+  if (!cfg || !hX || !hVT || !k || !hsigma || !hU || cfg->participants < 1 || !cfg->local_n)
+    return fail(ctx, BBT_ERR_ARG, "fedsvd_host: NULL argument");
+  const int P = cfg->participants;
+  const size_t m = cfg->m;
+  std::vector<double*> dX(P, nullptr), dVT(P, nullptr);
+  double *ds = nullptr, *dU = nullptr;
+  bbt_status st = BBT_OK;
+  auto cleanup = [&]() {
+    for (auto p : dX) if (p) cudaFree(p);
+    for (auto p : dVT) if (p) cudaFree(p);
+    if (ds) cudaFree(ds);
+    if (dU) cudaFree(dU);
+  };
+  cudaError_t e = cudaSuccess;
+  for (int c = 0; c < P && e == cudaSuccess; ++c) {
+    const size_t bytes = m * cfg->local_n[c] * sizeof(double);
+    e = cudaMalloc(&dX[c], bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&dVT[c], bytes);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dX[c], hX[c], bytes, cudaMemcpyHostToDevice, ctx->stream);
+  }
+  if (e == cudaSuccess) e = cudaMalloc(&ds, m * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&dU, m * m * sizeof(double));
+  if (e != cudaSuccess) {
+    cleanup();
+    return cuda_fail(ctx, e, "fedsvd_host: staging");
+  }
+  st = fedsvd(ctx, cfg, dX.data(), ds, dU, dVT.data(), k);
+  if (st == BBT_OK) {
+    const int kk = *k;
+    e = cudaMemcpyAsync(hsigma, ds, kk * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(hU, dU, m * kk * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
+    for (int c = 0; c < P && e == cudaSuccess; ++c)
+      e = cudaMemcpyAsync(hVT[c], dVT[c], (size_t)kk * cfg->local_n[c] * sizeof(double), cudaMemcpyDeviceToHost,
+                          ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) st = cuda_fail(ctx, e, "fedsvd_host: copy-out");
+  }
+  cleanup();
+  return st;
+}
+
+bbt_status bbt_dgemm(bbt_ctx* ctx, int transa, int transb, int M, int N, long K, double alpha, const double* A,
+                     long lda, const double* B, long ldb, double beta, double* C, long ldc) {
+  if (!ctx) return BBT_ERR_ARG;
+  if (M < 0 || N < 0 || K < 0 || (M > 0 && N > 0 && (bad(C) || (K > 0 && (bad(A) || bad(B))))))
+    return fail(ctx, BBT_ERR_ARG, "dgemm: bad arguments");
+  const long am = transa ? K : M, bm = transb ? N : K;
+  if (lda < (am > 1 ? am : 1) || ldb < (bm > 1 ? bm : 1) || ldc < (M > 1 ? M : 1))
+    return fail(ctx, BBT_ERR_ARG, "dgemm: leading dimension too small");
+  BBT_TRY(ensure(ctx, (size_t)257 * M * N * 8 + (1 << 20)));
+  return dgemm(ctx, transa != 0, transb != 0, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
+}
+
+bbt_status bbt_profile(bbt_ctx* ctx, int enable) {
+  if (!ctx) return BBT_ERR_ARG;
+  BBT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  for (auto& r : ctx->recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
+  ctx->recs.clear();
+  for (int i = 0; i < 8; ++i) { ctx->prof_ms[i] = 0; ctx->prof_work[i] = 0; ctx->prof_n[i] = 0; }
+  ctx->prof = enable != 0;
+  return BBT_OK;
+}
+
+bbt_status bbt_profile_get(bbt_ctx* ctx, int cls, double* ms, uint64_t* launches, double* work) {
+  if (!ctx || cls < 0 || cls >= BBT_PROF_CLASSES) return BBT_ERR_ARG;
+  BBT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  for (auto& r : ctx->recs) {
+    float t = 0;
+    BBT_CUDA(ctx, cudaEventElapsedTime(&t, r.a, r.b));
+    ctx->prof_ms[r.cls] += t;
+    ctx->prof_n[r.cls] += 1;
+    ctx->prof_work[r.cls] += r.work;
+    cudaEventDestroy(r.a);
+    cudaEventDestroy(r.b);
+  }
+  ctx->recs.clear();
+  if (ms) *ms = ctx->prof_ms[cls];
+  if (launches) *launches = ctx->prof_n[cls];
+  if (work) *work = ctx->prof_work[cls];
+  return BBT_OK;
+}
+
+bbt_status bbt_fedsvd_stage_ms(const bbt_ctx* ctx, double* ms, int n) {
+  if (!ctx || !ms || n < 6) return BBT_ERR_ARG;
+  for (int i = 0; i < 6; ++i) ms[i] = ctx->stage_ms[i];
+  return BBT_OK;
+}
+
+}  // extern "C"

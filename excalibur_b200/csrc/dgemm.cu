@@ -1,0 +1,223 @@
+// FP64 GEMM on the FP64 tensor path (DMMA, mma.sync m8n8k4 .f64).
+//
+// Column-major BLAS convention: C = alpha * op(A) op(B) + beta * C with
+// op(A) M x K and op(B) K x N.  A CTA computes a 128 x 64 tile of C with
+// 8 warps (4 x 2), each warp a 32 x 32 block as 4 x 4 m8n8k4 fragments;
+// K advances 16 at a time through double-buffered shared-memory tiles
+// (register-staged global loads overlap the tensor work of the previous
+// tile).  For the tall-skinny shapes of Householder QR (K up to 10^6,
+// M*N small) K is split across CTAs; the partial tiles are summed in a
+// fixed order by a second kernel so results are deterministic.
+#include <cuda_runtime.h>
+
+#include "internal.h"
+
+namespace bbt {
+namespace {
+
+constexpr int BM = 128, BN = 64, BK = 16;
+constexpr int PADA = 4, PADB = 4;
+constexpr int THREADS = 256;
+
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+template <bool TA, bool TB>
+__global__ void __launch_bounds__(THREADS, 2)
+dgemm_kernel(int M, int N, long K, long kchunk, double alpha, const double* __restrict__ A, long lda,
+             const double* __restrict__ B, long ldb, double beta, double* __restrict__ C, long ldc,
+             double* __restrict__ P) {
+  extern __shared__ double smem_[];
+  auto As = reinterpret_cast<double(*)[BK][BM + PADA]>(smem_);
+  auto Bs = reinterpret_cast<double(*)[BK][BN + PADB]>(smem_ + 2 * BK * (BM + PADA));
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = warp & 3, wn = warp >> 2;
+  const int i0 = blockIdx.x * BM, j0 = blockIdx.y * BN;
+  const long kbeg = (long)blockIdx.z * kchunk;
+  const long kend = min(K, kbeg + kchunk);
+
+  double acc[4][4][2];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
+
+  double ra[BM * BK / THREADS];   // 8
+  double rb[BN * BK / THREADS];   // 4
+
+  auto load = [&](long k0) {
+#pragma unroll
+    for (int r = 0; r < BM * BK / THREADS; ++r) {
+      const int e = tid + r * THREADS;
+      int il, kl;
+      if (TA) { kl = e % BK; il = e / BK; } else { il = e % BM; kl = e / BM; }
+      const int i = i0 + il;
+      const long k = k0 + kl;
+      double v = 0.0;
+      if (i < M && k < kend) v = TA ? A[k + (long)i * lda] : A[(long)i + k * lda];
+      ra[r] = v;
+    }
+#pragma unroll
+    for (int r = 0; r < BN * BK / THREADS; ++r) {
+      const int e = tid + r * THREADS;
+      int jl, kl;
+      if (TB) { jl = e % BN; kl = e / BN; } else { kl = e % BK; jl = e / BK; }
+      const int j = j0 + jl;
+      const long k = k0 + kl;
+      double v = 0.0;
+      if (j < N && k < kend) v = TB ? B[(long)j + k * ldb] : B[k + (long)j * ldb];
+      rb[r] = v;
+    }
+  };
+  auto store = [&](int buf) {
+#pragma unroll
+    for (int r = 0; r < BM * BK / THREADS; ++r) {
+      const int e = tid + r * THREADS;
+      int il, kl;
+      if (TA) { kl = e % BK; il = e / BK; } else { il = e % BM; kl = e / BM; }
+      As[buf][kl][il] = ra[r];
+    }
+#pragma unroll
+    for (int r = 0; r < BN * BK / THREADS; ++r) {
+      const int e = tid + r * THREADS;
+      int jl, kl;
+      if (TB) { jl = e % BN; kl = e / BN; } else { kl = e % BK; jl = e / BK; }
+      Bs[buf][kl][jl] = rb[r];
+    }
+  };
+
+  if (kbeg < kend) {
+    load(kbeg);
+    store(0);
+    __syncthreads();
+    int buf = 0;
+    for (long k0 = kbeg; k0 < kend; k0 += BK) {
+      const bool more = k0 + BK < kend;
+      if (more) load(k0 + BK);
+#pragma unroll
+      for (int ks = 0; ks < BK; ks += 4) {
+        double af[4], bf[4];
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+          af[t] = As[buf][ks + (lane & 3)][wm * 32 + t * 8 + (lane >> 2)];
+          bf[t] = Bs[buf][ks + (lane & 3)][wn * 32 + t * 8 + (lane >> 2)];
+        }
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int b = 0; b < 4; ++b) dmma(acc[a][b][0], acc[a][b][1], af[a], bf[b]);
+      }
+      if (more) {
+        store(buf ^ 1);
+        __syncthreads();
+        buf ^= 1;
+      }
+    }
+  }
+
+  // epilogue: fragment (a,b) element e at row wm*32+a*8+lane/4, col wn*32+b*8+2*(lane%4)+e
+  double* out = P ? P + (long)blockIdx.z * M * (long)N : C;
+  const long ldo = P ? M : ldc;
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    const int i = i0 + wm * 32 + a * 8 + (lane >> 2);
+    if (i >= M) continue;
+#pragma unroll
+    for (int b = 0; b < 4; ++b)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int j = j0 + wn * 32 + b * 8 + 2 * (lane & 3) + e;
+        if (j >= N) continue;
+        double* c = out + i + (long)j * ldo;
+        const double v = alpha * acc[a][b][e];
+        if (P || beta == 0.0) *c = v;
+        else *c = v + beta * (*c);
+      }
+  }
+}
+
+// C = beta*C + sum_z P[z] in order z = 0..S-1.
+__global__ void splitk_reduce(int M, int N, int S, const double* __restrict__ P, double beta,
+                              double* __restrict__ C, long ldc) {
+  const long total = (long)M * N;
+  for (long f = blockIdx.x * (long)blockDim.x + threadIdx.x; f < total; f += (long)gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int z = 0; z < S; ++z) s += P[(long)z * total + f];
+    const int i = (int)(f % M);
+    const long j = f / M;
+    double* c = C + i + j * ldc;
+    *c = (beta == 0.0) ? s : s + beta * (*c);
+  }
+}
+
+constexpr int SMEM_BYTES = 2 * BK * (BM + PADA + BN + PADB) * (int)sizeof(double);
+
+template <bool TA, bool TB>
+cudaError_t launch(dim3 g, cudaStream_t st, int M, int N, long K, long kc, double alpha, const double* A,
+                   long lda, const double* B, long ldb, double beta, double* C, long ldc, double* P) {
+  static bool attr = false;   // set once per process (per kernel instantiation)
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(dgemm_kernel<TA, TB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         SMEM_BYTES);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  dgemm_kernel<TA, TB><<<g, THREADS, SMEM_BYTES, st>>>(M, N, K, kc, alpha, A, lda, B, ldb, beta, C, ldc, P);
+  return cudaSuccess;
+}
+
+}  // namespace
+
+bbt_status dgemm(bbt_ctx* ctx, bool ta, bool tb, int M, int N, long K, double alpha, const double* A,
+                 long lda, const double* B, long ldb, double beta, double* C, long ldc, int splits) {
+  if (M < 0 || N < 0 || K < 0) return fail(ctx, BBT_ERR_ARG, "dgemm: M=%d N=%d K=%ld", M, N, K);
+  if (M == 0 || N == 0) return BBT_OK;
+  const int tm = (M + BM - 1) / BM, tn = (N + BN - 1) / BN;
+  if (splits <= 0) {
+    const long tiles = (long)tm * tn;
+    const long target = 2L * ctx->num_sms;
+    splits = 1;
+    if (tiles < target && K >= 2048) {
+      long s = (target + tiles - 1) / tiles;
+      const long maxs = K / 1024;
+      if (s > maxs) s = maxs;
+      if (s > 256) s = 256;
+      splits = (int)(s < 1 ? 1 : s);
+    }
+  }
+  long kc = (K + splits - 1) / splits;
+  kc = ((kc + BK - 1) / BK) * BK;
+  if (kc == 0) kc = BK;
+  splits = (int)((K + kc - 1) / kc);
+  if (splits < 1) splits = 1;
+  double* P = nullptr;
+  size_t mark = ctx->ws.top;
+  if (splits > 1) {
+    P = ctx->ws.take<double>((size_t)splits * M * N);
+    if (!P) return fail(ctx, BBT_ERR_NOMEM, "dgemm: split-K workspace (%d x %d x %d)", splits, M, N);
+  }
+  dim3 g(tm, tn, splits);
+  if (K == 0) {   // C = beta * C
+    g.z = 1;
+    P = nullptr;
+  }
+  cudaError_t e;
+  ProfScope prof(ctx, BBT_PROF_DGEMM, 2.0 * M * (double)N * (double)K);
+  if (!ta && !tb) e = launch<false, false>(g, ctx->stream, M, N, K, kc, alpha, A, lda, B, ldb, beta, C, ldc, P);
+  else if (ta && !tb) e = launch<true, false>(g, ctx->stream, M, N, K, kc, alpha, A, lda, B, ldb, beta, C, ldc, P);
+  else if (!ta && tb) e = launch<false, true>(g, ctx->stream, M, N, K, kc, alpha, A, lda, B, ldb, beta, C, ldc, P);
+  else e = launch<true, true>(g, ctx->stream, M, N, K, kc, alpha, A, lda, B, ldb, beta, C, ldc, P);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "dgemm: shared-memory attribute");
+  BBT_LAUNCHED(ctx);
+  if (P) {
+    splitk_reduce<<<4 * ctx->num_sms, 256, 0, ctx->stream>>>(M, N, splits, P, beta, C, ldc);
+    BBT_LAUNCHED(ctx);
+  }
+  ctx->ws.top = mark;
+  return BBT_OK;
+}
+
+}  // namespace bbt

@@ -1,0 +1,163 @@
+// Internal declarations shared by the CUDA sources of libexcalibur_b200.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/bbtsvd_b200.h"
+
+namespace bbt {
+
+// Device workspace: one growing allocation per context, carved per call.
+struct Arena {
+  char* base = nullptr;
+  size_t cap = 0;
+  size_t top = 0;
+  cudaError_t reserve(size_t bytes);   // grows (frees and reallocates) when needed
+  void reset() { top = 0; }
+  template <class T>
+  T* take(size_t count) {
+    size_t off = (top + 255) & ~size_t(255);
+    size_t need = off + count * sizeof(T);
+    if (need > cap) return nullptr;
+    top = need;
+    return reinterpret_cast<T*>(base + off);
+  }
+};
+
+}  // namespace bbt
+
+namespace bbt {
+struct ProfRec {
+  cudaEvent_t a, b;
+  int cls;
+  double work;
+};
+}  // namespace bbt
+
+struct bbt_ctx {
+  int device = 0;
+  int num_sms = 0;
+  cudaStream_t own = nullptr;
+  cudaStream_t stream = nullptr;
+  bbt::Arena ws;
+  std::string err;
+  uint64_t launches = 0;
+  int* d_flag = nullptr;         // device error flag for bounded waits
+  unsigned* d_barrier = nullptr; // grid-barrier state (count, generation)
+  double stage_ms[8] = {0};
+  bool prof = false;
+  std::vector<bbt::ProfRec> recs;          // pending event pairs
+  double prof_ms[8] = {0}, prof_work[8] = {0};
+  uint64_t prof_n[8] = {0};
+};
+
+namespace bbt {
+
+bbt_status fail(bbt_ctx* ctx, bbt_status s, const char* fmt, ...);
+bbt_status cuda_fail(bbt_ctx* ctx, cudaError_t e, const char* what);
+
+#define BBT_CUDA(ctx, call)                                   \
+  do {                                                        \
+    cudaError_t e_ = (call);                                  \
+    if (e_ != cudaSuccess) return bbt::cuda_fail(ctx, e_, #call); \
+  } while (0)
+
+#define BBT_LAUNCHED(ctx)                                        \
+  do {                                                           \
+    (ctx)->launches++;                                           \
+    cudaError_t e_ = cudaGetLastError();                         \
+    if (e_ != cudaSuccess) return bbt::cuda_fail(ctx, e_, "kernel launch"); \
+  } while (0)
+
+// Event-bracketed launch region for the profiler (no-op when profiling is off).
+struct ProfScope {
+  bbt_ctx* ctx;
+  ProfRec r;
+  bool on;
+  ProfScope(bbt_ctx* c, int cls, double work) : ctx(c), on(c->prof) {
+    if (!on) return;
+    r.cls = cls;
+    r.work = work;
+    cudaEventCreate(&r.a);
+    cudaEventCreate(&r.b);
+    cudaEventRecord(r.a, c->stream);
+  }
+  ~ProfScope() {
+    if (!on) return;
+    cudaEventRecord(r.b, ctx->stream);
+    ctx->recs.push_back(r);
+  }
+};
+
+#define BBT_TRY(call)                       \
+  do {                                      \
+    bbt_status s_ = (call);                 \
+    if (s_ != BBT_OK) return s_;            \
+  } while (0)
+
+// ---- kernels exposed across translation units (all stream-ordered) ----
+
+// Sturm / bisection / twisted (sturm.cu, twisted.cu)
+bbt_status sturm_counts(bbt_ctx* ctx, int n, const double* a, const double* b, const double* mu,
+                        int nmu, int* counts);
+bbt_status bisect(bbt_ctx* ctx, int n, const double* a, const double* b, double lo, double hi,
+                  double tol, int top_k, double* sigma, int* count);
+bbt_status twisted(bbt_ctx* ctx, int n, int cnt, const double* sigma, const double* a,
+                   const double* b, double* U, int ldu, double* V, bool sign_fix);
+bbt_status bidiag_svd(bbt_ctx* ctx, int k, const double* a, const double* b, double* U, double* V,
+                      double* sigma, int top_k, bool global_sign);
+// d_out[0] = ||a||^2 + ||b||^2 (the bisection bound, bbtsvd.cpp:936)
+bbt_status bidiag_bound(bbt_ctx* ctx, int n, const double* a, const double* b, double* d_out);
+
+// Givens masks (givens.cu)
+bbt_status givens_mask(bbt_ctx* ctx, size_t m, size_t n, size_t passes, double* x, bool mask,
+                       bool is_left, unsigned seed);
+bbt_status block_shift_mask(bbt_ctx* ctx, size_t m, size_t n, size_t passes, double* x, bool mask,
+                            bool is_left, unsigned seed);
+
+// FP64 GEMM, column-major BLAS convention (dgemm.cu):
+//   C = alpha * op(A) * op(B) + beta * C,  op(A) M x K, op(B) K x N.
+// splits > 1 splits K; partial products are summed in a fixed order.
+bbt_status dgemm(bbt_ctx* ctx, bool ta, bool tb, int M, int N, long K, double alpha,
+                 const double* A, long lda, const double* B, long ldb, double beta, double* C,
+                 long ldc, int splits = 0);
+
+// Householder QR, column-major A (rows x cols, lda), rows >= cols (qr.cu).
+struct QrPlan {
+  int nb = 32;
+};
+bbt_status geqrf(bbt_ctx* ctx, long rows, int cols, double* A, long lda, double* tau,
+                 double* T /* (cols/nb+1) * nb * nb */, const QrPlan& plan);
+bbt_status orgqr(bbt_ctx* ctx, long rows, int cols, double* A, long lda, const double* tau,
+                 const double* T, const QrPlan& plan);
+// C (rows x ncols) <- H_0 H_1 ... H_{k-1} C.  Reflector j is column j of V
+// from row j down (unit diagonal implied); V(r, c) is read at V[r*rs + c*cs].
+// C is column-major (ld ldc) or, with c_rowmajor, row-major (ld ldc).
+bbt_status ormqr_left_notrans(bbt_ctx* ctx, long rows, int k, const double* V, long rs, long cs,
+                              const double* tau, double* C, long ldc, int ncols, bool c_rowmajor,
+                              const QrPlan& plan);
+size_t qr_workspace_bytes(long rows, int cols, int ncols_apply, const QrPlan& plan);
+
+// Ralha one-sided bidiagonalisation of W (m x m row-major, overwritten) (ralha.cu).
+bbt_status ralha(bbt_ctx* ctx, int m, double* W, double* house, double* tau, double* alpha,
+                 double* beta, double* V, double* cs);
+
+// Small helpers (util.cu)
+bbt_status transpose(bbt_ctx* ctx, int rows, int cols, const double* src, long lds, double* dst,
+                     long ldd);   // dst (cols x rows, row-major) = src^T
+bbt_status copy2d(bbt_ctx* ctx, int rows, int cols, const double* src, long lds, double* dst,
+                  long ldd);
+bbt_status fill(bbt_ctx* ctx, double* p, size_t n, double v);
+// RT (m x m row-major) = R^T, R = upper triangle of the top of column-major A
+bbt_status r_transpose(bbt_ctx* ctx, int m, const double* A, long lda, double* RT);
+
+// Whole pipeline (fedsvd.cu)
+bbt_status fedsvd(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* blocks, double* sigma,
+                  double* U, double* const* VT, int* k);
+size_t fedsvd_workspace_bytes(const bbt_fedsvd_config* cfg);
+
+}  // namespace bbt

@@ -1,0 +1,343 @@
+// Ralha one-sided bidiagonalisation (Excalibur src/client.cpp:801-958,
+// overlapped variant :829-910) as ONE persistent cooperative kernel.
+//
+// The reference runs m-2 steps; each needs the Gram row g = W[i+1:] w_i
+// plus four dot products, one ring all-reduce of m+3-i doubles across the
+// participants, a Householder reflector (dlarfg), its application to rows
+// i+1.. (dgemv + dger), and a Gram-Schmidt update of row i.  Here the
+// participants' column slabs sit side by side in one m x m row-major
+// matrix, so the all-reduce is the in-device reduction of each dot product,
+// and a step is two grid-wide phases separated by bounded grid barriers:
+//
+//   B1 (column-partitioned): every CTA forms the reflector from g (same
+//      arithmetic in every CTA), writes its share of the Householder store,
+//      vt = sum_t h_t W[i+1+t] for its columns, the next row i+1 after the
+//      update, and row i of V (w_i - beta v_{i-1}) / alpha_i.
+//   B2 (row-partitioned, one warp per row): W[r] += (-tau vt) h_r for
+//      r > i, and, in the same pass, the next step's Gram row
+//      g'[r] = W[r] . W[i+1]; CTA 0 adds the next step's four dots.
+//
+// Barriers spin a bounded number of times; on a timeout every CTA stops and
+// the host reports BBT_ERR_TIMEOUT.
+#include <cooperative_groups.h>
+#include <cuda_runtime.h>
+
+#include "internal.h"
+
+namespace bbt {
+namespace {
+
+constexpr int RT = 256;                 // threads per CTA
+constexpr int RW = RT / 32;             // warps per CTA
+constexpr long SPIN_LIMIT = 20000000;   // ~seconds of polling before giving up
+
+struct RalhaArgs {
+  int m;
+  double* W;       // m x m row-major, rows are the vectors
+  double* house;   // m x m row-major, zero on entry
+  double* tau;     // m, zero on entry
+  double* alpha;   // m
+  double* beta;    // m-1 (lower bidiagonal)
+  double* V;       // m x m row-major, left vectors, zero on entry
+  double* g;       // 2 x m: Gram rows, ping-pong between steps
+  double* extra;   // 2 x 4: the four extra dots, ping-pong between steps
+  double* vt;      // m
+  double* tv;      // m: -tau * vt
+  double* nextw;   // m: row i+1 after the update
+  unsigned* bar;   // [0] arrivals, [1] generation
+  int* err;
+};
+
+__device__ __forceinline__ bool grid_sync(unsigned* bar, int* err) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned* gen = bar + 1;
+    const unsigned g0 = *gen;
+    __threadfence();
+    const unsigned arrived = atomicAdd(bar, 1u) + 1u;
+    if (arrived == gridDim.x) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      long spins = 0;
+      while (*gen == g0) {
+        if (++spins > SPIN_LIMIT) { atomicExch(err, 1); break; }
+        if (*(volatile int*)err) break;
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return *(volatile int*)err == 0;
+}
+
+__device__ double block_sum(double v, double* sh) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  __syncthreads();
+  if (lane == 0) sh[w] = v;
+  __syncthreads();
+  double s = 0.0;
+  for (int k = 0; k < RW; ++k) s += sh[k];
+  __syncthreads();
+  return s;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Gram row for step i from rows r >= i+1 against row `piv`, into out.
+__device__ void gram_rows(const RalhaArgs& A, int i, const double* piv, double* out) {
+  const int m = A.m;
+  const int gw = blockIdx.x * RW + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  const int nw = gridDim.x * RW;
+  for (int r = i + 1 + gw; r < m; r += nw) {
+    const double* row = A.W + (long)r * m;
+    double s = 0.0;
+    for (int c = lane; c < m; c += 32) s += row[c] * piv[c];
+    s = warp_sum(s);
+    if (lane == 0) out[r - i - 1] = s;
+  }
+}
+
+__global__ void __launch_bounds__(RT) ralha_kernel(RalhaArgs A) {
+  __shared__ double sh[RW];
+  __shared__ double scal[6];   // beta_{i-1}, alpha_i, tau, scale, 1/alpha_i
+  __shared__ double red[RW][33];
+  const int m = A.m;
+  const int tid = threadIdx.x;
+  // ---- step 0 set-up: alpha_0, v_0 (CTA 0); Gram row of w_0 (all)
+  if (blockIdx.x == 0) {
+    double s = 0.0;
+    for (int c = tid; c < m; c += RT) s += A.W[c] * A.W[c];
+    s = block_sum(s, sh);
+    const double a0 = sqrt(s);
+    if (tid == 0) A.alpha[0] = a0;
+    const double inv = 1.0 / a0;
+    for (int c = tid; c < m; c += RT) A.V[c] = inv * A.W[c];
+    if (tid == 0) A.house[0] = 1.0;
+  }
+  gram_rows(A, 0, A.W, A.g);
+  if (!grid_sync(A.bar, A.err)) return;
+
+  // columns owned in B1
+  const int cw = (m + gridDim.x - 1) / gridDim.x;
+  const int c0 = blockIdx.x * cw;
+  const int c1 = min(m, c0 + cw);
+
+  for (int i = 0; i + 2 < m; ++i) {
+    const int len = m - 1 - i;   // g[0..len)
+    const double* g = A.g + (long)(i & 1) * m;
+    double* gn = A.g + (long)((i + 1) & 1) * m;
+    const double* ex = A.extra + (i & 1) * 4;
+    double* exn = A.extra + ((i + 1) & 1) * 4;
+    // ---- scalars (identical in every CTA)
+    {
+      double s = 0.0;
+      for (int t = 1 + tid; t < len; t += RT) s += g[t] * g[t];
+      s = block_sum(s, sh);
+      if (tid == 0) {
+        const double al = g[0];
+        double be = al, ta = 0.0, scl = 0.0;
+        if (s != 0.0) {   // dlarfg
+          const double h = hypot(al, sqrt(s));
+          be = -copysign(h, al);
+          ta = (be - al) / be;
+          scl = 1.0 / (al - be);
+        }
+        scal[2] = ta;
+        scal[3] = scl;
+        if (i > 0) {
+          const double b = ex[0];
+          const double vv = ex[1], ww = ex[2], vw = ex[3];
+          const double a = sqrt(vv * (b * b) + ww - 2 * b * vw);
+          scal[0] = b;
+          scal[1] = a;
+          scal[4] = 1.0 / a;
+          if (blockIdx.x == 0) { A.beta[i - 1] = b; A.alpha[i] = a; }
+        }
+        if (blockIdx.x == 0) A.tau[i + 1] = ta;
+      }
+      __syncthreads();
+    }
+    const double ta = scal[2], scl = scal[3];
+    // ---- B1: Householder store, vt, next row, V row i (my columns)
+    // house column i+1 from row i+1: (1, g[1:] * scale); rows split across CTAs
+    for (int t = blockIdx.x * RT + tid; t < len; t += gridDim.x * RT)
+      A.house[(long)(i + 1 + t) * m + (i + 1)] = (t == 0) ? 1.0 : g[t] * scl;
+    {
+      // vt[c] = sum_t h_t W[i+1+t][c] with h_0 = 1, h_t = g[t]*scale
+      const int ncol = c1 - c0;
+      for (int cb = 0; cb < ncol; cb += 32) {
+        const int c = c0 + cb + (tid & 31);
+        double s = 0.0;
+        if (c < c1)
+          for (int t = tid >> 5; t < len; t += RW) {
+            const double h = (t == 0) ? 1.0 : g[t] * scl;
+            s += h * A.W[(long)(i + 1 + t) * m + c];
+          }
+        red[tid >> 5][tid & 31] = s;
+        __syncthreads();
+        if (tid < 32 && c0 + cb + tid < c1) {
+          const int cc = c0 + cb + tid;
+          double v = 0.0;
+          for (int k = 0; k < RW; ++k) v += red[k][tid];
+          A.vt[cc] = v;
+          const double tvv = -ta * v;
+          A.tv[cc] = tvv;
+          A.nextw[cc] = A.W[(long)(i + 1) * m + cc] + tvv;   // h_0 = 1
+        }
+        __syncthreads();
+      }
+      if (i > 0) {
+        const double b = scal[0], inva = scal[4];
+        for (int c = c0 + tid; c < c1; c += RT) {
+          const double w = A.W[(long)i * m + c] + (-b) * A.V[(long)(i - 1) * m + c];
+          A.W[(long)i * m + c] = w;
+          A.V[(long)i * m + c] = inva * w;
+        }
+      }
+    }
+    if (!grid_sync(A.bar, A.err)) return;
+    // ---- B2: rank-1 update of rows i+1.., next Gram row, next extras
+    {
+      const int gw = blockIdx.x * RW + (tid >> 5), lane = tid & 31;
+      const int nw = gridDim.x * RW;
+      for (int r = i + 1 + gw; r < m; r += nw) {
+        const int t = r - i - 1;
+        const double h = (t == 0) ? 1.0 : g[t] * scl;
+        double* row = A.W + (long)r * m;
+        double s = 0.0;
+        for (int c = lane; c < m; c += 32) {
+          const double w = row[c] + A.tv[c] * h;
+          row[c] = w;
+          s += w * A.nextw[c];
+        }
+        s = warp_sum(s);
+        // g for step i+1 has entries for rows >= i+2
+        if (lane == 0 && r >= i + 2) gn[r - i - 2] = s;
+      }
+      if (blockIdx.x == 0) {
+        // extras for step i+1: w_{i+1}.v_i, v_i.v_i, w_{i+1}.w_{i+1}, v_i.w_{i+1}
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+        const double* v = A.V + (long)i * m;
+        for (int c = tid; c < m; c += RT) {
+          const double w = A.nextw[c];
+          s0 += w * v[c];
+          s1 += v[c] * v[c];
+          s2 += w * w;
+        }
+        s0 = block_sum(s0, sh);
+        s1 = block_sum(s1, sh);
+        s2 = block_sum(s2, sh);
+        if (tid == 0) { exn[0] = s0; exn[1] = s1; exn[2] = s2; exn[3] = s0; }
+      }
+    }
+    if (!grid_sync(A.bar, A.err)) return;
+  }
+  // ---- tail steps i = m-2, m-1 (client.cpp:897-905), CTA 0
+  if (blockIdx.x != 0) return;
+  for (int i = (m >= 3 ? m - 2 : 1); i < m; ++i) {
+    const double* vp = A.V + (long)(i - 1) * m;
+    double* wi = A.W + (long)i * m;
+    double s = 0.0;
+    for (int c = tid; c < m; c += RT) s += wi[c] * vp[c];
+    const double b = block_sum(s, sh);
+    double q = 0.0;
+    for (int c = tid; c < m; c += RT) {
+      const double w = wi[c] + (-b) * vp[c];
+      wi[c] = w;
+      q += w * w;
+    }
+    q = block_sum(q, sh);
+    const double a = sqrt(q);
+    const double inv = 1.0 / a;
+    for (int c = tid; c < m; c += RT) A.V[(long)i * m + c] = inv * wi[c];
+    if (tid == 0) { A.beta[i - 1] = b; A.alpha[i] = a; }
+    __syncthreads();
+  }
+}
+
+// Lower -> upper bidiagonal with drotg (client.cpp:947-954); one thread.
+__device__ void drotg_ref(double& a, double& b, double& c, double& s) {
+  const double roe = fabs(a) > fabs(b) ? a : b;
+  const double scale = fabs(a) + fabs(b);
+  double r;
+  if (scale == 0.0) {
+    c = 1.0; s = 0.0; r = 0.0;
+  } else {
+    const double as = a / scale, bs = b / scale;
+    r = scale * sqrt(as * as + bs * bs);
+    r = copysign(1.0, roe) * r;
+    c = a / r;
+    s = b / r;
+  }
+  a = r;
+}
+
+__global__ void lower_to_upper_kernel(int m, double* __restrict__ alpha, double* __restrict__ beta,
+                                      double* __restrict__ cs) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  for (int i = 0; i + 1 < m; ++i) {
+    double a = alpha[i], b = beta[i], c, s;
+    drotg_ref(a, b, c, s);
+    alpha[i] = a;
+    cs[2 * i] = c;
+    cs[2 * i + 1] = s;
+    beta[i] = s * alpha[i + 1];
+    alpha[i + 1] = c * alpha[i + 1];
+  }
+}
+
+}  // namespace
+
+bbt_status ralha(bbt_ctx* ctx, int m, double* W, double* house, double* tau, double* alpha,
+                 double* beta, double* V, double* cs) {
+  if (m < 3) return fail(ctx, BBT_ERR_UNSUPPORTED, "ralha: m=%d (the reference needs m >= 3)", m);
+  size_t mark = ctx->ws.top;
+  RalhaArgs A;
+  A.m = m;
+  A.W = W;
+  A.house = house;
+  A.tau = tau;
+  A.alpha = alpha;
+  A.beta = beta;
+  A.V = V;
+  A.g = ctx->ws.take<double>(2 * (size_t)m);
+  A.extra = ctx->ws.take<double>(8);
+  A.vt = ctx->ws.take<double>(m);
+  A.tv = ctx->ws.take<double>(m);
+  A.nextw = ctx->ws.take<double>(m);
+  if (!A.nextw) return fail(ctx, BBT_ERR_NOMEM, "ralha: workspace");
+  A.bar = ctx->d_barrier;
+  A.err = ctx->d_flag;
+  BBT_CUDA(ctx, cudaMemsetAsync(house, 0, (size_t)m * m * sizeof(double), ctx->stream));
+  BBT_CUDA(ctx, cudaMemsetAsync(V, 0, (size_t)m * m * sizeof(double), ctx->stream));
+  BBT_CUDA(ctx, cudaMemsetAsync(tau, 0, (size_t)m * sizeof(double), ctx->stream));
+  BBT_CUDA(ctx, cudaMemsetAsync(ctx->d_barrier, 0, 2 * sizeof(unsigned), ctx->stream));
+  BBT_CUDA(ctx, cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), ctx->stream));
+  int per_sm = 0;
+  BBT_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ralha_kernel, RT, 0));
+  if (per_sm < 1) return fail(ctx, BBT_ERR_CUDA, "ralha: kernel does not fit an SM");
+  int grid = (m + 31) / 32;                 // at least 32 columns per CTA in B1
+  if (grid > ctx->num_sms) grid = ctx->num_sms;
+  if (grid < 1) grid = 1;
+  void* args[] = {&A};
+  ProfScope prof(ctx, BBT_PROF_RALHA, 16.0 * (double)m * m * m / 3.0);
+  BBT_CUDA(ctx, cudaLaunchCooperativeKernel((void*)ralha_kernel, dim3(grid), dim3(RT), args, 0, ctx->stream));
+  BBT_LAUNCHED(ctx);
+  lower_to_upper_kernel<<<1, 1, 0, ctx->stream>>>(m, alpha, beta, cs);
+  BBT_LAUNCHED(ctx);
+  int herr = 0;
+  BBT_CUDA(ctx, cudaMemcpyAsync(&herr, ctx->d_flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  BBT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  ctx->ws.top = mark;
+  if (herr) return fail(ctx, BBT_ERR_TIMEOUT, "ralha: grid barrier timed out");
+  return BBT_OK;
+}
+
+}  // namespace bbt

@@ -1,0 +1,285 @@
+// Sturm counts and the reference's bisection tree on the GPU.
+//
+// Excalibur's negative_count (src/bbtsvd.cpp:7-17) is a stationary-qd
+// Sturm count of B^T B - mu^2 I; bisection_singular_values (:19-52) walks a
+// binary tree over [lo, hi] depth first, upper half first, and stops a
+// branch when the midpoint no longer splits it (or the width is <= tol),
+// emitting that midpoint.  Every value is therefore fixed by the tree, not
+// by the traversal order, so the tree can be walked breadth first: all live
+// intervals of a level in parallel.  Each round resolves DEPTH levels at
+// once ("multisection"): the 2^DEPTH - 1 midpoints below a live interval are
+// counted by separate threads, then one thread per interval replays the
+// reference's rules over that subtree.  Intervals are kept in descending
+// order, terminal ones included, so the final list is already the
+// reference's output order and top_k is a truncation.
+//
+// Arithmetic: every product, quotient and sum is rounded on its own
+// (__dmul_rn / __ddiv_rn / __dadd_rn: no FMA contraction), as in the
+// reference's build, so counts and singular values match it bit for bit.
+#include <cuda_runtime.h>
+
+#include "internal.h"
+
+namespace bbt {
+namespace {
+
+constexpr int DEPTH = 3;                 // tree levels resolved per round
+constexpr int NPTS = (1 << DEPTH) - 1;   // midpoints counted per live interval
+constexpr int FAN = 1 << DEPTH;          // max intervals one interval becomes
+constexpr int SMEM_PAIRS_MAX = 12288;    // stage (beta^2, alpha^2) in SMEM up to this n
+
+// (b2[i-1], a2[i]) with b2[-1] unused; squares rounded once, as pow(x,2)
+// folded to x*x in the reference's -O3 build.
+__global__ void squares_kernel(int n, const double* __restrict__ a, const double* __restrict__ b,
+                               double2* __restrict__ q) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    double ai = a[i];
+    double bi = (i > 0) ? b[i - 1] : 0.0;
+    q[i] = make_double2(__dmul_rn(bi, bi), __dmul_rn(ai, ai));
+  }
+}
+
+// One Sturm count, q in SMEM or global.  Follows bbtsvd.cpp:9-15 exactly.
+__device__ __forceinline__ int sturm(int n, const double2* q, double mu) {
+  const double mu2 = __dmul_rn(mu, mu);
+  double t = -mu2;
+  double d = __dadd_rn(q[0].y, t);
+  int neg = d < 0.0;
+  for (int i = 1; i < n; ++i) {
+    const double2 qi = q[i];
+    const double r = __ddiv_rn(qi.x, d);
+    t = __dsub_rn(__dmul_rn(t, r), mu2);
+    d = __dadd_rn(qi.y, t);
+    neg += d < 0.0;
+  }
+  return neg;
+}
+
+__device__ __forceinline__ void stage_pairs(int n, const double2* __restrict__ q, double2* sq) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) sq[i] = q[i];
+  __syncthreads();
+}
+
+__global__ void counts_kernel(int n, const double2* __restrict__ q, const double* __restrict__ mu,
+                              int nmu, int* __restrict__ out, int use_smem) {
+  extern __shared__ double2 sq[];
+  const double2* src = q;
+  if (use_smem) { stage_pairs(n, q, sq); src = sq; }
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nmu; j += gridDim.x * blockDim.x)
+    out[j] = sturm(n, src, mu[j]);
+}
+
+struct Node {
+  double lo, hi;
+  int clo, chi;
+  int done;   // 1: terminal (value = lo), 0: live
+  int pad;
+};
+
+__device__ __forceinline__ double midpoint(double lo, double hi) {
+  return __dmul_rn(__dadd_rn(lo, hi), 0.5);   // (lo + hi) / 2, the sum rounded once
+}
+
+// Counts at the 2^DEPTH - 1 midpoints of the subtree under every live node.
+__global__ void expand_kernel(int n, const double2* __restrict__ q, const Node* __restrict__ nodes,
+                              int nnodes, int* __restrict__ cnt, int use_smem) {
+  extern __shared__ double2 sq[];
+  const double2* src = q;
+  if (use_smem) { stage_pairs(n, q, sq); src = sq; }
+  const long total = (long)nnodes * NPTS;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total;
+       t += (long)gridDim.x * blockDim.x) {
+    const int u = (int)(t / NPTS);
+    const int h = (int)(t % NPTS) + 1;       // heap index in the subtree
+    const Node nd = nodes[u];
+    if (nd.done) continue;
+    double lo = nd.lo, hi = nd.hi;
+    const int depth = 31 - __clz(h);
+    for (int bit = depth - 1; bit >= 0; --bit) {
+      const double mid = midpoint(lo, hi);
+      if ((h >> bit) & 1) lo = mid; else hi = mid;
+    }
+    cnt[(long)u * NPTS + h - 1] = sturm(n, src, midpoint(lo, hi));
+  }
+}
+
+// One thread per node: replay the reference's pop/emit/push rules over the
+// node's subtree (upper child first) and write the resulting intervals in
+// descending order.
+__global__ void resolve_kernel(const Node* __restrict__ nodes, int nnodes, const int* __restrict__ cnt,
+                               double tol, Node* __restrict__ out, int* __restrict__ nout) {
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= nnodes) return;
+  Node nd = nodes[u];
+  Node* o = out + (long)u * FAN;
+  if (nd.done) { o[0] = nd; nout[u] = 1; return; }
+  struct Item { double lo, hi; int clo, chi, h; };
+  Item st[DEPTH + 2];
+  int sp = 0, k = 0;
+  st[sp++] = {nd.lo, nd.hi, nd.clo, nd.chi, 1};
+  while (sp > 0) {
+    const Item it = st[--sp];
+    const double mid = midpoint(it.lo, it.hi);
+    if (__dsub_rn(it.hi, it.lo) <= tol || mid == it.lo || mid == it.hi) {
+      o[k++] = {mid, mid, it.clo, it.chi, 1, 0};
+      continue;
+    }
+    if (it.h > NPTS) {                        // below this round's subtree: live next round
+      o[k++] = {it.lo, it.hi, it.clo, it.chi, 0, 0};
+      continue;
+    }
+    const int cm = cnt[(long)u * NPTS + it.h - 1];
+    if (cm > it.clo) st[sp++] = {it.lo, mid, it.clo, cm, 2 * it.h};       // lower, popped last
+    if (it.chi > cm) st[sp++] = {mid, it.hi, cm, it.chi, 2 * it.h + 1};   // upper, popped first
+  }
+  nout[u] = k;
+}
+
+// Single block: exclusive scan of nout, scatter into the next node list
+// (truncated to top_k), report (count, live count).
+__global__ void compact_kernel(const Node* __restrict__ cand, const int* __restrict__ nout, int nnodes,
+                               int top_k, Node* __restrict__ next, int* __restrict__ stats) {
+  __shared__ int warp_sums[32];
+  __shared__ int carry;
+  __shared__ int live_total;
+  if (threadIdx.x == 0) { carry = 0; live_total = 0; }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int base = 0; base < nnodes; base += blockDim.x) {
+    const int u = base + threadIdx.x;
+    const int v = (u < nnodes) ? nout[u] : 0;
+    int x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_sums[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+      int w = (lane < nw) ? warp_sums[lane] : 0;
+      for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, w, o);
+        if (lane >= o) w += y;
+      }
+      if (lane < nw) warp_sums[lane] = w;
+    }
+    __syncthreads();
+    const int excl = carry + (wid > 0 ? warp_sums[wid - 1] : 0) + x - v;
+    int live = 0;
+    for (int j = 0; j < v; ++j) {
+      const int dst = excl + j;
+      if (dst < top_k) {
+        const Node c = cand[(long)u * FAN + j];
+        next[dst] = c;
+        live += !c.done;
+      }
+    }
+    if (live) atomicAdd(&live_total, live);
+    __syncthreads();
+    if (threadIdx.x == 0) carry += warp_sums[nw - 1];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    stats[0] = carry < top_k ? carry : top_k;
+    stats[1] = live_total;
+  }
+}
+
+__global__ void emit_kernel(const Node* __restrict__ nodes, int n, double* __restrict__ sigma) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) sigma[i] = nodes[i].lo;
+}
+
+__global__ void root_kernel(double lo, double hi, const int* __restrict__ c, Node* nodes) {
+  nodes[0] = {lo, hi, c[0], c[1], 0, 0};
+}
+
+int smem_bytes(int n) { return n <= SMEM_PAIRS_MAX ? n * (int)sizeof(double2) : 0; }
+
+}  // namespace
+
+bbt_status sturm_counts(bbt_ctx* ctx, int n, const double* a, const double* b, const double* mu,
+                        int nmu, int* counts) {
+  if (n < 1 || nmu < 0) return fail(ctx, BBT_ERR_ARG, "sturm_counts: n=%d nmu=%d", n, nmu);
+  if (nmu == 0) return BBT_OK;
+  size_t mark = ctx->ws.top;
+  double2* q = ctx->ws.take<double2>(n);
+  if (!q) return fail(ctx, BBT_ERR_NOMEM, "sturm_counts: workspace");
+  squares_kernel<<<(n + 255) / 256, 256, 0, ctx->stream>>>(n, a, b, q);
+  BBT_LAUNCHED(ctx);
+  const int sm = smem_bytes(n);
+  if (sm > 48 * 1024)
+    BBT_CUDA(ctx, cudaFuncSetAttribute(counts_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  const int threads = 128;
+  int blocks = (nmu + threads - 1) / threads;
+  counts_kernel<<<blocks, threads, sm, ctx->stream>>>(n, q, mu, nmu, counts, sm > 0);
+  BBT_LAUNCHED(ctx);
+  ctx->ws.top = mark;
+  return BBT_OK;
+}
+
+bbt_status bisect(bbt_ctx* ctx, int n, const double* a, const double* b, double lo, double hi,
+                  double tol, int top_k, double* sigma, int* count) {
+  *count = 0;
+  if (n < 1) return fail(ctx, BBT_ERR_ARG, "bisection: n=%d", n);
+  if (top_k <= 0) return BBT_OK;
+  size_t mark = ctx->ws.top;
+  double2* q = ctx->ws.take<double2>(n);
+  double* ends = ctx->ws.take<double>(2);
+  int* c2 = ctx->ws.take<int>(2);
+  const int cap = n + 2;                    // live + terminal intervals never exceed the count range
+  Node* nodes = ctx->ws.take<Node>(cap);
+  Node* cand = ctx->ws.take<Node>((size_t)cap * FAN);
+  int* nout = ctx->ws.take<int>(cap);
+  int* cnt = ctx->ws.take<int>((size_t)cap * NPTS);
+  int* stats = ctx->ws.take<int>(2);
+  if (!stats) return fail(ctx, BBT_ERR_NOMEM, "bisection: workspace");
+  squares_kernel<<<(n + 255) / 256, 256, 0, ctx->stream>>>(n, a, b, q);
+  BBT_LAUNCHED(ctx);
+  const int sm = smem_bytes(n);
+  if (sm > 48 * 1024) {
+    BBT_CUDA(ctx, cudaFuncSetAttribute(counts_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    BBT_CUDA(ctx, cudaFuncSetAttribute(expand_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  }
+  double hend[2] = {lo, hi};
+  BBT_CUDA(ctx, cudaMemcpyAsync(ends, hend, sizeof(hend), cudaMemcpyHostToDevice, ctx->stream));
+  counts_kernel<<<1, 32, sm, ctx->stream>>>(n, q, ends, 2, c2, sm > 0);
+  BBT_LAUNCHED(ctx);
+  int hc[2];
+  BBT_CUDA(ctx, cudaMemcpyAsync(hc, c2, sizeof(hc), cudaMemcpyDeviceToHost, ctx->stream));
+  BBT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (!(hc[0] <= hc[1])) { ctx->ws.top = mark; return BBT_OK; }   // bbtsvd.cpp:26
+  root_kernel<<<1, 1, 0, ctx->stream>>>(lo, hi, c2, nodes);
+  BBT_LAUNCHED(ctx);
+  int N = 1, live = 1;
+  const int limit = top_k < cap ? top_k : cap;
+  ProfScope prof(ctx, BBT_PROF_BISECT, 0.0);
+  for (int round = 0; live > 0; ++round) {
+    if (round > 4096) return fail(ctx, BBT_ERR_TIMEOUT, "bisection: no convergence");
+    const long work = (long)N * NPTS;
+    int threads = 128;
+    long blocks = (work + threads - 1) / threads;
+    if (blocks > 65535) blocks = 65535;
+    expand_kernel<<<(int)blocks, threads, sm, ctx->stream>>>(n, q, nodes, N, cnt, sm > 0);
+    BBT_LAUNCHED(ctx);
+    resolve_kernel<<<(N + 127) / 128, 128, 0, ctx->stream>>>(nodes, N, cnt, tol, cand, nout);
+    BBT_LAUNCHED(ctx);
+    compact_kernel<<<1, 1024, 0, ctx->stream>>>(cand, nout, N, limit, nodes, stats);
+    BBT_LAUNCHED(ctx);
+    int hs[2];
+    BBT_CUDA(ctx, cudaMemcpyAsync(hs, stats, sizeof(hs), cudaMemcpyDeviceToHost, ctx->stream));
+    BBT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    N = hs[0];
+    live = hs[1];
+  }
+  if (N > 0) {
+    emit_kernel<<<(N + 255) / 256, 256, 0, ctx->stream>>>(nodes, N, sigma);
+    BBT_LAUNCHED(ctx);
+  }
+  *count = N;
+  ctx->ws.top = mark;
+  return BBT_OK;
+}
+
+}  // namespace bbt

@@ -1,0 +1,305 @@
+// Twisted-factorisation singular vectors and the bidiagonal SVD driver.
+//
+// Excalibur src/bbtsvd.cpp:54-147 computes, per singular value w, a
+// stationary (dstqds) and a progressive (dpqds) qd transform of the
+// LDL^T factorisation of B^T B - w^2 I, twists at argmin |gamma|, solves for
+// v, couples the factorisation over to B B^T - w^2 I and solves for u.
+// Each singular value is an independent O(n) recurrence, so one thread owns
+// one singular value.  The recurrences' work arrays are laid out
+// interleaved, element i of every thread's array contiguous
+// ([i][thread]), so a warp's loads and stores are coalesced; u lands
+// directly in U (n x cnt row-major, the reference's layout) and v goes
+// through the same interleaved layout and a tiled transpose into V.
+//
+// As in sturm.cu every operation is rounded separately (no FMA) in the
+// reference's order, and the 2-norm is the scaled sum of squares, so results
+// match the oracle bit for bit and the reference to rounding of its BLAS
+// dnrm2.
+#include <cuda_runtime.h>
+
+#include "internal.h"
+
+namespace bbt {
+namespace {
+
+#define MUL __dmul_rn
+#define DIV __ddiv_rn
+#define ADD __dadd_rn
+#define SUB __dsub_rn
+
+// LDL^T of B^T B, bbtsvd.cpp:54-63 (one thread: an O(n) recurrence).
+__global__ void ldl_kernel(int n, const double* __restrict__ a, const double* __restrict__ b,
+                           double* __restrict__ L, double* __restrict__ D) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  D[0] = MUL(a[0], a[0]);
+  for (int i = 1; i < n; ++i) {
+    const double ab = MUL(a[i - 1], b[i - 1]);
+    L[i - 1] = DIV(ab, D[i - 1]);
+    D[i] = SUB(ADD(MUL(a[i], a[i]), MUL(b[i - 1], b[i - 1])), DIV(MUL(ab, ab), D[i - 1]));
+  }
+}
+
+// Scaled sum-of-squares 2-norm in ascending index order (the oracle's norm).
+struct Nrm {
+  double scale = 0.0, ssq = 1.0;
+  __device__ __forceinline__ void add(double x) {
+    const double v = fabs(x);
+    if (v != 0.0) {
+      if (scale < v) {
+        const double r = DIV(scale, v);
+        ssq = ADD(1.0, MUL(MUL(ssq, r), r));
+        scale = v;
+      } else {
+        const double r = DIV(v, scale);
+        ssq = ADD(ssq, MUL(r, r));
+      }
+    }
+  }
+  __device__ __forceinline__ double get() const { return MUL(scale, sqrt(ssq)); }
+};
+
+// x[k] = 1, backward with lo, forward with up, normalise.  x has stride ld.
+// Returns the first index of max |x_i| after scaling.
+__device__ int twisted_solve(int n, int k, const double* lo, const double* up, long ldw, double* x,
+                             long ld) {
+  x[(long)k * ld] = 1.0;
+  double prev = 1.0;
+  for (int i = k - 1; i >= 0; --i) {
+    prev = MUL(-lo[(long)i * ldw], prev);
+    x[(long)i * ld] = prev;
+  }
+  prev = 1.0;
+  for (int i = k + 1; i < n; ++i) {
+    prev = MUL(-up[(long)(i - 1) * ldw], prev);
+    x[(long)i * ld] = prev;
+  }
+  Nrm nr;
+  for (int i = 0; i < n; ++i) nr.add(x[(long)i * ld]);
+  const double r = DIV(1.0, nr.get());
+  int best = 0;
+  double bv = 0.0;
+  for (int i = 0; i < n; ++i) {
+    const double v = MUL(x[(long)i * ld], r);
+    x[(long)i * ld] = v;
+    const double av = fabs(v);
+    if (i == 0 || av > bv) { bv = av; best = i; }   // first largest |x_i| (cblas_idamax)
+  }
+  return best;
+}
+
+// One thread per singular value j (bbtsvd.cpp:93-135, then the v sign rule
+// of :944-955 when sign_fix).  Work arrays are [i * cnt + j].
+__global__ void __launch_bounds__(64) twisted_kernel(
+    int n, int cnt, const double* __restrict__ sigma, const double* __restrict__ a,
+    const double* __restrict__ b, const double* __restrict__ L, const double* __restrict__ D,
+    double* __restrict__ S, double* __restrict__ Pp, double* __restrict__ DP, double* __restrict__ RP,
+    double* __restrict__ LP, double* __restrict__ UP, double* __restrict__ Vt, double* __restrict__ U,
+    int ldu, signed char* __restrict__ vsign, int sign_fix) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= cnt) return;
+  const long w = cnt;   // interleave stride
+  double* s = S + j;
+  double* p = Pp + j;
+  double* dp = DP + j;
+  double* rp = RP + j;
+  double* lp = LP + j;
+  double* up = UP + j;
+  const double om = sigma[j];
+  const double w2 = MUL(om, om);
+  // dstqds, bbtsvd.cpp:73-81
+  double si = -w2;
+  s[0] = si;
+  for (int i = 0; i + 1 < n; ++i) {
+    const double d = ADD(D[i], si);
+    dp[(long)i * w] = d;
+    const double l = DIV(MUL(D[i], L[i]), d);
+    lp[(long)i * w] = l;
+    si = SUB(MUL(MUL(l, L[i]), si), w2);
+    s[(long)(i + 1) * w] = si;
+  }
+  dp[(long)(n - 1) * w] = ADD(D[n - 1], si);
+  // dpqds, bbtsvd.cpp:83-91, with gamma (:107) and its argmin (:108)
+  double pi = SUB(D[n - 1], w2);
+  p[(long)(n - 1) * w] = pi;
+  // first index of the smallest |gamma_i| in ascending order; a NaN
+  // gamma_0 wins outright and other NaNs never do (the oracle's argmin)
+  int k = n - 1;
+  double gbest = fabs(ADD(ADD(s[(long)(n - 1) * w], pi), w2));
+  double g0 = gbest;
+  for (int i = n - 2; i >= 0; --i) {
+    const double r = ADD(MUL(D[i], MUL(L[i], L[i])), pi);
+    rp[(long)(i + 1) * w] = r;
+    up[(long)i * w] = DIV(MUL(L[i], D[i]), r);
+    pi = SUB(DIV(MUL(pi, D[i]), r), w2);
+    p[(long)i * w] = pi;
+    const double g = fabs(ADD(ADD(s[(long)i * w], pi), w2));
+    if (g == g && (gbest != gbest || g <= gbest)) { gbest = g; k = i; }
+    g0 = g;
+  }
+  if (g0 != g0) k = 0;
+  rp[0] = pi;
+  // v (:111)
+  const int pv = twisted_solve(n, k, lp, up, w, Vt + j, w);
+  // coupling (:114-124): s[n] = -w2, p[n] = 1, rp[n] = 1
+  int k2 = 0;
+  double g2best = 0.0;
+  double dprev = 0.0;
+  for (int i = 0; i < n; ++i) {
+    const double s_i = s[(long)i * w];
+    const double s_n = (i + 1 < n) ? s[(long)(i + 1) * w] : -w2;
+    const double p_i = p[(long)i * w];
+    const double p_n = (i + 1 < n) ? p[(long)(i + 1) * w] : 1.0;
+    const double r_n = (i + 1 < n) ? rp[(long)(i + 1) * w] : 1.0;
+    const double d_new = MUL(DIV(s_n, s_i), dp[(long)i * w]);
+    const double g_old = ADD(ADD(s_i, p_i), w2);
+    const double g_new = fabs(DIV(MUL(MUL(-w2, g_old), r_n), MUL(s_i, p_n)));
+    if (i == 0 || g_new < g2best) { g2best = g_new; k2 = i; }
+    const double r_new = MUL(DIV(p_i, p_n), r_n);
+    if (i > 0) {
+      lp[(long)(i - 1) * w] = MUL(DIV(a[i], dprev), b[i - 1]);
+      up[(long)(i - 1) * w] = MUL(DIV(a[i], r_new), b[i - 1]);
+    }
+    dprev = d_new;
+  }
+  // u (:126), column j of U
+  twisted_solve(n, k2, lp, up, w, U + j, ldu);
+  signed char sg = 1;
+  if (sign_fix) {   // bbtsvd.cpp:944-955: align v with B^T u at v's largest entry
+    const double vp = Vt[(long)pv * w + j];
+    double sgn;
+    if (pv == 0) sgn = DIV(MUL(U[j], a[0]), om);
+    else sgn = DIV(ADD(MUL(U[(long)(pv - 1) * ldu + j], b[pv - 1]), MUL(U[(long)pv * ldu + j], a[pv])), om);
+    if (MUL(sgn, vp) < 0) sg = -1;
+  }
+  vsign[j] = sg;
+}
+
+// V (cnt x n) = sign_j * Vt^T, Vt interleaved (n x cnt).
+__global__ void vtranspose_kernel(int n, int cnt, const double* __restrict__ Vt,
+                                  const signed char* __restrict__ vsign, double* __restrict__ V) {
+  __shared__ double tile[32][33];
+  const int i0 = blockIdx.x * 32, j0 = blockIdx.y * 32;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int i = i0 + r, j = j0 + threadIdx.x;
+    if (i < n && j < cnt) tile[r][threadIdx.x] = Vt[(long)i * cnt + j];
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int j = j0 + r, i = i0 + threadIdx.x;
+    if (i < n && j < cnt) {
+      const double v = tile[threadIdx.x][r];
+      V[(long)j * n + i] = vsign[j] < 0 ? -v : v;
+    }
+  }
+}
+
+// bbtsvd.cpp:957-967: a value equal (to 1e-15) to alpha_i gets unit vectors.
+__global__ void check_none_kernel(int k, int top_k, const double* __restrict__ sigma,
+                                  const double* __restrict__ a, double* __restrict__ U,
+                                  double* __restrict__ V) {
+  const int i = blockIdx.x;
+  if (i >= top_k) return;
+  if (!(fabs(SUB(sigma[i], a[i])) < 1e-15)) return;
+  for (int j = threadIdx.x; j < k; j += blockDim.x) {
+    if (j == i) U[(long)i * top_k + i] = 1.0;
+    if (j > i && j < top_k) U[(long)i * top_k + j] = 0.0;
+    if (j > i) U[(long)j * top_k + i] = 0.0;
+    V[(long)i * k + j] = (j == i) ? 1.0 : 0.0;
+  }
+}
+
+// client.cpp:988-995: make the largest |entry| of each u positive, flipping
+// u and v together.  One thread per column of U (k x cnt row-major).
+__global__ void global_sign_kernel(int k, int cnt, double* __restrict__ U, double* __restrict__ V) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= cnt) return;
+  int best = 0;
+  double bv = fabs(U[j]);
+  for (int i = 1; i < k; ++i) {
+    const double v = fabs(U[(long)i * cnt + j]);
+    if (v > bv) { bv = v; best = i; }
+  }
+  if (U[(long)best * cnt + j] < 0) {
+    for (int i = 0; i < k; ++i) U[(long)i * cnt + j] = -U[(long)i * cnt + j];
+    for (int i = 0; i < k; ++i) V[(long)j * k + i] = -V[(long)j * k + i];
+  }
+}
+
+// ||a||^2 + ||b||^2 with the scaled norm (bbtsvd.cpp:936), one thread.
+__global__ void bound_kernel(int n, const double* __restrict__ a, const double* __restrict__ b,
+                             double* __restrict__ out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  Nrm na, nb;
+  for (int i = 0; i < n; ++i) na.add(a[i]);
+  for (int i = 0; i + 1 < n; ++i) nb.add(b[i]);
+  const double x = na.get(), y = nb.get();
+  out[0] = ADD(MUL(x, x), MUL(y, y));
+}
+
+}  // namespace
+
+bbt_status twisted(bbt_ctx* ctx, int n, int cnt, const double* sigma, const double* a,
+                   const double* b, double* U, int ldu, double* V, bool sign_fix) {
+  if (n < 1 || cnt < 0 || cnt > n) return fail(ctx, BBT_ERR_ARG, "twisted: n=%d cnt=%d", n, cnt);
+  if (cnt == 0) return BBT_OK;
+  size_t mark = ctx->ws.top;
+  const size_t col = (size_t)(n + 1) * cnt;
+  double* L = ctx->ws.take<double>(n);
+  double* D = ctx->ws.take<double>(n);
+  double* S = ctx->ws.take<double>(col);
+  double* P = ctx->ws.take<double>(col);
+  double* DP = ctx->ws.take<double>(col);
+  double* RP = ctx->ws.take<double>(col);
+  double* LP = ctx->ws.take<double>(col);
+  double* UPa = ctx->ws.take<double>(col);
+  double* Vt = ctx->ws.take<double>((size_t)n * cnt);
+  signed char* vs = ctx->ws.take<signed char>(cnt);
+  if (!vs) return fail(ctx, BBT_ERR_NOMEM, "twisted: workspace (%zu MB)", (col * 7 * 8) >> 20);
+  ProfScope prof(ctx, BBT_PROF_TWISTED, 0.0);
+  ldl_kernel<<<1, 1, 0, ctx->stream>>>(n, a, b, L, D);
+  BBT_LAUNCHED(ctx);
+  twisted_kernel<<<(cnt + 31) / 32, 32, 0, ctx->stream>>>(n, cnt, sigma, a, b, L, D, S, P, DP, RP, LP,
+                                                         UPa, Vt, U, ldu, vs, sign_fix ? 1 : 0);
+  BBT_LAUNCHED(ctx);
+  dim3 tb(32, 8), tg((n + 31) / 32, (cnt + 31) / 32);
+  vtranspose_kernel<<<tg, tb, 0, ctx->stream>>>(n, cnt, Vt, vs, V);
+  BBT_LAUNCHED(ctx);
+  ctx->ws.top = mark;
+  return BBT_OK;
+}
+
+bbt_status bidiag_bound(bbt_ctx* ctx, int n, const double* a, const double* b, double* out) {
+  bound_kernel<<<1, 1, 0, ctx->stream>>>(n, a, b, out);
+  BBT_LAUNCHED(ctx);
+  return BBT_OK;
+}
+
+bbt_status bidiag_svd(bbt_ctx* ctx, int k, const double* a, const double* b, double* U, double* V,
+                      double* sigma, int top_k, bool global_sign) {
+  if (k < 1 || top_k < 1 || top_k > k) return fail(ctx, BBT_ERR_ARG, "bidiagonal svd: k=%d top_k=%d", k, top_k);
+  size_t mark = ctx->ws.top;
+  double* bound = ctx->ws.take<double>(1);
+  if (!bound) return fail(ctx, BBT_ERR_NOMEM, "bidiagonal svd: workspace");
+  bound_kernel<<<1, 1, 0, ctx->stream>>>(k, a, b, bound);
+  BBT_LAUNCHED(ctx);
+  double hb = 0;
+  BBT_CUDA(ctx, cudaMemcpyAsync(&hb, bound, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  BBT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  int cnt = 0;
+  BBT_TRY(bisect(ctx, k, a, b, 0.0, hb, 1e-20, top_k, sigma, &cnt));
+  if (cnt < top_k) {
+    ctx->ws.top = mark;
+    return fail(ctx, BBT_ERR_COUNT, "bisection found %d singular values, %d requested", cnt, top_k);
+  }
+  BBT_TRY(twisted(ctx, k, top_k, sigma, a, b, U, top_k, V, true));
+  check_none_kernel<<<top_k, 128, 0, ctx->stream>>>(k, top_k, sigma, a, U, V);
+  BBT_LAUNCHED(ctx);
+  if (global_sign) {
+    global_sign_kernel<<<(top_k + 63) / 64, 64, 0, ctx->stream>>>(k, top_k, U, V);
+    BBT_LAUNCHED(ctx);
+  }
+  ctx->ws.top = mark;
+  return BBT_OK;
+}
+
+}  // namespace bbt

@@ -1,0 +1,172 @@
+/*
+ * bbtsvd_b200.h — C ABI of the B200 (sm_100a) implementation of Excalibur's
+ * matrix-factorisation hot path.
+ *
+ * Two layers:
+ *   1. The reference's own C++ API (Excalibur include/bbtsvd.hpp:22-47) is
+ *      exported with identical mangled signatures by libexcalibur_b200.so
+ *      (host pointers in, host pointers out), so the reference's
+ *      DecentralizedClient links it in place of src/bbtsvd.cpp.
+ *   2. This header: extern "C", device pointers, stream-ordered, every call
+ *      returns a bbt_status instead of asserting.  The entries for the math
+ *      that the reference keeps inline in DecentralizedClient::run()
+ *      (local QR, global QR, Ralha bidiagonalisation, back-transforms) and
+ *      a whole-pipeline entry for P participants held as separate device
+ *      buffers on one GPU are additions with a cited reference site each.
+ *
+ * Layout conventions follow the reference: "row-major m x n" means element
+ * (i, j) at x[i*n + j]; a participant's block is row-major m x local_n.
+ * Device pointers must be 8-byte aligned.  A bbt_ctx owns one CUDA stream
+ * (or borrows the caller's), a device workspace and the last error text; it
+ * is not thread-safe — use one context per host thread.
+ */
+#ifndef BBTSVD_B200_H
+#define BBTSVD_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  BBT_OK = 0,
+  BBT_ERR_ARG = 1,          /* invalid size / pointer / option */
+  BBT_ERR_CUDA = 2,         /* a CUDA runtime call failed */
+  BBT_ERR_COUNT = 3,        /* bisection found fewer singular values than requested
+                               (the reference asserts here, bbtsvd.cpp:938) */
+  BBT_ERR_NOMEM = 4,        /* device allocation failed */
+  BBT_ERR_TIMEOUT = 5,      /* a bounded device-side wait gave up */
+  BBT_ERR_UNSUPPORTED = 6   /* shape or mode outside what the reference supports */
+} bbt_status;
+
+typedef struct bbt_ctx bbt_ctx;
+
+/* ---- context ----------------------------------------------------------- */
+bbt_status bbt_create(bbt_ctx** ctx, int device);
+bbt_status bbt_destroy(bbt_ctx* ctx);
+/* Borrow a cudaStream_t (passed as void*); NULL restores the context's own. */
+bbt_status bbt_set_stream(bbt_ctx* ctx, void* stream);
+bbt_status bbt_synchronize(bbt_ctx* ctx);
+const char* bbt_last_error(const bbt_ctx* ctx);
+const char* bbt_status_string(bbt_status s);
+/* Kernels launched by this context since creation (all are this library's). */
+uint64_t bbt_kernel_launches(const bbt_ctx* ctx);
+
+/* ---- bidiagonal SVD (Excalibur src/bbtsvd.cpp) ---------------------------
+ * alpha[n] is the diagonal, beta[n-1] the superdiagonal of an upper
+ * bidiagonal B.                                                             */
+
+/* Sturm count of B^T B - mu^2 I for nmu shifts: counts[i] = number of
+ * negative pivots at mu[i].  Replaces negative_count, bbtsvd.cpp:7-17. */
+bbt_status bbt_negative_count(bbt_ctx* ctx, int n, const double* d_alpha, const double* d_beta,
+                              const double* d_mu, int nmu, int* d_counts);
+
+/* Singular values in (lo, hi] by the reference's bisection tree (upper half
+ * first, stop when the midpoint no longer splits the interval or the width
+ * is <= tol), at most top_k, descending; *h_count receives how many.
+ * Replaces bisection_singular_values, bbtsvd.cpp:19-52. */
+bbt_status bbt_bisection(bbt_ctx* ctx, int n, const double* d_alpha, const double* d_beta,
+                         double lo, double hi, double tol, int top_k, double* d_sigma,
+                         int* h_count);
+
+/* Twisted-factorisation singular vectors for cnt singular values:
+ * v_i -> row i of d_V (cnt x n), u_i -> column i of d_U (n x cnt).
+ * Replaces two_side_singular_vectors_twisted_factorization,
+ * bbtsvd.cpp:138-147. */
+bbt_status bbt_twisted_vectors(bbt_ctx* ctx, int n, int cnt, const double* d_sigma,
+                               const double* d_alpha, const double* d_beta, double* d_U,
+                               double* d_V);
+
+/* Top-k bisection + twisted vectors + the reference's sign fixes.
+ * d_U: k x top_k row-major, d_V: top_k x k row-major, d_sigma: top_k.
+ * Replaces bidiagonal_bisection_twisted_svd (top-k overload),
+ * bbtsvd.cpp:932-968. */
+bbt_status bbt_bidiagonal_svd(bbt_ctx* ctx, int k, const double* d_alpha, const double* d_beta,
+                              double* d_U, double* d_V, double* d_sigma, int top_k);
+
+/* ---- data masks (Excalibur src/bbtsvd.cpp) --------------------------------
+ * The random tables are drawn on the host with the reference's own calls
+ * (srand(seed), std::default_random_engine(seed), std::shuffle, rand()), so
+ * the result equals the reference's bit for bit and glibc's rand() state is
+ * left as the reference leaves it.                                          */
+
+/* Replaces givens_mask_cache_optimized_parallel_with_simd,
+ * bbtsvd.cpp:727-876.  In place on d_x (row-major m x n). */
+bbt_status bbt_givens_mask(bbt_ctx* ctx, size_t m, size_t n, size_t mask_times, double* d_x,
+                           int mask, int is_left, unsigned seed);
+
+/* Replaces block_shift_mask, bbtsvd.cpp:533-669 (direct path for a rotated
+ * dimension <= 10000, near-square virtual-matrix path above it). */
+bbt_status bbt_block_shift_mask(bbt_ctx* ctx, size_t m, size_t n, size_t mask_times, double* d_x,
+                                int mask, int is_left, unsigned seed);
+
+/* ---- QR (Excalibur src/client.cpp) ----------------------------------------
+ * Householder QR of A = X^T, X row-major m x local_n (so A is column-major
+ * local_n x m, local_n >= m).  d_rt receives R^T (row-major m x m, lower
+ * triangular: the reference's shrinked_x).  With compute_q, d_x is
+ * overwritten by Q^T (row-major m x local_n; the reference's local_v);
+ * otherwise d_x holds the Householder vectors.
+ * Replaces DecentralizedClient::local_qr_reduction, client.cpp:417-445. */
+bbt_status bbt_local_qr(bbt_ctx* ctx, size_t m, size_t local_n, double* d_x, double* d_rt,
+                        int compute_q);
+
+/* ---- FP64 GEMM ------------------------------------------------------------
+ * Column-major BLAS convention: C = alpha op(A) op(B) + beta C, op(A) M x K,
+ * op(B) K x N (trans: 0 = 'N', 1 = 'T').  On the FP64 tensor path (DMMA).
+ * Replaces the cblas_dgemm calls of the back-transforms, client.cpp:1011,
+ * 1018, 1179, 1190. */
+bbt_status bbt_dgemm(bbt_ctx* ctx, int transa, int transb, int M, int N, long K, double alpha,
+                     const double* d_A, long lda, const double* d_B, long ldb, double beta,
+                     double* d_C, long ldc);
+
+/* ---- kernel profiling -------------------------------------------------------
+ * With profiling on, every launch of the library's kernels of a class is
+ * bracketed by CUDA events on the launching stream.  bbt_profile_get
+ * (synchronises) returns, per class, the summed event time, the number of
+ * launches and the algorithmic work (flops for BBT_PROF_DGEMM and
+ * BBT_PROF_PANEL, bytes moved for BBT_PROF_MASK) since profiling was
+ * switched on. */
+enum { BBT_PROF_DGEMM = 0, BBT_PROF_PANEL = 1, BBT_PROF_MASK = 2, BBT_PROF_RALHA = 3,
+       BBT_PROF_BISECT = 4, BBT_PROF_TWISTED = 5, BBT_PROF_CLASSES = 6 };
+bbt_status bbt_profile(bbt_ctx* ctx, int enable);
+bbt_status bbt_profile_get(bbt_ctx* ctx, int cls, double* ms, uint64_t* launches, double* work);
+
+/* ---- whole pipeline ------------------------------------------------------
+ * DecentralizedClient::run() (client.cpp:447-1200), short-and-wide branch
+ * (m <= global_n), svd_mode 1 (two-sided) with opt_control 3, for P
+ * participants held as separate device buffers on one GPU; the socket
+ * all-reduce / all-gather become in-device reductions.                     */
+typedef struct {
+  int participants;              /* P >= 1 */
+  size_t m;                      /* rows of every block (reference: m) */
+  const size_t* local_n;         /* P column counts (reference: local_n) */
+  unsigned public_seed;          /* shared mask seed (client.cpp:498) */
+  const unsigned* private_seeds; /* P private mask seeds (client.cpp:531) */
+  int top_k;                     /* <= 0: all singular values (client.cpp:971) */
+  int precision;                 /* 0: plain FP64 (the only mode so far) */
+} bbt_fedsvd_config;
+
+/* Device-resident run.  d_blocks[c]: row-major m x local_n[c] input, used as
+ * workspace (overwritten).  Outputs: d_sigma[m], d_U row-major m x k (the
+ * reference's FinalU), d_VT[c] row-major k x local_n[c] (FinalVT); *h_k is
+ * the number of singular values k.  Replaces client.cpp:572-1199. */
+bbt_status bbt_fedsvd_run(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* d_blocks,
+                          double* d_sigma, double* d_U, double* const* d_VT, int* h_k);
+
+/* Same with host buffers (pinned or pageable): copies in, runs, copies out;
+ * inputs are not modified. */
+bbt_status bbt_fedsvd_run_host(bbt_ctx* ctx, const bbt_fedsvd_config* cfg,
+                               const double* const* h_blocks, double* h_sigma, double* h_U,
+                               double* const* h_VT, int* h_k);
+
+/* Per-stage wall time (ms, CUDA events) of the last bbt_fedsvd_run, in the
+ * reference's phase order: local_qr, apply_mask, global_qr, bi_diag, bsvd,
+ * combine_svd_remove_mask.  n must be >= 6. */
+bbt_status bbt_fedsvd_stage_ms(const bbt_ctx* ctx, double* ms, int n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BBTSVD_B200_H */
