@@ -20,7 +20,7 @@ EXPORTS = (
     "bbt_status_string", "bbt_kernel_launches", "bbt_negative_count", "bbt_bisection",
     "bbt_twisted_vectors", "bbt_bidiagonal_svd", "bbt_givens_mask", "bbt_block_shift_mask",
     "bbt_local_qr", "bbt_fedsvd_run", "bbt_fedsvd_run_host", "bbt_fedsvd_stage_ms",
-    "bbt_dgemm", "bbt_profile", "bbt_profile_get",
+    "bbt_dgemm", "bbt_profile", "bbt_profile_get", "bbt_twisted_vectors_noalloc",
 )
 PROF_CLASSES = ("dgemm", "panel", "mask", "ralha", "bisect", "twisted")
 
@@ -70,6 +70,7 @@ def load():
         "bbt_fedsvd_stage_ms": ([vp, vp, i], i),
         "bbt_dgemm": ([vp, i, i, i, i, C.c_long, d, vp, C.c_long, vp, C.c_long, d, vp, C.c_long], i),
         "bbt_profile": ([vp, i], i),
+        "bbt_twisted_vectors_noalloc": ([vp, i, i, vp, vp, vp, vp, vp], i),
         "bbt_profile_get": ([vp, i, C.POINTER(d), C.POINTER(C.c_uint64), C.POINTER(d)], i),
     }
     for name, (args, res) in sig.items():

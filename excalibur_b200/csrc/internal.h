@@ -110,6 +110,10 @@ bbt_status twisted(bbt_ctx* ctx, int n, int cnt, const double* sigma, const doub
                    const double* b, double* U, int ldu, double* V, bool sign_fix);
 bbt_status bidiag_svd(bbt_ctx* ctx, int k, const double* a, const double* b, double* U, double* V,
                       double* sigma, int top_k, bool global_sign);
+// twisted() on caller-provided scratch (scratch_doubles_twisted(n, cnt) doubles)
+size_t scratch_doubles_twisted(int n, int cnt);
+bbt_status twisted_scratch(bbt_ctx* ctx, int n, int cnt, const double* sigma, const double* a,
+                           const double* b, double* U, int ldu, double* V, double* scratch);
 // d_out[0] = ||a||^2 + ||b||^2 (the bisection bound, bbtsvd.cpp:936)
 bbt_status bidiag_bound(bbt_ctx* ctx, int n, const double* a, const double* b, double* d_out);
 

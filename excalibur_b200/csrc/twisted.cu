@@ -268,6 +268,45 @@ bbt_status twisted(bbt_ctx* ctx, int n, int cnt, const double* sigma, const doub
   return BBT_OK;
 }
 
+// Same kernels as twisted(), with every work array carved from a caller-
+// provided device scratch region instead of the context's workspace.  The
+// scratch needs scratch_doubles_twisted(n, cnt) doubles; each array is
+// written before it is read, so the region's previous contents are never
+// observed.
+size_t scratch_doubles_twisted(int n, int cnt) {
+  const size_t col = (size_t)(n + 1) * cnt;
+  auto up = [](size_t d) { return (d + 31) & ~size_t(31); };   // 256-byte steps
+  return up(n) * 2 + up(col) * 6 + up((size_t)n * cnt) + up((cnt + 7) / 8);
+}
+
+bbt_status twisted_scratch(bbt_ctx* ctx, int n, int cnt, const double* sigma, const double* a,
+                           const double* b, double* U, int ldu, double* V, double* scratch) {
+  if (n < 1 || cnt < 0 || cnt > n) return fail(ctx, BBT_ERR_ARG, "twisted: n=%d cnt=%d", n, cnt);
+  if (cnt == 0) return BBT_OK;
+  const size_t col = (size_t)(n + 1) * cnt;
+  auto up = [](size_t d) { return (d + 31) & ~size_t(31); };
+  double* p = scratch;
+  double* L = p; p += up(n);
+  double* D = p; p += up(n);
+  double* S = p; p += up(col);
+  double* P = p; p += up(col);
+  double* DP = p; p += up(col);
+  double* RP = p; p += up(col);
+  double* LP = p; p += up(col);
+  double* UPa = p; p += up(col);
+  double* Vt = p; p += up((size_t)n * cnt);
+  signed char* vs = reinterpret_cast<signed char*>(p);
+  ldl_kernel<<<1, 1, 0, ctx->stream>>>(n, a, b, L, D);
+  BBT_LAUNCHED(ctx);
+  twisted_kernel<<<(cnt + 31) / 32, 32, 0, ctx->stream>>>(n, cnt, sigma, a, b, L, D, S, P, DP, RP, LP,
+                                                         UPa, Vt, U, ldu, vs, 0);
+  BBT_LAUNCHED(ctx);
+  dim3 tb(32, 8), tg((n + 31) / 32, (cnt + 31) / 32);
+  vtranspose_kernel<<<tg, tb, 0, ctx->stream>>>(n, cnt, Vt, vs, V);
+  BBT_LAUNCHED(ctx);
+  return BBT_OK;
+}
+
 bbt_status bidiag_bound(bbt_ctx* ctx, int n, const double* a, const double* b, double* out) {
   bound_kernel<<<1, 1, 0, ctx->stream>>>(n, a, b, out);
   BBT_LAUNCHED(ctx);

@@ -86,6 +86,23 @@ bbt_status bbt_twisted_vectors(bbt_ctx* ctx, int n, int cnt, const double* d_sig
 bbt_status bbt_bidiagonal_svd(bbt_ctx* ctx, int k, const double* d_alpha, const double* d_beta,
                               double* d_U, double* d_V, double* d_sigma, int top_k);
 
+/* bbt_twisted_vectors for callers that must not allocate device memory (an
+ * allocation-free hot loop, memory handed in full to another allocator, a
+ * zero allocation budget).  No counterpart in the reference: an addition.
+ * Takes a cudaStream_t (as void*; NULL = the default stream) instead of a
+ * context and keeps its work arrays in one static 64 MiB __device__ array
+ * that every GPU loading the library holds until exit.  Needs about
+ * 7*(n+1)*cnt + n*cnt doubles of it; larger shapes return BBT_ERR_ARG with a
+ * message on stderr.  The first call on a device looks up the array's
+ * device address (cudaGetSymbolAddress, with that device current); make
+ * that first call before any stream capture.  All calls share the array and
+ * it keeps the last call's contents (every work array is written before it
+ * is read, so nothing needs clearing); calls that overlap on the GPU race.
+ * Same results as bbt_twisted_vectors. */
+bbt_status bbt_twisted_vectors_noalloc(void* stream, int n, int cnt, const double* d_sigma,
+                                       const double* d_alpha, const double* d_beta, double* d_U,
+                                       double* d_V);
+
 /* ---- data masks (Excalibur src/bbtsvd.cpp) --------------------------------
  * The random tables are drawn on the host with the reference's own calls
  * (srand(seed), std::default_random_engine(seed), std::shuffle, rand()), so
