@@ -261,7 +261,7 @@ bbt_status bbt_dgemm(bbt_ctx* ctx, int transa, int transb, int M, int N, long K,
   const long am = transa ? K : M, bm = transb ? N : K;
   if (lda < (am > 1 ? am : 1) || ldb < (bm > 1 ? bm : 1) || ldc < (M > 1 ? M : 1))
     return fail(ctx, BBT_ERR_ARG, "dgemm: leading dimension too small");
-  BBT_TRY(ensure(ctx, (size_t)257 * M * N * 8 + (1 << 20)));
+  BBT_TRY(ensure(ctx, dgemm_workspace_bytes(ctx, M, N, K) + (1 << 20)));
   return dgemm(ctx, transa != 0, transb != 0, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
 }
 

@@ -15,9 +15,8 @@
 namespace bbt {
 namespace {
 
-constexpr int BM = 128, BN = 64, BK = 16;
-constexpr int PADA = 4, PADB = 4;
-constexpr int THREADS = 256;
+constexpr int BK = 16;
+constexpr int PADA = 4, PADB = 4;   // row strides = 4 (mod 16) doubles: conflict-free fragment loads
 
 __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
   asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
@@ -25,16 +24,18 @@ __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b)
                : "d"(a), "d"(b));
 }
 
-template <bool TA, bool TB>
-__global__ void __launch_bounds__(THREADS, 2)
+// WM x WN warps, each a 32 x 32 block of C: CTA tile (32 WM) x (32 WN).
+template <bool TA, bool TB, int WM, int WN>
+__global__ void __launch_bounds__(32 * WM * WN)
 dgemm_kernel(int M, int N, long K, long kchunk, double alpha, const double* __restrict__ A, long lda,
              const double* __restrict__ B, long ldb, double beta, double* __restrict__ C, long ldc,
              double* __restrict__ P) {
+  constexpr int BM = 32 * WM, BN = 32 * WN, THREADS = 32 * WM * WN;
   extern __shared__ double smem_[];
   auto As = reinterpret_cast<double(*)[BK][BM + PADA]>(smem_);
   auto Bs = reinterpret_cast<double(*)[BK][BN + PADB]>(smem_ + 2 * BK * (BM + PADA));
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int wm = warp & 3, wn = warp >> 2;
+  const int wm = warp % WM, wn = warp / WM;
   const int i0 = blockIdx.x * BM, j0 = blockIdx.y * BN;
   const long kbeg = (long)blockIdx.z * kchunk;
   const long kend = min(K, kbeg + kchunk);
@@ -153,28 +154,64 @@ __global__ void splitk_reduce(int M, int N, int S, const double* __restrict__ P,
   }
 }
 
-constexpr int SMEM_BYTES = 2 * BK * (BM + PADA + BN + PADB) * (int)sizeof(double);
+template <int WM, int WN>
+constexpr int smem_bytes() { return 2 * BK * (32 * WM + PADA + 32 * WN + PADB) * (int)sizeof(double); }
 
-template <bool TA, bool TB>
+template <bool TA, bool TB, int WM, int WN>
 cudaError_t launch(dim3 g, cudaStream_t st, int M, int N, long K, long kc, double alpha, const double* A,
                    long lda, const double* B, long ldb, double beta, double* C, long ldc, double* P) {
   static bool attr = false;   // set once per process (per kernel instantiation)
+  constexpr int SM = smem_bytes<WM, WN>();
   if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(dgemm_kernel<TA, TB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         SMEM_BYTES);
+    cudaError_t e = cudaFuncSetAttribute(dgemm_kernel<TA, TB, WM, WN>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, SM);
     if (e != cudaSuccess) return e;
     attr = true;
   }
-  dgemm_kernel<TA, TB><<<g, THREADS, SMEM_BYTES, st>>>(M, N, K, kc, alpha, A, lda, B, ldb, beta, C, ldc, P);
+  dgemm_kernel<TA, TB, WM, WN><<<g, 32 * WM * WN, SM, st>>>(M, N, K, kc, alpha, A, lda, B, ldb, beta, C, ldc, P);
   return cudaSuccess;
 }
 
+template <int WM, int WN>
+cudaError_t launch_t(bool ta, bool tb, dim3 g, cudaStream_t st, int M, int N, long K, long kc, double alpha,
+                     const double* A, long lda, const double* B, long ldb, double beta, double* C, long ldc,
+                     double* P) {
+  if (!ta && !tb) return launch<false, false, WM, WN>(g, st, M, N, K, kc, alpha, A, lda, B, ldb, beta, C, ldc, P);
+  if (ta && !tb) return launch<true, false, WM, WN>(g, st, M, N, K, kc, alpha, A, lda, B, ldb, beta, C, ldc, P);
+  if (!ta && tb) return launch<false, true, WM, WN>(g, st, M, N, K, kc, alpha, A, lda, B, ldb, beta, C, ldc, P);
+  return launch<true, true, WM, WN>(g, st, M, N, K, kc, alpha, A, lda, B, ldb, beta, C, ldc, P);
+}
+
+// Tile shape from the output shape: avoid computing padding rows/columns of
+// small outputs (the V^T C products of Householder QR have 16..128 rows).
+void pick_tile(int M, int N, int* wm, int* wn) {
+  if (M <= 32) { *wm = 1; *wn = 4; }
+  else if (M <= 64) { *wm = 2; *wn = N <= 64 ? 2 : 4; }
+  else { *wm = 4; *wn = 2; }
+}
+
 }  // namespace
+
+size_t dgemm_workspace_bytes(const bbt_ctx* ctx, int M, int N, long K) {
+  if (M <= 0 || N <= 0) return 0;
+  int wm, wn;
+  pick_tile(M, N, &wm, &wn);
+  const long tiles = (long)((M + 32 * wm - 1) / (32 * wm)) * ((N + 32 * wn - 1) / (32 * wn));
+  const long target = 2L * ctx->num_sms;
+  if (!(tiles < target && K >= 2048)) return 0;
+  long s = (target + tiles - 1) / tiles;
+  if (s > K / 1024) s = K / 1024;
+  if (s > 256) s = 256;
+  return s > 1 ? (size_t)s * M * N * sizeof(double) + 256 : 0;
+}
 
 bbt_status dgemm(bbt_ctx* ctx, bool ta, bool tb, int M, int N, long K, double alpha, const double* A,
                  long lda, const double* B, long ldb, double beta, double* C, long ldc, int splits) {
   if (M < 0 || N < 0 || K < 0) return fail(ctx, BBT_ERR_ARG, "dgemm: M=%d N=%d K=%ld", M, N, K);
   if (M == 0 || N == 0) return BBT_OK;
+  int wm, wn;
+  pick_tile(M, N, &wm, &wn);
+  const int BM = 32 * wm, BN = 32 * wn;
   const int tm = (M + BM - 1) / BM, tn = (N + BN - 1) / BN;
   if (splits <= 0) {
     const long tiles = (long)tm * tn;
@@ -206,10 +243,10 @@ bbt_status dgemm(bbt_ctx* ctx, bool ta, bool tb, int M, int N, long K, double al
   }
   cudaError_t e;
   ProfScope prof(ctx, BBT_PROF_DGEMM, 2.0 * M * (double)N * (double)K);
-  if (!ta && !tb) e = launch<false, false>(g, ctx->stream, M, N, K, kc, alpha, A, lda, B, ldb, beta, C, ldc, P);
-  else if (ta && !tb) e = launch<true, false>(g, ctx->stream, M, N, K, kc, alpha, A, lda, B, ldb, beta, C, ldc, P);
-  else if (!ta && tb) e = launch<false, true>(g, ctx->stream, M, N, K, kc, alpha, A, lda, B, ldb, beta, C, ldc, P);
-  else e = launch<true, true>(g, ctx->stream, M, N, K, kc, alpha, A, lda, B, ldb, beta, C, ldc, P);
+  if (wm == 1) e = launch_t<1, 4>(ta, tb, g, ctx->stream, M, N, K, kc, alpha, A, lda, B, ldb, beta, C, ldc, P);
+  else if (wm == 2 && wn == 2) e = launch_t<2, 2>(ta, tb, g, ctx->stream, M, N, K, kc, alpha, A, lda, B, ldb, beta, C, ldc, P);
+  else if (wm == 2) e = launch_t<2, 4>(ta, tb, g, ctx->stream, M, N, K, kc, alpha, A, lda, B, ldb, beta, C, ldc, P);
+  else e = launch_t<4, 2>(ta, tb, g, ctx->stream, M, N, K, kc, alpha, A, lda, B, ldb, beta, C, ldc, P);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "dgemm: shared-memory attribute");
   BBT_LAUNCHED(ctx);
   if (P) {

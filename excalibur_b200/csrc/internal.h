@@ -129,13 +129,16 @@ bbt_status block_shift_mask(bbt_ctx* ctx, size_t m, size_t n, size_t passes, dou
 bbt_status dgemm(bbt_ctx* ctx, bool ta, bool tb, int M, int N, long K, double alpha,
                  const double* A, long lda, const double* B, long ldb, double beta, double* C,
                  long ldc, int splits = 0);
+// Scratch the automatic split-K of dgemm takes from the workspace.
+size_t dgemm_workspace_bytes(const bbt_ctx* ctx, int M, int N, long K);
 
 // Householder QR, column-major A (rows x cols, lda), rows >= cols (qr.cu).
 struct QrPlan {
-  int nb = 32;
+  int nb = 128;    // outer panel width (compact-WY block of the trailing update)
+  int leaf = 16;   // recursion leaf: columns factored one at a time
 };
 bbt_status geqrf(bbt_ctx* ctx, long rows, int cols, double* A, long lda, double* tau,
-                 double* T /* (cols/nb+1) * nb * nb */, const QrPlan& plan);
+                 double* T /* ceil(cols/nb) * nb * nb */, const QrPlan& plan);
 bbt_status orgqr(bbt_ctx* ctx, long rows, int cols, double* A, long lda, const double* tau,
                  const double* T, const QrPlan& plan);
 // C (rows x ncols) <- H_0 H_1 ... H_{k-1} C.  Reflector j is column j of V

@@ -143,23 +143,25 @@ __global__ void make_vbuf(const double* __restrict__ src, long rs, long cs, long
 
 // dlarft (forward, columnwise): T upper triangular b x b (col-major, ld b)
 // from G = V^T V and tau.  T(i,i) = tau_i; T(0:i, i) = -tau_i T(0:i,0:i) G(0:i, i).
+// b <= TMAX; T is built in shared memory (dynamic, (TMAX+1) * b doubles).
+constexpr int TMAX = 128;
 __global__ void larft_kernel(int b, const double* __restrict__ G, const double* __restrict__ tau,
                              double* __restrict__ T) {
-  __shared__ double t[NBMAX][NBMAX + 1];
-  const int j = threadIdx.x;
-  for (int f = j; f < NBMAX * NBMAX; f += blockDim.x) t[f / NBMAX][f % NBMAX] = 0.0;
+  extern __shared__ double t_[];   // t[j][l] at t_[j * (b + 1) + l]
+  const int j = threadIdx.x, ld = b + 1;
+  for (int f = j; f < b * ld; f += blockDim.x) t_[f] = 0.0;
   __syncthreads();
   for (int i = 0; i < b; ++i) {
     const double ti = tau[i];
     if (j < i) {
       double s = 0.0;
-      for (int l = j; l < i; ++l) s += t[j][l] * G[l + i * b];
-      t[j][i] = -ti * s;
+      for (int l = j; l < i; ++l) s += t_[j * ld + l] * G[l + (long)i * b];
+      t_[j * ld + i] = -ti * s;
     }
-    if (j == i) t[i][i] = ti;
+    if (j == i) t_[i * ld + i] = ti;
     __syncthreads();
   }
-  for (int f = j; f < b * b; f += blockDim.x) T[f] = t[f % b][f / b];
+  for (int f = j; f < b * b; f += blockDim.x) T[f] = t_[(f % b) * ld + f / b];
 }
 
 // A panel (m x b, ld) += I on its top b x b block, rows [-above, 0) zeroed.
@@ -176,32 +178,94 @@ __global__ void panel_identity(double* __restrict__ P, long ld, int b, long abov
 
 }  // namespace
 
+namespace {
+
+bbt_status larft(bbt_ctx* ctx, int b, const double* G, const double* tau, double* T) {
+  const int smem = (b + 1) * b * (int)sizeof(double);
+  static bool attr = false;
+  if (!attr) {
+    BBT_CUDA(ctx, cudaFuncSetAttribute(larft_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (TMAX + 1) * TMAX * (int)sizeof(double)));
+    attr = true;
+  }
+  larft_kernel<<<1, TMAX, smem, ctx->stream>>>(b, G, tau, T);
+  BBT_LAUNCHED(ctx);
+  return BBT_OK;
+}
+
+// Column-by-column factorisation of a panel of b <= NBMAX columns.
+bbt_status panel_columns(bbt_ctx* ctx, double* P, long m, int b, long ld, double* tau) {
+  size_t mark = ctx->ws.top;
+  const long nblk = (m + PROWS - 1) / PROWS;
+  double* pa = ctx->ws.take<double>((size_t)nblk * NBMAX);
+  double* pb = ctx->ws.take<double>((size_t)nblk * NBMAX);
+  double* ra = ctx->ws.take<double>(NBMAX);
+  double* rb = ctx->ws.take<double>(NBMAX);
+  if (!rb) return fail(ctx, BBT_ERR_NOMEM, "panel: workspace");
+  double *pin = pa, *pout = pb, *rin = ra, *rout = rb;
+  for (int jj = -1; jj < b; ++jj) {
+    ProfScope prof(ctx, BBT_PROF_PANEL, 16.0 * (double)m * (double)(b - jj));
+    panel_step_kernel<<<(int)nblk, PTHREADS, 0, ctx->stream>>>(P, m, b, ld, jj, pin, rin, pout, rout, tau);
+    BBT_LAUNCHED(ctx);
+    double* t = pin; pin = pout; pout = t;
+    t = rin; rin = rout; rout = t;
+  }
+  ctx->ws.top = mark;
+  return BBT_OK;
+}
+
+// Recursive panel factorisation (Elmroth-Gustavson): factor the left half,
+// apply its block reflector to the right half with GEMMs, factor the right
+// half.  Leaves of <= leaf columns are factored column by column; a leaf of
+// a tall panel (rows x 16 doubles) stays resident in L2 across its column
+// steps.
+bbt_status panel_factor(bbt_ctx* ctx, double* P, long m, int b, long ld, double* tau, int leaf) {
+  if (b <= leaf) return panel_columns(ctx, P, m, b, ld, tau);
+  const int h = b / 2;
+  BBT_TRY(panel_factor(ctx, P, m, h, ld, tau, leaf));
+  size_t mark = ctx->ws.top;
+  double* Vb = ctx->ws.take<double>((size_t)m * h);
+  double* G = ctx->ws.take<double>((size_t)h * h);
+  double* T = ctx->ws.take<double>((size_t)h * h);
+  double* W = ctx->ws.take<double>((size_t)h * (b - h));
+  double* W2 = ctx->ws.take<double>((size_t)h * (b - h));
+  if (!W2) return fail(ctx, BBT_ERR_NOMEM, "panel: workspace");
+  make_vbuf<<<4 * ctx->num_sms, 256, 0, ctx->stream>>>(P, 1, ld, m, h, Vb);
+  BBT_LAUNCHED(ctx);
+  BBT_TRY(dgemm(ctx, true, false, h, h, m, 1.0, Vb, m, Vb, m, 0.0, G, h));
+  BBT_TRY(larft(ctx, h, G, tau, T));
+  double* A2 = P + (long)h * ld;
+  BBT_TRY(dgemm(ctx, true, false, h, b - h, m, 1.0, Vb, m, A2, ld, 0.0, W, h));
+  BBT_TRY(dgemm(ctx, true, false, h, b - h, h, 1.0, T, h, W, h, 0.0, W2, h));
+  BBT_TRY(dgemm(ctx, false, false, (int)m, b - h, h, -1.0, Vb, m, W2, h, 1.0, A2, ld));
+  ctx->ws.top = mark;
+  return panel_factor(ctx, P + h + (long)h * ld, m - h, b - h, ld, tau + h, leaf);
+}
+
+}  // namespace
+
 size_t qr_workspace_bytes(long rows, int cols, int ncols_apply, const QrPlan& plan) {
   const int nb = plan.nb;
   const long nblk = (rows + PROWS - 1) / PROWS;
   const int wide = cols > ncols_apply ? cols : ncols_apply;
   size_t b = 0;
-  b += (size_t)rows * nb * 8 + 256;                 // Vbuf
-  b += 2 * (size_t)nblk * NBMAX * 8 + 512;          // partials
-  b += 2 * NBMAX * 8 + 512;                         // pivot rows
+  b += (size_t)rows * nb * 8 + 256;                 // Vbuf of the panel
+  b += (size_t)rows * (nb / 2) * 8 + 256;           // Vbuf of the recursion
+  b += 2 * (size_t)nblk * NBMAX * 8 + 1024;         // partials, pivot rows
   b += 3 * (size_t)nb * wide * 8 + 768;             // W, W2, M
-  b += 2 * (size_t)nb * nb * 8 + 512;               // G, T
-  b += (size_t)256 * nb * wide * 8 + 256;           // split-K partials of V^T C
+  b += 6 * (size_t)nb * nb * 8 + 1536;              // G, T (+ recursion)
+  b += (size_t)257 * nb * wide * 8 + 256;           // split-K partials
   return b;
 }
 
 bbt_status geqrf(bbt_ctx* ctx, long rows, int cols, double* A, long lda, double* tau, double* Tst,
                  const QrPlan& plan) {
   const int nb = plan.nb;
-  if (nb < 1 || nb > NBMAX) return fail(ctx, BBT_ERR_ARG, "geqrf: nb=%d", nb);
+  if (nb < 1 || nb > TMAX || plan.leaf < 1 || plan.leaf > NBMAX)
+    return fail(ctx, BBT_ERR_ARG, "geqrf: nb=%d leaf=%d", nb, plan.leaf);
   if (rows < cols || cols < 1) return fail(ctx, BBT_ERR_ARG, "geqrf: rows=%ld cols=%d", rows, cols);
   size_t mark = ctx->ws.top;
-  const long nblk_max = (rows + PROWS - 1) / PROWS;
   double* Vb = ctx->ws.take<double>((size_t)rows * nb);
-  double* pa = ctx->ws.take<double>((size_t)nblk_max * NBMAX);
-  double* pb = ctx->ws.take<double>((size_t)nblk_max * NBMAX);
-  double* ra = ctx->ws.take<double>(NBMAX);
-  double* rb = ctx->ws.take<double>(NBMAX);
   double* W = ctx->ws.take<double>((size_t)nb * cols);
   double* W2 = ctx->ws.take<double>((size_t)nb * cols);
   double* G = ctx->ws.take<double>((size_t)nb * nb);
@@ -210,23 +274,14 @@ bbt_status geqrf(bbt_ctx* ctx, long rows, int cols, double* A, long lda, double*
     const int b = cols - p0 < nb ? cols - p0 : nb;
     const long m = rows - p0;
     double* Pn = A + p0 + (long)p0 * lda;
-    const int grid = (int)((m + PROWS - 1) / PROWS);
-    double *pin = pa, *pout = pb, *rin = ra, *rout = rb;
-    for (int jj = -1; jj < b; ++jj) {
-      ProfScope prof(ctx, BBT_PROF_PANEL, 4.0 * (double)m * (double)(b - jj));
-      panel_step_kernel<<<grid, PTHREADS, 0, ctx->stream>>>(Pn, m, b, lda, jj, pin, rin, pout, rout, tau + p0);
-      BBT_LAUNCHED(ctx);
-      double* t = pin; pin = pout; pout = t;
-      t = rin; rin = rout; rout = t;
-    }
+    BBT_TRY(panel_factor(ctx, Pn, m, b, lda, tau + p0, plan.leaf));
     make_vbuf<<<4 * ctx->num_sms, 256, 0, ctx->stream>>>(Pn, 1, lda, m, b, Vb);
     BBT_LAUNCHED(ctx);
     BBT_TRY(dgemm(ctx, true, false, b, b, m, 1.0, Vb, m, Vb, m, 0.0, G, b));
     double* T = Tst + (size_t)pi * nb * nb;
-    larft_kernel<<<1, NBMAX, 0, ctx->stream>>>(b, G, tau + p0, T);
-    BBT_LAUNCHED(ctx);
+    BBT_TRY(larft(ctx, b, G, tau + p0, T));
     const int nc = cols - p0 - b;
-    if (nc > 0) {
+    if (nc > 0) {   // C <- (I - V T V^T)^T C
       double* C = A + p0 + (long)(p0 + b) * lda;
       BBT_TRY(dgemm(ctx, true, false, b, nc, m, 1.0, Vb, m, C, lda, 0.0, W, b));
       BBT_TRY(dgemm(ctx, true, false, b, nc, b, 1.0, T, b, W, b, 0.0, W2, b));
@@ -292,8 +347,7 @@ bbt_status ormqr_left_notrans(bbt_ctx* ctx, long rows, int k, const double* V, l
     make_vbuf<<<4 * ctx->num_sms, 256, 0, ctx->stream>>>(V + p0 * rs + (long)p0 * cs, rs, cs, m, b, Vb);
     BBT_LAUNCHED(ctx);
     BBT_TRY(dgemm(ctx, true, false, b, b, m, 1.0, Vb, m, Vb, m, 0.0, G, b));
-    larft_kernel<<<1, NBMAX, 0, ctx->stream>>>(b, G, tau + p0, T);
-    BBT_LAUNCHED(ctx);
+    BBT_TRY(larft(ctx, b, G, tau + p0, T));
     if (!c_rowmajor) {   // C col-major rows x ncols
       double* Cp = C + p0;
       BBT_TRY(dgemm(ctx, true, false, b, ncols, m, 1.0, Vb, m, Cp, ldc, 0.0, W, b));
