@@ -30,10 +30,16 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 CONFIGS = {
-    # name: (participants, m, local_n, spectrum)
+    # name: (participants, m, local_n (first participant; see make_blocks), spectrum)
     "c2": (2, 1000, 500_000, "geometric"),
     "c1": (2, 100, 1000, "gaussian"),
+    "c3": (64, 512, 0, "scaled"),   # rows per participant uniform in [10,000, 200,000]
 }
+
+
+def c3_rows(seed=0):
+    """Row counts of the 64 participants of c3 (seeded)."""
+    return [int(r) for r in np.random.default_rng(seed).integers(10_000, 200_001, 64)]
 METRIC = "SVD wall-s at rel err <=1e-10 vs FP64 oracle"
 
 
@@ -97,6 +103,11 @@ def make_blocks(torch, dev, P, m, n, spectrum, seed=0):
     g = torch.Generator(device=dev).manual_seed(seed)
     if spectrum == "gaussian":
         return [torch.randn(m, n, generator=g, device=dev, dtype=torch.float64) for _ in range(P)], None
+    if spectrum == "scaled":   # c3: N(0,1) entries times 10^U[-2,2] per participant
+        rows = c3_rows(seed)
+        scl = np.random.default_rng(seed + 1).uniform(-2.0, 2.0, P)
+        return [torch.randn(m, r, generator=g, device=dev, dtype=torch.float64) * float(10.0 ** f)
+                for r, f in zip(rows, scl)], None
     G = torch.randn(P * n, m, generator=g, device=dev, dtype=torch.float64)
     Q, R = torch.linalg.qr(G)
     Q *= torch.sign(torch.diagonal(R))
@@ -112,10 +123,11 @@ def make_blocks(torch, dev, P, m, n, spectrum, seed=0):
 
 
 def fp64_oracle(torch, blocks):
-    """FP64 SVD of the stored X on the GPU (cuSOLVER QR + SVD): the
-    measurement's accuracy oracle, not part of the timed path."""
-    X = torch.cat(blocks, dim=1)                 # m x global_n
-    R = torch.linalg.qr(X.T, mode="r")[1]        # X^T = Q R  ->  X = R^T Q^T
+    """FP64 SVD of the stored X on the GPU (cuSOLVER Householder QR of every
+    block, QR of the stacked R factors, SVD): the measurement's accuracy
+    oracle, not part of the timed path.  X^T = Q R, so X = R^T Q^T."""
+    Rs = [torch.linalg.qr(b.T, mode="r")[1] for b in blocks]
+    R = torch.linalg.qr(torch.cat(Rs, dim=0), mode="r")[1]
     Ur, s, Vh = torch.linalg.svd(R.T)
     return s, Ur
 
@@ -140,8 +152,10 @@ def accuracy(torch, s_ref, U_ref, s, U):
 # ---------------------------------------------------------------- reference arm
 def reference_run(P, m, n, seed=0, threads=None, workdir=None):
     """One run of the reference's own pipeline (oracle/_ref/ref_pipeline, P
-    processes over loopback TCP).  Returns (max run seconds over participants,
-    per-phase seconds of participant 0)."""
+    processes over loopback TCP; n is one local_n for all or a list).
+    Returns (max run seconds over participants, per-phase seconds of
+    participant 0, threads used)."""
+    ns = list(n) if isinstance(n, (list, tuple)) else [n] * P
     exe = os.path.join(ROOT, "oracle", "_ref", "ref_pipeline")
     if not os.path.exists(exe):
         raise FileNotFoundError(exe)
@@ -150,14 +164,14 @@ def reference_run(P, m, n, seed=0, threads=None, workdir=None):
     rng = np.random.default_rng(seed)
     with tempfile.TemporaryDirectory(dir=workdir) as td:
         for c in range(P):
-            rng.standard_normal((m, n)).tofile(os.path.join(td, f"Client{c}.mat"))
+            rng.standard_normal((m, ns[c])).tofile(os.path.join(td, f"Client{c}.mat"))
         env = dict(os.environ, OMP_NUM_THREADS=str(threads), OPENBLAS_NUM_THREADS=str(threads))
         port = 20000 + (os.getpid() * 7 + int(time.time())) % 20000
         procs = []
         for c in range(P):
             od = os.path.join(td, f"o{c}")
             os.makedirs(od)
-            procs.append(subprocess.Popen([exe, str(c), str(P), str(m), str(n), str(port), td, td, "0", "1", "-1", od],
+            procs.append(subprocess.Popen([exe, str(c), str(P), str(m), str(ns[c]), str(port), td, td, "0", "1", "-1", od],
                                           stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL, env=env, cwd=td))
         for pr in procs:
             if pr.wait(timeout=1800) != 0:
@@ -165,23 +179,34 @@ def reference_run(P, m, n, seed=0, threads=None, workdir=None):
         times = [list(map(float, open(os.path.join(td, f"o{c}", "time.txt")).read().split())) for c in range(P)]
     total = max(t[0] for t in times)
     ph = times[0]
+    used = min(threads * P, cores)
     phases = dict(zip(("total", "local_qr", "global_qr", "apply_mask", "exchange", "bi_diag", "bsvd", "combine",
                        "comm"), ph))
-    return total, phases, threads * P
+    return total, phases, used
 
 
 def reference_extrapolated(P, m, n_full, n_sample, steps=1, seed=0):
-    """Reference time on a bounded sample (local_n = n_sample), extrapolated to
-    local_n = n_full: the phases whose work grows with local_n (local QR, the
-    V back-transform in combine) scale by n_full/n_sample, the m-sized
-    phases (masks, global QR, Ralha, bisection) are kept."""
+    """Reference time on a bounded sample (local_n = n_sample; lists allowed),
+    extrapolated to local_n = n_full: the phases whose work grows with
+    local_n (local QR, the V back-transform in combine) scale by the row
+    ratio, the m-sized phases (masks, global QR, Ralha, bisection) are kept."""
     vals = []
+    full = sum(n_full) if isinstance(n_full, (list, tuple)) else n_full * P
+    samp = sum(n_sample) if isinstance(n_sample, (list, tuple)) else n_sample * P
     for i in range(steps):
         total, ph, cores = reference_run(P, m, n_sample, seed=seed + i)
-        scale = n_full / n_sample
+        scale = full / samp
         grow = ph["local_qr"] + ph["combine"]
         vals.append(total + grow * (scale - 1.0))
     return statistics.median(vals), cores, ph
+
+
+def sample_rows(args, P, n):
+    """(full local_n, sampled local_n) for the CPU reference sample."""
+    if args.config == "c3":
+        full = c3_rows(0)
+        return full, [max(3100, r // 20) for r in full]
+    return n, min(args.cpu_sample_rows, n)
 
 
 # ---------------------------------------------------------------- our arm
@@ -215,6 +240,9 @@ def run_ours(args, rank, world):
     pristine = [b.clone() for b in blocks]
     s_ref, U_ref = fp64_oracle(torch, pristine)
     pub, priv = eb.reference_seeds(0, P)
+    tuned = None
+    if sum(1 for b in pristine if b.shape[1] // m > 5) >= 8:   # batched local QR: tune it once
+        tuned = ctx.fedsvd_tune(m, [b.shape[1] for b in pristine])
 
     def step():
         for b, p0 in zip(blocks, pristine):
@@ -255,7 +283,7 @@ def run_ours(args, rank, world):
         t = torch.tensor([sec], device=dev)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         sec = float(t)
-    res = {"sec": sec, "host_sec": statistics.median(times), "stage_ms": stage, "acc": acc,
+    res = {"sec": sec, "host_sec": statistics.median(times), "stage_ms": stage, "acc": acc, "tuned": tuned,
            "launches": launches, "prof": prof, "clocks": clk.summary()}
     if rank == 0:
         res["dgemm_peak"] = cublas_dgemm_peak(torch, dev)
@@ -267,7 +295,7 @@ def run_ours(args, rank, world):
         torch.cuda.empty_cache()
         outbuf = (torch.empty(m, dtype=torch.float64).pin_memory().numpy(),
                   torch.empty(m * m, dtype=torch.float64).pin_memory().numpy(),
-                  [torch.empty(m * nn, dtype=torch.float64).pin_memory().numpy() for nn in [n] * P])
+                  [torch.empty(m * p0.shape[1], dtype=torch.float64).pin_memory().numpy() for p0 in pristine])
         ctx.fedsvd_host(hb, pub, priv, out=outbuf)     # warm
         et = []
         for _ in range(max(1, min(args.steps, 3))):
@@ -276,7 +304,7 @@ def run_ours(args, rank, world):
             et.append(time.perf_counter() - t0)
         k = len(sg)
         res["e2e"] = {"value": statistics.median(et), "unit": "s", "h2d_bytes_per_step": int(sum(h.nbytes for h in hb)),
-                      "d2h_bytes_per_step": int(8 * (k + m * k + k * n * P))}
+                      "d2h_bytes_per_step": int(8 * (k + m * k + k * sum(h.shape[1] for h in hb)))}
     return res
 
 
@@ -287,23 +315,29 @@ def main():
     P, m, n, spectrum = CONFIGS[args.config]
     if args.rows:
         n = args.rows
-    workload = f"{args.config}: {P} participants x {n} x {m} FP64 (reference m={m}, local_n={n})"
+    if args.config == "c3":
+        rows = c3_rows(0)
+        workload = (f"c3: 64 participants, rows {min(rows)}..{max(rows)} (sum {sum(rows)}) x 512 FP64, "
+                    f"entries N(0,1) x 10^U[-2,2] per participant")
+    else:
+        workload = f"{args.config}: {P} participants x {n} x {m} FP64 (reference m={m}, local_n={n})"
     cfg = {"workload": workload, "participants": P, "m": m, "local_n": n, "spectrum": spectrum,
            "mode": "svd_mode 1 (two-sided), opt_control 3, full spectrum",
-           "l2": "inputs (%.1f GB) larger than L2; restored from a device copy before each step" % (P * m * n * 8 / 1e9),
+           "l2": "inputs (%.1f GB) larger than L2; restored from a device copy before each step" % (
+               (sum(c3_rows(0)) if args.config == "c3" else P * n) * m * 8 / 1e9),
            "parallelism": "replicas only" if args.gpus > 1 else "1 GPU"}
     if args.impl == "reference":
         if rank != 0:
             return
-        ns = min(args.cpu_sample_rows, n)
+        nfull, ns = sample_rows(args, P, n)
         vals = []
         for i in range(args.warmup + args.steps):
-            v, cores, ph = reference_extrapolated(P, m, n, ns, steps=1, seed=i)
+            v, cores, ph = reference_extrapolated(P, m, nfull, ns, steps=1, seed=i)
             if i >= args.warmup:
                 vals.append(v)
         val = statistics.median(vals)
         sample = (f"reference pipeline (oracle/_ref, its own sources) at local_n={ns}; local QR and "
-                  f"back-transform phases scaled by {n}/{ns}")
+                  f"back-transform phases scaled to the full row count")
         print(json.dumps({"impl": "reference", "metric": METRIC, "value": val, "unit": "s", "n_gpus": args.gpus,
                           "steps": args.steps, "warmup": args.warmup, "ms_per_step": val * 1e3,
                           "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -345,17 +379,20 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
             "accuracy": res["acc"], "stage_ms": res["stage_ms"], "host_s_per_step": res["host_sec"],
             "gpu_launches": res["launches"], "roofline": roof,
+            "batched_local_qr": (None if res["tuned"] is None else
+                                 {"streams": res["tuned"][0], "panel_width": res["tuned"][1],
+                                  "tuning_ms": res["tuned"][2], "graph": "captured on the 2nd call, replayed after"}),
             "kernel_classes": {k: {"ms": v[0], "launches": v[1]} for k, v in prof.items()},
             "clocks": res["clocks"]}
     if "e2e" in res:
         line["e2e"] = res["e2e"]
     if not args.no_cpu_baseline:
-        ns = min(args.cpu_sample_rows, n)
+        nfull, ns = sample_rows(args, P, n)
         try:
-            v, cores, ph = reference_extrapolated(P, m, n, ns, steps=1)
+            v, cores, ph = reference_extrapolated(P, m, nfull, ns, steps=1)
             line["cpu_baseline"] = {"value": v, "unit": "s", "cores": cores, "kind": "reference",
                                     "sample": f"reference pipeline at local_n={ns}, local QR and back-transform "
-                                              f"phases scaled by {n}/{ns}", "sample_phases_s": ph}
+                                              f"phases scaled to the full row count", "sample_phases_s": ph}
         except Exception as e:   # the checker build is missing on this machine
             line["cpu_baseline"] = {"value": None, "unit": "s", "cores": os.cpu_count(), "kind": "reference",
                                     "sample": f"unavailable: {e}"}

@@ -185,20 +185,21 @@ class Context:
         self.sync()
         return rt
 
-    def _config(self, m, local_n, public_seed, private_seeds, top_k, precision):
+    def _config(self, m, local_n, public_seed, private_seeds, top_k, svd_mode, precision):
         P = len(local_n)
         self._ln = (C.c_size_t * P)(*local_n)
         self._ps = (C.c_uint * P)(*[s & 0xFFFFFFFF for s in private_seeds])
-        return FedSVDConfig(P, m, self._ln, public_seed & 0xFFFFFFFF, self._ps, top_k, precision)
+        return FedSVDConfig(P, m, self._ln, public_seed & 0xFFFFFFFF, self._ps, top_k, svd_mode, precision)
 
-    def fedsvd(self, blocks, public_seed, private_seeds, top_k=-1, precision=0):
+    def fedsvd(self, blocks, public_seed, private_seeds, top_k=-1, svd_mode=1, precision=0):
         """DecentralizedClient::run() for P participants on this GPU
         (client.cpp:447-1200).  blocks: list of m x local_n CUDA tensors,
-        overwritten.  Returns (sigma k, FinalU m x k, [FinalVT_c k x local_n])."""
+        overwritten.  Returns (sigma k, FinalU m x k, [FinalVT_c k x local_n]);
+        FinalU is None in svd_mode 3 and the FinalVT list None in svd_mode 2."""
         P = len(blocks)
         m = blocks[0].shape[0]
         ln = [b.shape[1] for b in blocks]
-        cfg = self._config(m, ln, public_seed, private_seeds, top_k, precision)
+        cfg = self._config(m, ln, public_seed, private_seeds, top_k, svd_mode, precision)
         sig = self._empty(m)
         U = self._empty(m * m)
         VT = [self._empty(m * n) for n in ln]
@@ -210,15 +211,27 @@ class Context:
                     "fedsvd")
         self.sync()
         k = k.value
-        return sig[:k], U[: m * k].view(m, k), [v[: k * n].view(k, n) for v, n in zip(VT, ln)]
+        Uo = U[: m * k].view(m, k) if svd_mode != 3 else None
+        VTo = [v[: k * n].view(k, n) for v, n in zip(VT, ln)] if svd_mode != 2 else None
+        return sig[:k], Uo, VTo
 
-    def fedsvd_host(self, blocks, public_seed, private_seeds, top_k=-1, precision=0, out=None):
+    def fedsvd_tune(self, m, local_n, top_k=-1, svd_mode=1):
+        """Autotune the batched local QR for these shapes (kept in the
+        context).  Returns (streams, panel width, ms)."""
+        cfg = self._config(m, list(local_n), 0, [0] * len(local_n), top_k, svd_mode, 0)
+        st, nb, ms = C.c_int(), C.c_int(), C.c_double()
+        self._pre()
+        self._check(self.L.bbt_fedsvd_tune(self.h, C.byref(cfg), C.byref(st), C.byref(nb), C.byref(ms)),
+                    "fedsvd_tune")
+        return st.value, nb.value, ms.value
+
+    def fedsvd_host(self, blocks, public_seed, private_seeds, top_k=-1, svd_mode=1, precision=0, out=None):
         """Same through the host-pointer entry (bbt_fedsvd_run_host): numpy
         blocks in, numpy results out (copies timed inside the call)."""
         P = len(blocks)
         m = blocks[0].shape[0]
         ln = [b.shape[1] for b in blocks]
-        cfg = self._config(m, ln, public_seed, private_seeds, top_k, precision)
+        cfg = self._config(m, ln, public_seed, private_seeds, top_k, svd_mode, precision)
         blocks = [np.ascontiguousarray(b, dtype=np.float64) for b in blocks]
         if out is None:
             out = (np.empty(m), np.empty(m * m), [np.empty(m * n) for n in ln])
@@ -260,6 +273,23 @@ class Context:
             self._check(self.L.bbt_profile_get(self.h, i, C.byref(ms), C.byref(n), C.byref(w)), "profile_get")
             out[name] = (ms.value, n.value, w.value)
         return out
+
+    def svd_dense(self, X, top_k=-1):
+        """SVD of a dense m x m matrix (CUDA tensor, overwritten) by Ralha
+        bidiagonalisation + bisection + twisted vectors + back-transforms.
+        Returns (sigma k, U m x k, VT k x m)."""
+        m = X.shape[0]
+        assert X.shape == (m, m)
+        sig = self._empty(m)
+        U = self._empty(m * m)
+        VT = self._empty(m * m)
+        k = C.c_int(0)
+        self._pre()
+        self._check(self.L.bbt_svd_dense(self.h, m, self._p(X), top_k, self._p(sig), self._p(U), self._p(VT),
+                                         C.byref(k)), "svd_dense")
+        self.sync()
+        k = k.value
+        return sig[:k], U[: m * k].view(m, k), VT[: k * m].view(k, m)
 
     def stage_ms(self):
         """Per-phase ms of the last fedsvd: local_qr, apply_mask, global_qr,

@@ -21,6 +21,7 @@ EXPORTS = (
     "bbt_twisted_vectors", "bbt_bidiagonal_svd", "bbt_givens_mask", "bbt_block_shift_mask",
     "bbt_local_qr", "bbt_fedsvd_run", "bbt_fedsvd_run_host", "bbt_fedsvd_stage_ms",
     "bbt_dgemm", "bbt_profile", "bbt_profile_get", "bbt_twisted_vectors_noalloc",
+    "bbt_svd_dense", "bbt_fedsvd_tune",
 )
 PROF_CLASSES = ("dgemm", "panel", "mask", "ralha", "bisect", "twisted")
 
@@ -33,6 +34,7 @@ class FedSVDConfig(C.Structure):
         ("public_seed", C.c_uint),
         ("private_seeds", C.POINTER(C.c_uint)),
         ("top_k", C.c_int),
+        ("svd_mode", C.c_int),
         ("precision", C.c_int),
     ]
 
@@ -70,6 +72,8 @@ def load():
         "bbt_fedsvd_stage_ms": ([vp, vp, i], i),
         "bbt_dgemm": ([vp, i, i, i, i, C.c_long, d, vp, C.c_long, vp, C.c_long, d, vp, C.c_long], i),
         "bbt_profile": ([vp, i], i),
+        "bbt_svd_dense": ([vp, i, vp, i, vp, vp, vp, C.POINTER(i)], i),
+        "bbt_fedsvd_tune": ([vp, C.POINTER(FedSVDConfig), C.POINTER(i), C.POINTER(i), C.POINTER(d)], i),
         "bbt_twisted_vectors_noalloc": ([vp, i, i, vp, vp, vp, vp, vp], i),
         "bbt_profile_get": ([vp, i, C.POINTER(d), C.POINTER(C.c_uint64), C.POINTER(d)], i),
     }

@@ -104,6 +104,9 @@ bbt_status bbt_destroy(bbt_ctx* ctx) {
   if (!ctx) return BBT_ERR_ARG;
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
+  if (ctx->qr_graph) cudaGraphExecDestroy(ctx->qr_graph);
+  for (auto s : ctx->side) cudaStreamDestroy(s);
+  for (auto e : ctx->side_ev) cudaEventDestroy(e);
   if (ctx->ws.base) cudaFree(ctx->ws.base);
   if (ctx->d_flag) cudaFree(ctx->d_flag);
   if (ctx->d_barrier) cudaFree(ctx->d_barrier);
@@ -203,17 +206,21 @@ bbt_status bbt_local_qr(bbt_ctx* ctx, size_t m, size_t local_n, double* x, doubl
 bbt_status bbt_fedsvd_run(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* blocks,
                           double* sigma, double* U, double* const* VT, int* k) {
   if (!ctx) return BBT_ERR_ARG;
-  if (!cfg || !blocks || !VT || !k || bad(sigma) || bad(U)) return fail(ctx, BBT_ERR_ARG, "fedsvd: NULL argument");
+  if (!cfg || !blocks || !k || bad(sigma)) return fail(ctx, BBT_ERR_ARG, "fedsvd: NULL argument");
+  const bool want_u = cfg->svd_mode != 3, want_v = cfg->svd_mode != 2;
+  if ((want_u && bad(U)) || (want_v && !VT)) return fail(ctx, BBT_ERR_ARG, "fedsvd: NULL output");
   for (int c = 0; c < cfg->participants; ++c)
-    if (bad(blocks[c]) || bad(VT[c])) return fail(ctx, BBT_ERR_ARG, "fedsvd: participant %d buffer", c);
+    if (bad(blocks[c]) || (want_v && bad(VT[c]))) return fail(ctx, BBT_ERR_ARG, "fedsvd: participant %d buffer", c);
   return fedsvd(ctx, cfg, blocks, sigma, U, VT, k);
 }
 
 bbt_status bbt_fedsvd_run_host(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, const double* const* hX,
                                double* hsigma, double* hU, double* const* hVT, int* k) {
   if (!ctx) return BBT_ERR_ARG;
-  if (!cfg || !hX || !hVT || !k || !hsigma || !hU || cfg->participants < 1 || !cfg->local_n)
+  if (!cfg || !hX || !k || !hsigma || cfg->participants < 1 || !cfg->local_n)
     return fail(ctx, BBT_ERR_ARG, "fedsvd_host: NULL argument");
+  const bool want_u = cfg->svd_mode != 3, want_v = cfg->svd_mode != 2;
+  if ((want_u && !hU) || (want_v && !hVT)) return fail(ctx, BBT_ERR_ARG, "fedsvd_host: NULL output");
   const int P = cfg->participants;
   const size_t m = cfg->m;
   std::vector<double*> dX(P, nullptr), dVT(P, nullptr);
@@ -229,11 +236,11 @@ bbt_status bbt_fedsvd_run_host(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, const
   for (int c = 0; c < P && e == cudaSuccess; ++c) {
     const size_t bytes = m * cfg->local_n[c] * sizeof(double);
     e = cudaMalloc(&dX[c], bytes);
-    if (e == cudaSuccess) e = cudaMalloc(&dVT[c], bytes);
+    if (e == cudaSuccess && want_v) e = cudaMalloc(&dVT[c], bytes);
     if (e == cudaSuccess) e = cudaMemcpyAsync(dX[c], hX[c], bytes, cudaMemcpyHostToDevice, ctx->stream);
   }
   if (e == cudaSuccess) e = cudaMalloc(&ds, m * sizeof(double));
-  if (e == cudaSuccess) e = cudaMalloc(&dU, m * m * sizeof(double));
+  if (e == cudaSuccess && want_u) e = cudaMalloc(&dU, m * m * sizeof(double));
   if (e != cudaSuccess) {
     cleanup();
     return cuda_fail(ctx, e, "fedsvd_host: staging");
@@ -242,8 +249,9 @@ bbt_status bbt_fedsvd_run_host(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, const
   if (st == BBT_OK) {
     const int kk = *k;
     e = cudaMemcpyAsync(hsigma, ds, kk * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(hU, dU, m * kk * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
-    for (int c = 0; c < P && e == cudaSuccess; ++c)
+    if (e == cudaSuccess && want_u)
+      e = cudaMemcpyAsync(hU, dU, m * kk * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
+    for (int c = 0; c < P && e == cudaSuccess && want_v; ++c)
       e = cudaMemcpyAsync(hVT[c], dVT[c], (size_t)kk * cfg->local_n[c] * sizeof(double), cudaMemcpyDeviceToHost,
                           ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
@@ -292,6 +300,19 @@ bbt_status bbt_profile_get(bbt_ctx* ctx, int cls, double* ms, uint64_t* launches
   if (launches) *launches = ctx->prof_n[cls];
   if (work) *work = ctx->prof_work[cls];
   return BBT_OK;
+}
+
+bbt_status bbt_fedsvd_tune(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, int* streams, int* nb, double* ms) {
+  if (!ctx) return BBT_ERR_ARG;
+  if (!cfg) return fail(ctx, BBT_ERR_ARG, "fedsvd_tune: NULL config");
+  return fedsvd_tune(ctx, cfg, streams, nb, ms);
+}
+
+bbt_status bbt_svd_dense(bbt_ctx* ctx, int m, double* X, int top_k, double* sigma, double* U, double* VT,
+                         int* k) {
+  if (!ctx) return BBT_ERR_ARG;
+  if (!k || m < 1 || bad(X) || bad(sigma) || bad(U) || bad(VT)) return fail(ctx, BBT_ERR_ARG, "svd_dense: bad arguments");
+  return svd_dense(ctx, m, X, top_k, sigma, U, VT, k);
 }
 
 bbt_status bbt_fedsvd_stage_ms(const bbt_ctx* ctx, double* ms, int n) {

@@ -29,14 +29,17 @@ template <bool TA, bool TB, int WM, int WN>
 __global__ void __launch_bounds__(32 * WM * WN)
 dgemm_kernel(int M, int N, long K, long kchunk, double alpha, const double* __restrict__ A, long lda,
              const double* __restrict__ B, long ldb, double beta, double* __restrict__ C, long ldc,
-             double* __restrict__ P) {
+             double* __restrict__ P, int nfast) {
   constexpr int BM = 32 * WM, BN = 32 * WN, THREADS = 32 * WM * WN;
+  // nfast: blockIdx.x walks the N tiles, so the CTAs that share a block of
+  // rows of A run together and read it from HBM once (tall A, narrow C).
+  const int bm = nfast ? blockIdx.y : blockIdx.x, bn = nfast ? blockIdx.x : blockIdx.y;
   extern __shared__ double smem_[];
   auto As = reinterpret_cast<double(*)[BK][BM + PADA]>(smem_);
   auto Bs = reinterpret_cast<double(*)[BK][BN + PADB]>(smem_ + 2 * BK * (BM + PADA));
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wm = warp % WM, wn = warp / WM;
-  const int i0 = blockIdx.x * BM, j0 = blockIdx.y * BN;
+  const int i0 = bm * BM, j0 = bn * BN;
   const long kbeg = (long)blockIdx.z * kchunk;
   const long kend = min(K, kbeg + kchunk);
 
@@ -159,7 +162,7 @@ constexpr int smem_bytes() { return 2 * BK * (32 * WM + PADA + 32 * WN + PADB) *
 
 template <bool TA, bool TB, int WM, int WN>
 cudaError_t launch(dim3 g, cudaStream_t st, int M, int N, long K, long kc, double alpha, const double* A,
-                   long lda, const double* B, long ldb, double beta, double* C, long ldc, double* P) {
+                   long lda, const double* B, long ldb, double beta, double* C, long ldc, double* P, int nfast) {
   static bool attr = false;   // set once per process (per kernel instantiation)
   constexpr int SM = smem_bytes<WM, WN>();
   if (!attr) {
@@ -168,18 +171,19 @@ cudaError_t launch(dim3 g, cudaStream_t st, int M, int N, long K, long kc, doubl
     if (e != cudaSuccess) return e;
     attr = true;
   }
-  dgemm_kernel<TA, TB, WM, WN><<<g, 32 * WM * WN, SM, st>>>(M, N, K, kc, alpha, A, lda, B, ldb, beta, C, ldc, P);
+  dgemm_kernel<TA, TB, WM, WN><<<g, 32 * WM * WN, SM, st>>>(M, N, K, kc, alpha, A, lda, B, ldb, beta, C, ldc, P,
+                                                             nfast);
   return cudaSuccess;
 }
 
 template <int WM, int WN>
 cudaError_t launch_t(bool ta, bool tb, dim3 g, cudaStream_t st, int M, int N, long K, long kc, double alpha,
                      const double* A, long lda, const double* B, long ldb, double beta, double* C, long ldc,
-                     double* P) {
-  if (!ta && !tb) return launch<false, false, WM, WN>(g, st, M, N, K, kc, alpha, A, lda, B, ldb, beta, C, ldc, P);
-  if (ta && !tb) return launch<true, false, WM, WN>(g, st, M, N, K, kc, alpha, A, lda, B, ldb, beta, C, ldc, P);
-  if (!ta && tb) return launch<false, true, WM, WN>(g, st, M, N, K, kc, alpha, A, lda, B, ldb, beta, C, ldc, P);
-  return launch<true, true, WM, WN>(g, st, M, N, K, kc, alpha, A, lda, B, ldb, beta, C, ldc, P);
+                     double* P, int nf) {
+  if (!ta && !tb) return launch<false, false, WM, WN>(g, st, M, N, K, kc, alpha, A, lda, B, ldb, beta, C, ldc, P, nf);
+  if (ta && !tb) return launch<true, false, WM, WN>(g, st, M, N, K, kc, alpha, A, lda, B, ldb, beta, C, ldc, P, nf);
+  if (!ta && tb) return launch<false, true, WM, WN>(g, st, M, N, K, kc, alpha, A, lda, B, ldb, beta, C, ldc, P, nf);
+  return launch<true, true, WM, WN>(g, st, M, N, K, kc, alpha, A, lda, B, ldb, beta, C, ldc, P, nf);
 }
 
 // Tile shape from the output shape: avoid computing padding rows/columns of
@@ -236,17 +240,18 @@ bbt_status dgemm(bbt_ctx* ctx, bool ta, bool tb, int M, int N, long K, double al
     P = ctx->ws.take<double>((size_t)splits * M * N);
     if (!P) return fail(ctx, BBT_ERR_NOMEM, "dgemm: split-K workspace (%d x %d x %d)", splits, M, N);
   }
-  dim3 g(tm, tn, splits);
+  const int nfast = (tm >= tn && tm <= 65535) ? 1 : 0;
+  dim3 g(nfast ? tn : tm, nfast ? tm : tn, splits);
   if (K == 0) {   // C = beta * C
     g.z = 1;
     P = nullptr;
   }
   cudaError_t e;
   ProfScope prof(ctx, BBT_PROF_DGEMM, 2.0 * M * (double)N * (double)K);
-  if (wm == 1) e = launch_t<1, 4>(ta, tb, g, ctx->stream, M, N, K, kc, alpha, A, lda, B, ldb, beta, C, ldc, P);
-  else if (wm == 2 && wn == 2) e = launch_t<2, 2>(ta, tb, g, ctx->stream, M, N, K, kc, alpha, A, lda, B, ldb, beta, C, ldc, P);
-  else if (wm == 2) e = launch_t<2, 4>(ta, tb, g, ctx->stream, M, N, K, kc, alpha, A, lda, B, ldb, beta, C, ldc, P);
-  else e = launch_t<4, 2>(ta, tb, g, ctx->stream, M, N, K, kc, alpha, A, lda, B, ldb, beta, C, ldc, P);
+  if (wm == 1) e = launch_t<1, 4>(ta, tb, g, ctx->stream, M, N, K, kc, alpha, A, lda, B, ldb, beta, C, ldc, P, nfast);
+  else if (wm == 2 && wn == 2) e = launch_t<2, 2>(ta, tb, g, ctx->stream, M, N, K, kc, alpha, A, lda, B, ldb, beta, C, ldc, P, nfast);
+  else if (wm == 2) e = launch_t<2, 4>(ta, tb, g, ctx->stream, M, N, K, kc, alpha, A, lda, B, ldb, beta, C, ldc, P, nfast);
+  else e = launch_t<4, 2>(ta, tb, g, ctx->stream, M, N, K, kc, alpha, A, lda, B, ldb, beta, C, ldc, P, nfast);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "dgemm: shared-memory attribute");
   BBT_LAUNCHED(ctx);
   if (P) {

@@ -53,6 +53,15 @@ struct bbt_ctx {
   std::vector<bbt::ProfRec> recs;          // pending event pairs
   double prof_ms[8] = {0}, prof_work[8] = {0};
   uint64_t prof_n[8] = {0};
+  bool allow_coop = true;        // false in the concurrent sub-streams of the batched QR
+  // batched local QR: side streams, the captured graph and the tuned schedule
+  std::vector<cudaStream_t> side;
+  std::vector<cudaEvent_t> side_ev;
+  cudaGraphExec_t qr_graph = nullptr;
+  std::vector<size_t> qr_key;
+  uint64_t qr_graph_nodes = 0;
+  int tuned_streams = 0, tuned_nb = 0;   // 0: not tuned
+  std::vector<size_t> tuned_key;
 };
 
 namespace bbt {
@@ -149,6 +158,16 @@ bbt_status ormqr_left_notrans(bbt_ctx* ctx, long rows, int k, const double* V, l
                               const QrPlan& plan);
 size_t qr_workspace_bytes(long rows, int cols, int ncols_apply, const QrPlan& plan);
 
+// Vectors of clusters of singular values (relative spacing < 1e-7) by block
+// inverse iteration from the twisted vectors (clusters.cu).  U: n x k
+// row-major, V: k x n row-major, both in place.
+bbt_status refine_clusters(bbt_ctx* ctx, int n, int k, const double* a, const double* b, const double* sigma,
+                           double* U, double* V, int* nclusters);
+
+// Two-sided Householder bidiagonalisation A = Q B P^T of a column-major n x n
+// A (LAPACK dgebrd storage), one cooperative kernel (gebrd.cu).
+bbt_status gebrd(bbt_ctx* ctx, int n, double* A, double* d, double* e, double* tauq, double* taup);
+
 // Ralha one-sided bidiagonalisation of W (m x m row-major, overwritten) (ralha.cu).
 bbt_status ralha(bbt_ctx* ctx, int m, double* W, double* house, double* tau, double* alpha,
                  double* beta, double* V, double* cs);
@@ -166,5 +185,7 @@ bbt_status r_transpose(bbt_ctx* ctx, int m, const double* A, long lda, double* R
 bbt_status fedsvd(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* blocks, double* sigma,
                   double* U, double* const* VT, int* k);
 size_t fedsvd_workspace_bytes(const bbt_fedsvd_config* cfg);
+bbt_status fedsvd_tune(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, int* streams, int* nb, double* ms);
+bbt_status svd_dense(bbt_ctx* ctx, int m, double* X, int top_k, double* sigma, double* U, double* VT, int* k);
 
 }  // namespace bbt

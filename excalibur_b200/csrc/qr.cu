@@ -15,6 +15,7 @@
 #include <cuda_runtime.h>
 
 #include "internal.h"
+#include "sync.cuh"
 
 namespace bbt {
 namespace {
@@ -45,23 +46,42 @@ __device__ __forceinline__ void reflector(double alpha, double xx, double& beta,
 // P: the panel, m rows (row 0 = the panel's first row), b columns, ld.
 // pin/pout: per-CTA partials [cta][NBMAX]; entry c holds sum over rows > jj of
 // A[i][jj] * A[i][c] (entry jj: the squared norm).  prow_in/out: pivot row.
-__global__ void __launch_bounds__(PTHREADS)
-panel_step_kernel(double* __restrict__ P, long m, int b, long ld, int jj, const double* __restrict__ pin,
-                  const double* __restrict__ prow_in, double* __restrict__ pout,
-                  double* __restrict__ prow_out, double* __restrict__ tau) {
+__device__ __forceinline__ void panel_step(double* __restrict__ P, long m, int b, long ld, int jj,
+                                           const double* __restrict__ pin, const double* __restrict__ prow_in,
+                                           double* __restrict__ pout, double* __restrict__ prow_out,
+                                           double* __restrict__ tau) {
   __shared__ double red[PTHREADS / 32][NBMAX];
   __shared__ double wv[NBMAX];
   __shared__ double sc[3];   // beta, tau, scale
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int ncta = gridDim.x;
   const int nx = jj + 1;   // next column
-  // 1. reduce the previous step's partials (same order in every CTA)
+  // 1. reduce the previous step's partials, the same way in every CTA: each
+  //    thread sums a strided subset of the CTAs, then a fixed-order tree
+  //    over the threads (all loads of a thread are independent: one round
+  //    trip to L2 instead of ncta serial ones)
   if (jj >= 0) {
+    double part[NBMAX];
+#pragma unroll
+    for (int c = 0; c < NBMAX; ++c) part[c] = 0.0;
+    for (int q = tid; q < ncta; q += PTHREADS) {
+#pragma unroll
+      for (int c = 0; c < NBMAX; ++c)
+        if (c >= jj && c < b) part[c] += pin[(long)q * NBMAX + c];
+    }
+#pragma unroll
+    for (int c = 0; c < NBMAX; ++c) {
+      if (c < jj || c >= b) continue;
+      double v = part[c];
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+      if (lane == 0) red[warp][c] = v;
+    }
+    __syncthreads();
     for (int c = tid; c < b; c += PTHREADS) {
       if (c < jj) continue;
-      double s = 0.0;
-      for (int q = 0; q < ncta; ++q) s += pin[(long)q * NBMAX + c];
-      wv[c] = s;
+      double v = 0.0;
+      for (int w = 0; w < PTHREADS / 32; ++w) v += red[w][c];
+      wv[c] = v;
     }
     __syncthreads();
     if (tid == 0) {
@@ -78,38 +98,41 @@ panel_step_kernel(double* __restrict__ P, long m, int b, long ld, int jj, const 
   double acc[NBMAX];
 #pragma unroll
   for (int c = 0; c < NBMAX; ++c) acc[c] = 0.0;
-  const long r0 = (long)blockIdx.x * PROWS;
-  for (int rr = 0; rr < ROWS_PER_THREAD; ++rr) {
-    const long i = r0 + rr * PTHREADS + tid;
-    if (i >= m || i < jj) continue;
-    double* row = P + i;   // element c at row[c*ld]
-    double vi = 0.0;
-    if (jj >= 0) {
-      if (i == jj) {
-        row[(long)jj * ld] = beta;
-        vi = 1.0;
-      } else {
-        vi = row[(long)jj * ld] * scl;
-        row[(long)jj * ld] = vi;
-      }
-    }
-    double y = 0.0;   // updated A[i][nx]
-#pragma unroll
-    for (int c = 0; c < NBMAX; ++c) {
-      if (c <= jj || c >= b) continue;
-      double a = row[(long)c * ld];
+  // 2. update this CTA's row chunks and accumulate the next column's dots
+  for (long r0 = (long)blockIdx.x * PROWS; r0 < m; r0 += (long)gridDim.x * PROWS) {
+    for (int rr = 0; rr < ROWS_PER_THREAD; ++rr) {
+      const long i = r0 + rr * PTHREADS + tid;
+      if (i >= m || i < jj) continue;
+      double* row = P + i;   // element c at row[c*ld]
+      double vi = 0.0;
       if (jj >= 0) {
-        a -= ta * wv[c] * vi;
-        row[(long)c * ld] = a;
+        if (i == jj) {
+          row[(long)jj * ld] = beta;
+          vi = 1.0;
+        } else {
+          vi = row[(long)jj * ld] * scl;
+          row[(long)jj * ld] = vi;
+        }
       }
-      if (c == nx) y = a;
-      if (i > nx) acc[c] += y * a;   // c >= nx here, y already set at c == nx
+      double y = 0.0;   // updated A[i][nx]
+#pragma unroll
+      for (int c = 0; c < NBMAX; ++c) {
+        if (c <= jj || c >= b) continue;
+        double a = row[(long)c * ld];
+        if (jj >= 0) {
+          a -= ta * wv[c] * vi;
+          row[(long)c * ld] = a;
+        }
+        if (c == nx) y = a;
+        if (i > nx) acc[c] += y * a;   // c >= nx here, y already set at c == nx
+      }
+      if (i == nx && nx < b)
+        for (int c = nx; c < b; ++c) prow_out[c] = row[(long)c * ld];
     }
-    if (i == nx && nx < b)
-      for (int c = nx; c < b; ++c) prow_out[c] = row[(long)c * ld];
   }
   if (nx >= b) return;
   // 3. block-reduce the partials for column nx
+  __syncthreads();   // red[] was read in step 1
 #pragma unroll
   for (int c = 0; c < NBMAX; ++c) {
     if (c < nx || c >= b) continue;
@@ -123,6 +146,33 @@ panel_step_kernel(double* __restrict__ P, long m, int b, long ld, int jj, const 
     double s = 0.0;
     for (int w = 0; w < PTHREADS / 32; ++w) s += red[w][c];
     pout[(long)blockIdx.x * NBMAX + c] = s;
+  }
+}
+
+// Panel step for column jj (jj = -1: prologue, only the partials of column 0).
+// P: the panel, m rows (row 0 = the panel's first row), b columns, ld.
+// pin/pout: per-CTA partials [cta][NBMAX]; entry c holds sum over rows > jj of
+// A[i][jj] * A[i][c] (entry jj: the squared norm).  prow_in/out: pivot row.
+__global__ void __launch_bounds__(PTHREADS)
+panel_step_kernel(double* __restrict__ P, long m, int b, long ld, int jj, const double* __restrict__ pin,
+                  const double* __restrict__ prow_in, double* __restrict__ pout,
+                  double* __restrict__ prow_out, double* __restrict__ tau) {
+  panel_step(P, m, b, ld, jj, pin, prow_in, pout, prow_out, tau);
+}
+
+// All b column steps of a leaf panel in one cooperative launch, one bounded
+// grid barrier between consecutive steps (the partials and pivot row of step
+// jj are read by every CTA in step jj+1).
+__global__ void __launch_bounds__(PTHREADS)
+panel_leaf_kernel(double* __restrict__ P, long m, int b, long ld, double* __restrict__ pa,
+                  double* __restrict__ pb, double* __restrict__ ra, double* __restrict__ rb,
+                  double* __restrict__ tau, unsigned* bar, int* err) {
+  double *pin = pa, *pout = pb, *rin = ra, *rout = rb;
+  for (int jj = -1; jj < b; ++jj) {
+    panel_step(P, m, b, ld, jj, pin, rin, pout, rout, tau);
+    if (jj + 1 < b && !grid_sync(bar, err)) return;
+    double* t = pin; pin = pout; pout = t;
+    t = rin; rin = rout; rout = t;
   }
 }
 
@@ -193,22 +243,44 @@ bbt_status larft(bbt_ctx* ctx, int b, const double* G, const double* tau, double
   return BBT_OK;
 }
 
-// Column-by-column factorisation of a panel of b <= NBMAX columns.
+// Column-by-column factorisation of a panel of b <= NBMAX columns: one
+// cooperative launch when the grid fits on the GPU at once, otherwise one
+// launch per column.
 bbt_status panel_columns(bbt_ctx* ctx, double* P, long m, int b, long ld, double* tau) {
+  static int coop_blocks = -1;   // co-resident CTAs of panel_leaf_kernel per SM
+  if (coop_blocks < 0) {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, panel_leaf_kernel, PTHREADS, 0) != cudaSuccess)
+      per_sm = 0;
+    coop_blocks = per_sm;
+  }
   size_t mark = ctx->ws.top;
-  const long nblk = (m + PROWS - 1) / PROWS;
+  long nblk = (m + PROWS - 1) / PROWS;
+  const long coop_max = (long)coop_blocks * ctx->num_sms;
+  const bool coop = coop_max > 0 && ctx->allow_coop;
+  if (coop && nblk > coop_max) nblk = coop_max;   // grid-stride over the row chunks
   double* pa = ctx->ws.take<double>((size_t)nblk * NBMAX);
   double* pb = ctx->ws.take<double>((size_t)nblk * NBMAX);
   double* ra = ctx->ws.take<double>(NBMAX);
   double* rb = ctx->ws.take<double>(NBMAX);
   if (!rb) return fail(ctx, BBT_ERR_NOMEM, "panel: workspace");
-  double *pin = pa, *pout = pb, *rin = ra, *rout = rb;
-  for (int jj = -1; jj < b; ++jj) {
-    ProfScope prof(ctx, BBT_PROF_PANEL, 16.0 * (double)m * (double)(b - jj));
-    panel_step_kernel<<<(int)nblk, PTHREADS, 0, ctx->stream>>>(P, m, b, ld, jj, pin, rin, pout, rout, tau);
+  if (coop) {
+    ProfScope prof(ctx, BBT_PROF_PANEL, 8.0 * (double)m * (double)b * (double)(b + 1));
+    BBT_CUDA(ctx, cudaMemsetAsync(ctx->d_barrier, 0, 2 * sizeof(unsigned), ctx->stream));
+    BBT_CUDA(ctx, cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), ctx->stream));
+    void* args[] = {&P, &m, &b, &ld, &pa, &pb, &ra, &rb, &tau, &ctx->d_barrier, &ctx->d_flag};
+    BBT_CUDA(ctx, cudaLaunchCooperativeKernel((void*)panel_leaf_kernel, dim3((unsigned)nblk), dim3(PTHREADS),
+                                              args, 0, ctx->stream));
     BBT_LAUNCHED(ctx);
-    double* t = pin; pin = pout; pout = t;
-    t = rin; rin = rout; rout = t;
+  } else {
+    double *pin = pa, *pout = pb, *rin = ra, *rout = rb;
+    for (int jj = -1; jj < b; ++jj) {
+      ProfScope prof(ctx, BBT_PROF_PANEL, 16.0 * (double)m * (double)(b - jj));
+      panel_step_kernel<<<(int)nblk, PTHREADS, 0, ctx->stream>>>(P, m, b, ld, jj, pin, rin, pout, rout, tau);
+      BBT_LAUNCHED(ctx);
+      double* t = pin; pin = pout; pout = t;
+      t = rin; rin = rout; rout = t;
+    }
   }
   ctx->ws.top = mark;
   return BBT_OK;

@@ -23,13 +23,13 @@
 #include <cuda_runtime.h>
 
 #include "internal.h"
+#include "sync.cuh"
 
 namespace bbt {
 namespace {
 
 constexpr int RT = 256;                 // threads per CTA
 constexpr int RW = RT / 32;             // warps per CTA
-constexpr long SPIN_LIMIT = 20000000;   // ~seconds of polling before giving up
 
 struct RalhaArgs {
   int m;
@@ -47,31 +47,6 @@ struct RalhaArgs {
   unsigned* bar;   // [0] arrivals, [1] generation
   int* err;
 };
-
-__device__ __forceinline__ bool grid_sync(unsigned* bar, int* err) {
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    volatile unsigned* gen = bar + 1;
-    const unsigned g0 = *gen;
-    __threadfence();
-    const unsigned arrived = atomicAdd(bar, 1u) + 1u;
-    if (arrived == gridDim.x) {
-      atomicExch(bar, 0u);
-      __threadfence();
-      atomicAdd(bar + 1, 1u);
-    } else {
-      long spins = 0;
-      while (*gen == g0) {
-        if (++spins > SPIN_LIMIT) { atomicExch(err, 1); break; }
-        if (*(volatile int*)err) break;
-        __nanosleep(64);
-      }
-    }
-    __threadfence();
-  }
-  __syncthreads();
-  return *(volatile int*)err == 0;
-}
 
 __device__ double block_sum(double v, double* sh) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;

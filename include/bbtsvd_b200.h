@@ -150,6 +150,18 @@ enum { BBT_PROF_DGEMM = 0, BBT_PROF_PANEL = 1, BBT_PROF_MASK = 2, BBT_PROF_RALHA
 bbt_status bbt_profile(bbt_ctx* ctx, int enable);
 bbt_status bbt_profile_get(bbt_ctx* ctx, int cls, double* ms, uint64_t* launches, double* work);
 
+/* ---- dense SVD ---------------------------------------------------------------
+ * SVD X = U diag(sigma) VT of one dense m x m matrix (row-major,
+ * overwritten): two-sided Householder bidiagonalisation (LAPACK dgebrd
+ * semantics; the reference's one-sided Ralha recurrence, client.cpp:829-910,
+ * is not accurate enough for small singular values of a dense matrix), the
+ * Sturm count of singular values (client.cpp:966-971), bisection + twisted
+ * vectors with the sign conventions (client.cpp:984-995, bbtsvd.cpp:932-968)
+ * and the two reflector back-transforms.  Outputs: d_sigma[k] descending,
+ * d_U row-major m x k, d_VT row-major k x m; top_k <= 0 means all. */
+bbt_status bbt_svd_dense(bbt_ctx* ctx, int m, double* d_X, int top_k, double* d_sigma, double* d_U,
+                         double* d_VT, int* h_k);
+
 /* ---- whole pipeline ------------------------------------------------------
  * DecentralizedClient::run() (client.cpp:447-1200), short-and-wide branch
  * (m <= global_n), svd_mode 1 (two-sided) with opt_control 3, for P
@@ -162,13 +174,18 @@ typedef struct {
   unsigned public_seed;          /* shared mask seed (client.cpp:498) */
   const unsigned* private_seeds; /* P private mask seeds (client.cpp:531) */
   int top_k;                     /* <= 0: all singular values (client.cpp:971) */
-  int precision;                 /* 0: plain FP64 (the only mode so far) */
+  int svd_mode;                  /* client.cpp:186-192: 0 full SVD (the reference calls dbdsdc on the
+                                    leading k x k bidiagonal; here bisection + twisted vectors on it),
+                                    1 two-sided, 2 left vectors only (no FinalVT), 3 right vectors
+                                    only (no FinalU) */
+  int precision;                 /* 0: plain FP64 */
 } bbt_fedsvd_config;
 
 /* Device-resident run.  d_blocks[c]: row-major m x local_n[c] input, used as
  * workspace (overwritten).  Outputs: d_sigma[m], d_U row-major m x k (the
- * reference's FinalU), d_VT[c] row-major k x local_n[c] (FinalVT); *h_k is
- * the number of singular values k.  Replaces client.cpp:572-1199. */
+ * reference's FinalU; may be NULL in svd_mode 3), d_VT[c] row-major
+ * k x local_n[c] (FinalVT; d_VT may be NULL in svd_mode 2); *h_k is the
+ * number of singular values k.  Replaces client.cpp:572-1199. */
 bbt_status bbt_fedsvd_run(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* d_blocks,
                           double* d_sigma, double* d_U, double* const* d_VT, int* h_k);
 
@@ -177,6 +194,14 @@ bbt_status bbt_fedsvd_run(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* co
 bbt_status bbt_fedsvd_run_host(bbt_ctx* ctx, const bbt_fedsvd_config* cfg,
                                const double* const* h_blocks, double* h_sigma, double* h_U,
                                double* const* h_VT, int* h_k);
+
+/* Autotuner of the batched local QR (the QR of every participant with
+ * local_n / m > 5, client.cpp:572-589, issued on concurrent streams and
+ * replayed as one CUDA graph): times every (streams, panel width) candidate
+ * on synthetic blocks of cfg's shapes and keeps the fastest in ctx for later
+ * bbt_fedsvd_run calls with the same shapes.  Outputs may be NULL. */
+bbt_status bbt_fedsvd_tune(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, int* streams, int* panel_width,
+                           double* ms);
 
 /* Per-stage wall time (ms, CUDA events) of the last bbt_fedsvd_run, in the
  * reference's phase order: local_qr, apply_mask, global_qr, bi_diag, bsvd,

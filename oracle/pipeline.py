@@ -158,8 +158,23 @@ def apply_house(house, tau, C):
     return C
 
 
-def run(blocks, public_seed, private_seeds, top_k=-1, return_stages=False):
-    """DecentralizedClient::run(), svd_mode 1 (two-sided), opt_control 3."""
+def leading_svd(a, b, k):
+    """svd_mode 0: LAPACK SVD of the leading k x k bidiagonal (the reference
+    calls dbdsdc with n = k, client.cpp:975-980); U m x k and V k x m padded
+    with zeros as in the reference's zero-initialised buffers."""
+    m = len(a)
+    B = np.diag(a[:k]) + (np.diag(b[:k - 1], 1) if k > 1 else 0)
+    Uk, s, Vk = np.linalg.svd(np.atleast_2d(B))
+    U = np.zeros((m, k))
+    V = np.zeros((k, m))
+    U[:k] = Uk
+    V[:, :k] = Vk
+    return s, U, V
+
+
+def run(blocks, public_seed, private_seeds, top_k=-1, svd_mode=1, return_stages=False):
+    """DecentralizedClient::run(), opt_control 3; svd_mode 0 (full, dbdsdc),
+    1 (two-sided), 2 (left only) or 3 (right only)."""
     P = len(blocks)
     m = blocks[0].shape[0]
     local_n = [b.shape[1] for b in blocks]
@@ -203,17 +218,25 @@ def run(blocks, public_seed, private_seeds, top_k=-1, return_stages=False):
     k = negative_count(a, b, bound) - negative_count(a, b, 0.0)
     if top_k > 0:
         k = min(k, top_k)
-    sigma, Ub, Vb = bidiagonal_svd(a, b, k)                       # :984
+    if svd_mode == 0:
+        sigma, Ub, Vb = leading_svd(a, b, k)                      # :975-980
+    else:
+        sigma, Ub, Vb = bidiagonal_svd(a, b, k)                   # :984
     for i in range(k):                                            # :988-995
         p = int(np.argmax(np.abs(Ub[:, i])))
         if Ub[p, i] < 0:
             Ub[:, i] = -Ub[:, i]
             Vb[i] = -Vb[i]
     stages["bsvd"] = (sigma.copy(), Ub.copy(), Vb.copy())
-    FinalU = np.zeros((m, k))                                     # :1007-1115
-    for c in range(P):
-        FinalU[pos[c]:pos[c + 1]] = (Vb @ Vr[c]).T
-    FinalU = block_shift_mask(FinalU, MASK_PASSES, False, True, public_seed)
+    FinalU = None
+    if svd_mode != 3:                                             # :1002-1115
+        FinalU = np.zeros((m, k))
+        for c in range(P):
+            FinalU[pos[c]:pos[c + 1]] = (Vb @ Vr[c]).T
+        FinalU = block_shift_mask(FinalU, MASK_PASSES, False, True, public_seed)
+    if svd_mode == 2:
+        out = (sigma, FinalU, None)
+        return (out + (stages,)) if return_stages else out
     U2 = Ub.copy()                                                # :1127-1128
     for i in range(m - 2, -1, -1):
         c_, s_ = cs[i]

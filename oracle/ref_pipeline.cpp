@@ -47,7 +47,7 @@ int main(int argc, char** argv) {
             negative_count(k, a, b, 0);
   if (topk > 0 && topk < cnt) cnt = topk;
   double* sig = new double[cnt > 0 ? cnt : 1]();
-  if (mode == 0 || mode == 4) {
+  if (mode == 0 || mode == 4) {   // dbdsdc left the singular values in x_diagonal
     for (int i = 0; i < cnt; ++i) sig[i] = a[i];
   } else {
     int got = 0;
@@ -55,8 +55,10 @@ int main(int argc, char** argv) {
     bisection_singular_values(k, a, b, 0, bound, 1e-20, cnt, sig, &got);
   }
   dump(out + "/sigma.bin", sig, cnt);
-  if (cid == 0 && c->FinalU) dump(out + "/U.bin", c->FinalU, m * (size_t)cnt);
-  if (c->FinalVT) dump(out + "/VT.bin", c->FinalVT, (size_t)cnt * ln);
+  // FinalU / FinalVT are left unset by the reference in the modes that skip
+  // them (svd_mode 3 / 2, client.cpp:491-492)
+  if (cid == 0 && mode != 3 && mode != 4) dump(out + "/U.bin", c->FinalU, m * (size_t)cnt);
+  if (mode != 2 && mode != 4) dump(out + "/VT.bin", c->FinalVT, (size_t)cnt * ln);
   if (mode != 0 && mode != 4) {
     dump(out + "/ab.bin", a, m);
     FILE* fp = fopen((out + "/ab.bin").c_str(), "ab");

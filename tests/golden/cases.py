@@ -64,6 +64,13 @@ def mask_cases():
     return out
 
 
+def pipeline_mode_cases():
+    """name -> (pipeline case, svd_mode, top_k): the other svd modes and top-k
+    on the same inputs (client.cpp:186-192, 971)."""
+    return {"c1_mode0": ("c1", 0, -1), "c1_mode2_top10": ("c1", 2, 10), "c1_mode3_top10": ("c1", 3, 10),
+            "c1_mode1_top10": ("c1", 1, 10), "p3_mode0_top7": ("p3_uneven", 0, 7)}
+
+
 def pipeline_cases():
     """name -> (blocks, seed).  ``c1`` is the 2 x (1000 x 100) N(0,1) case
     (row-stacked 2000 x 100), held as the reference's m=100 x local_n=1000."""

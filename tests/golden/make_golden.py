@@ -123,10 +123,11 @@ def run_reference_pipeline(blocks, seed, mode=1, topk=-1):
                 raise RuntimeError("reference participant failed")
         sig = np.fromfile(os.path.join(td, "out0", "sigma.bin"))
         k = len(sig)
-        U = np.fromfile(os.path.join(td, "out0", "U.bin")).reshape(m, k)
-        VT = [np.fromfile(os.path.join(td, f"out{c}", "VT.bin")).reshape(k, blocks[c].shape[1])
-              for c in range(P)]
-        ab = np.fromfile(os.path.join(td, "out0", "ab.bin"))
+        U = np.fromfile(os.path.join(td, "out0", "U.bin")).reshape(m, k) if mode not in (3, 4) else None
+        VT = ([np.fromfile(os.path.join(td, f"out{c}", "VT.bin")).reshape(k, blocks[c].shape[1])
+               for c in range(P)] if mode not in (2, 4) else None)
+        abf = os.path.join(td, "out0", "ab.bin")
+        ab = np.fromfile(abf) if os.path.exists(abf) else np.zeros(0)
         secs = [float(open(os.path.join(td, f"out{c}", "time.txt")).read().split()[0]) for c in range(P)]
     return sig, U, VT, ab, secs
 
@@ -137,6 +138,16 @@ def pipeline_fixtures():
         sig, U, VT, ab, secs = run_reference_pipeline(blocks, seed)
         d = dict(x_sha=sha(*blocks), seed=np.uint32(seed), sigma=sig, U=U, ab=ab)
         for c, v in enumerate(VT):
+            d[f"VT{c}"] = v
+        out[name] = d
+    base = cases.pipeline_cases()
+    for name, (case, mode, topk) in cases.pipeline_mode_cases().items():
+        blocks, seed = base[case]
+        sig, U, VT, ab, secs = run_reference_pipeline(blocks, seed, mode=mode, topk=topk)
+        d = dict(x_sha=sha(*blocks), seed=np.uint32(seed), sigma=sig, svd_mode=np.int32(mode), top_k=np.int32(topk))
+        if U is not None:
+            d["U"] = U
+        for c, v in enumerate(VT or []):
             d[f"VT{c}"] = v
         out[name] = d
     return out

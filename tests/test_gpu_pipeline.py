@@ -18,11 +18,33 @@ def ctx():
     return context()
 
 
-def run(ctx, blocks, seed):
+def run(ctx, blocks, seed, top_k=-1, svd_mode=1):
     pub, priv = oracle.reference_seeds(seed, len(blocks))
     dev = [ctx._dev(b.copy()) for b in blocks]
-    s, U, VT = ctx.fedsvd(dev, pub, priv)
-    return s.cpu().numpy(), U.cpu().numpy(), [v.cpu().numpy() for v in VT]
+    s, U, VT = ctx.fedsvd(dev, pub, priv, top_k=top_k, svd_mode=svd_mode)
+    return (s.cpu().numpy(), None if U is None else U.cpu().numpy(),
+            None if VT is None else [v.cpu().numpy() for v in VT])
+
+
+@pytest.mark.parametrize("name", sorted(cases.pipeline_mode_cases()))
+def test_pipeline_modes_match_reference(ctx, golden, name):
+    """svd_mode 0 (the reference's dbdsdc on the leading k x k bidiagonal),
+    2 (left only), 3 (right only) and top-k (client.cpp:186-192, 971-985)."""
+    g = golden(f"pipe__{name}")
+    case, mode, topk = cases.pipeline_mode_cases()[name]
+    blocks, seed = cases.pipeline_cases()[case]
+    s, U, VT = run(ctx, blocks, seed, top_k=topk, svd_mode=mode)
+    assert len(s) == len(g["sigma"])
+    assert np.max(np.abs(s - g["sigma"]) / g["sigma"]) < 1e-12
+    if mode != 3:
+        assert np.max(np.abs(U - g["U"])) < 1e-9
+    else:
+        assert U is None
+    if mode != 2:
+        for c, v in enumerate(VT):
+            assert np.max(np.abs(v - g[f"VT{c}"])) < 1e-9
+    else:
+        assert VT is None
 
 
 @pytest.mark.parametrize("name", PIPES)
@@ -78,3 +100,39 @@ def test_pipeline_geometric_spectrum(ctx):
     assert np.max(np.abs(s - sv) / sv) < 1e-10 * 1e4   # conditioning bound for s_min ~ 1e-6
     X = np.concatenate(blocks, axis=1)
     assert np.max(np.abs(U @ np.diag(s) @ np.concatenate(VT, axis=1) - X)) < 1e-13
+
+
+def test_batched_local_qr_graph_replay(ctx):
+    """Ten participants (c3-like uneven rows): the local QRs run on
+    concurrent streams, eagerly on the first call, captured into a CUDA graph
+    on the second and replayed on the third; every call matches the oracle."""
+    rng = np.random.default_rng(33)
+    m = 32
+    rows = [int(r) for r in rng.integers(200, 900, 10)]
+    blocks = [rng.standard_normal((m, n)) * 10.0 ** rng.uniform(-2, 2) for n in rows]
+    pub, priv = oracle.reference_seeds(4, len(blocks))
+    so, Uo, VTo = pipeline.run(blocks, pub, priv)
+    dev = [ctx._dev(b.copy()) for b in blocks]
+    for call in range(3):
+        for d, b in zip(dev, blocks):
+            d.copy_(ctx.torch.as_tensor(b, device=d.device))
+        s, U, VT = ctx.fedsvd(dev, pub, priv)
+        s, U = s.cpu().numpy(), U.cpu().numpy()
+        assert np.max(np.abs(s - so) / so) < 1e-12, call
+        assert np.max(np.abs(U - Uo)) < 1e-9, call
+        for v, w in zip(VT, VTo):
+            assert np.max(np.abs(v.cpu().numpy() - w)) < 1e-9, call
+
+
+def test_autotuned_batched_local_qr(ctx):
+    rng = np.random.default_rng(34)
+    m = 24
+    rows = [int(r) for r in rng.integers(150, 600, 9)]
+    blocks = [rng.standard_normal((m, n)) for n in rows]
+    st, nb, ms = ctx.fedsvd_tune(m, rows)
+    assert st in (1, 4, 8, 16) and nb in (64, 128) and ms > 0
+    pub, priv = oracle.reference_seeds(6, len(blocks))
+    so, Uo, VTo = pipeline.run(blocks, pub, priv)
+    s, U, VT = ctx.fedsvd([ctx._dev(b.copy()) for b in blocks], pub, priv)
+    assert np.max(np.abs(s.cpu().numpy() - so) / so) < 1e-12
+    assert np.max(np.abs(U.cpu().numpy() - Uo)) < 1e-9

@@ -30,7 +30,7 @@ PIPES = sorted(cases.pipeline_cases())
 def test_every_fixture_has_a_case():
     names = {os.path.basename(f)[:-4] for f in glob.glob(os.path.join(GOLD, "*.npz"))}
     want = ({f"bidiag__{n}" for n in BIDIAG} | {f"mask__{n}" for n in MASKS}
-            | {f"pipe__{n}" for n in PIPES})
+            | {f"pipe__{n}" for n in PIPES} | {f"pipe__{n}" for n in cases.pipeline_mode_cases()})
     assert names == want
 
 
@@ -103,3 +103,27 @@ def test_pipeline_against_lapack_svd():
     sv = np.linalg.svd(X, compute_uv=False)
     assert np.max(np.abs(s - sv) / sv) < 1e-12
     assert np.max(np.abs(U @ np.diag(s) @ np.concatenate(VT, axis=1) - X)) < 1e-11
+
+
+MODES = sorted(cases.pipeline_mode_cases())
+
+
+@pytest.mark.parametrize("name", MODES)
+def test_pipeline_modes_match_reference(golden, name):
+    g = golden(f"pipe__{name}")
+    case, mode, topk = cases.pipeline_mode_cases()[name]
+    blocks, seed = cases.pipeline_cases()[case]
+    assert sha(*blocks) == str(g["x_sha"])
+    pub, priv = oracle.reference_seeds(seed, len(blocks))
+    s, U, VT = pipeline.run(blocks, pub, priv, top_k=topk, svd_mode=mode)
+    assert len(s) == len(g["sigma"])
+    assert np.max(np.abs(s - g["sigma"]) / g["sigma"]) < 1e-13
+    if mode != 3:
+        assert np.max(np.abs(U - g["U"])) < 1e-10
+    else:
+        assert U is None and "U" not in g
+    if mode != 2:
+        for c, v in enumerate(VT):
+            assert np.max(np.abs(v - g[f"VT{c}"])) < 1e-10
+    else:
+        assert VT is None
