@@ -185,6 +185,40 @@ class Context:
         self.sync()
         return rt
 
+    def rademacher(self, N, n, seed):
+        """S (N x n, +-1 in bf16; returned as an int16 tensor of bf16 bit
+        patterns, row pitch n rounded up to 8)."""
+        pitch = (n + 7) // 8 * 8
+        S = self._empty(N, pitch, dtype=self.torch.int16)
+        self._pre()
+        self._check(self.L.bbt_rademacher(self.h, N, n, seed, self._p(S)), "rademacher")
+        self.sync()
+        return S
+
+    def sketch_bf16x3(self, x, S, N):
+        """Y (m x N) = X S^T for X (m x n, CUDA float64) on the tensor cores
+        (BF16x3 pieces of X, FP32 accumulation per K-chunk)."""
+        m, n = x.shape
+        Y = self._empty(m, N)
+        self._pre()
+        self._check(self.L.bbt_sketch_bf16x3(self.h, m, n, self._p(x), N, self._p(S), self._p(Y)), "sketch_bf16x3")
+        self.sync()
+        return Y
+
+    def mixed_local_qr(self, x, want_w=True):
+        """Precision-1 local QR of X (m x local_n, CUDA float64, overwritten
+        by Q_p^T).  Returns (R as an m x m tensor holding the column-major
+        upper-triangular R, i.e. R^T row-major; W likewise, or None) with
+        X^T = Q_p W R and Q_p W orthonormal."""
+        m, n = x.shape
+        R = self._empty(m, m)
+        W = self._empty(m, m) if want_w else None
+        self._pre()
+        self._check(self.L.bbt_mixed_local_qr(self.h, m, n, self._p(x), self._p(R),
+                                              self._p(W) if W is not None else None), "mixed_local_qr")
+        self.sync()
+        return R, W
+
     def _config(self, m, local_n, public_seed, private_seeds, top_k, svd_mode, precision):
         P = len(local_n)
         self._ln = (C.c_size_t * P)(*local_n)
@@ -215,10 +249,10 @@ class Context:
         VTo = [v[: k * n].view(k, n) for v, n in zip(VT, ln)] if svd_mode != 2 else None
         return sig[:k], Uo, VTo
 
-    def fedsvd_tune(self, m, local_n, top_k=-1, svd_mode=1):
-        """Autotune the batched local QR for these shapes (kept in the
-        context).  Returns (streams, panel width, ms)."""
-        cfg = self._config(m, list(local_n), 0, [0] * len(local_n), top_k, svd_mode, 0)
+    def fedsvd_tune(self, m, local_n, top_k=-1, svd_mode=1, precision=0):
+        """Autotune the batched local QR for these shapes and precision mode
+        (kept in the context).  Returns (streams, panel width, ms)."""
+        cfg = self._config(m, list(local_n), 0, [0] * len(local_n), top_k, svd_mode, precision)
         st, nb, ms = C.c_int(), C.c_int(), C.c_double()
         self._pre()
         self._check(self.L.bbt_fedsvd_tune(self.h, C.byref(cfg), C.byref(st), C.byref(nb), C.byref(ms)),

@@ -12,7 +12,7 @@ LIBPATH = os.path.join(HERE, "libexcalibur_b200.so")
 
 BBT_OK = 0
 STATUS = {0: "BBT_OK", 1: "BBT_ERR_ARG", 2: "BBT_ERR_CUDA", 3: "BBT_ERR_COUNT", 4: "BBT_ERR_NOMEM",
-          5: "BBT_ERR_TIMEOUT", 6: "BBT_ERR_UNSUPPORTED"}
+          5: "BBT_ERR_TIMEOUT", 6: "BBT_ERR_UNSUPPORTED", 7: "BBT_ERR_NUMERIC"}
 
 # Every extern "C" symbol declared in include/bbtsvd_b200.h.
 EXPORTS = (
@@ -21,9 +21,9 @@ EXPORTS = (
     "bbt_twisted_vectors", "bbt_bidiagonal_svd", "bbt_givens_mask", "bbt_block_shift_mask",
     "bbt_local_qr", "bbt_fedsvd_run", "bbt_fedsvd_run_host", "bbt_fedsvd_stage_ms",
     "bbt_dgemm", "bbt_profile", "bbt_profile_get", "bbt_twisted_vectors_noalloc",
-    "bbt_svd_dense", "bbt_fedsvd_tune",
+    "bbt_svd_dense", "bbt_fedsvd_tune", "bbt_rademacher", "bbt_sketch_bf16x3", "bbt_mixed_local_qr",
 )
-PROF_CLASSES = ("dgemm", "panel", "mask", "ralha", "bisect", "twisted")
+PROF_CLASSES = ("dgemm", "panel", "mask", "ralha", "bisect", "twisted", "sketch", "chol")
 
 
 class FedSVDConfig(C.Structure):
@@ -76,6 +76,9 @@ def load():
         "bbt_fedsvd_tune": ([vp, C.POINTER(FedSVDConfig), C.POINTER(i), C.POINTER(i), C.POINTER(d)], i),
         "bbt_twisted_vectors_noalloc": ([vp, i, i, vp, vp, vp, vp, vp], i),
         "bbt_profile_get": ([vp, i, C.POINTER(d), C.POINTER(C.c_uint64), C.POINTER(d)], i),
+        "bbt_rademacher": ([vp, i, st, C.c_ulonglong, vp], i),
+        "bbt_sketch_bf16x3": ([vp, i, st, vp, i, vp, vp], i),
+        "bbt_mixed_local_qr": ([vp, st, st, vp, vp, vp], i),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

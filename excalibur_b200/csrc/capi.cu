@@ -73,6 +73,7 @@ const char* bbt_status_string(bbt_status s) {
     case BBT_ERR_NOMEM: return "out of device memory";
     case BBT_ERR_TIMEOUT: return "device-side wait timed out";
     case BBT_ERR_UNSUPPORTED: return "unsupported shape or mode";
+    case BBT_ERR_NUMERIC: return "Cholesky breakdown in the mixed-precision local QR";
   }
   return "unknown status";
 }
@@ -271,6 +272,39 @@ bbt_status bbt_dgemm(bbt_ctx* ctx, int transa, int transb, int M, int N, long K,
     return fail(ctx, BBT_ERR_ARG, "dgemm: leading dimension too small");
   BBT_TRY(ensure(ctx, dgemm_workspace_bytes(ctx, M, N, K) + (1 << 20)));
   return dgemm(ctx, transa != 0, transb != 0, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
+}
+
+bbt_status bbt_rademacher(bbt_ctx* ctx, int N, size_t local_n, unsigned long long seed, void* d_S) {
+  if (!ctx) return BBT_ERR_ARG;
+  if (N < 1 || local_n < 1 || local_n > ((size_t)1 << 31) || bad(d_S))
+    return fail(ctx, BBT_ERR_ARG, "rademacher: bad arguments");
+  return rademacher(ctx, N, (long)local_n, d_S, seed);
+}
+
+bbt_status bbt_sketch_bf16x3(bbt_ctx* ctx, int m, size_t local_n, const double* d_x, int N, const void* d_S,
+                             double* d_Y) {
+  if (!ctx) return BBT_ERR_ARG;
+  if (m < 1 || local_n < 1 || local_n > ((size_t)1 << 31) || N < 128 || N % 128 != 0 || bad(d_x) || bad(d_S) ||
+      bad(d_Y))
+    return fail(ctx, BBT_ERR_ARG, "sketch: bad arguments (N must be a positive multiple of 128)");
+  BBT_TRY(ensure(ctx, sketch_workspace_bytes(ctx, m, (long)local_n, N) + (1 << 20)));
+  BBT_TRY(clear_tc_flags(ctx));
+  BBT_TRY(sketch_bf16x3(ctx, m, (long)local_n, d_x, (long)local_n, N, d_S, sketch_pitch((long)local_n), d_Y));
+  return check_tc_flags(ctx, "sketch");
+}
+
+bbt_status bbt_mixed_local_qr(bbt_ctx* ctx, size_t m, size_t local_n, double* d_x, double* d_r, double* d_w) {
+  if (!ctx) return BBT_ERR_ARG;
+  if (m < 1 || local_n <= m || local_n > ((size_t)1 << 31) || m > 65536 || bad(d_x) || bad(d_r))
+    return fail(ctx, BBT_ERR_ARG, "mixed_local_qr: needs local_n > m");
+  const int mi = (int)m, N = sketch_rows(mi);
+  const long n = (long)local_n;
+  BBT_TRY(ensure(ctx, mixed_qr_workspace_bytes(ctx, mi, n) + (size_t)N * sketch_pitch(n) * 2 + (1 << 20)));
+  void* S = ctx->ws.take<char>((size_t)N * sketch_pitch(n) * 2);
+  BBT_TRY(rademacher(ctx, N, n, S, 0x5EED5EEDull));
+  BBT_TRY(clear_tc_flags(ctx));
+  BBT_TRY(mixed_local_qr(ctx, mi, n, d_x, S, sketch_pitch(n), d_r, d_w));
+  return check_tc_flags(ctx, "mixed_local_qr");
 }
 
 bbt_status bbt_profile(bbt_ctx* ctx, int enable) {

@@ -1,0 +1,273 @@
+// FP64 Cholesky factorisation and right-side triangular solve, recursive:
+// the diagonal leaves run as small SIMT kernels, everything above them as
+// FP64 tensor-core GEMMs (dgemm.cu).  Used by the mixed-precision local QR
+// (mixedqr.cu), whose R factor is built from Gram matrices.
+#include <cuda_runtime.h>
+
+#include "internal.h"
+
+namespace bbt {
+namespace {
+
+constexpr int PB = 64;   // Cholesky leaf
+constexpr int TB = 32;   // triangular-solve leaf
+
+// Upper Cholesky G = R^T R of an n x n (n <= PB) diagonal block, in place:
+// R in the upper triangle, zeros below.  A pivot that is not positive sets
+// *flag and is replaced by 1 so the factorisation still completes.
+__global__ void __launch_bounds__(256) potrf_leaf(int n, double* __restrict__ G, long ld, int* flag) {
+  __shared__ double a[PB][PB + 1];
+  const int t = threadIdx.x;
+  for (int f = t; f < n * n; f += blockDim.x) {
+    const int i = f % n, k = f / n;
+    a[i][k] = (i <= k) ? G[i + (long)k * ld] : 0.0;
+  }
+  __syncthreads();
+  for (int j = 0; j < n; ++j) {
+    double d = a[j][j];
+    if (!(d > 0.0) || !isfinite(d)) {
+      if (t == 0) atomicExch(flag, 1);
+      d = 1.0;
+    }
+    const double r = sqrt(d);
+    __syncthreads();
+    for (int k = j + t; k < n; k += blockDim.x) a[j][k] = (k == j) ? r : a[j][k] / r;
+    __syncthreads();
+    const int w = n - j - 1;
+    for (int f = t; f < w * w; f += blockDim.x) {
+      const int i = j + 1 + f % w, k = j + 1 + f / w;
+      if (i <= k) a[i][k] -= a[j][i] * a[j][k];
+    }
+    __syncthreads();
+  }
+  for (int f = t; f < n * n; f += blockDim.x) {
+    const int i = f % n, k = f / n;
+    G[i + (long)k * ld] = (i <= k) ? a[i][k] : 0.0;
+  }
+}
+
+// A (rows x n, column-major) <- A R^{-1}, R upper n x n (n <= TB): one thread
+// per row, forward substitution along the row.
+__global__ void __launch_bounds__(128) trsm_leaf(long rows, int n, const double* __restrict__ R, long ldr,
+                                                 double* __restrict__ A, long lda) {
+  __shared__ double r[TB][TB + 1];
+  for (int f = threadIdx.x; f < n * n; f += blockDim.x) {
+    const int i = f % n, j = f / n;
+    r[i][j] = (i <= j) ? R[i + (long)j * ldr] : 0.0;
+  }
+  __syncthreads();
+  for (long row = blockIdx.x * (long)blockDim.x + threadIdx.x; row < rows; row += (long)gridDim.x * blockDim.x) {
+    double x[TB];
+#pragma unroll
+    for (int j = 0; j < TB; ++j)
+      if (j < n) x[j] = A[row + (long)j * lda];
+#pragma unroll
+    for (int j = 0; j < TB; ++j) {
+      if (j < n) {
+        double s = x[j];
+#pragma unroll
+        for (int i = 0; i < j; ++i) s -= x[i] * r[i][j];
+        x[j] = s / r[j][j];
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < TB; ++j)
+      if (j < n) A[row + (long)j * lda] = x[j];
+  }
+}
+
+// G12 (n1 x n2, above the diagonal) <- X^T for X = G21 (n2 x n1, below), then X <- 0.
+__global__ void mirror_kernel(int n1, int n2, double* __restrict__ G, long ld) {
+  const long total = (long)n1 * n2;
+  for (long f = blockIdx.x * (long)blockDim.x + threadIdx.x; f < total; f += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(f % n1), k = (int)(f / n1);
+    double* lo = G + (n1 + k) + (long)i * ld;
+    G[i + (long)(n1 + k) * ld] = *lo;
+    *lo = 0.0;
+  }
+}
+
+// G_ii += rel * max_j G_jj (one block).
+__global__ void shift_diag_kernel(int n, double* __restrict__ G, long ld, double rel) {
+  __shared__ double sh[256];
+  double mx = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) mx = fmax(mx, G[i + (long)i * ld]);
+  sh[threadIdx.x] = mx;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sh[threadIdx.x] = fmax(sh[threadIdx.x], sh[threadIdx.x + o]);
+    __syncthreads();
+  }
+  const double s = rel * sh[0];
+  for (int i = threadIdx.x; i < n; i += blockDim.x) G[i + (long)i * ld] += s;
+}
+
+__global__ void identity_kernel(int n, double* __restrict__ W, long ld) {
+  const long total = (long)n * n;
+  for (long f = blockIdx.x * (long)blockDim.x + threadIdx.x; f < total; f += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(f % n), j = (int)(f / n);
+    W[i + (long)j * ld] = (i == j) ? 1.0 : 0.0;
+  }
+}
+
+// Signs of LAPACK's Householder QR from the top block of an orthonormal Q.
+// Householder QR of Q (and of any A = Q R+ with R+ positive-diagonal)
+// produces Q D with D = diag(d), d_j = sign(beta_j) = -sign(alpha_j); the
+// compact-WY identity I - Q1 D = Y1 T Y1^T makes the unpivoted LU of
+// I - Q1 D have pivots tau_j = 1 - d_j c_j >= 1, where c_j is the j-th
+// diagonal entry of Q1 after the elimination of the previous columns.  So
+// d_j = -sign(c_j) (c_j = 0 -> -1, dlarfg's choice for alpha = 0), and the
+// elimination runs on Q1 itself with multipliers l_ij = -d_j q_ij / (1 + |c_j|).
+// Leaf: one CTA, up to TB columns of a tall panel (rows >= cols).
+__global__ void __launch_bounds__(1024) lu_sign_leaf(int rows, int cols, double* __restrict__ A, long lda,
+                                                     double* __restrict__ d) {
+  __shared__ double rowj[TB];
+  __shared__ double sdj, su;
+  for (int j = 0; j < cols; ++j) {
+    if (threadIdx.x == 0) {
+      const double c = A[j + (long)j * lda];
+      sdj = c < 0.0 ? 1.0 : -1.0;
+      su = 1.0 + fabs(c);
+      d[j] = sdj;
+    }
+    if (threadIdx.x > j && threadIdx.x < cols) rowj[threadIdx.x] = A[j + (long)threadIdx.x * lda];
+    __syncthreads();
+    const double f = -sdj / su;
+    for (int i = j + 1 + threadIdx.x; i < rows; i += blockDim.x) {
+      const double l = f * A[i + (long)j * lda];
+      A[i + (long)j * lda] = l;
+      for (int k = j + 1; k < cols; ++k) A[i + (long)k * lda] -= l * rowj[k];
+    }
+    __syncthreads();
+  }
+}
+
+// B (n x ncols) <- L^{-1} B, L unit lower n x n (n <= TB): one thread per column.
+__global__ void __launch_bounds__(128) trsm_llu_leaf(int n, long ncols, const double* __restrict__ L, long ldl,
+                                                     double* __restrict__ B, long ldb) {
+  __shared__ double l[TB][TB + 1];
+  for (int f = threadIdx.x; f < n * n; f += blockDim.x) {
+    const int i = f % n, k = f / n;
+    l[i][k] = (i > k) ? L[i + (long)k * ldl] : 0.0;
+  }
+  __syncthreads();
+  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < ncols; c += (long)gridDim.x * blockDim.x) {
+    double x[TB];
+#pragma unroll
+    for (int i = 0; i < TB; ++i)
+      if (i < n) x[i] = B[i + c * ldb];
+#pragma unroll
+    for (int i = 0; i < TB; ++i) {
+      if (i < n) {
+        double s = x[i];
+#pragma unroll
+        for (int k = 0; k < i; ++k) s -= l[i][k] * x[k];
+        x[i] = s;
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < TB; ++i)
+      if (i < n) B[i + c * ldb] = x[i];
+  }
+}
+
+// Row j of R (column-major, ld m) and column j of W (column-major, ld m) times d_j.
+__global__ void apply_signs_kernel(int m, const double* __restrict__ d, double* __restrict__ R,
+                                   double* __restrict__ W) {
+  const long total = (long)m * m;
+  for (long f = blockIdx.x * (long)blockDim.x + threadIdx.x; f < total; f += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(f % m), j = (int)(f / m);
+    R[f] *= d[i];
+    if (W) W[f] *= d[j];
+  }
+}
+
+int split_point(int n) { return (n / 2 + TB - 1) / TB * TB; }
+
+bbt_status trsm_left_lower_unit(bbt_ctx* ctx, int n, long ncols, const double* L, long ldl, double* B, long ldb) {
+  if (n <= 0 || ncols <= 0) return BBT_OK;
+  if (n <= TB) {
+    long blocks = (ncols + 127) / 128;
+    if (blocks > 16L * ctx->num_sms) blocks = 16L * ctx->num_sms;
+    trsm_llu_leaf<<<(unsigned)blocks, 128, 0, ctx->stream>>>(n, ncols, L, ldl, B, ldb);
+    BBT_LAUNCHED(ctx);
+    return BBT_OK;
+  }
+  const int h = split_point(n);
+  BBT_TRY(trsm_left_lower_unit(ctx, h, ncols, L, ldl, B, ldb));
+  BBT_TRY(dgemm(ctx, false, false, n - h, (int)ncols, h, -1.0, L + h, ldl, B, ldb, 1.0, B + h, ldb));
+  return trsm_left_lower_unit(ctx, n - h, ncols, L + h + (long)h * ldl, ldl, B + h, ldb);
+}
+
+}  // namespace
+
+bbt_status householder_signs(bbt_ctx* ctx, int rows, int cols, double* A, long lda, double* d) {
+  if (cols <= 0) return BBT_OK;
+  if (cols <= TB) {
+    ProfScope prof(ctx, BBT_PROF_CHOL, (double)rows * cols * cols);
+    lu_sign_leaf<<<1, 1024, 0, ctx->stream>>>(rows, cols, A, lda, d);
+    BBT_LAUNCHED(ctx);
+    return BBT_OK;
+  }
+  const int h = split_point(cols);
+  BBT_TRY(householder_signs(ctx, rows, h, A, lda, d));
+  BBT_TRY(trsm_left_lower_unit(ctx, h, cols - h, A, lda, A + (long)h * lda, lda));
+  BBT_TRY(dgemm(ctx, false, false, rows - h, cols - h, h, -1.0, A + h, lda, A + (long)h * lda, lda, 1.0,
+                A + h + (long)h * lda, lda));
+  return householder_signs(ctx, rows - h, cols - h, A + h + (long)h * lda, lda, d + h);
+}
+
+bbt_status apply_signs(bbt_ctx* ctx, int m, const double* d, double* R, double* W) {
+  apply_signs_kernel<<<2 * ctx->num_sms, 256, 0, ctx->stream>>>(m, d, R, W);
+  BBT_LAUNCHED(ctx);
+  return BBT_OK;
+}
+
+bbt_status trsm_right_upper(bbt_ctx* ctx, long rows, int n, const double* R, long ldr, double* A, long lda) {
+  if (rows <= 0 || n <= 0) return BBT_OK;
+  if (n <= TB) {
+    long blocks = (rows + 127) / 128;
+    if (blocks > 16L * ctx->num_sms) blocks = 16L * ctx->num_sms;
+    ProfScope prof(ctx, BBT_PROF_CHOL, (double)rows * n * n);
+    trsm_leaf<<<(unsigned)blocks, 128, 0, ctx->stream>>>(rows, n, R, ldr, A, lda);
+    BBT_LAUNCHED(ctx);
+    return BBT_OK;
+  }
+  const int n1 = split_point(n), n2 = n - n1;
+  BBT_TRY(trsm_right_upper(ctx, rows, n1, R, ldr, A, lda));
+  BBT_TRY(dgemm(ctx, false, false, (int)rows, n2, n1, -1.0, A, lda, R + (long)n1 * ldr, ldr, 1.0, A + (long)n1 * lda,
+                lda));
+  return trsm_right_upper(ctx, rows, n2, R + n1 + (long)n1 * ldr, ldr, A + (long)n1 * lda, lda);
+}
+
+bbt_status potrf_upper(bbt_ctx* ctx, int n, double* G, long ld, int* flag) {
+  if (n <= 0) return BBT_OK;
+  if (n <= PB) {
+    ProfScope prof(ctx, BBT_PROF_CHOL, (double)n * n * n / 3.0);
+    potrf_leaf<<<1, 256, 0, ctx->stream>>>(n, G, ld, flag);
+    BBT_LAUNCHED(ctx);
+    return BBT_OK;
+  }
+  const int n1 = split_point(n), n2 = n - n1;
+  BBT_TRY(potrf_upper(ctx, n1, G, ld, flag));
+  BBT_TRY(trsm_right_upper(ctx, n2, n1, G, ld, G + n1, ld));   // G21 <- G21 R11^{-1} = R12^T
+  BBT_TRY(dgemm(ctx, false, true, n2, n2, n1, -1.0, G + n1, ld, G + n1, ld, 1.0, G + n1 + (long)n1 * ld, ld));
+  BBT_TRY(potrf_upper(ctx, n2, G + n1 + (long)n1 * ld, ld, flag));
+  mirror_kernel<<<2 * ctx->num_sms, 256, 0, ctx->stream>>>(n1, n2, G, ld);
+  BBT_LAUNCHED(ctx);
+  return BBT_OK;
+}
+
+bbt_status shift_diag(bbt_ctx* ctx, int n, double* G, long ld, double rel) {
+  shift_diag_kernel<<<1, 256, 0, ctx->stream>>>(n, G, ld, rel);
+  BBT_LAUNCHED(ctx);
+  return BBT_OK;
+}
+
+bbt_status identity(bbt_ctx* ctx, int n, double* W, long ld) {
+  identity_kernel<<<2 * ctx->num_sms, 256, 0, ctx->stream>>>(n, W, ld);
+  BBT_LAUNCHED(ctx);
+  return BBT_OK;
+}
+
+}  // namespace bbt

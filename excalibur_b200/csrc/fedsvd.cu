@@ -68,7 +68,8 @@ __global__ void embed_leading(int m, int kk, const double* __restrict__ Us, cons
 
 struct Layout {
   int P = 0;
-  size_t m = 0, rg = 0;
+  int precision = 0;
+  size_t m = 0, rg = 0, nmax = 0;
   std::vector<size_t> n, r, rpos;
   std::vector<bool> qr;
 };
@@ -76,11 +77,13 @@ struct Layout {
 bbt_status plan(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, Layout& L) {
   if (!cfg || cfg->participants < 1 || !cfg->local_n || !cfg->private_seeds)
     return fail(ctx, BBT_ERR_ARG, "fedsvd: bad config");
-  if (cfg->precision != 0) return fail(ctx, BBT_ERR_UNSUPPORTED, "fedsvd: precision mode %d", cfg->precision);
+  if (cfg->precision != 0 && cfg->precision != 1)
+    return fail(ctx, BBT_ERR_UNSUPPORTED, "fedsvd: precision mode %d (0 plain, 1 mixed)", cfg->precision);
   if (cfg->svd_mode < 0 || cfg->svd_mode > 3)
     return fail(ctx, BBT_ERR_UNSUPPORTED, "fedsvd: svd_mode %d (4, linear regression, is not built)", cfg->svd_mode);
   L.P = cfg->participants;
   L.m = cfg->m;
+  L.precision = cfg->precision;
   if (L.m < 3) return fail(ctx, BBT_ERR_UNSUPPORTED, "fedsvd: m=%zu (the reference needs m >= 3)", L.m);
   size_t gn = 0;
   L.rpos.push_back(0);
@@ -88,6 +91,7 @@ bbt_status plan(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, Layout& L) {
     const size_t n = cfg->local_n[c];
     if (n < 1) return fail(ctx, BBT_ERR_ARG, "fedsvd: local_n[%d]=0", c);
     L.n.push_back(n);
+    L.nmax = std::max(L.nmax, n);
     L.r.push_back(reduced_width(L.m, n));
     L.qr.push_back(has_local_qr(L.m, n));
     gn += n;
@@ -104,11 +108,16 @@ bbt_status plan(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, Layout& L) {
   return BBT_OK;
 }
 
-size_t scratch_bytes(const Layout& L) {
+size_t qr_scratch(const bbt_ctx* ctx, const Layout& L, long rows, const QrPlan& qp) {
+  if (L.precision == 1) return mixed_qr_workspace_bytes(ctx, (int)L.m, rows) + (8u << 20);
+  return qr_workspace_bytes(rows, (int)L.m, (int)L.m, qp) + (8u << 20);
+}
+
+size_t scratch_bytes(const bbt_ctx* ctx, const Layout& L) {
   QrPlan qp;
   size_t s = 0;
   for (int c = 0; c < L.P; ++c)
-    if (L.qr[c]) s = std::max(s, qr_workspace_bytes((long)L.n[c], (int)L.m, (int)L.m, qp));
+    if (L.qr[c]) s = std::max(s, qr_scratch(ctx, L, (long)L.n[c], qp));
   s = std::max(s, qr_workspace_bytes((long)L.rg, (int)L.m, (int)L.m, qp));
   const size_t m = L.m;
   s = std::max(s, (7 * (m + 1) * m + 4 * m) * 8 + 4096);          // twisted
@@ -129,12 +138,24 @@ size_t persistent_bytes(const Layout& L) {
   b += (4 * m * m + 6 * m) * 8 + 2048;                               // W, house, Vr, U_b(+V_b), alpha...
   b += m * m * 8 + 256;                                              // V_b
   b += m * std::max(m, L.rg) * 8 + 256;                              // tmp
+  if (L.precision == 1) {                                            // W_c, Z, the sketch S
+    b += (size_t)(L.P + 1) * (m * m * 8 + 256);
+    b += (size_t)sketch_rows((int)m) * sketch_pitch((long)L.nmax) * 2 + 256;
+  }
   return b;
 }
 
 // ---- batched local QR (all participants, concurrent streams, CUDA graph) --
 
-size_t qr_scratch(long rows, int m, const QrPlan& qp) { return qr_workspace_bytes(rows, m, m, qp) + (8u << 20); }
+// What every participant's local QR needs besides its block: the precision
+// mode, the shared sketch (mode 1) and the per-participant outputs.
+struct QrJob {
+  int precision = 0;
+  const void* S = nullptr;
+  long spitch = 0;
+  std::vector<double*> RT, tau, T, W;
+  bool compute_v = false;
+};
 
 // Participants needing a local QR, largest first, each to the stream with the
 // least work so far (longest-processing-time order).
@@ -152,34 +173,34 @@ std::vector<std::vector<int>> schedule(const Layout& L, int streams) {
   return out;
 }
 
-size_t batched_scratch(const Layout& L, int streams, const QrPlan& qp) {
+size_t batched_scratch(const bbt_ctx* ctx, const Layout& L, int streams, const QrPlan& qp) {
   if (streams <= 1) {
     size_t s = 0;
-    for (int c = 0; c < L.P; ++c) if (L.qr[c]) s = std::max(s, qr_scratch((long)L.n[c], (int)L.m, qp));
+    for (int c = 0; c < L.P; ++c) if (L.qr[c]) s = std::max(s, qr_scratch(ctx, L, (long)L.n[c], qp));
     return s;
   }
   size_t tot = 0;
   for (auto& lst : schedule(L, streams)) {
     size_t s = 0;
-    for (int c : lst) s = std::max(s, qr_scratch((long)L.n[c], (int)L.m, qp));
+    for (int c : lst) s = std::max(s, qr_scratch(ctx, L, (long)L.n[c], qp));
     tot += s + 4096;
   }
   return tot;
 }
 
-bbt_status qr_one(bbt_ctx* c, int mi, double* X, long n, double* RT, double* tau, double* T, bool compute_v,
-                  const QrPlan& qp) {
-  BBT_TRY(geqrf(c, n, mi, X, n, tau, T, qp));
-  BBT_TRY(r_transpose(c, mi, X, n, RT));
-  if (compute_v) BBT_TRY(orgqr(c, n, mi, X, n, tau, T, qp));   // X_c <- Q (= local_v)
+bbt_status qr_one(bbt_ctx* c, int mi, double* X, long n, int p, const QrJob& job, const QrPlan& qp) {
+  if (job.precision == 1)   // R (column-major) is R^T row-major: the same bytes as r_transpose's output
+    return mixed_local_qr(c, mi, n, X, job.S, job.spitch, job.RT[p], job.compute_v ? job.W[p] : nullptr);
+  BBT_TRY(geqrf(c, n, mi, X, n, job.tau[p], job.T[p], qp));
+  BBT_TRY(r_transpose(c, mi, X, n, job.RT[p]));
+  if (job.compute_v) BBT_TRY(orgqr(c, n, mi, X, n, job.tau[p], job.T[p], qp));   // X_c <- Q (= local_v)
   return BBT_OK;
 }
 
 // Issue every participant's QR on its side stream (fork/join through events
 // on ctx->stream).  Sub-contexts share the device arena in disjoint slices.
-bbt_status issue_batched(bbt_ctx* ctx, const Layout& L, double* const* X, const std::vector<double*>& RT,
-                         const std::vector<double*>& tau, const std::vector<double*>& T, bool compute_v,
-                         int streams, const QrPlan& qp) {
+bbt_status issue_batched(bbt_ctx* ctx, const Layout& L, double* const* X, const QrJob& job, int streams,
+                         const QrPlan& qp) {
   const int mi = (int)L.m;
   auto sched = schedule(L, streams);
   while ((int)ctx->side.size() < streams) {
@@ -196,7 +217,7 @@ bbt_status issue_batched(bbt_ctx* ctx, const Layout& L, double* const* X, const 
   for (int s = 0; s < streams; ++s) {
     if (sched[s].empty()) continue;
     size_t slice = 0;
-    for (int c : sched[s]) slice = std::max(slice, qr_scratch((long)L.n[c], mi, qp));
+    for (int c : sched[s]) slice = std::max(slice, qr_scratch(ctx, L, (long)L.n[c], qp));
     char* base = ctx->ws.take<char>(slice);
     if (!base) return fail(ctx, BBT_ERR_NOMEM, "batched local QR: workspace slice");
     bbt_ctx sub;
@@ -210,7 +231,7 @@ bbt_status issue_batched(bbt_ctx* ctx, const Layout& L, double* const* X, const 
     sub.d_barrier = ctx->d_barrier;
     BBT_CUDA(ctx, cudaStreamWaitEvent(sub.stream, ctx->side_ev[streams], 0));
     for (int c : sched[s]) {
-      bbt_status st = qr_one(&sub, mi, X[c], (long)L.n[c], RT[c], tau[c], T[c], compute_v, qp);
+      bbt_status st = qr_one(&sub, mi, X[c], (long)L.n[c], c, job, qp);
       if (st != BBT_OK) { ctx->err = sub.err; return st; }
     }
     ctx->launches += sub.launches;
@@ -220,23 +241,23 @@ bbt_status issue_batched(bbt_ctx* ctx, const Layout& L, double* const* X, const 
   return BBT_OK;
 }
 
-bbt_status local_qr_stage(bbt_ctx* ctx, const Layout& L, double* const* X, const std::vector<double*>& RT,
-                          const std::vector<double*>& tau, const std::vector<double*>& T, bool compute_v,
-                          int streams, const QrPlan& qp, bool use_graph) {
+bbt_status local_qr_stage(bbt_ctx* ctx, const Layout& L, double* const* X, const QrJob& job, int streams,
+                          const QrPlan& qp, bool use_graph) {
   const int mi = (int)L.m;
   if (streams <= 1) {
     for (int c = 0; c < L.P; ++c)
-      if (L.qr[c]) BBT_TRY(qr_one(ctx, mi, X[c], (long)L.n[c], RT[c], tau[c], T[c], compute_v, qp));
+      if (L.qr[c]) BBT_TRY(qr_one(ctx, mi, X[c], (long)L.n[c], c, job, qp));
     return BBT_OK;
   }
-  std::vector<size_t> key = {L.m, (size_t)compute_v, (size_t)streams, (size_t)qp.nb, (size_t)ctx->ws.base,
-                             ctx->ws.cap, ctx->ws.top};
+  std::vector<size_t> key = {L.m, (size_t)job.compute_v, (size_t)streams, (size_t)qp.nb, (size_t)ctx->ws.base,
+                             ctx->ws.cap, ctx->ws.top, (size_t)job.precision, (size_t)job.S};
   for (int c = 0; c < L.P; ++c) {
     key.push_back((size_t)X[c]);
     key.push_back(L.n[c]);
-    key.push_back((size_t)RT[c]);
+    key.push_back((size_t)job.RT[c]);
+    key.push_back(job.W.empty() ? 0 : (size_t)job.W[c]);
   }
-  if (!use_graph) return issue_batched(ctx, L, X, RT, tau, T, compute_v, streams, qp);
+  if (!use_graph) return issue_batched(ctx, L, X, job, streams, qp);
   if (ctx->qr_graph && key == ctx->qr_key) {
     BBT_CUDA(ctx, cudaGraphLaunch(ctx->qr_graph, ctx->stream));
     ctx->launches += ctx->qr_graph_nodes;
@@ -245,13 +266,13 @@ bbt_status local_qr_stage(bbt_ctx* ctx, const Layout& L, double* const* X, const
   if (ctx->qr_key != key) {   // first call with this shape: run eagerly (sets every kernel attribute)
     ctx->qr_key = key;
     if (ctx->qr_graph) { cudaGraphExecDestroy(ctx->qr_graph); ctx->qr_graph = nullptr; }
-    return issue_batched(ctx, L, X, RT, tau, T, compute_v, streams, qp);
+    return issue_batched(ctx, L, X, job, streams, qp);
   }
   // second call: capture the same schedule once, replay it from now on
   const uint64_t before = ctx->launches;
   const size_t top = ctx->ws.top;
   BBT_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed));
-  bbt_status st = issue_batched(ctx, L, X, RT, tau, T, compute_v, streams, qp);
+  bbt_status st = issue_batched(ctx, L, X, job, streams, qp);
   cudaGraph_t g = nullptr;
   cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
   if (st != BBT_OK) { if (g) cudaGraphDestroy(g); return st; }
@@ -273,7 +294,8 @@ size_t fedsvd_workspace_bytes(const bbt_fedsvd_config* cfg) {
   Layout L;
   bbt_ctx dummy;
   if (plan(&dummy, cfg, L) != BBT_OK) return 0;
-  return persistent_bytes(L) + scratch_bytes(L);
+  dummy.num_sms = 148;
+  return persistent_bytes(L) + scratch_bytes(&dummy, L);
 }
 
 bbt_status fedsvd(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* X, double* sigma,
@@ -289,7 +311,7 @@ bbt_status fedsvd(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* X, 
   {
     int nqr = 0;
     for (int c = 0; c < P; ++c) nqr += L.qr[c];
-    std::vector<size_t> skey = {L.m};
+    std::vector<size_t> skey = {L.m, (size_t)L.precision};
     for (int c = 0; c < P; ++c) skey.push_back(L.n[c]);
     if (ctx->tuned_streams > 0 && ctx->tuned_key == skey) {
       streams = ctx->tuned_streams;
@@ -298,7 +320,8 @@ bbt_status fedsvd(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* X, 
       streams = 8;
     }
   }
-  const size_t need = persistent_bytes(L) + std::max(scratch_bytes(L), batched_scratch(L, streams, qp) + (64u << 20));
+  const size_t need =
+      persistent_bytes(L) + std::max(scratch_bytes(ctx, L), batched_scratch(ctx, L, streams, qp) + (64u << 20));
   if (ctx->ws.cap < need) BBT_CUDA(ctx, ctx->ws.reserve(need));
   ctx->ws.reset();
   const size_t tq = ((m + qp.nb - 1) / qp.nb) * qp.nb * qp.nb;
@@ -324,6 +347,21 @@ bbt_status fedsvd(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* X, 
   int* cnt = ctx->ws.take<int>(8);
   double* tmp = ctx->ws.take<double>(m * std::max(m, rg));
   if (!tmp) return fail(ctx, BBT_ERR_NOMEM, "fedsvd: workspace");
+  QrJob job;
+  job.precision = L.precision;
+  job.RT = RT;
+  job.tau = tauc;
+  job.T = Tc;
+  double* Z = nullptr;
+  void* S = nullptr;
+  if (L.precision == 1) {
+    for (int c = 0; c < P; ++c) job.W.push_back(ctx->ws.take<double>(m * m));
+    Z = ctx->ws.take<double>(m * m);
+    S = ctx->ws.take<char>((size_t)sketch_rows(mi) * sketch_pitch((long)L.nmax) * 2);
+    if (!S) return fail(ctx, BBT_ERR_NOMEM, "fedsvd: workspace (mixed precision)");
+    job.S = S;
+    job.spitch = sketch_pitch((long)L.nmax);
+  }
 
   cudaEvent_t ev[7];
   for (auto& e : ev) BBT_CUDA(ctx, cudaEventCreate(&e));
@@ -335,13 +373,21 @@ bbt_status fedsvd(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* X, 
 
   // 1) local QR (client.cpp:572-589): A = X_c^T column-major n x m, in place
   const bool compute_u = cfg->svd_mode != 3, compute_v = cfg->svd_mode != 2;   // client.cpp:491-492
+  job.compute_v = compute_v;
   std::vector<double*> masked(P);
   for (int c = 0; c < P; ++c) masked[c] = L.qr[c] ? RT[c] : X[c];
+  if (L.precision == 1) {
+    bool any = false;
+    for (int c = 0; c < P; ++c) any = any || L.qr[c];
+    if (any) BBT_TRY(rademacher(ctx, sketch_rows(mi), (long)L.nmax, S, 0x5EED5EEDull));
+    BBT_TRY(clear_tc_flags(ctx));
+  }
   {
     const size_t mark = ctx->ws.top;
-    BBT_TRY(local_qr_stage(ctx, L, X, RT, tauc, Tc, compute_v, streams, qp, true));
+    BBT_TRY(local_qr_stage(ctx, L, X, job, streams, qp, true));
     ctx->ws.top = mark;
   }
+  if (L.precision == 1) BBT_TRY(check_tc_flags(ctx, "fedsvd: mixed-precision local QR"));
   BBT_CUDA(ctx, cudaEventRecord(ev[1], ctx->stream));
   // 2) masks (client.cpp:593-596)
   for (int c = 0; c < P; ++c) {
@@ -397,7 +443,10 @@ bbt_status fedsvd(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* X, 
     BBT_TRY(dgemm(ctx, false, true, rc, k, m, 1.0, M + L.rpos[c], (long)rg, Ub, k, 0.0, tmp, rc));
     BBT_TRY(block_shift_mask(ctx, (size_t)k, (size_t)rc, MASK_PASSES, tmp, false, false, cfg->private_seeds[c]));
     const long n = (long)L.n[c];
-    if (L.qr[c]) {   // FinalVT^T (n x k col-major) = Q_c (n x m) tmp^T (m x k)
+    if (L.qr[c] && L.precision == 1) {   // Q_c = Q_p W_c: FinalVT^T = Q_p (W_c tmp^T)
+      BBT_TRY(dgemm(ctx, false, false, mi, k, m, 1.0, job.W[c], (long)m, tmp, rc, 0.0, Z, (long)m));
+      BBT_TRY(dgemm(ctx, false, false, (int)n, k, m, 1.0, X[c], n, Z, (long)m, 0.0, VT[c], n));
+    } else if (L.qr[c]) {   // FinalVT^T (n x k col-major) = Q_c (n x m) tmp^T (m x k)
       BBT_TRY(dgemm(ctx, false, false, (int)n, k, m, 1.0, X[c], n, tmp, rc, 0.0, VT[c], n));
     } else {
       BBT_CUDA(ctx, cudaMemcpyAsync(VT[c], tmp, (size_t)k * n * sizeof(double), cudaMemcpyDeviceToDevice,
@@ -441,23 +490,36 @@ bbt_status fedsvd_tune(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, int* best_str
   for (int c = 0; c < P; ++c)
     if (L.qr[c]) BBT_CUDA(ctx, cudaMalloc(&blocks[c], L.m * L.n[c] * sizeof(double)));
   const int cand_s[] = {1, 4, 8, 16};
-  const int cand_nb[] = {64, 128};
+  // the panel width only matters to the Householder (precision 0) path
+  const std::vector<int> cand_nb = L.precision == 1 ? std::vector<int>{128} : std::vector<int>{64, 128};
   size_t need = 0;
   for (int nb : cand_nb)
     for (int st : cand_s) {
       QrPlan qp;
       qp.nb = nb;
-      need = std::max(need, batched_scratch(L, st, qp));
+      need = std::max(need, batched_scratch(ctx, L, st, qp));
     }
   const size_t tq = ((L.m + 63) / 64) * 128 * 128;
+  const size_t sbytes = (size_t)sketch_rows(mi) * sketch_pitch((long)L.nmax) * 2;
   need += (size_t)P * (L.m * L.m + L.m + tq) * 8 + (size_t)P * 1024 + (64u << 20);
+  if (L.precision == 1) need += (size_t)P * (L.m * L.m * 8 + 256) + sbytes + 256;
   if (ctx->ws.cap < need) BBT_CUDA(ctx, ctx->ws.reserve(need));
   ctx->ws.reset();
-  std::vector<double*> RT(P), tau(P), T(P);
+  QrJob job;
+  job.precision = L.precision;
+  job.compute_v = true;
   for (int c = 0; c < P; ++c) {
-    RT[c] = ctx->ws.take<double>(L.m * L.m);
-    tau[c] = ctx->ws.take<double>(L.m);
-    T[c] = ctx->ws.take<double>(tq);
+    job.RT.push_back(ctx->ws.take<double>(L.m * L.m));
+    job.tau.push_back(ctx->ws.take<double>(L.m));
+    job.T.push_back(ctx->ws.take<double>(tq));
+    if (L.precision == 1) job.W.push_back(ctx->ws.take<double>(L.m * L.m));
+  }
+  if (L.precision == 1) {
+    void* S = ctx->ws.take<char>(sbytes);
+    if (!S) return fail(ctx, BBT_ERR_NOMEM, "tune: workspace");
+    BBT_TRY(rademacher(ctx, sketch_rows(mi), (long)L.nmax, S, 0x5EED5EEDull));
+    job.S = S;
+    job.spitch = sketch_pitch((long)L.nmax);
   }
   cudaEvent_t e0, e1;
   BBT_CUDA(ctx, cudaEventCreate(&e0));
@@ -476,7 +538,7 @@ bbt_status fedsvd_tune(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, int* best_str
           }
         const size_t mark = ctx->ws.top;
         BBT_CUDA(ctx, cudaEventRecord(e0, ctx->stream));
-        BBT_TRY(local_qr_stage(ctx, L, blocks.data(), RT, tau, T, true, st, qp, false));
+        BBT_TRY(local_qr_stage(ctx, L, blocks.data(), job, st, qp, false));
         BBT_CUDA(ctx, cudaEventRecord(e1, ctx->stream));
         BBT_CUDA(ctx, cudaEventSynchronize(e1));
         ctx->ws.top = mark;
@@ -489,7 +551,7 @@ bbt_status fedsvd_tune(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, int* best_str
   cudaEventDestroy(e1);
   ctx->tuned_streams = bs;
   ctx->tuned_nb = bnb;
-  ctx->tuned_key.assign(1, L.m);
+  ctx->tuned_key = {L.m, (size_t)L.precision};
   for (int c = 0; c < P; ++c) ctx->tuned_key.push_back(L.n[c]);
   (void)mi;
   if (best_streams) *best_streams = bs;

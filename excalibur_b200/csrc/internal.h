@@ -66,6 +66,10 @@ struct bbt_ctx {
 
 namespace bbt {
 
+// Slots of ctx->d_flag (16 ints) besides slot 0, the grid-barrier timeout
+// flag: the sketch pipeline's wait status and the Cholesky breakdown flag.
+enum { FLAG_SKETCH = 4, FLAG_CHOL = 5 };
+
 bbt_status fail(bbt_ctx* ctx, bbt_status s, const char* fmt, ...);
 bbt_status cuda_fail(bbt_ctx* ctx, cudaError_t e, const char* what);
 
@@ -180,6 +184,39 @@ bbt_status copy2d(bbt_ctx* ctx, int rows, int cols, const double* src, long lds,
 bbt_status fill(bbt_ctx* ctx, double* p, size_t n, double v);
 // RT (m x m row-major) = R^T, R = upper triangle of the top of column-major A
 bbt_status r_transpose(bbt_ctx* ctx, int m, const double* A, long lda, double* RT);
+
+// Split-precision sketch (sketch.cu): Y^T (m x N row-major FP64) = X S^T,
+// X row-major m x n FP64, S (N x n bf16, row pitch sketch_pitch(n)) +-1.
+long sketch_pitch(long n);
+int sketch_rows(int m);   // N used by the mixed local QR: 2m rounded up to 128
+size_t sketch_workspace_bytes(const bbt_ctx* ctx, int m, long n, int N);
+bbt_status rademacher(bbt_ctx* ctx, int N, long n, void* S, uint64_t seed);
+bbt_status sketch_bf16x3(bbt_ctx* ctx, int m, long n, const double* X, long ldx, int N, const void* S,
+                         long spitch, double* Y);
+
+// FP64 Cholesky / triangular solve (chol.cu), column-major.
+// A (rows x n) <- A R^{-1}, R upper n x n.
+bbt_status trsm_right_upper(bbt_ctx* ctx, long rows, int n, const double* R, long ldr, double* A, long lda);
+// G = R^T R in place (R upper, zeros below); a non-positive pivot sets *flag.
+bbt_status potrf_upper(bbt_ctx* ctx, int n, double* G, long ld, int* flag);
+bbt_status shift_diag(bbt_ctx* ctx, int n, double* G, long ld, double rel);
+bbt_status identity(bbt_ctx* ctx, int n, double* W, long ld);
+// d (cols) <- the row signs of LAPACK's Householder R for the orthonormal
+// matrix whose top block is A (rows x cols, rows >= cols; overwritten).
+bbt_status householder_signs(bbt_ctx* ctx, int rows, int cols, double* A, long lda, double* d);
+// R (m x m column-major) <- D R, W (optional) <- W D.
+bbt_status apply_signs(bbt_ctx* ctx, int m, const double* d, double* R, double* W);
+
+// Mixed-precision local QR (mixedqr.cu): X (row-major m x n = column-major
+// A = X^T, n x m) -> Q_p in place, R (m x m column-major upper), W = R_3^{-1}
+// (optional) with Q = Q_p W.  S: sketch_rows(m) x n Rademacher bf16 (row
+// pitch spitch >= n, a multiple of 8).
+size_t mixed_qr_workspace_bytes(const bbt_ctx* ctx, int m, long n);
+bbt_status mixed_local_qr(bbt_ctx* ctx, int m, long n, double* X, const void* S, long spitch, double* R,
+                          double* W);
+// Clear / read (with a stream sync) the sketch and Cholesky flags.
+bbt_status clear_tc_flags(bbt_ctx* ctx);
+bbt_status check_tc_flags(bbt_ctx* ctx, const char* what);
 
 // Whole pipeline (fedsvd.cu)
 bbt_status fedsvd(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* blocks, double* sigma,

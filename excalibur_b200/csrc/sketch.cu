@@ -1,0 +1,429 @@
+// Split-precision (BF16x3) sketch product on the 5th-generation tensor cores.
+//
+//   Y^T (m x N, row-major FP64) = X (m x n, row-major FP64) * S^T,
+//   S (N x n) a Rademacher (+-1) sketch held exactly in bf16.
+//
+// X is split into three bf16 pieces x0 + x1 + x2 (x0 = bf16(x), x1 =
+// bf16(x - x0), x2 = bf16(x - x0 - x1): 24 significant bits), so that
+// X S^T = x0 S^T + x1 S^T + x2 S^T with every product exact.  The tensor
+// cores accumulate in FP32 (with truncation: the error grows with the number
+// of accumulation steps), so the FP32 tile in tensor memory only ever holds
+// GROUP = 4 K-blocks (256 terms); the epilogue warps then drain it into FP64
+// registers while the MMAs fill the other half of a double-buffered
+// accumulator.  K is split across CTAs only for parallelism; the FP64
+// partial tiles are summed in a fixed order by a second kernel.
+//
+// Kernel structure (one CTA = 320 threads per 128 x 128 output tile):
+//   warp 8, one lane : TMA producer -- per K-block of 64, the three 128 x 64
+//                      bf16 tiles of x0/x1/x2 (one 3-D tensor map) and the
+//                      128 x 64 tile of S, SWIZZLE_128B, into a 3-stage ring;
+//   warp 9, one lane : tcgen05.mma issuer -- 3 pieces x 4 MMAs of
+//                      128 x 128 x 16 (kind::f16, bf16 in, f32 accumulate)
+//                      per K-block into TMEM buffer (group & 1);
+//                      tcgen05.commit frees each stage and hands each full
+//                      buffer to the epilogue;
+//   warps 0-7        : accumulators -- warp w reads TMEM lanes 32 (w % 4)..
+//                      and columns 64 (w / 4).., adds them to 64 FP64
+//                      registers per thread, releases the buffer; at the end
+//                      writes its 32 x 64 FP64 block of the partial tile.
+// Every mbarrier wait is bounded; a wait that gives up sets an error flag
+// and the CTA drains its copies, frees its tensor memory and returns.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "internal.h"
+
+namespace bbt {
+namespace {
+
+constexpr int TM = 128, TN = 128, TK = 64;
+constexpr int PIECES = 3;
+constexpr int STAGES = 3;
+constexpr int GROUP = 4;                                  // K-blocks per FP32 accumulation
+constexpr int EPI_WARPS = 8;
+constexpr int THREADS = (EPI_WARPS + 2) * 32;
+constexpr int A_TILE = TM * TK * 2;                       // 16 KB
+constexpr int B_TILE = TN * TK * 2;                       // 16 KB
+constexpr int STAGE_BYTES = PIECES * A_TILE + B_TILE;     // 64 KB
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
+constexpr uint32_t TMEM_COLS = 2 * TN;
+constexpr long SPIN_LIMIT = 1L << 24;
+constexpr int MAX_SPLITS = 32;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+// Bounded wait for the phase of the given parity to complete.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  for (long it = 0; it < SPIN_LIMIT; ++it) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map, uint32_t bar, int x, int y, int z) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(dst),
+      "l"(map), "r"(bar), "r"(x), "r"(y), "r"(z)
+      : "memory");
+}
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, uint32_t bar, int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::"r"(dst),
+      "l"(map), "r"(bar), "r"(x), "r"(y)
+      : "memory");
+}
+
+// Shared-memory matrix descriptor of a K-major SWIZZLE_128B tile (rows of
+// 128 B, 8-row groups 1024 B apart): start >> 4, leading offset 1 (unused
+// for swizzled K-major), stride offset 1024 >> 4, descriptor version 1,
+// layout type 2 (128-byte swizzle).
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+  return (uint64_t)((saddr & 0x3FFFFu) >> 4) | (1ull << 16) | (64ull << 32) | (1ull << 46) | (2ull << 61);
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc));
+}
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// 32 lanes x 16 consecutive 32-bit columns: thread t gets lane (base lane + t).
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+        "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+struct SketchArgs {
+  double* part;       // [splits][M][N]
+  int M, N;
+  int kblocks, kb_per_split;
+  int* err;
+};
+
+__global__ void __launch_bounds__(THREADS, 1)
+sketch_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, SketchArgs P) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint64_t* bars = (uint64_t*)(smem + STAGES * STAGE_BYTES);
+  uint32_t* tmem_slot = (uint32_t*)(bars + 2 * STAGES + 4);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int n0 = blockIdx.x * TN, m0 = blockIdx.y * TM;
+  const int kb0 = blockIdx.z * P.kb_per_split;
+  const int nk = min(P.kblocks - kb0, P.kb_per_split);
+  const int ngroups = (nk + GROUP - 1) / GROUP;
+  const uint32_t full0 = smem_u32(bars), empty0 = smem_u32(bars + STAGES);
+  const uint32_t accf0 = smem_u32(bars + 2 * STAGES), acce0 = smem_u32(bars + 2 * STAGES + 2);
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(full0 + 8 * s, 1);
+      mbar_init(empty0 + 8 * s, 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(accf0 + 8 * b, 1);
+      mbar_init(acce0 + 8 * b, EPI_WARPS);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == EPI_WARPS) {
+    if (lane == 0) {   // ---- TMA producer
+      int issued = 0;
+      bool ok = true;
+      for (int kb = 0; kb < nk; ++kb) {
+        const int s = kb % STAGES;
+        const uint32_t ph = (uint32_t)(kb / STAGES) & 1u;
+        if (!mbar_wait(empty0 + 8 * s, ph ^ 1u)) { ok = false; break; }
+        const uint32_t fb = full0 + 8 * s;
+        mbar_expect_tx(fb, STAGE_BYTES);
+        const uint32_t st = smem_u32(smem + (size_t)s * STAGE_BYTES);
+        const int kx = (kb0 + kb) * TK;
+        for (int p = 0; p < PIECES; ++p) tma_load_3d(st + p * A_TILE, &tmA, fb, kx, m0, p);
+        tma_load_2d(st + PIECES * A_TILE, &tmB, fb, kx, n0);
+        ++issued;
+      }
+      if (!ok) atomicExch(P.err, 1);
+      // drain: every issued copy has landed before the CTA may exit
+      for (int kb = max(0, issued - STAGES); kb < issued; ++kb)
+        if (!mbar_wait(full0 + 8 * (kb % STAGES), (uint32_t)(kb / STAGES) & 1u)) atomicExch(P.err, 4);
+    }
+  } else if (warp == EPI_WARPS + 1) {
+    if (lane == 0) {   // ---- MMA issuer
+      const uint32_t idesc =
+          (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TN >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
+      bool ok = true;
+      for (int g = 0; g < ngroups && ok; ++g) {
+        const int buf = g & 1;
+        if (!mbar_wait(acce0 + 8 * buf, ((uint32_t)(g >> 1) & 1u) ^ 1u)) { ok = false; break; }
+        tc_fence_after();
+        const uint32_t d = tmem + (uint32_t)(buf * TN);
+        const int kend = min(nk, (g + 1) * GROUP);
+        for (int kb = g * GROUP; kb < kend; ++kb) {
+          const int s = kb % STAGES;
+          const uint32_t ph = (uint32_t)(kb / STAGES) & 1u;
+          if (!mbar_wait(full0 + 8 * s, ph)) { ok = false; break; }
+          tc_fence_after();
+          const uint32_t st = smem_u32(smem + (size_t)s * STAGE_BYTES);
+          const uint64_t bd = sw128_desc(st + PIECES * A_TILE);
+          for (int p = 0; p < PIECES; ++p) {
+            const uint64_t ad = sw128_desc(st + p * A_TILE);
+#pragma unroll
+            for (int kk = 0; kk < TK / 16; ++kk)   // +32 bytes along K = +2 in the descriptor's address field
+              mma_bf16(d, ad + 2 * kk, bd + 2 * kk, idesc, (kb != g * GROUP || p != 0 || kk != 0) ? 1u : 0u);
+          }
+          mma_commit(empty0 + 8 * s);
+        }
+        mma_commit(accf0 + 8 * buf);   // arrives once this group's MMAs have completed
+      }
+      if (!ok) atomicExch(P.err, 2);
+    }
+  } else {
+    // ---- accumulators: lanes 32 (warp % 4).., columns 64 (warp / 4)..
+    const int q = warp & 3, ch = warp >> 2;
+    double acc[64];
+#pragma unroll
+    for (int i = 0; i < 64; ++i) acc[i] = 0.0;
+    bool ok = true;
+    for (int g = 0; g < ngroups; ++g) {
+      const int buf = g & 1;
+      if (!mbar_wait(accf0 + 8 * buf, (uint32_t)(g >> 1) & 1u)) { ok = false; break; }
+      tc_fence_after();
+      const uint32_t base = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(buf * TN + ch * 64);
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        uint32_t v[16];
+        tmem_ld16(base + (uint32_t)(c * 16), v);
+#pragma unroll
+        for (int i = 0; i < 16; ++i) acc[c * 16 + i] += (double)__uint_as_float(v[i]);
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(acce0 + 8 * buf);
+    }
+    if (!ok) {
+      if (lane == 0) atomicExch(P.err, 3);
+    } else {
+      const int row = m0 + q * 32 + lane;
+      if (row < P.M) {
+        double2* o = reinterpret_cast<double2*>(P.part + ((size_t)blockIdx.z * P.M + row) * P.N + n0 + ch * 64);
+#pragma unroll
+        for (int i = 0; i < 32; ++i) o[i] = make_double2(acc[2 * i], acc[2 * i + 1]);
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+  }
+}
+
+// X (m x n row-major, ld ldx) -> three bf16 pieces A[p][i][j] (row pitch `pitch`).
+__global__ void split3_kernel(int m, long n, const double* __restrict__ X, long ldx, __nv_bfloat16* __restrict__ A,
+                              long pitch) {
+  const long total = (long)m * n;
+  const size_t plane = (size_t)m * pitch;
+  for (long f = blockIdx.x * (long)blockDim.x + threadIdx.x; f < total; f += (long)gridDim.x * blockDim.x) {
+    const long i = f / n, j = f - i * n;
+    const double x = X[i * ldx + j];
+    const __nv_bfloat16 b0 = __double2bfloat16(x);
+    const double r1 = x - (double)__bfloat162float(b0);
+    const __nv_bfloat16 b1 = __double2bfloat16(r1);
+    const double r2 = r1 - (double)__bfloat162float(b1);
+    const __nv_bfloat16 b2 = __double2bfloat16(r2);
+    const size_t o = (size_t)i * pitch + j;
+    A[o] = b0;
+    A[plane + o] = b1;
+    A[2 * plane + o] = b2;
+  }
+}
+
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {   // splitmix64 finaliser
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+// S (N x n, row pitch `pitch`) with independent +-1 entries.
+__global__ void rademacher_kernel(int N, long n, long pitch, __nv_bfloat16* __restrict__ S, uint64_t seed) {
+  const long total = (long)N * n;
+  const __nv_bfloat16_raw plus = {0x3F80}, minus = {0xBF80};
+  for (long f = blockIdx.x * (long)blockDim.x + threadIdx.x; f < total; f += (long)gridDim.x * blockDim.x) {
+    const long i = f / n, j = f - i * n;
+    S[(size_t)i * pitch + j] = (mix64(seed ^ (uint64_t)f * 0xD1B54A32D192ED03ull) & 1u) ? __nv_bfloat16(plus)
+                                                                                           : __nv_bfloat16(minus);
+  }
+}
+
+__global__ void sketch_reduce(long MN, int splits, const double* __restrict__ part, double* __restrict__ Y) {
+  for (long f = blockIdx.x * (long)blockDim.x + threadIdx.x; f < MN; f += (long)gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int z = 0; z < splits; ++z) s += part[(size_t)z * MN + f];
+    Y[f] = s;
+  }
+}
+
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiled encode_fn() {
+  static EncodeTiled fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiled>(p);
+  }
+  return fn;
+}
+
+struct Split {
+  int splits, kb_per_split, kblocks;
+};
+
+// K split: the number of splits s (<= MAX_SPLITS) minimising
+// (waves of CTAs) x (K-blocks per CTA), the smallest s within 2% of it.
+Split plan_split(int m, long n, int N, int num_sms) {
+  Split r;
+  r.kblocks = (int)((n + TK - 1) / TK);
+  const long tiles = (long)(N / TN) * ((m + TM - 1) / TM);
+  double best = 1e300;
+  int bs = 1;
+  const int smax = std::min(MAX_SPLITS, r.kblocks);
+  std::vector<double> cost(smax + 1);
+  for (int s = 1; s <= smax; ++s) {
+    const long waves = (tiles * s + num_sms - 1) / num_sms;
+    cost[s] = (double)waves * ((r.kblocks + s - 1) / s);
+    best = std::min(best, cost[s]);
+  }
+  for (int s = 1; s <= smax; ++s)
+    if (cost[s] <= 1.02 * best) { bs = s; break; }
+  r.kb_per_split = (r.kblocks + bs - 1) / bs;
+  r.splits = (r.kblocks + r.kb_per_split - 1) / r.kb_per_split;
+  return r;
+}
+
+}  // namespace
+
+long sketch_pitch(long n) { return (n + 7) / 8 * 8; }
+
+int sketch_rows(int m) { return (2 * m + TN - 1) / TN * TN; }
+
+size_t sketch_workspace_bytes(const bbt_ctx* ctx, int m, long n, int N) {
+  const Split s = plan_split(m, n, N, ctx->num_sms > 0 ? ctx->num_sms : 148);
+  return (size_t)PIECES * m * sketch_pitch(n) * 2 + (size_t)s.splits * m * N * 8 + 4096;
+}
+
+bbt_status rademacher(bbt_ctx* ctx, int N, long n, void* S, uint64_t seed) {
+  rademacher_kernel<<<8 * ctx->num_sms, 256, 0, ctx->stream>>>(N, n, sketch_pitch(n), (__nv_bfloat16*)S, seed);
+  BBT_LAUNCHED(ctx);
+  return BBT_OK;
+}
+
+// Stream-ordered; a pipeline wait that gave up leaves a nonzero code in
+// ctx->d_flag[FLAG_SKETCH] (cleared and read by the caller).
+bbt_status sketch_bf16x3(bbt_ctx* ctx, int m, long n, const double* X, long ldx, int N, const void* S, long spitch,
+                         double* Y) {
+  if (m < 1 || n < 1 || N < TN || N % TN != 0 || n > (1L << 31) - TK || spitch < n || spitch % 8 != 0)
+    return fail(ctx, BBT_ERR_ARG, "sketch: m=%d n=%ld N=%d", m, n, N);
+  EncodeTiled enc = encode_fn();
+  if (!enc) return fail(ctx, BBT_ERR_CUDA, "sketch: cuTensorMapEncodeTiled is not available");
+  const long pitch = sketch_pitch(n);
+  const Split sp = plan_split(m, n, N, ctx->num_sms);
+  const size_t mark = ctx->ws.top;
+  __nv_bfloat16* A = ctx->ws.take<__nv_bfloat16>((size_t)PIECES * m * pitch);
+  double* part = ctx->ws.take<double>((size_t)sp.splits * m * N);
+  if (!part) return fail(ctx, BBT_ERR_NOMEM, "sketch: workspace");
+  split3_kernel<<<8 * ctx->num_sms, 256, 0, ctx->stream>>>(m, n, X, ldx, A, pitch);
+  BBT_LAUNCHED(ctx);
+
+  CUtensorMap ta, tb;
+  {
+    const cuuint64_t dims[3] = {(cuuint64_t)n, (cuuint64_t)m, (cuuint64_t)PIECES};
+    const cuuint64_t strides[2] = {(cuuint64_t)pitch * 2, (cuuint64_t)pitch * 2 * m};
+    const cuuint32_t box[3] = {TK, TM, 1}, es[3] = {1, 1, 1};
+    if (enc(&ta, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, A, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return fail(ctx, BBT_ERR_CUDA, "sketch: tensor map of X");
+  }
+  {
+    const cuuint64_t dims[2] = {(cuuint64_t)n, (cuuint64_t)N};
+    const cuuint64_t strides[1] = {(cuuint64_t)spitch * 2};
+    const cuuint32_t box[2] = {TK, TN}, es[2] = {1, 1};
+    if (enc(&tb, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(S), dims, strides, box, es,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return fail(ctx, BBT_ERR_CUDA, "sketch: tensor map of S");
+  }
+  static bool attr = false;
+  if (!attr) {
+    BBT_CUDA(ctx, cudaFuncSetAttribute(sketch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+    attr = true;
+  }
+  SketchArgs a;
+  a.part = part;
+  a.M = m;
+  a.N = N;
+  a.kblocks = sp.kblocks;
+  a.kb_per_split = sp.kb_per_split;
+  a.err = ctx->d_flag + FLAG_SKETCH;
+  {
+    ProfScope prof(ctx, BBT_PROF_SKETCH, 2.0 * PIECES * (double)m * N * n);
+    sketch_kernel<<<dim3(N / TN, (m + TM - 1) / TM, sp.splits), THREADS, SMEM_BYTES, ctx->stream>>>(ta, tb, a);
+    BBT_LAUNCHED(ctx);
+  }
+  const long MN = (long)m * N;
+  sketch_reduce<<<4 * ctx->num_sms, 256, 0, ctx->stream>>>(MN, sp.splits, part, Y);
+  BBT_LAUNCHED(ctx);
+  ctx->ws.top = mark;
+  return BBT_OK;
+}
+
+}  // namespace bbt

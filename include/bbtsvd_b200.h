@@ -38,7 +38,9 @@ typedef enum {
                                (the reference asserts here, bbtsvd.cpp:938) */
   BBT_ERR_NOMEM = 4,        /* device allocation failed */
   BBT_ERR_TIMEOUT = 5,      /* a bounded device-side wait gave up */
-  BBT_ERR_UNSUPPORTED = 6   /* shape or mode outside what the reference supports */
+  BBT_ERR_UNSUPPORTED = 6,  /* shape or mode outside what the reference supports */
+  BBT_ERR_NUMERIC = 7       /* a Cholesky pivot of the mixed-precision local QR was not
+                               positive (rank-deficient block); rerun with precision 0 */
 } bbt_status;
 
 typedef struct bbt_ctx bbt_ctx;
@@ -138,6 +140,26 @@ bbt_status bbt_dgemm(bbt_ctx* ctx, int transa, int transb, int M, int N, long K,
                      const double* d_A, long lda, const double* d_B, long ldb, double beta,
                      double* d_C, long ldc);
 
+/* ---- split-precision sketch and mixed-precision local QR -----------------
+ * bbt_rademacher: d_S (N x local_n bf16, row pitch round_up(local_n, 8)
+ * elements) <- independent +-1 entries drawn from `seed`.
+ * bbt_sketch_bf16x3: d_Y (row-major m x N, FP64) = X S^T for X row-major
+ * m x local_n FP64, as three bf16 pieces of X times the exact bf16 S on the
+ * tensor cores (tcgen05, FP32 accumulation per K-chunk, FP64 across chunks).
+ * N must be a multiple of 128.
+ * bbt_mixed_local_qr: the precision-1 local QR.  d_x (row-major m x
+ * local_n, local_n > m) is overwritten by Q_p^T, d_r receives R (m x m
+ * column-major, upper triangular, positive diagonal; equal as memory to the
+ * row-major R^T of bbt_local_qr up to row signs), d_w (may be NULL) receives
+ * W (m x m column-major) with Q = Q_p W orthonormal and A = X^T = Q R.
+ * Additive: the reference has no split-precision path (its local QR is
+ * client.cpp:417-445). */
+bbt_status bbt_rademacher(bbt_ctx* ctx, int N, size_t local_n, unsigned long long seed, void* d_S);
+bbt_status bbt_sketch_bf16x3(bbt_ctx* ctx, int m, size_t local_n, const double* d_x, int N,
+                             const void* d_S, double* d_Y);
+bbt_status bbt_mixed_local_qr(bbt_ctx* ctx, size_t m, size_t local_n, double* d_x, double* d_r,
+                              double* d_w);
+
 /* ---- kernel profiling -------------------------------------------------------
  * With profiling on, every launch of the library's kernels of a class is
  * bracketed by CUDA events on the launching stream.  bbt_profile_get
@@ -146,7 +168,8 @@ bbt_status bbt_dgemm(bbt_ctx* ctx, int transa, int transb, int M, int N, long K,
  * BBT_PROF_PANEL, bytes moved for BBT_PROF_MASK) since profiling was
  * switched on. */
 enum { BBT_PROF_DGEMM = 0, BBT_PROF_PANEL = 1, BBT_PROF_MASK = 2, BBT_PROF_RALHA = 3,
-       BBT_PROF_BISECT = 4, BBT_PROF_TWISTED = 5, BBT_PROF_CLASSES = 6 };
+       BBT_PROF_BISECT = 4, BBT_PROF_TWISTED = 5, BBT_PROF_SKETCH = 6, BBT_PROF_CHOL = 7,
+       BBT_PROF_CLASSES = 8 };
 bbt_status bbt_profile(bbt_ctx* ctx, int enable);
 bbt_status bbt_profile_get(bbt_ctx* ctx, int cls, double* ms, uint64_t* launches, double* work);
 
@@ -178,7 +201,9 @@ typedef struct {
                                     leading k x k bidiagonal; here bisection + twisted vectors on it),
                                     1 two-sided, 2 left vectors only (no FinalVT), 3 right vectors
                                     only (no FinalU) */
-  int precision;                 /* 0: plain FP64 */
+  int precision;                 /* 0: plain FP64 (the reference's Householder local QR);
+                                    1: mixed -- local QR by a BF16x3 tensor-core sketch
+                                    and one FP64 Cholesky-QR refinement pass */
 } bbt_fedsvd_config;
 
 /* Device-resident run.  d_blocks[c]: row-major m x local_n[c] input, used as
