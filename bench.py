@@ -9,6 +9,11 @@ vectors, back-transforms) on inputs resident in HBM; the 8 GB inputs are
 larger than L2, and are restored from a pristine device copy before every
 step (outside the timed events).
 
+By default both precision modes are timed: plain FP64 (the reference's
+Householder local QR) and mixed (BF16x3 tensor-core sketch + FP64
+Cholesky-QR refinement); the JSON value is the mixed run, the plain run sits
+beside it under "plain".
+
 Prints one JSON line (rank 0).  --impl reference times the reference's own
 CPU implementation (oracle/_ref, built from the reference's sources) on a
 bounded sample of the same workload.
@@ -41,6 +46,7 @@ def c3_rows(seed=0):
     """Row counts of the 64 participants of c3 (seeded)."""
     return [int(r) for r in np.random.default_rng(seed).integers(10_000, 200_001, 64)]
 METRIC = "SVD wall-s at rel err <=1e-10 vs FP64 oracle"
+PRECISION = {"plain": 0, "mixed": 1}
 
 
 def parse():
@@ -54,6 +60,8 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-sample-rows", type=int, default=50_000)
+    p.add_argument("--precision", default="both", choices=["both", "mixed", "plain"],
+                   help="both: time plain FP64 then mixed; the JSON value is the mixed run")
     return p.parse_args()
 
 
@@ -228,6 +236,9 @@ def cublas_dgemm_peak(torch, dev):
 
 
 def run_ours(args, rank, world):
+    """Times the pipeline at each requested precision (plain FP64 first, then
+    mixed); returns {precision: result} plus the end-to-end measurement of the
+    headline precision."""
     import torch
     import excalibur_b200 as eb
     P, m, n, spectrum = CONFIGS[args.config]
@@ -240,72 +251,97 @@ def run_ours(args, rank, world):
     pristine = [b.clone() for b in blocks]
     s_ref, U_ref = fp64_oracle(torch, pristine)
     pub, priv = eb.reference_seeds(0, P)
-    tuned = None
-    if sum(1 for b in pristine if b.shape[1] // m > 5) >= 8:   # batched local QR: tune it once
-        tuned = ctx.fedsvd_tune(m, [b.shape[1] for b in pristine])
-
-    def step():
-        for b, p0 in zip(blocks, pristine):
-            b.copy_(p0)
-        torch.cuda.synchronize()
-        return ctx.fedsvd(blocks, pub, priv)
-
-    for _ in range(args.warmup):
-        out = step()
-    acc = accuracy(torch, s_ref, U_ref, out[0], out[1])
-    del out
-    if world > 1:
-        torch.distributed.barrier()
-    torch.cuda.synchronize()
-    l0 = ctx.launches()
-    times = []
-    stage = {}
-    ctx.profile(True)
-    with Clocks(dev.index) as clk:
-        for _ in range(args.steps):
+    batched = sum(1 for b in pristine if b.shape[1] // m > 5) >= 8
+    precisions = {"both": ["plain", "mixed"], "plain": ["plain"], "mixed": ["mixed"]}[args.precision]
+    out_all = {}
+    for pname in precisions:
+        prec = PRECISION[pname]
+        tuned = ctx.fedsvd_tune(m, [b.shape[1] for b in pristine], precision=prec) if batched else None
+        for _ in range(args.warmup):
             for b, p0 in zip(blocks, pristine):
                 b.copy_(p0)
             torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            out = ctx.fedsvd(blocks, pub, priv)      # synchronises before returning
-            times.append(time.perf_counter() - t0)
-            for kk, v in ctx.stage_ms().items():
-                stage[kk] = stage.get(kk, 0.0) + v / args.steps
-            del out
-    prof = ctx.profile_get()
-    ctx.profile(False)
-    launches = (ctx.launches() - l0) // args.steps
-    torch.cuda.synchronize()
-    # device time of a step = sum of its stage events (CUDA events on the stream)
-    dev_ms = sum(stage.values())
-    sec = dev_ms / 1e3
-    if world > 1:
-        t = torch.tensor([sec], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        sec = float(t)
-    res = {"sec": sec, "host_sec": statistics.median(times), "stage_ms": stage, "acc": acc, "tuned": tuned,
-           "launches": launches, "prof": prof, "clocks": clk.summary()}
+            out = ctx.fedsvd(blocks, pub, priv, precision=prec)
+        acc = accuracy(torch, s_ref, U_ref, out[0], out[1])
+        del out
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        l0 = ctx.launches()
+        times = []
+        stage = {}
+        ctx.profile(True)
+        with Clocks(dev.index) as clk:
+            for _ in range(args.steps):
+                for b, p0 in zip(blocks, pristine):
+                    b.copy_(p0)
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                out = ctx.fedsvd(blocks, pub, priv, precision=prec)      # synchronises before returning
+                times.append(time.perf_counter() - t0)
+                for kk, v in ctx.stage_ms().items():
+                    stage[kk] = stage.get(kk, 0.0) + v / args.steps
+                del out
+        prof = ctx.profile_get()
+        ctx.profile(False)
+        launches = (ctx.launches() - l0) // args.steps
+        torch.cuda.synchronize()
+        # device time of a step = sum of its stage events (CUDA events on the stream)
+        sec = sum(stage.values()) / 1e3
+        if world > 1:
+            t = torch.tensor([sec], device=dev)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            sec = float(t)
+        out_all[pname] = {"sec": sec, "host_sec": statistics.median(times), "stage_ms": stage, "acc": acc,
+                          "tuned": tuned, "launches": launches, "prof": prof, "clocks": clk.summary()}
+    res = {"runs": out_all, "head": precisions[-1]}
     if rank == 0:
         res["dgemm_peak"] = cublas_dgemm_peak(torch, dev)
     if not args.no_e2e:
         # end to end through the host-pointer C-ABI entry: pinned host inputs,
         # H2D + pipeline + D2H inside the timed call
+        prec = PRECISION[res["head"]]
         hb = [p0.cpu().pin_memory().numpy() for p0 in pristine]
         del blocks
         torch.cuda.empty_cache()
         outbuf = (torch.empty(m, dtype=torch.float64).pin_memory().numpy(),
                   torch.empty(m * m, dtype=torch.float64).pin_memory().numpy(),
                   [torch.empty(m * p0.shape[1], dtype=torch.float64).pin_memory().numpy() for p0 in pristine])
-        ctx.fedsvd_host(hb, pub, priv, out=outbuf)     # warm
+        ctx.fedsvd_host(hb, pub, priv, precision=prec, out=outbuf)     # warm
         et = []
         for _ in range(max(1, min(args.steps, 3))):
             t0 = time.perf_counter()
-            sg, Ug, VTg = ctx.fedsvd_host(hb, pub, priv, out=outbuf)
+            sg, Ug, VTg = ctx.fedsvd_host(hb, pub, priv, precision=prec, out=outbuf)
             et.append(time.perf_counter() - t0)
         k = len(sg)
-        res["e2e"] = {"value": statistics.median(et), "unit": "s", "h2d_bytes_per_step": int(sum(h.nbytes for h in hb)),
+        res["e2e"] = {"value": statistics.median(et), "unit": "s", "precision": res["head"],
+                      "h2d_bytes_per_step": int(sum(h.nbytes for h in hb)),
                       "d2h_bytes_per_step": int(8 * (k + m * k + k * sum(h.shape[1] for h in hb)))}
     return res
+
+
+def roofline(prof, dgemm_peak):
+    """Roofline of the dominant kernel class (by event time) of a run."""
+    dom = max(prof, key=lambda k: prof[k][0])
+    ms, nl, work = prof[dom]
+    share = ms / sum(v[0] for v in prof.values())
+    if dom == "dgemm":
+        achieved = work / (ms * 1e-3) / 1e12
+        return {"kernel": "dgemm_kernel (DMMA m8n8k4 FP64)", "bound": "tensor", "achieved": achieved,
+                "peak": dgemm_peak, "unit": "TFLOP/s", "frac": achieved / dgemm_peak, "traffic": None,
+                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 figure)",
+                "launches": nl, "share": share}
+    peaks = measured_peaks()
+    achieved = work / (ms * 1e-3) / 1e9 if work else 0.0
+    return {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+            "frac": achieved / peaks["hbm_gbs"], "traffic": None, "launches": nl, "share": share}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        return json.load(open(path))
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "source": "fallback"}
 
 
 def main():
@@ -356,34 +392,34 @@ def main():
         torch.distributed.destroy_process_group()
     if rank != 0:
         return
-    # dominant kernel class by event time
-    prof = res["prof"]
-    dom = max(prof, key=lambda k: prof[k][0])
-    ms, nl, work = prof[dom]
-    if dom in ("dgemm",):
-        achieved = work / (ms * 1e-3) / 1e12
-        peak = res["dgemm_peak"]
-        roof = {"kernel": "dgemm_kernel (DMMA m8n8k4 FP64)", "bound": "tensor", "achieved": achieved, "peak": peak,
-                "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
-                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 figure)",
-                "launches": nl, "share": ms / sum(v[0] for v in prof.values())}
-    else:
-        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
-            os.path.join(ROOT, "MEASURED_PEAKS.json")) else {"hbm_gbs": 6650.0}
-        achieved = work / (ms * 1e-3) / 1e9 if work else 0.0
-        roof = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                "frac": achieved / peaks["hbm_gbs"], "traffic": None, "launches": nl,
-                "share": ms / sum(v[0] for v in prof.values())}
-    line = {"metric": METRIC, "value": res["sec"], "unit": "s", "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": res["sec"] * 1e3, "higher_is_better": False,
+    runs = res["runs"]
+    head = runs[res["head"]]
+    prof = head["prof"]
+    line = {"metric": METRIC, "value": head["sec"], "unit": "s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": head["sec"] * 1e3, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
-            "accuracy": res["acc"], "stage_ms": res["stage_ms"], "host_s_per_step": res["host_sec"],
-            "gpu_launches": res["launches"], "roofline": roof,
-            "batched_local_qr": (None if res["tuned"] is None else
-                                 {"streams": res["tuned"][0], "panel_width": res["tuned"][1],
-                                  "tuning_ms": res["tuned"][2], "graph": "captured on the 2nd call, replayed after"}),
-            "kernel_classes": {k: {"ms": v[0], "launches": v[1]} for k, v in prof.items()},
-            "clocks": res["clocks"]}
+            "precision": res["head"], "accuracy": head["acc"], "stage_ms": head["stage_ms"],
+            "host_s_per_step": head["host_sec"], "gpu_launches": head["launches"],
+            "roofline": roofline(prof, res["dgemm_peak"]),
+            "batched_local_qr": (None if head["tuned"] is None else
+                                 {"streams": head["tuned"][0], "panel_width": head["tuned"][1],
+                                  "tuning_ms": head["tuned"][2], "graph": "captured on the 2nd call, replayed after"}),
+            "kernel_classes": {k: {"ms": v[0], "launches": v[1]} for k, v in prof.items() if v[1]},
+            "clocks": head["clocks"]}
+    if prof.get("sketch", (0, 0, 0))[1]:
+        ms, nl, work = prof["sketch"]
+        pk = measured_peaks()
+        ach = work / (ms * 1e-3) / 1e12
+        line["roofline_sketch"] = {"kernel": "sketch_kernel (tcgen05 kind::f16 BF16x3, TMA, TMEM)",
+                                   "bound": "tensor", "achieved": ach, "peak": pk["bf16_tflops"], "unit": "TFLOP/s",
+                                   "frac": ach / pk["bf16_tflops"], "launches": nl,
+                                   "note": "achieved counts the 3 bf16 products (2 * 3 * m * N * n per launch)"}
+    if "plain" in runs and "mixed" in runs:
+        pl = runs["plain"]
+        line["plain"] = {"value": pl["sec"], "unit": "s", "accuracy": pl["acc"], "stage_ms": pl["stage_ms"],
+                         "gpu_launches": pl["launches"], "roofline": roofline(pl["prof"], res["dgemm_peak"]),
+                         "kernel_classes": {k: {"ms": v[0], "launches": v[1]} for k, v in pl["prof"].items() if v[1]}}
+        line["mixed_speedup_vs_plain"] = pl["sec"] / head["sec"]
     if "e2e" in res:
         line["e2e"] = res["e2e"]
     if not args.no_cpu_baseline:
