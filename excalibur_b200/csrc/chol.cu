@@ -9,71 +9,72 @@
 namespace bbt {
 namespace {
 
-constexpr int PB = 64;   // Cholesky leaf
+constexpr int PB = 32;   // Cholesky leaf (one warp)
 constexpr int TB = 32;   // triangular-solve leaf
+constexpr int LB = 16;   // sign-recovery LU leaf
 
 // Upper Cholesky G = R^T R of an n x n (n <= PB) diagonal block, in place:
-// R in the upper triangle, zeros below.  A pivot that is not positive sets
-// *flag and is replaced by 1 so the factorisation still completes.
-__global__ void __launch_bounds__(256) potrf_leaf(int n, double* __restrict__ G, long ld, int* flag) {
+// R in the upper triangle, zeros below.  One warp: lane k owns column k in
+// shared memory, so the n sequential steps synchronise with __syncwarp only.
+// A pivot that is not positive sets *flag and is replaced by 1 so the
+// factorisation still completes.
+__global__ void __launch_bounds__(32) potrf_leaf(int n, double* __restrict__ G, long ld, int* flag) {
   __shared__ double a[PB][PB + 1];
-  const int t = threadIdx.x;
-  for (int f = t; f < n * n; f += blockDim.x) {
-    const int i = f % n, k = f / n;
-    a[i][k] = (i <= k) ? G[i + (long)k * ld] : 0.0;
-  }
-  __syncthreads();
+  const int k = threadIdx.x;
+  for (int i = 0; i < PB; ++i) a[i][k] = (i <= k && k < n) ? G[i + (long)k * ld] : 0.0;
+  __syncwarp();
   for (int j = 0; j < n; ++j) {
     double d = a[j][j];
     if (!(d > 0.0) || !isfinite(d)) {
-      if (t == 0) atomicExch(flag, 1);
+      if (k == 0) atomicExch(flag, 1);
       d = 1.0;
     }
     const double r = sqrt(d);
-    __syncthreads();
-    for (int k = j + t; k < n; k += blockDim.x) a[j][k] = (k == j) ? r : a[j][k] / r;
-    __syncthreads();
-    const int w = n - j - 1;
-    for (int f = t; f < w * w; f += blockDim.x) {
-      const int i = j + 1 + f % w, k = j + 1 + f / w;
-      if (i <= k) a[i][k] -= a[j][i] * a[j][k];
+    __syncwarp();
+    if (k >= j && k < n) a[j][k] = (k == j) ? r : a[j][k] / r;
+    __syncwarp();
+    if (k > j && k < n) {
+      const double ajk = a[j][k];
+      for (int i = j + 1; i <= k; ++i) a[i][k] -= a[j][i] * ajk;
     }
-    __syncthreads();
+    __syncwarp();
   }
-  for (int f = t; f < n * n; f += blockDim.x) {
-    const int i = f % n, k = f / n;
-    G[i + (long)k * ld] = (i <= k) ? a[i][k] : 0.0;
-  }
+  if (k < n)
+    for (int i = 0; i < n; ++i) G[i + (long)k * ld] = (i <= k) ? a[i][k] : 0.0;
 }
 
-// A (rows x n, column-major) <- A R^{-1}, R upper n x n (n <= TB): one thread
-// per row, forward substitution along the row.
+// A (rows x n, column-major) <- A R^{-1}, R upper n x n (n <= NB): one thread
+// per row, forward substitution along the row.  Columns past n are zero in
+// shared memory (unit diagonal), so the unrolled loops need no guards.
+template <int NB>
 __global__ void __launch_bounds__(128) trsm_leaf(long rows, int n, const double* __restrict__ R, long ldr,
                                                  double* __restrict__ A, long lda) {
-  __shared__ double r[TB][TB + 1];
-  for (int f = threadIdx.x; f < n * n; f += blockDim.x) {
-    const int i = f % n, j = f / n;
-    r[i][j] = (i <= j) ? R[i + (long)j * ldr] : 0.0;
+  __shared__ double r[NB][NB + 1];
+  __shared__ double rinv[NB];
+  for (int f = threadIdx.x; f < NB * NB; f += blockDim.x) {
+    const int i = f % NB, j = f / NB;
+    r[i][j] = (i < n && j < n) ? (i <= j ? R[i + (long)j * ldr] : 0.0) : (i == j ? 1.0 : 0.0);
   }
   __syncthreads();
-  for (long row = blockIdx.x * (long)blockDim.x + threadIdx.x; row < rows; row += (long)gridDim.x * blockDim.x) {
-    double x[TB];
+  if (threadIdx.x < NB) rinv[threadIdx.x] = 1.0 / r[threadIdx.x][threadIdx.x];
+  __syncthreads();
+  // one row per thread (no row loop: the shared-memory reads of R must not be
+  // hoisted into registers across rows)
+  const long row = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (row >= rows) return;
+  double x[NB];
 #pragma unroll
-    for (int j = 0; j < TB; ++j)
-      if (j < n) x[j] = A[row + (long)j * lda];
+  for (int j = 0; j < NB; ++j) x[j] = (j < n) ? A[row + (long)j * lda] : 0.0;
 #pragma unroll
-    for (int j = 0; j < TB; ++j) {
-      if (j < n) {
-        double s = x[j];
+  for (int j = 0; j < NB; ++j) {
+    double s = x[j];
 #pragma unroll
-        for (int i = 0; i < j; ++i) s -= x[i] * r[i][j];
-        x[j] = s / r[j][j];
-      }
-    }
-#pragma unroll
-    for (int j = 0; j < TB; ++j)
-      if (j < n) A[row + (long)j * lda] = x[j];
+    for (int i = 0; i < j; ++i) s -= x[i] * r[i][j];
+    x[j] = s * rinv[j];
   }
+#pragma unroll
+  for (int j = 0; j < NB; ++j)
+    if (j < n) A[row + (long)j * lda] = x[j];
 }
 
 // G12 (n1 x n2, above the diagonal) <- X^T for X = G21 (n2 x n1, below), then X <- 0.
@@ -102,6 +103,14 @@ __global__ void shift_diag_kernel(int n, double* __restrict__ G, long ld, double
   for (int i = threadIdx.x; i < n; i += blockDim.x) G[i + (long)i * ld] += s;
 }
 
+__global__ void symmetrize_kernel(int n, double* __restrict__ G, long ld) {
+  const long total = (long)n * n;
+  for (long f = blockIdx.x * (long)blockDim.x + threadIdx.x; f < total; f += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(f % n), j = (int)(f / n);
+    if (i > j) G[i + (long)j * ld] = G[j + (long)i * ld];
+  }
+}
+
 __global__ void identity_kernel(int n, double* __restrict__ W, long ld) {
   const long total = (long)n * n;
   for (long f = blockIdx.x * (long)blockDim.x + threadIdx.x; f < total; f += (long)gridDim.x * blockDim.x) {
@@ -121,7 +130,7 @@ __global__ void identity_kernel(int n, double* __restrict__ W, long ld) {
 // Leaf: one CTA, up to TB columns of a tall panel (rows >= cols).
 __global__ void __launch_bounds__(1024) lu_sign_leaf(int rows, int cols, double* __restrict__ A, long lda,
                                                      double* __restrict__ d) {
-  __shared__ double rowj[TB];
+  __shared__ double rowj[LB];
   __shared__ double sdj, su;
   for (int j = 0; j < cols; ++j) {
     if (threadIdx.x == 0) {
@@ -142,33 +151,69 @@ __global__ void __launch_bounds__(1024) lu_sign_leaf(int rows, int cols, double*
   }
 }
 
-// B (n x ncols) <- L^{-1} B, L unit lower n x n (n <= TB): one thread per column.
+// The same elimination with the panel in registers: thread t owns row t
+// (rows <= 1024), row j is broadcast through shared memory at step j.
+__global__ void __launch_bounds__(1024) lu_sign_leaf_reg(int rows, int cols, double* __restrict__ A, long lda,
+                                                         double* __restrict__ d) {
+  __shared__ double rowj[LB];
+  __shared__ double sf;
+  const int i = threadIdx.x;
+  const bool live = i < rows;
+  double x[LB];
+#pragma unroll
+  for (int k = 0; k < LB; ++k) x[k] = (live && k < cols) ? A[i + (long)k * lda] : 0.0;
+#pragma unroll
+  for (int j = 0; j < LB; ++j) {
+    if (j < cols) {
+      if (i == j) {
+#pragma unroll
+        for (int k = 0; k < LB; ++k) rowj[k] = x[k];
+        const double c = x[j];
+        const double dj = c < 0.0 ? 1.0 : -1.0;
+        d[j] = dj;
+        sf = -dj / (1.0 + fabs(c));
+      }
+      __syncthreads();
+      if (i > j && live) {
+        const double l = sf * x[j];
+        x[j] = l;
+#pragma unroll
+        for (int k = j + 1; k < LB; ++k) x[k] -= l * rowj[k];
+      }
+      __syncthreads();
+    }
+  }
+  if (live)
+#pragma unroll
+    for (int k = 0; k < LB; ++k)
+      if (k < cols) A[i + (long)k * lda] = x[k];
+}
+
+// B (n x ncols) <- L^{-1} B, L unit lower n x n (n <= LB): one thread per
+// column; rows past n are zero in shared memory.
 __global__ void __launch_bounds__(128) trsm_llu_leaf(int n, long ncols, const double* __restrict__ L, long ldl,
                                                      double* __restrict__ B, long ldb) {
-  __shared__ double l[TB][TB + 1];
-  for (int f = threadIdx.x; f < n * n; f += blockDim.x) {
-    const int i = f % n, k = f / n;
-    l[i][k] = (i > k) ? L[i + (long)k * ldl] : 0.0;
+  __shared__ double l[LB][LB + 1];
+  for (int f = threadIdx.x; f < LB * LB; f += blockDim.x) {
+    const int i = f % LB, k = f / LB;
+    l[i][k] = (i > k && i < n) ? L[i + (long)k * ldl] : 0.0;
   }
   __syncthreads();
-  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < ncols; c += (long)gridDim.x * blockDim.x) {
-    double x[TB];
+  const long c = blockIdx.x * (long)blockDim.x + threadIdx.x;   // one column per thread
+  if (c >= ncols) return;
+  double x[LB];
 #pragma unroll
-    for (int i = 0; i < TB; ++i)
-      if (i < n) x[i] = B[i + c * ldb];
+  for (int i = 0; i < LB; ++i) x[i] = (i < n) ? B[i + c * ldb] : 0.0;
 #pragma unroll
-    for (int i = 0; i < TB; ++i) {
-      if (i < n) {
-        double s = x[i];
+  for (int i = 1; i < LB; ++i) {
+    double s = x[i];
 #pragma unroll
-        for (int k = 0; k < i; ++k) s -= l[i][k] * x[k];
-        x[i] = s;
-      }
-    }
-#pragma unroll
-    for (int i = 0; i < TB; ++i)
-      if (i < n) B[i + c * ldb] = x[i];
+    for (int k = 0; k < i; ++k) s -= l[i][k] * x[k];
+    x[i] = s;
   }
+#pragma unroll
+  for (int i = 0; i < LB; ++i)
+    if (i < n) B[i + c * ldb] = x[i];
 }
 
 // Row j of R (column-major, ld m) and column j of W (column-major, ld m) times d_j.
@@ -186,14 +231,13 @@ int split_point(int n) { return (n / 2 + TB - 1) / TB * TB; }
 
 bbt_status trsm_left_lower_unit(bbt_ctx* ctx, int n, long ncols, const double* L, long ldl, double* B, long ldb) {
   if (n <= 0 || ncols <= 0) return BBT_OK;
-  if (n <= TB) {
-    long blocks = (ncols + 127) / 128;
-    if (blocks > 16L * ctx->num_sms) blocks = 16L * ctx->num_sms;
+  if (n <= LB) {
+    const long blocks = (ncols + 127) / 128;
     trsm_llu_leaf<<<(unsigned)blocks, 128, 0, ctx->stream>>>(n, ncols, L, ldl, B, ldb);
     BBT_LAUNCHED(ctx);
     return BBT_OK;
   }
-  const int h = split_point(n);
+  const int h = (n / 2 + LB - 1) / LB * LB;
   BBT_TRY(trsm_left_lower_unit(ctx, h, ncols, L, ldl, B, ldb));
   BBT_TRY(dgemm(ctx, false, false, n - h, (int)ncols, h, -1.0, L + h, ldl, B, ldb, 1.0, B + h, ldb));
   return trsm_left_lower_unit(ctx, n - h, ncols, L + h + (long)h * ldl, ldl, B + h, ldb);
@@ -203,13 +247,16 @@ bbt_status trsm_left_lower_unit(bbt_ctx* ctx, int n, long ncols, const double* L
 
 bbt_status householder_signs(bbt_ctx* ctx, int rows, int cols, double* A, long lda, double* d) {
   if (cols <= 0) return BBT_OK;
-  if (cols <= TB) {
+  if (cols <= LB) {
     ProfScope prof(ctx, BBT_PROF_CHOL, (double)rows * cols * cols);
-    lu_sign_leaf<<<1, 1024, 0, ctx->stream>>>(rows, cols, A, lda, d);
+    if (rows <= 1024)
+      lu_sign_leaf_reg<<<1, 1024, 0, ctx->stream>>>(rows, cols, A, lda, d);
+    else
+      lu_sign_leaf<<<1, 1024, 0, ctx->stream>>>(rows, cols, A, lda, d);
     BBT_LAUNCHED(ctx);
     return BBT_OK;
   }
-  const int h = split_point(cols);
+  const int h = (cols / 2 + LB - 1) / LB * LB;   // a multiple of the leaf width, < cols
   BBT_TRY(householder_signs(ctx, rows, h, A, lda, d));
   BBT_TRY(trsm_left_lower_unit(ctx, h, cols - h, A, lda, A + (long)h * lda, lda));
   BBT_TRY(dgemm(ctx, false, false, rows - h, cols - h, h, -1.0, A + h, lda, A + (long)h * lda, lda, 1.0,
@@ -226,10 +273,12 @@ bbt_status apply_signs(bbt_ctx* ctx, int m, const double* d, double* R, double* 
 bbt_status trsm_right_upper(bbt_ctx* ctx, long rows, int n, const double* R, long ldr, double* A, long lda) {
   if (rows <= 0 || n <= 0) return BBT_OK;
   if (n <= TB) {
-    long blocks = (rows + 127) / 128;
-    if (blocks > 16L * ctx->num_sms) blocks = 16L * ctx->num_sms;
+    const long blocks = (rows + 127) / 128;
     ProfScope prof(ctx, BBT_PROF_CHOL, (double)rows * n * n);
-    trsm_leaf<<<(unsigned)blocks, 128, 0, ctx->stream>>>(rows, n, R, ldr, A, lda);
+    if (n <= 16)
+      trsm_leaf<16><<<(unsigned)blocks, 128, 0, ctx->stream>>>(rows, n, R, ldr, A, lda);
+    else
+      trsm_leaf<TB><<<(unsigned)blocks, 128, 0, ctx->stream>>>(rows, n, R, ldr, A, lda);
     BBT_LAUNCHED(ctx);
     return BBT_OK;
   }
@@ -244,7 +293,7 @@ bbt_status potrf_upper(bbt_ctx* ctx, int n, double* G, long ld, int* flag) {
   if (n <= 0) return BBT_OK;
   if (n <= PB) {
     ProfScope prof(ctx, BBT_PROF_CHOL, (double)n * n * n / 3.0);
-    potrf_leaf<<<1, 256, 0, ctx->stream>>>(n, G, ld, flag);
+    potrf_leaf<<<1, 32, 0, ctx->stream>>>(n, G, ld, flag);
     BBT_LAUNCHED(ctx);
     return BBT_OK;
   }
@@ -260,6 +309,12 @@ bbt_status potrf_upper(bbt_ctx* ctx, int n, double* G, long ld, int* flag) {
 
 bbt_status shift_diag(bbt_ctx* ctx, int n, double* G, long ld, double rel) {
   shift_diag_kernel<<<1, 256, 0, ctx->stream>>>(n, G, ld, rel);
+  BBT_LAUNCHED(ctx);
+  return BBT_OK;
+}
+
+bbt_status symmetrize_upper(bbt_ctx* ctx, int n, double* G, long ld) {
+  symmetrize_kernel<<<2 * ctx->num_sms, 256, 0, ctx->stream>>>(n, G, ld);
   BBT_LAUNCHED(ctx);
   return BBT_OK;
 }

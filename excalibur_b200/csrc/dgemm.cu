@@ -31,15 +31,19 @@ dgemm_kernel(int M, int N, long K, long kchunk, double alpha, const double* __re
              const double* __restrict__ B, long ldb, double beta, double* __restrict__ C, long ldc,
              double* __restrict__ P, int nfast) {
   constexpr int BM = 32 * WM, BN = 32 * WN, THREADS = 32 * WM * WN;
-  // nfast: blockIdx.x walks the N tiles, so the CTAs that share a block of
-  // rows of A run together and read it from HBM once (tall A, narrow C).
-  const int bm = nfast ? blockIdx.y : blockIdx.x, bn = nfast ? blockIdx.x : blockIdx.y;
+  // nfast bit 0: blockIdx.x walks the N tiles, so the CTAs that share a
+  // block of rows of A run together and read it from HBM once (tall A,
+  // narrow C).  Bit 1: only tiles touching the upper triangle of C are
+  // computed (symmetric products A^T A; the caller mirrors the rest).
+  const int nf = nfast & 1;
+  const int bm = nf ? blockIdx.y : blockIdx.x, bn = nf ? blockIdx.x : blockIdx.y;
   extern __shared__ double smem_[];
   auto As = reinterpret_cast<double(*)[BK][BM + PADA]>(smem_);
   auto Bs = reinterpret_cast<double(*)[BK][BN + PADB]>(smem_ + 2 * BK * (BM + PADA));
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wm = warp % WM, wn = warp / WM;
   const int i0 = bm * BM, j0 = bn * BN;
+  if ((nfast & 2) && i0 >= j0 + BN) return;   // entirely below the diagonal
   const long kbeg = (long)blockIdx.z * kchunk;
   const long kend = min(K, kbeg + kchunk);
 
@@ -210,7 +214,7 @@ size_t dgemm_workspace_bytes(const bbt_ctx* ctx, int M, int N, long K) {
 }
 
 bbt_status dgemm(bbt_ctx* ctx, bool ta, bool tb, int M, int N, long K, double alpha, const double* A,
-                 long lda, const double* B, long ldb, double beta, double* C, long ldc, int splits) {
+                 long lda, const double* B, long ldb, double beta, double* C, long ldc, int splits, bool upper) {
   if (M < 0 || N < 0 || K < 0) return fail(ctx, BBT_ERR_ARG, "dgemm: M=%d N=%d K=%ld", M, N, K);
   if (M == 0 || N == 0) return BBT_OK;
   int wm, wn;
@@ -240,8 +244,8 @@ bbt_status dgemm(bbt_ctx* ctx, bool ta, bool tb, int M, int N, long K, double al
     P = ctx->ws.take<double>((size_t)splits * M * N);
     if (!P) return fail(ctx, BBT_ERR_NOMEM, "dgemm: split-K workspace (%d x %d x %d)", splits, M, N);
   }
-  const int nfast = (tm >= tn && tm <= 65535) ? 1 : 0;
-  dim3 g(nfast ? tn : tm, nfast ? tm : tn, splits);
+  const int nfast = ((tm >= tn && tm <= 65535) ? 1 : 0) | (upper ? 2 : 0);
+  dim3 g((nfast & 1) ? tn : tm, (nfast & 1) ? tm : tn, splits);
   if (K == 0) {   // C = beta * C
     g.z = 1;
     P = nullptr;

@@ -118,6 +118,7 @@ size_t scratch_bytes(const bbt_ctx* ctx, const Layout& L) {
   size_t s = 0;
   for (int c = 0; c < L.P; ++c)
     if (L.qr[c]) s = std::max(s, qr_scratch(ctx, L, (long)L.n[c], qp));
+  if (L.precision == 1) s = std::max(s, qr_scratch(ctx, L, (long)L.rg, qp));
   s = std::max(s, qr_workspace_bytes((long)L.rg, (int)L.m, (int)L.m, qp));
   const size_t m = L.m;
   s = std::max(s, (7 * (m + 1) * m + 4 * m) * 8 + 4096);          // twisted
@@ -138,9 +139,9 @@ size_t persistent_bytes(const Layout& L) {
   b += (4 * m * m + 6 * m) * 8 + 2048;                               // W, house, Vr, U_b(+V_b), alpha...
   b += m * m * 8 + 256;                                              // V_b
   b += m * std::max(m, L.rg) * 8 + 256;                              // tmp
-  if (L.precision == 1) {                                            // W_c, Z, the sketch S
-    b += (size_t)(L.P + 1) * (m * m * 8 + 256);
-    b += (size_t)sketch_rows((int)m) * sketch_pitch((long)L.nmax) * 2 + 256;
+  if (L.precision == 1) {                                            // W_c, W_g, Z, R_g, the sketch S
+    b += (size_t)(L.P + 3) * (m * m * 8 + 256);
+    b += (size_t)sketch_rows((int)m) * sketch_pitch((long)std::max(L.nmax, L.rg)) * 2 + 256;
   }
   return b;
 }
@@ -352,15 +353,18 @@ bbt_status fedsvd(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* X, 
   job.RT = RT;
   job.tau = tauc;
   job.T = Tc;
-  double* Z = nullptr;
+  double *Z = nullptr, *Wg = nullptr, *Rg = nullptr;
   void* S = nullptr;
+  const long sk_cols = (long)std::max(L.nmax, L.rg);   // the sketch serves the local and the global QR
   if (L.precision == 1) {
     for (int c = 0; c < P; ++c) job.W.push_back(ctx->ws.take<double>(m * m));
     Z = ctx->ws.take<double>(m * m);
-    S = ctx->ws.take<char>((size_t)sketch_rows(mi) * sketch_pitch((long)L.nmax) * 2);
+    Wg = ctx->ws.take<double>(m * m);
+    Rg = ctx->ws.take<double>(m * m);
+    S = ctx->ws.take<char>((size_t)sketch_rows(mi) * sketch_pitch(sk_cols) * 2);
     if (!S) return fail(ctx, BBT_ERR_NOMEM, "fedsvd: workspace (mixed precision)");
     job.S = S;
-    job.spitch = sketch_pitch((long)L.nmax);
+    job.spitch = sketch_pitch(sk_cols);
   }
 
   cudaEvent_t ev[7];
@@ -377,9 +381,7 @@ bbt_status fedsvd(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* X, 
   std::vector<double*> masked(P);
   for (int c = 0; c < P; ++c) masked[c] = L.qr[c] ? RT[c] : X[c];
   if (L.precision == 1) {
-    bool any = false;
-    for (int c = 0; c < P; ++c) any = any || L.qr[c];
-    if (any) BBT_TRY(rademacher(ctx, sketch_rows(mi), (long)L.nmax, S, 0x5EED5EEDull));
+    BBT_TRY(rademacher(ctx, sketch_rows(mi), sk_cols, S, 0x5EED5EEDull));
     BBT_TRY(clear_tc_flags(ctx));
   }
   {
@@ -398,10 +400,18 @@ bbt_status fedsvd(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* X, 
   // 3) repartition + global QR of M^T (client.cpp:681-794)
   for (int c = 0; c < P; ++c)
     BBT_TRY(copy2d(ctx, mi, (int)L.r[c], masked[c], (long)L.r[c], M + L.rpos[c], (long)rg));
-  BBT_TRY(geqrf(ctx, (long)rg, mi, M, (long)rg, taug, Tg, qp));
-  r_rowmajor<<<4 * ctx->num_sms, 256, 0, ctx->stream>>>(mi, M, (long)rg, W);
-  BBT_LAUNCHED(ctx);
-  if (compute_v) BBT_TRY(orgqr(ctx, (long)rg, mi, M, (long)rg, taug, Tg, qp));   // M <- Q_g (rg x m)
+  if (L.precision == 1) {   // M <- Q_p, Q_g = Q_p W_g, R_g with dgeqrf's signs (mixedqr.cu)
+    const size_t mark = ctx->ws.top;
+    BBT_TRY(mixed_local_qr(ctx, mi, (long)rg, M, S, job.spitch, Rg, compute_v ? Wg : nullptr));
+    ctx->ws.top = mark;
+    BBT_TRY(transpose(ctx, mi, mi, Rg, (long)m, W, (long)m));   // W (row-major) = R_g
+    BBT_TRY(check_tc_flags(ctx, "fedsvd: mixed-precision global QR"));
+  } else {
+    BBT_TRY(geqrf(ctx, (long)rg, mi, M, (long)rg, taug, Tg, qp));
+    r_rowmajor<<<4 * ctx->num_sms, 256, 0, ctx->stream>>>(mi, M, (long)rg, W);
+    BBT_LAUNCHED(ctx);
+    if (compute_v) BBT_TRY(orgqr(ctx, (long)rg, mi, M, (long)rg, taug, Tg, qp));   // M <- Q_g (rg x m)
+  }
   BBT_CUDA(ctx, cudaEventRecord(ev[3], ctx->stream));
   // 4) Ralha bidiagonalisation, lower -> upper (client.cpp:801-954)
   BBT_TRY(ralha(ctx, mi, W, house, tauh, alpha, beta, Vr, cs));
@@ -437,10 +447,15 @@ bbt_status fedsvd(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* X, 
   rot_sweep<<<(k + 127) / 128, 128, 0, ctx->stream>>>(mi, k, cs, Ub);
   BBT_LAUNCHED(ctx);
   BBT_TRY(ormqr_left_notrans(ctx, (long)m, mi, house, (long)m, 1, tauh, Ub, k, k, true, qp));
+  if (L.precision == 1)   // Q_g U2 = Q_p (W_g U2): Rg (free by now) <- W_g U2, m x k column-major
+    BBT_TRY(dgemm(ctx, false, true, mi, k, m, 1.0, Wg, (long)m, Ub, k, 0.0, Rg, (long)m));
   for (int c = 0; c < P; ++c) {   // :1179-1195
     const int rc = (int)L.r[c];
     // tmp (k x r_c row-major) = U2^T Q_g[rows_c, :]^T  ==  column-major r_c x k = Q_g[rows_c,:] U2
-    BBT_TRY(dgemm(ctx, false, true, rc, k, m, 1.0, M + L.rpos[c], (long)rg, Ub, k, 0.0, tmp, rc));
+    if (L.precision == 1)
+      BBT_TRY(dgemm(ctx, false, false, rc, k, m, 1.0, M + L.rpos[c], (long)rg, Rg, (long)m, 0.0, tmp, rc));
+    else
+      BBT_TRY(dgemm(ctx, false, true, rc, k, m, 1.0, M + L.rpos[c], (long)rg, Ub, k, 0.0, tmp, rc));
     BBT_TRY(block_shift_mask(ctx, (size_t)k, (size_t)rc, MASK_PASSES, tmp, false, false, cfg->private_seeds[c]));
     const long n = (long)L.n[c];
     if (L.qr[c] && L.precision == 1) {   // Q_c = Q_p W_c: FinalVT^T = Q_p (W_c tmp^T)

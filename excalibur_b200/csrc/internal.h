@@ -138,10 +138,12 @@ bbt_status block_shift_mask(bbt_ctx* ctx, size_t m, size_t n, size_t passes, dou
 
 // FP64 GEMM, column-major BLAS convention (dgemm.cu):
 //   C = alpha * op(A) * op(B) + beta * C,  op(A) M x K, op(B) K x N.
-// splits > 1 splits K; partial products are summed in a fixed order.
+// splits > 1 splits K; partial products are summed in a fixed order.  With
+// upper, only the tiles that touch the upper triangle of C are computed (the
+// rest of C is left undefined): for symmetric products.
 bbt_status dgemm(bbt_ctx* ctx, bool ta, bool tb, int M, int N, long K, double alpha,
                  const double* A, long lda, const double* B, long ldb, double beta, double* C,
-                 long ldc, int splits = 0);
+                 long ldc, int splits = 0, bool upper = false);
 // Scratch the automatic split-K of dgemm takes from the workspace.
 size_t dgemm_workspace_bytes(const bbt_ctx* ctx, int M, int N, long K);
 
@@ -201,6 +203,8 @@ bbt_status trsm_right_upper(bbt_ctx* ctx, long rows, int n, const double* R, lon
 bbt_status potrf_upper(bbt_ctx* ctx, int n, double* G, long ld, int* flag);
 bbt_status shift_diag(bbt_ctx* ctx, int n, double* G, long ld, double rel);
 bbt_status identity(bbt_ctx* ctx, int n, double* W, long ld);
+// Lower triangle of G (n x n column-major) <- upper triangle transposed.
+bbt_status symmetrize_upper(bbt_ctx* ctx, int n, double* G, long ld);
 // d (cols) <- the row signs of LAPACK's Householder R for the orthonormal
 // matrix whose top block is A (rows x cols, rows >= cols; overwritten).
 bbt_status householder_signs(bbt_ctx* ctx, int rows, int cols, double* A, long lda, double* d);

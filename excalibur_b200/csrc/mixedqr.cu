@@ -66,12 +66,14 @@ bbt_status mixed_local_qr(bbt_ctx* ctx, int m, long n, double* X, const void* S,
   // 1. Y^T (m x N row-major) = X S^T  ==  Y = S A (N x m column-major)
   BBT_TRY(sketch_bf16x3(ctx, m, n, X, n, N, S, spitch, Y));
   // 2. R_p = chol(Y^T Y + 1e-14 max diag)
-  BBT_TRY(dgemm(ctx, true, false, m, m, N, 1.0, Y, N, Y, N, 0.0, Gp, m));
+  BBT_TRY(dgemm(ctx, true, false, m, m, N, 1.0, Y, N, Y, N, 0.0, Gp, m, 0, true));
+  BBT_TRY(symmetrize_upper(ctx, m, Gp, m));
   BBT_TRY(shift_diag(ctx, m, Gp, m, 1e-14));
   BBT_TRY(potrf_upper(ctx, m, Gp, m, flag));
   // 3. Q_p = A R_p^{-1} (in place), G = Q_p^T Q_p, R_3 = chol(G), R = R_3 R_p
   BBT_TRY(trsm_right_upper(ctx, n, m, Gp, m, X, n));
-  BBT_TRY(dgemm(ctx, true, false, m, m, n, 1.0, X, n, X, n, 0.0, G, m));
+  BBT_TRY(dgemm(ctx, true, false, m, m, n, 1.0, X, n, X, n, 0.0, G, m, 0, true));
+  BBT_TRY(symmetrize_upper(ctx, m, G, m));
   BBT_TRY(potrf_upper(ctx, m, G, m, flag));
   BBT_TRY(dgemm(ctx, false, false, m, m, m, 1.0, G, m, Gp, m, 0.0, R, m));
   // 4. W = R_3^{-1}, so Q = Q_p W
