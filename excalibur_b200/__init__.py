@@ -185,6 +185,103 @@ class Context:
         self.sync()
         return rt
 
+    # -- learned bisection brackets (mlp.cu) ------------------------------------
+    def gebrd(self, A):
+        """Householder bidiagonalisation of a dense n x n matrix held
+        column-major (a CUDA tensor holding X^T; overwritten).  Returns (d, e)."""
+        n = A.shape[0]
+        d, e = self._empty(n), self._empty(n)
+        self._pre()
+        self._check(self.L.bbt_gebrd(self.h, n, self._p(A), self._p(d), self._p(e)), "gebrd")
+        self.sync()
+        return d, e[: n - 1]
+
+    def bidiagonal_singular_values(self, alpha, beta, brackets=None, top_k=None):
+        """The reference's bisection on [0, ||a||^2 + ||b||^2] with tol 1e-20
+        (bbtsvd.cpp:936-940); with brackets (count x 2, descending), the
+        learned-bracket variant.  Returns sigma (or (sigma, stats))."""
+        a, b = self._dev(alpha), self._dev(beta if len(beta) else np.zeros(1))
+        n = a.numel()
+        bound = float((a * a).sum() + ((b[: n - 1] * b[: n - 1]).sum() if n > 1 else 0.0))
+        top_k = n if top_k is None else top_k
+        if brackets is None:
+            return self.bisection_singular_values(a, b, 0.0, bound, 1e-20, top_k)
+        s = self._empty(max(n, 1))
+        cnt = C.c_int(0)
+        st = (C.c_longlong * 4)()
+        br = self._dev(brackets)
+        self._pre()
+        self._check(self.L.bbt_bisection_bracketed(self.h, n, self._p(a), self._p(b), 0.0, bound, 1e-20, top_k,
+                                                   self._p(br), self._p(s), C.byref(cnt), st), "bisection_bracketed")
+        self.sync()
+        return s[: cnt.value], {"sturm_evals": st[0], "rounds": st[1], "jumps": st[2], "verify_evals": st[3]}
+
+    def bisection_stats(self):
+        st = (C.c_longlong * 4)()
+        self._check(self.L.bbt_bisection_stats(self.h, st), "bisection_stats")
+        return {"sturm_evals": st[0], "rounds": st[1], "jumps": st[2], "verify_evals": st[3]}
+
+    def mlp_param_count(self):
+        return int(self.L.bbt_mlp_param_count())
+
+    def mlp_features(self, alpha, beta, count=None):
+        a, b = self._dev(alpha), self._dev(beta if len(beta) else np.zeros(1))
+        k = a.numel()
+        count = k if count is None else count
+        X = self._empty(count, 10)
+        self._pre()
+        self._check(self.L.bbt_mlp_features(self.h, k, self._p(a), self._p(b), count, self._p(X)), "mlp_features")
+        self.sync()
+        return X
+
+    def mlp_forward(self, X, theta):
+        X, theta = self._dev(X), self._dev(theta)
+        out = self._empty(X.shape[0], 2)
+        self._pre()
+        self._check(self.L.bbt_mlp_forward(self.h, X.shape[0], self._p(X), self._p(theta), self._p(out)),
+                    "mlp_forward")
+        self.sync()
+        return out
+
+    def mlp_grad(self, X, y, theta, grad=None, loss=None):
+        """Mean Gaussian-NLL loss and its gradient over the batch (device)."""
+        X, y, theta = self._dev(X), self._dev(y), self._dev(theta)
+        grad = self._empty(theta.numel()) if grad is None else grad
+        loss = self._empty(1) if loss is None else loss
+        self._pre()
+        self._check(self.L.bbt_mlp_grad(self.h, X.shape[0], self._p(X), self._p(y), self._p(theta), self._p(grad),
+                                        self._p(loss)), "mlp_grad")
+        self.sync()
+        return grad, loss
+
+    def mlp_adam(self, theta, grad, m, v, lr, step):
+        self._pre()
+        self._check(self.L.bbt_mlp_adam(self.h, self._p(theta), self._p(grad), self._p(m), self._p(v), lr, step),
+                    "mlp_adam")
+        self.sync()
+
+    def mlp_brackets(self, alpha, beta, theta, count=None, z=3.0):
+        a, b = self._dev(alpha), self._dev(beta if len(beta) else np.zeros(1))
+        k = a.numel()
+        count = k if count is None else count
+        theta = self._dev(theta)
+        br = self._empty(count, 2)
+        self._pre()
+        self._check(self.L.bbt_mlp_brackets(self.h, k, self._p(a), self._p(b), count, self._p(theta), z,
+                                            self._p(br)), "mlp_brackets")
+        self.sync()
+        return br
+
+    def set_bracket_model(self, theta=None, z=3.0):
+        """Use the learned brackets inside every bisection of this context
+        (theta: numpy parameters; None switches them off)."""
+        if theta is None:
+            self._check(self.L.bbt_set_bracket_model(self.h, None, z), "set_bracket_model")
+            return
+        th = np.ascontiguousarray(theta, dtype=np.float64)
+        assert th.size == self.mlp_param_count()
+        self._check(self.L.bbt_set_bracket_model(self.h, th.ctypes.data_as(C.c_void_p), z), "set_bracket_model")
+
     def rademacher(self, N, n, seed):
         """S (N x n, +-1 in bf16; returned as an int16 tensor of bf16 bit
         patterns, row pitch n rounded up to 8)."""

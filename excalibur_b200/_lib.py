@@ -22,6 +22,8 @@ EXPORTS = (
     "bbt_local_qr", "bbt_fedsvd_run", "bbt_fedsvd_run_host", "bbt_fedsvd_stage_ms",
     "bbt_dgemm", "bbt_profile", "bbt_profile_get", "bbt_twisted_vectors_noalloc",
     "bbt_svd_dense", "bbt_fedsvd_tune", "bbt_rademacher", "bbt_sketch_bf16x3", "bbt_mixed_local_qr",
+    "bbt_mlp_param_count", "bbt_mlp_features", "bbt_mlp_forward", "bbt_mlp_grad", "bbt_mlp_adam",
+    "bbt_mlp_brackets", "bbt_bisection_bracketed", "bbt_set_bracket_model", "bbt_bisection_stats", "bbt_gebrd",
 )
 PROF_CLASSES = ("dgemm", "panel", "mask", "ralha", "bisect", "twisted", "sketch", "chol")
 
@@ -79,6 +81,16 @@ def load():
         "bbt_rademacher": ([vp, i, st, C.c_ulonglong, vp], i),
         "bbt_sketch_bf16x3": ([vp, i, st, vp, i, vp, vp], i),
         "bbt_mixed_local_qr": ([vp, st, st, vp, vp, vp], i),
+        "bbt_mlp_param_count": ([], i),
+        "bbt_mlp_features": ([vp, i, vp, vp, i, vp], i),
+        "bbt_mlp_forward": ([vp, i, vp, vp, vp], i),
+        "bbt_mlp_grad": ([vp, i, vp, vp, vp, vp, vp], i),
+        "bbt_mlp_adam": ([vp, vp, vp, vp, vp, d, i], i),
+        "bbt_mlp_brackets": ([vp, i, vp, vp, i, vp, d, vp], i),
+        "bbt_bisection_bracketed": ([vp, i, vp, vp, d, d, d, i, vp, vp, C.POINTER(i), C.POINTER(C.c_longlong)], i),
+        "bbt_set_bracket_model": ([vp, vp, d], i),
+        "bbt_bisection_stats": ([vp, C.POINTER(C.c_longlong)], i),
+        "bbt_gebrd": ([vp, i, vp, vp, vp], i),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

@@ -111,6 +111,7 @@ bbt_status bbt_destroy(bbt_ctx* ctx) {
   if (ctx->ws.base) cudaFree(ctx->ws.base);
   if (ctx->d_flag) cudaFree(ctx->d_flag);
   if (ctx->d_barrier) cudaFree(ctx->d_barrier);
+  if (ctx->bracket_theta) cudaFree(ctx->bracket_theta);
   if (ctx->own) cudaStreamDestroy(ctx->own);
   delete ctx;
   return BBT_OK;
@@ -150,6 +151,94 @@ bbt_status bbt_bisection(bbt_ctx* ctx, int n, const double* a, const double* b, 
     return fail(ctx, BBT_ERR_ARG, "bisection: bad arguments");
   BBT_TRY(ensure(ctx, (size_t)(n + 2) * 48 * 18 + (1 << 20)));
   return bisect(ctx, n, a, b, lo, hi, tol, top_k, sigma, count);
+}
+
+bbt_status bbt_bisection_bracketed(bbt_ctx* ctx, int n, const double* a, const double* b, double lo, double hi,
+                                   double tol, int top_k, const double* brackets, double* sigma, int* count,
+                                   long long* stats) {
+  if (!ctx) return BBT_ERR_ARG;
+  if (!count) return fail(ctx, BBT_ERR_ARG, "bisection: count is NULL");
+  *count = 0;
+  if (n < 1 || bad(a) || (n > 1 && bad(b)) || (top_k > 0 && (bad(sigma) || bad(brackets))))
+    return fail(ctx, BBT_ERR_ARG, "bisection: bad arguments");
+  const int tk = top_k < n ? top_k : n;
+  BBT_TRY(ensure(ctx, (size_t)(n + 2) * 48 * 18 + (size_t)tk * 64 + (1 << 20)));
+  long st[4];
+  BBT_TRY(bisect(ctx, n, a, b, lo, hi, tol, top_k, sigma, count, brackets, st));
+  if (stats) for (int i = 0; i < 4; ++i) stats[i] = st[i];
+  return BBT_OK;
+}
+
+int bbt_mlp_param_count(void) { return MLP_PARAMS; }
+
+bbt_status bbt_mlp_features(bbt_ctx* ctx, int k, const double* a, const double* b, int count, double* X) {
+  if (!ctx) return BBT_ERR_ARG;
+  if (k < 1 || count < 0 || count > k || bad(a) || (k > 1 && bad(b)) || (count > 0 && bad(X)))
+    return fail(ctx, BBT_ERR_ARG, "mlp_features: bad arguments");
+  BBT_TRY(ensure(ctx, 1 << 20));
+  double* s6 = ctx->ws.take<double>(8);
+  BBT_TRY(mlp_summary(ctx, k, a, b, s6));
+  return count > 0 ? mlp_features(ctx, k, count, s6, X) : BBT_OK;
+}
+
+bbt_status bbt_mlp_forward(bbt_ctx* ctx, int B, const double* X, const double* theta, double* out) {
+  if (!ctx) return BBT_ERR_ARG;
+  if (B < 0 || (B > 0 && (bad(X) || bad(theta) || bad(out)))) return fail(ctx, BBT_ERR_ARG, "mlp_forward: bad arguments");
+  return mlp_forward(ctx, B, X, theta, out);
+}
+
+bbt_status bbt_mlp_grad(bbt_ctx* ctx, int B, const double* X, const double* y, const double* theta, double* grad,
+                        double* loss) {
+  if (!ctx) return BBT_ERR_ARG;
+  if (B < 1 || bad(X) || bad(y) || bad(theta) || bad(grad) || bad(loss))
+    return fail(ctx, BBT_ERR_ARG, "mlp_grad: bad arguments");
+  BBT_TRY(ensure(ctx, ((size_t)MLP_PARAMS + 2) * B * 8 + (1 << 20)));
+  return mlp_grad(ctx, B, X, y, theta, grad, loss);
+}
+
+bbt_status bbt_mlp_adam(bbt_ctx* ctx, double* theta, const double* grad, double* m, double* v, double lr, int step) {
+  if (!ctx) return BBT_ERR_ARG;
+  if (bad(theta) || bad(grad) || bad(m) || bad(v) || step < 1) return fail(ctx, BBT_ERR_ARG, "mlp_adam: bad arguments");
+  return mlp_adam(ctx, theta, grad, m, v, lr, step);
+}
+
+bbt_status bbt_mlp_brackets(bbt_ctx* ctx, int k, const double* a, const double* b, int count, const double* theta,
+                            double z, double* br) {
+  if (!ctx) return BBT_ERR_ARG;
+  if (k < 1 || count < 1 || count > k || bad(a) || (k > 1 && bad(b)) || bad(theta) || bad(br))
+    return fail(ctx, BBT_ERR_ARG, "mlp_brackets: bad arguments");
+  BBT_TRY(ensure(ctx, (size_t)count * 8 * 14 + (1 << 20)));
+  return mlp_brackets(ctx, k, count, a, b, theta, z, br);
+}
+
+bbt_status bbt_set_bracket_model(bbt_ctx* ctx, const double* theta, double z) {
+  if (!ctx) return BBT_ERR_ARG;
+  BBT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (!theta) {
+    if (ctx->bracket_theta) cudaFree(ctx->bracket_theta);
+    ctx->bracket_theta = nullptr;
+    return BBT_OK;
+  }
+  if (!(z > 0.0)) return fail(ctx, BBT_ERR_ARG, "set_bracket_model: z must be positive");
+  if (!ctx->bracket_theta) BBT_CUDA(ctx, cudaMalloc(&ctx->bracket_theta, MLP_PARAMS * sizeof(double)));
+  BBT_CUDA(ctx, cudaMemcpy(ctx->bracket_theta, theta, MLP_PARAMS * sizeof(double), cudaMemcpyHostToDevice));
+  ctx->bracket_z = z;
+  return BBT_OK;
+}
+
+bbt_status bbt_bisection_stats(bbt_ctx* ctx, long long* stats) {
+  if (!ctx || !stats) return BBT_ERR_ARG;
+  for (int i = 0; i < 4; ++i) stats[i] = ctx->bisect_stats[i];
+  return BBT_OK;
+}
+
+bbt_status bbt_gebrd(bbt_ctx* ctx, int n, double* A, double* d, double* e) {
+  if (!ctx) return BBT_ERR_ARG;
+  if (n < 2 || bad(A) || bad(d) || bad(e)) return fail(ctx, BBT_ERR_ARG, "gebrd: bad arguments");
+  BBT_TRY(ensure(ctx, (size_t)n * 4 * 8 + (1 << 20)));
+  double* tq = ctx->ws.take<double>(n);
+  double* tp = ctx->ws.take<double>(n);
+  return gebrd(ctx, n, A, d, e, tq, tp);
 }
 
 bbt_status bbt_twisted_vectors(bbt_ctx* ctx, int n, int cnt, const double* sigma, const double* a,

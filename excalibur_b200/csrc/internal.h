@@ -62,6 +62,11 @@ struct bbt_ctx {
   uint64_t qr_graph_nodes = 0;
   int tuned_streams = 0, tuned_nb = 0;   // 0: not tuned
   std::vector<size_t> tuned_key;
+  // learned bisection brackets: MLP parameters (device copy, owned) and the
+  // half-width multiplier; stats of the last bisection that used them
+  double* bracket_theta = nullptr;
+  double bracket_z = 3.0;
+  long bisect_stats[4] = {0, 0, 0, 0};
 };
 
 namespace bbt {
@@ -117,8 +122,13 @@ struct ProfScope {
 // Sturm / bisection / twisted (sturm.cu, twisted.cu)
 bbt_status sturm_counts(bbt_ctx* ctx, int n, const double* a, const double* b, const double* mu,
                         int nmu, int* counts);
+// brackets (optional): [lo, hi] per j-th largest value (j < min(top_k, k)),
+// snapped to the reference's tree, verified by Sturm counts, used to skip
+// levels; stats (optional, 4): Sturm evaluations (verification included),
+// rounds, jumps taken, Sturm evaluations spent on verification.
 bbt_status bisect(bbt_ctx* ctx, int n, const double* a, const double* b, double lo, double hi,
-                  double tol, int top_k, double* sigma, int* count);
+                  double tol, int top_k, double* sigma, int* count, const double* brackets = nullptr,
+                  long* stats = nullptr);
 bbt_status twisted(bbt_ctx* ctx, int n, int cnt, const double* sigma, const double* a,
                    const double* b, double* U, int ldu, double* V, bool sign_fix);
 bbt_status bidiag_svd(bbt_ctx* ctx, int k, const double* a, const double* b, double* U, double* V,
@@ -221,6 +231,19 @@ bbt_status mixed_local_qr(bbt_ctx* ctx, int m, long n, double* X, const void* S,
 // Clear / read (with a stream sync) the sketch and Cholesky flags.
 bbt_status clear_tc_flags(bbt_ctx* ctx);
 bbt_status check_tc_flags(bbt_ctx* ctx, const char* what);
+
+// Learned brackets (mlp.cu).  MLP_PARAMS doubles of parameters.
+enum { MLP_FEATURES = 10, MLP_HIDDEN = 32,
+       MLP_PARAMS = MLP_HIDDEN * MLP_FEATURES + MLP_HIDDEN + MLP_HIDDEN * MLP_HIDDEN + MLP_HIDDEN +
+                    2 * MLP_HIDDEN + 2 };
+bbt_status mlp_summary(bbt_ctx* ctx, int k, const double* a, const double* b, double* s6);
+bbt_status mlp_features(bbt_ctx* ctx, int k, int count, const double* s6, double* X);
+bbt_status mlp_forward(bbt_ctx* ctx, int B, const double* X, const double* theta, double* out);
+bbt_status mlp_grad(bbt_ctx* ctx, int B, const double* X, const double* y, const double* theta, double* grad,
+                    double* loss);
+bbt_status mlp_adam(bbt_ctx* ctx, double* theta, const double* grad, double* m, double* v, double lr, int t);
+bbt_status mlp_brackets(bbt_ctx* ctx, int k, int count, const double* a, const double* b, const double* theta,
+                        double z, double* br);
 
 // Whole pipeline (fedsvd.cu)
 bbt_status fedsvd(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* blocks, double* sigma,

@@ -18,6 +18,8 @@
 // reference's build, so counts and singular values match it bit for bit.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "internal.h"
 
 namespace bbt {
@@ -197,6 +199,59 @@ __global__ void root_kernel(double lo, double hi, const int* __restrict__ c, Nod
 
 int smem_bytes(int n) { return n <= SMEM_PAIRS_MAX ? n * (int)sizeof(double2) : 0; }
 
+// ---- learned brackets (proposed by the MLP of mlp.cu) ----------------------
+// Each bracket [L, U] of the j-th largest value is snapped to the deepest node
+// of the reference's tree that contains it: descend from the root by the same
+// midpoint arithmetic as resolve_kernel, stopping at a terminal node or where
+// the bracket straddles the midpoint.  Entry t of the table belongs to the
+// value of ascending rank rbase + t, i.e. j = chi_root - 1 - (rbase + t);
+// pad = 1 marks a candidate, 0 one that can no longer help, -1 one rejected.
+__global__ void snap_kernel(int count, const double* __restrict__ br, double rlo, double rhi, double tol, int cb,
+                            int rbase, Node* __restrict__ table) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= count) return;
+  const double L = br[2 * j], U = br[2 * j + 1];
+  double lo = rlo, hi = rhi;
+  for (int d = 0; d < 4096; ++d) {
+    const double mid = midpoint(lo, hi);
+    if (__dsub_rn(hi, lo) <= tol || mid == lo || mid == hi) break;
+    if (U < mid) hi = mid;
+    else if (L >= mid) lo = mid;
+    else break;
+  }
+  table[(cb - 1 - j) - rbase] = {lo, hi, 0, 0, 0, (L <= U) ? 1 : 0};
+}
+
+// A live interval holding one value and strictly containing that value's
+// snapped node is checked against that node by two exact Sturm counts (lazily: only
+// when such a jump is possible).  With the same count range, every level in
+// between holds exactly the same values, so the reference's walk through
+// them ends in that node: the interval becomes the node.  Otherwise the
+// entry is rejected and plain bisection goes on.
+__global__ void jump_kernel(int n, const double2* __restrict__ q, Node* __restrict__ nodes, int N,
+                            Node* __restrict__ table, int tcount, int rbase, int* __restrict__ stat) {
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= N) return;
+  const Node nd = nodes[u];
+  if (nd.done || nd.chi - nd.clo != 1) return;   // single-value intervals only
+  const int t = nd.clo - rbase;
+  if (t < 0 || t >= tcount) return;
+  const Node tb = table[t];
+  if (tb.pad != 1) return;
+  if (!(tb.lo >= nd.lo && tb.hi <= nd.hi)) return;
+  if (!(__dsub_rn(tb.hi, tb.lo) < __dsub_rn(nd.hi, nd.lo))) {   // not deeper (yet): try again next round
+    return;
+  }
+  const int clo = sturm(n, q, tb.lo), chi = sturm(n, q, tb.hi);
+  atomicAdd(stat, 2);
+  if (clo == nd.clo && chi == nd.chi) {
+    nodes[u].lo = tb.lo;
+    nodes[u].hi = tb.hi;
+    atomicAdd(stat + 1, 1);
+  }
+  table[t].pad = -1;   // used or rejected: never tried again
+}
+
 }  // namespace
 
 bbt_status sturm_counts(bbt_ctx* ctx, int n, const double* a, const double* b, const double* mu,
@@ -220,8 +275,9 @@ bbt_status sturm_counts(bbt_ctx* ctx, int n, const double* a, const double* b, c
 }
 
 bbt_status bisect(bbt_ctx* ctx, int n, const double* a, const double* b, double lo, double hi,
-                  double tol, int top_k, double* sigma, int* count) {
+                  double tol, int top_k, double* sigma, int* count, const double* brackets, long* stats_out) {
   *count = 0;
+  if (stats_out) for (int i = 0; i < 4; ++i) stats_out[i] = 0;
   if (n < 1) return fail(ctx, BBT_ERR_ARG, "bisection: n=%d", n);
   if (top_k <= 0) return BBT_OK;
   size_t mark = ctx->ws.top;
@@ -233,7 +289,7 @@ bbt_status bisect(bbt_ctx* ctx, int n, const double* a, const double* b, double 
   Node* cand = ctx->ws.take<Node>((size_t)cap * FAN);
   int* nout = ctx->ws.take<int>(cap);
   int* cnt = ctx->ws.take<int>((size_t)cap * NPTS);
-  int* stats = ctx->ws.take<int>(2);
+  int* stats = ctx->ws.take<int>(4);
   if (!stats) return fail(ctx, BBT_ERR_NOMEM, "bisection: workspace");
   squares_kernel<<<(n + 255) / 256, 256, 0, ctx->stream>>>(n, a, b, q);
   BBT_LAUNCHED(ctx);
@@ -255,8 +311,29 @@ bbt_status bisect(bbt_ctx* ctx, int n, const double* a, const double* b, double 
   int N = 1, live = 1;
   const int limit = top_k < cap ? top_k : cap;
   ProfScope prof(ctx, BBT_PROF_BISECT, 0.0);
+  long evals = 2;
+  // learned brackets: snapped to the tree, verified lazily in jump_kernel
+  Node* table = nullptr;
+  int tcount = 0, rbase = 0;
+  int* jstat = stats + 2;   // [Sturm evaluations of verification, jumps]
+  BBT_CUDA(ctx, cudaMemsetAsync(stats, 0, 4 * sizeof(int), ctx->stream));
+  if (brackets) {
+    tcount = std::min(hc[1] - hc[0], limit);
+    rbase = hc[1] - tcount;
+    if (tcount > 0) {
+      table = ctx->ws.take<Node>(tcount);
+      if (!table) return fail(ctx, BBT_ERR_NOMEM, "bisection: bracket table");
+      snap_kernel<<<(tcount + 127) / 128, 128, 0, ctx->stream>>>(tcount, brackets, lo, hi, tol, hc[1], rbase, table);
+      BBT_LAUNCHED(ctx);
+    }
+  }
   for (int round = 0; live > 0; ++round) {
     if (round > 4096) return fail(ctx, BBT_ERR_TIMEOUT, "bisection: no convergence");
+    if (table) {
+      jump_kernel<<<(N + 127) / 128, 128, 0, ctx->stream>>>(n, q, nodes, N, table, tcount, rbase, jstat);
+      BBT_LAUNCHED(ctx);
+    }
+    evals += (long)live * NPTS;
     const long work = (long)N * NPTS;
     int threads = 128;
     long blocks = (work + threads - 1) / threads;
@@ -272,10 +349,19 @@ bbt_status bisect(bbt_ctx* ctx, int n, const double* a, const double* b, double 
     BBT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     N = hs[0];
     live = hs[1];
+    if (stats_out) stats_out[1] = round + 1;
   }
   if (N > 0) {
     emit_kernel<<<(N + 255) / 256, 256, 0, ctx->stream>>>(nodes, N, sigma);
     BBT_LAUNCHED(ctx);
+  }
+  if (stats_out) {   // [Sturm evaluations, rounds, jumps taken, verification evaluations]
+    int hs[4];
+    BBT_CUDA(ctx, cudaMemcpyAsync(hs, stats, sizeof(hs), cudaMemcpyDeviceToHost, ctx->stream));
+    BBT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    stats_out[0] = evals + hs[2];
+    stats_out[2] = hs[3];
+    stats_out[3] = hs[2];
   }
   *count = N;
   ctx->ws.top = mark;

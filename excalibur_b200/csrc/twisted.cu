@@ -325,7 +325,13 @@ bbt_status bidiag_svd(bbt_ctx* ctx, int k, const double* a, const double* b, dou
   BBT_CUDA(ctx, cudaMemcpyAsync(&hb, bound, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   BBT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   int cnt = 0;
-  BBT_TRY(bisect(ctx, k, a, b, 0.0, hb, 1e-20, top_k, sigma, &cnt));
+  double* br = nullptr;
+  if (ctx->bracket_theta) {   // learned brackets (verified inside bisect; never change the result)
+    br = ctx->ws.take<double>(2 * (size_t)top_k);
+    if (!br) return fail(ctx, BBT_ERR_NOMEM, "bidiagonal svd: bracket workspace");
+    BBT_TRY(mlp_brackets(ctx, k, top_k, a, b, ctx->bracket_theta, ctx->bracket_z, br));
+  }
+  BBT_TRY(bisect(ctx, k, a, b, 0.0, hb, 1e-20, top_k, sigma, &cnt, br, ctx->bisect_stats));
   if (cnt < top_k) {
     ctx->ws.top = mark;
     return fail(ctx, BBT_ERR_COUNT, "bisection found %d singular values, %d requested", cnt, top_k);

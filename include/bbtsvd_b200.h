@@ -140,6 +140,44 @@ bbt_status bbt_dgemm(bbt_ctx* ctx, int transa, int transb, int M, int N, long K,
                      const double* d_A, long lda, const double* d_B, long ldb, double beta,
                      double* d_C, long ldc);
 
+/* ---- learned bisection brackets -------------------------------------------
+ * A small MLP (parameters: bbt_mlp_param_count() doubles) maps per-bidiagonal
+ * features (norms of a and b, their maxima, min |a|, dimension) and the index
+ * fraction of the j-th largest singular value to (mu, ell): a centre log2
+ * (sigma_j / g), g = max_i(|a_i| + max(|b_{i-1}|, |b_i|)), and a log spread.
+ * Training runs on the device through these entries (features, forward,
+ * per-batch gradient of the Gaussian negative log-likelihood, Adam).
+ * bbt_mlp_brackets: br[2j], br[2j+1] = g 2^(mu -/+ z e^ell) for j < count.
+ * bbt_bisection_bracketed: bbt_bisection with such brackets.  Each bracket
+ * is snapped to a node of the reference's bisection tree; once the bisection
+ * has isolated that value in an interval strictly containing the node, two
+ * exact Sturm counts verify the node and the interval jumps to it (skipping
+ * the levels in between); a node that fails is ignored.  The result is
+ * bit-identical to bbt_bisection; stats (may be NULL) = {Sturm evaluations
+ * (verification included), rounds, jumps taken, verification evaluations}.
+ * bbt_set_bracket_model: use these parameters (host array, copied; NULL
+ * turns the model off) inside bbt_bidiagonal_svd, bbt_fedsvd_run and
+ * bbt_svd_dense; bbt_bisection_stats reports the stats of the last
+ * bisection run by those.
+ * bbt_gebrd: Householder bidiagonalisation (diagonal d, superdiagonal e) of a
+ * dense column-major n x n matrix (overwritten), to generate training data.
+ * Additive: the reference's bisection has no learned part (bbtsvd.cpp:19-52). */
+int bbt_mlp_param_count(void);
+bbt_status bbt_mlp_features(bbt_ctx* ctx, int k, const double* d_a, const double* d_b, int count, double* d_X);
+bbt_status bbt_mlp_forward(bbt_ctx* ctx, int batch, const double* d_X, const double* d_theta, double* d_out);
+bbt_status bbt_mlp_grad(bbt_ctx* ctx, int batch, const double* d_X, const double* d_y, const double* d_theta,
+                        double* d_grad, double* d_loss);
+bbt_status bbt_mlp_adam(bbt_ctx* ctx, double* d_theta, const double* d_grad, double* d_m, double* d_v, double lr,
+                        int step);
+bbt_status bbt_mlp_brackets(bbt_ctx* ctx, int k, const double* d_a, const double* d_b, int count,
+                            const double* d_theta, double z, double* d_brackets);
+bbt_status bbt_bisection_bracketed(bbt_ctx* ctx, int n, const double* d_alpha, const double* d_beta, double lo,
+                                   double hi, double tol, int top_k, const double* d_brackets, double* d_sigma,
+                                   int* count, long long* stats);
+bbt_status bbt_set_bracket_model(bbt_ctx* ctx, const double* theta, double z);
+bbt_status bbt_bisection_stats(bbt_ctx* ctx, long long* stats);
+bbt_status bbt_gebrd(bbt_ctx* ctx, int n, double* d_A, double* d_d, double* d_e);
+
 /* ---- split-precision sketch and mixed-precision local QR -----------------
  * bbt_rademacher: d_S (N x local_n bf16, row pitch round_up(local_n, 8)
  * elements) <- independent +-1 entries drawn from `seed`.
