@@ -392,6 +392,23 @@ class Context:
         self.sync()
         return C
 
+    def dgemm_ozaki(self, transa, transb, A, B, alpha=1.0, beta=0.0, C=None, upper=False):
+        """dgemm's contract (same tensor conventions) computed from exact int8
+        slices on the tensor cores (FP64-accurate)."""
+        M = A.shape[0] if transa else A.shape[1]
+        K = A.shape[1] if transa else A.shape[0]
+        N = B.shape[0] if not transb else B.shape[1]
+        K2 = B.shape[1] if not transb else B.shape[0]
+        assert K == K2, (K, K2)
+        if C is None:
+            C = self.torch.zeros(N, M, dtype=self.torch.float64, device=f"cuda:{self.device}")
+        self._pre()
+        self._check(self.L.bbt_dgemm_ozaki(self.h, int(transa), int(transb), M, N, K, alpha, self._p(A), A.shape[1],
+                                           self._p(B), B.shape[1], beta, self._p(C), C.shape[1], int(upper)),
+                    "dgemm_ozaki")
+        self.sync()
+        return C
+
     def profile(self, enable=True):
         self._check(self.L.bbt_profile(self.h, int(bool(enable))), "profile")
 

@@ -24,8 +24,9 @@ EXPORTS = (
     "bbt_svd_dense", "bbt_fedsvd_tune", "bbt_rademacher", "bbt_sketch_bf16x3", "bbt_mixed_local_qr",
     "bbt_mlp_param_count", "bbt_mlp_features", "bbt_mlp_forward", "bbt_mlp_grad", "bbt_mlp_adam",
     "bbt_mlp_brackets", "bbt_bisection_bracketed", "bbt_set_bracket_model", "bbt_bisection_stats", "bbt_gebrd",
+    "bbt_dgemm_ozaki",
 )
-PROF_CLASSES = ("dgemm", "panel", "mask", "ralha", "bisect", "twisted", "sketch", "chol")
+PROF_CLASSES = ("dgemm", "panel", "mask", "ralha", "bisect", "twisted", "sketch", "chol", "ozaki")
 
 
 class FedSVDConfig(C.Structure):
@@ -91,6 +92,7 @@ def load():
         "bbt_set_bracket_model": ([vp, vp, d], i),
         "bbt_bisection_stats": ([vp, C.POINTER(C.c_longlong)], i),
         "bbt_gebrd": ([vp, i, vp, vp, vp], i),
+        "bbt_dgemm_ozaki": ([vp, i, i, i, i, C.c_long, d, vp, C.c_long, vp, C.c_long, d, vp, C.c_long, i], i),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

@@ -363,6 +363,21 @@ bbt_status bbt_dgemm(bbt_ctx* ctx, int transa, int transb, int M, int N, long K,
   return dgemm(ctx, transa != 0, transb != 0, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
 }
 
+bbt_status bbt_dgemm_ozaki(bbt_ctx* ctx, int transa, int transb, int M, int N, long K, double alpha, const double* A,
+                           long lda, const double* B, long ldb, double beta, double* C, long ldc, int upper) {
+  if (!ctx) return BBT_ERR_ARG;
+  if (M < 1 || N < 1 || K < 1 || bad(A) || bad(B) || bad(C) || (upper && M != N))
+    return fail(ctx, BBT_ERR_ARG, "dgemm_ozaki: bad arguments");
+  const long am = transa ? K : M, bm = transb ? N : K;
+  if (lda < am || ldb < bm || ldc < M) return fail(ctx, BBT_ERR_ARG, "dgemm_ozaki: leading dimension too small");
+  BBT_TRY(ensure(ctx, oz_workspace_bytes(ctx, M, N, K, false) + (1 << 20)));
+  BBT_TRY(clear_tc_flags(ctx));
+  const long rsA = transa ? lda : 1, csA = transa ? 1 : lda;
+  const long rsB = transb ? 1 : ldb, csB = transb ? ldb : 1;
+  BBT_TRY(gemm_oz(ctx, M, N, K, alpha, A, rsA, csA, B, rsB, csB, beta, C, ldc, false, upper != 0));
+  return check_tc_flags(ctx, "dgemm_ozaki");
+}
+
 bbt_status bbt_rademacher(bbt_ctx* ctx, int N, size_t local_n, unsigned long long seed, void* d_S) {
   if (!ctx) return BBT_ERR_ARG;
   if (N < 1 || local_n < 1 || local_n > ((size_t)1 << 31) || bad(d_S))
@@ -401,7 +416,7 @@ bbt_status bbt_profile(bbt_ctx* ctx, int enable) {
   BBT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   for (auto& r : ctx->recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
   ctx->recs.clear();
-  for (int i = 0; i < 8; ++i) { ctx->prof_ms[i] = 0; ctx->prof_work[i] = 0; ctx->prof_n[i] = 0; }
+  for (int i = 0; i < BBT_PROF_CLASSES; ++i) { ctx->prof_ms[i] = 0; ctx->prof_work[i] = 0; ctx->prof_n[i] = 0; }
   ctx->prof = enable != 0;
   return BBT_OK;
 }

@@ -270,7 +270,8 @@ bbt_status apply_signs(bbt_ctx* ctx, int m, const double* d, double* R, double* 
   return BBT_OK;
 }
 
-bbt_status trsm_right_upper(bbt_ctx* ctx, long rows, int n, const double* R, long ldr, double* A, long lda) {
+bbt_status trsm_right_upper(bbt_ctx* ctx, long rows, int n, const double* R, long ldr, double* A, long lda,
+                            bool oz) {
   if (rows <= 0 || n <= 0) return BBT_OK;
   if (n <= TB) {
     const long blocks = (rows + 127) / 128;
@@ -283,10 +284,14 @@ bbt_status trsm_right_upper(bbt_ctx* ctx, long rows, int n, const double* R, lon
     return BBT_OK;
   }
   const int n1 = split_point(n), n2 = n - n1;
-  BBT_TRY(trsm_right_upper(ctx, rows, n1, R, ldr, A, lda));
-  BBT_TRY(dgemm(ctx, false, false, (int)rows, n2, n1, -1.0, A, lda, R + (long)n1 * ldr, ldr, 1.0, A + (long)n1 * lda,
-                lda));
-  return trsm_right_upper(ctx, rows, n2, R + n1 + (long)n1 * ldr, ldr, A + (long)n1 * lda, lda);
+  BBT_TRY(trsm_right_upper(ctx, rows, n1, R, ldr, A, lda, oz));
+  if (oz && oz_worthwhile((int)rows, n2, n1))   // A2 -= A1 R12 from exact int8 slices (ozaki.cu)
+    BBT_TRY(gemm_oz(ctx, (int)rows, n2, n1, -1.0, A, 1, lda, R + (long)n1 * ldr, ldr, 1, 1.0, A + (long)n1 * lda, lda,
+                    false, false));
+  else
+    BBT_TRY(dgemm(ctx, false, false, (int)rows, n2, n1, -1.0, A, lda, R + (long)n1 * ldr, ldr, 1.0,
+                  A + (long)n1 * lda, lda));
+  return trsm_right_upper(ctx, rows, n2, R + n1 + (long)n1 * ldr, ldr, A + (long)n1 * lda, lda, oz);
 }
 
 bbt_status potrf_upper(bbt_ctx* ctx, int n, double* G, long ld, int* flag) {

@@ -118,7 +118,11 @@ size_t scratch_bytes(const bbt_ctx* ctx, const Layout& L) {
   size_t s = 0;
   for (int c = 0; c < L.P; ++c)
     if (L.qr[c]) s = std::max(s, qr_scratch(ctx, L, (long)L.n[c], qp));
-  if (L.precision == 1) s = std::max(s, qr_scratch(ctx, L, (long)L.rg, qp));
+  if (L.precision == 1) {
+    s = std::max(s, qr_scratch(ctx, L, (long)L.rg, qp));
+    for (int c = 0; c < L.P; ++c)   // the V back-transform from int8 slices
+      if (L.qr[c]) s = std::max(s, oz_workspace_bytes(ctx, (int)L.n[c], (int)L.m, (long)L.m, false) + (8u << 20));
+  }
   s = std::max(s, qr_workspace_bytes((long)L.rg, (int)L.m, (int)L.m, qp));
   const size_t m = L.m;
   s = std::max(s, (7 * (m + 1) * m + 4 * m) * 8 + 4096);          // twisted
@@ -460,7 +464,10 @@ bbt_status fedsvd(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* X, 
     const long n = (long)L.n[c];
     if (L.qr[c] && L.precision == 1) {   // Q_c = Q_p W_c: FinalVT^T = Q_p (W_c tmp^T)
       BBT_TRY(dgemm(ctx, false, false, mi, k, m, 1.0, job.W[c], (long)m, tmp, rc, 0.0, Z, (long)m));
-      BBT_TRY(dgemm(ctx, false, false, (int)n, k, m, 1.0, X[c], n, Z, (long)m, 0.0, VT[c], n));
+      if (oz_worthwhile((int)n, k, (long)m))   // FinalVT^T (n x k) = Q_p Z from exact int8 slices; 6 slices
+        BBT_TRY(gemm_oz(ctx, (int)n, k, (long)m, 1.0, X[c], 1, n, Z, (long)m, 1, 0.0, VT[c], n, false, false, 6));
+      else
+        BBT_TRY(dgemm(ctx, false, false, (int)n, k, m, 1.0, X[c], n, Z, (long)m, 0.0, VT[c], n));
     } else if (L.qr[c]) {   // FinalVT^T (n x k col-major) = Q_c (n x m) tmp^T (m x k)
       BBT_TRY(dgemm(ctx, false, false, (int)n, k, m, 1.0, X[c], n, tmp, rc, 0.0, VT[c], n));
     } else {
@@ -471,6 +478,7 @@ bbt_status fedsvd(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* X, 
   }
   BBT_CUDA(ctx, cudaEventRecord(ev[6], ctx->stream));
   BBT_CUDA(ctx, cudaEventSynchronize(ev[6]));
+  if (L.precision == 1) BBT_TRY(check_tc_flags(ctx, "fedsvd: tensor-core back-transform"));
   for (int s = 0; s < 6; ++s) {
     float ms = 0;
     BBT_CUDA(ctx, cudaEventElapsedTime(&ms, ev[s], ev[s + 1]));

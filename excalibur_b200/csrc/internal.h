@@ -51,8 +51,8 @@ struct bbt_ctx {
   double stage_ms[8] = {0};
   bool prof = false;
   std::vector<bbt::ProfRec> recs;          // pending event pairs
-  double prof_ms[8] = {0}, prof_work[8] = {0};
-  uint64_t prof_n[8] = {0};
+  double prof_ms[16] = {0}, prof_work[16] = {0};
+  uint64_t prof_n[16] = {0};
   bool allow_coop = true;        // false in the concurrent sub-streams of the batched QR
   // batched local QR: side streams, the captured graph and the tuned schedule
   std::vector<cudaStream_t> side;
@@ -208,7 +208,9 @@ bbt_status sketch_bf16x3(bbt_ctx* ctx, int m, long n, const double* X, long ldx,
 
 // FP64 Cholesky / triangular solve (chol.cu), column-major.
 // A (rows x n) <- A R^{-1}, R upper n x n.
-bbt_status trsm_right_upper(bbt_ctx* ctx, long rows, int n, const double* R, long ldr, double* A, long lda);
+// oz: the updates of large row counts from exact int8 slices (ozaki.cu).
+bbt_status trsm_right_upper(bbt_ctx* ctx, long rows, int n, const double* R, long ldr, double* A, long lda,
+                            bool oz = false);
 // G = R^T R in place (R upper, zeros below); a non-positive pivot sets *flag.
 bbt_status potrf_upper(bbt_ctx* ctx, int n, double* G, long ld, int* flag);
 bbt_status shift_diag(bbt_ctx* ctx, int n, double* G, long ld, double rel);
@@ -220,6 +222,17 @@ bbt_status symmetrize_upper(bbt_ctx* ctx, int n, double* G, long ld);
 bbt_status householder_signs(bbt_ctx* ctx, int rows, int cols, double* A, long lda, double* d);
 // R (m x m column-major) <- D R, W (optional) <- W D.
 bbt_status apply_signs(bbt_ctx* ctx, int m, const double* d, double* R, double* W);
+
+// FP64-accurate GEMM from exact int8 slices on the tensor cores (ozaki.cu):
+// C (M x N column-major) = alpha A B^T + beta C, A(i,k) = A[i rsA + k csA],
+// B(j,k) = B[j rsB + k csB]; each operand needs a unit stride in i or k.
+// same: B is A (slices shared); upper: only tiles touching C's upper triangle;
+// S (4..8): slices per operand -- error ~2^-(7S) of the row/column scales.
+size_t oz_workspace_bytes(const bbt_ctx* ctx, int M, int N, long K, bool same);
+bool oz_worthwhile(int M, int N, long K);
+bbt_status gemm_oz(bbt_ctx* ctx, int M, int N, long K, double alpha, const double* A, long rsA, long csA,
+                   const double* B, long rsB, long csB, double beta, double* C, long ldc, bool same, bool upper,
+                   int S = 8);
 
 // Mixed-precision local QR (mixedqr.cu): X (row-major m x n = column-major
 // A = X^T, n x m) -> Q_p in place, R (m x m column-major upper), W = R_3^{-1}

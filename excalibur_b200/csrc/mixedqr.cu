@@ -49,6 +49,8 @@ size_t mixed_qr_workspace_bytes(const bbt_ctx* ctx, int m, long n) {
   size_t s = sketch_workspace_bytes(ctx, m, n, N);
   s = std::max(s, dgemm_workspace_bytes(ctx, m, m, n));
   s = std::max(s, dgemm_workspace_bytes(ctx, m, m, N));
+  s = std::max(s, oz_workspace_bytes(ctx, m, m, n, true));                   // Gram
+  s = std::max(s, oz_workspace_bytes(ctx, (int)n, m - (m / 2 + 31) / 32 * 32, (m / 2 + 31) / 32 * 32, false));
   return s + ((size_t)N * m + 3 * (size_t)m * m + m) * 8 + 8192;
 }
 
@@ -70,9 +72,13 @@ bbt_status mixed_local_qr(bbt_ctx* ctx, int m, long n, double* X, const void* S,
   BBT_TRY(symmetrize_upper(ctx, m, Gp, m));
   BBT_TRY(shift_diag(ctx, m, Gp, m, 1e-14));
   BBT_TRY(potrf_upper(ctx, m, Gp, m, flag));
-  // 3. Q_p = A R_p^{-1} (in place), G = Q_p^T Q_p, R_3 = chol(G), R = R_3 R_p
-  BBT_TRY(trsm_right_upper(ctx, n, m, Gp, m, X, n));
-  BBT_TRY(dgemm(ctx, true, false, m, m, n, 1.0, X, n, X, n, 0.0, G, m, 0, true));
+  // 3. Q_p = A R_p^{-1} (in place), G = Q_p^T Q_p, R_3 = chol(G), R = R_3 R_p; the large
+  //    products from exact int8 slices on the tensor cores (ozaki.cu), FP64-accurate
+  BBT_TRY(trsm_right_upper(ctx, n, m, Gp, m, X, n, true));
+  if (oz_worthwhile(m, m, n))   // 7 slices: the Gram's errors act on R multiplicatively (~2^-50 relative)
+    BBT_TRY(gemm_oz(ctx, m, m, n, 1.0, X, n, 1, X, n, 1, 0.0, G, m, true, true, 7));
+  else
+    BBT_TRY(dgemm(ctx, true, false, m, m, n, 1.0, X, n, X, n, 0.0, G, m, 0, true));
   BBT_TRY(symmetrize_upper(ctx, m, G, m));
   BBT_TRY(potrf_upper(ctx, m, G, m, flag));
   BBT_TRY(dgemm(ctx, false, false, m, m, m, 1.0, G, m, Gp, m, 0.0, R, m));

@@ -193,6 +193,16 @@ bbt_status bbt_gebrd(bbt_ctx* ctx, int n, double* d_A, double* d_d, double* d_e)
  * Additive: the reference has no split-precision path (its local QR is
  * client.cpp:417-445). */
 bbt_status bbt_rademacher(bbt_ctx* ctx, int N, size_t local_n, unsigned long long seed, void* d_S);
+/* bbt_dgemm_ozaki: bbt_dgemm's contract (column-major, op = 'N'/'T') computed
+ * from exact int8 slices on the tensor cores (tcgen05 kind::i8): each row of
+ * op(A) and column of op(B) is scaled by a power of two and split into 8
+ * slices of at most 7 bits (rounded to nearest); the 36 slice pairs with
+ * p + q < 8 are accumulated exactly in int32 and combined in FP64, accurate
+ * to ~2^-56 of the row and column scales per term.  upper (M == N): only the tiles touching the upper
+ * triangle of C are computed, the rest of C is left as it was. */
+bbt_status bbt_dgemm_ozaki(bbt_ctx* ctx, int transa, int transb, int M, int N, long K, double alpha,
+                           const double* d_A, long lda, const double* d_B, long ldb, double beta,
+                           double* d_C, long ldc, int upper);
 bbt_status bbt_sketch_bf16x3(bbt_ctx* ctx, int m, size_t local_n, const double* d_x, int N,
                              const void* d_S, double* d_Y);
 bbt_status bbt_mixed_local_qr(bbt_ctx* ctx, size_t m, size_t local_n, double* d_x, double* d_r,
@@ -207,7 +217,7 @@ bbt_status bbt_mixed_local_qr(bbt_ctx* ctx, size_t m, size_t local_n, double* d_
  * switched on. */
 enum { BBT_PROF_DGEMM = 0, BBT_PROF_PANEL = 1, BBT_PROF_MASK = 2, BBT_PROF_RALHA = 3,
        BBT_PROF_BISECT = 4, BBT_PROF_TWISTED = 5, BBT_PROF_SKETCH = 6, BBT_PROF_CHOL = 7,
-       BBT_PROF_CLASSES = 8 };
+       BBT_PROF_OZAKI = 8, BBT_PROF_CLASSES = 9 };
 bbt_status bbt_profile(bbt_ctx* ctx, int enable);
 bbt_status bbt_profile_get(bbt_ctx* ctx, int cls, double* ms, uint64_t* launches, double* work);
 
