@@ -9,10 +9,11 @@
 // matrix, so the all-reduce is the in-device reduction of each dot product,
 // and a step is two grid-wide phases separated by bounded grid barriers:
 //
-//   B1 (column-partitioned): every CTA forms the reflector from g (same
-//      arithmetic in every CTA), writes its share of the Householder store,
-//      vt = sum_t h_t W[i+1+t] for its columns, the next row i+1 after the
-//      update, and row i of V (w_i - beta v_{i-1}) / alpha_i.
+//   B1 (column-partitioned, one CTA per SM, 8 columns x 32 row phases per
+//      pass): every CTA forms the reflector from g (same arithmetic in every
+//      CTA), writes its share of the Householder store, vt = sum_t h_t
+//      W[i+1+t] for its columns, the next row i+1 after the update, and row
+//      i of V (w_i - beta v_{i-1}) / alpha_i.
 //   B2 (row-partitioned, one warp per row): W[r] += (-tau vt) h_r for
 //      r > i, and, in the same pass, the next step's Gram row
 //      g'[r] = W[r] . W[i+1]; CTA 0 adds the next step's four dots.
@@ -30,6 +31,7 @@ namespace {
 
 constexpr int RT = 256;                 // threads per CTA
 constexpr int RW = RT / 32;             // warps per CTA
+constexpr int CB = 8;                   // columns per pass of B1
 
 struct RalhaArgs {
   int m;
@@ -82,7 +84,7 @@ __device__ void gram_rows(const RalhaArgs& A, int i, const double* piv, double* 
 __global__ void __launch_bounds__(RT) ralha_kernel(RalhaArgs A) {
   __shared__ double sh[RW];
   __shared__ double scal[6];   // beta_{i-1}, alpha_i, tau, scale, 1/alpha_i
-  __shared__ double red[RW][33];
+  __shared__ double red[RT / CB][CB + 1];
   const int m = A.m;
   const int tid = threadIdx.x;
   // ---- step 0 set-up: alpha_0, v_0 (CTA 0); Gram row of w_0 (all)
@@ -145,22 +147,23 @@ __global__ void __launch_bounds__(RT) ralha_kernel(RalhaArgs A) {
     for (int t = blockIdx.x * RT + tid; t < len; t += gridDim.x * RT)
       A.house[(long)(i + 1 + t) * m + (i + 1)] = (t == 0) ? 1.0 : g[t] * scl;
     {
-      // vt[c] = sum_t h_t W[i+1+t][c] with h_0 = 1, h_t = g[t]*scale
+      // vt[c] = sum_t h_t W[i+1+t][c] with h_0 = 1, h_t = g[t]*scale: CB columns per
+      // pass, RT / CB row phases (a warp reads 64-byte row segments of 4 rows)
       const int ncol = c1 - c0;
-      for (int cb = 0; cb < ncol; cb += 32) {
-        const int c = c0 + cb + (tid & 31);
+      for (int cb = 0; cb < ncol; cb += CB) {
+        const int c = c0 + cb + (tid % CB);
         double s = 0.0;
         if (c < c1)
-          for (int t = tid >> 5; t < len; t += RW) {
+          for (int t = tid / CB; t < len; t += RT / CB) {
             const double h = (t == 0) ? 1.0 : g[t] * scl;
             s += h * A.W[(long)(i + 1 + t) * m + c];
           }
-        red[tid >> 5][tid & 31] = s;
+        red[tid / CB][tid % CB] = s;
         __syncthreads();
-        if (tid < 32 && c0 + cb + tid < c1) {
+        if (tid < CB && c0 + cb + tid < c1) {
           const int cc = c0 + cb + tid;
           double v = 0.0;
-          for (int k = 0; k < RW; ++k) v += red[k][tid];
+          for (int k = 0; k < RT / CB; ++k) v += red[k][tid];
           A.vt[cc] = v;
           const double tvv = -ta * v;
           A.tv[cc] = tvv;
@@ -298,7 +301,8 @@ bbt_status ralha(bbt_ctx* ctx, int m, double* W, double* house, double* tau, dou
   int per_sm = 0;
   BBT_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ralha_kernel, RT, 0));
   if (per_sm < 1) return fail(ctx, BBT_ERR_CUDA, "ralha: kernel does not fit an SM");
-  int grid = (m + 31) / 32;                 // at least 32 columns per CTA in B1
+  int grid = (m + CB - 1) / CB;             // at least CB columns per CTA in B1, one CTA per SM
+  if (grid > ctx->num_sms * per_sm) grid = ctx->num_sms * per_sm;
   if (grid > ctx->num_sms) grid = ctx->num_sms;
   if (grid < 1) grid = 1;
   void* args[] = {&A};
