@@ -112,6 +112,11 @@ bbt_status bbt_destroy(bbt_ctx* ctx) {
   if (ctx->d_flag) cudaFree(ctx->d_flag);
   if (ctx->d_barrier) cudaFree(ctx->d_barrier);
   if (ctx->bracket_theta) cudaFree(ctx->bracket_theta);
+  if (ctx->io_ws.base) cudaFree(ctx->io_ws.base);
+  if (ctx->copy_in) cudaStreamDestroy(ctx->copy_in);
+  if (ctx->copy_out) cudaStreamDestroy(ctx->copy_out);
+  for (auto e : ctx->in_ready) cudaEventDestroy(e);
+  for (auto e : ctx->vt_done) cudaEventDestroy(e);
   if (ctx->own) cudaStreamDestroy(ctx->own);
   delete ctx;
   return BBT_OK;
@@ -313,41 +318,55 @@ bbt_status bbt_fedsvd_run_host(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, const
   if ((want_u && !hU) || (want_v && !hVT)) return fail(ctx, BBT_ERR_ARG, "fedsvd_host: NULL output");
   const int P = cfg->participants;
   const size_t m = cfg->m;
-  std::vector<double*> dX(P, nullptr), dVT(P, nullptr);
-  double *ds = nullptr, *dU = nullptr;
-  bbt_status st = BBT_OK;
-  auto cleanup = [&]() {
-    for (auto p : dX) if (p) cudaFree(p);
-    for (auto p : dVT) if (p) cudaFree(p);
-    if (ds) cudaFree(ds);
-    if (dU) cudaFree(dU);
-  };
+  // staging in a grow-only arena kept by the context (no allocation per call)
+  size_t need = m * sizeof(double) + m * m * sizeof(double) + 4096;
+  for (int c = 0; c < P; ++c) need += (want_v ? 2 : 1) * (m * cfg->local_n[c] * sizeof(double) + 256);
+  if (ctx->io_ws.cap < need) BBT_CUDA(ctx, ctx->io_ws.reserve(need));
+  ctx->io_ws.reset();
+  std::vector<double*> dX(P), dVT(P, nullptr);
+  for (int c = 0; c < P; ++c) {
+    dX[c] = ctx->io_ws.take<double>(m * cfg->local_n[c]);
+    if (want_v) dVT[c] = ctx->io_ws.take<double>(m * cfg->local_n[c]);
+  }
+  double* ds = ctx->io_ws.take<double>(m);
+  double* dU = ctx->io_ws.take<double>(m * m);
+  if (!ctx->copy_in) BBT_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->copy_in, cudaStreamNonBlocking));
+  if (!ctx->copy_out) BBT_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->copy_out, cudaStreamNonBlocking));
+  while ((int)ctx->in_ready.size() < P) {
+    cudaEvent_t a, b;
+    BBT_CUDA(ctx, cudaEventCreateWithFlags(&a, cudaEventDisableTiming));
+    BBT_CUDA(ctx, cudaEventCreateWithFlags(&b, cudaEventDisableTiming));
+    ctx->in_ready.push_back(a);
+    ctx->vt_done.push_back(b);
+  }
+  // the copy streams start after all earlier work on the context's stream
+  BBT_CUDA(ctx, cudaEventRecord(ctx->vt_done[0], ctx->stream));
+  BBT_CUDA(ctx, cudaStreamWaitEvent(ctx->copy_in, ctx->vt_done[0], 0));
+  BBT_CUDA(ctx, cudaStreamWaitEvent(ctx->copy_out, ctx->vt_done[0], 0));
+  for (int c = 0; c < P; ++c) {   // participant by participant: the first QR starts after one block
+    BBT_CUDA(ctx, cudaMemcpyAsync(dX[c], hX[c], m * cfg->local_n[c] * sizeof(double), cudaMemcpyHostToDevice,
+                                  ctx->copy_in));
+    BBT_CUDA(ctx, cudaEventRecord(ctx->in_ready[c], ctx->copy_in));
+  }
+  ctx->vt_dst.assign(P, nullptr);
+  if (want_v)
+    for (int c = 0; c < P; ++c) ctx->vt_dst[c] = hVT[c];   // copied out by the pipeline as each is done
+  ctx->io_on = true;
+  bbt_status st = fedsvd(ctx, cfg, dX.data(), ds, dU, dVT.data(), k);
+  ctx->io_on = false;
   cudaError_t e = cudaSuccess;
-  for (int c = 0; c < P && e == cudaSuccess; ++c) {
-    const size_t bytes = m * cfg->local_n[c] * sizeof(double);
-    e = cudaMalloc(&dX[c], bytes);
-    if (e == cudaSuccess && want_v) e = cudaMalloc(&dVT[c], bytes);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(dX[c], hX[c], bytes, cudaMemcpyHostToDevice, ctx->stream);
-  }
-  if (e == cudaSuccess) e = cudaMalloc(&ds, m * sizeof(double));
-  if (e == cudaSuccess && want_u) e = cudaMalloc(&dU, m * m * sizeof(double));
-  if (e != cudaSuccess) {
-    cleanup();
-    return cuda_fail(ctx, e, "fedsvd_host: staging");
-  }
-  st = fedsvd(ctx, cfg, dX.data(), ds, dU, dVT.data(), k);
   if (st == BBT_OK) {
     const int kk = *k;
     e = cudaMemcpyAsync(hsigma, ds, kk * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess && want_u)
       e = cudaMemcpyAsync(hU, dU, m * kk * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
-    for (int c = 0; c < P && e == cudaSuccess && want_v; ++c)
-      e = cudaMemcpyAsync(hVT[c], dVT[c], (size_t)kk * cfg->local_n[c] * sizeof(double), cudaMemcpyDeviceToHost,
-                          ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) st = cuda_fail(ctx, e, "fedsvd_host: copy-out");
   }
-  cleanup();
+  // every copy issued on the copy streams has finished before the buffers may be reused
+  const cudaError_t e1 = cudaStreamSynchronize(ctx->copy_in), e2 = cudaStreamSynchronize(ctx->copy_out);
+  if (st == BBT_OK && e1 != cudaSuccess) st = cuda_fail(ctx, e1, "fedsvd_host: copy-in");
+  if (st == BBT_OK && e2 != cudaSuccess) st = cuda_fail(ctx, e2, "fedsvd_host: copy-out");
   return st;
 }
 

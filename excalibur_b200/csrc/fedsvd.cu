@@ -251,9 +251,14 @@ bbt_status local_qr_stage(bbt_ctx* ctx, const Layout& L, double* const* X, const
   const int mi = (int)L.m;
   if (streams <= 1) {
     for (int c = 0; c < L.P; ++c)
-      if (L.qr[c]) BBT_TRY(qr_one(ctx, mi, X[c], (long)L.n[c], c, job, qp));
+      if (L.qr[c]) {
+        if (ctx->io_on) BBT_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->in_ready[c], 0));
+        BBT_TRY(qr_one(ctx, mi, X[c], (long)L.n[c], c, job, qp));
+      }
     return BBT_OK;
   }
+  if (ctx->io_on)   // the batched schedule (and its graph) starts once every block has arrived
+    for (int c = 0; c < L.P; ++c) BBT_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->in_ready[c], 0));
   std::vector<size_t> key = {L.m, (size_t)job.compute_v, (size_t)streams, (size_t)qp.nb, (size_t)ctx->ws.base,
                              ctx->ws.cap, ctx->ws.top, (size_t)job.precision, (size_t)job.S};
   for (int c = 0; c < L.P; ++c) {
@@ -394,6 +399,8 @@ bbt_status fedsvd(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* X, 
     ctx->ws.top = mark;
   }
   if (L.precision == 1) BBT_TRY(check_tc_flags(ctx, "fedsvd: mixed-precision local QR"));
+  if (ctx->io_on)
+    for (int c = 0; c < P; ++c) BBT_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->in_ready[c], 0));
   BBT_CUDA(ctx, cudaEventRecord(ev[1], ctx->stream));
   // 2) masks (client.cpp:593-596)
   for (int c = 0; c < P; ++c) {
@@ -473,6 +480,12 @@ bbt_status fedsvd(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* X, 
     } else {
       BBT_CUDA(ctx, cudaMemcpyAsync(VT[c], tmp, (size_t)k * n * sizeof(double), cudaMemcpyDeviceToDevice,
                                     ctx->stream));
+    }
+    if (ctx->io_on && ctx->vt_dst[c]) {   // FinalVT_c leaves while the next participant is computed
+      BBT_CUDA(ctx, cudaEventRecord(ctx->vt_done[c], ctx->stream));
+      BBT_CUDA(ctx, cudaStreamWaitEvent(ctx->copy_out, ctx->vt_done[c], 0));
+      BBT_CUDA(ctx, cudaMemcpyAsync(ctx->vt_dst[c], VT[c], (size_t)k * n * sizeof(double), cudaMemcpyDeviceToHost,
+                                    ctx->copy_out));
     }
   }
   }

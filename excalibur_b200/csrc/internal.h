@@ -67,6 +67,14 @@ struct bbt_ctx {
   double* bracket_theta = nullptr;
   double bracket_z = 3.0;
   long bisect_stats[4] = {0, 0, 0, 0};
+  // host-buffer pipeline entry: staging arena, copy streams, and the events
+  // that let participant c's work start as soon as its block has arrived and
+  // FinalVT_c leave as soon as it is computed
+  bbt::Arena io_ws;
+  cudaStream_t copy_in = nullptr, copy_out = nullptr;
+  bool io_on = false;
+  std::vector<cudaEvent_t> in_ready, vt_done;
+  std::vector<double*> vt_dst;
 };
 
 namespace bbt {
