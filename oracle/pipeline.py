@@ -172,18 +172,119 @@ def leading_svd(a, b, k):
     return s, U, V
 
 
+def _bsvd(alpha, beta, top_k, svd_mode):
+    """lower -> upper, sigma count, the bidiagonal SVD and the sign convention
+    (client.cpp:947-995); shared by both branches."""
+    a, b, cs = lower_to_upper(alpha, beta)                        # :947-954
+    bound = np.linalg.norm(a) ** 2 + np.linalg.norm(b) ** 2       # :966-971
+    k = negative_count(a, b, bound) - negative_count(a, b, 0.0)
+    if top_k > 0:
+        k = min(k, top_k)
+    if svd_mode in (0, 4):
+        sigma, Ub, Vb = leading_svd(a, b, k)                      # :975-980 (dbdsdc)
+    else:
+        sigma, Ub, Vb = bidiagonal_svd(a, b, k)                   # :984
+    for i in range(k):                                            # :988-995
+        p = int(np.argmax(np.abs(Ub[:, i])))
+        if Ub[p, i] < 0:
+            Ub[:, i] = -Ub[:, i]
+            Vb[i] = -Vb[i]
+    return (a, b, cs), sigma, Ub, Vb, k
+
+
+def _rotate_house(Ub, cs, house, tau):
+    """U2 = H (G^T U_b): the Givens sweep undone, then the Ralha reflectors
+    (client.cpp:1127-1128, 1135 / 1176)."""
+    n = Ub.shape[0]
+    U2 = Ub.copy()
+    for i in range(n - 2, -1, -1):
+        c_, s_ = cs[i]
+        x, y = U2[i].copy(), U2[i + 1].copy()
+        U2[i] = c_ * x - s_ * y
+        U2[i + 1] = c_ * y + s_ * x
+    return apply_house(house, tau, U2)
+
+
+def run_tall(blocks_t, public_seed, private_seeds, top_k=-1, svd_mode=1, y=None, return_stages=False):
+    """The tall-and-skinny branch, m > global_n (client.cpp:543-568, 627-679,
+    805-814, 1002-1015, 1071-1105, 1119-1169).  The reference stores each
+    participant's block transposed here: blocks_t[c] is X_c^T, local_n x m
+    row-major (client.cpp:549, 1248).  Returns (sigma, FinalU k x m,
+    [FinalVT_c k x local_n]); with svd_mode 4 (linear regression, labels y
+    of length m) the third item is [w_c (local_n)] and FinalU is None."""
+    P = len(blocks_t)
+    m = blocks_t[0].shape[1]
+    local_n = [x.shape[0] for x in blocks_t]
+    global_n = sum(local_n)
+    if m <= global_n:
+        raise ValueError("run_tall needs m > global_n")
+    stages = {}
+    masked = []
+    for c in range(P):                                            # :548-551
+        x = np.ascontiguousarray(blocks_t[c], dtype=np.float64)
+        x = block_shift_mask(x, MASK_PASSES, True, True, private_seeds[c])
+        x = block_shift_mask(x, MASK_PASSES, True, False, public_seed)
+        masked.append(x)
+    Mt = np.concatenate(masked, axis=0)                           # global_n x m, repartition :627-659
+    part, pos = row_split(m, P)
+    npos = np.concatenate([[0], np.cumsum(local_n)])
+    slabs, uq = [], []
+    for c in range(P):
+        S = Mt[:, pos[c]:pos[c + 1]].copy()                       # global_n x m_part
+        if part[c] > global_n:                                    # :661-667
+            r, q = local_qr(S)                                    # QR of S^T: R^T, Q^T (global_n x m_part)
+            slabs.append(r)
+            uq.append(q)
+        else:
+            slabs.append(S)
+            uq.append(None)
+    alpha, beta, house, tau, Vr = ralha(slabs)                    # bidiagonal_m = global_n, :805-910
+    stages["ralha_lower"] = (alpha.copy(), beta.copy())
+    (a, b, cs), sigma, Ub, Vb, k = _bsvd(alpha, beta, top_k, svd_mode)
+    stages["bidiagonal"] = (a, b)
+    compute_u, compute_v = svd_mode != 3, svd_mode != 2
+    parts, FinalU, out3, sut = [], None, None, None
+    if compute_u:                                                 # :1002-1015
+        for c in range(P):
+            t = Vb @ Vr[c]
+            parts.append(t @ uq[c] if uq[c] is not None else t)  # k x m_part
+        if svd_mode == 4:                                         # :1023-1044
+            ym = block_shift_mask(np.asarray(y, float).reshape(1, m), MASK_PASSES, True, False, public_seed).ravel()
+            sut = sum(parts[c] @ ym[pos[c]:pos[c + 1]] for c in range(P)) / sigma
+        else:
+            FinalU = np.concatenate(parts, axis=1)                # k x m, :1071-1096
+            FinalU = block_shift_mask(FinalU, MASK_PASSES, False, False, public_seed)   # :1098-1105
+    if compute_v:                                                 # :1119-1169
+        U2 = _rotate_house(Ub, cs, house, tau)                    # global_n x k
+        out3 = []
+        if svd_mode == 4:
+            w = U2 @ sut
+            for c in range(P):
+                wc = w[npos[c]:npos[c + 1]].reshape(1, -1)
+                out3.append(block_shift_mask(wc, MASK_PASSES, False, False, private_seeds[c]).ravel())
+        else:
+            for c in range(P):
+                t = np.ascontiguousarray(U2[npos[c]:npos[c + 1]].T)
+                out3.append(block_shift_mask(t, MASK_PASSES, False, False, private_seeds[c]))
+    out = (sigma, FinalU, out3)
+    return (out + (stages,)) if return_stages else out
+
+
 def run(blocks, public_seed, private_seeds, top_k=-1, svd_mode=1, return_stages=False):
-    """DecentralizedClient::run(), opt_control 3; svd_mode 0 (full, dbdsdc),
-    1 (two-sided), 2 (left only) or 3 (right only)."""
+    """DecentralizedClient::run(), opt_control 3, short-and-wide layout
+    (m <= global_n, blocks X_c row-major m x local_n); svd_mode 0 (full,
+    dbdsdc), 1 (two-sided), 2 (left only) or 3 (right only).  m == global_n
+    runs without the global QR (client.cpp:795-798) and takes the V
+    back-transform of the tall branch (:1129-1160)."""
     P = len(blocks)
     m = blocks[0].shape[0]
     local_n = [b.shape[1] for b in blocks]
     global_n = sum(local_n)
     if m > global_n:
-        raise NotImplementedError("tall-and-skinny branch (m > global_n)")
+        raise ValueError("m > global_n: the tall-and-skinny branch takes transposed blocks (run_tall)")
     red = [reduced_width(m, n) for n in local_n]
     rg = sum(red)
-    if rg <= m:
+    if rg <= m and m < global_n:
         raise ValueError("the V back-transform needs reduced_global_n > m (client.cpp:1179)")
     stages = {}
     masked, local_q = [], []
@@ -201,32 +302,23 @@ def run(blocks, public_seed, private_seeds, top_k=-1, svd_mode=1, return_stages=
     stages["masked"] = [x.copy() for x in masked]
     M = np.concatenate(masked, axis=1)                            # m x rg, repartition :681-703
     part, pos = row_split(m, P)
-    # global Householder QR of M^T (client.cpp:705-794), panel by panel in
-    # the reference; one dgeqrf here (same reflectors, up to rounding)
-    qr, tau_g, _, info = lapack.dgeqrf(np.asfortranarray(M.T))
-    assert info == 0
-    Rg = np.triu(qr[:m, :])
-    Qg, _, info = lapack.dorgqr(qr, tau_g)
-    assert info == 0
-    stages["global_r"] = Rg.copy()
-    slabs = [Rg[:, pos[c]:pos[c + 1]].copy() for c in range(P)]
+    Qg = None
+    if rg > m:
+        # global Householder QR of M^T (client.cpp:705-794), panel by panel in
+        # the reference; one dgeqrf here (same reflectors, up to rounding)
+        qr, tau_g, _, info = lapack.dgeqrf(np.asfortranarray(M.T))
+        assert info == 0
+        W = np.triu(qr[:m, :])
+        Qg, _, info = lapack.dorgqr(qr, tau_g)
+        assert info == 0
+    else:
+        W = M.T.copy()                                            # in-place transpose, :795-798
+    stages["global_r"] = W.copy()
+    slabs = [W[:, pos[c]:pos[c + 1]].copy() for c in range(P)]
     alpha, beta, house, tau, Vr = ralha(slabs)                    # :801-945
     stages["ralha_lower"] = (alpha.copy(), beta.copy())
-    a, b, cs = lower_to_upper(alpha, beta)                        # :947-954
+    (a, b, cs), sigma, Ub, Vb, k = _bsvd(alpha, beta, top_k, svd_mode)
     stages["bidiagonal"] = (a.copy(), b.copy())
-    bound = np.linalg.norm(a) ** 2 + np.linalg.norm(b) ** 2       # :966-971
-    k = negative_count(a, b, bound) - negative_count(a, b, 0.0)
-    if top_k > 0:
-        k = min(k, top_k)
-    if svd_mode == 0:
-        sigma, Ub, Vb = leading_svd(a, b, k)                      # :975-980
-    else:
-        sigma, Ub, Vb = bidiagonal_svd(a, b, k)                   # :984
-    for i in range(k):                                            # :988-995
-        p = int(np.argmax(np.abs(Ub[:, i])))
-        if Ub[p, i] < 0:
-            Ub[:, i] = -Ub[:, i]
-            Vb[i] = -Vb[i]
     stages["bsvd"] = (sigma.copy(), Ub.copy(), Vb.copy())
     FinalU = None
     if svd_mode != 3:                                             # :1002-1115
@@ -237,18 +329,18 @@ def run(blocks, public_seed, private_seeds, top_k=-1, svd_mode=1, return_stages=
     if svd_mode == 2:
         out = (sigma, FinalU, None)
         return (out + (stages,)) if return_stages else out
-    U2 = Ub.copy()                                                # :1127-1128
-    for i in range(m - 2, -1, -1):
-        c_, s_ = cs[i]
-        x, y = U2[i].copy(), U2[i + 1].copy()
-        U2[i] = c_ * x - s_ * y
-        U2[i + 1] = c_ * y + s_ * x
-    U2 = apply_house(house, tau, U2)                              # :1176
-    rpos = np.concatenate([[0], np.cumsum(red)])
+    U2 = _rotate_house(Ub, cs, house, tau)                        # :1127-1176
     FinalVT = []
-    for c in range(P):
-        t = U2.T @ Qg[rpos[c]:rpos[c + 1], :].T                   # :1179
-        t = block_shift_mask(t, MASK_PASSES, False, False, private_seeds[c])
-        FinalVT.append(t @ local_q[c] if local_q[c] is not None else t)   # :1188-1195
+    if m == global_n:                                             # :1129-1160
+        npos = np.concatenate([[0], np.cumsum(local_n)])
+        for c in range(P):
+            t = np.ascontiguousarray(U2[npos[c]:npos[c + 1]].T)
+            FinalVT.append(block_shift_mask(t, MASK_PASSES, False, False, private_seeds[c]))
+    else:
+        rpos = np.concatenate([[0], np.cumsum(red)])
+        for c in range(P):
+            t = U2.T @ Qg[rpos[c]:rpos[c + 1], :].T               # :1179
+            t = block_shift_mask(t, MASK_PASSES, False, False, private_seeds[c])
+            FinalVT.append(t @ local_q[c] if local_q[c] is not None else t)   # :1188-1195
     out = (sigma, FinalU, FinalVT)
     return (out + (stages,)) if return_stages else out

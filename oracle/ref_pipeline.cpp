@@ -6,12 +6,16 @@
 //   <out>/sigma.bin   singular values (recomputed from the participant's
 //                     final bidiagonal with the reference's own bisection,
 //                     the same call run() makes at client.cpp:984)
-//   <out>/U.bin       FinalU, m x sigma_count row-major (client 0 only)
+//   <out>/U.bin       FinalU (client 0 only): m x sigma_count row-major, or
+//                     sigma_count x m when m > global_n (client.cpp:1071-1105)
 //   <out>/VT.bin      FinalVT, sigma_count x local_n row-major
-//   <out>/ab.bin      alpha[m], beta[m-1] after the lower->upper rotation
+//   <out>/w.bin       w_lr, local_n (svd_mode 4, linear regression)
+//   <out>/ab.bin      alpha[k], beta[k-1] after the lower->upper rotation,
+//                     k = min(m, global_n) (the bidiagonal's order, :805-814)
 //   <out>/time.txt    the reference's own run() timer (run_begin..run_finish)
 //                     followed by its phase timers
 // Usage: ref_pipeline cid nclient m local_n port dpath logdir seed mode topk out
+#include <algorithm>
 #include <cstdio>
 #include <string>
 #include <unistd.h>
@@ -40,7 +44,7 @@ int main(int argc, char** argv) {
                                                    dpath, false, false, logdir, seed, 3);
   // Singular values: run() keeps them in a local; recompute them from the
   // final bidiagonal with the same bisection run() used (client.cpp:966-985).
-  int k = (int)m;
+  int k = (int)std::min(m, c->global_n);
   double* a = c->x_diagonal;
   double* b = c->x_upper_diagonal;
   int cnt = negative_count(k, a, b, pow(cblas_dnrm2(k, a, 1), 2) + pow(cblas_dnrm2(k - 1, b, 1), 2)) -
@@ -59,10 +63,11 @@ int main(int argc, char** argv) {
   // them (svd_mode 3 / 2, client.cpp:491-492)
   if (cid == 0 && mode != 3 && mode != 4) dump(out + "/U.bin", c->FinalU, m * (size_t)cnt);
   if (mode != 2 && mode != 4) dump(out + "/VT.bin", c->FinalVT, (size_t)cnt * ln);
+  if (mode == 4) dump(out + "/w.bin", c->w_lr, ln);
   if (mode != 0 && mode != 4) {
-    dump(out + "/ab.bin", a, m);
+    dump(out + "/ab.bin", a, k);
     FILE* fp = fopen((out + "/ab.bin").c_str(), "ab");
-    fwrite(b, sizeof(double), m - 1, fp);
+    fwrite(b, sizeof(double), k - 1, fp);
     fclose(fp);
   }
   FILE* ft = fopen((out + "/time.txt").c_str(), "w");

@@ -82,3 +82,36 @@ def pipeline_cases():
     rng = np.random.default_rng(9)
     out["noqr"] = ([rng.standard_normal((40, n)) for n in (160, 200)], 9)
     return out
+
+
+def tall_cases():
+    """name -> (blocks_t, seed, y): the tall-and-skinny branch (m > global_n),
+    where the reference holds each participant's block transposed, local_n x m
+    row-major (client.cpp:549, 1248); y (length m) is the label vector of
+    svd_mode 4, held by the last participant (client.cpp:1026-1029)."""
+    out = {}
+    rng = np.random.default_rng(31)
+    # every column slab m_part = 250 > global_n = 80: local QR of each slab
+    out["t_qr"] = ([rng.standard_normal((n, 500)) for n in (30, 50)], 31, rng.standard_normal(500))
+    rng = np.random.default_rng(32)
+    # m_part = 34, 33, 33 <= global_n = 75: slabs go to Ralha as they are
+    out["t_noqr"] = ([rng.standard_normal((n, 100)) for n in (20, 30, 25)], 32, rng.standard_normal(100))
+    rng = np.random.default_rng(33)
+    # m_part = 51, 50, 50 against global_n = 50: only the first slab is reduced
+    out["t_mixed"] = ([rng.standard_normal((n, 151)) for n in (10, 25, 15)], 33, rng.standard_normal(151))
+    return out
+
+
+def tall_mode_cases():
+    """name -> (tall case, svd_mode, top_k)."""
+    return {"t_qr_mode0": ("t_qr", 0, -1), "t_qr_mode2_top10": ("t_qr", 2, 10),
+            "t_qr_mode3_top10": ("t_qr", 3, 10), "t_qr_mode4": ("t_qr", 4, -1),
+            "t_mixed_mode4": ("t_mixed", 4, -1), "t_noqr_mode1_top7": ("t_noqr", 1, 7)}
+
+
+def square_cases():
+    """name -> (blocks, seed): m == global_n in the short-and-wide layout, the
+    case without a global QR whose V comes from rows of the rotated bidiagonal
+    U (client.cpp:795-798, 1129-1160)."""
+    rng = np.random.default_rng(41)
+    return {"sq80": ([rng.standard_normal((80, n)) for n in (30, 50)], 41)}

@@ -15,7 +15,9 @@ EXCALIBUR_REF), never the oracle restatement:
 Inputs are regenerated from numpy seeds; each fixture stores a SHA-256 of
 its inputs so a test can tell a changed generator from a changed result.
 
-Usage:  python tests/golden/make_golden.py   (needs the reference checkout)
+Usage:  python tests/golden/make_golden.py [PREFIX ...]
+        (needs the reference checkout; with prefixes, only the fixtures whose
+        names start with one of them are rewritten)
 """
 import ctypes as C
 import hashlib
@@ -100,22 +102,27 @@ def mask_fixtures(R):
     return out
 
 
-def run_reference_pipeline(blocks, seed, mode=1, topk=-1):
-    """P reference processes over loopback; returns (sigma, FinalU, [FinalVT_c],
-    alpha_beta_c0, run_seconds_per_participant)."""
+def run_reference_pipeline(blocks, seed, mode=1, topk=-1, tall=False, y=None):
+    """P reference processes over loopback; returns (sigma, FinalU, [FinalVT_c]
+    or [w_c] in svd_mode 4, alpha_beta_c0, run_seconds_per_participant).
+    ``tall``: the blocks are local_n x m (the reference's layout when
+    m > global_n) and FinalU comes back k x m."""
     P = len(blocks)
-    m = blocks[0].shape[0]
+    m = blocks[0].shape[1] if tall else blocks[0].shape[0]
+    ln = [x.shape[0] if tall else x.shape[1] for x in blocks]
     with tempfile.TemporaryDirectory() as td:
         port = random.randint(20000, 40000)
         procs = []
         for c, x in enumerate(blocks):
             np.ascontiguousarray(x, dtype=np.float64).tofile(os.path.join(td, f"Client{c}.mat"))
+        if y is not None:
+            np.ascontiguousarray(y, dtype=np.float64).tofile(os.path.join(td, "y.mat"))
         env = dict(os.environ, OMP_NUM_THREADS=str(max(1, (os.cpu_count() or 2) // P)))
         for c, x in enumerate(blocks):
             od = os.path.join(td, f"out{c}")
             os.makedirs(od)
             procs.append(subprocess.Popen(
-                [os.path.join(REFDIR, "ref_pipeline"), str(c), str(P), str(m), str(x.shape[1]),
+                [os.path.join(REFDIR, "ref_pipeline"), str(c), str(P), str(m), str(ln[c]),
                  str(port), td, td, str(seed), str(mode), str(topk), od],
                 stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL, env=env, cwd=td))
         for pr in procs:
@@ -123,9 +130,13 @@ def run_reference_pipeline(blocks, seed, mode=1, topk=-1):
                 raise RuntimeError("reference participant failed")
         sig = np.fromfile(os.path.join(td, "out0", "sigma.bin"))
         k = len(sig)
-        U = np.fromfile(os.path.join(td, "out0", "U.bin")).reshape(m, k) if mode not in (3, 4) else None
-        VT = ([np.fromfile(os.path.join(td, f"out{c}", "VT.bin")).reshape(k, blocks[c].shape[1])
-               for c in range(P)] if mode not in (2, 4) else None)
+        U = (np.fromfile(os.path.join(td, "out0", "U.bin")).reshape((k, m) if tall else (m, k))
+             if mode not in (3, 4) else None)
+        if mode == 4:
+            VT = [np.fromfile(os.path.join(td, f"out{c}", "w.bin")) for c in range(P)]
+        else:
+            VT = ([np.fromfile(os.path.join(td, f"out{c}", "VT.bin")).reshape(k, ln[c])
+                   for c in range(P)] if mode != 2 else None)
         abf = os.path.join(td, "out0", "ab.bin")
         ab = np.fromfile(abf) if os.path.exists(abf) else np.zeros(0)
         secs = [float(open(os.path.join(td, f"out{c}", "time.txt")).read().split()[0]) for c in range(P)]
@@ -150,6 +161,31 @@ def pipeline_fixtures():
         for c, v in enumerate(VT or []):
             d[f"VT{c}"] = v
         out[name] = d
+    tall = cases.tall_cases()
+    for name, (blocks, seed, y) in tall.items():
+        sig, U, VT, ab, secs = run_reference_pipeline(blocks, seed, tall=True)
+        d = dict(x_sha=sha(*blocks), seed=np.uint32(seed), sigma=sig, U=U, ab=ab)
+        for c, v in enumerate(VT):
+            d[f"VT{c}"] = v
+        out[name] = d
+    for name, (case, mode, topk) in cases.tall_mode_cases().items():
+        blocks, seed, y = tall[case]
+        sig, U, VT, ab, secs = run_reference_pipeline(blocks, seed, mode=mode, topk=topk, tall=True,
+                                                      y=y if mode == 4 else None)
+        d = dict(x_sha=sha(*blocks, y), seed=np.uint32(seed), sigma=sig, svd_mode=np.int32(mode),
+                 top_k=np.int32(topk))
+        if U is not None:
+            d["U"] = U
+        for c, v in enumerate(VT or []):
+            d[f"w{c}" if mode == 4 else f"VT{c}"] = v
+        out[name] = d
+    for name, (blocks, seed) in cases.square_cases().items():
+        for mode in (1, 0):
+            sig, U, VT, ab, secs = run_reference_pipeline(blocks, seed, mode=mode)
+            d = dict(x_sha=sha(*blocks), seed=np.uint32(seed), sigma=sig, U=U, ab=ab, svd_mode=np.int32(mode))
+            for c, v in enumerate(VT):
+                d[f"VT{c}"] = v
+            out[f"{name}_mode{mode}"] = d
     return out
 
 
@@ -163,6 +199,8 @@ def main():
                    ("pipe", pipeline_fixtures())):
         for name, arrs in d.items():
             fx[f"{grp}__{name}"] = arrs
+    keep = sys.argv[1:]
+    fx = {k: v for k, v in fx.items() if not keep or any(k.startswith(p) for p in keep)}
     for key, arrs in fx.items():
         np.savez_compressed(os.path.join(HERE, f"{key}.npz"), **arrs)
     print(f"wrote {len(fx)} fixtures to {HERE}")

@@ -30,7 +30,9 @@ PIPES = sorted(cases.pipeline_cases())
 def test_every_fixture_has_a_case():
     names = {os.path.basename(f)[:-4] for f in glob.glob(os.path.join(GOLD, "*.npz"))}
     want = ({f"bidiag__{n}" for n in BIDIAG} | {f"mask__{n}" for n in MASKS}
-            | {f"pipe__{n}" for n in PIPES} | {f"pipe__{n}" for n in cases.pipeline_mode_cases()})
+            | {f"pipe__{n}" for n in PIPES} | {f"pipe__{n}" for n in cases.pipeline_mode_cases()}
+            | {f"pipe__{n}" for n in cases.tall_cases()} | {f"pipe__{n}" for n in cases.tall_mode_cases()}
+            | {f"pipe__{n}_mode{m}" for n in cases.square_cases() for m in (0, 1)})
     assert names == want
 
 
@@ -127,3 +129,67 @@ def test_pipeline_modes_match_reference(golden, name):
             assert np.max(np.abs(v - g[f"VT{c}"])) < 1e-10
     else:
         assert VT is None
+
+
+TALL = sorted(cases.tall_cases())
+TALL_MODES = sorted(cases.tall_mode_cases())
+
+
+def _check_outputs(g, s, U, out3, mode):
+    assert len(s) == len(g["sigma"])
+    assert np.max(np.abs(s - g["sigma"]) / g["sigma"]) < 1e-13
+    if mode not in (3, 4):
+        assert np.max(np.abs(U - g["U"])) < 1e-10
+    else:
+        assert U is None and "U" not in g
+    if mode == 4:
+        for c, w in enumerate(out3):
+            assert np.max(np.abs(w - g[f"w{c}"])) < 1e-12
+    elif mode != 2:
+        for c, v in enumerate(out3):
+            assert np.max(np.abs(v - g[f"VT{c}"])) < 1e-10
+    else:
+        assert out3 is None
+
+
+@pytest.mark.parametrize("name", TALL)
+def test_tall_pipeline_matches_reference(golden, name):
+    g = golden(f"pipe__{name}")
+    blocks, seed, _ = cases.tall_cases()[name]
+    assert sha(*blocks) == str(g["x_sha"])
+    pub, priv = oracle.reference_seeds(seed, len(blocks))
+    s, U, VT, st = pipeline.run_tall(blocks, pub, priv, return_stages=True)
+    _check_outputs(g, s, U, VT, 1)
+    a, b = st["bidiagonal"]
+    assert np.max(np.abs(np.abs(np.concatenate([a, b])) - np.abs(g["ab"]))) < 1e-10
+
+
+@pytest.mark.parametrize("name", TALL_MODES)
+def test_tall_modes_match_reference(golden, name):
+    g = golden(f"pipe__{name}")
+    case, mode, topk = cases.tall_mode_cases()[name]
+    blocks, seed, y = cases.tall_cases()[case]
+    assert sha(*blocks, y) == str(g["x_sha"])
+    pub, priv = oracle.reference_seeds(seed, len(blocks))
+    s, U, out3 = pipeline.run_tall(blocks, pub, priv, top_k=topk, svd_mode=mode, y=y)
+    _check_outputs(g, s, U, out3, mode)
+
+
+def test_tall_lr_is_least_squares():
+    """svd_mode 4 returns w = V diag(1/sigma) U^T y, the least-squares solution
+    of X w = y with X = [X_0 | X_1 | ...] (client.cpp:1023-1160)."""
+    blocks, seed, y = cases.tall_cases()["t_qr"]
+    pub, priv = oracle.reference_seeds(seed, len(blocks))
+    _, _, w = pipeline.run_tall(blocks, pub, priv, svd_mode=4, y=y)
+    X = np.concatenate([b.T for b in blocks], axis=1)
+    assert np.max(np.abs(np.concatenate(w) - np.linalg.lstsq(X, y, rcond=None)[0])) < 1e-12
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_square_matches_reference(golden, mode):
+    g = golden(f"pipe__sq80_mode{mode}")
+    blocks, seed = cases.square_cases()["sq80"]
+    assert sha(*blocks) == str(g["x_sha"])
+    pub, priv = oracle.reference_seeds(seed, len(blocks))
+    s, U, VT = pipeline.run(blocks, pub, priv, svd_mode=mode)
+    _check_outputs(g, s, U, VT, mode)
