@@ -316,23 +316,59 @@ class Context:
         self.sync()
         return R, W
 
-    def _config(self, m, local_n, public_seed, private_seeds, top_k, svd_mode, precision):
+    def _config(self, m, local_n, public_seed, private_seeds, top_k, svd_mode, precision, labels=None):
         P = len(local_n)
         self._ln = (C.c_size_t * P)(*local_n)
         self._ps = (C.c_uint * P)(*[s & 0xFFFFFFFF for s in private_seeds])
-        return FedSVDConfig(P, m, self._ln, public_seed & 0xFFFFFFFF, self._ps, top_k, svd_mode, precision)
+        return FedSVDConfig(P, m, self._ln, public_seed & 0xFFFFFFFF, self._ps, top_k, svd_mode, precision,
+                            labels)
 
-    def fedsvd(self, blocks, public_seed, private_seeds, top_k=-1, svd_mode=1, precision=0):
+    @staticmethod
+    def _shapes(blocks, tall):
+        """(m, [local_n]) of the blocks in the branch's layout: X_c (m x
+        local_n) short-and-wide, X_c^T (local_n x m) tall-and-skinny."""
+        if tall:
+            m, ln = blocks[0].shape[1], [b.shape[0] for b in blocks]
+            if m <= sum(ln):
+                raise ValueError(f"tall layout needs m={m} > global_n={sum(ln)}")
+        else:
+            m, ln = blocks[0].shape[0], [b.shape[1] for b in blocks]
+            if m > sum(ln):
+                raise ValueError(f"m={m} > global_n={sum(ln)}: pass the blocks transposed with tall=True")
+        return m, ln
+
+    @staticmethod
+    def _outputs(U, VT, m, ln, k, svd_mode, tall):
+        if svd_mode in (3, 4):
+            Uo = None
+        else:
+            Uo = U[: m * k].reshape(k, m) if tall else U[: m * k].reshape(m, k)
+        if svd_mode == 2:
+            VTo = None
+        elif svd_mode == 4:
+            VTo = [v[:n] for v, n in zip(VT, ln)]
+        else:
+            VTo = [v[: k * n].reshape(k, n) for v, n in zip(VT, ln)]
+        return Uo, VTo
+
+    def fedsvd(self, blocks, public_seed, private_seeds, top_k=-1, svd_mode=1, precision=0, tall=False,
+               labels=None):
         """DecentralizedClient::run() for P participants on this GPU
-        (client.cpp:447-1200).  blocks: list of m x local_n CUDA tensors,
-        overwritten.  Returns (sigma k, FinalU m x k, [FinalVT_c k x local_n]);
-        FinalU is None in svd_mode 3 and the FinalVT list None in svd_mode 2."""
+        (client.cpp:447-1200).  blocks (CUDA tensors, overwritten): m x
+        local_n each, or with tall=True (m > global_n) local_n x m each, the
+        reference's layout in its tall-and-skinny branch.  Returns (sigma k,
+        FinalU, [FinalVT_c k x local_n]); FinalU is m x k (k x m with tall),
+        None in svd_modes 3 and 4; the FinalVT list is None in svd_mode 2.
+        svd_mode 4 (linear regression, tall only) takes labels (CUDA tensor,
+        m) and returns [w_c (local_n)] in place of FinalVT."""
         P = len(blocks)
-        m = blocks[0].shape[0]
-        ln = [b.shape[1] for b in blocks]
-        cfg = self._config(m, ln, public_seed, private_seeds, top_k, svd_mode, precision)
-        sig = self._empty(m)
-        U = self._empty(m * m)
+        m, ln = self._shapes(blocks, tall)
+        kmax = min(m, sum(ln))
+        y = labels.contiguous() if labels is not None else None
+        cfg = self._config(m, ln, public_seed, private_seeds, top_k, svd_mode, precision,
+                           C.c_void_p(y.data_ptr()) if y is not None else None)
+        sig = self._empty(kmax)
+        U = self._empty(m * kmax)
         VT = [self._empty(m * n) for n in ln]
         bp = (C.c_void_p * P)(*[b.data_ptr() for b in blocks])
         vp = (C.c_void_p * P)(*[v.data_ptr() for v in VT])
@@ -342,8 +378,7 @@ class Context:
                     "fedsvd")
         self.sync()
         k = k.value
-        Uo = U[: m * k].view(m, k) if svd_mode != 3 else None
-        VTo = [v[: k * n].view(k, n) for v, n in zip(VT, ln)] if svd_mode != 2 else None
+        Uo, VTo = self._outputs(U, VT, m, ln, k, svd_mode, tall)
         return sig[:k], Uo, VTo
 
     def fedsvd_tune(self, m, local_n, top_k=-1, svd_mode=1, precision=0):
@@ -356,16 +391,20 @@ class Context:
                     "fedsvd_tune")
         return st.value, nb.value, ms.value
 
-    def fedsvd_host(self, blocks, public_seed, private_seeds, top_k=-1, svd_mode=1, precision=0, out=None):
+    def fedsvd_host(self, blocks, public_seed, private_seeds, top_k=-1, svd_mode=1, precision=0, out=None,
+                    tall=False, labels=None):
         """Same through the host-pointer entry (bbt_fedsvd_run_host): numpy
-        blocks in, numpy results out (copies timed inside the call)."""
+        blocks (and labels) in, numpy results out (copies timed inside the
+        call)."""
         P = len(blocks)
-        m = blocks[0].shape[0]
-        ln = [b.shape[1] for b in blocks]
-        cfg = self._config(m, ln, public_seed, private_seeds, top_k, svd_mode, precision)
+        m, ln = self._shapes(blocks, tall)
+        kmax = min(m, sum(ln))
+        y = np.ascontiguousarray(labels, dtype=np.float64) if labels is not None else None
+        cfg = self._config(m, ln, public_seed, private_seeds, top_k, svd_mode, precision,
+                           C.c_void_p(y.ctypes.data) if y is not None else None)
         blocks = [np.ascontiguousarray(b, dtype=np.float64) for b in blocks]
         if out is None:
-            out = (np.empty(m), np.empty(m * m), [np.empty(m * n) for n in ln])
+            out = (np.empty(kmax), np.empty(m * kmax), [np.empty(m * n) for n in ln])
         sig, U, VT = out
         bp = (C.c_void_p * P)(*[b.ctypes.data for b in blocks])
         vp = (C.c_void_p * P)(*[v.ctypes.data for v in VT])
@@ -373,7 +412,8 @@ class Context:
         self._check(self.L.bbt_fedsvd_run_host(self.h, C.byref(cfg), bp, C.c_void_p(sig.ctypes.data),
                                                C.c_void_p(U.ctypes.data), vp, C.byref(k)), "fedsvd_host")
         k = k.value
-        return sig[:k], U[: m * k].reshape(m, k), [v[: k * n].reshape(k, n) for v, n in zip(VT, ln)]
+        Uo, VTo = self._outputs(U, VT, m, ln, k, svd_mode, tall)
+        return sig[:k], Uo, VTo
 
     def dgemm(self, transa, transb, A, B, alpha=1.0, beta=0.0, C=None):
         """C = alpha op(A) op(B) + beta C on column-major data.  A, B, C are

@@ -39,6 +39,7 @@ class FedSVDConfig(C.Structure):
         ("top_k", C.c_int),
         ("svd_mode", C.c_int),
         ("precision", C.c_int),
+        ("labels", C.c_void_p),
     ]
 
 

@@ -3,6 +3,7 @@
 // pipeline entry.  All arithmetic is in the kernels of the other sources.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -302,7 +303,8 @@ bbt_status bbt_fedsvd_run(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* co
                           double* sigma, double* U, double* const* VT, int* k) {
   if (!ctx) return BBT_ERR_ARG;
   if (!cfg || !blocks || !k || bad(sigma)) return fail(ctx, BBT_ERR_ARG, "fedsvd: NULL argument");
-  const bool want_u = cfg->svd_mode != 3, want_v = cfg->svd_mode != 2;
+  const bool want_u = cfg->svd_mode != 3 && cfg->svd_mode != 4, want_v = cfg->svd_mode != 2;
+  if (cfg->svd_mode == 4 && bad(cfg->labels)) return fail(ctx, BBT_ERR_ARG, "fedsvd: svd_mode 4 labels");
   if ((want_u && bad(U)) || (want_v && !VT)) return fail(ctx, BBT_ERR_ARG, "fedsvd: NULL output");
   for (int c = 0; c < cfg->participants; ++c)
     if (bad(blocks[c]) || (want_v && bad(VT[c]))) return fail(ctx, BBT_ERR_ARG, "fedsvd: participant %d buffer", c);
@@ -314,12 +316,17 @@ bbt_status bbt_fedsvd_run_host(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, const
   if (!ctx) return BBT_ERR_ARG;
   if (!cfg || !hX || !k || !hsigma || cfg->participants < 1 || !cfg->local_n)
     return fail(ctx, BBT_ERR_ARG, "fedsvd_host: NULL argument");
-  const bool want_u = cfg->svd_mode != 3, want_v = cfg->svd_mode != 2;
-  if ((want_u && !hU) || (want_v && !hVT)) return fail(ctx, BBT_ERR_ARG, "fedsvd_host: NULL output");
+  const bool lr = cfg->svd_mode == 4;
+  const bool want_u = cfg->svd_mode != 3 && !lr, want_v = cfg->svd_mode != 2;
+  if ((want_u && !hU) || (want_v && !hVT) || (lr && !cfg->labels))
+    return fail(ctx, BBT_ERR_ARG, "fedsvd_host: NULL output");
   const int P = cfg->participants;
   const size_t m = cfg->m;
+  size_t gn = 0;
+  for (int c = 0; c < P; ++c) gn += cfg->local_n[c];
+  const size_t kmax = std::min(m, gn);   // singular values: the bidiagonal's order
   // staging in a grow-only arena kept by the context (no allocation per call)
-  size_t need = m * sizeof(double) + m * m * sizeof(double) + 4096;
+  size_t need = (m + 2 * kmax + m * kmax) * sizeof(double) + 8192;
   for (int c = 0; c < P; ++c) need += (want_v ? 2 : 1) * (m * cfg->local_n[c] * sizeof(double) + 256);
   if (ctx->io_ws.cap < need) BBT_CUDA(ctx, ctx->io_ws.reserve(need));
   ctx->io_ws.reset();
@@ -328,8 +335,9 @@ bbt_status bbt_fedsvd_run_host(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, const
     dX[c] = ctx->io_ws.take<double>(m * cfg->local_n[c]);
     if (want_v) dVT[c] = ctx->io_ws.take<double>(m * cfg->local_n[c]);
   }
-  double* ds = ctx->io_ws.take<double>(m);
-  double* dU = ctx->io_ws.take<double>(m * m);
+  double* ds = ctx->io_ws.take<double>(kmax);
+  double* dU = ctx->io_ws.take<double>(m * kmax);
+  double* dy = lr ? ctx->io_ws.take<double>(m) : nullptr;
   if (!ctx->copy_in) BBT_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->copy_in, cudaStreamNonBlocking));
   if (!ctx->copy_out) BBT_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->copy_out, cudaStreamNonBlocking));
   while ((int)ctx->in_ready.size() < P) {
@@ -348,11 +356,17 @@ bbt_status bbt_fedsvd_run_host(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, const
                                   ctx->copy_in));
     BBT_CUDA(ctx, cudaEventRecord(ctx->in_ready[c], ctx->copy_in));
   }
+  bbt_fedsvd_config dcfg = *cfg;
+  if (lr) {   // the labels follow the blocks on the copy stream
+    BBT_CUDA(ctx, cudaMemcpyAsync(dy, cfg->labels, m * sizeof(double), cudaMemcpyHostToDevice, ctx->copy_in));
+    BBT_CUDA(ctx, cudaEventRecord(ctx->in_ready[P - 1], ctx->copy_in));
+    dcfg.labels = dy;
+  }
   ctx->vt_dst.assign(P, nullptr);
   if (want_v)
     for (int c = 0; c < P; ++c) ctx->vt_dst[c] = hVT[c];   // copied out by the pipeline as each is done
   ctx->io_on = true;
-  bbt_status st = fedsvd(ctx, cfg, dX.data(), ds, dU, dVT.data(), k);
+  bbt_status st = fedsvd(ctx, &dcfg, dX.data(), ds, dU, dVT.data(), k);
   ctx->io_on = false;
   cudaError_t e = cudaSuccess;
   if (st == BBT_OK) {

@@ -1,15 +1,17 @@
 // DecentralizedClient::run() (Excalibur src/client.cpp:447-1200) for P
 // participants held as separate device buffers on one GPU.
 //
-// Short-and-wide branch (m <= global_n), svd_mode 1, opt_control 3:
+// Short-and-wide branch (m <= global_n), opt_control 3:
 //   local QR of every wide block (local_n / m > 5)          client.cpp:572-589
 //   public (row) then private (column) Givens masks          :593-596
 //   repartition = the column concatenation M = [M_0 | ...]  :681-703
-//   Householder QR of M^T, Q_g kept                          :705-794
+//   Householder QR of M^T, Q_g kept (none if m == global_n)  :705-798
 //   Ralha bidiagonalisation of R_g                           :801-954
 //   bisection + twisted vectors, sign convention            :963-995
 //   FinalU = unmask_pub((V_b Vr)^T)                          :1002-1115
-//   FinalVT_c = unmask_priv_c(U2^T Q_g[c]^T) Q_c^T           :1119-1195
+//   FinalVT_c = unmask_priv_c(U2^T Q_g[c]^T) Q_c^T           :1174-1195
+//     (m == global_n: unmask_priv_c(U2[rows of c]^T))        :1129-1169
+// Tall-and-skinny branch (m > global_n): fedsvd_tall below.
 // The ring all-reduce / all-gather of the reference become reductions
 // inside the kernels (Ralha) or plain device-memory reads (U all-gather).
 #include <cuda_runtime.h>
@@ -23,6 +25,7 @@ namespace bbt {
 namespace {
 
 constexpr int MASK_PASSES = 32;            // client.cpp:536
+constexpr size_t MASK_SCRATCH_CAP = (size_t)2 << 30;
 constexpr double LOCAL_QR_THRESHOLD = 5.0; // client.cpp:482
 
 size_t reduced_width(size_t m, size_t n) {   // client.cpp:505,510,517 (integer ratio)
@@ -66,21 +69,54 @@ __global__ void embed_leading(int m, int kk, const double* __restrict__ Us, cons
   }
 }
 
+// Scale each of k entries of x by 1/sigma (client.cpp:1045).
+__global__ void div_sigma(int k, const double* __restrict__ sigma, double* __restrict__ x) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < k) x[j] = x[j] / sigma[j];
+}
+
 struct Layout {
   int P = 0;
   int precision = 0;
   size_t m = 0, rg = 0, nmax = 0;
   std::vector<size_t> n, r, rpos;
   std::vector<bool> qr;
+  // tall-and-skinny branch (m > global_n): column slabs of X
+  bool tall = false;
+  size_t gn = 0, wn = 0;              // global_n; Ralha columns sum_c min(m_part[c], global_n)
+  std::vector<size_t> npos;           // n_pos
+  std::vector<size_t> part, ppos;     // m_part / m_part_pos (client.cpp:613-624)
+  std::vector<size_t> wpos;           // slab c's first column in the Ralha matrix
 };
+
+// The slab QRs of the tall-and-skinny branch as a short-and-wide local-QR
+// layout: slab c is global_n x m_part[c] row-major (= column-major A of
+// m_part[c] x global_n, the shape local_qr_reduction(m_part, global_n) takes,
+// client.cpp:661-667), reduced when m_part[c] > global_n.
+Layout slab_layout(const Layout& L) {
+  Layout q;
+  q.P = L.P;
+  q.precision = L.precision;
+  q.m = L.gn;
+  q.rpos.push_back(0);
+  for (int c = 0; c < L.P; ++c) {
+    q.n.push_back(L.part[c]);
+    q.nmax = std::max(q.nmax, L.part[c]);
+    q.qr.push_back(L.part[c] > L.gn);
+    q.r.push_back(std::min(L.part[c], L.gn));
+    q.rg += q.r.back();
+    q.rpos.push_back(q.rg);
+  }
+  return q;
+}
 
 bbt_status plan(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, Layout& L) {
   if (!cfg || cfg->participants < 1 || !cfg->local_n || !cfg->private_seeds)
     return fail(ctx, BBT_ERR_ARG, "fedsvd: bad config");
   if (cfg->precision != 0 && cfg->precision != 1)
     return fail(ctx, BBT_ERR_UNSUPPORTED, "fedsvd: precision mode %d (0 plain, 1 mixed)", cfg->precision);
-  if (cfg->svd_mode < 0 || cfg->svd_mode > 3)
-    return fail(ctx, BBT_ERR_UNSUPPORTED, "fedsvd: svd_mode %d (4, linear regression, is not built)", cfg->svd_mode);
+  if (cfg->svd_mode < 0 || cfg->svd_mode > 4)
+    return fail(ctx, BBT_ERR_UNSUPPORTED, "fedsvd: svd_mode %d (0..4)", cfg->svd_mode);
   L.P = cfg->participants;
   L.m = cfg->m;
   L.precision = cfg->precision;
@@ -98,12 +134,35 @@ bbt_status plan(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, Layout& L) {
     L.rg += L.r.back();
     L.rpos.push_back(L.rg);
   }
-  if (L.m > gn)
-    return fail(ctx, BBT_ERR_UNSUPPORTED, "fedsvd: m=%zu > global_n=%zu (tall-and-skinny branch)", L.m, gn);
-  if (L.rg <= L.m)
+  L.gn = gn;
+  L.tall = L.m > gn;
+  L.npos.push_back(0);
+  for (int c = 0; c < L.P; ++c) L.npos.push_back(L.npos.back() + L.n[c]);
+  if (cfg->svd_mode == 4 && !L.tall)
+    return fail(ctx, BBT_ERR_UNSUPPORTED,
+                "fedsvd: svd_mode 4 (linear regression) needs m > global_n, the reference's vertical layout "
+                "(client.cpp:1180)");
+  if (cfg->svd_mode == 4 && !cfg->labels) return fail(ctx, BBT_ERR_ARG, "fedsvd: svd_mode 4 without labels");
+  if (L.tall) {
+    if (gn < 3) return fail(ctx, BBT_ERR_UNSUPPORTED, "fedsvd: global_n=%zu (the bidiagonal needs >= 3)", gn);
+    if (gn > (size_t)1 << 16) return fail(ctx, BBT_ERR_UNSUPPORTED, "fedsvd: global_n=%zu too large", gn);
+    if (L.m > ((size_t)1 << 31) - 1) return fail(ctx, BBT_ERR_UNSUPPORTED, "fedsvd: m=%zu too large", L.m);
+    L.ppos.push_back(0);
+    for (int c = 0; c < L.P; ++c) {   // row_split (client.cpp:613-624)
+      L.part.push_back(L.m / L.P + ((size_t)c < L.m % L.P ? 1 : 0));
+      L.ppos.push_back(L.ppos.back() + L.part.back());
+      L.wpos.push_back(L.wn);
+      L.wn += std::min(L.part.back(), gn);
+    }
+    for (int c = 0; c < L.P; ++c)
+      if (L.part[c] < 1) return fail(ctx, BBT_ERR_UNSUPPORTED, "fedsvd: m=%zu < P=%d", L.m, L.P);
+    return BBT_OK;
+  }
+  if (L.rg <= L.m && L.m < gn)
     return fail(ctx, BBT_ERR_UNSUPPORTED,
                 "fedsvd: reduced_global_n=%zu <= m=%zu (the reference's V back-transform needs the global QR)",
                 L.rg, L.m);
+  if (L.rg == L.m) L.precision = 0;   // m == global_n: no QR anywhere, nothing to run in split precision
   if (L.m > (size_t)1 << 20) return fail(ctx, BBT_ERR_UNSUPPORTED, "fedsvd: m=%zu too large", L.m);
   return BBT_OK;
 }
@@ -127,9 +186,11 @@ size_t scratch_bytes(const bbt_ctx* ctx, const Layout& L) {
   const size_t m = L.m;
   s = std::max(s, (7 * (m + 1) * m + 4 * m) * 8 + 4096);          // twisted
   s = std::max(s, (m + 2) * (1 + 8 + 1 + 7) * 48 + 4096);         // bisection nodes
-  size_t mask = 0;
-  for (int c = 0; c < L.P; ++c) mask = std::max(mask, (size_t)MASK_PASSES * (std::max(m, L.r[c]) + 1) * 24);
-  s = std::max(s, mask + 4096);
+  size_t mask = mask_workspace_bytes(m, m, MASK_PASSES, true);   // FinalU (m x k, k <= m)
+  for (int c = 0; c < L.P; ++c)
+    mask = std::max({mask, mask_workspace_bytes(m, L.r[c], MASK_PASSES, true),
+                     mask_workspace_bytes(m, L.r[c], MASK_PASSES, false)});
+  s = std::max(s, std::min(mask, MASK_SCRATCH_CAP) + 4096);   // larger masks run in batches of vectors
   return s + (64u << 20);
 }
 
@@ -298,6 +359,266 @@ bbt_status local_qr_stage(bbt_ctx* ctx, const Layout& L, double* const* X, const
   return BBT_OK;
 }
 
+// ---- tall-and-skinny branch (m > global_n) --------------------------------
+
+size_t tall_persistent_bytes(const Layout& L, const Layout& Q, int svd_mode) {
+  const size_t g = L.gn, m = L.m;
+  QrPlan qp;
+  const size_t tq = ((g + qp.nb - 1) / qp.nb) * qp.nb * qp.nb;
+  size_t b = 0;
+  for (int c = 0; c < L.P; ++c)
+    if (Q.qr[c]) {
+      b += g * L.part[c] * 8 + 256;              // the slab, then its Q (or Q_p)
+      b += (g * g + g + tq) * 8 + 768;           // R^T, tau, T
+      if (L.precision == 1) b += g * g * 8 + 256;   // W_c
+    }
+  b += 2 * (g * L.wn * 8 + 256);                 // Ralha matrix, Vr
+  b += 5 * (g * g * 8 + 256) + (6 * g + 16) * 8 + 2048;   // house, U_b, V_b, tmp, Z; tau, alpha, beta, cs
+  if (L.precision == 1) b += (size_t)sketch_rows((int)g) * sketch_pitch((long)Q.nmax) * 2 + 256;
+  if (svd_mode == 4) b += (m * g + m + 2 * g) * 8 + 1024;   // U (k x m), masked y, Sigma^-1 U^T y, w
+  return b;
+}
+
+size_t tall_scratch_bytes(const bbt_ctx* ctx, const Layout& L, const Layout& Q) {
+  QrPlan qp;
+  const size_t g = L.gn;
+  size_t s = 0;
+  for (int c = 0; c < L.P; ++c)
+    if (Q.qr[c]) {
+      s = std::max(s, qr_scratch(ctx, Q, (long)L.part[c], qp));
+      if (L.precision == 1)   // FinalU parts from int8 slices
+        s = std::max(s, oz_workspace_bytes(ctx, (int)L.part[c], (int)g, (long)g, false) + (8u << 20));
+    }
+  s = std::max(s, qr_workspace_bytes((long)g, (int)g, (int)g, qp));   // the reflectors of Ralha on U_b
+  s = std::max(s, (7 * (g + 1) * g + 4 * g) * 8 + 4096);              // twisted
+  s = std::max(s, (g + 2) * (1 + 8 + 1 + 7) * 48 + 4096);             // bisection nodes
+  size_t mask = std::max(mask_workspace_bytes(g, L.m, MASK_PASSES, false),    // FinalU (k x m, k <= g)
+                         mask_workspace_bytes(1, L.m, MASK_PASSES, false));   // y
+  for (int c = 0; c < L.P; ++c)
+    mask = std::max({mask, mask_workspace_bytes(L.n[c], L.m, MASK_PASSES, true),
+                     mask_workspace_bytes(L.n[c], L.m, MASK_PASSES, false),
+                     mask_workspace_bytes(g, L.n[c], MASK_PASSES, false)});
+  s = std::max(s, std::min(mask, MASK_SCRATCH_CAP) + 4096);   // larger masks run in batches of vectors
+  s = std::max(s, dgemm_workspace_bytes(ctx, (int)g, 1, (long)L.m));
+  return s + (64u << 20);
+}
+
+// client.cpp:543-568 (masks), 627-679 (repartition into column slabs, local
+// QR of slabs wider than global_n), 805-954 (Ralha, bidiagonal order
+// global_n), 963-995 (bidiagonal SVD), 1002-1105 (FinalU, k x m), 1023-1048
+// and 1136-1160 (svd_mode 4), 1119-1169 (FinalVT_c from rows of U2).
+bbt_status fedsvd_tall(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, const Layout& L, double* const* X,
+                       double* sigma, double* Uout, double* const* VT, int* kout) {
+  const int P = L.P, mode = cfg->svd_mode;
+  const size_t m = L.m, g = L.gn, wn = L.wn;
+  const int gi = (int)g;
+  const Layout Q = slab_layout(L);
+  QrPlan qp;
+  int streams = 1;
+  {
+    int nqr = 0;
+    for (int c = 0; c < P; ++c) nqr += Q.qr[c];
+    std::vector<size_t> skey = {L.m, (size_t)L.precision};
+    for (int c = 0; c < P; ++c) skey.push_back(L.n[c]);
+    if (ctx->tuned_streams > 0 && ctx->tuned_key == skey) {
+      streams = ctx->tuned_streams;
+      qp.nb = ctx->tuned_nb;
+    } else if (nqr >= 8) {
+      streams = 8;
+    }
+  }
+  const size_t need = tall_persistent_bytes(L, Q, mode) +
+                      std::max(tall_scratch_bytes(ctx, L, Q), batched_scratch(ctx, Q, streams, qp) + (64u << 20));
+  if (ctx->ws.cap < need) BBT_CUDA(ctx, ctx->ws.reserve(need));
+  ctx->ws.reset();
+  const size_t tq = ((g + qp.nb - 1) / qp.nb) * qp.nb * qp.nb;
+  std::vector<double*> slab(P, nullptr), RT(P, nullptr), tauc(P, nullptr), Tc(P, nullptr);
+  QrJob job;
+  job.precision = L.precision;
+  for (int c = 0; c < P; ++c)
+    if (Q.qr[c]) {
+      slab[c] = ctx->ws.take<double>(g * L.part[c]);
+      RT[c] = ctx->ws.take<double>(g * g);
+      tauc[c] = ctx->ws.take<double>(g);
+      Tc[c] = ctx->ws.take<double>(tq);
+    }
+  double* W = ctx->ws.take<double>(g * wn);
+  double* Vr = ctx->ws.take<double>(g * wn);
+  double* house = ctx->ws.take<double>(g * g);
+  double* Ub = ctx->ws.take<double>(g * g);
+  double* Vb = ctx->ws.take<double>(g * g);
+  double* tmp = ctx->ws.take<double>(g * g);
+  double* Z = ctx->ws.take<double>(g * g);
+  double* tauh = ctx->ws.take<double>(g);
+  double* alpha = ctx->ws.take<double>(g);
+  double* beta = ctx->ws.take<double>(g);
+  double* cs = ctx->ws.take<double>(2 * g);
+  double* scal = ctx->ws.take<double>(8);
+  int* cnt = ctx->ws.take<int>(8);
+  if (!cnt) return fail(ctx, BBT_ERR_NOMEM, "fedsvd: workspace");
+  job.RT = RT;
+  job.tau = tauc;
+  job.T = Tc;
+  void* S = nullptr;
+  if (L.precision == 1) {
+    job.W.assign(P, nullptr);
+    for (int c = 0; c < P; ++c)
+      if (Q.qr[c]) job.W[c] = ctx->ws.take<double>(g * g);
+    S = ctx->ws.take<char>((size_t)sketch_rows(gi) * sketch_pitch((long)Q.nmax) * 2);
+    if (!S) return fail(ctx, BBT_ERR_NOMEM, "fedsvd: workspace (mixed precision)");
+    job.S = S;
+    job.spitch = sketch_pitch((long)Q.nmax);
+  }
+  double *Ulr = nullptr, *ym = nullptr, *sut = nullptr, *wfull = nullptr;
+  if (mode == 4) {
+    Ulr = ctx->ws.take<double>(m * g);
+    ym = ctx->ws.take<double>(m);
+    sut = ctx->ws.take<double>(g);
+    wfull = ctx->ws.take<double>(g);
+    if (!wfull) return fail(ctx, BBT_ERR_NOMEM, "fedsvd: workspace (linear regression)");
+  }
+  const bool compute_u = mode != 3, compute_v = mode != 2;   // client.cpp:491-492
+  job.compute_v = compute_u;   // the slab's Q enters FinalU (u_reduction_tall_and_skinny, :664-666)
+
+  cudaEvent_t ev[7];
+  for (auto& e : ev) BBT_CUDA(ctx, cudaEventCreate(&e));
+  struct EvGuard {
+    cudaEvent_t* e;
+    ~EvGuard() { for (int i = 0; i < 7; ++i) cudaEventDestroy(e[i]); }
+  } guard{ev};
+  BBT_CUDA(ctx, cudaEventRecord(ev[0], ctx->stream));
+  // 1) masks: private on the left (rows of X_c^T), public on the right (:548-551)
+  for (int c = 0; c < P; ++c) {
+    if (ctx->io_on) BBT_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->in_ready[c], 0));
+    BBT_TRY(block_shift_mask(ctx, L.n[c], m, MASK_PASSES, X[c], true, true, cfg->private_seeds[c]));
+    BBT_TRY(block_shift_mask(ctx, L.n[c], m, MASK_PASSES, X[c], true, false, cfg->public_seed));
+  }
+  BBT_CUDA(ctx, cudaEventRecord(ev[1], ctx->stream));
+  // 2) repartition (:627-659): slab c = rows n_pos.. of every masked block,
+  //    columns m_part_pos[c].., global_n x m_part[c]; a slab that is not
+  //    reduced goes straight into its columns of the Ralha matrix
+  for (int c = 0; c < P; ++c) {
+    double* dst = Q.qr[c] ? slab[c] : W + L.wpos[c];
+    const long ldd = Q.qr[c] ? (long)L.part[c] : (long)wn;
+    for (int d = 0; d < P; ++d)
+      BBT_TRY(copy2d(ctx, (int)L.n[d], (int)L.part[c], X[d] + L.ppos[c], (long)m, dst + L.npos[d] * ldd, ldd));
+  }
+  BBT_CUDA(ctx, cudaEventRecord(ev[2], ctx->stream));
+  // 3) local QR of the slabs with m_part > global_n (:661-677): R^T replaces the slab
+  if (L.precision == 1) {
+    BBT_TRY(rademacher(ctx, sketch_rows(gi), (long)Q.nmax, S, 0x5EED5EEDull));
+    BBT_TRY(clear_tc_flags(ctx));
+  }
+  {
+    const size_t mark = ctx->ws.top;
+    const bool io = ctx->io_on;
+    ctx->io_on = false;   // every block has been waited for above
+    bbt_status st = local_qr_stage(ctx, Q, slab.data(), job, streams, qp, true);
+    ctx->io_on = io;
+    BBT_TRY(st);
+    ctx->ws.top = mark;
+  }
+  if (L.precision == 1) BBT_TRY(check_tc_flags(ctx, "fedsvd: mixed-precision slab QR"));
+  for (int c = 0; c < P; ++c)
+    if (Q.qr[c]) BBT_TRY(copy2d(ctx, gi, gi, RT[c], (long)g, W + L.wpos[c], (long)wn));
+  BBT_CUDA(ctx, cudaEventRecord(ev[3], ctx->stream));
+  // 4) Ralha of the global_n x wn matrix (:805-954)
+  BBT_TRY(ralha(ctx, gi, (int)wn, W, house, tauh, alpha, beta, Vr, cs));
+  BBT_CUDA(ctx, cudaEventRecord(ev[4], ctx->stream));
+  // 5) singular values / vectors (:963-995); svd_mode 4 takes dbdsdc's path as mode 0
+  BBT_TRY(bidiag_bound(ctx, gi, alpha, beta, scal));
+  BBT_CUDA(ctx, cudaMemsetAsync(scal + 1, 0, sizeof(double), ctx->stream));
+  BBT_TRY(sturm_counts(ctx, gi, alpha, beta, scal, 2, cnt));
+  int hc[2];
+  BBT_CUDA(ctx, cudaMemcpyAsync(hc, cnt, sizeof(hc), cudaMemcpyDeviceToHost, ctx->stream));
+  BBT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  int k = hc[0] - hc[1];
+  if (cfg->top_k > 0) k = std::min(k, cfg->top_k);
+  if (k < 1) return fail(ctx, BBT_ERR_COUNT, "fedsvd: no singular values in (0, bound]");
+  if ((mode == 0 || mode == 4) && k < gi) {
+    BBT_TRY(bidiag_svd(ctx, k, alpha, beta, tmp, W, sigma, k, true));   // leading k x k (W is free)
+    embed_leading<<<4 * ctx->num_sms, 256, 0, ctx->stream>>>(gi, k, tmp, W, Ub, Vb);
+    BBT_LAUNCHED(ctx);
+  } else {
+    BBT_TRY(bidiag_svd(ctx, gi, alpha, beta, Ub, Vb, sigma, k, true));   // Ub g x k, Vb k x g
+  }
+  BBT_CUDA(ctx, cudaEventRecord(ev[5], ctx->stream));
+  // 6) U (:1002-1015): part_c = V_b Vr_c (Q_c^T), k x m_part[c], at columns
+  //    m_part_pos[c] of FinalU (k x m row-major = column-major m x k)
+  if (compute_u) {
+    double* U = mode == 4 ? Ulr : Uout;
+    for (int c = 0; c < P; ++c) {
+      const int pc = (int)L.part[c];
+      double* dst = U + L.ppos[c];
+      if (!Q.qr[c]) {   // column-major part_c^T = Vr_c^T V_b^T
+        BBT_TRY(dgemm(ctx, false, false, pc, k, g, 1.0, Vr + L.wpos[c], (long)wn, Vb, (long)g, 0.0, dst, (long)m));
+        continue;
+      }
+      BBT_TRY(dgemm(ctx, false, false, gi, k, g, 1.0, Vr + L.wpos[c], (long)wn, Vb, (long)g, 0.0, tmp, (long)g));
+      if (L.precision == 1) {   // Q_c = Q_p W_c: part_c^T = Q_p (W_c tmp)
+        BBT_TRY(dgemm(ctx, false, false, gi, k, g, 1.0, job.W[c], (long)g, tmp, (long)g, 0.0, Z, (long)g));
+        if (oz_worthwhile(pc, k, (long)g))
+          BBT_TRY(gemm_oz(ctx, pc, k, (long)g, 1.0, slab[c], 1, pc, Z, (long)g, 1, 0.0, dst, (long)m, false, false, 6));
+        else
+          BBT_TRY(dgemm(ctx, false, false, pc, k, g, 1.0, slab[c], pc, Z, (long)g, 0.0, dst, (long)m));
+      } else {
+        BBT_TRY(dgemm(ctx, false, false, pc, k, g, 1.0, slab[c], pc, tmp, (long)g, 0.0, dst, (long)m));
+      }
+    }
+    if (mode == 4) {   // Sigma^-1 U^T y with the public mask on y (:1026-1045)
+      BBT_CUDA(ctx, cudaMemcpyAsync(ym, cfg->labels, m * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+      BBT_TRY(block_shift_mask(ctx, 1, m, MASK_PASSES, ym, true, false, cfg->public_seed));
+      BBT_TRY(dgemm(ctx, true, false, k, 1, (long)m, 1.0, Ulr, (long)m, ym, (long)m, 0.0, sut, k));
+      div_sigma<<<(k + 127) / 128, 128, 0, ctx->stream>>>(k, sigma, sut);
+      BBT_LAUNCHED(ctx);
+    } else {   // the public unmask of FinalU (:1098-1105)
+      BBT_TRY(block_shift_mask(ctx, (size_t)k, m, MASK_PASSES, Uout, false, false, cfg->public_seed));
+    }
+  }
+  // 7) V (:1119-1169): U2 = H (G^T U_b), global_n x k; participant c owns rows n_pos[c]..
+  if (compute_v) {
+    rot_sweep<<<(k + 127) / 128, 128, 0, ctx->stream>>>(gi, k, cs, Ub);
+    BBT_LAUNCHED(ctx);
+    BBT_TRY(ormqr_left_notrans(ctx, (long)g, gi, house, (long)g, 1, tauh, Ub, k, k, true, qp));
+    if (mode == 4)   // w = U2 Sigma^-1 U^T y (:1140)
+      BBT_TRY(dgemm(ctx, true, false, gi, 1, k, 1.0, Ub, k, sut, k, 0.0, wfull, (long)g));
+    for (int c = 0; c < P; ++c) {
+      const int nc = (int)L.n[c];
+      size_t bytes;
+      if (mode == 4) {   // w_c, unmasked with the private seed (:1141-1153)
+        BBT_CUDA(ctx, cudaMemcpyAsync(VT[c], wfull + L.npos[c], nc * sizeof(double), cudaMemcpyDeviceToDevice,
+                                      ctx->stream));
+        BBT_TRY(block_shift_mask(ctx, 1, (size_t)nc, MASK_PASSES, VT[c], false, false, cfg->private_seeds[c]));
+        bytes = (size_t)nc * sizeof(double);
+      } else {           // FinalVT_c = U2[rows of c]^T, unmasked (:1161-1166)
+        BBT_TRY(transpose(ctx, nc, k, Ub + L.npos[c] * k, k, VT[c], nc));
+        BBT_TRY(block_shift_mask(ctx, (size_t)k, (size_t)nc, MASK_PASSES, VT[c], false, false,
+                                 cfg->private_seeds[c]));
+        bytes = (size_t)k * nc * sizeof(double);
+      }
+      if (ctx->io_on && ctx->vt_dst[c]) {
+        BBT_CUDA(ctx, cudaEventRecord(ctx->vt_done[c], ctx->stream));
+        BBT_CUDA(ctx, cudaStreamWaitEvent(ctx->copy_out, ctx->vt_done[c], 0));
+        BBT_CUDA(ctx, cudaMemcpyAsync(ctx->vt_dst[c], VT[c], bytes, cudaMemcpyDeviceToHost, ctx->copy_out));
+      }
+    }
+  }
+  BBT_CUDA(ctx, cudaEventRecord(ev[6], ctx->stream));
+  BBT_CUDA(ctx, cudaEventSynchronize(ev[6]));
+  if (L.precision == 1) BBT_TRY(check_tc_flags(ctx, "fedsvd: tensor-core back-transform"));
+  // stage order of the reference's timers: local_qr, apply_mask, global_qr
+  // (here the repartition gather; this branch has no global QR), bi_diag,
+  // bsvd, combine_svd_remove_mask
+  const int from[6] = {2, 0, 1, 3, 4, 5}, to[6] = {3, 1, 2, 4, 5, 6};
+  for (int s = 0; s < 6; ++s) {
+    float ms = 0;
+    BBT_CUDA(ctx, cudaEventElapsedTime(&ms, ev[from[s]], ev[to[s]]));
+    ctx->stage_ms[s] = ms;
+  }
+  *kout = k;
+  return BBT_OK;
+}
+
 }  // namespace
 
 size_t fedsvd_workspace_bytes(const bbt_fedsvd_config* cfg) {
@@ -305,6 +626,10 @@ size_t fedsvd_workspace_bytes(const bbt_fedsvd_config* cfg) {
   bbt_ctx dummy;
   if (plan(&dummy, cfg, L) != BBT_OK) return 0;
   dummy.num_sms = 148;
+  if (L.tall) {
+    const Layout Q = slab_layout(L);
+    return tall_persistent_bytes(L, Q, cfg->svd_mode) + tall_scratch_bytes(&dummy, L, Q);
+  }
   return persistent_bytes(L) + scratch_bytes(&dummy, L);
 }
 
@@ -312,6 +637,7 @@ bbt_status fedsvd(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* X, 
                   double* Uout, double* const* VT, int* kout) {
   Layout L;
   BBT_TRY(plan(ctx, cfg, L));
+  if (L.tall) return fedsvd_tall(ctx, cfg, L, X, sigma, Uout, VT, kout);
   const int P = L.P;
   const size_t m = L.m, rg = L.rg;
   const int mi = (int)m;
@@ -411,7 +737,9 @@ bbt_status fedsvd(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* X, 
   // 3) repartition + global QR of M^T (client.cpp:681-794)
   for (int c = 0; c < P; ++c)
     BBT_TRY(copy2d(ctx, mi, (int)L.r[c], masked[c], (long)L.r[c], M + L.rpos[c], (long)rg));
-  if (L.precision == 1) {   // M <- Q_p, Q_g = Q_p W_g, R_g with dgeqrf's signs (mixedqr.cu)
+  if (rg == m) {   // m == global_n: no global QR, Ralha takes M^T (the in-place transpose, client.cpp:795-798)
+    BBT_TRY(transpose(ctx, mi, mi, M, (long)rg, W, (long)m));
+  } else if (L.precision == 1) {   // M <- Q_p, Q_g = Q_p W_g, R_g with dgeqrf's signs (mixedqr.cu)
     const size_t mark = ctx->ws.top;
     BBT_TRY(mixed_local_qr(ctx, mi, (long)rg, M, S, job.spitch, Rg, compute_v ? Wg : nullptr));
     ctx->ws.top = mark;
@@ -425,7 +753,7 @@ bbt_status fedsvd(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* X, 
   }
   BBT_CUDA(ctx, cudaEventRecord(ev[3], ctx->stream));
   // 4) Ralha bidiagonalisation, lower -> upper (client.cpp:801-954)
-  BBT_TRY(ralha(ctx, mi, W, house, tauh, alpha, beta, Vr, cs));
+  BBT_TRY(ralha(ctx, mi, mi, W, house, tauh, alpha, beta, Vr, cs));
   BBT_CUDA(ctx, cudaEventRecord(ev[4], ctx->stream));
   // 5) singular values / vectors (client.cpp:963-995)
   BBT_TRY(bidiag_bound(ctx, mi, alpha, beta, scal));
@@ -462,6 +790,17 @@ bbt_status fedsvd(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* X, 
     BBT_TRY(dgemm(ctx, false, true, mi, k, m, 1.0, Wg, (long)m, Ub, k, 0.0, Rg, (long)m));
   for (int c = 0; c < P; ++c) {   // :1179-1195
     const int rc = (int)L.r[c];
+    if (rg == m) {   // m == global_n: FinalVT_c = U2[rows of c]^T, unmasked (client.cpp:1161-1166)
+      BBT_TRY(transpose(ctx, rc, k, Ub + L.rpos[c] * k, k, VT[c], rc));
+      BBT_TRY(block_shift_mask(ctx, (size_t)k, (size_t)rc, MASK_PASSES, VT[c], false, false, cfg->private_seeds[c]));
+      if (ctx->io_on && ctx->vt_dst[c]) {
+        BBT_CUDA(ctx, cudaEventRecord(ctx->vt_done[c], ctx->stream));
+        BBT_CUDA(ctx, cudaStreamWaitEvent(ctx->copy_out, ctx->vt_done[c], 0));
+        BBT_CUDA(ctx, cudaMemcpyAsync(ctx->vt_dst[c], VT[c], (size_t)k * rc * sizeof(double), cudaMemcpyDeviceToHost,
+                                      ctx->copy_out));
+      }
+      continue;
+    }
     // tmp (k x r_c row-major) = U2^T Q_g[rows_c, :]^T  ==  column-major r_c x k = Q_g[rows_c,:] U2
     if (L.precision == 1)
       BBT_TRY(dgemm(ctx, false, false, rc, k, m, 1.0, M + L.rpos[c], (long)rg, Rg, (long)m, 0.0, tmp, rc));
@@ -515,8 +854,11 @@ __global__ void fill_hash(double* __restrict__ x, size_t n, unsigned seed) {
 // candidate on synthetic blocks of the configuration's shapes and keeps the
 // fastest for later fedsvd calls with the same shapes.
 bbt_status fedsvd_tune(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, int* best_streams, int* best_nb, double* best_ms) {
-  Layout L;
-  BBT_TRY(plan(ctx, cfg, L));
+  bbt_fedsvd_config shape = *cfg;   // the QRs depend on the shapes only
+  if (shape.svd_mode == 4) shape.svd_mode = 1;
+  Layout L0;
+  BBT_TRY(plan(ctx, &shape, L0));
+  const Layout L = L0.tall ? slab_layout(L0) : L0;   // the QRs this configuration runs
   const int P = L.P, mi = (int)L.m;
   std::vector<double*> blocks(P, nullptr);
   struct Free {
@@ -587,8 +929,8 @@ bbt_status fedsvd_tune(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, int* best_str
   cudaEventDestroy(e1);
   ctx->tuned_streams = bs;
   ctx->tuned_nb = bnb;
-  ctx->tuned_key = {L.m, (size_t)L.precision};
-  for (int c = 0; c < P; ++c) ctx->tuned_key.push_back(L.n[c]);
+  ctx->tuned_key = {L0.m, (size_t)L0.precision};
+  for (int c = 0; c < P; ++c) ctx->tuned_key.push_back(L0.n[c]);
   (void)mi;
   if (best_streams) *best_streams = bs;
   if (best_nb) *best_nb = bnb;

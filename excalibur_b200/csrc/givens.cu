@@ -285,6 +285,18 @@ bbt_status givens_mask(bbt_ctx* ctx, size_t m, size_t n, size_t passes, double* 
   return apply_tables(ctx, T, m, n, x, is_left);
 }
 
+size_t mask_workspace_bytes(size_t m, size_t n, size_t passes, bool is_left) {
+  const size_t k = is_left ? m : n, nvec = is_left ? n : m;
+  if (k <= 10000) return passes * (k + 2) * 24 + 1024;
+  size_t vm, vn, rem;
+  square_convert(k, &vm, &vn, &rem);
+  const size_t tables = passes * (std::max(vm + rem, vn) + 2) * 24 + 1024;
+  return nvec * (2 * vm * vn + vm + rem) * 8 + 3 * 256 + tables;
+}
+
+// The vectors of x (columns for is_left, rows otherwise) are masked
+// independently with the same rotation tables, so the virtual-matrix path
+// processes them in batches sized to the free workspace.
 bbt_status block_shift_mask(bbt_ctx* ctx, size_t m, size_t n, size_t passes, double* x, bool mask,
                             bool is_left, unsigned seed) {
   srand(seed);
@@ -292,65 +304,75 @@ bbt_status block_shift_mask(bbt_ctx* ctx, size_t m, size_t n, size_t passes, dou
   if (k <= 10000) return givens_mask(ctx, m, n, passes, x, mask, is_left, seed);
   size_t vm, vn, rem;
   square_convert(k, &vm, &vn, &rem);
-  const long nvec = (long)(is_left ? n : m);
+  const long nv_all = (long)(is_left ? n : m);
   const long vs = is_left ? 1 : (long)n, es = is_left ? (long)n : 1;
-  size_t mark = ctx->ws.top;
-  double* Z = ctx->ws.take<double>((size_t)nvec * vm * vn);
-  double* S = ctx->ws.take<double>((size_t)nvec * vm * vn);
-  double* Rb = ctx->ws.take<double>((size_t)nvec * (vm + rem));
-  if (!Rb) return fail(ctx, BBT_ERR_NOMEM, "block_shift_mask: workspace");
+  const size_t per_vec = (2 * vm * vn + vm + rem) * 8;
+  const size_t fixed = 3 * 256 + passes * (std::max(vm + rem, vn) + 2) * 24 + 2048;
+  const size_t room = ctx->ws.room();
+  const long batch = room > fixed ? (long)std::min<size_t>((size_t)nv_all, (room - fixed) / per_vec) : 0;
+  if (batch < 1)
+    return fail(ctx, BBT_ERR_NOMEM, "block_shift_mask: workspace (%zu bytes per vector of %zu)", per_vec, k);
+  const size_t mark = ctx->ws.top;
+  double* Z = ctx->ws.take<double>((size_t)batch * vm * vn);
+  double* S = ctx->ws.take<double>((size_t)batch * vm * vn);
+  double* Rb = ctx->ws.take<double>((size_t)batch * (vm + rem));
+  if (!Z || !S || !Rb) return fail(ctx, BBT_ERR_NOMEM, "block_shift_mask: workspace");
   const int thr = 256;
   const int grid = 4 * ctx->num_sms;
-  const size_t zr = (size_t)vm, zc = (size_t)nvec * vn;    // Z as LEFT target: vm x (nvec*vn)
-  const size_t yr = (size_t)vm * nvec, yc = vn;            // Z as right target: (vm*nvec) x vn
-  const size_t rw = vm + rem;
   const unsigned s1 = seed + 1000, s2 = seed + 2000, s3 = seed + 3000, s4 = seed + 4000, s5 = seed + 5000;
-  gather_body<<<grid, thr, 0, ctx->stream>>>(x, vs, es, nvec, (int)vm, (int)vn, mask ? Z : S);
-  BBT_LAUNCHED(ctx);
-  if (mask) {   // bbtsvd.cpp:560-613
-    if (rem) {
-      strip_io<<<grid, thr, 0, ctx->stream>>>(x, vs, es, nvec, (int)vm, (int)vn, (int)rem, Z, Rb, 1, 1);
+  for (long v0 = 0; v0 < nv_all; v0 += batch) {
+    const long nvec = std::min(batch, nv_all - v0);
+    double* xb = x + v0 * vs;
+    const size_t zr = (size_t)vm, zc = (size_t)nvec * vn;    // Z as LEFT target: vm x (nvec*vn)
+    const size_t yr = (size_t)vm * nvec, yc = vn;            // Z as right target: (vm*nvec) x vn
+    const size_t rw = vm + rem;
+    gather_body<<<grid, thr, 0, ctx->stream>>>(xb, vs, es, nvec, (int)vm, (int)vn, mask ? Z : S);
+    BBT_LAUNCHED(ctx);
+    if (mask) {   // bbtsvd.cpp:560-613
+      if (rem) {
+        strip_io<<<grid, thr, 0, ctx->stream>>>(xb, vs, es, nvec, (int)vm, (int)vn, (int)rem, Z, Rb, 1, 1);
+        BBT_LAUNCHED(ctx);
+        BBT_TRY(givens_mask(ctx, nvec, rw, passes, Rb, true, false, s1));
+        strip_io<<<grid, thr, 0, ctx->stream>>>(xb, vs, es, nvec, (int)vm, (int)vn, (int)rem, Z, Rb, 0, 0);
+        BBT_LAUNCHED(ctx);
+      }
+      BBT_TRY(givens_mask(ctx, zr, zc, passes, Z, true, true, s2));
+      shift_rows<<<grid, thr, 0, ctx->stream>>>(Z, S, nvec, (int)vm, (int)vn, 1);
       BBT_LAUNCHED(ctx);
-      BBT_TRY(givens_mask(ctx, nvec, rw, passes, Rb, true, false, s1));
-      strip_io<<<grid, thr, 0, ctx->stream>>>(x, vs, es, nvec, (int)vm, (int)vn, (int)rem, Z, Rb, 0, 0);
+      BBT_TRY(givens_mask(ctx, zr, zc, passes, S, true, true, s3));
+      BBT_TRY(givens_mask(ctx, yr, yc, passes, S, true, false, s4));
+      if (rem) {
+        strip_io<<<grid, thr, 0, ctx->stream>>>(xb, vs, es, nvec, (int)vm, (int)vn, (int)rem, S, Rb, 1, 0);
+        BBT_LAUNCHED(ctx);
+        BBT_TRY(givens_mask(ctx, nvec, rw, passes, Rb, true, false, s5));
+        strip_io<<<grid, thr, 0, ctx->stream>>>(xb, vs, es, nvec, (int)vm, (int)vn, (int)rem, S, Rb, 0, 1);
+        BBT_LAUNCHED(ctx);
+      }
+      scatter_body<<<grid, thr, 0, ctx->stream>>>(xb, vs, es, nvec, (int)vm, (int)vn, S);
+      BBT_LAUNCHED(ctx);
+    } else {      // bbtsvd.cpp:615-663
+      if (rem) {
+        strip_io<<<grid, thr, 0, ctx->stream>>>(xb, vs, es, nvec, (int)vm, (int)vn, (int)rem, S, Rb, 1, 1);
+        BBT_LAUNCHED(ctx);
+        BBT_TRY(givens_mask(ctx, nvec, rw, passes, Rb, false, false, s5));
+        strip_io<<<grid, thr, 0, ctx->stream>>>(xb, vs, es, nvec, (int)vm, (int)vn, (int)rem, S, Rb, 0, 0);
+        BBT_LAUNCHED(ctx);
+      }
+      BBT_TRY(givens_mask(ctx, zr, zc, passes, S, false, true, s3));
+      BBT_TRY(givens_mask(ctx, yr, yc, passes, S, false, false, s4));
+      shift_rows<<<grid, thr, 0, ctx->stream>>>(S, Z, nvec, (int)vm, (int)vn, 0);
+      BBT_LAUNCHED(ctx);
+      BBT_TRY(givens_mask(ctx, zr, zc, passes, Z, false, true, s2));
+      if (rem) {
+        strip_io<<<grid, thr, 0, ctx->stream>>>(xb, vs, es, nvec, (int)vm, (int)vn, (int)rem, Z, Rb, 1, 0);
+        BBT_LAUNCHED(ctx);
+        BBT_TRY(givens_mask(ctx, nvec, rw, passes, Rb, false, false, s1));
+        strip_io<<<grid, thr, 0, ctx->stream>>>(xb, vs, es, nvec, (int)vm, (int)vn, (int)rem, Z, Rb, 0, 1);
+        BBT_LAUNCHED(ctx);
+      }
+      scatter_body<<<grid, thr, 0, ctx->stream>>>(xb, vs, es, nvec, (int)vm, (int)vn, Z);
       BBT_LAUNCHED(ctx);
     }
-    BBT_TRY(givens_mask(ctx, zr, zc, passes, Z, true, true, s2));
-    shift_rows<<<grid, thr, 0, ctx->stream>>>(Z, S, nvec, (int)vm, (int)vn, 1);
-    BBT_LAUNCHED(ctx);
-    BBT_TRY(givens_mask(ctx, zr, zc, passes, S, true, true, s3));
-    BBT_TRY(givens_mask(ctx, yr, yc, passes, S, true, false, s4));
-    if (rem) {
-      strip_io<<<grid, thr, 0, ctx->stream>>>(x, vs, es, nvec, (int)vm, (int)vn, (int)rem, S, Rb, 1, 0);
-      BBT_LAUNCHED(ctx);
-      BBT_TRY(givens_mask(ctx, nvec, rw, passes, Rb, true, false, s5));
-      strip_io<<<grid, thr, 0, ctx->stream>>>(x, vs, es, nvec, (int)vm, (int)vn, (int)rem, S, Rb, 0, 1);
-      BBT_LAUNCHED(ctx);
-    }
-    scatter_body<<<grid, thr, 0, ctx->stream>>>(x, vs, es, nvec, (int)vm, (int)vn, S);
-    BBT_LAUNCHED(ctx);
-  } else {      // bbtsvd.cpp:615-663
-    if (rem) {
-      strip_io<<<grid, thr, 0, ctx->stream>>>(x, vs, es, nvec, (int)vm, (int)vn, (int)rem, S, Rb, 1, 1);
-      BBT_LAUNCHED(ctx);
-      BBT_TRY(givens_mask(ctx, nvec, rw, passes, Rb, false, false, s5));
-      strip_io<<<grid, thr, 0, ctx->stream>>>(x, vs, es, nvec, (int)vm, (int)vn, (int)rem, S, Rb, 0, 0);
-      BBT_LAUNCHED(ctx);
-    }
-    BBT_TRY(givens_mask(ctx, zr, zc, passes, S, false, true, s3));
-    BBT_TRY(givens_mask(ctx, yr, yc, passes, S, false, false, s4));
-    shift_rows<<<grid, thr, 0, ctx->stream>>>(S, Z, nvec, (int)vm, (int)vn, 0);
-    BBT_LAUNCHED(ctx);
-    BBT_TRY(givens_mask(ctx, zr, zc, passes, Z, false, true, s2));
-    if (rem) {
-      strip_io<<<grid, thr, 0, ctx->stream>>>(x, vs, es, nvec, (int)vm, (int)vn, (int)rem, Z, Rb, 1, 0);
-      BBT_LAUNCHED(ctx);
-      BBT_TRY(givens_mask(ctx, nvec, rw, passes, Rb, false, false, s1));
-      strip_io<<<grid, thr, 0, ctx->stream>>>(x, vs, es, nvec, (int)vm, (int)vn, (int)rem, Z, Rb, 0, 1);
-      BBT_LAUNCHED(ctx);
-    }
-    scatter_body<<<grid, thr, 0, ctx->stream>>>(x, vs, es, nvec, (int)vm, (int)vn, Z);
-    BBT_LAUNCHED(ctx);
   }
   ctx->ws.top = mark;
   return BBT_OK;

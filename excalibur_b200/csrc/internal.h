@@ -18,14 +18,20 @@ struct Arena {
   size_t top = 0;
   cudaError_t reserve(size_t bytes);   // grows (frees and reallocates) when needed
   void reset() { top = 0; }
+  // A failed take leaves the arena exhausted, so every later take of the same
+  // scope fails too and checking the last pointer of a group is enough.
   template <class T>
   T* take(size_t count) {
     size_t off = (top + 255) & ~size_t(255);
     size_t need = off + count * sizeof(T);
-    if (need > cap) return nullptr;
+    if (need > cap) {
+      top = cap;
+      return nullptr;
+    }
     top = need;
     return reinterpret_cast<T*>(base + off);
   }
+  size_t room() const { return top < cap ? cap - top : 0; }
 };
 
 }  // namespace bbt
@@ -153,6 +159,9 @@ bbt_status givens_mask(bbt_ctx* ctx, size_t m, size_t n, size_t passes, double* 
                        bool is_left, unsigned seed);
 bbt_status block_shift_mask(bbt_ctx* ctx, size_t m, size_t n, size_t passes, double* x, bool mask,
                             bool is_left, unsigned seed);
+// Workspace block_shift_mask uses to process every vector in one batch (it
+// splits the vectors into batches when less is free).
+size_t mask_workspace_bytes(size_t m, size_t n, size_t passes, bool is_left);
 
 // FP64 GEMM, column-major BLAS convention (dgemm.cu):
 //   C = alpha * op(A) * op(B) + beta * C,  op(A) M x K, op(B) K x N.
@@ -192,8 +201,10 @@ bbt_status refine_clusters(bbt_ctx* ctx, int n, int k, const double* a, const do
 // A (LAPACK dgebrd storage), one cooperative kernel (gebrd.cu).
 bbt_status gebrd(bbt_ctx* ctx, int n, double* A, double* d, double* e, double* tauq, double* taup);
 
-// Ralha one-sided bidiagonalisation of W (m x m row-major, overwritten) (ralha.cu).
-bbt_status ralha(bbt_ctx* ctx, int m, double* W, double* house, double* tau, double* alpha,
+// Ralha one-sided bidiagonalisation of W (m x n row-major, overwritten; the
+// participants' column slabs side by side); V (m x n) receives the left
+// vectors, house (m x m) the reflectors (ralha.cu).
+bbt_status ralha(bbt_ctx* ctx, int m, int n, double* W, double* house, double* tau, double* alpha,
                  double* beta, double* V, double* cs);
 
 // Small helpers (util.cu)

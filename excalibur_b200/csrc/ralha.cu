@@ -6,7 +6,10 @@
 // participants, a Householder reflector (dlarfg), its application to rows
 // i+1.. (dgemv + dger), and a Gram-Schmidt update of row i.  Here the
 // participants' column slabs sit side by side in one m x m row-major
-// matrix, so the all-reduce is the in-device reduction of each dot product,
+// matrix (m rows, n columns: n = m after the global QR of the short-and-wide
+// branch, n = sum_c min(m_part[c], global_n) in the tall-and-skinny branch,
+// client.cpp:805-814), so the all-reduce is the in-device reduction of each
+// dot product,
 // and a step is two grid-wide phases separated by bounded grid barriers:
 //
 //   B1 (column-partitioned, one CTA per SM, 8 columns x 32 row phases per
@@ -34,18 +37,18 @@ constexpr int RW = RT / 32;             // warps per CTA
 constexpr int CB = 8;                   // columns per pass of B1
 
 struct RalhaArgs {
-  int m;
-  double* W;       // m x m row-major, rows are the vectors
+  int m, n;
+  double* W;       // m x n row-major, rows are the vectors
   double* house;   // m x m row-major, zero on entry
   double* tau;     // m, zero on entry
   double* alpha;   // m
   double* beta;    // m-1 (lower bidiagonal)
-  double* V;       // m x m row-major, left vectors, zero on entry
+  double* V;       // m x n row-major, left vectors, zero on entry
   double* g;       // 2 x m: Gram rows, ping-pong between steps
   double* extra;   // 2 x 4: the four extra dots, ping-pong between steps
-  double* vt;      // m
-  double* tv;      // m: -tau * vt
-  double* nextw;   // m: row i+1 after the update
+  double* vt;      // n
+  double* tv;      // n: -tau * vt
+  double* nextw;   // n: row i+1 after the update
   unsigned* bar;   // [0] arrivals, [1] generation
   int* err;
 };
@@ -69,13 +72,13 @@ __device__ __forceinline__ double warp_sum(double v) {
 
 // Gram row for step i from rows r >= i+1 against row `piv`, into out.
 __device__ void gram_rows(const RalhaArgs& A, int i, const double* piv, double* out) {
-  const int m = A.m;
+  const int m = A.m, n = A.n;
   const int gw = blockIdx.x * RW + (threadIdx.x >> 5), lane = threadIdx.x & 31;
   const int nw = gridDim.x * RW;
   for (int r = i + 1 + gw; r < m; r += nw) {
-    const double* row = A.W + (long)r * m;
+    const double* row = A.W + (long)r * n;
     double s = 0.0;
-    for (int c = lane; c < m; c += 32) s += row[c] * piv[c];
+    for (int c = lane; c < n; c += 32) s += row[c] * piv[c];
     s = warp_sum(s);
     if (lane == 0) out[r - i - 1] = s;
   }
@@ -85,26 +88,26 @@ __global__ void __launch_bounds__(RT) ralha_kernel(RalhaArgs A) {
   __shared__ double sh[RW];
   __shared__ double scal[6];   // beta_{i-1}, alpha_i, tau, scale, 1/alpha_i
   __shared__ double red[RT / CB][CB + 1];
-  const int m = A.m;
+  const int m = A.m, n = A.n;
   const int tid = threadIdx.x;
   // ---- step 0 set-up: alpha_0, v_0 (CTA 0); Gram row of w_0 (all)
   if (blockIdx.x == 0) {
     double s = 0.0;
-    for (int c = tid; c < m; c += RT) s += A.W[c] * A.W[c];
+    for (int c = tid; c < n; c += RT) s += A.W[c] * A.W[c];
     s = block_sum(s, sh);
     const double a0 = sqrt(s);
     if (tid == 0) A.alpha[0] = a0;
     const double inv = 1.0 / a0;
-    for (int c = tid; c < m; c += RT) A.V[c] = inv * A.W[c];
+    for (int c = tid; c < n; c += RT) A.V[c] = inv * A.W[c];
     if (tid == 0) A.house[0] = 1.0;
   }
   gram_rows(A, 0, A.W, A.g);
   if (!grid_sync(A.bar, A.err)) return;
 
   // columns owned in B1
-  const int cw = (m + gridDim.x - 1) / gridDim.x;
+  const int cw = (n + gridDim.x - 1) / gridDim.x;
   const int c0 = blockIdx.x * cw;
-  const int c1 = min(m, c0 + cw);
+  const int c1 = min(n, c0 + cw);
 
   for (int i = 0; i + 2 < m; ++i) {
     const int len = m - 1 - i;   // g[0..len)
@@ -156,7 +159,7 @@ __global__ void __launch_bounds__(RT) ralha_kernel(RalhaArgs A) {
         if (c < c1)
           for (int t = tid / CB; t < len; t += RT / CB) {
             const double h = (t == 0) ? 1.0 : g[t] * scl;
-            s += h * A.W[(long)(i + 1 + t) * m + c];
+            s += h * A.W[(long)(i + 1 + t) * n + c];
           }
         red[tid / CB][tid % CB] = s;
         __syncthreads();
@@ -167,16 +170,16 @@ __global__ void __launch_bounds__(RT) ralha_kernel(RalhaArgs A) {
           A.vt[cc] = v;
           const double tvv = -ta * v;
           A.tv[cc] = tvv;
-          A.nextw[cc] = A.W[(long)(i + 1) * m + cc] + tvv;   // h_0 = 1
+          A.nextw[cc] = A.W[(long)(i + 1) * n + cc] + tvv;   // h_0 = 1
         }
         __syncthreads();
       }
       if (i > 0) {
         const double b = scal[0], inva = scal[4];
         for (int c = c0 + tid; c < c1; c += RT) {
-          const double w = A.W[(long)i * m + c] + (-b) * A.V[(long)(i - 1) * m + c];
-          A.W[(long)i * m + c] = w;
-          A.V[(long)i * m + c] = inva * w;
+          const double w = A.W[(long)i * n + c] + (-b) * A.V[(long)(i - 1) * n + c];
+          A.W[(long)i * n + c] = w;
+          A.V[(long)i * n + c] = inva * w;
         }
       }
     }
@@ -188,9 +191,9 @@ __global__ void __launch_bounds__(RT) ralha_kernel(RalhaArgs A) {
       for (int r = i + 1 + gw; r < m; r += nw) {
         const int t = r - i - 1;
         const double h = (t == 0) ? 1.0 : g[t] * scl;
-        double* row = A.W + (long)r * m;
+        double* row = A.W + (long)r * n;
         double s = 0.0;
-        for (int c = lane; c < m; c += 32) {
+        for (int c = lane; c < n; c += 32) {
           const double w = row[c] + A.tv[c] * h;
           row[c] = w;
           s += w * A.nextw[c];
@@ -202,8 +205,8 @@ __global__ void __launch_bounds__(RT) ralha_kernel(RalhaArgs A) {
       if (blockIdx.x == 0) {
         // extras for step i+1: w_{i+1}.v_i, v_i.v_i, w_{i+1}.w_{i+1}, v_i.w_{i+1}
         double s0 = 0.0, s1 = 0.0, s2 = 0.0;
-        const double* v = A.V + (long)i * m;
-        for (int c = tid; c < m; c += RT) {
+        const double* v = A.V + (long)i * n;
+        for (int c = tid; c < n; c += RT) {
           const double w = A.nextw[c];
           s0 += w * v[c];
           s1 += v[c] * v[c];
@@ -220,13 +223,13 @@ __global__ void __launch_bounds__(RT) ralha_kernel(RalhaArgs A) {
   // ---- tail steps i = m-2, m-1 (client.cpp:897-905), CTA 0
   if (blockIdx.x != 0) return;
   for (int i = (m >= 3 ? m - 2 : 1); i < m; ++i) {
-    const double* vp = A.V + (long)(i - 1) * m;
-    double* wi = A.W + (long)i * m;
+    const double* vp = A.V + (long)(i - 1) * n;
+    double* wi = A.W + (long)i * n;
     double s = 0.0;
-    for (int c = tid; c < m; c += RT) s += wi[c] * vp[c];
+    for (int c = tid; c < n; c += RT) s += wi[c] * vp[c];
     const double b = block_sum(s, sh);
     double q = 0.0;
-    for (int c = tid; c < m; c += RT) {
+    for (int c = tid; c < n; c += RT) {
       const double w = wi[c] + (-b) * vp[c];
       wi[c] = w;
       q += w * w;
@@ -234,7 +237,7 @@ __global__ void __launch_bounds__(RT) ralha_kernel(RalhaArgs A) {
     q = block_sum(q, sh);
     const double a = sqrt(q);
     const double inv = 1.0 / a;
-    for (int c = tid; c < m; c += RT) A.V[(long)i * m + c] = inv * wi[c];
+    for (int c = tid; c < n; c += RT) A.V[(long)i * n + c] = inv * wi[c];
     if (tid == 0) { A.beta[i - 1] = b; A.alpha[i] = a; }
     __syncthreads();
   }
@@ -273,12 +276,14 @@ __global__ void lower_to_upper_kernel(int m, double* __restrict__ alpha, double*
 
 }  // namespace
 
-bbt_status ralha(bbt_ctx* ctx, int m, double* W, double* house, double* tau, double* alpha,
+bbt_status ralha(bbt_ctx* ctx, int m, int n, double* W, double* house, double* tau, double* alpha,
                  double* beta, double* V, double* cs) {
   if (m < 3) return fail(ctx, BBT_ERR_UNSUPPORTED, "ralha: m=%d (the reference needs m >= 3)", m);
+  if (n < 1) return fail(ctx, BBT_ERR_ARG, "ralha: n=%d", n);
   size_t mark = ctx->ws.top;
   RalhaArgs A;
   A.m = m;
+  A.n = n;
   A.W = W;
   A.house = house;
   A.tau = tau;
@@ -287,26 +292,26 @@ bbt_status ralha(bbt_ctx* ctx, int m, double* W, double* house, double* tau, dou
   A.V = V;
   A.g = ctx->ws.take<double>(2 * (size_t)m);
   A.extra = ctx->ws.take<double>(8);
-  A.vt = ctx->ws.take<double>(m);
-  A.tv = ctx->ws.take<double>(m);
-  A.nextw = ctx->ws.take<double>(m);
+  A.vt = ctx->ws.take<double>(n);
+  A.tv = ctx->ws.take<double>(n);
+  A.nextw = ctx->ws.take<double>(n);
   if (!A.nextw) return fail(ctx, BBT_ERR_NOMEM, "ralha: workspace");
   A.bar = ctx->d_barrier;
   A.err = ctx->d_flag;
   BBT_CUDA(ctx, cudaMemsetAsync(house, 0, (size_t)m * m * sizeof(double), ctx->stream));
-  BBT_CUDA(ctx, cudaMemsetAsync(V, 0, (size_t)m * m * sizeof(double), ctx->stream));
+  BBT_CUDA(ctx, cudaMemsetAsync(V, 0, (size_t)m * n * sizeof(double), ctx->stream));
   BBT_CUDA(ctx, cudaMemsetAsync(tau, 0, (size_t)m * sizeof(double), ctx->stream));
   BBT_CUDA(ctx, cudaMemsetAsync(ctx->d_barrier, 0, 2 * sizeof(unsigned), ctx->stream));
   BBT_CUDA(ctx, cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), ctx->stream));
   int per_sm = 0;
   BBT_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ralha_kernel, RT, 0));
   if (per_sm < 1) return fail(ctx, BBT_ERR_CUDA, "ralha: kernel does not fit an SM");
-  int grid = (m + CB - 1) / CB;             // at least CB columns per CTA in B1, one CTA per SM
+  int grid = (n + CB - 1) / CB;             // at least CB columns per CTA in B1, one CTA per SM
   if (grid > ctx->num_sms * per_sm) grid = ctx->num_sms * per_sm;
   if (grid > ctx->num_sms) grid = ctx->num_sms;
   if (grid < 1) grid = 1;
   void* args[] = {&A};
-  ProfScope prof(ctx, BBT_PROF_RALHA, 16.0 * (double)m * m * m / 3.0);
+  ProfScope prof(ctx, BBT_PROF_RALHA, 16.0 * (double)m * m * n / 3.0);
   BBT_CUDA(ctx, cudaLaunchCooperativeKernel((void*)ralha_kernel, dim3(grid), dim3(RT), args, 0, ctx->stream));
   BBT_LAUNCHED(ctx);
   lower_to_upper_kernel<<<1, 1, 0, ctx->stream>>>(m, alpha, beta, cs);

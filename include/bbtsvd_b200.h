@@ -234,13 +234,24 @@ bbt_status bbt_svd_dense(bbt_ctx* ctx, int m, double* d_X, int top_k, double* d_
                          double* d_VT, int* h_k);
 
 /* ---- whole pipeline ------------------------------------------------------
- * DecentralizedClient::run() (client.cpp:447-1200), short-and-wide branch
- * (m <= global_n), svd_mode 1 (two-sided) with opt_control 3, for P
+ * DecentralizedClient::run() (client.cpp:447-1200) with opt_control 3, for P
  * participants held as separate device buffers on one GPU; the socket
- * all-reduce / all-gather become in-device reductions.                     */
+ * all-reduce / all-gather become in-device reductions.  Both branches of the
+ * reference:
+ *   short-and-wide, m <= global_n (client.cpp:570-606, 680-800, 1174-1195):
+ *     block c is X_c, row-major m x local_n[c]; local QR of blocks with
+ *     local_n / m > 5, global QR of the masked blocks (none when
+ *     m == global_n), Ralha of the m x m result;
+ *   tall-and-skinny, m > global_n (client.cpp:543-568, 627-679, 1119-1169):
+ *     block c is X_c^T, row-major local_n[c] x m (the reference's file layout
+ *     in this branch); the masked blocks are repartitioned into column slabs
+ *     of m_part[c] rows of X, slabs with m_part[c] > global_n are reduced by
+ *     a local QR, and Ralha runs on the global_n x sum_c min(m_part[c],
+ *     global_n) concatenation.
+ * The global matrix is X = [X_0 | X_1 | ...] (m x global_n) in both. */
 typedef struct {
   int participants;              /* P >= 1 */
-  size_t m;                      /* rows of every block (reference: m) */
+  size_t m;                      /* rows of X (reference: m) */
   const size_t* local_n;         /* P column counts (reference: local_n) */
   unsigned public_seed;          /* shared mask seed (client.cpp:498) */
   const unsigned* private_seeds; /* P private mask seeds (client.cpp:531) */
@@ -248,17 +259,25 @@ typedef struct {
   int svd_mode;                  /* client.cpp:186-192: 0 full SVD (the reference calls dbdsdc on the
                                     leading k x k bidiagonal; here bisection + twisted vectors on it),
                                     1 two-sided, 2 left vectors only (no FinalVT), 3 right vectors
-                                    only (no FinalU) */
+                                    only (no FinalU), 4 linear regression (tall-and-skinny only, as in
+                                    the reference, client.cpp:1023-1160): w = V diag(1/sigma) U^T y,
+                                    the least-squares solution of X w = y, returned per participant
+                                    in place of FinalVT; no FinalU */
   int precision;                 /* 0: plain FP64 (the reference's Householder local QR);
                                     1: mixed -- local QR by a BF16x3 tensor-core sketch
                                     and one FP64 Cholesky-QR refinement pass */
+  const double* labels;          /* svd_mode 4: y, m values (device memory for bbt_fedsvd_run, host
+                                    memory for bbt_fedsvd_run_host; the reference's y.mat, held by
+                                    the last participant); NULL otherwise */
 } bbt_fedsvd_config;
 
-/* Device-resident run.  d_blocks[c]: row-major m x local_n[c] input, used as
- * workspace (overwritten).  Outputs: d_sigma[m], d_U row-major m x k (the
- * reference's FinalU; may be NULL in svd_mode 3), d_VT[c] row-major
- * k x local_n[c] (FinalVT; d_VT may be NULL in svd_mode 2); *h_k is the
- * number of singular values k.  Replaces client.cpp:572-1199. */
+/* Device-resident run.  d_blocks[c]: participant c's input in the branch's
+ * layout (above), used as workspace (overwritten).  Outputs: d_sigma
+ * (min(m, global_n) values), d_U = FinalU, row-major m x k (short-and-wide)
+ * or k x m (tall-and-skinny, client.cpp:1071-1105); may be NULL in
+ * svd_modes 3 and 4), d_VT[c] = FinalVT_c, row-major k x local_n[c] (d_VT may
+ * be NULL in svd_mode 2), or in svd_mode 4 w_c (local_n[c] values);
+ * *h_k is the number of singular values k.  Replaces client.cpp:543-1199. */
 bbt_status bbt_fedsvd_run(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* d_blocks,
                           double* d_sigma, double* d_U, double* const* d_VT, int* h_k);
 

@@ -1,7 +1,9 @@
 """ORACLE — test infrastructure, not product code.
 
-numpy restatement of Excalibur's ``DecentralizedClient::run()`` for the
-short-and-wide branch (m <= global_n, ``src/client.cpp:570-606, 680-1199``),
+numpy restatement of Excalibur's ``DecentralizedClient::run()``: the
+short-and-wide branch (m <= global_n, ``src/client.cpp:570-606, 680-1199``,
+``run``) and the tall-and-skinny branch with its linear-regression mode
+(m > global_n, ``src/client.cpp:543-568, 627-679, 1002-1169``, ``run_tall``),
 with all P participants held in one process.  The reference's socket
 collectives become plain array operations; its ``ring_all_reduce_sum``
 becomes a sum over participants in index order.
@@ -282,6 +284,8 @@ def run(blocks, public_seed, private_seeds, top_k=-1, svd_mode=1, return_stages=
     global_n = sum(local_n)
     if m > global_n:
         raise ValueError("m > global_n: the tall-and-skinny branch takes transposed blocks (run_tall)")
+    if svd_mode == 4:
+        raise ValueError("svd_mode 4 exists only in the tall-and-skinny branch (client.cpp:1180)")
     red = [reduced_width(m, n) for n in local_n]
     rg = sum(red)
     if rg <= m and m < global_n:
