@@ -13,6 +13,7 @@ raises if the library or a GPU is missing.
     sigma, U, VT = ctx.fedsvd(blocks, public_seed, private_seeds)
 """
 import ctypes as C
+import os
 
 import numpy as np
 
@@ -411,6 +412,28 @@ class Context:
         k = C.c_int(0)
         self._check(self.L.bbt_fedsvd_run_host(self.h, C.byref(cfg), bp, C.c_void_p(sig.ctypes.data),
                                                C.c_void_p(U.ctypes.data), vp, C.byref(k)), "fedsvd_host")
+        k = k.value
+        Uo, VTo = self._outputs(U, VT, m, ln, k, svd_mode, tall)
+        return sig[:k], Uo, VTo
+
+    def fedsvd_files(self, dpath, m, local_n, public_seed, private_seeds, top_k=-1, svd_mode=1, precision=0,
+                     out=None):
+        """The pipeline on the reference's on-disk input (bbt_fedsvd_run_files):
+        dpath/Client<c>.mat (m * local_n[c] float64 in the branch's layout,
+        see excalibur_b200.datafiles) and, in svd_mode 4, dpath/y.mat.
+        Returns numpy results as fedsvd_host."""
+        P = len(local_n)
+        ln = [int(n) for n in local_n]
+        tall = m > sum(ln)
+        kmax = min(m, sum(ln))
+        cfg = self._config(m, ln, public_seed, private_seeds, top_k, svd_mode, precision)
+        if out is None:
+            out = (np.empty(kmax), np.empty(m * kmax), [np.empty(m * n) for n in ln])
+        sig, U, VT = out
+        vp = (C.c_void_p * P)(*[v.ctypes.data for v in VT])
+        k = C.c_int(0)
+        self._check(self.L.bbt_fedsvd_run_files(self.h, C.byref(cfg), os.fsencode(dpath), C.c_void_p(sig.ctypes.data),
+                                                C.c_void_p(U.ctypes.data), vp, C.byref(k)), "fedsvd_files")
         k = k.value
         Uo, VTo = self._outputs(U, VT, m, ln, k, svd_mode, tall)
         return sig[:k], Uo, VTo

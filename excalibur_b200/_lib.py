@@ -12,14 +12,14 @@ LIBPATH = os.path.join(HERE, "libexcalibur_b200.so")
 
 BBT_OK = 0
 STATUS = {0: "BBT_OK", 1: "BBT_ERR_ARG", 2: "BBT_ERR_CUDA", 3: "BBT_ERR_COUNT", 4: "BBT_ERR_NOMEM",
-          5: "BBT_ERR_TIMEOUT", 6: "BBT_ERR_UNSUPPORTED", 7: "BBT_ERR_NUMERIC"}
+          5: "BBT_ERR_TIMEOUT", 6: "BBT_ERR_UNSUPPORTED", 7: "BBT_ERR_NUMERIC", 8: "BBT_ERR_IO"}
 
 # Every extern "C" symbol declared in include/bbtsvd_b200.h.
 EXPORTS = (
     "bbt_create", "bbt_destroy", "bbt_set_stream", "bbt_synchronize", "bbt_last_error",
     "bbt_status_string", "bbt_kernel_launches", "bbt_negative_count", "bbt_bisection",
     "bbt_twisted_vectors", "bbt_bidiagonal_svd", "bbt_givens_mask", "bbt_block_shift_mask",
-    "bbt_local_qr", "bbt_fedsvd_run", "bbt_fedsvd_run_host", "bbt_fedsvd_stage_ms",
+    "bbt_local_qr", "bbt_fedsvd_run", "bbt_fedsvd_run_host", "bbt_fedsvd_run_files", "bbt_fedsvd_stage_ms",
     "bbt_dgemm", "bbt_profile", "bbt_profile_get", "bbt_twisted_vectors_noalloc",
     "bbt_svd_dense", "bbt_fedsvd_tune", "bbt_rademacher", "bbt_sketch_bf16x3", "bbt_mixed_local_qr",
     "bbt_mlp_param_count", "bbt_mlp_features", "bbt_mlp_forward", "bbt_mlp_grad", "bbt_mlp_adam",
@@ -73,6 +73,7 @@ def load():
         "bbt_local_qr": ([vp, st, st, vp, vp, i], i),
         "bbt_fedsvd_run": ([vp, C.POINTER(FedSVDConfig), vp, vp, vp, vp, C.POINTER(i)], i),
         "bbt_fedsvd_run_host": ([vp, C.POINTER(FedSVDConfig), vp, vp, vp, vp, C.POINTER(i)], i),
+        "bbt_fedsvd_run_files": ([vp, C.POINTER(FedSVDConfig), C.c_char_p, vp, vp, vp, C.POINTER(i)], i),
         "bbt_fedsvd_stage_ms": ([vp, vp, i], i),
         "bbt_dgemm": ([vp, i, i, i, i, C.c_long, d, vp, C.c_long, vp, C.c_long, d, vp, C.c_long], i),
         "bbt_profile": ([vp, i], i),

@@ -1,6 +1,6 @@
 // extern "C" entry points (include/bbtsvd_b200.h): argument checks, context
-// and workspace management, host<->device staging for the host-pointer
-// pipeline entry.  All arithmetic is in the kernels of the other sources.
+// and workspace management (the host-buffer and file entries of the pipeline
+// are in hostio.cu).  All arithmetic is in the kernels of the other sources.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -75,6 +75,7 @@ const char* bbt_status_string(bbt_status s) {
     case BBT_ERR_TIMEOUT: return "device-side wait timed out";
     case BBT_ERR_UNSUPPORTED: return "unsupported shape or mode";
     case BBT_ERR_NUMERIC: return "Cholesky breakdown in the mixed-precision local QR";
+    case BBT_ERR_IO: return "input file missing, of the wrong size or unreadable";
   }
   return "unknown status";
 }
@@ -118,6 +119,9 @@ bbt_status bbt_destroy(bbt_ctx* ctx) {
   if (ctx->copy_out) cudaStreamDestroy(ctx->copy_out);
   for (auto e : ctx->in_ready) cudaEventDestroy(e);
   for (auto e : ctx->vt_done) cudaEventDestroy(e);
+  if (ctx->io_pinned) cudaFreeHost(ctx->io_pinned);
+  for (auto e : ctx->io_stage_ev)
+    if (e) cudaEventDestroy(e);
   if (ctx->own) cudaStreamDestroy(ctx->own);
   delete ctx;
   return BBT_OK;
@@ -309,79 +313,6 @@ bbt_status bbt_fedsvd_run(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* co
   for (int c = 0; c < cfg->participants; ++c)
     if (bad(blocks[c]) || (want_v && bad(VT[c]))) return fail(ctx, BBT_ERR_ARG, "fedsvd: participant %d buffer", c);
   return fedsvd(ctx, cfg, blocks, sigma, U, VT, k);
-}
-
-bbt_status bbt_fedsvd_run_host(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, const double* const* hX,
-                               double* hsigma, double* hU, double* const* hVT, int* k) {
-  if (!ctx) return BBT_ERR_ARG;
-  if (!cfg || !hX || !k || !hsigma || cfg->participants < 1 || !cfg->local_n)
-    return fail(ctx, BBT_ERR_ARG, "fedsvd_host: NULL argument");
-  const bool lr = cfg->svd_mode == 4;
-  const bool want_u = cfg->svd_mode != 3 && !lr, want_v = cfg->svd_mode != 2;
-  if ((want_u && !hU) || (want_v && !hVT) || (lr && !cfg->labels))
-    return fail(ctx, BBT_ERR_ARG, "fedsvd_host: NULL output");
-  const int P = cfg->participants;
-  const size_t m = cfg->m;
-  size_t gn = 0;
-  for (int c = 0; c < P; ++c) gn += cfg->local_n[c];
-  const size_t kmax = std::min(m, gn);   // singular values: the bidiagonal's order
-  // staging in a grow-only arena kept by the context (no allocation per call)
-  size_t need = (m + 2 * kmax + m * kmax) * sizeof(double) + 8192;
-  for (int c = 0; c < P; ++c) need += (want_v ? 2 : 1) * (m * cfg->local_n[c] * sizeof(double) + 256);
-  if (ctx->io_ws.cap < need) BBT_CUDA(ctx, ctx->io_ws.reserve(need));
-  ctx->io_ws.reset();
-  std::vector<double*> dX(P), dVT(P, nullptr);
-  for (int c = 0; c < P; ++c) {
-    dX[c] = ctx->io_ws.take<double>(m * cfg->local_n[c]);
-    if (want_v) dVT[c] = ctx->io_ws.take<double>(m * cfg->local_n[c]);
-  }
-  double* ds = ctx->io_ws.take<double>(kmax);
-  double* dU = ctx->io_ws.take<double>(m * kmax);
-  double* dy = lr ? ctx->io_ws.take<double>(m) : nullptr;
-  if (!ctx->copy_in) BBT_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->copy_in, cudaStreamNonBlocking));
-  if (!ctx->copy_out) BBT_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->copy_out, cudaStreamNonBlocking));
-  while ((int)ctx->in_ready.size() < P) {
-    cudaEvent_t a, b;
-    BBT_CUDA(ctx, cudaEventCreateWithFlags(&a, cudaEventDisableTiming));
-    BBT_CUDA(ctx, cudaEventCreateWithFlags(&b, cudaEventDisableTiming));
-    ctx->in_ready.push_back(a);
-    ctx->vt_done.push_back(b);
-  }
-  // the copy streams start after all earlier work on the context's stream
-  BBT_CUDA(ctx, cudaEventRecord(ctx->vt_done[0], ctx->stream));
-  BBT_CUDA(ctx, cudaStreamWaitEvent(ctx->copy_in, ctx->vt_done[0], 0));
-  BBT_CUDA(ctx, cudaStreamWaitEvent(ctx->copy_out, ctx->vt_done[0], 0));
-  for (int c = 0; c < P; ++c) {   // participant by participant: the first QR starts after one block
-    BBT_CUDA(ctx, cudaMemcpyAsync(dX[c], hX[c], m * cfg->local_n[c] * sizeof(double), cudaMemcpyHostToDevice,
-                                  ctx->copy_in));
-    BBT_CUDA(ctx, cudaEventRecord(ctx->in_ready[c], ctx->copy_in));
-  }
-  bbt_fedsvd_config dcfg = *cfg;
-  if (lr) {   // the labels follow the blocks on the copy stream
-    BBT_CUDA(ctx, cudaMemcpyAsync(dy, cfg->labels, m * sizeof(double), cudaMemcpyHostToDevice, ctx->copy_in));
-    BBT_CUDA(ctx, cudaEventRecord(ctx->in_ready[P - 1], ctx->copy_in));
-    dcfg.labels = dy;
-  }
-  ctx->vt_dst.assign(P, nullptr);
-  if (want_v)
-    for (int c = 0; c < P; ++c) ctx->vt_dst[c] = hVT[c];   // copied out by the pipeline as each is done
-  ctx->io_on = true;
-  bbt_status st = fedsvd(ctx, &dcfg, dX.data(), ds, dU, dVT.data(), k);
-  ctx->io_on = false;
-  cudaError_t e = cudaSuccess;
-  if (st == BBT_OK) {
-    const int kk = *k;
-    e = cudaMemcpyAsync(hsigma, ds, kk * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
-    if (e == cudaSuccess && want_u)
-      e = cudaMemcpyAsync(hU, dU, m * kk * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-    if (e != cudaSuccess) st = cuda_fail(ctx, e, "fedsvd_host: copy-out");
-  }
-  // every copy issued on the copy streams has finished before the buffers may be reused
-  const cudaError_t e1 = cudaStreamSynchronize(ctx->copy_in), e2 = cudaStreamSynchronize(ctx->copy_out);
-  if (st == BBT_OK && e1 != cudaSuccess) st = cuda_fail(ctx, e1, "fedsvd_host: copy-in");
-  if (st == BBT_OK && e2 != cudaSuccess) st = cuda_fail(ctx, e2, "fedsvd_host: copy-out");
-  return st;
 }
 
 bbt_status bbt_dgemm(bbt_ctx* ctx, int transa, int transb, int M, int N, long K, double alpha, const double* A,

@@ -313,13 +313,13 @@ bbt_status local_qr_stage(bbt_ctx* ctx, const Layout& L, double* const* X, const
   if (streams <= 1) {
     for (int c = 0; c < L.P; ++c)
       if (L.qr[c]) {
-        if (ctx->io_on) BBT_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->in_ready[c], 0));
+        if (ctx->io_on) BBT_TRY(wait_input(ctx, c));
         BBT_TRY(qr_one(ctx, mi, X[c], (long)L.n[c], c, job, qp));
       }
     return BBT_OK;
   }
   if (ctx->io_on)   // the batched schedule (and its graph) starts once every block has arrived
-    for (int c = 0; c < L.P; ++c) BBT_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->in_ready[c], 0));
+    for (int c = 0; c < L.P; ++c) BBT_TRY(wait_input(ctx, c));
   std::vector<size_t> key = {L.m, (size_t)job.compute_v, (size_t)streams, (size_t)qp.nb, (size_t)ctx->ws.base,
                              ctx->ws.cap, ctx->ws.top, (size_t)job.precision, (size_t)job.S};
   for (int c = 0; c < L.P; ++c) {
@@ -489,7 +489,7 @@ bbt_status fedsvd_tall(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, const Layout&
   BBT_CUDA(ctx, cudaEventRecord(ev[0], ctx->stream));
   // 1) masks: private on the left (rows of X_c^T), public on the right (:548-551)
   for (int c = 0; c < P; ++c) {
-    if (ctx->io_on) BBT_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->in_ready[c], 0));
+    if (ctx->io_on) BBT_TRY(wait_input(ctx, c));
     BBT_TRY(block_shift_mask(ctx, L.n[c], m, MASK_PASSES, X[c], true, true, cfg->private_seeds[c]));
     BBT_TRY(block_shift_mask(ctx, L.n[c], m, MASK_PASSES, X[c], true, false, cfg->public_seed));
   }
@@ -726,7 +726,7 @@ bbt_status fedsvd(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* X, 
   }
   if (L.precision == 1) BBT_TRY(check_tc_flags(ctx, "fedsvd: mixed-precision local QR"));
   if (ctx->io_on)
-    for (int c = 0; c < P; ++c) BBT_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->in_ready[c], 0));
+    for (int c = 0; c < P; ++c) BBT_TRY(wait_input(ctx, c));
   BBT_CUDA(ctx, cudaEventRecord(ev[1], ctx->stream));
   // 2) masks (client.cpp:593-596)
   for (int c = 0; c < P; ++c) {

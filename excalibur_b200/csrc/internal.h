@@ -81,6 +81,12 @@ struct bbt_ctx {
   bool io_on = false;
   std::vector<cudaEvent_t> in_ready, vt_done;
   std::vector<double*> vt_dst;
+  // file entry: two pinned staging buffers and their copy events; the gate
+  // blocks until participant c's input has been read and its copy enqueued
+  void* io_pinned = nullptr;
+  cudaEvent_t io_stage_ev[2] = {nullptr, nullptr};
+  bool (*io_gate)(void*, int) = nullptr;
+  void* io_gate_arg = nullptr;
 };
 
 namespace bbt {
@@ -90,6 +96,9 @@ namespace bbt {
 enum { FLAG_SKETCH = 4, FLAG_CHOL = 5 };
 
 bbt_status fail(bbt_ctx* ctx, bbt_status s, const char* fmt, ...);
+// Order ctx->stream after participant c's input (host-entry runs): passes the
+// file gate first, then waits on ctx->in_ready[c] (hostio.cu).
+bbt_status wait_input(bbt_ctx* ctx, int c);
 bbt_status cuda_fail(bbt_ctx* ctx, cudaError_t e, const char* what);
 
 #define BBT_CUDA(ctx, call)                                   \

@@ -39,8 +39,9 @@ typedef enum {
   BBT_ERR_NOMEM = 4,        /* device allocation failed */
   BBT_ERR_TIMEOUT = 5,      /* a bounded device-side wait gave up */
   BBT_ERR_UNSUPPORTED = 6,  /* shape or mode outside what the reference supports */
-  BBT_ERR_NUMERIC = 7       /* a Cholesky pivot of the mixed-precision local QR was not
+  BBT_ERR_NUMERIC = 7,      /* a Cholesky pivot of the mixed-precision local QR was not
                                positive (rank-deficient block); rerun with precision 0 */
+  BBT_ERR_IO = 8            /* an input file is missing, of the wrong size or unreadable */
 } bbt_status;
 
 typedef struct bbt_ctx bbt_ctx;
@@ -286,6 +287,19 @@ bbt_status bbt_fedsvd_run(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* co
 bbt_status bbt_fedsvd_run_host(bbt_ctx* ctx, const bbt_fedsvd_config* cfg,
                                const double* const* h_blocks, double* h_sigma, double* h_U,
                                double* const* h_VT, int* h_k);
+
+/* Same with the reference's on-disk input (client.cpp:210-213, 1028;
+ * utils.cpp:237-252): participant c's block is read from
+ * <dpath>/Client<c>.mat, raw float64 of m * local_n[c] values in the branch's
+ * layout (row-major m x local_n[c], or local_n[c] x m when m > global_n, as the
+ * reference's generate_data.cpp writes them), and in svd_mode 4 the labels
+ * from <dpath>/y.mat (m values; cfg->labels is ignored).  Files are checked
+ * before any work starts; a missing or wrongly sized file returns BBT_ERR_IO
+ * with its name.  A host thread reads them through pinned staging while the
+ * GPU works on the participants already read.  Outputs as
+ * bbt_fedsvd_run_host. */
+bbt_status bbt_fedsvd_run_files(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, const char* dpath,
+                                double* h_sigma, double* h_U, double* const* h_VT, int* h_k);
 
 /* Autotuner of the batched local QR (the QR of every participant with
  * local_n / m > 5, client.cpp:572-589, issued on concurrent streams and
