@@ -455,6 +455,60 @@ class Context:
         self.sync()
         return C
 
+    def dgemm_crt(self, A, B, alpha=1.0, beta=0.0, C=None, bits=53):
+        """C (M x N) = alpha A^T B + beta C for column-major A (K x M) and B
+        (K x N) -- row-major tensors of M x K and N x K -- from exact integer
+        products on the int8 tensor cores (operand rows rounded to `bits`
+        bits).  C is returned as a row-major N x M tensor (its column-major
+        transpose), as dgemm does."""
+        M, K = A.shape
+        N, K2 = B.shape
+        assert K == K2, (K, K2)
+        if C is None:
+            C = self._empty(N, M)
+        self._pre()
+        self._check(self.L.bbt_dgemm_crt(self.h, M, N, K, alpha, self._p(A), A.shape[1], self._p(B), B.shape[1], beta,
+                                         self._p(C), C.shape[1], bits), "dgemm_crt")
+        self.sync()
+        return C
+
+    def gram_dd(self, X):
+        """Upper triangle of G = X X^T (X row-major m x n, CUDA float64) as a
+        double-double (Gh, Gl), each a row-major m x m tensor holding the
+        column-major matrix (entries strictly below the diagonal undefined)."""
+        m, n = X.shape
+        Gh, Gl = self._empty(m, m), self._empty(m, m)
+        self._pre()
+        self._check(self.L.bbt_gram_dd(self.h, m, n, self._p(X), X.shape[1], self._p(Gh), self._p(Gl)), "gram_dd")
+        self.sync()
+        return Gh, Gl
+
+    def exact_local_qr(self, X):
+        """Exact-Gram QR of A = X^T (X row-major m x local_n CUDA float64,
+        kept): returns (R, W, Rp, scale), R m x m with dgeqrf's row signs, all
+        as row-major tensors holding the column-major matrices (R.T is R)."""
+        m, n = X.shape
+        R, W, Rp = self._empty(m, m), self._empty(m, m), self._empty(m, m)
+        sc = self._empty(m)
+        self._pre()
+        self._check(self.L.bbt_exact_local_qr(self.h, m, n, self._p(X), self._p(R), self._p(W), self._p(Rp),
+                                              self._p(sc)), "exact_local_qr")
+        self.sync()
+        return R, W, Rp, sc
+
+    def exact_apply_q(self, X, scale, Rp, Z):
+        """C = A_int Rp^-1 Z (rows x k) for the integers of A = X^T; Z is a
+        row-major k x m tensor holding the column-major m x k matrix.
+        Returns C as a row-major k x rows tensor (column-major rows x k)."""
+        m, n = X.shape
+        k = Z.shape[0]
+        Cout = self._empty(k, n)
+        self._pre()
+        self._check(self.L.bbt_exact_apply_q(self.h, m, n, self._p(X), X.shape[1], self._p(scale), self._p(Rp),
+                                             self._p(Z), k, self._p(Cout), n), "exact_apply_q")
+        self.sync()
+        return Cout
+
     def dgemm_ozaki(self, transa, transb, A, B, alpha=1.0, beta=0.0, C=None, upper=False):
         """dgemm's contract (same tensor conventions) computed from exact int8
         slices on the tensor cores (FP64-accurate)."""

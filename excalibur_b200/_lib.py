@@ -24,9 +24,9 @@ EXPORTS = (
     "bbt_svd_dense", "bbt_fedsvd_tune", "bbt_rademacher", "bbt_sketch_bf16x3", "bbt_mixed_local_qr",
     "bbt_mlp_param_count", "bbt_mlp_features", "bbt_mlp_forward", "bbt_mlp_grad", "bbt_mlp_adam",
     "bbt_mlp_brackets", "bbt_bisection_bracketed", "bbt_set_bracket_model", "bbt_bisection_stats", "bbt_gebrd",
-    "bbt_dgemm_ozaki",
+    "bbt_dgemm_ozaki", "bbt_dgemm_crt", "bbt_gram_dd", "bbt_exact_local_qr", "bbt_exact_apply_q",
 )
-PROF_CLASSES = ("dgemm", "panel", "mask", "ralha", "bisect", "twisted", "sketch", "chol", "ozaki")
+PROF_CLASSES = ("dgemm", "panel", "mask", "ralha", "bisect", "twisted", "sketch", "chol", "ozaki", "crt")
 
 
 class FedSVDConfig(C.Structure):
@@ -95,6 +95,10 @@ def load():
         "bbt_bisection_stats": ([vp, C.POINTER(C.c_longlong)], i),
         "bbt_gebrd": ([vp, i, vp, vp, vp], i),
         "bbt_dgemm_ozaki": ([vp, i, i, i, i, C.c_long, d, vp, C.c_long, vp, C.c_long, d, vp, C.c_long, i], i),
+        "bbt_dgemm_crt": ([vp, i, i, C.c_long, d, vp, C.c_long, vp, C.c_long, d, vp, C.c_long, i], i),
+        "bbt_gram_dd": ([vp, i, C.c_long, vp, C.c_long, vp, vp], i),
+        "bbt_exact_local_qr": ([vp, i, st, vp, vp, vp, vp, vp], i),
+        "bbt_exact_apply_q": ([vp, i, st, vp, C.c_long, vp, vp, vp, i, vp, C.c_long], i),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

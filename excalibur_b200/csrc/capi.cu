@@ -342,6 +342,72 @@ bbt_status bbt_dgemm_ozaki(bbt_ctx* ctx, int transa, int transb, int M, int N, l
   return check_tc_flags(ctx, "dgemm_ozaki");
 }
 
+bbt_status bbt_dgemm_crt(bbt_ctx* ctx, int M, int N, long K, double alpha, const double* A, long lda, const double* B,
+                         long ldb, double beta, double* C, long ldc, int bits) {
+  if (!ctx) return BBT_ERR_ARG;
+  if (M < 1 || N < 1 || K < 1 || bad(A) || bad(B) || bad(C) || lda < K || ldb < K || ldc < M || bits < 8 || bits > 53)
+    return fail(ctx, BBT_ERR_ARG, "dgemm_crt: bad arguments");
+  const int n = crt_moduli(bits, bits, K);
+  if (n < 1) return fail(ctx, BBT_ERR_ARG, "dgemm_crt: %d bits over K=%ld", bits, K);
+  const long Kp = crt_pitch(K);
+  BBT_TRY(ensure(ctx, (size_t)n * (M + N) * Kp + crt_product_bytes(ctx, M, N, K, n, false) + (size_t)(M + N) * 16 +
+                          (4 << 20)));
+  BBT_TRY(clear_tc_flags(ctx));
+  BBT_TRY(gemm_crt(ctx, M, N, K, alpha, A, lda, 1, B, ldb, 1, beta, C, ldc, false, false, bits));
+  return check_tc_flags(ctx, "dgemm_crt");
+}
+
+bbt_status bbt_gram_dd(bbt_ctx* ctx, int m, long n, const double* X, long ldx, double* Gh, double* Gl) {
+  if (!ctx) return BBT_ERR_ARG;
+  if (m < 1 || n < 1 || bad(X) || bad(Gh) || bad(Gl) || ldx < n) return fail(ctx, BBT_ERR_ARG, "gram_dd: bad arguments");
+  const int nm = crt_moduli(53, 53, n);
+  if (nm < 1) return fail(ctx, BBT_ERR_ARG, "gram_dd: n=%ld too long", n);
+  const long Kp = crt_pitch(n);
+  BBT_TRY(ensure(ctx, (size_t)nm * m * Kp + crt_product_bytes(ctx, m, m, n, nm, true) + (size_t)m * 16 + (4 << 20)));
+  BBT_TRY(clear_tc_flags(ctx));
+  int8_t* RX = ctx->ws.take<int8_t>((size_t)nm * m * Kp);
+  double* s = ctx->ws.take<double>(m);
+  const size_t mark = ctx->ws.top;
+  BBT_TRY(crt_row_scales(ctx, m, n, X, ldx, s));
+  ctx->ws.top = mark;
+  uint8_t* R = ctx->ws.take<uint8_t>(crt_product_bytes(ctx, m, m, n, nm, true));
+  if (!R) return fail(ctx, BBT_ERR_NOMEM, "gram_dd: workspace");
+  BBT_TRY(crt_residues_rows(ctx, m, n, X, ldx, s, 53, nm, RX, Kp));
+  int splits = 1;
+  BBT_TRY(crt_product(ctx, m, m, n, nm, RX, RX, Kp, true, R, &splits));
+  BBT_TRY(crt_combine_dd(ctx, m, m, nm, splits, R, true, s, s, 2 * 52, Gh, Gl, m));
+  return check_tc_flags(ctx, "gram_dd");
+}
+
+bbt_status bbt_exact_local_qr(bbt_ctx* ctx, int m, size_t local_n, const double* x, double* R, double* W, double* Rp,
+                              double* scale) {
+  if (!ctx) return BBT_ERR_ARG;
+  if (m < 2 || local_n < (size_t)m || local_n > ((size_t)1 << 31) || bad(x) || bad(R) || bad(W) || bad(Rp) ||
+      bad(scale))
+    return fail(ctx, BBT_ERR_ARG, "exact_local_qr: bad arguments");
+  const int mi = m, N = sketch_rows(mi);
+  const long pitch = sketch_pitch((long)local_n);
+  const size_t sbytes = (size_t)N * pitch * 2 + 256;
+  BBT_TRY(ensure(ctx, exact_qr_workspace_bytes(ctx, mi, (long)local_n) + sbytes + (16 << 20)));
+  void* S = ctx->ws.take<char>(sbytes);
+  BBT_TRY(rademacher(ctx, N, (long)local_n, S, 0x5EED5EEDull));
+  BBT_TRY(clear_tc_flags(ctx));
+  BBT_TRY(exact_local_qr(ctx, mi, (long)local_n, x, S, pitch, R, W, Rp, scale));
+  return check_tc_flags(ctx, "exact_local_qr");
+}
+
+bbt_status bbt_exact_apply_q(bbt_ctx* ctx, int m, size_t rows, const double* x, long ldx, const double* scale,
+                             const double* Rp, const double* Z, int k, double* C, long ldc) {
+  if (!ctx) return BBT_ERR_ARG;
+  if (m < 2 || rows < 1 || rows > ((size_t)1 << 31) || k < 1 || k > 65535 || ldx < (long)rows || ldc < (long)rows ||
+      bad(x) || bad(scale) || bad(Rp) || bad(Z) || bad(C))
+    return fail(ctx, BBT_ERR_ARG, "exact_apply_q: bad arguments");
+  BBT_TRY(ensure(ctx, exact_apply_workspace_bytes(ctx, (long)rows, m, k) + (16 << 20)));
+  BBT_TRY(clear_tc_flags(ctx));
+  BBT_TRY(exact_apply_q(ctx, m, (long)rows, x, ldx, scale, Rp, Z, k, C, ldc));
+  return check_tc_flags(ctx, "exact_apply_q");
+}
+
 bbt_status bbt_rademacher(bbt_ctx* ctx, int N, size_t local_n, unsigned long long seed, void* d_S) {
   if (!ctx) return BBT_ERR_ARG;
   if (N < 1 || local_n < 1 || local_n > ((size_t)1 << 31) || bad(d_S))

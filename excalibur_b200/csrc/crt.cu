@@ -1,0 +1,817 @@
+// Exact integer matrix products on the int8 tensor cores by the Chinese
+// remainder theorem: the FP64-accurate (and, for the Gram matrix, exact)
+// products of the mixed-precision path.
+//
+//   C (M x N, column-major) = A B^T,  A(i, k), B(j, k) given as residue planes.
+//
+// Every row of an operand is scaled by a power of two s_i (|x / s_i| < 1/2)
+// and rounded to a b-bit integer t = rint(x 2^(b-1) / s_i), |t| <= 2^(b-2).
+// The integer product T = A_int B_int^T is then computed exactly modulo n
+// pairwise coprime moduli p <= 256: with residues in [-128, 127] every
+// modulus is one int8 x int8 -> int32 GEMM (tcgen05 kind::i8, 128 x 256 tiles,
+// one TMEM accumulator), exact for up to 2^16 terms per K-split.  The
+// residues of T are written as bytes and the integer is rebuilt from them
+// (crt_combine): with y_p = (T mod p) ((M/p)^-1 mod p) mod p, T/M = sum_p y_p / p
+// mod 1 (M = prod p), evaluated as a 128-bit fixed-point sum of y_p
+// floor(2^128 / p) whose wrap-around discards the integer part exactly.  n is
+// chosen so that |T| < M / 2, so the centred fraction times M is T itself, to
+// about 2^-110 of the largest possible |T|.
+//
+// Against the slice-pair (Ozaki) products of ozaki.cu this needs n int8
+// products instead of S(S+1)/2, each with a 256-column accumulator instead of
+// S accumulators sharing 512 TMEM columns (so half the shared-memory operand
+// traffic per multiply-add), at the price of a per-output epilogue: it pays
+// where K is long (the Gram matrix).
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "internal.h"
+#include "tc.cuh"
+
+namespace bbt {
+namespace {
+
+using namespace tc;
+
+constexpr int MAXMOD = 24;
+// Pairwise coprime, largest first after 2^8: 255 = 3 5 17, 253 = 11 23,
+// 247 = 13 19, 217 = 7 31; the others are primes.
+constexpr int MODULI[MAXMOD] = {256, 255, 253, 251, 247, 241, 239, 233, 229, 227, 223, 217,
+                                211, 199, 197, 193, 191, 181, 179, 173, 167, 163, 157, 151};
+
+constexpr int TM = 128, TN = 256, TK = 128;   // TK: bytes of K per stage row (SWIZZLE_128B)
+constexpr int STAGES = 4;
+constexpr int A_TILE = TM * TK, B_TILE = TN * TK;
+constexpr int STAGE_BYTES = A_TILE + B_TILE;   // 48 KB
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
+constexpr int EPI_WARPS = 8;
+constexpr int THREADS = (EPI_WARPS + 2) * 32;
+constexpr uint32_t TMEM_COLS = 2 * TN;          // two accumulators: modulus p+1 runs while p drains
+constexpr int MAX_KB_PER_SPLIT = 65536 / TK;    // |T| < 2^16 * 2^14 per split: no int32 overflow
+constexpr int MAX_SPLITS = 64;
+
+struct Mods {
+  int n;
+  int p[MAXMOD];
+  int c16[MAXMOD];     // 2^16 mod p
+  float invf[MAXMOD];  // 1 / p
+  int inv[MAXMOD];     // ((M / p) mod p)^-1 mod p
+  uint32_t F[MAXMOD][4];   // floor(2^128 / p), 32-bit limbs, least significant first
+  double mod_hi, mod_lo;   // M as a double-double
+  double mod_bits;         // log2 M
+};
+
+// ---- residues of integer-valued operands --------------------------------
+
+__device__ __forceinline__ int centre(int r, int p) {
+  const int hi = (p - 1) >> 1, lo = hi - p + 1;
+  if (r > hi) r -= p;
+  if (r > hi) r -= p;
+  if (r < lo) r += p;
+  if (r < lo) r += p;
+  return r;
+}
+
+// t an integer-valued double, |t| <= 2^53 (so |t / p| < 2^51).  Rounding and
+// the conversion to an integer by adding 1.5 2^52 (the integer lands in the
+// low mantissa bits) instead of conversion instructions.
+__device__ __forceinline__ int residue(double t, int p, double invp) {
+  const double RND = 6755399441055744.0;   // 1.5 * 2^52
+  const double q = (t * invp + RND) - RND;
+  const double r = fma(-q, (double)p, t);   // exact, |r| < 2p
+  return centre(__double2loint(r + RND), p);
+}
+
+// Residue of an integer-valued double of any size below 2^100: t = m 2^e with
+// an integer m < 2^53, residue(m) times 2^e mod p.
+__device__ __forceinline__ int residue_big(double t, int p, double invp) {
+  if (fabs(t) < 9007199254740992.0) return residue(t, p, invp);   // 2^53
+  int e = 0;
+  frexp(t, &e);
+  e -= 53;
+  int r = residue(ldexp(t, -e), p, invp);
+  for (int s = 0; s < e; ++s) r = centre(2 * r, p);
+  return r;
+}
+
+// Row maxima: blocks of 256 threads over (rows, chunks of 8192 columns); the
+// maximum of non-negative doubles is the maximum of their bit patterns, so
+// chunks combine by atomicMax.  Short rows: one warp per row.
+__global__ void rowmax_kernel(int rows, long K, const double* __restrict__ X, long rs,
+                              unsigned long long* __restrict__ mx) {
+  __shared__ double sh[8];
+  for (int i = blockIdx.y; i < rows; i += gridDim.y) {
+    const long k0 = (long)blockIdx.x * 8192;
+    const double* x = X + (long)i * rs;
+    double m = 0.0;
+    for (long k = k0 + threadIdx.x; k < K && k < k0 + 8192; k += blockDim.x) m = fmax(m, fabs(x[k]));
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, sh[w]);
+      atomicMax(mx + i, (unsigned long long)__double_as_longlong(m));
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void rowmax_short_kernel(int rows, long K, const double* __restrict__ X, long rs,
+                                    unsigned long long* __restrict__ mx) {
+  const int lane = threadIdx.x & 31;
+  for (long i = (blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5; i < rows; i += ((long)gridDim.x * blockDim.x) >> 5) {
+    const double* x = X + i * rs;
+    double m = 0.0;
+    for (long k = lane; k < K; k += 32) m = fmax(m, fabs(x[k]));
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (lane == 0) mx[i] = (unsigned long long)__double_as_longlong(m);
+  }
+}
+
+// s_i = 2^(e+1) with max |x| in [2^(e-1), 2^e) (1 for an all-zero row)
+__global__ void scale_kernel(int rows, const unsigned long long* __restrict__ mx, double* __restrict__ scale) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= rows) return;
+  const double m = __longlong_as_double((long long)mx[i]);
+  int e = 0;
+  if (m > 0.0) frexp(m, &e);
+  scale[i] = ldexp(1.0, e + 1);
+}
+
+struct ModTab {
+  int n;
+  int p[MAXMOD];
+  double invp[MAXMOD];
+  int c36[MAXMOD], c18[MAXMOD];   // 2^36, 2^18 mod p
+  int off[MAXMOD];                // a multiple of p above 2^23
+  uint32_t magic35[MAXMOD];       // ceil(2^35 / p): exact quotients below 2^27
+};
+
+// t = a 2^36 + b 2^18 + c (|t| <= 2^51): |a| <= 2^15, 0 <= b, c < 2^18, exact.
+struct Pieces {
+  int a, b, c;
+};
+__device__ __forceinline__ Pieces pieces(double t) {
+  const double RND = 6755399441055744.0;
+  const double a = floor(t * 0x1p-36);
+  const double rem = fma(-a, 0x1p36, t);
+  const double b = floor(rem * 0x1p-18);
+  const double c = fma(-b, 0x1p18, rem);
+  return {__double2loint(a + RND), __double2loint(b + RND), __double2loint(c + RND)};
+}
+// The centred residue from the pieces: x = a c36 + b c18 + c + off lies in
+// [0, 2^27) and its multiply-high quotient by p is exact.
+__device__ __forceinline__ int residue_pieces(const Pieces& t, const ModTab& T, int q) {
+  const int p = T.p[q];
+  const uint32_t x = (uint32_t)(t.a * T.c36[q] + t.b * T.c18[q] + t.c + T.off[q]);
+  int r = (int)(x - (__umulhi(x, T.magic35[q]) >> 3) * (uint32_t)p);
+  if (r > ((p - 1) >> 1)) r -= p;
+  return r;
+}
+
+// Rows contiguous in k: planes out[p][i][k] (row pitch Kp), four elements per thread.
+__global__ void residues_rows_kernel(int rows, long K, const double* __restrict__ X, long rs,
+                                     const double* __restrict__ scale, int b, ModTab T, int8_t* __restrict__ out,
+                                     long Kp) {
+  const long kq = (K + 3) / 4;
+  const long total = (long)rows * kq;
+  const size_t plane = (size_t)rows * Kp;
+  for (long f = blockIdx.x * (long)blockDim.x + threadIdx.x; f < total; f += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(f / kq);
+    const long k = (f - (long)i * kq) * 4;
+    const double mul = ldexp(1.0, b - 1) / scale[i];   // powers of two: exact
+    const double* x = X + (long)i * rs + k;
+    Pieces t[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) t[e] = pieces((k + e < K) ? rint(x[e] * mul) : 0.0);
+    int8_t* o = out + (size_t)i * Kp + k;
+    for (int q = 0; q < T.n; ++q) {
+      uint32_t w = 0;
+#pragma unroll
+      for (int e = 0; e < 4; ++e) w |= (uint32_t)(uint8_t)(int8_t)residue_pieces(t[e], T, q) << (8 * e);
+      if (k + 4 <= K) {
+        *reinterpret_cast<uint32_t*>(o + q * plane) = w;
+      } else {
+        for (int e = 0; k + e < K; ++e) o[q * plane + e] = (int8_t)(w >> (8 * e));
+      }
+    }
+  }
+}
+
+// Rows contiguous in i, K stride cs; the scale belongs to the K index
+// (kscale) -- the integers are those residues_rows_kernel forms for the
+// transposed operand.  32 x 32 tiles staged through shared memory.
+__global__ void __launch_bounds__(256) residues_cols_kernel(int rows, long K, const double* __restrict__ X, long cs,
+                                                            const double* __restrict__ kscale, int b, ModTab T,
+                                                            int8_t* __restrict__ out, long Kp) {
+  __shared__ double tile[32][33];
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const int i0 = blockIdx.x * 32;
+  const long k0 = (long)blockIdx.y * 32;
+  for (int r = ty; r < 32; r += 8) {   // tile[k][i]
+    const long k = k0 + r;
+    const int i = i0 + tx;
+    tile[r][tx] = (i < rows && k < K) ? rint(X[i + k * cs] * (ldexp(1.0, b - 1) / kscale[k])) : 0.0;
+  }
+  __syncthreads();
+  const size_t plane = (size_t)rows * Kp;
+  const long k = k0 + tx;
+  for (int r = ty; r < 32; r += 8) {
+    const int i = i0 + r;
+    if (i < rows && k < K) {
+      const Pieces t = pieces(tile[tx][r]);
+      for (int q = 0; q < T.n; ++q) out[q * plane + (size_t)i * Kp + k] = (int8_t)residue_pieces(t, T, q);
+    }
+  }
+}
+
+// Double-double rows (hi + lo), rows contiguous in k, b up to 100 bits:
+// t = T_hi + T_lo with T_hi = rint(hi 2^(b-1) / s_i) (any size, m 2^e with an
+// integer m < 2^53) and T_lo = rint(lo 2^(b-1) / s_i + the fraction of hi's).
+__global__ void residues_dd_kernel(int rows, long K, const double* __restrict__ Xh, const double* __restrict__ Xl,
+                                   long rs, const double* __restrict__ scale, int b, ModTab T,
+                                   int8_t* __restrict__ out, long Kp) {
+  const long total = (long)rows * K;
+  const size_t plane = (size_t)rows * Kp;
+  for (long f = blockIdx.x * (long)blockDim.x + threadIdx.x; f < total; f += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(f / K);
+    const long k = f - (long)i * K;
+    const double mul = ldexp(1.0, b - 1) / scale[i];
+    const double h = Xh[(long)i * rs + k] * mul, l = Xl[(long)i * rs + k] * mul;
+    const double th = rint(h);
+    const double tl = rint(l + (h - th));
+    for (int q = 0; q < T.n; ++q) {
+      const int p = T.p[q];
+      const int r = centre(residue_big(th, p, T.invp[q]) + residue_big(tl, p, T.invp[q]), p);
+      out[q * plane + (size_t)i * Kp + k] = (int8_t)r;
+    }
+  }
+}
+
+// ---- one int8 GEMM per modulus ------------------------------------------
+
+struct CrtArgs {
+  uint8_t* out;   // residues of T: out[((z * n + q) * N + j) * M + i]
+  int M, N;
+  int kblocks, kb_per_split;
+  int n;
+  int upper;      // 1: skip tiles strictly below the diagonal
+  int p[MAXMOD], c16[MAXMOD];
+  uint32_t magic[MAXMOD];   // ceil(2^32 / p): exact quotients below 2^24
+  int off[MAXMOD];          // 2^31 mod p
+  int* err;
+};
+
+__global__ void __launch_bounds__(THREADS, 1)
+crt_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, CrtArgs P) {
+  const int n0 = blockIdx.x * TN, m0 = blockIdx.y * TM;
+  if (P.upper && m0 >= n0 + TN) return;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint64_t* bars = (uint64_t*)(smem + STAGES * STAGE_BYTES);
+  uint32_t* tmem_slot = (uint32_t*)(bars + 2 * STAGES + 4);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int kb0 = blockIdx.z * P.kb_per_split;
+  const int nk = min(P.kblocks - kb0, P.kb_per_split);
+  const uint32_t full0 = smem_u32(bars), empty0 = smem_u32(bars + STAGES);
+  const uint32_t accf0 = smem_u32(bars + 2 * STAGES), acce0 = smem_u32(bars + 2 * STAGES + 2);
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(full0 + 8 * s, 1);
+      mbar_init(empty0 + 8 * s, 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(accf0 + 8 * b, 1);
+      mbar_init(acce0 + 8 * b, EPI_WARPS);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const int total = P.n * nk;
+
+  if (warp == EPI_WARPS) {
+    if (lane == 0) {   // ---- TMA producer: modulus after modulus, K-block after K-block
+      int issued = 0;
+      bool ok = true;
+      for (int it = 0; it < total; ++it) {
+        const int q = it / nk, kb = it - q * nk;
+        const int s = it % STAGES;
+        const uint32_t ph = (uint32_t)(it / STAGES) & 1u;
+        if (!mbar_wait(empty0 + 8 * s, ph ^ 1u)) { ok = false; break; }
+        const uint32_t fb = full0 + 8 * s;
+        mbar_expect_tx(fb, (uint32_t)STAGE_BYTES);
+        const uint32_t st = smem_u32(smem + (size_t)s * STAGE_BYTES);
+        const int kx = (kb0 + kb) * TK;
+        tma_load_3d(st, &tmA, fb, kx, m0, q);
+        tma_load_3d(st + A_TILE, &tmB, fb, kx, n0, q);
+        ++issued;
+      }
+      if (!ok) atomicExch(P.err, 1);
+      for (int it = max(0, issued - STAGES); it < issued; ++it)
+        if (!mbar_wait(full0 + 8 * (it % STAGES), (uint32_t)(it / STAGES) & 1u)) atomicExch(P.err, 4);
+    }
+  } else if (warp == EPI_WARPS + 1) {
+    if (lane == 0) {   // ---- MMA issuer: int8 x int8 -> int32, K-major, 128 x 256 x 32 per instruction
+      const uint32_t idesc =
+          (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TN >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
+      bool ok = true;
+      for (int q = 0; q < P.n && ok; ++q) {
+        const int buf = q & 1, use = q >> 1;
+        if (use > 0 && !mbar_wait(acce0 + 8 * buf, (uint32_t)(use - 1) & 1u)) { ok = false; break; }
+        tc_fence_after();
+        const uint32_t d = tmem + (uint32_t)(buf * TN);
+        for (int kb = 0; kb < nk; ++kb) {
+          const int it = q * nk + kb;
+          const int s = it % STAGES;
+          if (!mbar_wait(full0 + 8 * s, (uint32_t)(it / STAGES) & 1u)) { ok = false; break; }
+          tc_fence_after();
+          const uint32_t st = smem_u32(smem + (size_t)s * STAGE_BYTES);
+          const uint64_t ad = sw128_desc(st), bd = sw128_desc(st + A_TILE);
+#pragma unroll
+          for (int kk = 0; kk < TK / 32; ++kk)   // +32 bytes along K = +2 in the descriptor's address field
+            mma_i8(d, ad + 2 * kk, bd + 2 * kk, idesc, (kb != 0 || kk != 0) ? 1u : 0u);
+          mma_commit(empty0 + 8 * s);
+        }
+        mma_commit(accf0 + 8 * buf);
+      }
+      if (!ok) atomicExch(P.err, 2);
+    }
+  } else {
+    // ---- epilogue: TMEM lanes 32 (warp % 4).., columns 128 (warp / 4).. of the accumulator;
+    //      T mod p as a byte per element, i (the TMEM lane) contiguous in memory
+    const int q4 = warp & 3, ch = warp >> 2;
+    const int i = m0 + q4 * 32 + lane;
+    bool ok = true;
+    for (int q = 0; q < P.n; ++q) {
+      const int buf = q & 1, use = q >> 1;
+      if (!mbar_wait(accf0 + 8 * buf, (uint32_t)use & 1u)) { ok = false; break; }
+      tc_fence_after();
+      const int p = P.p[q], c16 = P.c16[q];
+      const uint32_t magic = P.magic[q], off = (uint32_t)P.off[q];
+      uint8_t* o = P.out + ((size_t)blockIdx.z * P.n + q) * (size_t)P.N * P.M;
+#pragma unroll 1
+      for (int c = 0; c < TN / 2 / 16; ++c) {
+        uint32_t v[16];
+        tmem_ld16(tmem + ((uint32_t)(q4 * 32) << 16) + (uint32_t)(buf * TN + ch * (TN / 2) + c * 16), v);
+        const int j0 = n0 + ch * (TN / 2) + c * 16;
+#pragma unroll
+        for (int e = 0; e < 16; ++e) {
+          // a = (h - 2^15) 2^16 + lo with 0 <= h, lo < 2^16: h c16 + lo (< 2^24) is
+          // congruent to a + 2^31 mod p, reduced exactly by the multiply-high
+          // quotient; off = 2^31 mod p is taken back out
+          const uint32_t a = v[e] ^ 0x80000000u;
+          const uint32_t x = (a >> 16) * (uint32_t)c16 + (a & 0xFFFFu);
+          int r = (int)(x - __umulhi(x, magic) * (uint32_t)p) - (int)off;
+          if (r < 0) r += p;
+          const int j = j0 + e;
+          if (i < P.M && j < P.N) o[(size_t)j * P.M + i] = (uint8_t)r;
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(acce0 + 8 * buf);
+    }
+    if (!ok && lane == 0) atomicExch(P.err, 3);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+  }
+}
+
+// ---- rebuilding T from its residues ---------------------------------------
+
+struct CombArgs {
+  const uint8_t* R;
+  int M, N, n, splits, upper;
+  int p[MAXMOD], inv[MAXMOD];
+  uint32_t magic32[MAXMOD];   // ceil(2^32 / p): exact quotients below 2^24
+  uint32_t F[MAXMOD][4];
+  double mod_hi, mod_lo;
+};
+
+// x mod p for 0 <= x < 2^24 by the multiply-high quotient.
+__device__ __forceinline__ uint32_t mod_small(uint32_t x, uint32_t p, uint32_t magic) {
+  return x - __umulhi(x, magic) * p;
+}
+
+// The centred fraction f = T / M (mod 1) as a signed 128-bit fixed-point
+// number (two 64-bit halves).
+__device__ __forceinline__ void crt_fraction(const CombArgs& A, long f, long total, uint64_t& hi, uint64_t& lo) {
+  uint64_t L0 = 0, L1 = 0, L2 = 0, L3 = 0;
+  for (int q = 0; q < A.n; ++q) {
+    uint32_t s = 0;
+    for (int z = 0; z < A.splits; ++z) s += A.R[((size_t)z * A.n + q) * total + f];
+    const uint32_t p = (uint32_t)A.p[q], mg = A.magic32[q];
+    const uint32_t y = mod_small(mod_small(s, p, mg) * (uint32_t)A.inv[q], p, mg);
+    L0 += (uint64_t)y * A.F[q][0];   // 32 x 32 -> 64-bit products, < 2^40 each
+    L1 += (uint64_t)y * A.F[q][1];
+    L2 += (uint64_t)y * A.F[q][2];
+    L3 += (uint64_t)y * A.F[q][3];
+  }
+  L1 += L0 >> 32;
+  L2 += L1 >> 32;
+  L3 += L2 >> 32;
+  lo = (L0 & 0xFFFFFFFFull) | (L1 << 32);
+  hi = (L2 & 0xFFFFFFFFull) | (L3 << 32);
+}
+
+__device__ __forceinline__ void two_sum(double a, double b, double& s, double& e) {
+  s = a + b;
+  const double bb = s - a;
+  e = (a - (s - bb)) + (b - bb);
+}
+
+// A signed 128-bit integer (two's complement, hi:lo) as a double-double: its
+// magnitude split exactly into three 53-bit chunks, summed with error terms.
+__device__ __forceinline__ void fixed_to_dd(uint64_t hi, uint64_t lo, double& dh, double& dl) {
+  const bool neg = (int64_t)hi < 0;
+  if (neg) {
+    lo = ~lo + 1;
+    hi = ~hi + (lo == 0 ? 1 : 0);
+  }
+  const uint64_t m53 = (1ull << 53) - 1;
+  const double c0 = (double)(lo & m53);
+  const double c1 = ldexp((double)(((lo >> 53) | (hi << 11)) & m53), 53);
+  const double c2 = ldexp((double)(hi >> 42), 106);
+  double s, e1, t, e2;
+  two_sum(c2, c1, s, e1);
+  two_sum(s, c0, t, e2);
+  const double e = e1 + e2;
+  dh = t + e;
+  dl = e - (dh - t);
+  if (neg) {
+    dh = -dh;
+    dl = -dl;
+  }
+}
+
+__device__ __forceinline__ void two_prod(double a, double b, double& p, double& e) {
+  p = a * b;
+  e = fma(a, b, -p);
+}
+
+// C (column-major, ldc) = alpha * sa_i sb_j 2^-shift T + beta * C
+__global__ void combine_kernel(CombArgs A, const double* __restrict__ sa, const double* __restrict__ sb, int shift,
+                               double alpha, double beta, double* __restrict__ C, long ldc) {
+  const long total = (long)A.M * A.N;
+  for (long f = blockIdx.x * (long)blockDim.x + threadIdx.x; f < total; f += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(f % A.M);
+    const long j = f / A.M;
+    if (A.upper && (i / TM) * TM >= (j / TN) * TN + TN) continue;   // tile never computed
+    uint64_t hi, lo;
+    crt_fraction(A, f, total, hi, lo);
+    double dh, dl;
+    fixed_to_dd(hi, lo, dh, dl);
+    const double v = ldexp((dh + dl) * A.mod_hi, -128 - shift) * (sa ? sa[i] : 1.0) * sb[j];
+    double* c = C + i + j * ldc;
+    *c = (beta == 0.0) ? alpha * v : alpha * v + beta * (*c);
+  }
+}
+
+// The same value as a double-double (Ch + Cl), alpha = 1, beta = 0.
+__global__ void combine_dd_kernel(CombArgs A, const double* __restrict__ sa, const double* __restrict__ sb, int shift,
+                                  double* __restrict__ Ch, double* __restrict__ Cl, long ldc) {
+  const long total = (long)A.M * A.N;
+  for (long f = blockIdx.x * (long)blockDim.x + threadIdx.x; f < total; f += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(f % A.M);
+    const long j = f / A.M;
+    if (A.upper && (i / TM) * TM >= (j / TN) * TN + TN) continue;
+    uint64_t hi, lo;
+    crt_fraction(A, f, total, hi, lo);
+    double fh, fl;
+    fixed_to_dd(hi, lo, fh, fl);
+    // (fh + fl) (mod_hi + mod_lo), then exact power-of-two scalings
+    double p, e;
+    two_prod(fh, A.mod_hi, p, e);
+    e += fh * A.mod_lo + fl * A.mod_hi;
+    const double s = p + e;
+    const double t = e - (s - p);
+    const double sc = ldexp((sa ? sa[i] : 1.0) * sb[j], -128 - shift);
+    Ch[i + j * ldc] = s * sc;
+    Cl[i + j * ldc] = t * sc;
+  }
+}
+
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiled encode_fn() {
+  static EncodeTiled fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiled>(p);
+  }
+  return fn;
+}
+
+// ---- host tables -------------------------------------------------------------
+
+int inverse_mod(int a, int p) {   // a^-1 mod p, gcd(a, p) = 1
+  int t = 0, nt = 1, r = p, nr = a % p;
+  while (nr) {
+    const int q = r / nr;
+    int x = t - q * nt;
+    t = nt;
+    nt = x;
+    x = r - q * nr;
+    r = nr;
+    nr = x;
+  }
+  return t < 0 ? t + p : t;
+}
+
+Mods make_mods(int n) {
+  Mods m{};
+  m.n = n;
+  double bits = 0.0, hi = 1.0, lo = 0.0;
+  for (int q = 0; q < n; ++q) {
+    const int p = MODULI[q];
+    m.p[q] = p;
+    m.c16[q] = 65536 % p;
+    m.invf[q] = 1.0f / (float)p;
+    int prod = 1;   // (M / p) mod p
+    for (int r = 0; r < n; ++r)
+      if (r != q) prod = (int)((long)prod * (MODULI[r] % p) % p);
+    m.inv[q] = inverse_mod(prod, p);
+    unsigned __int128 F = ~(unsigned __int128)0 / (unsigned)p;
+    if (~(unsigned __int128)0 % (unsigned)p == (unsigned)p - 1) F += 1;   // p divides 2^128
+    for (int l = 0; l < 4; ++l) m.F[q][l] = (uint32_t)(F >> (32 * l));
+    // M as a double-double: (hi + lo) * p with an exact error term
+    const double ph = hi * p;
+    const double pe = std::fma(hi, (double)p, -ph) + lo * p;
+    hi = ph + pe;
+    lo = pe - (hi - ph);
+    bits += std::log2((double)p);
+  }
+  m.mod_hi = hi;
+  m.mod_lo = lo;
+  m.mod_bits = bits;
+  return m;
+}
+
+ModTab mod_tab(int n) {
+  ModTab t{};
+  t.n = n;
+  for (int q = 0; q < n; ++q) {
+    const int p = MODULI[q];
+    t.p[q] = p;
+    t.invp[q] = 1.0 / p;
+    t.c36[q] = (int)(((uint64_t)1 << 36) % (uint64_t)p);
+    t.c18[q] = (1 << 18) % p;
+    t.off[q] = p * (((1 << 23) + p - 1) / p);
+    t.magic35[q] = (uint32_t)((((uint64_t)1 << 35) + p - 1) / p);
+  }
+  return t;
+}
+
+struct Plan {
+  int splits, kb_per_split, kblocks;
+};
+
+Plan plan(int M, int N, long K, int num_sms, bool upper) {
+  Plan r;
+  r.kblocks = (int)((K + TK - 1) / TK);
+  const long tm = (M + TM - 1) / TM, tn = (N + TN - 1) / TN;
+  long tiles = 0;
+  for (long a = 0; a < tm; ++a)
+    for (long b = 0; b < tn; ++b) tiles += (!upper || a * TM < b * TN + TN);
+  const int smin = (r.kblocks + MAX_KB_PER_SPLIT - 1) / MAX_KB_PER_SPLIT;
+  const int smax = std::max(smin, std::min(MAX_SPLITS, r.kblocks));
+  double best = 1e300;
+  int bs = smin;
+  for (int s = smin; s <= smax; ++s) {
+    const long waves = (tiles * s + num_sms - 1) / num_sms;
+    const double cost = (double)waves * ((r.kblocks + s - 1) / s + 8) + 2.0 * s;
+    if (cost < best * 0.98) { best = cost; bs = s; }
+  }
+  r.kb_per_split = (r.kblocks + bs - 1) / bs;
+  r.splits = (r.kblocks + r.kb_per_split - 1) / r.kb_per_split;
+  return r;
+}
+
+}  // namespace
+
+long crt_pitch(long K) { return (K + 15) / 16 * 16; }
+
+int crt_moduli(int bits_a, int bits_b, long K) {
+  const double need = (bits_a - 2) + (bits_b - 2) + std::log2((double)std::max(K, 1L)) + 2.0;
+  double bits = 0.0;
+  for (int n = 0; n < MAXMOD; ++n) {
+    bits += std::log2((double)MODULI[n]);
+    if (bits >= need) return n + 1;
+  }
+  return -1;
+}
+
+bbt_status crt_row_scales(bbt_ctx* ctx, int rows, long K, const double* X, long rs, double* scale) {
+  unsigned long long* mx = ctx->ws.take<unsigned long long>(rows);
+  if (!mx) return fail(ctx, BBT_ERR_NOMEM, "crt: workspace (row maxima)");
+  BBT_CUDA(ctx, cudaMemsetAsync(mx, 0, (size_t)rows * 8, ctx->stream));
+  if (K <= 4096) {
+    rowmax_short_kernel<<<8 * ctx->num_sms, 256, 0, ctx->stream>>>(rows, K, X, rs, mx);
+  } else {
+    const unsigned gy = (unsigned)std::min(rows, 65535);
+    rowmax_kernel<<<dim3((unsigned)((K + 8191) / 8192), gy), 256, 0, ctx->stream>>>(rows, K, X, rs, mx);
+  }
+  BBT_LAUNCHED(ctx);
+  scale_kernel<<<(rows + 255) / 256, 256, 0, ctx->stream>>>(rows, mx, scale);
+  BBT_LAUNCHED(ctx);
+  return BBT_OK;   // mx stays taken until the caller releases its workspace mark
+}
+
+bbt_status crt_residues_rows(bbt_ctx* ctx, int rows, long K, const double* X, long rs, const double* scale, int b,
+                             int n, int8_t* planes, long Kp) {
+  if (b < 2 || b > 53) return fail(ctx, BBT_ERR_ARG, "crt: %d-bit integers from doubles", b);
+  residues_rows_kernel<<<16 * ctx->num_sms, 256, 0, ctx->stream>>>(rows, K, X, rs, scale, b, mod_tab(n), planes, Kp);
+  BBT_LAUNCHED(ctx);
+  return BBT_OK;
+}
+
+bbt_status crt_residues_cols(bbt_ctx* ctx, int rows, long K, const double* X, long cs, const double* kscale, int b,
+                             int n, int8_t* planes, long Kp) {
+  if (b < 2 || b > 53) return fail(ctx, BBT_ERR_ARG, "crt: %d-bit integers from doubles", b);
+  const long gy = (K + 31) / 32;
+  if (gy > 65535) return fail(ctx, BBT_ERR_ARG, "crt: K=%ld too long for the column layout", K);
+  residues_cols_kernel<<<dim3((unsigned)((rows + 31) / 32), (unsigned)gy), 256, 0, ctx->stream>>>(
+      rows, K, X, cs, kscale, b, mod_tab(n), planes, Kp);
+  BBT_LAUNCHED(ctx);
+  return BBT_OK;
+}
+
+bbt_status crt_residues_dd(bbt_ctx* ctx, int rows, long K, const double* Xh, const double* Xl, long rs,
+                           const double* scale, int b, int n, int8_t* planes, long Kp) {
+  if (b < 2 || b > 100) return fail(ctx, BBT_ERR_ARG, "crt: %d-bit integers from double-doubles", b);
+  residues_dd_kernel<<<8 * ctx->num_sms, 256, 0, ctx->stream>>>(rows, K, Xh, Xl, rs, scale, b, mod_tab(n), planes, Kp);
+  BBT_LAUNCHED(ctx);
+  return BBT_OK;
+}
+
+size_t crt_product_bytes(const bbt_ctx* ctx, int M, int N, long K, int n, bool upper) {
+  const int sms = ctx->num_sms > 0 ? ctx->num_sms : 148;
+  const Plan pl = plan(M, N, K, sms, upper);
+  return (size_t)pl.splits * n * (size_t)M * N + 4096;
+}
+
+bbt_status crt_product(bbt_ctx* ctx, int M, int N, long K, int n, const int8_t* RA, const int8_t* RB, long Kp,
+                       bool upper, uint8_t* R, int* splits_out) {
+  if (n < 1 || n > MAXMOD) return fail(ctx, BBT_ERR_ARG, "crt: %d moduli", n);
+  if (M < 1 || N < 1 || K < 1) return fail(ctx, BBT_ERR_ARG, "crt: M=%d N=%d K=%ld", M, N, K);
+  const unsigned gy = (unsigned)((M + TM - 1) / TM);
+  if (gy > 65535) return fail(ctx, BBT_ERR_ARG, "crt: M=%d too large", M);
+  EncodeTiled enc = encode_fn();
+  if (!enc) return fail(ctx, BBT_ERR_CUDA, "crt: cuTensorMapEncodeTiled is not available");
+  const Plan pl = plan(M, N, K, ctx->num_sms, upper);
+  CUtensorMap ta, tb;
+  {
+    const cuuint64_t dims[3] = {(cuuint64_t)K, (cuuint64_t)M, (cuuint64_t)n};
+    const cuuint64_t strides[2] = {(cuuint64_t)Kp, (cuuint64_t)Kp * M};
+    const cuuint32_t box[3] = {TK, TM, 1}, es[3] = {1, 1, 1};
+    if (enc(&ta, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<int8_t*>(RA), dims, strides, box, es,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return fail(ctx, BBT_ERR_CUDA, "crt: tensor map of A");
+  }
+  {
+    const cuuint64_t dims[3] = {(cuuint64_t)K, (cuuint64_t)N, (cuuint64_t)n};
+    const cuuint64_t strides[2] = {(cuuint64_t)Kp, (cuuint64_t)Kp * N};
+    const cuuint32_t box[3] = {TK, TN, 1}, es[3] = {1, 1, 1};
+    if (enc(&tb, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<int8_t*>(RB), dims, strides, box, es,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return fail(ctx, BBT_ERR_CUDA, "crt: tensor map of B");
+  }
+  static bool attr = false;
+  if (!attr) {
+    BBT_CUDA(ctx, cudaFuncSetAttribute(crt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+    attr = true;
+  }
+  const Mods md = make_mods(n);
+  CrtArgs a;
+  a.out = R;
+  a.M = M;
+  a.N = N;
+  a.kblocks = pl.kblocks;
+  a.kb_per_split = pl.kb_per_split;
+  a.n = n;
+  a.upper = upper ? 1 : 0;
+  for (int q = 0; q < n; ++q) {
+    a.p[q] = md.p[q];
+    a.c16[q] = md.c16[q];
+    a.magic[q] = (uint32_t)((((uint64_t)1 << 32) + md.p[q] - 1) / md.p[q]);
+    a.off[q] = (int)(((uint64_t)1 << 31) % (uint64_t)md.p[q]);
+  }
+  a.err = ctx->d_flag + FLAG_SKETCH;
+  ProfScope prof(ctx, BBT_PROF_CRT, (upper ? 1.0 : 2.0) * (double)M * N * K);
+  crt_kernel<<<dim3((N + TN - 1) / TN, gy, pl.splits), THREADS, SMEM_BYTES, ctx->stream>>>(ta, tb, a);
+  BBT_LAUNCHED(ctx);
+  *splits_out = pl.splits;
+  return BBT_OK;
+}
+
+namespace {
+CombArgs comb_args(const uint8_t* R, int M, int N, int n, int splits, bool upper) {
+  const Mods md = make_mods(n);
+  CombArgs c;
+  c.R = R;
+  c.M = M;
+  c.N = N;
+  c.n = n;
+  c.splits = splits;
+  c.upper = upper ? 1 : 0;
+  for (int q = 0; q < n; ++q) {
+    c.p[q] = md.p[q];
+    c.inv[q] = md.inv[q];
+    c.magic32[q] = (uint32_t)((((uint64_t)1 << 32) + md.p[q] - 1) / md.p[q]);
+    for (int l = 0; l < 4; ++l) c.F[q][l] = md.F[q][l];
+  }
+  c.mod_hi = md.mod_hi;
+  c.mod_lo = md.mod_lo;
+  return c;
+}
+}  // namespace
+
+bbt_status crt_combine(bbt_ctx* ctx, int M, int N, int n, int splits, const uint8_t* R, bool upper, const double* sa,
+                       const double* sb, int shift, double alpha, double beta, double* C, long ldc) {
+  combine_kernel<<<8 * ctx->num_sms, 256, 0, ctx->stream>>>(comb_args(R, M, N, n, splits, upper), sa, sb, shift, alpha,
+                                                           beta, C, ldc);
+  BBT_LAUNCHED(ctx);
+  return BBT_OK;
+}
+
+bbt_status crt_combine_dd(bbt_ctx* ctx, int M, int N, int n, int splits, const uint8_t* R, bool upper,
+                          const double* sa, const double* sb, int shift, double* Ch, double* Cl, long ldc) {
+  combine_dd_kernel<<<8 * ctx->num_sms, 256, 0, ctx->stream>>>(comb_args(R, M, N, n, splits, upper), sa, sb, shift, Ch,
+                                                              Cl, ldc);
+  BBT_LAUNCHED(ctx);
+  return BBT_OK;
+}
+
+size_t crt_gemm_workspace_bytes(const bbt_ctx* ctx, int M, int N, long K, int bits, bool same, bool upper) {
+  const int n = crt_moduli(bits, bits, K);
+  if (n < 1) return 0;
+  const long Kp = crt_pitch(K);
+  return (size_t)n * (same ? M : M + N) * Kp + crt_product_bytes(ctx, M, N, K, n, upper) + (size_t)(M + N) * 16 +
+         (size_t)std::max(M, N) * 8 + 8192;
+}
+
+// The Gram matrix of a long operand: K long enough for the CRT product (one
+// exact int8 GEMM per modulus, 128 x 256 tiles) to beat the slice pairs.
+bool crt_worthwhile(int M, int N, long K) { return M >= 128 && N >= 128 && K >= 16384 && (double)M * N * K >= 4e9; }
+
+// C = alpha A B^T + beta C for strided FP64 operands (each with a unit stride
+// in its row or its K index), every operand rounded to b bits per row.
+bbt_status gemm_crt(bbt_ctx* ctx, int M, int N, long K, double alpha, const double* A, long rsA, long csA,
+                    const double* B, long rsB, long csB, double beta, double* C, long ldc, bool same, bool upper,
+                    int bits) {
+  const int n = crt_moduli(bits, bits, K);
+  if (n < 1) return fail(ctx, BBT_ERR_ARG, "crt: %d bits over K=%ld needs too many moduli", bits, K);
+  const long Kp = crt_pitch(K);
+  const size_t mark = ctx->ws.top;
+  int8_t* RA = ctx->ws.take<int8_t>((size_t)n * M * Kp);
+  int8_t* RB = same ? RA : ctx->ws.take<int8_t>((size_t)n * N * Kp);
+  double* sa = ctx->ws.take<double>(M);
+  double* sb = same ? sa : ctx->ws.take<double>(N);
+  uint8_t* R = ctx->ws.take<uint8_t>(crt_product_bytes(ctx, M, N, K, n, upper));
+  if (!R) return fail(ctx, BBT_ERR_NOMEM, "crt: workspace");
+  auto prep = [&](int rows, const double* X, long rs, long cs, double* s, int8_t* planes) -> bbt_status {
+    if (cs == 1) {
+      const size_t m2 = ctx->ws.top;
+      BBT_TRY(crt_row_scales(ctx, rows, K, X, rs, s));
+      ctx->ws.top = m2;
+      return crt_residues_rows(ctx, rows, K, X, rs, s, bits, n, planes, Kp);
+    }
+    if (rs == 1) {   // scales of rows contiguous in i: the row maxima over K of the transposed view
+      return fail(ctx, BBT_ERR_ARG, "crt: row scales of a column-contiguous operand are not built");
+    }
+    return fail(ctx, BBT_ERR_ARG, "crt: operand needs a unit stride");
+  };
+  BBT_TRY(prep(M, A, rsA, csA, sa, RA));
+  if (!same) BBT_TRY(prep(N, B, rsB, csB, sb, RB));
+  int splits = 1;
+  BBT_TRY(crt_product(ctx, M, N, K, n, RA, RB, Kp, upper, R, &splits));
+  BBT_TRY(crt_combine(ctx, M, N, n, splits, R, upper, sa, sb, 2 * (bits - 1), alpha, beta, C, ldc));
+  ctx->ws.top = mark;
+  return BBT_OK;
+}
+
+}  // namespace bbt

@@ -1,0 +1,182 @@
+// Double-double (about 106-bit) triangular solves with an FP64 triangular
+// factor, for the preconditioned exact Gram of the mixed-precision local QR:
+//
+//   solve R^T X = B  (trans)   or   R X = B,   R upper m x m (column-major, FP64),
+//   X, B m x k column-major double-doubles (hi + lo arrays), in place.
+//
+// Blocked in 32-row panels: a leaf kernel solves a diagonal block for every
+// column (one thread per column, substitution in double-double), an update
+// kernel subtracts the block's contribution from the rows still to solve
+// (one thread per element, products of an FP64 and a double-double
+// accumulated in double-double).  The double-double operations are the
+// classical error-free transformations (Knuth's two-sum, the FMA two-product)
+// with the usual renormalisations.
+#include <cuda_runtime.h>
+
+#include "internal.h"
+
+namespace bbt {
+namespace {
+
+constexpr int NB = 32;
+
+struct dd {
+  double hi, lo;
+};
+
+__device__ __forceinline__ dd two_sum(double a, double b) {
+  const double s = a + b;
+  const double bb = s - a;
+  return {s, (a - (s - bb)) + (b - bb)};
+}
+__device__ __forceinline__ dd quick_two_sum(double a, double b) {   // |a| >= |b|
+  const double s = a + b;
+  return {s, b - (s - a)};
+}
+__device__ __forceinline__ dd dd_add(dd x, dd y) {
+  dd s = two_sum(x.hi, y.hi);
+  const dd t = two_sum(x.lo, y.lo);
+  s.lo += t.hi;
+  s = quick_two_sum(s.hi, s.lo);
+  s.lo += t.lo;
+  return quick_two_sum(s.hi, s.lo);
+}
+// a (double) times x (double-double)
+__device__ __forceinline__ dd dd_mul_d(dd x, double a) {
+  const double p = x.hi * a;
+  const double e = fma(x.hi, a, -p) + x.lo * a;
+  return quick_two_sum(p, e);
+}
+// x / a (a double): q1 = x.hi / a, the remainder x - q1 a exactly, then its quotient
+__device__ __forceinline__ dd dd_div_d(dd x, double a) {
+  const double q1 = x.hi / a;
+  const double p = q1 * a;
+  const double pe = fma(q1, a, -p);
+  const dd r = dd_add(x, {-p, -pe});
+  const double q2 = r.hi / a;
+  return quick_two_sum(q1, q2);
+}
+
+// Diagonal block [j0, j0 + nb) of R: X[j0.., c] <- R_jj^{-T} X (trans) or R_jj^{-1} X.
+__global__ void leaf_kernel(int trans, int nb, int j0, int k, const double* __restrict__ R, long ldr,
+                            double* __restrict__ Xh, double* __restrict__ Xl, long ldx) {
+  __shared__ double Rs[NB][NB + 1];   // Rs[r][c] = R(j0 + r, j0 + c)
+  for (int f = threadIdx.x; f < NB * NB; f += blockDim.x) {
+    const int r = f % NB, c = f / NB;
+    Rs[r][c] = (r < nb && c < nb) ? R[(j0 + r) + (long)(j0 + c) * ldr] : 0.0;
+  }
+  __syncthreads();
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= k) return;
+  double* xh = Xh + (long)col * ldx + j0;
+  double* xl = Xl + (long)col * ldx + j0;
+  dd x[NB];
+  for (int r = 0; r < nb; ++r) x[r] = {xh[r], xl[r]};
+  if (trans) {   // forward: R^T is lower, row r of R^T is column r of R
+    for (int r = 0; r < nb; ++r) {
+      dd s = x[r];
+      for (int t = 0; t < r; ++t) s = dd_add(s, dd_mul_d(x[t], -Rs[t][r]));
+      x[r] = dd_div_d(s, Rs[r][r]);
+    }
+  } else {       // backward with the upper R
+    for (int r = nb - 1; r >= 0; --r) {
+      dd s = x[r];
+      for (int t = r + 1; t < nb; ++t) s = dd_add(s, dd_mul_d(x[t], -Rs[r][t]));
+      x[r] = dd_div_d(s, Rs[r][r]);
+    }
+  }
+  for (int r = 0; r < nb; ++r) {
+    xh[r] = x[r].hi;
+    xl[r] = x[r].lo;
+  }
+}
+
+// X[i, c] -= sum_t A(i, t) X[j0 + t, c] for rows i in [r0, r1), A(i, t) =
+// R(j0 + t, i) (trans) or R(i, j0 + t).
+__global__ void update_kernel(int trans, int nb, int j0, int r0, int r1, int k, const double* __restrict__ R,
+                              long ldr, double* __restrict__ Xh, double* __restrict__ Xl, long ldx) {
+  const int i = r0 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int col = blockIdx.y;
+  if (i >= r1 || col >= k) return;
+  const double* bh = Xh + (long)col * ldx + j0;
+  const double* bl = Xl + (long)col * ldx + j0;
+  dd s = {0.0, 0.0};
+  for (int t = 0; t < nb; ++t) {
+    const double a = trans ? R[(j0 + t) + (long)i * ldr] : R[i + (long)(j0 + t) * ldr];
+    s = dd_add(s, dd_mul_d({bh[t], bl[t]}, a));
+  }
+  const long o = (long)col * ldx + i;
+  const dd x = dd_add({Xh[o], Xl[o]}, {-s.hi, -s.lo});
+  Xh[o] = x.hi;
+  Xl[o] = x.lo;
+}
+
+__global__ void dd_transpose_kernel(int m, const double* __restrict__ Ah, const double* __restrict__ Al, long lda,
+                                    double* __restrict__ Th, double* __restrict__ Tl, long ldt) {
+  __shared__ double th[32][33], tl[32][33];
+  const int bx = blockIdx.x * 32, by = blockIdx.y * 32;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int i = bx + threadIdx.x, j = by + r;
+    if (i < m && j < m) {
+      th[r][threadIdx.x] = Ah[i + (long)j * lda];
+      tl[r][threadIdx.x] = Al[i + (long)j * lda];
+    }
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int i = by + threadIdx.x, j = bx + r;
+    if (i < m && j < m) {
+      Th[i + (long)j * ldt] = th[threadIdx.x][r];
+      Tl[i + (long)j * ldt] = tl[threadIdx.x][r];
+    }
+  }
+}
+
+__global__ void dd_symmetrize_kernel(int m, double* __restrict__ Gh, double* __restrict__ Gl, long ld) {
+  const long total = (long)m * m;
+  for (long f = blockIdx.x * (long)blockDim.x + threadIdx.x; f < total; f += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(f % m), j = (int)(f / m);
+    if (i > j) {
+      Gh[i + (long)j * ld] = Gh[j + (long)i * ld];
+      Gl[i + (long)j * ld] = Gl[j + (long)i * ld];
+    }
+  }
+}
+
+}  // namespace
+
+bbt_status dd_trsm_left(bbt_ctx* ctx, bool trans, int m, int k, const double* R, long ldr, double* Xh, double* Xl,
+                        long ldx) {
+  if (m < 1 || k < 1) return BBT_OK;
+  const int nblk = (m + NB - 1) / NB;
+  for (int s = 0; s < nblk; ++s) {
+    const int b = trans ? s : nblk - 1 - s;
+    const int j0 = b * NB, nb = (j0 + NB <= m) ? NB : m - j0;
+    leaf_kernel<<<(k + 63) / 64, 64, 0, ctx->stream>>>(trans ? 1 : 0, nb, j0, k, R, ldr, Xh, Xl, ldx);
+    BBT_LAUNCHED(ctx);
+    const int r0 = trans ? j0 + nb : 0, r1 = trans ? m : j0;   // rows still to solve
+    if (r1 > r0) {
+      if (k > 65535) return fail(ctx, BBT_ERR_ARG, "dd_trsm: k=%d", k);
+      update_kernel<<<dim3((unsigned)((r1 - r0 + 127) / 128), (unsigned)k), 128, 0, ctx->stream>>>(
+          trans ? 1 : 0, nb, j0, r0, r1, k, R, ldr, Xh, Xl, ldx);
+      BBT_LAUNCHED(ctx);
+    }
+  }
+  return BBT_OK;
+}
+
+bbt_status dd_transpose(bbt_ctx* ctx, int m, const double* Ah, const double* Al, long lda, double* Th, double* Tl,
+                        long ldt) {
+  dim3 b(32, 8), g((m + 31) / 32, (m + 31) / 32);
+  dd_transpose_kernel<<<g, b, 0, ctx->stream>>>(m, Ah, Al, lda, Th, Tl, ldt);
+  BBT_LAUNCHED(ctx);
+  return BBT_OK;
+}
+
+bbt_status dd_symmetrize_upper(bbt_ctx* ctx, int m, double* Gh, double* Gl, long ld) {
+  dd_symmetrize_kernel<<<2 * ctx->num_sms, 256, 0, ctx->stream>>>(m, Gh, Gl, ld);
+  BBT_LAUNCHED(ctx);
+  return BBT_OK;
+}
+
+}  // namespace bbt

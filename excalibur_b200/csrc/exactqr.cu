@@ -1,0 +1,169 @@
+// Exact-Gram local QR (precision mode 2): the R factor of A = X^T without
+// forming Q, and the products with the implicit Q, for the participant
+// blocks (the replacement of client.cpp:417-445's dgeqrf/dorgqr and of the
+// back-transform products with local_v, :1188-1195) and for the global QR
+// (:705-794 and the products with its Q, :1179).
+//
+//   1. R_p = chol(Y^T Y + shift), Y = S A the BF16x3 sketch (sketch.cu) --
+//      a preconditioner: A R_p^-1 is well conditioned;
+//   2. G = X X^T exactly: every row of X rounded to a 53-bit integer relative
+//      to a power-of-two row scale (exact for every entry whose exponent is
+//      within 0..-1 of its row's largest, the rest to 2^-53 of that largest),
+//      the integer product computed exactly from int8 residues on the tensor
+//      cores (crt.cu) and kept as a double-double;
+//   3. G_Q = R_p^-T G R_p^-1 in double-double (ddsolve.cu): the Gram of
+//      Q_p = A_int R_p^-1 to ~2^-100 of its norm, well conditioned, so
+//      R_3 = chol(G_Q) in FP64 is as accurate as R_3 can be;
+//   4. R = R_3 R_p, W = R_3^-1, Q = A_int R_p^-1 W (never formed), and
+//      dgeqrf's row signs recovered from Q's top block as mixedqr.cu does.
+//
+// Products with Q (exact_apply_q) use the same integers A_int, so Q and R
+// describe the same matrix: C = Q Z = A_int (R_p^-1 (W Z)) with R_p^-1 (W Z)
+// solved in double-double, rounded to 80-bit integers per column and
+// multiplied exactly by A_int (19 moduli at K = 1000).  No triangular solve
+// over the long dimension of A is left: the Gram and the back-transform are
+// the only passes over it.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "internal.h"
+
+namespace bbt {
+namespace {
+
+constexpr int GRAM_BITS = 53;
+constexpr int Z_BITS = 80;
+
+__global__ void dd_scale_rows_kernel(int m, int k, const double* __restrict__ s, double* __restrict__ Zh,
+                                     double* __restrict__ Zl, long ld) {
+  const long total = (long)m * k;
+  for (long f = blockIdx.x * (long)blockDim.x + threadIdx.x; f < total; f += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(f % m);
+    const long j = f / m;
+    Zh[i + j * ld] *= s[i];   // powers of two: exact
+    Zl[i + j * ld] *= s[i];
+  }
+}
+
+__global__ void zero_kernel(double* __restrict__ p, long n) {
+  for (long f = blockIdx.x * (long)blockDim.x + threadIdx.x; f < n; f += (long)gridDim.x * blockDim.x) p[f] = 0.0;
+}
+
+}  // namespace
+
+size_t exact_qr_workspace_bytes(const bbt_ctx* ctx, int m, long n) {
+  const int N = sketch_rows(m);
+  const int nm = crt_moduli(GRAM_BITS, GRAM_BITS, n);
+  const long Kp = crt_pitch(n);
+  size_t s = sketch_workspace_bytes(ctx, m, n, N);
+  s = std::max(s, dgemm_workspace_bytes(ctx, m, m, N));
+  s = std::max(s, (size_t)nm * m * Kp + crt_product_bytes(ctx, m, m, n, nm, true) + (size_t)m * 8 + 4096);
+  return s + ((size_t)N * m + 6 * (size_t)m * m + 2 * m) * 8 + 16384;
+}
+
+bbt_status exact_local_qr(bbt_ctx* ctx, int m, long n, const double* X, const void* S, long spitch, double* R,
+                          double* W, double* Rp, double* scale) {
+  if (n < m) return fail(ctx, BBT_ERR_ARG, "exact local QR: n=%ld < m=%d", n, m);
+  const int nm = crt_moduli(GRAM_BITS, GRAM_BITS, n);
+  if (nm < 1) return fail(ctx, BBT_ERR_ARG, "exact local QR: n=%ld too long", n);
+  const int N = sketch_rows(m);
+  const size_t mark = ctx->ws.top;
+  double* Y = ctx->ws.take<double>((size_t)N * m);
+  double* Gh = ctx->ws.take<double>((size_t)m * m);
+  double* Gl = ctx->ws.take<double>((size_t)m * m);
+  double* Th = ctx->ws.take<double>((size_t)m * m);
+  double* Tl = ctx->ws.take<double>((size_t)m * m);
+  double* dsig = ctx->ws.take<double>(m);
+  if (!dsig) return fail(ctx, BBT_ERR_NOMEM, "exact local QR: workspace");
+  int* flag = ctx->d_flag + FLAG_CHOL;
+  // 1. the preconditioner from the sketch
+  BBT_TRY(sketch_bf16x3(ctx, m, n, X, n, N, S, spitch, Y));
+  BBT_TRY(dgemm(ctx, true, false, m, m, N, 1.0, Y, N, Y, N, 0.0, Rp, m, 0, true));
+  BBT_TRY(symmetrize_upper(ctx, m, Rp, m));
+  BBT_TRY(shift_diag(ctx, m, Rp, m, 1e-14));
+  BBT_TRY(potrf_upper(ctx, m, Rp, m, flag));
+  // 2. the exact Gram of the 53-bit rows of X, as a double-double
+  {
+    const size_t m2 = ctx->ws.top;
+    const long Kp = crt_pitch(n);
+    int8_t* RX = ctx->ws.take<int8_t>((size_t)nm * m * Kp);
+    const size_t m3 = ctx->ws.top;
+    BBT_TRY(crt_row_scales(ctx, m, n, X, n, scale));
+    ctx->ws.top = m3;
+    uint8_t* Rb = ctx->ws.take<uint8_t>(crt_product_bytes(ctx, m, m, n, nm, true));
+    if (!Rb) return fail(ctx, BBT_ERR_NOMEM, "exact local QR: Gram workspace");
+    BBT_TRY(crt_residues_rows(ctx, m, n, X, n, scale, GRAM_BITS, nm, RX, Kp));
+    int splits = 1;
+    BBT_TRY(crt_product(ctx, m, m, n, nm, RX, RX, Kp, true, Rb, &splits));
+    BBT_TRY(crt_combine_dd(ctx, m, m, nm, splits, Rb, true, scale, scale, 2 * (GRAM_BITS - 1), Gh, Gl, m));
+    BBT_TRY(dd_symmetrize_upper(ctx, m, Gh, Gl, m));
+    ctx->ws.top = m2;
+  }
+  // 3. G_Q = R_p^-T (R_p^-T G)^T in double-double (G symmetric)
+  BBT_TRY(dd_trsm_left(ctx, true, m, m, Rp, m, Gh, Gl, m));
+  BBT_TRY(dd_transpose(ctx, m, Gh, Gl, m, Th, Tl, m));
+  BBT_TRY(dd_trsm_left(ctx, true, m, m, Rp, m, Th, Tl, m));
+  // 4. R_3 = chol(G_Q), R = R_3 R_p, W = R_3^-1 (Gh is free again)
+  BBT_TRY(potrf_upper(ctx, m, Th, m, flag));
+  BBT_TRY(dgemm(ctx, false, false, m, m, m, 1.0, Th, m, Rp, m, 0.0, R, m));
+  BBT_TRY(identity(ctx, m, W, m));
+  BBT_TRY(trsm_right_upper(ctx, m, m, Th, m, W, m));
+  // 5. dgeqrf's row signs from Q's top m x m block: A[:m] R_p^-1 W
+  BBT_TRY(copy2d(ctx, m, m, X, n, Gh, m));   // columns of A[:m] = rows of X, first m entries
+  BBT_TRY(trsm_right_upper(ctx, m, m, Rp, m, Gh, m));
+  BBT_TRY(dgemm(ctx, false, false, m, m, m, 1.0, Gh, m, W, m, 0.0, Tl, m));
+  BBT_TRY(householder_signs(ctx, m, m, Tl, m, dsig));
+  BBT_TRY(apply_signs(ctx, m, dsig, R, W));
+  ctx->ws.top = mark;
+  return BBT_OK;
+}
+
+size_t exact_apply_workspace_bytes(const bbt_ctx* ctx, long rows, int m, int k) {
+  const int nm = crt_moduli(GRAM_BITS, Z_BITS, m);
+  const long Kp = crt_pitch(m);
+  return (size_t)nm * (rows + k) * Kp + crt_product_bytes(ctx, (int)rows, k, m, nm, false) +
+         (4 * (size_t)m * k + 2 * (size_t)k) * 8 + 16384;
+}
+
+// C (rows x k, column-major, ldc) = A_int R_p^-1 Z, A_int(j, i) the 53-bit
+// integers of X(i, j) = X[i ldx + j] (i < m, j < rows) at the row scales of X
+// (those exact_local_qr used), Z (m x k, column-major, FP64).
+bbt_status exact_apply_q(bbt_ctx* ctx, int m, long rows, const double* X, long ldx, const double* scale,
+                         const double* Rp, const double* Z, int k, double* C, long ldc) {
+  const int nm = crt_moduli(GRAM_BITS, Z_BITS, m);
+  if (nm < 1) return fail(ctx, BBT_ERR_ARG, "exact apply: m=%d", m);
+  if (rows > 0x7fffffffL) return fail(ctx, BBT_ERR_ARG, "exact apply: rows=%ld", rows);
+  const size_t mark = ctx->ws.top;
+  const long Kp = crt_pitch(m);
+  double* Zh = ctx->ws.take<double>((size_t)m * k);
+  double* Zl = ctx->ws.take<double>((size_t)m * k);
+  double* t = ctx->ws.take<double>(k);
+  int8_t* RA = ctx->ws.take<int8_t>((size_t)nm * rows * Kp);
+  int8_t* RB = ctx->ws.take<int8_t>((size_t)nm * k * Kp);
+  uint8_t* Rb = ctx->ws.take<uint8_t>(crt_product_bytes(ctx, (int)rows, k, m, nm, false));
+  if (!Rb) return fail(ctx, BBT_ERR_NOMEM, "exact apply: workspace");
+  // Z2 = diag(scale) R_p^-1 Z in double-double (the row scales of X fold into Z's rows)
+  BBT_TRY(copy2d(ctx, m, k, Z, m, Zh, m));
+  zero_kernel<<<2 * ctx->num_sms, 256, 0, ctx->stream>>>(Zl, (long)m * k);
+  BBT_LAUNCHED(ctx);
+  BBT_TRY(dd_trsm_left(ctx, false, m, k, Rp, m, Zh, Zl, m));
+  dd_scale_rows_kernel<<<2 * ctx->num_sms, 256, 0, ctx->stream>>>(m, k, scale, Zh, Zl, m);
+  BBT_LAUNCHED(ctx);
+  // residues: B rows = columns of Z2 (80-bit integers, their own scales); A rows = columns of X
+  {
+    const size_t m2 = ctx->ws.top;
+    BBT_TRY(crt_row_scales(ctx, k, m, Zh, m, t));
+    ctx->ws.top = m2;
+  }
+  BBT_TRY(crt_residues_dd(ctx, k, m, Zh, Zl, m, t, Z_BITS, nm, RB, Kp));
+  BBT_TRY(crt_residues_cols(ctx, (int)rows, m, X, ldx, scale, GRAM_BITS, nm, RA, Kp));
+  int splits = 1;
+  BBT_TRY(crt_product(ctx, (int)rows, k, m, nm, RA, RB, Kp, false, Rb, &splits));
+  BBT_TRY(crt_combine(ctx, (int)rows, k, nm, splits, Rb, false, nullptr, t, (GRAM_BITS - 1) + (Z_BITS - 1), 1.0,
+                      0.0, C, ldc));
+  ctx->ws.top = mark;
+  return BBT_OK;
+}
+
+}  // namespace bbt

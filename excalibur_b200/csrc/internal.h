@@ -262,6 +262,56 @@ bbt_status gemm_oz(bbt_ctx* ctx, int M, int N, long K, double alpha, const doubl
                    const double* B, long rsB, long csB, double beta, double* C, long ldc, bool same, bool upper,
                    int S = 8);
 
+// Exact integer products on the int8 tensor cores by the Chinese remainder
+// theorem (crt.cu).  Operands are rounded per row to b-bit integers
+// (t = rint(x 2^(b-1) / s_i), s_i a power of two above 2 max|x|) and given as
+// residue planes [modulus][row][Kp] (int8, centred); the product's residues
+// are bytes [split][modulus][N][M] that crt_combine turns back into
+// C = alpha sa_i sb_j 2^-shift T + beta C (or a double-double).
+long crt_pitch(long K);
+int crt_moduli(int bits_a, int bits_b, long K);   // moduli for an exact product; -1 if too many
+bbt_status crt_row_scales(bbt_ctx* ctx, int rows, long K, const double* X, long rs, double* scale);
+bbt_status crt_residues_rows(bbt_ctx* ctx, int rows, long K, const double* X, long rs, const double* scale, int b,
+                             int n, int8_t* planes, long Kp);
+// X(i, k) = X[i + k cs] with the scale of K index k (the transposed layout of
+// the same integers as crt_residues_rows on X^T)
+bbt_status crt_residues_cols(bbt_ctx* ctx, int rows, long K, const double* X, long cs, const double* kscale, int b,
+                             int n, int8_t* planes, long Kp);
+bbt_status crt_residues_dd(bbt_ctx* ctx, int rows, long K, const double* Xh, const double* Xl, long rs,
+                           const double* scale, int b, int n, int8_t* planes, long Kp);
+size_t crt_product_bytes(const bbt_ctx* ctx, int M, int N, long K, int n, bool upper);
+bbt_status crt_product(bbt_ctx* ctx, int M, int N, long K, int n, const int8_t* RA, const int8_t* RB, long Kp,
+                       bool upper, uint8_t* R, int* splits);
+bbt_status crt_combine(bbt_ctx* ctx, int M, int N, int n, int splits, const uint8_t* R, bool upper, const double* sa,
+                       const double* sb, int shift, double alpha, double beta, double* C, long ldc);
+bbt_status crt_combine_dd(bbt_ctx* ctx, int M, int N, int n, int splits, const uint8_t* R, bool upper,
+                          const double* sa, const double* sb, int shift, double* Ch, double* Cl, long ldc);
+size_t crt_gemm_workspace_bytes(const bbt_ctx* ctx, int M, int N, long K, int bits, bool same, bool upper);
+bool crt_worthwhile(int M, int N, long K);
+// C = alpha A B^T + beta C, operands contiguous along K (csA = csB = 1).
+bbt_status gemm_crt(bbt_ctx* ctx, int M, int N, long K, double alpha, const double* A, long rsA, long csA,
+                    const double* B, long rsB, long csB, double beta, double* C, long ldc, bool same, bool upper,
+                    int bits);
+
+// Double-double triangular solves with an FP64 upper-triangular R (ddsolve.cu):
+// X (m x k column-major, hi + lo arrays) <- R^-T X (trans) or R^-1 X.
+bbt_status dd_trsm_left(bbt_ctx* ctx, bool trans, int m, int k, const double* R, long ldr, double* Xh, double* Xl,
+                        long ldx);
+bbt_status dd_transpose(bbt_ctx* ctx, int m, const double* Ah, const double* Al, long lda, double* Th, double* Tl,
+                        long ldt);
+bbt_status dd_symmetrize_upper(bbt_ctx* ctx, int m, double* Gh, double* Gl, long ld);
+
+// Exact-Gram local QR (exactqr.cu): X row-major m x n (= column-major A = X^T,
+// kept), R (m x m column-major, dgeqrf's row signs), W = R_3^-1 D, the
+// preconditioner Rp and the row scales of X's 53-bit integers; Q = A_int Rp^-1 W.
+size_t exact_qr_workspace_bytes(const bbt_ctx* ctx, int m, long n);
+bbt_status exact_local_qr(bbt_ctx* ctx, int m, long n, const double* X, const void* S, long spitch, double* R,
+                          double* W, double* Rp, double* scale);
+// C (rows x k column-major) = A_int Rp^-1 Z for A_int(j, i) the integers of X[i ldx + j].
+size_t exact_apply_workspace_bytes(const bbt_ctx* ctx, long rows, int m, int k);
+bbt_status exact_apply_q(bbt_ctx* ctx, int m, long rows, const double* X, long ldx, const double* scale,
+                         const double* Rp, const double* Z, int k, double* C, long ldc);
+
 // Mixed-precision local QR (mixedqr.cu): X (row-major m x n = column-major
 // A = X^T, n x m) -> Q_p in place, R (m x m column-major upper), W = R_3^{-1}
 // (optional) with Q = Q_p W.  S: sketch_rows(m) x n Rademacher bf16 (row

@@ -30,6 +30,8 @@
 
 namespace bbt {
 
+constexpr int GRAM_BITS = 50;   // rows of Q_p rounded to 50 bits for the CRT Gram (15 moduli at c2's sizes)
+
 bbt_status clear_tc_flags(bbt_ctx* ctx) {
   BBT_CUDA(ctx, cudaMemsetAsync(ctx->d_flag + FLAG_SKETCH, 0, 2 * sizeof(int), ctx->stream));
   return BBT_OK;
@@ -50,6 +52,7 @@ size_t mixed_qr_workspace_bytes(const bbt_ctx* ctx, int m, long n) {
   s = std::max(s, dgemm_workspace_bytes(ctx, m, m, n));
   s = std::max(s, dgemm_workspace_bytes(ctx, m, m, N));
   s = std::max(s, oz_workspace_bytes(ctx, m, m, n, true));                   // Gram
+  s = std::max(s, crt_gemm_workspace_bytes(ctx, m, m, n, GRAM_BITS, true, true));
   s = std::max(s, oz_workspace_bytes(ctx, (int)n, m - (m / 2 + 31) / 32 * 32, (m / 2 + 31) / 32 * 32, false));
   return s + ((size_t)N * m + 3 * (size_t)m * m + m) * 8 + 8192;
 }
@@ -75,7 +78,9 @@ bbt_status mixed_local_qr(bbt_ctx* ctx, int m, long n, double* X, const void* S,
   // 3. Q_p = A R_p^{-1} (in place), G = Q_p^T Q_p, R_3 = chol(G), R = R_3 R_p; the large
   //    products from exact int8 slices on the tensor cores (ozaki.cu), FP64-accurate
   BBT_TRY(trsm_right_upper(ctx, n, m, Gp, m, X, n, true));
-  if (oz_worthwhile(m, m, n))   // 7 slices: the Gram's errors act on R multiplicatively (~2^-50 relative)
+  if (crt_worthwhile(m, m, n))   // exact product of 50-bit rows (crt.cu): errors ~2^-50 relative, as R needs
+    BBT_TRY(gemm_crt(ctx, m, m, n, 1.0, X, n, 1, X, n, 1, 0.0, G, m, true, true, GRAM_BITS));
+  else if (oz_worthwhile(m, m, n))   // 7 slices: the Gram's errors act on R multiplicatively (~2^-50 relative)
     BBT_TRY(gemm_oz(ctx, m, m, n, 1.0, X, n, 1, X, n, 1, 0.0, G, m, true, true, 7));
   else
     BBT_TRY(dgemm(ctx, true, false, m, m, n, 1.0, X, n, X, n, 0.0, G, m, 0, true));

@@ -218,7 +218,7 @@ bbt_status bbt_mixed_local_qr(bbt_ctx* ctx, size_t m, size_t local_n, double* d_
  * switched on. */
 enum { BBT_PROF_DGEMM = 0, BBT_PROF_PANEL = 1, BBT_PROF_MASK = 2, BBT_PROF_RALHA = 3,
        BBT_PROF_BISECT = 4, BBT_PROF_TWISTED = 5, BBT_PROF_SKETCH = 6, BBT_PROF_CHOL = 7,
-       BBT_PROF_OZAKI = 8, BBT_PROF_CLASSES = 9 };
+       BBT_PROF_OZAKI = 8, BBT_PROF_CRT = 9, BBT_PROF_CLASSES = 10 };
 bbt_status bbt_profile(bbt_ctx* ctx, int enable);
 bbt_status bbt_profile_get(bbt_ctx* ctx, int cls, double* ms, uint64_t* launches, double* work);
 
@@ -233,6 +233,38 @@ bbt_status bbt_profile_get(bbt_ctx* ctx, int cls, double* ms, uint64_t* launches
  * d_U row-major m x k, d_VT row-major k x m; top_k <= 0 means all. */
 bbt_status bbt_svd_dense(bbt_ctx* ctx, int m, double* d_X, int top_k, double* d_sigma, double* d_U,
                          double* d_VT, int* h_k);
+
+/* ---- exact integer products on the int8 tensor cores (CRT) ---------------
+ * Rows of each operand are rounded to `bits`-bit integers relative to a
+ * power-of-two row scale (bits <= 53: every double whose exponent is within
+ * bits - 53 of its row's largest stays exact); their integer product is
+ * computed exactly from int8 residues modulo up to 24 pairwise coprime
+ * moduli <= 256 (one tcgen05 int8 GEMM per modulus) and rebuilt by the
+ * Chinese remainder theorem.
+ * bbt_dgemm_crt: d_C (M x N, column-major, ldc) = alpha A^T B + beta C for
+ * column-major d_A (K x M, lda) and d_B (K x N, ldb), rounded to a double.
+ * bbt_gram_dd: the upper triangle of G = X X^T for a row-major m x n d_X
+ * (ldx), as a double-double d_Gh + d_Gl (column-major m x m) with 53-bit rows:
+ * exact up to about 2^-100 of the largest entry. */
+bbt_status bbt_dgemm_crt(bbt_ctx* ctx, int M, int N, long K, double alpha, const double* d_A, long lda,
+                         const double* d_B, long ldb, double beta, double* d_C, long ldc, int bits);
+bbt_status bbt_gram_dd(bbt_ctx* ctx, int m, long n, const double* d_X, long ldx, double* d_Gh, double* d_Gl);
+
+/* ---- exact-Gram local QR (precision mode 2) --------------------------------
+ * bbt_exact_local_qr: the R factor of A = X^T for a row-major m x local_n d_x
+ * (local_n >= m; not modified) from the BF16x3 sketch's preconditioner R_p
+ * and the exact Gram of X's 53-bit rows (bbt_gram_dd), preconditioned in
+ * double-double: d_R (m x m, column-major, dgeqrf's row signs), d_W, d_Rp
+ * (m x m column-major) and d_scale (m) describe Q = A_int R_p^-1 W, with
+ * A_int X^T's rows rounded to 53-bit integers at the row scales d_scale.
+ * bbt_exact_apply_q: d_C (rows x k column-major, ldc) = A_int R_p^-1 d_Z for
+ * d_Z (m x k column-major), A_int(j, i) the integers of d_x[i ldx + j] --
+ * with the outputs of bbt_exact_local_qr for the same d_x and Z = W Z',
+ * d_C = Q Z' (R_p^-1 W Z' solved in double-double and multiplied exactly). */
+bbt_status bbt_exact_local_qr(bbt_ctx* ctx, int m, size_t local_n, const double* d_x, double* d_R, double* d_W,
+                              double* d_Rp, double* d_scale);
+bbt_status bbt_exact_apply_q(bbt_ctx* ctx, int m, size_t rows, const double* d_x, long ldx, const double* d_scale,
+                             const double* d_Rp, const double* d_Z, int k, double* d_C, long ldc);
 
 /* ---- whole pipeline ------------------------------------------------------
  * DecentralizedClient::run() (client.cpp:447-1200) with opt_control 3, for P
