@@ -46,7 +46,7 @@ def c3_rows(seed=0):
     """Row counts of the 64 participants of c3 (seeded)."""
     return [int(r) for r in np.random.default_rng(seed).integers(10_000, 200_001, 64)]
 METRIC = "SVD wall-s at rel err <=1e-10 vs FP64 oracle"
-PRECISION = {"plain": 0, "mixed": 1}
+PRECISION = {"plain": 0, "mixed": 1, "exact": 2}
 
 
 def parse():
@@ -60,7 +60,7 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-sample-rows", type=int, default=50_000)
-    p.add_argument("--precision", default="both", choices=["both", "mixed", "plain"],
+    p.add_argument("--precision", default="both", choices=["both", "mixed", "plain", "exact", "all"],
                    help="both: time plain FP64 then mixed; the JSON value is the mixed run")
     return p.parse_args()
 
@@ -252,7 +252,8 @@ def run_ours(args, rank, world):
     s_ref, U_ref = fp64_oracle(torch, pristine)
     pub, priv = eb.reference_seeds(0, P)
     batched = sum(1 for b in pristine if b.shape[1] // m > 5) >= 8
-    precisions = {"both": ["plain", "mixed"], "plain": ["plain"], "mixed": ["mixed"]}[args.precision]
+    precisions = {"both": ["plain", "mixed"], "plain": ["plain"], "mixed": ["mixed"], "exact": ["exact"],
+                  "all": ["plain", "mixed", "exact"]}[args.precision]
     out_all = {}
     for pname in precisions:
         prec = PRECISION[pname]

@@ -142,6 +142,12 @@ __global__ void scale_kernel(int rows, const unsigned long long* __restrict__ mx
   scale[i] = ldexp(1.0, e + 1);
 }
 
+// 2^(b-1) / s for s a normal power of two, by exponent arithmetic.
+__device__ __forceinline__ double pow2_ratio(int b, double s) {
+  const int e = (int)((__double_as_longlong(s) >> 52) & 0x7FF) - 1023;
+  return __longlong_as_double((long long)(1023 + (b - 1) - e) << 52);
+}
+
 struct ModTab {
   int n;
   int p[MAXMOD];
@@ -173,17 +179,17 @@ __device__ __forceinline__ int residue_pieces(const Pieces& t, const ModTab& T, 
   return r;
 }
 
-// Rows contiguous in k: planes out[p][i][k] (row pitch Kp), four elements per thread.
+// Rows contiguous in k: planes out[p][i][k] (row pitch Kp), four elements per
+// thread; rows over blockIdx.y, K over the x grid.
 __global__ void residues_rows_kernel(int rows, long K, const double* __restrict__ X, long rs,
                                      const double* __restrict__ scale, int b, ModTab T, int8_t* __restrict__ out,
                                      long Kp) {
   const long kq = (K + 3) / 4;
-  const long total = (long)rows * kq;
   const size_t plane = (size_t)rows * Kp;
-  for (long f = blockIdx.x * (long)blockDim.x + threadIdx.x; f < total; f += (long)gridDim.x * blockDim.x) {
-    const int i = (int)(f / kq);
-    const long k = (f - (long)i * kq) * 4;
-    const double mul = ldexp(1.0, b - 1) / scale[i];   // powers of two: exact
+  for (int i = blockIdx.y; i < rows; i += gridDim.y)
+  for (long kk = blockIdx.x * (long)blockDim.x + threadIdx.x; kk < kq; kk += (long)gridDim.x * blockDim.x) {
+    const long k = kk * 4;
+    const double mul = pow2_ratio(b, scale[i]);   // a power of two: exact
     const double* x = X + (long)i * rs + k;
     Pieces t[4];
 #pragma unroll
@@ -215,7 +221,7 @@ __global__ void __launch_bounds__(256) residues_cols_kernel(int rows, long K, co
   for (int r = ty; r < 32; r += 8) {   // tile[k][i]
     const long k = k0 + r;
     const int i = i0 + tx;
-    tile[r][tx] = (i < rows && k < K) ? rint(X[i + k * cs] * (ldexp(1.0, b - 1) / kscale[k])) : 0.0;
+    tile[r][tx] = (i < rows && k < K) ? rint(X[i + k * cs] * pow2_ratio(b, kscale[k])) : 0.0;
   }
   __syncthreads();
   const size_t plane = (size_t)rows * Kp;
@@ -240,7 +246,7 @@ __global__ void residues_dd_kernel(int rows, long K, const double* __restrict__ 
   for (long f = blockIdx.x * (long)blockDim.x + threadIdx.x; f < total; f += (long)gridDim.x * blockDim.x) {
     const int i = (int)(f / K);
     const long k = f - (long)i * K;
-    const double mul = ldexp(1.0, b - 1) / scale[i];
+    const double mul = pow2_ratio(b, scale[i]);
     const double h = Xh[(long)i * rs + k] * mul, l = Xl[(long)i * rs + k] * mul;
     const double th = rint(h);
     const double tl = rint(l + (h - th));
@@ -470,9 +476,9 @@ __device__ __forceinline__ void two_prod(double a, double b, double& p, double& 
 __global__ void combine_kernel(CombArgs A, const double* __restrict__ sa, const double* __restrict__ sb, int shift,
                                double alpha, double beta, double* __restrict__ C, long ldc) {
   const long total = (long)A.M * A.N;
-  for (long f = blockIdx.x * (long)blockDim.x + threadIdx.x; f < total; f += (long)gridDim.x * blockDim.x) {
-    const int i = (int)(f % A.M);
-    const long j = f / A.M;
+  for (int j = blockIdx.y; j < A.N; j += gridDim.y)
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.M; i += gridDim.x * blockDim.x) {
+    const long f = i + (long)j * A.M;
     if (A.upper && (i / TM) * TM >= (j / TN) * TN + TN) continue;   // tile never computed
     uint64_t hi, lo;
     crt_fraction(A, f, total, hi, lo);
@@ -488,9 +494,9 @@ __global__ void combine_kernel(CombArgs A, const double* __restrict__ sa, const 
 __global__ void combine_dd_kernel(CombArgs A, const double* __restrict__ sa, const double* __restrict__ sb, int shift,
                                   double* __restrict__ Ch, double* __restrict__ Cl, long ldc) {
   const long total = (long)A.M * A.N;
-  for (long f = blockIdx.x * (long)blockDim.x + threadIdx.x; f < total; f += (long)gridDim.x * blockDim.x) {
-    const int i = (int)(f % A.M);
-    const long j = f / A.M;
+  for (int j = blockIdx.y; j < A.N; j += gridDim.y)
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.M; i += gridDim.x * blockDim.x) {
+    const long f = i + (long)j * A.M;
     if (A.upper && (i / TM) * TM >= (j / TN) * TN + TN) continue;
     uint64_t hi, lo;
     crt_fraction(A, f, total, hi, lo);
@@ -642,7 +648,9 @@ bbt_status crt_row_scales(bbt_ctx* ctx, int rows, long K, const double* X, long 
 bbt_status crt_residues_rows(bbt_ctx* ctx, int rows, long K, const double* X, long rs, const double* scale, int b,
                              int n, int8_t* planes, long Kp) {
   if (b < 2 || b > 53) return fail(ctx, BBT_ERR_ARG, "crt: %d-bit integers from doubles", b);
-  residues_rows_kernel<<<16 * ctx->num_sms, 256, 0, ctx->stream>>>(rows, K, X, rs, scale, b, mod_tab(n), planes, Kp);
+  const long kq = (K + 3) / 4;
+  const unsigned gx = (unsigned)std::min<long>((kq + 255) / 256, 4096), gy = (unsigned)std::min(rows, 65535);
+  residues_rows_kernel<<<dim3(gx, gy), 256, 0, ctx->stream>>>(rows, K, X, rs, scale, b, mod_tab(n), planes, Kp);
   BBT_LAUNCHED(ctx);
   return BBT_OK;
 }
@@ -752,16 +760,16 @@ CombArgs comb_args(const uint8_t* R, int M, int N, int n, int splits, bool upper
 
 bbt_status crt_combine(bbt_ctx* ctx, int M, int N, int n, int splits, const uint8_t* R, bool upper, const double* sa,
                        const double* sb, int shift, double alpha, double beta, double* C, long ldc) {
-  combine_kernel<<<8 * ctx->num_sms, 256, 0, ctx->stream>>>(comb_args(R, M, N, n, splits, upper), sa, sb, shift, alpha,
-                                                           beta, C, ldc);
+  const dim3 g((unsigned)std::min((M + 255) / 256, 1024), (unsigned)std::min(N, 65535));
+  combine_kernel<<<g, 256, 0, ctx->stream>>>(comb_args(R, M, N, n, splits, upper), sa, sb, shift, alpha, beta, C, ldc);
   BBT_LAUNCHED(ctx);
   return BBT_OK;
 }
 
 bbt_status crt_combine_dd(bbt_ctx* ctx, int M, int N, int n, int splits, const uint8_t* R, bool upper,
                           const double* sa, const double* sb, int shift, double* Ch, double* Cl, long ldc) {
-  combine_dd_kernel<<<8 * ctx->num_sms, 256, 0, ctx->stream>>>(comb_args(R, M, N, n, splits, upper), sa, sb, shift, Ch,
-                                                              Cl, ldc);
+  const dim3 g((unsigned)std::min((M + 255) / 256, 1024), (unsigned)std::min(N, 65535));
+  combine_dd_kernel<<<g, 256, 0, ctx->stream>>>(comb_args(R, M, N, n, splits, upper), sa, sb, shift, Ch, Cl, ldc);
   BBT_LAUNCHED(ctx);
   return BBT_OK;
 }

@@ -5,10 +5,11 @@
 //   X, B m x k column-major double-doubles (hi + lo arrays), in place.
 //
 // Blocked in 32-row panels: a leaf kernel solves a diagonal block for every
-// column (one thread per column, substitution in double-double), an update
-// kernel subtracts the block's contribution from the rows still to solve
-// (one thread per element, products of an FP64 and a double-double
-// accumulated in double-double).  The double-double operations are the
+// column (one thread per column, right-looking substitution in double-double,
+// unrolled into registers), an update kernel subtracts the block's
+// contribution from the rows still to solve (one thread per row and four
+// columns, products of an FP64 and a double-double accumulated in
+// double-double).  The double-double operations are the
 // classical error-free transformations (Knuth's two-sum, the FMA two-product)
 // with the usual renormalisations.
 #include <cuda_runtime.h>
@@ -58,12 +59,15 @@ __device__ __forceinline__ dd dd_div_d(dd x, double a) {
 }
 
 // Diagonal block [j0, j0 + nb) of R: X[j0.., c] <- R_jj^{-T} X (trans) or R_jj^{-1} X.
+// Right-looking and fully unrolled: after x_r is known, every remaining
+// accumulator takes its term, so the updates of a step are independent.
+// Rows past nb are padded with an identity block and a zero right-hand side.
 __global__ void leaf_kernel(int trans, int nb, int j0, int k, const double* __restrict__ R, long ldr,
                             double* __restrict__ Xh, double* __restrict__ Xl, long ldx) {
   __shared__ double Rs[NB][NB + 1];   // Rs[r][c] = R(j0 + r, j0 + c)
   for (int f = threadIdx.x; f < NB * NB; f += blockDim.x) {
     const int r = f % NB, c = f / NB;
-    Rs[r][c] = (r < nb && c < nb) ? R[(j0 + r) + (long)(j0 + c) * ldr] : 0.0;
+    Rs[r][c] = (r < nb && c < nb) ? R[(j0 + r) + (long)(j0 + c) * ldr] : (r == c ? 1.0 : 0.0);
   }
   __syncthreads();
   const int col = blockIdx.x * blockDim.x + threadIdx.x;
@@ -71,44 +75,60 @@ __global__ void leaf_kernel(int trans, int nb, int j0, int k, const double* __re
   double* xh = Xh + (long)col * ldx + j0;
   double* xl = Xl + (long)col * ldx + j0;
   dd x[NB];
-  for (int r = 0; r < nb; ++r) x[r] = {xh[r], xl[r]};
-  if (trans) {   // forward: R^T is lower, row r of R^T is column r of R
-    for (int r = 0; r < nb; ++r) {
-      dd s = x[r];
-      for (int t = 0; t < r; ++t) s = dd_add(s, dd_mul_d(x[t], -Rs[t][r]));
-      x[r] = dd_div_d(s, Rs[r][r]);
+#pragma unroll
+  for (int r = 0; r < NB; ++r) x[r] = (r < nb) ? dd{xh[r], xl[r]} : dd{0.0, 0.0};
+  if (trans) {   // forward with R^T (lower): x_r, then rows t > r lose R(r, t) x_r
+#pragma unroll
+    for (int r = 0; r < NB; ++r) {
+      x[r] = dd_div_d(x[r], Rs[r][r]);
+#pragma unroll
+      for (int t = r + 1; t < NB; ++t) x[t] = dd_add(x[t], dd_mul_d(x[r], -Rs[r][t]));
     }
-  } else {       // backward with the upper R
-    for (int r = nb - 1; r >= 0; --r) {
-      dd s = x[r];
-      for (int t = r + 1; t < nb; ++t) s = dd_add(s, dd_mul_d(x[t], -Rs[r][t]));
-      x[r] = dd_div_d(s, Rs[r][r]);
+  } else {       // backward with the upper R: rows t < r lose R(t, r) x_r
+#pragma unroll
+    for (int r = NB - 1; r >= 0; --r) {
+      x[r] = dd_div_d(x[r], Rs[r][r]);
+#pragma unroll
+      for (int t = 0; t < r; ++t) x[t] = dd_add(x[t], dd_mul_d(x[r], -Rs[t][r]));
     }
   }
-  for (int r = 0; r < nb; ++r) {
-    xh[r] = x[r].hi;
-    xl[r] = x[r].lo;
-  }
+#pragma unroll
+  for (int r = 0; r < NB; ++r)
+    if (r < nb) {
+      xh[r] = x[r].hi;
+      xl[r] = x[r].lo;
+    }
 }
 
 // X[i, c] -= sum_t A(i, t) X[j0 + t, c] for rows i in [r0, r1), A(i, t) =
-// R(j0 + t, i) (trans) or R(i, j0 + t).
+// R(j0 + t, i) (trans) or R(i, j0 + t); four columns per thread (independent
+// accumulation chains sharing the loads of A).
+constexpr int UC = 4;
 __global__ void update_kernel(int trans, int nb, int j0, int r0, int r1, int k, const double* __restrict__ R,
                               long ldr, double* __restrict__ Xh, double* __restrict__ Xl, long ldx) {
   const int i = r0 + blockIdx.x * blockDim.x + threadIdx.x;
-  const int col = blockIdx.y;
-  if (i >= r1 || col >= k) return;
-  const double* bh = Xh + (long)col * ldx + j0;
-  const double* bl = Xl + (long)col * ldx + j0;
-  dd s = {0.0, 0.0};
+  const int c0 = blockIdx.y * UC;
+  if (i >= r1) return;
+  dd s[UC];
+#pragma unroll
+  for (int u = 0; u < UC; ++u) s[u] = {0.0, 0.0};
   for (int t = 0; t < nb; ++t) {
     const double a = trans ? R[(j0 + t) + (long)i * ldr] : R[i + (long)(j0 + t) * ldr];
-    s = dd_add(s, dd_mul_d({bh[t], bl[t]}, a));
+#pragma unroll
+    for (int u = 0; u < UC; ++u)
+      if (c0 + u < k) {
+        const long o = (long)(c0 + u) * ldx + j0 + t;
+        s[u] = dd_add(s[u], dd_mul_d({Xh[o], Xl[o]}, a));
+      }
   }
-  const long o = (long)col * ldx + i;
-  const dd x = dd_add({Xh[o], Xl[o]}, {-s.hi, -s.lo});
-  Xh[o] = x.hi;
-  Xl[o] = x.lo;
+#pragma unroll
+  for (int u = 0; u < UC; ++u)
+    if (c0 + u < k) {
+      const long o = (long)(c0 + u) * ldx + i;
+      const dd x = dd_add({Xh[o], Xl[o]}, {-s[u].hi, -s[u].lo});
+      Xh[o] = x.hi;
+      Xl[o] = x.lo;
+    }
 }
 
 __global__ void dd_transpose_kernel(int m, const double* __restrict__ Ah, const double* __restrict__ Al, long lda,
@@ -152,12 +172,13 @@ bbt_status dd_trsm_left(bbt_ctx* ctx, bool trans, int m, int k, const double* R,
   for (int s = 0; s < nblk; ++s) {
     const int b = trans ? s : nblk - 1 - s;
     const int j0 = b * NB, nb = (j0 + NB <= m) ? NB : m - j0;
-    leaf_kernel<<<(k + 63) / 64, 64, 0, ctx->stream>>>(trans ? 1 : 0, nb, j0, k, R, ldr, Xh, Xl, ldx);
+    leaf_kernel<<<(k + 31) / 32, 32, 0, ctx->stream>>>(trans ? 1 : 0, nb, j0, k, R, ldr, Xh, Xl, ldx);
     BBT_LAUNCHED(ctx);
     const int r0 = trans ? j0 + nb : 0, r1 = trans ? m : j0;   // rows still to solve
     if (r1 > r0) {
-      if (k > 65535) return fail(ctx, BBT_ERR_ARG, "dd_trsm: k=%d", k);
-      update_kernel<<<dim3((unsigned)((r1 - r0 + 127) / 128), (unsigned)k), 128, 0, ctx->stream>>>(
+      const int gy = (k + UC - 1) / UC;
+      if (gy > 65535) return fail(ctx, BBT_ERR_ARG, "dd_trsm: k=%d", k);
+      update_kernel<<<dim3((unsigned)((r1 - r0 + 127) / 128), (unsigned)gy), 128, 0, ctx->stream>>>(
           trans ? 1 : 0, nb, j0, r0, r1, k, R, ldr, Xh, Xl, ldx);
       BBT_LAUNCHED(ctx);
     }

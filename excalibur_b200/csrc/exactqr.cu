@@ -110,7 +110,7 @@ bbt_status exact_local_qr(bbt_ctx* ctx, int m, long n, const double* X, const vo
   BBT_TRY(identity(ctx, m, W, m));
   BBT_TRY(trsm_right_upper(ctx, m, m, Th, m, W, m));
   // 5. dgeqrf's row signs from Q's top m x m block: A[:m] R_p^-1 W
-  BBT_TRY(copy2d(ctx, m, m, X, n, Gh, m));   // columns of A[:m] = rows of X, first m entries
+  BBT_TRY(copy2d(ctx, m, m, X, n, Gh, m));   // column i of A[:m] = the first m entries of row i of X
   BBT_TRY(trsm_right_upper(ctx, m, m, Rp, m, Gh, m));
   BBT_TRY(dgemm(ctx, false, false, m, m, m, 1.0, Gh, m, W, m, 0.0, Tl, m));
   BBT_TRY(householder_signs(ctx, m, m, Tl, m, dsig));
@@ -144,7 +144,7 @@ bbt_status exact_apply_q(bbt_ctx* ctx, int m, long rows, const double* X, long l
   uint8_t* Rb = ctx->ws.take<uint8_t>(crt_product_bytes(ctx, (int)rows, k, m, nm, false));
   if (!Rb) return fail(ctx, BBT_ERR_NOMEM, "exact apply: workspace");
   // Z2 = diag(scale) R_p^-1 Z in double-double (the row scales of X fold into Z's rows)
-  BBT_TRY(copy2d(ctx, m, k, Z, m, Zh, m));
+  BBT_TRY(copy2d(ctx, k, m, Z, m, Zh, m));   // k columns of m entries (copy2d counts rows of its row-major view)
   zero_kernel<<<2 * ctx->num_sms, 256, 0, ctx->stream>>>(Zl, (long)m * k);
   BBT_LAUNCHED(ctx);
   BBT_TRY(dd_trsm_left(ctx, false, m, k, Rp, m, Zh, Zl, m));

@@ -113,8 +113,9 @@ Layout slab_layout(const Layout& L) {
 bbt_status plan(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, Layout& L) {
   if (!cfg || cfg->participants < 1 || !cfg->local_n || !cfg->private_seeds)
     return fail(ctx, BBT_ERR_ARG, "fedsvd: bad config");
-  if (cfg->precision != 0 && cfg->precision != 1)
-    return fail(ctx, BBT_ERR_UNSUPPORTED, "fedsvd: precision mode %d (0 plain, 1 mixed)", cfg->precision);
+  if (cfg->precision < 0 || cfg->precision > 2)
+    return fail(ctx, BBT_ERR_UNSUPPORTED, "fedsvd: precision mode %d (0 plain, 1 mixed, 2 exact Gram)",
+                cfg->precision);
   if (cfg->svd_mode < 0 || cfg->svd_mode > 4)
     return fail(ctx, BBT_ERR_UNSUPPORTED, "fedsvd: svd_mode %d (0..4)", cfg->svd_mode);
   L.P = cfg->participants;
@@ -136,6 +137,7 @@ bbt_status plan(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, Layout& L) {
   }
   L.gn = gn;
   L.tall = L.m > gn;
+  if (L.tall && L.precision == 2) L.precision = 1;   // the slab QRs of the tall branch run as mode 1
   L.npos.push_back(0);
   for (int c = 0; c < L.P; ++c) L.npos.push_back(L.npos.back() + L.n[c]);
   if (cfg->svd_mode == 4 && !L.tall)
@@ -169,6 +171,7 @@ bbt_status plan(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, Layout& L) {
 
 size_t qr_scratch(const bbt_ctx* ctx, const Layout& L, long rows, const QrPlan& qp) {
   if (L.precision == 1) return mixed_qr_workspace_bytes(ctx, (int)L.m, rows) + (8u << 20);
+  if (L.precision == 2) return exact_qr_workspace_bytes(ctx, (int)L.m, rows) + (8u << 20);
   return qr_workspace_bytes(rows, (int)L.m, (int)L.m, qp) + (8u << 20);
 }
 
@@ -181,6 +184,13 @@ size_t scratch_bytes(const bbt_ctx* ctx, const Layout& L) {
     s = std::max(s, qr_scratch(ctx, L, (long)L.rg, qp));
     for (int c = 0; c < L.P; ++c)   // the V back-transform from int8 slices
       if (L.qr[c]) s = std::max(s, oz_workspace_bytes(ctx, (int)L.n[c], (int)L.m, (long)L.m, false) + (8u << 20));
+  }
+  if (L.precision == 2) {   // the global QR and the exact products with the implicit Q's
+    s = std::max(s, qr_scratch(ctx, L, (long)L.rg, qp));
+    for (int c = 0; c < L.P; ++c) {
+      s = std::max(s, exact_apply_workspace_bytes(ctx, (long)L.r[c], (int)L.m, (int)L.m) + (8u << 20));
+      if (L.qr[c]) s = std::max(s, exact_apply_workspace_bytes(ctx, (long)L.n[c], (int)L.m, (int)L.m) + (8u << 20));
+    }
   }
   s = std::max(s, qr_workspace_bytes((long)L.rg, (int)L.m, (int)L.m, qp));
   const size_t m = L.m;
@@ -204,10 +214,11 @@ size_t persistent_bytes(const Layout& L) {
   b += (4 * m * m + 6 * m) * 8 + 2048;                               // W, house, Vr, U_b(+V_b), alpha...
   b += m * m * 8 + 256;                                              // V_b
   b += m * std::max(m, L.rg) * 8 + 256;                              // tmp
-  if (L.precision == 1) {                                            // W_c, W_g, Z, R_g, the sketch S
+  if (L.precision >= 1) {                                            // W_c, W_g, Z, R_g, the sketch S
     b += (size_t)(L.P + 3) * (m * m * 8 + 256);
     b += (size_t)sketch_rows((int)m) * sketch_pitch((long)std::max(L.nmax, L.rg)) * 2 + 256;
   }
+  if (L.precision == 2) b += (size_t)(L.P + 1) * ((m * m + m) * 8 + 512);   // R_p and the row scales
   return b;
 }
 
@@ -220,6 +231,7 @@ struct QrJob {
   const void* S = nullptr;
   long spitch = 0;
   std::vector<double*> RT, tau, T, W;
+  std::vector<double*> Rp, scale;   // precision 2: the preconditioner and X's row scales
   bool compute_v = false;
 };
 
@@ -257,6 +269,8 @@ size_t batched_scratch(const bbt_ctx* ctx, const Layout& L, int streams, const Q
 bbt_status qr_one(bbt_ctx* c, int mi, double* X, long n, int p, const QrJob& job, const QrPlan& qp) {
   if (job.precision == 1)   // R (column-major) is R^T row-major: the same bytes as r_transpose's output
     return mixed_local_qr(c, mi, n, X, job.S, job.spitch, job.RT[p], job.compute_v ? job.W[p] : nullptr);
+  if (job.precision == 2)   // X kept: Q = X_int^T Rp^-1 W is applied by exact products
+    return exact_local_qr(c, mi, n, X, job.S, job.spitch, job.RT[p], job.W[p], job.Rp[p], job.scale[p]);
   BBT_TRY(geqrf(c, n, mi, X, n, job.tau[p], job.T[p], qp));
   BBT_TRY(r_transpose(c, mi, X, n, job.RT[p]));
   if (job.compute_v) BBT_TRY(orgqr(c, n, mi, X, n, job.tau[p], job.T[p], qp));   // X_c <- Q (= local_v)
@@ -605,7 +619,7 @@ bbt_status fedsvd_tall(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, const Layout&
   }
   BBT_CUDA(ctx, cudaEventRecord(ev[6], ctx->stream));
   BBT_CUDA(ctx, cudaEventSynchronize(ev[6]));
-  if (L.precision == 1) BBT_TRY(check_tc_flags(ctx, "fedsvd: tensor-core back-transform"));
+  if (L.precision >= 1) BBT_TRY(check_tc_flags(ctx, "fedsvd: tensor-core back-transform"));
   // stage order of the reference's timers: local_qr, apply_mask, global_qr
   // (here the repartition gather; this branch has no global QR), bi_diag,
   // bsvd, combine_svd_remove_mask
@@ -688,10 +702,10 @@ bbt_status fedsvd(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* X, 
   job.RT = RT;
   job.tau = tauc;
   job.T = Tc;
-  double *Z = nullptr, *Wg = nullptr, *Rg = nullptr;
+  double *Z = nullptr, *Wg = nullptr, *Rg = nullptr, *Rpg = nullptr, *scg = nullptr;
   void* S = nullptr;
   const long sk_cols = (long)std::max(L.nmax, L.rg);   // the sketch serves the local and the global QR
-  if (L.precision == 1) {
+  if (L.precision >= 1) {
     for (int c = 0; c < P; ++c) job.W.push_back(ctx->ws.take<double>(m * m));
     Z = ctx->ws.take<double>(m * m);
     Wg = ctx->ws.take<double>(m * m);
@@ -700,6 +714,15 @@ bbt_status fedsvd(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* X, 
     if (!S) return fail(ctx, BBT_ERR_NOMEM, "fedsvd: workspace (mixed precision)");
     job.S = S;
     job.spitch = sketch_pitch(sk_cols);
+  }
+  if (L.precision == 2) {
+    for (int c = 0; c < P; ++c) {
+      job.Rp.push_back(ctx->ws.take<double>(m * m));
+      job.scale.push_back(ctx->ws.take<double>(m));
+    }
+    Rpg = ctx->ws.take<double>(m * m);
+    scg = ctx->ws.take<double>(m);
+    if (!scg) return fail(ctx, BBT_ERR_NOMEM, "fedsvd: workspace (exact Gram)");
   }
 
   cudaEvent_t ev[7];
@@ -715,7 +738,7 @@ bbt_status fedsvd(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* X, 
   job.compute_v = compute_v;
   std::vector<double*> masked(P);
   for (int c = 0; c < P; ++c) masked[c] = L.qr[c] ? RT[c] : X[c];
-  if (L.precision == 1) {
+  if (L.precision >= 1) {
     BBT_TRY(rademacher(ctx, sketch_rows(mi), sk_cols, S, 0x5EED5EEDull));
     BBT_TRY(clear_tc_flags(ctx));
   }
@@ -724,7 +747,7 @@ bbt_status fedsvd(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* X, 
     BBT_TRY(local_qr_stage(ctx, L, X, job, streams, qp, true));
     ctx->ws.top = mark;
   }
-  if (L.precision == 1) BBT_TRY(check_tc_flags(ctx, "fedsvd: mixed-precision local QR"));
+  if (L.precision >= 1) BBT_TRY(check_tc_flags(ctx, "fedsvd: mixed-precision local QR"));
   if (ctx->io_on)
     for (int c = 0; c < P; ++c) BBT_TRY(wait_input(ctx, c));
   BBT_CUDA(ctx, cudaEventRecord(ev[1], ctx->stream));
@@ -739,6 +762,12 @@ bbt_status fedsvd(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* X, 
     BBT_TRY(copy2d(ctx, mi, (int)L.r[c], masked[c], (long)L.r[c], M + L.rpos[c], (long)rg));
   if (rg == m) {   // m == global_n: no global QR, Ralha takes M^T (the in-place transpose, client.cpp:795-798)
     BBT_TRY(transpose(ctx, mi, mi, M, (long)rg, W, (long)m));
+  } else if (L.precision == 2) {   // M kept, Q_g = M_int^T Rp_g^-1 W_g (exactqr.cu)
+    const size_t mark = ctx->ws.top;
+    BBT_TRY(exact_local_qr(ctx, mi, (long)rg, M, S, job.spitch, Rg, Wg, Rpg, scg));
+    ctx->ws.top = mark;
+    BBT_TRY(transpose(ctx, mi, mi, Rg, (long)m, W, (long)m));   // W (row-major) = R_g
+    BBT_TRY(check_tc_flags(ctx, "fedsvd: exact-Gram global QR"));
   } else if (L.precision == 1) {   // M <- Q_p, Q_g = Q_p W_g, R_g with dgeqrf's signs (mixedqr.cu)
     const size_t mark = ctx->ws.top;
     BBT_TRY(mixed_local_qr(ctx, mi, (long)rg, M, S, job.spitch, Rg, compute_v ? Wg : nullptr));
@@ -786,7 +815,7 @@ bbt_status fedsvd(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* X, 
   rot_sweep<<<(k + 127) / 128, 128, 0, ctx->stream>>>(mi, k, cs, Ub);
   BBT_LAUNCHED(ctx);
   BBT_TRY(ormqr_left_notrans(ctx, (long)m, mi, house, (long)m, 1, tauh, Ub, k, k, true, qp));
-  if (L.precision == 1)   // Q_g U2 = Q_p (W_g U2): Rg (free by now) <- W_g U2, m x k column-major
+  if (L.precision >= 1)   // Q_g U2 = Q_p (W_g U2): Rg (free by now) <- W_g U2, m x k column-major
     BBT_TRY(dgemm(ctx, false, true, mi, k, m, 1.0, Wg, (long)m, Ub, k, 0.0, Rg, (long)m));
   for (int c = 0; c < P; ++c) {   // :1179-1195
     const int rc = (int)L.r[c];
@@ -802,13 +831,22 @@ bbt_status fedsvd(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* X, 
       continue;
     }
     // tmp (k x r_c row-major) = U2^T Q_g[rows_c, :]^T  ==  column-major r_c x k = Q_g[rows_c,:] U2
-    if (L.precision == 1)
+    if (L.precision == 2) {   // Q_g[rows_c,:] U2 = M_int^T[rows_c] Rp_g^-1 (W_g U2), exactly (exactqr.cu)
+      const size_t mark = ctx->ws.top;
+      BBT_TRY(exact_apply_q(ctx, mi, rc, M + L.rpos[c], (long)rg, scg, Rpg, Rg, k, tmp, rc));
+      ctx->ws.top = mark;
+    } else if (L.precision == 1)
       BBT_TRY(dgemm(ctx, false, false, rc, k, m, 1.0, M + L.rpos[c], (long)rg, Rg, (long)m, 0.0, tmp, rc));
     else
       BBT_TRY(dgemm(ctx, false, true, rc, k, m, 1.0, M + L.rpos[c], (long)rg, Ub, k, 0.0, tmp, rc));
     BBT_TRY(block_shift_mask(ctx, (size_t)k, (size_t)rc, MASK_PASSES, tmp, false, false, cfg->private_seeds[c]));
     const long n = (long)L.n[c];
-    if (L.qr[c] && L.precision == 1) {   // Q_c = Q_p W_c: FinalVT^T = Q_p (W_c tmp^T)
+    if (L.qr[c] && L.precision == 2) {   // Q_c = X_int^T Rp_c^-1 W_c: FinalVT^T = X_int^T Rp_c^-1 (W_c tmp^T)
+      BBT_TRY(dgemm(ctx, false, false, mi, k, m, 1.0, job.W[c], (long)m, tmp, rc, 0.0, Z, (long)m));
+      const size_t mark = ctx->ws.top;
+      BBT_TRY(exact_apply_q(ctx, mi, n, X[c], n, job.scale[c], job.Rp[c], Z, k, VT[c], n));
+      ctx->ws.top = mark;
+    } else if (L.qr[c] && L.precision == 1) {   // Q_c = Q_p W_c: FinalVT^T = Q_p (W_c tmp^T)
       BBT_TRY(dgemm(ctx, false, false, mi, k, m, 1.0, job.W[c], (long)m, tmp, rc, 0.0, Z, (long)m));
       if (oz_worthwhile((int)n, k, (long)m))   // FinalVT^T (n x k) = Q_p Z from exact int8 slices; 6 slices
         BBT_TRY(gemm_oz(ctx, (int)n, k, (long)m, 1.0, X[c], 1, n, Z, (long)m, 1, 0.0, VT[c], n, false, false, 6));
@@ -830,7 +868,7 @@ bbt_status fedsvd(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* X, 
   }
   BBT_CUDA(ctx, cudaEventRecord(ev[6], ctx->stream));
   BBT_CUDA(ctx, cudaEventSynchronize(ev[6]));
-  if (L.precision == 1) BBT_TRY(check_tc_flags(ctx, "fedsvd: tensor-core back-transform"));
+  if (L.precision >= 1) BBT_TRY(check_tc_flags(ctx, "fedsvd: tensor-core back-transform"));
   for (int s = 0; s < 6; ++s) {
     float ms = 0;
     BBT_CUDA(ctx, cudaEventElapsedTime(&ms, ev[s], ev[s + 1]));
@@ -869,7 +907,7 @@ bbt_status fedsvd_tune(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, int* best_str
     if (L.qr[c]) BBT_CUDA(ctx, cudaMalloc(&blocks[c], L.m * L.n[c] * sizeof(double)));
   const int cand_s[] = {1, 4, 8, 16};
   // the panel width only matters to the Householder (precision 0) path
-  const std::vector<int> cand_nb = L.precision == 1 ? std::vector<int>{128} : std::vector<int>{64, 128};
+  const std::vector<int> cand_nb = L.precision >= 1 ? std::vector<int>{128} : std::vector<int>{64, 128};
   size_t need = 0;
   for (int nb : cand_nb)
     for (int st : cand_s) {
@@ -880,7 +918,8 @@ bbt_status fedsvd_tune(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, int* best_str
   const size_t tq = ((L.m + 63) / 64) * 128 * 128;
   const size_t sbytes = (size_t)sketch_rows(mi) * sketch_pitch((long)L.nmax) * 2;
   need += (size_t)P * (L.m * L.m + L.m + tq) * 8 + (size_t)P * 1024 + (64u << 20);
-  if (L.precision == 1) need += (size_t)P * (L.m * L.m * 8 + 256) + sbytes + 256;
+  if (L.precision >= 1) need += (size_t)P * (L.m * L.m * 8 + 256) + sbytes + 256;
+  if (L.precision == 2) need += (size_t)P * ((L.m * L.m + L.m) * 8 + 512);
   if (ctx->ws.cap < need) BBT_CUDA(ctx, ctx->ws.reserve(need));
   ctx->ws.reset();
   QrJob job;
@@ -890,9 +929,13 @@ bbt_status fedsvd_tune(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, int* best_str
     job.RT.push_back(ctx->ws.take<double>(L.m * L.m));
     job.tau.push_back(ctx->ws.take<double>(L.m));
     job.T.push_back(ctx->ws.take<double>(tq));
-    if (L.precision == 1) job.W.push_back(ctx->ws.take<double>(L.m * L.m));
+    if (L.precision >= 1) job.W.push_back(ctx->ws.take<double>(L.m * L.m));
+    if (L.precision == 2) {
+      job.Rp.push_back(ctx->ws.take<double>(L.m * L.m));
+      job.scale.push_back(ctx->ws.take<double>(L.m));
+    }
   }
-  if (L.precision == 1) {
+  if (L.precision >= 1) {
     void* S = ctx->ws.take<char>(sbytes);
     if (!S) return fail(ctx, BBT_ERR_NOMEM, "tune: workspace");
     BBT_TRY(rademacher(ctx, sketch_rows(mi), (long)L.nmax, S, 0x5EED5EEDull));

@@ -81,15 +81,16 @@ def run(ctx, blocks, seed, precision, top_k=-1, svd_mode=1):
             None if VT is None else [v.cpu().numpy() for v in VT])
 
 
+@pytest.mark.parametrize("precision", [1, 2])
 @pytest.mark.parametrize("name", sorted(cases.pipeline_cases()))
-def test_mixed_pipeline_matches_reference(ctx, golden, name):
-    """precision=1 reproduces the reference's outputs on its own inputs:
-    singular values to 1e-12 relative, U and every FinalVT_c to 1e-9 (the
-    local R differs from dgeqrf's only by row signs, which the back-transform
-    cancels)."""
+def test_mixed_pipeline_matches_reference(ctx, golden, name, precision):
+    """precision 1 (sketch + Cholesky QR) and 2 (sketch + exact Gram)
+    reproduce the reference's outputs on its own inputs: singular values to
+    1e-12 relative, U and every FinalVT_c to 1e-9 (dgeqrf's row signs are
+    recovered, so the vectors match, not only their subspaces)."""
     g = golden(f"pipe__{name}")
     blocks, seed = cases.pipeline_cases()[name]
-    s, U, VT = run(ctx, blocks, seed, 1)
+    s, U, VT = run(ctx, blocks, seed, precision)
     assert len(s) == len(g["sigma"])
     assert np.max(np.abs(s - g["sigma"]) / g["sigma"]) < 1e-12
     assert np.max(np.abs(U - g["U"])) < 1e-9
@@ -97,12 +98,13 @@ def test_mixed_pipeline_matches_reference(ctx, golden, name):
         assert np.max(np.abs(v - g[f"VT{c}"])) < 1e-9
 
 
+@pytest.mark.parametrize("precision", [1, 2])
 @pytest.mark.parametrize("name", sorted(cases.pipeline_mode_cases()))
-def test_mixed_pipeline_modes(ctx, golden, name):
+def test_mixed_pipeline_modes(ctx, golden, name, precision):
     g = golden(f"pipe__{name}")
     case, mode, topk = cases.pipeline_mode_cases()[name]
     blocks, seed = cases.pipeline_cases()[case]
-    s, U, VT = run(ctx, blocks, seed, 1, top_k=topk, svd_mode=mode)
+    s, U, VT = run(ctx, blocks, seed, precision, top_k=topk, svd_mode=mode)
     assert np.max(np.abs(s - g["sigma"]) / g["sigma"]) < 1e-12
     if mode != 3:
         assert np.max(np.abs(U - g["U"])) < 1e-9
@@ -111,7 +113,8 @@ def test_mixed_pipeline_modes(ctx, golden, name):
             assert np.max(np.abs(v - g[f"VT{c}"])) < 1e-9
 
 
-def test_mixed_vs_plain_geometric(ctx):
+@pytest.mark.parametrize("precision", [1, 2])
+def test_mixed_vs_plain_geometric(ctx, precision):
     """The tall-skinny family (s from 1 to 1e-6, Haar factors) at reduced
     rows: mixed and plain agree with the exact spectrum to the conditioning
     bound, with each other to 1e-10 relative on sigma >= 1e-4, and the
@@ -124,7 +127,7 @@ def test_mixed_vs_plain_geometric(ctx):
     Xt = (Uq * sv) @ Vq.T
     blocks = [Xt[c * n:(c + 1) * n].T.copy() for c in range(P)]
     s0, U0, V0 = run(ctx, blocks, 3, 0)
-    s1, U1, V1 = run(ctx, blocks, 3, 1)
+    s1, U1, V1 = run(ctx, blocks, 3, precision)
     assert np.max(np.abs(s1 - sv) / sv) < 1e-10 * 1e4
     big = sv >= 1e-4
     assert np.max(np.abs(s1 - s0)[big] / s0[big]) < 1e-10
@@ -136,14 +139,15 @@ def test_mixed_vs_plain_geometric(ctx):
         assert subspace_angle(U1[:, grp], U0[:, grp]) < 1e-8
 
 
-def test_mixed_batched_graph_and_tune(ctx):
-    """Uneven participants on concurrent streams with precision=1: eager,
-    captured and replayed calls all match the oracle."""
+@pytest.mark.parametrize("precision", [1, 2])
+def test_mixed_batched_graph_and_tune(ctx, precision):
+    """Uneven participants on concurrent streams in both split-precision
+    modes: eager, captured and replayed calls all match the oracle."""
     rng = np.random.default_rng(35)
     m = 32
     rows = [int(r) for r in rng.integers(200, 900, 10)]
     blocks = [rng.standard_normal((m, n)) * 10.0 ** rng.uniform(-2, 2) for n in rows]
-    st, nb, ms = ctx.fedsvd_tune(m, rows, precision=1)
+    st, nb, ms = ctx.fedsvd_tune(m, rows, precision=precision)
     assert st in (1, 4, 8, 16) and ms > 0
     pub, priv = oracle.reference_seeds(4, len(blocks))
     so, Uo, VTo = pipeline.run(blocks, pub, priv)
@@ -151,7 +155,7 @@ def test_mixed_batched_graph_and_tune(ctx):
     for call in range(3):
         for d, b in zip(dev, blocks):
             d.copy_(ctx.torch.as_tensor(b, device=d.device))
-        s, U, VT = ctx.fedsvd(dev, pub, priv, precision=1)
+        s, U, VT = ctx.fedsvd(dev, pub, priv, precision=precision)
         s, U = s.cpu().numpy(), U.cpu().numpy()
         assert np.max(np.abs(s - so) / so) < 1e-12, call
         assert np.max(np.abs(U - Uo)) < 1e-9, call
