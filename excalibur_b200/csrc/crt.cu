@@ -27,6 +27,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <utility>
 #include <vector>
 
 #include "internal.h"
@@ -42,6 +43,54 @@ constexpr int MAXMOD = 24;
 // 247 = 13 19, 217 = 7 31; the others are primes.
 constexpr int MODULI[MAXMOD] = {256, 255, 253, 251, 247, 241, 239, 233, 229, 227, 223, 217,
                                 211, 199, 197, 193, 191, 181, 179, 173, 167, 163, 157, 151};
+
+// Compile-time constants of modulus Q of an NM-modulus set, for the kernels
+// templated on NM (every per-modulus constant becomes an immediate once the
+// loop over the moduli is unrolled).
+constexpr int inv_mod_c(int a, int p) {   // a^-1 mod p, gcd(a, p) = 1
+  int t = 0, nt = 1, r = p, nr = a % p;
+  while (nr) {
+    const int q = r / nr;
+    const int x = t - q * nt;
+    t = nt;
+    nt = x;
+    const int y = r - q * nr;
+    r = nr;
+    nr = y;
+  }
+  return t < 0 ? t + p : t;
+}
+constexpr int crt_inv_c(int q, int n) {   // ((M / p_q) mod p_q)^-1 mod p_q, M the product of n moduli
+  long long prod = 1;
+  for (int r = 0; r < n; ++r)
+    if (r != q) prod = prod * (MODULI[r] % MODULI[q]) % MODULI[q];
+  return inv_mod_c((int)prod, MODULI[q]);
+}
+constexpr uint32_t flimb_c(int p, int l) {   // 32-bit limb l of floor(2^128 / p), least significant first
+  const uint32_t digits[5] = {1, 0, 0, 0, 0};   // 2^128 in base 2^32, most significant first
+  uint32_t q[5] = {0, 0, 0, 0, 0};
+  uint64_t rem = 0;
+  for (int d = 0; d < 5; ++d) {
+    const uint64_t cur = (rem << 32) | digits[d];
+    q[d] = (uint32_t)(cur / (uint64_t)p);
+    rem = cur % (uint64_t)p;
+  }
+  return q[4 - l];
+}
+template <int Q>
+struct ModR {   // residues of an integer t = a 2^36 + b 2^18 + c
+  static constexpr int p = MODULI[Q];
+  static constexpr int c36 = (int)((1LL << 36) % p), c18 = (1 << 18) % p;
+  static constexpr int off = p * (((1 << 23) + p - 1) / p);
+  static constexpr uint32_t magic35 = (uint32_t)((((uint64_t)1 << 35) + p - 1) / p);
+};
+template <int Q, int NM>
+struct ModK {   // reconstruction from the residues of an NM-modulus set
+  static constexpr int p = MODULI[Q];
+  static constexpr uint32_t magic32 = (uint32_t)((((uint64_t)1 << 32) + p - 1) / p);
+  static constexpr uint32_t inv = (uint32_t)crt_inv_c(Q, NM);
+  static constexpr uint32_t F0 = flimb_c(p, 0), F1 = flimb_c(p, 1), F2 = flimb_c(p, 2), F3 = flimb_c(p, 3);
+};
 
 constexpr int TM = 128, TN = 256, TK = 128;   // TK: bytes of K per stage row (SWIZZLE_128B)
 constexpr int STAGES = 4;
@@ -169,21 +218,40 @@ __device__ __forceinline__ Pieces pieces(double t) {
   const double c = fma(-b, 0x1p18, rem);
   return {__double2loint(a + RND), __double2loint(b + RND), __double2loint(c + RND)};
 }
-// The centred residue from the pieces: x = a c36 + b c18 + c + off lies in
-// [0, 2^27) and its multiply-high quotient by p is exact.
-__device__ __forceinline__ int residue_pieces(const Pieces& t, const ModTab& T, int q) {
-  const int p = T.p[q];
-  const uint32_t x = (uint32_t)(t.a * T.c36[q] + t.b * T.c18[q] + t.c + T.off[q]);
-  int r = (int)(x - (__umulhi(x, T.magic35[q]) >> 3) * (uint32_t)p);
-  if (r > ((p - 1) >> 1)) r -= p;
+
+// The centred residue of modulus Q from the pieces: x = a c36 + b c18 + c +
+// off lies in [0, 2^27) and its multiply-high quotient by p is exact.
+template <int Q>
+__device__ __forceinline__ int res_q(const Pieces& t) {
+  using C = ModR<Q>;
+  const uint32_t x = (uint32_t)(t.a * C::c36 + t.b * C::c18 + t.c + C::off);
+  int r = (int)(x - (__umulhi(x, C::magic35) >> 3) * (uint32_t)C::p);
+  if (r > ((C::p - 1) >> 1)) r -= C::p;
   return r;
+}
+
+template <int Q>
+__device__ __forceinline__ void store4_q(const Pieces (&t)[4], int8_t* o, int valid) {
+  uint32_t w = 0;
+#pragma unroll
+  for (int e = 0; e < 4; ++e) w |= (uint32_t)(uint8_t)(int8_t)res_q<Q>(t[e]) << (8 * e);
+  if (valid == 4) {
+    *reinterpret_cast<uint32_t*>(o) = w;
+  } else {
+    for (int e = 0; e < valid; ++e) o[e] = (int8_t)(w >> (8 * e));
+  }
+}
+template <int... Q>
+__device__ __forceinline__ void store4_all(const Pieces (&t)[4], int8_t* o, size_t plane, int valid,
+                                           std::integer_sequence<int, Q...>) {
+  (store4_q<Q>(t, o + (size_t)Q * plane, valid), ...);
 }
 
 // Rows contiguous in k: planes out[p][i][k] (row pitch Kp), four elements per
 // thread; rows over blockIdx.y, K over the x grid.
+template <int NM>
 __global__ void residues_rows_kernel(int rows, long K, const double* __restrict__ X, long rs,
-                                     const double* __restrict__ scale, int b, ModTab T, int8_t* __restrict__ out,
-                                     long Kp) {
+                                     const double* __restrict__ scale, int b, int8_t* __restrict__ out, long Kp) {
   const long kq = (K + 3) / 4;
   const size_t plane = (size_t)rows * Kp;
   for (int i = blockIdx.y; i < rows; i += gridDim.y)
@@ -194,43 +262,43 @@ __global__ void residues_rows_kernel(int rows, long K, const double* __restrict_
     Pieces t[4];
 #pragma unroll
     for (int e = 0; e < 4; ++e) t[e] = pieces((k + e < K) ? rint(x[e] * mul) : 0.0);
-    int8_t* o = out + (size_t)i * Kp + k;
-    for (int q = 0; q < T.n; ++q) {
-      uint32_t w = 0;
-#pragma unroll
-      for (int e = 0; e < 4; ++e) w |= (uint32_t)(uint8_t)(int8_t)residue_pieces(t[e], T, q) << (8 * e);
-      if (k + 4 <= K) {
-        *reinterpret_cast<uint32_t*>(o + q * plane) = w;
-      } else {
-        for (int e = 0; k + e < K; ++e) o[q * plane + e] = (int8_t)(w >> (8 * e));
-      }
-    }
+    store4_all(t, out + (size_t)i * Kp + k, plane, (int)min(4L, K - k), std::make_integer_sequence<int, NM>{});
   }
+}
+
+template <int... Q>
+__device__ __forceinline__ void store1_all(const Pieces& t, int8_t* o, size_t plane, std::integer_sequence<int, Q...>) {
+  ((o[(size_t)Q * plane] = (int8_t)res_q<Q>(t)), ...);
 }
 
 // Rows contiguous in i, K stride cs; the scale belongs to the K index
 // (kscale) -- the integers are those residues_rows_kernel forms for the
-// transposed operand.  32 x 32 tiles staged through shared memory.
+// transposed operand.  Tiles of 128 K x 32 rows staged through shared memory
+// (coalesced along i on the way in); four consecutive K per thread on the way
+// out, packed into 32-bit stores (a warp writes 128 contiguous bytes of a plane).
+template <int NM>
 __global__ void __launch_bounds__(256) residues_cols_kernel(int rows, long K, const double* __restrict__ X, long cs,
-                                                            const double* __restrict__ kscale, int b, ModTab T,
+                                                            const double* __restrict__ kscale, int b,
                                                             int8_t* __restrict__ out, long Kp) {
-  __shared__ double tile[32][33];
+  __shared__ double tile[128][33];   // tile[k][i]
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
   const int i0 = blockIdx.x * 32;
-  const long k0 = (long)blockIdx.y * 32;
-  for (int r = ty; r < 32; r += 8) {   // tile[k][i]
+  const long k0 = (long)blockIdx.y * 128;
+  for (int r = ty; r < 128; r += 8) {
     const long k = k0 + r;
     const int i = i0 + tx;
     tile[r][tx] = (i < rows && k < K) ? rint(X[i + k * cs] * pow2_ratio(b, kscale[k])) : 0.0;
   }
   __syncthreads();
   const size_t plane = (size_t)rows * Kp;
-  const long k = k0 + tx;
+  const long k = k0 + 4 * tx;
   for (int r = ty; r < 32; r += 8) {
     const int i = i0 + r;
     if (i < rows && k < K) {
-      const Pieces t = pieces(tile[tx][r]);
-      for (int q = 0; q < T.n; ++q) out[q * plane + (size_t)i * Kp + k] = (int8_t)residue_pieces(t, T, q);
+      Pieces t[4];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) t[e] = pieces(tile[4 * tx + e][r]);
+      store4_all(t, out + (size_t)i * Kp + k, plane, (int)min(4L, K - k), std::make_integer_sequence<int, NM>{});
     }
   }
 }
@@ -261,8 +329,8 @@ __global__ void residues_dd_kernel(int rows, long K, const double* __restrict__ 
 // ---- one int8 GEMM per modulus ------------------------------------------
 
 struct CrtArgs {
-  uint8_t* out;   // residues of T: out[((z * n + q) * N + j) * M + i]
-  int M, N;
+  uint8_t* out;   // residues of T: out[((z * n + q) * N + j) * Mp + i], Mp = M rounded up to 4
+  int M, N, Mp;
   int kblocks, kb_per_split;
   int n;
   int upper;      // 1: skip tiles strictly below the diagonal
@@ -367,7 +435,7 @@ crt_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUte
       tc_fence_after();
       const int p = P.p[q], c16 = P.c16[q];
       const uint32_t magic = P.magic[q], off = (uint32_t)P.off[q];
-      uint8_t* o = P.out + ((size_t)blockIdx.z * P.n + q) * (size_t)P.N * P.M;
+      uint8_t* o = P.out + ((size_t)blockIdx.z * P.n + q) * (size_t)P.N * P.Mp;
 #pragma unroll 1
       for (int c = 0; c < TN / 2 / 16; ++c) {
         uint32_t v[16];
@@ -383,7 +451,7 @@ crt_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUte
           int r = (int)(x - __umulhi(x, magic) * (uint32_t)p) - (int)off;
           if (r < 0) r += p;
           const int j = j0 + e;
-          if (i < P.M && j < P.N) o[(size_t)j * P.M + i] = (uint8_t)r;
+          if (i < P.M && j < P.N) o[(size_t)j * P.Mp + i] = (uint8_t)r;
         }
       }
       tc_fence_before();
@@ -403,38 +471,60 @@ crt_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUte
 // ---- rebuilding T from its residues ---------------------------------------
 
 struct CombArgs {
-  const uint8_t* R;
-  int M, N, n, splits, upper;
-  int p[MAXMOD], inv[MAXMOD];
-  uint32_t magic32[MAXMOD];   // ceil(2^32 / p): exact quotients below 2^24
-  uint32_t F[MAXMOD][4];
-  double mod_hi, mod_lo;
+  const uint8_t* R;        // [split][modulus][N][Mp]
+  int M, N, Mp, splits, upper;
+  double mod_hi, mod_lo;   // M as a double-double
 };
 
 // x mod p for 0 <= x < 2^24 by the multiply-high quotient.
-__device__ __forceinline__ uint32_t mod_small(uint32_t x, uint32_t p, uint32_t magic) {
-  return x - __umulhi(x, magic) * p;
+template <class C>
+__device__ __forceinline__ uint32_t mod_c(uint32_t x) {
+  return x - __umulhi(x, C::magic32) * (uint32_t)C::p;
 }
 
-// The centred fraction f = T / M (mod 1) as a signed 128-bit fixed-point
-// number (two 64-bit halves).
-__device__ __forceinline__ void crt_fraction(const CombArgs& A, long f, long total, uint64_t& hi, uint64_t& lo) {
-  uint64_t L0 = 0, L1 = 0, L2 = 0, L3 = 0;
-  for (int q = 0; q < A.n; ++q) {
-    uint32_t s = 0;
-    for (int z = 0; z < A.splits; ++z) s += A.R[((size_t)z * A.n + q) * total + f];
-    const uint32_t p = (uint32_t)A.p[q], mg = A.magic32[q];
-    const uint32_t y = mod_small(mod_small(s, p, mg) * (uint32_t)A.inv[q], p, mg);
-    L0 += (uint64_t)y * A.F[q][0];   // 32 x 32 -> 64-bit products, < 2^40 each
-    L1 += (uint64_t)y * A.F[q][1];
-    L2 += (uint64_t)y * A.F[q][2];
-    L3 += (uint64_t)y * A.F[q][3];
+// Four consecutive outputs: one 32-bit word of residues per modulus (and split).
+template <int Q, int NM>
+__device__ __forceinline__ void frac4_q(const CombArgs& A, long f, long total, uint64_t (&L)[4][4]) {
+  using C = ModK<Q, NM>;
+  uint32_t s[4];
+  const uint32_t w = *reinterpret_cast<const uint32_t*>(A.R + (size_t)Q * total + f);
+#pragma unroll
+  for (int e = 0; e < 4; ++e) s[e] = (w >> (8 * e)) & 0xFFu;
+  for (int z = 1; z < A.splits; ++z) {
+    const uint32_t v = *reinterpret_cast<const uint32_t*>(A.R + ((size_t)z * NM + Q) * total + f);
+#pragma unroll
+    for (int e = 0; e < 4; ++e) s[e] += (v >> (8 * e)) & 0xFFu;
   }
-  L1 += L0 >> 32;
-  L2 += L1 >> 32;
-  L3 += L2 >> 32;
-  lo = (L0 & 0xFFFFFFFFull) | (L1 << 32);
-  hi = (L2 & 0xFFFFFFFFull) | (L3 << 32);
+#pragma unroll
+  for (int e = 0; e < 4; ++e) {
+    const uint32_t y = mod_c<C>(mod_c<C>(s[e]) * C::inv);
+    L[e][0] += (uint64_t)y * C::F0;   // 32 x 32 -> 64-bit products, < 2^40 each
+    L[e][1] += (uint64_t)y * C::F1;
+    L[e][2] += (uint64_t)y * C::F2;
+    L[e][3] += (uint64_t)y * C::F3;
+  }
+}
+template <int NM, int... Q>
+__device__ __forceinline__ void frac4_all(const CombArgs& A, long f, long total, uint64_t (&L)[4][4],
+                                          std::integer_sequence<int, Q...>) {
+  (frac4_q<Q, NM>(A, f, total, L), ...);
+}
+
+// The centred fractions T / M (mod 1) of four consecutive outputs as signed
+// 128-bit fixed-point numbers (two 64-bit halves each).
+template <int NM>
+__device__ __forceinline__ void crt_fraction4(const CombArgs& A, long f, long total, uint64_t (&hi)[4],
+                                              uint64_t (&lo)[4]) {
+  uint64_t L[4][4] = {};
+  frac4_all<NM>(A, f, total, L, std::make_integer_sequence<int, NM>{});
+#pragma unroll
+  for (int e = 0; e < 4; ++e) {
+    L[e][1] += L[e][0] >> 32;
+    L[e][2] += L[e][1] >> 32;
+    L[e][3] += L[e][2] >> 32;
+    lo[e] = (L[e][0] & 0xFFFFFFFFull) | (L[e][1] << 32);
+    hi[e] = (L[e][2] & 0xFFFFFFFFull) | (L[e][3] << 32);
+  }
 }
 
 __device__ __forceinline__ void two_sum(double a, double b, double& s, double& e) {
@@ -472,45 +562,57 @@ __device__ __forceinline__ void two_prod(double a, double b, double& p, double& 
   e = fma(a, b, -p);
 }
 
-// C (column-major, ldc) = alpha * sa_i sb_j 2^-shift T + beta * C
-__global__ void combine_kernel(CombArgs A, const double* __restrict__ sa, const double* __restrict__ sb, int shift,
-                               double alpha, double beta, double* __restrict__ C, long ldc) {
-  const long total = (long)A.M * A.N;
+// C (column-major, ldc) = alpha * sa_i sb_j 2^-shift T + beta * C; four
+// consecutive i per thread.
+template <int NM>
+__global__ void __launch_bounds__(256, 2)
+combine_kernel(CombArgs A, const double* __restrict__ sa, const double* __restrict__ sb, int shift, double alpha,
+               double beta, double* __restrict__ C, long ldc) {
+  const long total = (long)A.Mp * A.N;
   for (int j = blockIdx.y; j < A.N; j += gridDim.y)
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.M; i += gridDim.x * blockDim.x) {
-    const long f = i + (long)j * A.M;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) * 4; i < A.M; i += gridDim.x * blockDim.x * 4) {
     if (A.upper && (i / TM) * TM >= (j / TN) * TN + TN) continue;   // tile never computed
-    uint64_t hi, lo;
-    crt_fraction(A, f, total, hi, lo);
-    double dh, dl;
-    fixed_to_dd(hi, lo, dh, dl);
-    const double v = ldexp((dh + dl) * A.mod_hi, -128 - shift) * (sa ? sa[i] : 1.0) * sb[j];
-    double* c = C + i + j * ldc;
-    *c = (beta == 0.0) ? alpha * v : alpha * v + beta * (*c);
+    uint64_t hi[4], lo[4];
+    crt_fraction4<NM>(A, i + (long)j * A.Mp, total, hi, lo);
+    const double sbj = sb[j];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      if (i + e >= A.M) break;
+      double dh, dl;
+      fixed_to_dd(hi[e], lo[e], dh, dl);
+      const double v = ldexp((dh + dl) * A.mod_hi, -128 - shift) * (sa ? sa[i + e] : 1.0) * sbj;
+      double* c = C + (i + e) + (long)j * ldc;
+      *c = (beta == 0.0) ? alpha * v : alpha * v + beta * (*c);
+    }
   }
 }
 
 // The same value as a double-double (Ch + Cl), alpha = 1, beta = 0.
-__global__ void combine_dd_kernel(CombArgs A, const double* __restrict__ sa, const double* __restrict__ sb, int shift,
-                                  double* __restrict__ Ch, double* __restrict__ Cl, long ldc) {
-  const long total = (long)A.M * A.N;
+template <int NM>
+__global__ void __launch_bounds__(256, 2)
+combine_dd_kernel(CombArgs A, const double* __restrict__ sa, const double* __restrict__ sb, int shift,
+                  double* __restrict__ Ch, double* __restrict__ Cl, long ldc) {
+  const long total = (long)A.Mp * A.N;
   for (int j = blockIdx.y; j < A.N; j += gridDim.y)
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.M; i += gridDim.x * blockDim.x) {
-    const long f = i + (long)j * A.M;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) * 4; i < A.M; i += gridDim.x * blockDim.x * 4) {
     if (A.upper && (i / TM) * TM >= (j / TN) * TN + TN) continue;
-    uint64_t hi, lo;
-    crt_fraction(A, f, total, hi, lo);
-    double fh, fl;
-    fixed_to_dd(hi, lo, fh, fl);
-    // (fh + fl) (mod_hi + mod_lo), then exact power-of-two scalings
-    double p, e;
-    two_prod(fh, A.mod_hi, p, e);
-    e += fh * A.mod_lo + fl * A.mod_hi;
-    const double s = p + e;
-    const double t = e - (s - p);
-    const double sc = ldexp((sa ? sa[i] : 1.0) * sb[j], -128 - shift);
-    Ch[i + j * ldc] = s * sc;
-    Cl[i + j * ldc] = t * sc;
+    uint64_t hi[4], lo[4];
+    crt_fraction4<NM>(A, i + (long)j * A.Mp, total, hi, lo);
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      if (i + e >= A.M) break;
+      double fh, fl;
+      fixed_to_dd(hi[e], lo[e], fh, fl);
+      // (fh + fl) (mod_hi + mod_lo), then exact power-of-two scalings
+      double p, er;
+      two_prod(fh, A.mod_hi, p, er);
+      er += fh * A.mod_lo + fl * A.mod_hi;
+      const double s = p + er;
+      const double t = er - (s - p);
+      const double sc = ldexp((sa ? sa[i + e] : 1.0) * sb[j], -128 - shift);
+      Ch[(i + e) + (long)j * ldc] = s * sc;
+      Cl[(i + e) + (long)j * ldc] = t * sc;
+    }
   }
 }
 
@@ -617,6 +719,9 @@ Plan plan(int M, int N, long K, int num_sms, bool upper) {
 
 }  // namespace
 
+#define CRT_NM_CASES(X) \
+  X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15) X(16) X(17) X(18) X(19) X(20) X(21) X(22) X(23) X(24)
+
 long crt_pitch(long K) { return (K + 15) / 16 * 16; }
 
 int crt_moduli(int bits_a, int bits_b, long K) {
@@ -624,7 +729,7 @@ int crt_moduli(int bits_a, int bits_b, long K) {
   double bits = 0.0;
   for (int n = 0; n < MAXMOD; ++n) {
     bits += std::log2((double)MODULI[n]);
-    if (bits >= need) return n + 1;
+    if (bits >= need) return std::max(n + 1, 4);   // the kernels are built for 4..24 moduli
   }
   return -1;
 }
@@ -650,7 +755,16 @@ bbt_status crt_residues_rows(bbt_ctx* ctx, int rows, long K, const double* X, lo
   if (b < 2 || b > 53) return fail(ctx, BBT_ERR_ARG, "crt: %d-bit integers from doubles", b);
   const long kq = (K + 3) / 4;
   const unsigned gx = (unsigned)std::min<long>((kq + 255) / 256, 4096), gy = (unsigned)std::min(rows, 65535);
-  residues_rows_kernel<<<dim3(gx, gy), 256, 0, ctx->stream>>>(rows, K, X, rs, scale, b, mod_tab(n), planes, Kp);
+  switch (n) {
+#define CASE(NM)                                                                                          \
+  case NM:                                                                                                \
+    residues_rows_kernel<NM><<<dim3(gx, gy), 256, 0, ctx->stream>>>(rows, K, X, rs, scale, b, planes, Kp); \
+    break;
+    CRT_NM_CASES(CASE)
+#undef CASE
+    default:
+      return fail(ctx, BBT_ERR_ARG, "crt: %d moduli", n);
+  }
   BBT_LAUNCHED(ctx);
   return BBT_OK;
 }
@@ -658,10 +772,19 @@ bbt_status crt_residues_rows(bbt_ctx* ctx, int rows, long K, const double* X, lo
 bbt_status crt_residues_cols(bbt_ctx* ctx, int rows, long K, const double* X, long cs, const double* kscale, int b,
                              int n, int8_t* planes, long Kp) {
   if (b < 2 || b > 53) return fail(ctx, BBT_ERR_ARG, "crt: %d-bit integers from doubles", b);
-  const long gy = (K + 31) / 32;
+  const long gy = (K + 127) / 128;
   if (gy > 65535) return fail(ctx, BBT_ERR_ARG, "crt: K=%ld too long for the column layout", K);
-  residues_cols_kernel<<<dim3((unsigned)((rows + 31) / 32), (unsigned)gy), 256, 0, ctx->stream>>>(
-      rows, K, X, cs, kscale, b, mod_tab(n), planes, Kp);
+  const dim3 g((unsigned)((rows + 31) / 32), (unsigned)gy);
+  switch (n) {
+#define CASE(NM)                                                                                             \
+  case NM:                                                                                                   \
+    residues_cols_kernel<NM><<<g, 256, 0, ctx->stream>>>(rows, K, X, cs, kscale, b, planes, Kp);             \
+    break;
+    CRT_NM_CASES(CASE)
+#undef CASE
+    default:
+      return fail(ctx, BBT_ERR_ARG, "crt: %d moduli", n);
+  }
   BBT_LAUNCHED(ctx);
   return BBT_OK;
 }
@@ -677,7 +800,7 @@ bbt_status crt_residues_dd(bbt_ctx* ctx, int rows, long K, const double* Xh, con
 size_t crt_product_bytes(const bbt_ctx* ctx, int M, int N, long K, int n, bool upper) {
   const int sms = ctx->num_sms > 0 ? ctx->num_sms : 148;
   const Plan pl = plan(M, N, K, sms, upper);
-  return (size_t)pl.splits * n * (size_t)M * N + 4096;
+  return (size_t)pl.splits * n * (size_t)((M + 3) & ~3) * N + 4096;
 }
 
 bbt_status crt_product(bbt_ctx* ctx, int M, int N, long K, int n, const int8_t* RA, const int8_t* RB, long Kp,
@@ -718,6 +841,7 @@ bbt_status crt_product(bbt_ctx* ctx, int M, int N, long K, int n, const int8_t* 
   a.out = R;
   a.M = M;
   a.N = N;
+  a.Mp = (M + 3) & ~3;
   a.kblocks = pl.kblocks;
   a.kb_per_split = pl.kb_per_split;
   a.n = n;
@@ -743,15 +867,9 @@ CombArgs comb_args(const uint8_t* R, int M, int N, int n, int splits, bool upper
   c.R = R;
   c.M = M;
   c.N = N;
-  c.n = n;
+  c.Mp = (M + 3) & ~3;
   c.splits = splits;
   c.upper = upper ? 1 : 0;
-  for (int q = 0; q < n; ++q) {
-    c.p[q] = md.p[q];
-    c.inv[q] = md.inv[q];
-    c.magic32[q] = (uint32_t)((((uint64_t)1 << 32) + md.p[q] - 1) / md.p[q]);
-    for (int l = 0; l < 4; ++l) c.F[q][l] = md.F[q][l];
-  }
   c.mod_hi = md.mod_hi;
   c.mod_lo = md.mod_lo;
   return c;
@@ -760,16 +878,36 @@ CombArgs comb_args(const uint8_t* R, int M, int N, int n, int splits, bool upper
 
 bbt_status crt_combine(bbt_ctx* ctx, int M, int N, int n, int splits, const uint8_t* R, bool upper, const double* sa,
                        const double* sb, int shift, double alpha, double beta, double* C, long ldc) {
-  const dim3 g((unsigned)std::min((M + 255) / 256, 1024), (unsigned)std::min(N, 65535));
-  combine_kernel<<<g, 256, 0, ctx->stream>>>(comb_args(R, M, N, n, splits, upper), sa, sb, shift, alpha, beta, C, ldc);
+  const dim3 g((unsigned)std::min((M + 1023) / 1024, 1024), (unsigned)std::min(N, 65535));   // 4 outputs a thread
+  const CombArgs A = comb_args(R, M, N, n, splits, upper);
+  switch (n) {
+#define CASE(NM)                                                                                   \
+  case NM:                                                                                         \
+    combine_kernel<NM><<<g, 256, 0, ctx->stream>>>(A, sa, sb, shift, alpha, beta, C, ldc);          \
+    break;
+    CRT_NM_CASES(CASE)
+#undef CASE
+    default:
+      return fail(ctx, BBT_ERR_ARG, "crt: %d moduli", n);
+  }
   BBT_LAUNCHED(ctx);
   return BBT_OK;
 }
 
 bbt_status crt_combine_dd(bbt_ctx* ctx, int M, int N, int n, int splits, const uint8_t* R, bool upper,
                           const double* sa, const double* sb, int shift, double* Ch, double* Cl, long ldc) {
-  const dim3 g((unsigned)std::min((M + 255) / 256, 1024), (unsigned)std::min(N, 65535));
-  combine_dd_kernel<<<g, 256, 0, ctx->stream>>>(comb_args(R, M, N, n, splits, upper), sa, sb, shift, Ch, Cl, ldc);
+  const dim3 g((unsigned)std::min((M + 1023) / 1024, 1024), (unsigned)std::min(N, 65535));   // 4 outputs a thread
+  const CombArgs A = comb_args(R, M, N, n, splits, upper);
+  switch (n) {
+#define CASE(NM)                                                                                   \
+  case NM:                                                                                         \
+    combine_dd_kernel<NM><<<g, 256, 0, ctx->stream>>>(A, sa, sb, shift, Ch, Cl, ldc);              \
+    break;
+    CRT_NM_CASES(CASE)
+#undef CASE
+    default:
+      return fail(ctx, BBT_ERR_ARG, "crt: %d moduli", n);
+  }
   BBT_LAUNCHED(ctx);
   return BBT_OK;
 }
