@@ -333,6 +333,14 @@ def roofline(prof, dgemm_peak):
                 "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 figure)",
                 "launches": nl, "share": share}
     peaks = measured_peaks()
+    if dom == "crt":   # int8 operations of the per-modulus tcgen05 GEMMs
+        achieved = work / (ms * 1e-3) / 1e12
+        peak = 2.0 * peaks["bf16_tflops"]
+        return {"kernel": "crt_kernel (tcgen05 kind::i8, one GEMM per modulus)", "bound": "tensor",
+                "achieved": achieved, "peak": peak, "unit": "TOP/s (int8)", "frac": achieved / peak, "traffic": None,
+                "peak_source": "twice the measured dense bf16 burst (the tensor cores' 8-bit rate is twice their "
+                               "16-bit rate); MEASURED_PEAKS.json has no int8 figure",
+                "launches": nl, "share": share}
     achieved = work / (ms * 1e-3) / 1e9 if work else 0.0
     return {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
             "frac": achieved / peaks["hbm_gbs"], "traffic": None, "launches": nl, "share": share}

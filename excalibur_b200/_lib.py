@@ -26,7 +26,8 @@ EXPORTS = (
     "bbt_mlp_brackets", "bbt_bisection_bracketed", "bbt_set_bracket_model", "bbt_bisection_stats", "bbt_gebrd",
     "bbt_dgemm_ozaki", "bbt_dgemm_crt", "bbt_gram_dd", "bbt_exact_local_qr", "bbt_exact_apply_q",
 )
-PROF_CLASSES = ("dgemm", "panel", "mask", "ralha", "bisect", "twisted", "sketch", "chol", "ozaki", "crt")
+PROF_CLASSES = ("dgemm", "panel", "mask", "ralha", "bisect", "twisted", "sketch", "chol", "ozaki", "crt", "crt_prep",
+                "crt_combine", "dd")
 
 
 class FedSVDConfig(C.Structure):

@@ -738,6 +738,7 @@ bbt_status crt_row_scales(bbt_ctx* ctx, int rows, long K, const double* X, long 
   unsigned long long* mx = ctx->ws.take<unsigned long long>(rows);
   if (!mx) return fail(ctx, BBT_ERR_NOMEM, "crt: workspace (row maxima)");
   BBT_CUDA(ctx, cudaMemsetAsync(mx, 0, (size_t)rows * 8, ctx->stream));
+  ProfScope prof(ctx, BBT_PROF_CRT_PREP, 8.0 * (double)rows * K);
   if (K <= 4096) {
     rowmax_short_kernel<<<8 * ctx->num_sms, 256, 0, ctx->stream>>>(rows, K, X, rs, mx);
   } else {
@@ -755,6 +756,7 @@ bbt_status crt_residues_rows(bbt_ctx* ctx, int rows, long K, const double* X, lo
   if (b < 2 || b > 53) return fail(ctx, BBT_ERR_ARG, "crt: %d-bit integers from doubles", b);
   const long kq = (K + 3) / 4;
   const unsigned gx = (unsigned)std::min<long>((kq + 255) / 256, 4096), gy = (unsigned)std::min(rows, 65535);
+  ProfScope prof(ctx, BBT_PROF_CRT_PREP, (8.0 + n) * (double)rows * K);
   switch (n) {
 #define CASE(NM)                                                                                          \
   case NM:                                                                                                \
@@ -775,6 +777,7 @@ bbt_status crt_residues_cols(bbt_ctx* ctx, int rows, long K, const double* X, lo
   const long gy = (K + 127) / 128;
   if (gy > 65535) return fail(ctx, BBT_ERR_ARG, "crt: K=%ld too long for the column layout", K);
   const dim3 g((unsigned)((rows + 31) / 32), (unsigned)gy);
+  ProfScope prof(ctx, BBT_PROF_CRT_PREP, (8.0 + n) * (double)rows * K);
   switch (n) {
 #define CASE(NM)                                                                                             \
   case NM:                                                                                                   \
@@ -853,7 +856,7 @@ bbt_status crt_product(bbt_ctx* ctx, int M, int N, long K, int n, const int8_t* 
     a.off[q] = (int)(((uint64_t)1 << 31) % (uint64_t)md.p[q]);
   }
   a.err = ctx->d_flag + FLAG_SKETCH;
-  ProfScope prof(ctx, BBT_PROF_CRT, (upper ? 1.0 : 2.0) * (double)M * N * K);
+  ProfScope prof(ctx, BBT_PROF_CRT, (upper ? 1.0 : 2.0) * n * (double)M * N * K);   // int8 operations
   crt_kernel<<<dim3((N + TN - 1) / TN, gy, pl.splits), THREADS, SMEM_BYTES, ctx->stream>>>(ta, tb, a);
   BBT_LAUNCHED(ctx);
   *splits_out = pl.splits;
@@ -880,6 +883,7 @@ bbt_status crt_combine(bbt_ctx* ctx, int M, int N, int n, int splits, const uint
                        const double* sb, int shift, double alpha, double beta, double* C, long ldc) {
   const dim3 g((unsigned)std::min((M + 1023) / 1024, 1024), (unsigned)std::min(N, 65535));   // 4 outputs a thread
   const CombArgs A = comb_args(R, M, N, n, splits, upper);
+  ProfScope prof(ctx, BBT_PROF_CRT_COMBINE, ((double)n * splits + 8.0) * (double)M * N);
   switch (n) {
 #define CASE(NM)                                                                                   \
   case NM:                                                                                         \
@@ -898,6 +902,7 @@ bbt_status crt_combine_dd(bbt_ctx* ctx, int M, int N, int n, int splits, const u
                           const double* sa, const double* sb, int shift, double* Ch, double* Cl, long ldc) {
   const dim3 g((unsigned)std::min((M + 1023) / 1024, 1024), (unsigned)std::min(N, 65535));   // 4 outputs a thread
   const CombArgs A = comb_args(R, M, N, n, splits, upper);
+  ProfScope prof(ctx, BBT_PROF_CRT_COMBINE, ((double)n * splits + 8.0) * (double)M * N);
   switch (n) {
 #define CASE(NM)                                                                                   \
   case NM:                                                                                         \

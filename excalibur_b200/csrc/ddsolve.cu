@@ -8,8 +8,8 @@
 // column (one thread per column, right-looking substitution in double-double,
 // unrolled into registers), an update kernel subtracts the block's
 // contribution from the rows still to solve (one thread per row and four
-// columns, products of an FP64 and a double-double accumulated in
-// double-double).  The double-double operations are the
+// columns, products of an FP64 and a double-double accumulated as a
+// compensated dot product).  The double-double operations are the
 // classical error-free transformations (Knuth's two-sum, the FMA two-product)
 // with the usual renormalisations.
 #include <cuda_runtime.h>
@@ -48,15 +48,33 @@ __device__ __forceinline__ dd dd_mul_d(dd x, double a) {
   const double e = fma(x.hi, a, -p) + x.lo * a;
   return quick_two_sum(p, e);
 }
-// x / a (a double): q1 = x.hi / a, the remainder x - q1 a exactly, then its quotient
-__device__ __forceinline__ dd dd_div_d(dd x, double a) {
-  const double q1 = x.hi / a;
+// x / a given ia = 1/a rounded: q1 = x.hi ia, the remainder x - q1 a
+// exactly, then its quotient (q1's error is a few ulps, the correction
+// restores double-double accuracy without a division instruction)
+__device__ __forceinline__ dd dd_div_d(dd x, double a, double ia) {
+  const double q1 = x.hi * ia;
   const double p = q1 * a;
   const double pe = fma(q1, a, -p);
   const dd r = dd_add(x, {-p, -pe});
-  const double q2 = r.hi / a;
+  const double q2 = r.hi * ia;
   return quick_two_sum(q1, q2);
 }
+
+// Compensated accumulation of sum_t a_t x_t (a_t doubles, x_t double-doubles):
+// the running sum s with the exact error terms of its products and additions
+// gathered in c (TwoProduct / TwoSum), renormalised once at the end.
+struct dot2 {
+  double s = 0.0, c = 0.0;
+  __device__ __forceinline__ void add(double a, dd x) {
+    const double p = a * x.hi;
+    const double pe = fma(a, x.hi, -p);
+    const double t = s + p;
+    const double bb = t - s;
+    c += ((s - (t - bb)) + (p - bb)) + pe + a * x.lo;
+    s = t;
+  }
+  __device__ __forceinline__ dd value() const { return quick_two_sum(s, c); }
+};
 
 // Diagonal block [j0, j0 + nb) of R: X[j0.., c] <- R_jj^{-T} X (trans) or R_jj^{-1} X.
 // Right-looking and fully unrolled: after x_r is known, every remaining
@@ -65,10 +83,13 @@ __device__ __forceinline__ dd dd_div_d(dd x, double a) {
 __global__ void leaf_kernel(int trans, int nb, int j0, int k, const double* __restrict__ R, long ldr,
                             double* __restrict__ Xh, double* __restrict__ Xl, long ldx) {
   __shared__ double Rs[NB][NB + 1];   // Rs[r][c] = R(j0 + r, j0 + c)
+  __shared__ double Ri[NB];           // 1 / R(j0 + r, j0 + r)
   for (int f = threadIdx.x; f < NB * NB; f += blockDim.x) {
     const int r = f % NB, c = f / NB;
     Rs[r][c] = (r < nb && c < nb) ? R[(j0 + r) + (long)(j0 + c) * ldr] : (r == c ? 1.0 : 0.0);
   }
+  __syncthreads();
+  for (int r = threadIdx.x; r < NB; r += blockDim.x) Ri[r] = 1.0 / Rs[r][r];
   __syncthreads();
   const int col = blockIdx.x * blockDim.x + threadIdx.x;
   if (col >= k) return;
@@ -80,14 +101,14 @@ __global__ void leaf_kernel(int trans, int nb, int j0, int k, const double* __re
   if (trans) {   // forward with R^T (lower): x_r, then rows t > r lose R(r, t) x_r
 #pragma unroll
     for (int r = 0; r < NB; ++r) {
-      x[r] = dd_div_d(x[r], Rs[r][r]);
+      x[r] = dd_div_d(x[r], Rs[r][r], Ri[r]);
 #pragma unroll
       for (int t = r + 1; t < NB; ++t) x[t] = dd_add(x[t], dd_mul_d(x[r], -Rs[r][t]));
     }
   } else {       // backward with the upper R: rows t < r lose R(t, r) x_r
 #pragma unroll
     for (int r = NB - 1; r >= 0; --r) {
-      x[r] = dd_div_d(x[r], Rs[r][r]);
+      x[r] = dd_div_d(x[r], Rs[r][r], Ri[r]);
 #pragma unroll
       for (int t = 0; t < r; ++t) x[t] = dd_add(x[t], dd_mul_d(x[r], -Rs[t][r]));
     }
@@ -109,23 +130,22 @@ __global__ void update_kernel(int trans, int nb, int j0, int r0, int r1, int k, 
   const int i = r0 + blockIdx.x * blockDim.x + threadIdx.x;
   const int c0 = blockIdx.y * UC;
   if (i >= r1) return;
-  dd s[UC];
-#pragma unroll
-  for (int u = 0; u < UC; ++u) s[u] = {0.0, 0.0};
+  dot2 s[UC];
   for (int t = 0; t < nb; ++t) {
     const double a = trans ? R[(j0 + t) + (long)i * ldr] : R[i + (long)(j0 + t) * ldr];
 #pragma unroll
     for (int u = 0; u < UC; ++u)
       if (c0 + u < k) {
         const long o = (long)(c0 + u) * ldx + j0 + t;
-        s[u] = dd_add(s[u], dd_mul_d({Xh[o], Xl[o]}, a));
+        s[u].add(a, {Xh[o], Xl[o]});
       }
   }
 #pragma unroll
   for (int u = 0; u < UC; ++u)
     if (c0 + u < k) {
       const long o = (long)(c0 + u) * ldx + i;
-      const dd x = dd_add({Xh[o], Xl[o]}, {-s[u].hi, -s[u].lo});
+      const dd v = s[u].value();
+      const dd x = dd_add({Xh[o], Xl[o]}, {-v.hi, -v.lo});
       Xh[o] = x.hi;
       Xl[o] = x.lo;
     }
@@ -168,6 +188,7 @@ __global__ void dd_symmetrize_kernel(int m, double* __restrict__ Gh, double* __r
 bbt_status dd_trsm_left(bbt_ctx* ctx, bool trans, int m, int k, const double* R, long ldr, double* Xh, double* Xl,
                         long ldx) {
   if (m < 1 || k < 1) return BBT_OK;
+  ProfScope prof(ctx, BBT_PROF_DD, (double)m * m * k);
   const int nblk = (m + NB - 1) / NB;
   for (int s = 0; s < nblk; ++s) {
     const int b = trans ? s : nblk - 1 - s;

@@ -126,42 +126,73 @@ size_t exact_apply_workspace_bytes(const bbt_ctx* ctx, long rows, int m, int k) 
          (4 * (size_t)m * k + 2 * (size_t)k) * 8 + 16384;
 }
 
-// C (rows x k, column-major, ldc) = A_int R_p^-1 Z, A_int(j, i) the 53-bit
-// integers of X(i, j) = X[i ldx + j] (i < m, j < rows) at the row scales of X
-// (those exact_local_qr used), Z (m x k, column-major, FP64).
-bbt_status exact_apply_q(bbt_ctx* ctx, int m, long rows, const double* X, long ldx, const double* scale,
-                         const double* Rp, const double* Z, int k, double* C, long ldc) {
+size_t exact_operand_bytes(int m, int k) {
+  const int nm = crt_moduli(GRAM_BITS, Z_BITS, m);
+  return (size_t)nm * k * crt_pitch(m) + (size_t)k * 8 + 512;
+}
+
+// The Z side of C = A_int R_p^-1 Z: Z2 = diag(scale) R_p^-1 Z solved in
+// double-double (the row scales of X fold into Z's rows), then every column of
+// Z2 rounded to an 80-bit integer at its own scale t (k) and reduced to the
+// residue planes RB (exact_operand_bytes).  One operand serves every row block
+// of A_int that shares R_p and the row scales.
+bbt_status exact_operand(bbt_ctx* ctx, int m, const double* scale, const double* Rp, const double* Z, int k,
+                         ExactOperand& op) {
   const int nm = crt_moduli(GRAM_BITS, Z_BITS, m);
   if (nm < 1) return fail(ctx, BBT_ERR_ARG, "exact apply: m=%d", m);
-  if (rows > 0x7fffffffL) return fail(ctx, BBT_ERR_ARG, "exact apply: rows=%ld", rows);
+  op.m = m;
+  op.k = k;
+  op.nm = nm;
+  op.Kp = crt_pitch(m);
+  op.t = ctx->ws.take<double>(k);
+  op.RB = ctx->ws.take<int8_t>((size_t)nm * k * op.Kp);
   const size_t mark = ctx->ws.top;
-  const long Kp = crt_pitch(m);
   double* Zh = ctx->ws.take<double>((size_t)m * k);
   double* Zl = ctx->ws.take<double>((size_t)m * k);
-  double* t = ctx->ws.take<double>(k);
-  int8_t* RA = ctx->ws.take<int8_t>((size_t)nm * rows * Kp);
-  int8_t* RB = ctx->ws.take<int8_t>((size_t)nm * k * Kp);
-  uint8_t* Rb = ctx->ws.take<uint8_t>(crt_product_bytes(ctx, (int)rows, k, m, nm, false));
-  if (!Rb) return fail(ctx, BBT_ERR_NOMEM, "exact apply: workspace");
-  // Z2 = diag(scale) R_p^-1 Z in double-double (the row scales of X fold into Z's rows)
+  if (!Zl) return fail(ctx, BBT_ERR_NOMEM, "exact apply: workspace");
   BBT_TRY(copy2d(ctx, k, m, Z, m, Zh, m));   // k columns of m entries (copy2d counts rows of its row-major view)
   zero_kernel<<<2 * ctx->num_sms, 256, 0, ctx->stream>>>(Zl, (long)m * k);
   BBT_LAUNCHED(ctx);
   BBT_TRY(dd_trsm_left(ctx, false, m, k, Rp, m, Zh, Zl, m));
   dd_scale_rows_kernel<<<2 * ctx->num_sms, 256, 0, ctx->stream>>>(m, k, scale, Zh, Zl, m);
   BBT_LAUNCHED(ctx);
-  // residues: B rows = columns of Z2 (80-bit integers, their own scales); A rows = columns of X
   {
     const size_t m2 = ctx->ws.top;
-    BBT_TRY(crt_row_scales(ctx, k, m, Zh, m, t));
+    BBT_TRY(crt_row_scales(ctx, k, m, Zh, m, op.t));
     ctx->ws.top = m2;
   }
-  BBT_TRY(crt_residues_dd(ctx, k, m, Zh, Zl, m, t, Z_BITS, nm, RB, Kp));
-  BBT_TRY(crt_residues_cols(ctx, (int)rows, m, X, ldx, scale, GRAM_BITS, nm, RA, Kp));
+  BBT_TRY(crt_residues_dd(ctx, k, m, Zh, Zl, m, op.t, Z_BITS, nm, op.RB, op.Kp));
+  ctx->ws.top = mark;   // Zh, Zl die here; t and RB stay with the caller's mark
+  return BBT_OK;
+}
+
+// C (rows x k, column-major, ldc) = A_int R_p^-1 Z for a prepared Z operand,
+// A_int(j, i) the 53-bit integers of X(i, j) = X[i ldx + j] (i < m, j < rows)
+// at the row scales of X (those exact_local_qr used).
+bbt_status exact_apply_rows(bbt_ctx* ctx, const ExactOperand& op, long rows, const double* X, long ldx,
+                            const double* scale, double* C, long ldc) {
+  if (rows > 0x7fffffffL) return fail(ctx, BBT_ERR_ARG, "exact apply: rows=%ld", rows);
+  const int m = op.m, k = op.k, nm = op.nm;
+  const size_t mark = ctx->ws.top;
+  int8_t* RA = ctx->ws.take<int8_t>((size_t)nm * rows * op.Kp);
+  uint8_t* Rb = ctx->ws.take<uint8_t>(crt_product_bytes(ctx, (int)rows, k, m, nm, false));
+  if (!Rb) return fail(ctx, BBT_ERR_NOMEM, "exact apply: workspace");
+  BBT_TRY(crt_residues_cols(ctx, (int)rows, m, X, ldx, scale, GRAM_BITS, nm, RA, op.Kp));
   int splits = 1;
-  BBT_TRY(crt_product(ctx, (int)rows, k, m, nm, RA, RB, Kp, false, Rb, &splits));
-  BBT_TRY(crt_combine(ctx, (int)rows, k, nm, splits, Rb, false, nullptr, t, (GRAM_BITS - 1) + (Z_BITS - 1), 1.0,
+  BBT_TRY(crt_product(ctx, (int)rows, k, m, nm, RA, op.RB, op.Kp, false, Rb, &splits));
+  BBT_TRY(crt_combine(ctx, (int)rows, k, nm, splits, Rb, false, nullptr, op.t, (GRAM_BITS - 1) + (Z_BITS - 1), 1.0,
                       0.0, C, ldc));
+  ctx->ws.top = mark;
+  return BBT_OK;
+}
+
+// C (rows x k, column-major, ldc) = A_int R_p^-1 Z, Z (m x k, column-major, FP64).
+bbt_status exact_apply_q(bbt_ctx* ctx, int m, long rows, const double* X, long ldx, const double* scale,
+                         const double* Rp, const double* Z, int k, double* C, long ldc) {
+  const size_t mark = ctx->ws.top;
+  ExactOperand op;
+  BBT_TRY(exact_operand(ctx, m, scale, Rp, Z, k, op));
+  BBT_TRY(exact_apply_rows(ctx, op, rows, X, ldx, scale, C, ldc));
   ctx->ws.top = mark;
   return BBT_OK;
 }

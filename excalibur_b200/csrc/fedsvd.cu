@@ -187,6 +187,7 @@ size_t scratch_bytes(const bbt_ctx* ctx, const Layout& L) {
   }
   if (L.precision == 2) {   // the global QR and the exact products with the implicit Q's
     s = std::max(s, qr_scratch(ctx, L, (long)L.rg, qp));
+    s += exact_operand_bytes((int)L.m, (int)L.m);   // the global chain's prepared operand stays taken
     for (int c = 0; c < L.P; ++c) {
       s = std::max(s, exact_apply_workspace_bytes(ctx, (long)L.r[c], (int)L.m, (int)L.m) + (8u << 20));
       if (L.qr[c]) s = std::max(s, exact_apply_workspace_bytes(ctx, (long)L.n[c], (int)L.m, (int)L.m) + (8u << 20));
@@ -817,6 +818,8 @@ bbt_status fedsvd(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* X, 
   BBT_TRY(ormqr_left_notrans(ctx, (long)m, mi, house, (long)m, 1, tauh, Ub, k, k, true, qp));
   if (L.precision >= 1)   // Q_g U2 = Q_p (W_g U2): Rg (free by now) <- W_g U2, m x k column-major
     BBT_TRY(dgemm(ctx, false, true, mi, k, m, 1.0, Wg, (long)m, Ub, k, 0.0, Rg, (long)m));
+  ExactOperand zg;   // precision 2: Rp_g^-1 (W_g U2) as residue planes, shared by every participant
+  if (L.precision == 2 && rg > m) BBT_TRY(exact_operand(ctx, mi, scg, Rpg, Rg, k, zg));
   for (int c = 0; c < P; ++c) {   // :1179-1195
     const int rc = (int)L.r[c];
     if (rg == m) {   // m == global_n: FinalVT_c = U2[rows of c]^T, unmasked (client.cpp:1161-1166)
@@ -832,9 +835,7 @@ bbt_status fedsvd(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* X, 
     }
     // tmp (k x r_c row-major) = U2^T Q_g[rows_c, :]^T  ==  column-major r_c x k = Q_g[rows_c,:] U2
     if (L.precision == 2) {   // Q_g[rows_c,:] U2 = M_int^T[rows_c] Rp_g^-1 (W_g U2), exactly (exactqr.cu)
-      const size_t mark = ctx->ws.top;
-      BBT_TRY(exact_apply_q(ctx, mi, rc, M + L.rpos[c], (long)rg, scg, Rpg, Rg, k, tmp, rc));
-      ctx->ws.top = mark;
+      BBT_TRY(exact_apply_rows(ctx, zg, rc, M + L.rpos[c], (long)rg, scg, tmp, rc));
     } else if (L.precision == 1)
       BBT_TRY(dgemm(ctx, false, false, rc, k, m, 1.0, M + L.rpos[c], (long)rg, Rg, (long)m, 0.0, tmp, rc));
     else

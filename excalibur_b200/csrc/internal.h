@@ -307,7 +307,20 @@ bbt_status dd_symmetrize_upper(bbt_ctx* ctx, int m, double* Gh, double* Gl, long
 size_t exact_qr_workspace_bytes(const bbt_ctx* ctx, int m, long n);
 bbt_status exact_local_qr(bbt_ctx* ctx, int m, long n, const double* X, const void* S, long spitch, double* R,
                           double* W, double* Rp, double* scale);
-// C (rows x k column-major) = A_int Rp^-1 Z for A_int(j, i) the integers of X[i ldx + j].
+// C (rows x k column-major) = A_int Rp^-1 Z for A_int(j, i) the integers of X[i ldx + j];
+// the Z side can be prepared once (exact_operand, taken from the workspace)
+// and applied to several row blocks of A_int (exact_apply_rows).
+struct ExactOperand {
+  int m = 0, k = 0, nm = 0;
+  long Kp = 0;
+  double* t = nullptr;
+  int8_t* RB = nullptr;
+};
+size_t exact_operand_bytes(int m, int k);
+bbt_status exact_operand(bbt_ctx* ctx, int m, const double* scale, const double* Rp, const double* Z, int k,
+                         ExactOperand& op);
+bbt_status exact_apply_rows(bbt_ctx* ctx, const ExactOperand& op, long rows, const double* X, long ldx,
+                            const double* scale, double* C, long ldc);
 size_t exact_apply_workspace_bytes(const bbt_ctx* ctx, long rows, int m, int k);
 bbt_status exact_apply_q(bbt_ctx* ctx, int m, long rows, const double* X, long ldx, const double* scale,
                          const double* Rp, const double* Z, int k, double* C, long ldc);

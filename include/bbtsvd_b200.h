@@ -218,7 +218,8 @@ bbt_status bbt_mixed_local_qr(bbt_ctx* ctx, size_t m, size_t local_n, double* d_
  * switched on. */
 enum { BBT_PROF_DGEMM = 0, BBT_PROF_PANEL = 1, BBT_PROF_MASK = 2, BBT_PROF_RALHA = 3,
        BBT_PROF_BISECT = 4, BBT_PROF_TWISTED = 5, BBT_PROF_SKETCH = 6, BBT_PROF_CHOL = 7,
-       BBT_PROF_OZAKI = 8, BBT_PROF_CRT = 9, BBT_PROF_CLASSES = 10 };
+       BBT_PROF_OZAKI = 8, BBT_PROF_CRT = 9, BBT_PROF_CRT_PREP = 10, BBT_PROF_CRT_COMBINE = 11,
+       BBT_PROF_DD = 12, BBT_PROF_CLASSES = 13 };
 bbt_status bbt_profile(bbt_ctx* ctx, int enable);
 bbt_status bbt_profile_get(bbt_ctx* ctx, int cls, double* ms, uint64_t* launches, double* work);
 
