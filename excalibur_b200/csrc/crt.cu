@@ -7,9 +7,9 @@
 // Every row of an operand is scaled by a power of two s_i (|x / s_i| < 1/2)
 // and rounded to a b-bit integer t = rint(x 2^(b-1) / s_i), |t| <= 2^(b-2).
 // The integer product T = A_int B_int^T is then computed exactly modulo n
-// pairwise coprime moduli p <= 256: with residues in [-128, 127] every
-// modulus is one int8 x int8 -> int32 GEMM (tcgen05 kind::i8, 128 x 256 tiles,
-// one TMEM accumulator), exact for up to 2^16 terms per K-split.  The
+// pairwise coprime moduli p <= 256: with residues in [0, p) every modulus is
+// one u8 x u8 -> int32 GEMM (tcgen05 kind::i8, 128 x 256 tiles, one TMEM
+// accumulator), exact for up to 2^15 terms per K-split.  The
 // residues of T are written as bytes and the integer is rebuilt from them
 // (crt_combine): with y_p = (T mod p) ((M/p)^-1 mod p) mod p, T/M = sum_p y_p / p
 // mod 1 (M = prod p), evaluated as a 128-bit fixed-point sum of y_p
@@ -100,7 +100,7 @@ constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
 constexpr int EPI_WARPS = 8;
 constexpr int THREADS = (EPI_WARPS + 2) * 32;
 constexpr uint32_t TMEM_COLS = 2 * TN;          // two accumulators: modulus p+1 runs while p drains
-constexpr int MAX_KB_PER_SPLIT = 65536 / TK;    // |T| < 2^16 * 2^14 per split: no int32 overflow
+constexpr int MAX_KB_PER_SPLIT = 32768 / TK;    // T < 2^15 * 2^16 per split: no int32 overflow
 constexpr int MAX_SPLITS = 64;
 
 struct Mods {
@@ -219,15 +219,13 @@ __device__ __forceinline__ Pieces pieces(double t) {
   return {__double2loint(a + RND), __double2loint(b + RND), __double2loint(c + RND)};
 }
 
-// The centred residue of modulus Q from the pieces: x = a c36 + b c18 + c +
+// The residue in [0, p) of modulus Q from the pieces: x = a c36 + b c18 + c +
 // off lies in [0, 2^27) and its multiply-high quotient by p is exact.
 template <int Q>
 __device__ __forceinline__ int res_q(const Pieces& t) {
   using C = ModR<Q>;
   const uint32_t x = (uint32_t)(t.a * C::c36 + t.b * C::c18 + t.c + C::off);
-  int r = (int)(x - (__umulhi(x, C::magic35) >> 3) * (uint32_t)C::p);
-  if (r > ((C::p - 1) >> 1)) r -= C::p;
-  return r;
+  return (int)(x - (__umulhi(x, C::magic35) >> 3) * (uint32_t)C::p);
 }
 
 template <int Q>
@@ -320,7 +318,8 @@ __global__ void residues_dd_kernel(int rows, long K, const double* __restrict__ 
     const double tl = rint(l + (h - th));
     for (int q = 0; q < T.n; ++q) {
       const int p = T.p[q];
-      const int r = centre(residue_big(th, p, T.invp[q]) + residue_big(tl, p, T.invp[q]), p);
+      int r = centre(residue_big(th, p, T.invp[q]) + residue_big(tl, p, T.invp[q]), p);
+      if (r < 0) r += p;   // stored in [0, p)
       out[q * plane + (size_t)i * Kp + k] = (int8_t)r;
     }
   }
@@ -398,9 +397,9 @@ crt_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUte
         if (!mbar_wait(full0 + 8 * (it % STAGES), (uint32_t)(it / STAGES) & 1u)) atomicExch(P.err, 4);
     }
   } else if (warp == EPI_WARPS + 1) {
-    if (lane == 0) {   // ---- MMA issuer: int8 x int8 -> int32, K-major, 128 x 256 x 32 per instruction
-      const uint32_t idesc =
-          (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TN >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
+    if (lane == 0) {   // ---- MMA issuer: u8 x u8 -> int32, K-major, 128 x 256 x 32 per instruction
+      const uint32_t idesc =   // c_format S32, a/b unsigned 8-bit
+          (2u << 4) | (0u << 7) | (0u << 10) | ((uint32_t)(TN >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
       bool ok = true;
       for (int q = 0; q < P.n && ok; ++q) {
         const int buf = q & 1, use = q >> 1;
@@ -483,7 +482,10 @@ __device__ __forceinline__ uint32_t mod_c(uint32_t x) {
 }
 
 // Four consecutive outputs: one 32-bit word of residues per modulus (and split).
-template <int Q, int NM>
+// LIMBS = 4: the fraction to 128 bits (double-double outputs); 3: to 96 bits
+// (FP64 outputs: the missing 32 bits are below 2^-75 of the largest |T|), the
+// limbs of floor(2^96 / p) being the top three of floor(2^128 / p).
+template <int Q, int NM, int LIMBS>
 __device__ __forceinline__ void frac4_q(const CombArgs& A, long f, long total, uint64_t (&L)[4][4]) {
   using C = ModK<Q, NM>;
   uint32_t s[4];
@@ -498,25 +500,25 @@ __device__ __forceinline__ void frac4_q(const CombArgs& A, long f, long total, u
 #pragma unroll
   for (int e = 0; e < 4; ++e) {
     const uint32_t y = mod_c<C>(mod_c<C>(s[e]) * C::inv);
-    L[e][0] += (uint64_t)y * C::F0;   // 32 x 32 -> 64-bit products, < 2^40 each
+    if (LIMBS == 4) L[e][0] += (uint64_t)y * C::F0;   // 32 x 32 -> 64-bit products, < 2^40 each
     L[e][1] += (uint64_t)y * C::F1;
     L[e][2] += (uint64_t)y * C::F2;
     L[e][3] += (uint64_t)y * C::F3;
   }
 }
-template <int NM, int... Q>
+template <int NM, int LIMBS, int... Q>
 __device__ __forceinline__ void frac4_all(const CombArgs& A, long f, long total, uint64_t (&L)[4][4],
                                           std::integer_sequence<int, Q...>) {
-  (frac4_q<Q, NM>(A, f, total, L), ...);
+  (frac4_q<Q, NM, LIMBS>(A, f, total, L), ...);
 }
 
 // The centred fractions T / M (mod 1) of four consecutive outputs as signed
 // 128-bit fixed-point numbers (two 64-bit halves each).
-template <int NM>
+template <int NM, int LIMBS>
 __device__ __forceinline__ void crt_fraction4(const CombArgs& A, long f, long total, uint64_t (&hi)[4],
                                               uint64_t (&lo)[4]) {
   uint64_t L[4][4] = {};
-  frac4_all<NM>(A, f, total, L, std::make_integer_sequence<int, NM>{});
+  frac4_all<NM, LIMBS>(A, f, total, L, std::make_integer_sequence<int, NM>{});
 #pragma unroll
   for (int e = 0; e < 4; ++e) {
     L[e][1] += L[e][0] >> 32;
@@ -565,7 +567,7 @@ __device__ __forceinline__ void two_prod(double a, double b, double& p, double& 
 // C (column-major, ldc) = alpha * sa_i sb_j 2^-shift T + beta * C; four
 // consecutive i per thread.
 template <int NM>
-__global__ void __launch_bounds__(256, 2)
+__global__ void __launch_bounds__(256, 3)
 combine_kernel(CombArgs A, const double* __restrict__ sa, const double* __restrict__ sb, int shift, double alpha,
                double beta, double* __restrict__ C, long ldc) {
   const long total = (long)A.Mp * A.N;
@@ -573,7 +575,7 @@ combine_kernel(CombArgs A, const double* __restrict__ sa, const double* __restri
   for (int i = (blockIdx.x * blockDim.x + threadIdx.x) * 4; i < A.M; i += gridDim.x * blockDim.x * 4) {
     if (A.upper && (i / TM) * TM >= (j / TN) * TN + TN) continue;   // tile never computed
     uint64_t hi[4], lo[4];
-    crt_fraction4<NM>(A, i + (long)j * A.Mp, total, hi, lo);
+    crt_fraction4<NM, 3>(A, i + (long)j * A.Mp, total, hi, lo);
     const double sbj = sb[j];
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
@@ -597,7 +599,7 @@ combine_dd_kernel(CombArgs A, const double* __restrict__ sa, const double* __res
   for (int i = (blockIdx.x * blockDim.x + threadIdx.x) * 4; i < A.M; i += gridDim.x * blockDim.x * 4) {
     if (A.upper && (i / TM) * TM >= (j / TN) * TN + TN) continue;
     uint64_t hi[4], lo[4];
-    crt_fraction4<NM>(A, i + (long)j * A.Mp, total, hi, lo);
+    crt_fraction4<NM, 4>(A, i + (long)j * A.Mp, total, hi, lo);
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
       if (i + e >= A.M) break;

@@ -265,7 +265,7 @@ bbt_status gemm_oz(bbt_ctx* ctx, int M, int N, long K, double alpha, const doubl
 // Exact integer products on the int8 tensor cores by the Chinese remainder
 // theorem (crt.cu).  Operands are rounded per row to b-bit integers
 // (t = rint(x 2^(b-1) / s_i), s_i a power of two above 2 max|x|) and given as
-// residue planes [modulus][row][Kp] (int8, centred); the product's residues
+// residue planes [modulus][row][Kp] (bytes in [0, p)); the product's residues
 // are bytes [split][modulus][N][M] that crt_combine turns back into
 // C = alpha sa_i sb_j 2^-shift T + beta C (or a double-double).
 long crt_pitch(long K);
