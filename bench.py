@@ -9,10 +9,13 @@ vectors, back-transforms) on inputs resident in HBM; the 8 GB inputs are
 larger than L2, and are restored from a pristine device copy before every
 step (outside the timed events).
 
-By default both precision modes are timed: plain FP64 (the reference's
-Householder local QR) and mixed (BF16x3 tensor-core sketch + FP64
-Cholesky-QR refinement); the JSON value is the mixed run, the plain run sits
-beside it under "plain".
+By default the three precision modes are timed: plain FP64 (mode 0, the
+reference's Householder local QR), mixed (mode 1: BF16x3 tensor-core sketch +
+FP64 Cholesky-QR refinement) and exact Gram (mode 2: the sketch as a
+preconditioner of the exact Gram matrix, computed on the int8 tensor cores by
+the Chinese remainder theorem, and products with the implicit Q made exact the
+same way); the JSON value is mode 2, the other two sit beside it under
+"plain" and "mixed".
 
 Prints one JSON line (rank 0).  --impl reference times the reference's own
 CPU implementation (oracle/_ref, built from the reference's sources) on a
@@ -60,8 +63,9 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-sample-rows", type=int, default=50_000)
-    p.add_argument("--precision", default="both", choices=["both", "mixed", "plain", "exact", "all"],
-                   help="both: time plain FP64 then mixed; the JSON value is the mixed run")
+    p.add_argument("--precision", default="all", choices=["both", "mixed", "plain", "exact", "all"],
+                   help="all: plain FP64, mixed (mode 1) and exact Gram (mode 2), the JSON value is the last; "
+                        "both: plain then mixed")
     return p.parse_args()
 
 
@@ -425,12 +429,15 @@ def main():
                                    "frac": ach / peak, "launches": nl,
                                    "note": "algorithmic 2*m*N*n flops per launch against the measured bf16 "
                                            "burst peak / 3 (three bf16 products per FP64-equivalent product)"}
-    if "plain" in runs and "mixed" in runs:
-        pl = runs["plain"]
-        line["plain"] = {"value": pl["sec"], "unit": "s", "accuracy": pl["acc"], "stage_ms": pl["stage_ms"],
-                         "gpu_launches": pl["launches"], "roofline": roofline(pl["prof"], res["dgemm_peak"]),
-                         "kernel_classes": {k: {"ms": v[0], "launches": v[1]} for k, v in pl["prof"].items() if v[1]}}
-        line["mixed_speedup_vs_plain"] = pl["sec"] / head["sec"]
+    for other, o in runs.items():   # the other precision modes, beside the headline one
+        if other == res["head"]:
+            continue
+        line[other] = {"value": o["sec"], "unit": "s", "precision_mode": PRECISION[other], "accuracy": o["acc"],
+                       "stage_ms": o["stage_ms"], "gpu_launches": o["launches"],
+                       "roofline": roofline(o["prof"], res["dgemm_peak"]),
+                       "kernel_classes": {k: {"ms": v[0], "launches": v[1]} for k, v in o["prof"].items() if v[1]}}
+    if "plain" in runs and res["head"] != "plain":
+        line["speedup_vs_plain"] = runs["plain"]["sec"] / head["sec"]
     if "e2e" in res:
         line["e2e"] = res["e2e"]
     if not args.no_cpu_baseline:
