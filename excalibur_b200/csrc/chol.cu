@@ -4,6 +4,8 @@
 // (mixedqr.cu), whose R factor is built from Gram matrices.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "internal.h"
 
 namespace bbt {
@@ -76,6 +78,119 @@ __global__ void __launch_bounds__(128) trsm_leaf(long rows, int n, const double*
   for (int j = 0; j < NB; ++j)
     if (j < n) A[row + (long)j * lda] = x[j];
 }
+
+// Triangular solves of independent vectors, one launch: vector v of X is
+// x_j = X[v vs + j es] (a row of a column-major X: vs = 1, es = ld; a column:
+// vs = ld, es = 1), solved in place forward (FWD, j = 0, 1, ..) or backward
+// against the coefficients A(j, t) = T(t, j) (TRANS) or T(j, t):
+//   x_j <- (x_j - sum_{t solved} A(j, t) x_t) / A(j, j)   (no division if UNIT).
+// One CTA per group of up to 8 vectors (one warp each), held in shared
+// memory, so no CTA waits for another.  Left-looking in 32-element blocks:
+// the block first gathers the solved terms through VT x 32 tiles of A staged
+// in shared memory (four FMA chains per thread), then solves its diagonal
+// block in registers, one element per lane, broadcasting by warp shuffles.
+// For square and short operands (rows up to a few thousand), where the
+// recursive form spends its time in launches.
+constexpr int VC = 8, VT = 64;
+constexpr size_t VFIXED = (size_t)(VT + TB) * (TB + 1) * sizeof(double) + TB * sizeof(double);
+constexpr size_t VSMEM_MAX = 227 * 1024;
+
+size_t vec_smem(int n, int C) { return (size_t)(n + 4) * C * sizeof(double) + VFIXED; }
+
+template <bool TRANS, bool FWD, bool UNIT>
+__global__ void __launch_bounds__(256, 1) vec_solve_kernel(int n, long nvec, int C, const double* __restrict__ T,
+                                                           long ldt, double* __restrict__ X, long vs, long es) {
+  extern __shared__ double sm[];
+  const int np = n + 4;
+  double* x = sm;   // x[t * C + c]
+  double(*As)[TB + 1] = reinterpret_cast<double(*)[TB + 1]>(x + (size_t)np * C);
+  double(*Ad)[TB + 1] = As + VT;
+  double* Ai = reinterpret_cast<double*>(Ad + TB);
+  const long v0 = (long)blockIdx.x * C;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, nt = blockDim.x;
+  for (int f = threadIdx.x; f < np * C; f += nt) {   // vector index fastest
+    const int c = f % C, t = f / C;
+    x[f] = (t < n && v0 + c < nvec) ? X[(v0 + c) * vs + (long)t * es] : 0.0;
+  }
+  const int nblk = (n + TB - 1) / TB;
+  for (int s = 0; s < nblk; ++s) {
+    const int b = FWD ? s : nblk - 1 - s;
+    const int r0 = b * TB, nb = min(TB, n - r0);
+    const int ta = FWD ? 0 : r0 + nb, tb = FWD ? r0 : n;   // elements already solved
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int t0 = ta; t0 < tb; t0 += VT) {
+      const int tl = min(VT, tb - t0);
+      __syncthreads();
+      // As[tt][rr] = A(r0 + rr, t0 + tt), zero past the tile
+      for (int f = threadIdx.x; f < VT * TB; f += nt) {
+        const int tt = TRANS ? f % VT : f / TB, rr = TRANS ? f / VT : f % TB;
+        double a = 0.0;
+        if (tt < tl && rr < nb)
+          a = TRANS ? T[(t0 + tt) + (long)(r0 + rr) * ldt] : T[(r0 + rr) + (long)(t0 + tt) * ldt];
+        As[tt][rr] = a;
+      }
+      __syncthreads();
+      const double* xc = x + (size_t)t0 * C + w;
+      for (int tt = 0; tt < tl; tt += 4) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) acc[u] = fma(As[tt + u][lane], xc[(tt + u) * C], acc[u]);
+      }
+    }
+    // Ad[i][j] = A(r0 + i, r0 + j), identity past nb
+    for (int f = threadIdx.x; f < TB * TB; f += nt) {
+      const int i = f % TB, j = f / TB;
+      double a = (i == j) ? 1.0 : 0.0;
+      if (i < nb && j < nb && (FWD ? j < i : j > i))
+        a = TRANS ? T[(r0 + j) + (long)(r0 + i) * ldt] : T[(r0 + i) + (long)(r0 + j) * ldt];
+      else if (!UNIT && i == j && i < nb)
+        a = T[(r0 + i) + (long)(r0 + i) * ldt];
+      Ad[i][j] = a;
+    }
+    __syncthreads();
+    if (threadIdx.x < TB) Ai[threadIdx.x] = 1.0 / Ad[threadIdx.x][threadIdx.x];
+    __syncthreads();
+    const size_t o = (size_t)(r0 + lane) * C + w;
+    double xv = (lane < nb) ? x[o] - ((acc[0] + acc[1]) + (acc[2] + acc[3])) : 0.0;
+    if (FWD) {
+      for (int r = 0; r < nb; ++r) {
+        if (!UNIT && lane == r) xv *= Ai[r];
+        const double xr = __shfl_sync(0xffffffffu, xv, r);
+        if (lane > r) xv = fma(-Ad[lane][r], xr, xv);
+      }
+    } else {
+      for (int r = nb - 1; r >= 0; --r) {
+        if (!UNIT && lane == r) xv *= Ai[r];
+        const double xr = __shfl_sync(0xffffffffu, xv, r);
+        if (lane < r) xv = fma(-Ad[lane][r], xr, xv);
+      }
+    }
+    if (lane < nb) x[o] = xv;
+    __syncthreads();
+  }
+  for (int f = threadIdx.x; f < n * C; f += nt) {
+    const int c = f % C, t = f / C;
+    if (v0 + c < nvec) X[(v0 + c) * vs + (long)t * es] = x[f];
+  }
+}
+
+template <bool TRANS, bool FWD, bool UNIT>
+cudaError_t vec_solve(bbt_ctx* ctx, int n, long nvec, const double* T, long ldt, double* X, long vs, long es) {
+  static bool attr = false;
+  if (!attr) {
+    const cudaError_t e = cudaFuncSetAttribute(vec_solve_kernel<TRANS, FWD, UNIT>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)VSMEM_MAX);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  const int C = (int)std::min<long>(VC, std::max<long>(1, (nvec + ctx->num_sms - 1) / std::max(ctx->num_sms, 1)));
+  vec_solve_kernel<TRANS, FWD, UNIT><<<(unsigned)((nvec + C - 1) / C), 32 * C, vec_smem(n, C), ctx->stream>>>(
+      n, nvec, C, T, ldt, X, vs, es);
+  return cudaGetLastError();
+}
+
+// Where the single-launch vector solve applies: short operands (the
+// recursive form's GEMMs win on tall ones) whose vectors fit shared memory.
+bool vec_solve_fits(long nvec, int n) { return nvec <= 2048 && vec_smem(n, VC) <= VSMEM_MAX; }
 
 // G12 (n1 x n2, above the diagonal) <- X^T for X = G21 (n2 x n1, below), then X <- 0.
 __global__ void mirror_kernel(int n1, int n2, double* __restrict__ G, long ld) {
@@ -231,6 +346,11 @@ int split_point(int n) { return (n / 2 + TB - 1) / TB * TB; }
 
 bbt_status trsm_left_lower_unit(bbt_ctx* ctx, int n, long ncols, const double* L, long ldl, double* B, long ldb) {
   if (n <= 0 || ncols <= 0) return BBT_OK;
+  if (n > LB && vec_solve_fits(ncols, n)) {   // columns of B: x_j -= L(j, t) x_t
+    ProfScope prof(ctx, BBT_PROF_CHOL, (double)ncols * n * n);
+    BBT_CUDA(ctx, (vec_solve<false, true, true>(ctx, n, ncols, L, ldl, B, ldb, 1)));
+    return BBT_OK;
+  }
   if (n <= LB) {
     const long blocks = (ncols + 127) / 128;
     trsm_llu_leaf<<<(unsigned)blocks, 128, 0, ctx->stream>>>(n, ncols, L, ldl, B, ldb);
@@ -273,6 +393,11 @@ bbt_status apply_signs(bbt_ctx* ctx, int m, const double* d, double* R, double* 
 bbt_status trsm_right_upper(bbt_ctx* ctx, long rows, int n, const double* R, long ldr, double* A, long lda,
                             bool oz) {
   if (rows <= 0 || n <= 0) return BBT_OK;
+  if (n > TB && vec_solve_fits(rows, n)) {   // rows of A: x_j -= R(t, j) x_t, / R(j, j)
+    ProfScope prof(ctx, BBT_PROF_CHOL, (double)rows * n * n);
+    BBT_CUDA(ctx, (vec_solve<true, true, false>(ctx, n, rows, R, ldr, A, 1, lda)));
+    return BBT_OK;
+  }
   if (n <= TB) {
     const long blocks = (rows + 127) / 128;
     ProfScope prof(ctx, BBT_PROF_CHOL, (double)rows * n * n);

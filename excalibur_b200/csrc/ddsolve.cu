@@ -4,15 +4,22 @@
 //   solve R^T X = B  (trans)   or   R X = B,   R upper m x m (column-major, FP64),
 //   X, B m x k column-major double-doubles (hi + lo arrays), in place.
 //
-// Blocked in 32-row panels: a leaf kernel solves a diagonal block for every
-// column (one thread per column, right-looking substitution in double-double,
-// unrolled into registers), an update kernel subtracts the block's
-// contribution from the rows still to solve (one thread per row and four
-// columns, products of an FP64 and a double-double accumulated as a
-// compensated dot product).  The double-double operations are the
-// classical error-free transformations (Knuth's two-sum, the FMA two-product)
-// with the usual renormalisations.
+// Every column of X is an independent solve, so one CTA takes a group of up
+// to 8 columns (one warp each) and solves them start to finish with the
+// columns held in shared memory: one launch, no CTA waits for another.
+// Left-looking in 32-row blocks: the block's rows first gather the terms of
+// every row already solved (products of an FP64 and a double-double summed
+// as compensated dot products over rows of R staged through shared memory,
+// four independent chains per thread), then the 32 x 32 diagonal block is
+// solved in registers, one row per lane, broadcasting each solved row by
+// warp shuffles.  Columns too long for shared memory take a blocked
+// multi-launch path instead (a leaf kernel per diagonal block, an update
+// kernel for the rows still to solve).  The double-double operations are the
+// classical error-free transformations (Knuth's two-sum, the FMA
+// two-product) with the usual renormalisations.
 #include <cuda_runtime.h>
+
+#include <algorithm>
 
 #include "internal.h"
 
@@ -151,6 +158,115 @@ __global__ void update_kernel(int trans, int nb, int j0, int r0, int r1, int k, 
     }
 }
 
+// The single-launch solve (header).  Shared memory: the CTA's columns as
+// xh/xl[t * C + c] (m + 4 rows, zero past m), a VT x 32 tile of R and the
+// 32 x 32 diagonal block with its reciprocals.
+constexpr int VC = 8;    // columns per CTA at most (one warp each)
+constexpr int VT = 64;   // rows of R per staged tile
+constexpr size_t VFIXED = (size_t)(VT + NB) * (NB + 1) * sizeof(double) + NB * sizeof(double);
+constexpr size_t VSMEM_MAX = 227 * 1024;
+
+size_t cols_smem(int m, int C) { return 2 * (size_t)(m + 4) * C * sizeof(double) + VFIXED; }
+
+template <bool TRANS>
+__global__ void __launch_bounds__(256, 1) cols_kernel(int m, int k, int C, const double* __restrict__ R, long ldr,
+                                                      double* __restrict__ Xh, double* __restrict__ Xl, long ldx) {
+  extern __shared__ double sm[];
+  const int mp = m + 4;
+  double* xh = sm;
+  double* xl = xh + (size_t)mp * C;
+  double(*Rs)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(xl + (size_t)mp * C);
+  double(*Rd)[NB + 1] = Rs + VT;
+  double* Ri = reinterpret_cast<double*>(Rd + NB);
+  const int c0 = blockIdx.x * C, w = threadIdx.x >> 5, lane = threadIdx.x & 31, nt = blockDim.x;
+  for (int f = threadIdx.x; f < mp * C; f += nt) {   // column index fastest: 32-byte runs per column
+    const int c = f % C, t = f / C, col = c0 + c;
+    const bool ok = t < m && col < k;
+    xh[f] = ok ? Xh[(long)col * ldx + t] : 0.0;
+    xl[f] = ok ? Xl[(long)col * ldx + t] : 0.0;
+  }
+  const int nblk = (m + NB - 1) / NB;
+  for (int s = 0; s < nblk; ++s) {
+    const int b = TRANS ? s : nblk - 1 - s;
+    const int r0 = b * NB, nb = min(NB, m - r0);
+    const int ta = TRANS ? 0 : r0 + nb, tb = TRANS ? r0 : m;   // rows already solved
+    dd acc[4] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+    for (int t0 = ta; t0 < tb; t0 += VT) {
+      const int tl = min(VT, tb - t0);
+      __syncthreads();
+      // Rs[tt][rr] = coefficient of x[t0 + tt] in row r0 + rr: R(t, r) (TRANS) or R(r, t);
+      // zero past the tile, so the 4-way unrolled loop below needs no guard
+      for (int f = threadIdx.x; f < VT * NB; f += nt) {
+        const int tt = TRANS ? f % VT : f / NB, rr = TRANS ? f / VT : f % NB;
+        double v = 0.0;
+        if (tt < tl && rr < nb)
+          v = TRANS ? R[(t0 + tt) + (long)(r0 + rr) * ldr] : R[(r0 + rr) + (long)(t0 + tt) * ldr];
+        Rs[tt][rr] = v;
+      }
+      __syncthreads();
+      dot2 p[4];
+      const double* xhc = xh + (size_t)t0 * C + w;
+      const double* xlc = xl + (size_t)t0 * C + w;
+      for (int tt = 0; tt < tl; tt += 4) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) p[u].add(Rs[tt + u][lane], {xhc[(tt + u) * C], xlc[(tt + u) * C]});
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) acc[u] = dd_add(acc[u], p[u].value());
+    }
+    for (int f = threadIdx.x; f < NB * NB; f += nt) {
+      const int i = f % NB, j = f / NB;
+      Rd[i][j] = (i < nb && j < nb) ? (i <= j ? R[(r0 + i) + (long)(r0 + j) * ldr] : 0.0) : (i == j ? 1.0 : 0.0);
+    }
+    __syncthreads();
+    if (threadIdx.x < NB) Ri[threadIdx.x] = 1.0 / Rd[threadIdx.x][threadIdx.x];
+    __syncthreads();
+    const dd v = dd_add(dd_add(acc[0], acc[1]), dd_add(acc[2], acc[3]));
+    const size_t o = (size_t)(r0 + lane) * C + w;
+    dd x = {0.0, 0.0};
+    if (lane < nb) x = dd_add({xh[o], xl[o]}, {-v.hi, -v.lo});
+    if (TRANS) {   // forward with R^T: x_r, then rows t > r lose R(r, t) x_r
+      for (int r = 0; r < nb; ++r) {
+        if (lane == r) x = dd_div_d(x, Rd[r][r], Ri[r]);
+        const dd xr = {__shfl_sync(0xffffffffu, x.hi, r), __shfl_sync(0xffffffffu, x.lo, r)};
+        if (lane > r) x = dd_add(x, dd_mul_d(xr, -Rd[r][lane]));
+      }
+    } else {       // backward with R: rows t < r lose R(t, r) x_r
+      for (int r = nb - 1; r >= 0; --r) {
+        if (lane == r) x = dd_div_d(x, Rd[r][r], Ri[r]);
+        const dd xr = {__shfl_sync(0xffffffffu, x.hi, r), __shfl_sync(0xffffffffu, x.lo, r)};
+        if (lane < r) x = dd_add(x, dd_mul_d(xr, -Rd[lane][r]));
+      }
+    }
+    if (lane < nb) {
+      xh[o] = x.hi;
+      xl[o] = x.lo;
+    }
+    __syncthreads();
+  }
+  for (int f = threadIdx.x; f < m * C; f += nt) {
+    const int c = f % C, t = f / C, col = c0 + c;
+    if (col < k) {
+      Xh[(long)col * ldx + t] = xh[f];
+      Xl[(long)col * ldx + t] = xl[f];
+    }
+  }
+}
+
+template <bool TRANS>
+cudaError_t launch_cols(bbt_ctx* ctx, int m, int k, int C, const double* R, long ldr, double* Xh, double* Xl,
+                        long ldx) {
+  static bool attr = false;
+  if (!attr) {
+    const cudaError_t e =
+        cudaFuncSetAttribute(cols_kernel<TRANS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)VSMEM_MAX);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  cols_kernel<TRANS><<<(k + C - 1) / C, 32 * C, cols_smem(m, C), ctx->stream>>>(m, k, C, R, ldr, Xh, Xl, ldx);
+  return cudaGetLastError();
+}
+
 __global__ void dd_transpose_kernel(int m, const double* __restrict__ Ah, const double* __restrict__ Al, long lda,
                                     double* __restrict__ Th, double* __restrict__ Tl, long ldt) {
   __shared__ double th[32][33], tl[32][33];
@@ -189,6 +305,14 @@ bbt_status dd_trsm_left(bbt_ctx* ctx, bool trans, int m, int k, const double* R,
                         long ldx) {
   if (m < 1 || k < 1) return BBT_OK;
   ProfScope prof(ctx, BBT_PROF_DD, (double)m * m * k);
+  // about one CTA per SM; fewer columns per CTA where long columns fill shared memory
+  int C = std::min(VC, std::max(1, (k + ctx->num_sms - 1) / std::max(ctx->num_sms, 1)));
+  while (C > 1 && cols_smem(m, C) > VSMEM_MAX) --C;
+  if (cols_smem(m, C) <= VSMEM_MAX) {
+    BBT_CUDA(ctx, trans ? launch_cols<true>(ctx, m, k, C, R, ldr, Xh, Xl, ldx)
+                        : launch_cols<false>(ctx, m, k, C, R, ldr, Xh, Xl, ldx));
+    return BBT_OK;
+  }
   const int nblk = (m + NB - 1) / NB;
   for (int s = 0; s < nblk; ++s) {
     const int b = trans ? s : nblk - 1 - s;

@@ -299,7 +299,13 @@ typedef struct {
                                     in place of FinalVT; no FinalU */
   int precision;                 /* 0: plain FP64 (the reference's Householder local QR);
                                     1: mixed -- local QR by a BF16x3 tensor-core sketch
-                                    and one FP64 Cholesky-QR refinement pass */
+                                    and one FP64 Cholesky-QR refinement pass;
+                                    2: exact Gram -- the sketch as preconditioner, the
+                                    Gram of each block computed exactly from int8
+                                    residues (CRT), the congruence in double-double, Q
+                                    never formed and applied by exact products
+                                    (bbt_exact_local_qr, bbt_exact_apply_q); the
+                                    tall-and-skinny branch runs precision 2 as 1 */
   const double* labels;          /* svd_mode 4: y, m values (device memory for bbt_fedsvd_run, host
                                     memory for bbt_fedsvd_run_host; the reference's y.mat, held by
                                     the last participant); NULL otherwise */
