@@ -89,87 +89,157 @@ __global__ void __launch_bounds__(128) trsm_leaf(long rows, int n, const double*
 // the block first gathers the solved terms through VT x 32 tiles of A staged
 // in shared memory (four FMA chains per thread), then solves its diagonal
 // block in registers, one element per lane, broadcasting by warp shuffles.
-// For square and short operands (rows up to a few thousand), where the
-// recursive form spends its time in launches.
-constexpr int VC = 8, VT = 64;
-constexpr size_t VFIXED = (size_t)(VT + TB) * (TB + 1) * sizeof(double) + TB * sizeof(double);
+// The tiles and diagonal blocks are one fixed sequence of copies,
+// independent of X, double-buffered so that the next copy is in flight
+// while the current one is used.  For square and short operands (rows up to
+// a few thousand), where the recursive form spends its time in launches.
+constexpr int VC = 8, VT = 128, VS = VT + 2;   // VS: row stride of a staged tile (16-byte loads, distinct banks)
+constexpr size_t VFIXED = (size_t)2 * TB * VS * sizeof(double) + (size_t)2 * TB * (TB + 1) * sizeof(double) +
+                          TB * sizeof(double);
 constexpr size_t VSMEM_MAX = 227 * 1024;
 
-size_t vec_smem(int n, int C) { return (size_t)(n + 4) * C * sizeof(double) + VFIXED; }
+__host__ __device__ inline int vec_np(int n) { return (n + 5) & ~1; }
+size_t vec_smem(int n, int C) { return (size_t)vec_np(n) * C * sizeof(double) + VFIXED; }
+
+// 8-byte asynchronous global -> shared copy; zero-fills when !valid (no read).
+__device__ __forceinline__ void cp_async8(double* dst, const double* src, bool valid) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(valid ? 8 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+struct VecJob {
+  int diag, b, r0, nb, t0, tl, buf;
+};
+
+// Job sequence: for each block in solve order, its update tiles over the
+// solved elements, then its diagonal block.  (s, t0): the block of the solve
+// order and its next update start (a multiple of 32).
+template <bool FWD>
+__device__ __forceinline__ bool vec_next_job(int n, int nblk, int& s, int& t0, VecJob& J) {
+  if (s >= nblk) return false;
+  const int b = FWD ? s : nblk - 1 - s;
+  const int r0 = b * TB, nb = min(TB, n - r0);
+  const int tb = FWD ? r0 : n;
+  J.b = b;
+  J.r0 = r0;
+  J.nb = nb;
+  if (t0 < tb) {
+    J.diag = 0;
+    J.t0 = t0;
+    J.tl = min(VT, tb - t0);
+    t0 += VT;
+  } else {
+    J.diag = 1;
+    if (++s < nblk) {
+      const int b2 = FWD ? s : nblk - 1 - s;
+      t0 = FWD ? 0 : b2 * TB + min(TB, n - b2 * TB);
+    }
+  }
+  return true;
+}
 
 template <bool TRANS, bool FWD, bool UNIT>
 __global__ void __launch_bounds__(256, 1) vec_solve_kernel(int n, long nvec, int C, const double* __restrict__ T,
                                                            long ldt, double* __restrict__ X, long vs, long es) {
-  extern __shared__ double sm[];
-  const int np = n + 4;
-  double* x = sm;   // x[t * C + c]
-  double(*As)[TB + 1] = reinterpret_cast<double(*)[TB + 1]>(x + (size_t)np * C);
-  double(*Ad)[TB + 1] = As + VT;
-  double* Ai = reinterpret_cast<double*>(Ad + TB);
+  extern __shared__ double2 smv[];
+  const int np = vec_np(n);
+  double* x = reinterpret_cast<double*>(smv);   // x[c * np + t]
+  double* As = x + (size_t)np * C;              // [2][TB][VS]
+  double(*Ad)[TB + 1] = reinterpret_cast<double(*)[TB + 1]>(As + 2 * TB * VS);   // [2][TB]
+  double* Ai = reinterpret_cast<double*>(Ad + 2 * TB);
   const long v0 = (long)blockIdx.x * C;
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, nt = blockDim.x;
-  for (int f = threadIdx.x; f < np * C; f += nt) {   // vector index fastest
-    const int c = f % C, t = f / C;
-    x[f] = (t < n && v0 + c < nvec) ? X[(v0 + c) * vs + (long)t * es] : 0.0;
-  }
   const int nblk = (n + TB - 1) / TB;
-  for (int s = 0; s < nblk; ++s) {
-    const int b = FWD ? s : nblk - 1 - s;
-    const int r0 = b * TB, nb = min(TB, n - r0);
-    const int ta = FWD ? 0 : r0 + nb, tb = FWD ? r0 : n;   // elements already solved
-    double acc[4] = {0.0, 0.0, 0.0, 0.0};
-    for (int t0 = ta; t0 < tb; t0 += VT) {
-      const int tl = min(VT, tb - t0);
-      __syncthreads();
-      // As[tt][rr] = A(r0 + rr, t0 + tt), zero past the tile
+  int nu = 0;
+  auto issue = [&](VecJob& J) {
+    if (J.diag) {   // D[i][j] = A(r0 + i, r0 + j) in the solved direction and, unless UNIT, on the diagonal
+      double(*D)[TB + 1] = Ad + (J.b & 1) * TB;
+      for (int f = threadIdx.x; f < TB * TB; f += nt) {
+        const int i = f % TB, j = f / TB;
+        const bool ok = i < J.nb && j < J.nb && ((FWD ? j < i : j > i) || (!UNIT && i == j));
+        const double* src = TRANS ? T + (J.r0 + j) + (long)(J.r0 + i) * ldt : T + (J.r0 + i) + (long)(J.r0 + j) * ldt;
+        cp_async8(&D[i][j], ok ? src : T, ok);
+      }
+    } else {        // S[rr][tt] = A(r0 + rr, t0 + tt), zero past the tile
+      J.buf = nu++ & 1;
+      double* S = As + (size_t)J.buf * TB * VS;
       for (int f = threadIdx.x; f < VT * TB; f += nt) {
         const int tt = TRANS ? f % VT : f / TB, rr = TRANS ? f / VT : f % TB;
-        double a = 0.0;
-        if (tt < tl && rr < nb)
-          a = TRANS ? T[(t0 + tt) + (long)(r0 + rr) * ldt] : T[(r0 + rr) + (long)(t0 + tt) * ldt];
-        As[tt][rr] = a;
-      }
-      __syncthreads();
-      const double* xc = x + (size_t)t0 * C + w;
-      for (int tt = 0; tt < tl; tt += 4) {
-#pragma unroll
-        for (int u = 0; u < 4; ++u) acc[u] = fma(As[tt + u][lane], xc[(tt + u) * C], acc[u]);
+        const bool ok = tt < J.tl && rr < J.nb;
+        const double* src = TRANS ? T + (J.t0 + tt) + (long)(J.r0 + rr) * ldt : T + (J.r0 + rr) + (long)(J.t0 + tt) * ldt;
+        cp_async8(S + rr * VS + tt, ok ? src : T, ok);
       }
     }
-    // Ad[i][j] = A(r0 + i, r0 + j), identity past nb
-    for (int f = threadIdx.x; f < TB * TB; f += nt) {
-      const int i = f % TB, j = f / TB;
-      double a = (i == j) ? 1.0 : 0.0;
-      if (i < nb && j < nb && (FWD ? j < i : j > i))
-        a = TRANS ? T[(r0 + j) + (long)(r0 + i) * ldt] : T[(r0 + i) + (long)(r0 + j) * ldt];
-      else if (!UNIT && i == j && i < nb)
-        a = T[(r0 + i) + (long)(r0 + i) * ldt];
-      Ad[i][j] = a;
+    cp_async_commit();
+  };
+  int s = 0, tn = FWD ? 0 : n;
+  VecJob cur, nxt;
+  vec_next_job<FWD>(n, nblk, s, tn, cur);
+  issue(cur);
+  for (int f = threadIdx.x; f < np * C; f += nt) {   // vector index fastest
+    const int c = f % C, t = f / C;
+    x[(size_t)c * np + t] = (t < n && v0 + c < nvec) ? X[(v0 + c) * vs + (long)t * es] : 0.0;
+  }
+  double* xw = x + (size_t)w * np;   // this warp's vector
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  bool more = true;
+  while (more) {
+    more = vec_next_job<FWD>(n, nblk, s, tn, nxt);
+    if (more) {
+      issue(nxt);
+      cp_async_wait_1();
+    } else {
+      cp_async_wait_0();
     }
     __syncthreads();
-    if (threadIdx.x < TB) Ai[threadIdx.x] = 1.0 / Ad[threadIdx.x][threadIdx.x];
-    __syncthreads();
-    const size_t o = (size_t)(r0 + lane) * C + w;
-    double xv = (lane < nb) ? x[o] - ((acc[0] + acc[1]) + (acc[2] + acc[3])) : 0.0;
-    if (FWD) {
-      for (int r = 0; r < nb; ++r) {
-        if (!UNIT && lane == r) xv *= Ai[r];
-        const double xr = __shfl_sync(0xffffffffu, xv, r);
-        if (lane > r) xv = fma(-Ad[lane][r], xr, xv);
+    if (!cur.diag) {
+      const double* arow = As + (size_t)cur.buf * TB * VS + lane * VS;
+      const double* xv = xw + cur.t0;   // 16-byte aligned: np and t0 are even
+      for (int tt = 0; tt < cur.tl; tt += 4) {
+        const double2 a01 = *reinterpret_cast<const double2*>(arow + tt);
+        const double2 a23 = *reinterpret_cast<const double2*>(arow + tt + 2);
+        const double2 x01 = *reinterpret_cast<const double2*>(xv + tt);
+        const double2 x23 = *reinterpret_cast<const double2*>(xv + tt + 2);
+        acc[0] = fma(a01.x, x01.x, acc[0]);
+        acc[1] = fma(a01.y, x01.y, acc[1]);
+        acc[2] = fma(a23.x, x23.x, acc[2]);
+        acc[3] = fma(a23.y, x23.y, acc[3]);
       }
     } else {
-      for (int r = nb - 1; r >= 0; --r) {
-        if (!UNIT && lane == r) xv *= Ai[r];
-        const double xr = __shfl_sync(0xffffffffu, xv, r);
-        if (lane < r) xv = fma(-Ad[lane][r], xr, xv);
+      double(*D)[TB + 1] = Ad + (cur.b & 1) * TB;
+      if (threadIdx.x < TB) {
+        if (UNIT || threadIdx.x >= cur.nb) D[threadIdx.x][threadIdx.x] = 1.0;
+        Ai[threadIdx.x] = 1.0 / D[threadIdx.x][threadIdx.x];
       }
+      __syncthreads();
+      const int nb = cur.nb;
+      double xv = (lane < nb) ? xw[cur.r0 + lane] - ((acc[0] + acc[1]) + (acc[2] + acc[3])) : 0.0;
+      if (FWD) {
+        for (int r = 0; r < nb; ++r) {
+          if (!UNIT && lane == r) xv *= Ai[r];
+          const double xr = __shfl_sync(0xffffffffu, xv, r);
+          if (lane > r) xv = fma(-D[lane][r], xr, xv);
+        }
+      } else {
+        for (int r = nb - 1; r >= 0; --r) {
+          if (!UNIT && lane == r) xv *= Ai[r];
+          const double xr = __shfl_sync(0xffffffffu, xv, r);
+          if (lane < r) xv = fma(-D[lane][r], xr, xv);
+        }
+      }
+      if (lane < nb) xw[cur.r0 + lane] = xv;
+#pragma unroll
+      for (int u = 0; u < 4; ++u) acc[u] = 0.0;
     }
-    if (lane < nb) x[o] = xv;
     __syncthreads();
+    cur = nxt;
   }
   for (int f = threadIdx.x; f < n * C; f += nt) {
     const int c = f % C, t = f / C;
-    if (v0 + c < nvec) X[(v0 + c) * vs + (long)t * es] = x[f];
+    if (v0 + c < nvec) X[(v0 + c) * vs + (long)t * es] = x[(size_t)c * np + t];
   }
 }
 

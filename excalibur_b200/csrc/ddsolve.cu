@@ -159,96 +159,173 @@ __global__ void update_kernel(int trans, int nb, int j0, int r0, int r1, int k, 
 }
 
 // The single-launch solve (header).  Shared memory: the CTA's columns as
-// xh/xl[t * C + c] (m + 4 rows, zero past m), a VT x 32 tile of R and the
-// 32 x 32 diagonal block with its reciprocals.
-constexpr int VC = 8;    // columns per CTA at most (one warp each)
-constexpr int VT = 64;   // rows of R per staged tile
-constexpr size_t VFIXED = (size_t)(VT + NB) * (NB + 1) * sizeof(double) + NB * sizeof(double);
+// (hi, lo) pairs, column-major xs[c][mp] (mp = m + 4 rounded to even, zero
+// past m); two 32 x VT tiles of R with a row per output row (row stride VT + 2,
+// so a lane's 16-byte loads hit distinct banks) and two 32 x 32 diagonal
+// blocks, double-buffered: the next copy is in flight while the current one
+// is used; the diagonal's reciprocals.
+constexpr int VC = 8;     // columns per CTA at most (one warp each)
+constexpr int VT = 128;   // solved rows per staged tile
+constexpr int VS = VT + 2;
+constexpr size_t VFIXED = (size_t)2 * NB * VS * sizeof(double) + (size_t)2 * NB * (NB + 1) * sizeof(double) +
+                          NB * sizeof(double);
 constexpr size_t VSMEM_MAX = 227 * 1024;
 
-size_t cols_smem(int m, int C) { return 2 * (size_t)(m + 4) * C * sizeof(double) + VFIXED; }
+__host__ __device__ inline int cols_mp(int m) { return (m + 5) & ~1; }
+size_t cols_smem(int m, int C) { return (size_t)cols_mp(m) * C * sizeof(double2) + VFIXED; }
+
+// 8-byte asynchronous global -> shared copy; zero-fills when !valid (no read).
+__device__ __forceinline__ void cp_async8(double* dst, const double* src, bool valid) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(valid ? 8 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// The loads of the solve form one fixed sequence of jobs, independent of X:
+// for each 32-row block (in solve order) its update tiles of VT solved rows,
+// then its diagonal block.  Job j's copy is issued while job j - 1 is used.
+// Update tiles start at multiples of 32 (16-byte aligned rows of xs).
+struct ColsJob {
+  int diag, b, r0, nb, t0, tl, buf;
+};
+
+template <bool TRANS>
+__device__ __forceinline__ bool next_job(int m, int nblk, int& s, int& t0, ColsJob& J) {
+  // (s, t0): block s of the solve order and the start of its next update tile
+  if (s >= nblk) return false;
+  const int b = TRANS ? s : nblk - 1 - s;
+  const int r0 = b * NB, nb = min(NB, m - r0);
+  const int tb = TRANS ? r0 : m;
+  J.b = b;
+  J.r0 = r0;
+  J.nb = nb;
+  if (t0 < tb) {
+    J.diag = 0;
+    J.t0 = t0;
+    J.tl = min(VT, tb - t0);
+    t0 += VT;
+  } else {
+    J.diag = 1;
+    if (++s < nblk) {
+      const int b2 = TRANS ? s : nblk - 1 - s;
+      t0 = TRANS ? 0 : b2 * NB + min(NB, m - b2 * NB);
+    }
+  }
+  return true;
+}
 
 template <bool TRANS>
 __global__ void __launch_bounds__(256, 1) cols_kernel(int m, int k, int C, const double* __restrict__ R, long ldr,
                                                       double* __restrict__ Xh, double* __restrict__ Xl, long ldx) {
-  extern __shared__ double sm[];
-  const int mp = m + 4;
-  double* xh = sm;
-  double* xl = xh + (size_t)mp * C;
-  double(*Rs)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(xl + (size_t)mp * C);
-  double(*Rd)[NB + 1] = Rs + VT;
-  double* Ri = reinterpret_cast<double*>(Rd + NB);
+  extern __shared__ double4 sm4[];
+  const int mp = cols_mp(m);
+  double2* xs = reinterpret_cast<double2*>(sm4);                        // [C][mp]
+  double* Rs = reinterpret_cast<double*>(xs + (size_t)mp * C);          // [2][NB][VS]
+  double(*Rd)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(Rs + 2 * NB * VS);   // [2][NB]
+  double* Ri = reinterpret_cast<double*>(Rd + 2 * NB);
   const int c0 = blockIdx.x * C, w = threadIdx.x >> 5, lane = threadIdx.x & 31, nt = blockDim.x;
+  const int nblk = (m + NB - 1) / NB;
+  int nu = 0;   // update tiles issued so far: they alternate between the two buffers
+  auto issue = [&](ColsJob& J) {
+    if (J.diag) {   // Rd[i][j] = R(r0 + i, r0 + j), upper triangle; zero elsewhere (diagonal padding fixed later)
+      double(*D)[NB + 1] = Rd + (J.b & 1) * NB;
+      for (int f = threadIdx.x; f < NB * NB; f += nt) {
+        const int i = f % NB, j = f / NB;
+        const bool ok = i < J.nb && j < J.nb && i <= j;
+        cp_async8(&D[i][j], ok ? R + (J.r0 + i) + (long)(J.r0 + j) * ldr : R, ok);
+      }
+    } else {        // T[rr][tt] = coefficient of x[t0 + tt] in row r0 + rr: R(t, r) (TRANS) or R(r, t)
+      J.buf = nu++ & 1;
+      double* T = Rs + (size_t)J.buf * NB * VS;
+      for (int f = threadIdx.x; f < VT * NB; f += nt) {
+        const int tt = TRANS ? f % VT : f / NB, rr = TRANS ? f / VT : f % NB;
+        const bool ok = tt < J.tl && rr < J.nb;
+        const double* src = TRANS ? R + (J.t0 + tt) + (long)(J.r0 + rr) * ldr : R + (J.r0 + rr) + (long)(J.t0 + tt) * ldr;
+        cp_async8(T + rr * VS + tt, ok ? src : R, ok);
+      }
+    }
+    cp_async_commit();
+  };
+
+  int s = 0, tn = TRANS ? 0 : m;
+  ColsJob cur, nxt;
+  next_job<TRANS>(m, nblk, s, tn, cur);
+  issue(cur);
   for (int f = threadIdx.x; f < mp * C; f += nt) {   // column index fastest: 32-byte runs per column
     const int c = f % C, t = f / C, col = c0 + c;
     const bool ok = t < m && col < k;
-    xh[f] = ok ? Xh[(long)col * ldx + t] : 0.0;
-    xl[f] = ok ? Xl[(long)col * ldx + t] : 0.0;
+    xs[(size_t)c * mp + t] = ok ? make_double2(Xh[(long)col * ldx + t], Xl[(long)col * ldx + t]) : make_double2(0.0, 0.0);
   }
-  const int nblk = (m + NB - 1) / NB;
-  for (int s = 0; s < nblk; ++s) {
-    const int b = TRANS ? s : nblk - 1 - s;
-    const int r0 = b * NB, nb = min(NB, m - r0);
-    const int ta = TRANS ? 0 : r0 + nb, tb = TRANS ? r0 : m;   // rows already solved
-    dd acc[4] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
-    for (int t0 = ta; t0 < tb; t0 += VT) {
-      const int tl = min(VT, tb - t0);
-      __syncthreads();
-      // Rs[tt][rr] = coefficient of x[t0 + tt] in row r0 + rr: R(t, r) (TRANS) or R(r, t);
-      // zero past the tile, so the 4-way unrolled loop below needs no guard
-      for (int f = threadIdx.x; f < VT * NB; f += nt) {
-        const int tt = TRANS ? f % VT : f / NB, rr = TRANS ? f / VT : f % NB;
-        double v = 0.0;
-        if (tt < tl && rr < nb)
-          v = TRANS ? R[(t0 + tt) + (long)(r0 + rr) * ldr] : R[(r0 + rr) + (long)(t0 + tt) * ldr];
-        Rs[tt][rr] = v;
-      }
-      __syncthreads();
+  double2* xw = xs + (size_t)w * mp;   // this warp's column
+  dd acc[4] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+  bool more = true;
+  while (more) {
+    more = next_job<TRANS>(m, nblk, s, tn, nxt);
+    if (more) {
+      issue(nxt);
+      cp_async_wait_1();
+    } else {
+      cp_async_wait_0();
+    }
+    __syncthreads();
+    if (!cur.diag) {
+      const double* arow = Rs + (size_t)cur.buf * NB * VS + lane * VS;
+      const double2* xv = xw + cur.t0;
       dot2 p[4];
-      const double* xhc = xh + (size_t)t0 * C + w;
-      const double* xlc = xl + (size_t)t0 * C + w;
-      for (int tt = 0; tt < tl; tt += 4) {
-#pragma unroll
-        for (int u = 0; u < 4; ++u) p[u].add(Rs[tt + u][lane], {xhc[(tt + u) * C], xlc[(tt + u) * C]});
+      // zero past the tile, so the 4-way unrolled loop needs no guard (rows up to m + 2 < mp)
+      for (int tt = 0; tt < cur.tl; tt += 4) {
+        const double2 a01 = *reinterpret_cast<const double2*>(arow + tt);
+        const double2 a23 = *reinterpret_cast<const double2*>(arow + tt + 2);
+        const double2 x0 = xv[tt], x1 = xv[tt + 1], x2 = xv[tt + 2], x3 = xv[tt + 3];
+        p[0].add(a01.x, {x0.x, x0.y});
+        p[1].add(a01.y, {x1.x, x1.y});
+        p[2].add(a23.x, {x2.x, x2.y});
+        p[3].add(a23.y, {x3.x, x3.y});
       }
 #pragma unroll
       for (int u = 0; u < 4; ++u) acc[u] = dd_add(acc[u], p[u].value());
-    }
-    for (int f = threadIdx.x; f < NB * NB; f += nt) {
-      const int i = f % NB, j = f / NB;
-      Rd[i][j] = (i < nb && j < nb) ? (i <= j ? R[(r0 + i) + (long)(r0 + j) * ldr] : 0.0) : (i == j ? 1.0 : 0.0);
-    }
-    __syncthreads();
-    if (threadIdx.x < NB) Ri[threadIdx.x] = 1.0 / Rd[threadIdx.x][threadIdx.x];
-    __syncthreads();
-    const dd v = dd_add(dd_add(acc[0], acc[1]), dd_add(acc[2], acc[3]));
-    const size_t o = (size_t)(r0 + lane) * C + w;
-    dd x = {0.0, 0.0};
-    if (lane < nb) x = dd_add({xh[o], xl[o]}, {-v.hi, -v.lo});
-    if (TRANS) {   // forward with R^T: x_r, then rows t > r lose R(r, t) x_r
-      for (int r = 0; r < nb; ++r) {
-        if (lane == r) x = dd_div_d(x, Rd[r][r], Ri[r]);
-        const dd xr = {__shfl_sync(0xffffffffu, x.hi, r), __shfl_sync(0xffffffffu, x.lo, r)};
-        if (lane > r) x = dd_add(x, dd_mul_d(xr, -Rd[r][lane]));
+    } else {
+      double(*D)[NB + 1] = Rd + (cur.b & 1) * NB;
+      if (threadIdx.x < NB) {
+        if (threadIdx.x >= cur.nb) D[threadIdx.x][threadIdx.x] = 1.0;   // identity past the block
+        Ri[threadIdx.x] = 1.0 / D[threadIdx.x][threadIdx.x];
       }
-    } else {       // backward with R: rows t < r lose R(t, r) x_r
-      for (int r = nb - 1; r >= 0; --r) {
-        if (lane == r) x = dd_div_d(x, Rd[r][r], Ri[r]);
-        const dd xr = {__shfl_sync(0xffffffffu, x.hi, r), __shfl_sync(0xffffffffu, x.lo, r)};
-        if (lane < r) x = dd_add(x, dd_mul_d(xr, -Rd[lane][r]));
+      __syncthreads();
+      const int r0 = cur.r0, nb = cur.nb;
+      const dd v = dd_add(dd_add(acc[0], acc[1]), dd_add(acc[2], acc[3]));
+      dd x = {0.0, 0.0};
+      if (lane < nb) {
+        const double2 b = xw[r0 + lane];
+        x = dd_add({b.x, b.y}, {-v.hi, -v.lo});
       }
-    }
-    if (lane < nb) {
-      xh[o] = x.hi;
-      xl[o] = x.lo;
+      if (TRANS) {   // forward with R^T: x_r, then rows t > r lose R(r, t) x_r
+        for (int r = 0; r < nb; ++r) {
+          if (lane == r) x = dd_div_d(x, D[r][r], Ri[r]);
+          const dd xr = {__shfl_sync(0xffffffffu, x.hi, r), __shfl_sync(0xffffffffu, x.lo, r)};
+          if (lane > r) x = dd_add(x, dd_mul_d(xr, -D[r][lane]));
+        }
+      } else {       // backward with R: rows t < r lose R(t, r) x_r
+        for (int r = nb - 1; r >= 0; --r) {
+          if (lane == r) x = dd_div_d(x, D[r][r], Ri[r]);
+          const dd xr = {__shfl_sync(0xffffffffu, x.hi, r), __shfl_sync(0xffffffffu, x.lo, r)};
+          if (lane < r) x = dd_add(x, dd_mul_d(xr, -D[lane][r]));
+        }
+      }
+      if (lane < nb) xw[r0 + lane] = make_double2(x.hi, x.lo);
+#pragma unroll
+      for (int u = 0; u < 4; ++u) acc[u] = {0.0, 0.0};
     }
     __syncthreads();
+    cur = nxt;
   }
   for (int f = threadIdx.x; f < m * C; f += nt) {
     const int c = f % C, t = f / C, col = c0 + c;
     if (col < k) {
-      Xh[(long)col * ldx + t] = xh[f];
-      Xl[(long)col * ldx + t] = xl[f];
+      const double2 v = xs[(size_t)c * mp + t];
+      Xh[(long)col * ldx + t] = v.x;
+      Xl[(long)col * ldx + t] = v.y;
     }
   }
 }

@@ -13,16 +13,20 @@
 // and a step is two grid-wide phases separated by bounded grid barriers:
 //
 //   B1 (column-partitioned, one CTA per SM, 8 columns x 32 row phases per
-//      pass): every CTA forms the reflector from g (same arithmetic in every
-//      CTA), writes its share of the Householder store, vt = sum_t h_t
-//      W[i+1+t] for its columns, the next row i+1 after the update, and row
-//      i of V (w_i - beta v_{i-1}) / alpha_i.
+//      pass): every CTA forms the reflector from g and the step's extra
+//      dots from the CTAs' partial sums (the same sums in the same order in
+//      every CTA), writes its share of the Householder store, vt = sum_t
+//      h_t W[i+1+t] for its columns, the next row i+1 after the update, row
+//      i of V (w_i - beta v_{i-1}) / alpha_i, and its columns' share of the
+//      next step's extra dots (w_{i+1}.v_i, v_i.v_i, w_{i+1}.w_{i+1}).
 //   B2 (row-partitioned, one warp per row): W[r] += (-tau vt) h_r for
 //      r > i, and, in the same pass, the next step's Gram row
-//      g'[r] = W[r] . W[i+1]; CTA 0 adds the next step's four dots.
+//      g'[r] = W[r] . W[i+1].
+// The passes over W keep four loads in flight per thread.
 //
 // Barriers spin a bounded number of times; on a timeout every CTA stops and
 // the host reports BBT_ERR_TIMEOUT.
+#include <algorithm>
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
@@ -45,7 +49,7 @@ struct RalhaArgs {
   double* beta;    // m-1 (lower bidiagonal)
   double* V;       // m x n row-major, left vectors, zero on entry
   double* g;       // 2 x m: Gram rows, ping-pong between steps
-  double* extra;   // 2 x 4: the four extra dots, ping-pong between steps
+  double* part;    // 2 x grid x 4: per-CTA partial extra dots, ping-pong between steps
   double* vt;      // n
   double* tv;      // n: -tau * vt
   double* nextw;   // n: row i+1 after the update
@@ -63,6 +67,25 @@ __device__ double block_sum(double v, double* sh) {
   for (int k = 0; k < RW; ++k) s += sh[k];
   __syncthreads();
   return s;
+}
+
+// Four block-wide sums in one pass (two barriers).
+__device__ void block_sum4(double (&v)[4], double (*sh)[4]) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+    for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_down_sync(0xffffffffu, v[q], o);
+  if (lane == 0)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) sh[w][q] = v[q];
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    double t = 0.0;
+    for (int k = 0; k < RW; ++k) t += sh[k][q];
+    v[q] = t;
+  }
+  __syncthreads();
 }
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -84,8 +107,9 @@ __device__ void gram_rows(const RalhaArgs& A, int i, const double* piv, double* 
   }
 }
 
-__global__ void __launch_bounds__(RT) ralha_kernel(RalhaArgs A) {
+__global__ void __launch_bounds__(RT, 1) ralha_kernel(RalhaArgs A) {
   __shared__ double sh[RW];
+  __shared__ double sh4[RW][4];
   __shared__ double scal[6];   // beta_{i-1}, alpha_i, tau, scale, 1/alpha_i
   __shared__ double red[RT / CB][CB + 1];
   const int m = A.m, n = A.n;
@@ -113,13 +137,20 @@ __global__ void __launch_bounds__(RT) ralha_kernel(RalhaArgs A) {
     const int len = m - 1 - i;   // g[0..len)
     const double* g = A.g + (long)(i & 1) * m;
     double* gn = A.g + (long)((i + 1) & 1) * m;
-    const double* ex = A.extra + (i & 1) * 4;
-    double* exn = A.extra + ((i + 1) & 1) * 4;
-    // ---- scalars (identical in every CTA)
+    const double* pin = A.part + (long)(i & 1) * gridDim.x * 4;
+    double* pout = A.part + (long)((i + 1) & 1) * gridDim.x * 4;
+    // ---- scalars (identical in every CTA: the same sums in the same order)
     {
-      double s = 0.0;
-      for (int t = 1 + tid; t < len; t += RT) s += g[t] * g[t];
-      s = block_sum(s, sh);
+      double v4[4] = {0.0, 0.0, 0.0, 0.0};
+      for (int t = 1 + tid; t < len; t += RT) v4[0] += g[t] * g[t];
+      if (i > 0)   // the extra dots of this step: the CTAs' partial sums from the previous B1
+        for (int q = tid; q < gridDim.x; q += RT) {
+          v4[1] += pin[4 * q];
+          v4[2] += pin[4 * q + 1];
+          v4[3] += pin[4 * q + 2];
+        }
+      block_sum4(v4, sh4);
+      const double s = v4[0];
       if (tid == 0) {
         const double al = g[0];
         double be = al, ta = 0.0, scl = 0.0;
@@ -131,9 +162,9 @@ __global__ void __launch_bounds__(RT) ralha_kernel(RalhaArgs A) {
         }
         scal[2] = ta;
         scal[3] = scl;
-        if (i > 0) {
-          const double b = ex[0];
-          const double vv = ex[1], ww = ex[2], vw = ex[3];
+        if (i > 0) {   // w_i.v_{i-1}, v_{i-1}.v_{i-1}, w_i.w_i
+          const double b = v4[1];
+          const double vv = v4[2], ww = v4[3], vw = v4[1];
           const double a = sqrt(vv * (b * b) + ww - 2 * b * vw);
           scal[0] = b;
           scal[1] = a;
@@ -156,11 +187,28 @@ __global__ void __launch_bounds__(RT) ralha_kernel(RalhaArgs A) {
       for (int cb = 0; cb < ncol; cb += CB) {
         const int c = c0 + cb + (tid % CB);
         double s = 0.0;
-        if (c < c1)
-          for (int t = tid / CB; t < len; t += RT / CB) {
-            const double h = (t == 0) ? 1.0 : g[t] * scl;
-            s += h * A.W[(long)(i + 1 + t) * n + c];
+        if (c < c1) {
+          // four rows per iteration: their loads are in flight together
+          constexpr int PH = RT / CB;
+          const double* wc = A.W + (long)(i + 1) * n + c;
+          double s1 = 0.0;
+          int t = tid / CB;
+          if (t == 0) {
+            s = wc[0];   // h_0 = 1
+            t += PH;
           }
+          for (; t + 3 * PH < len; t += 4 * PH) {
+            const double w0 = wc[(long)t * n], w1 = wc[(long)(t + PH) * n];
+            const double w2 = wc[(long)(t + 2 * PH) * n], w3 = wc[(long)(t + 3 * PH) * n];
+            const double h0 = g[t], h1 = g[t + PH], h2 = g[t + 2 * PH], h3 = g[t + 3 * PH];
+            s += (h0 * scl) * w0;
+            s1 += (h1 * scl) * w1;
+            s += (h2 * scl) * w2;
+            s1 += (h3 * scl) * w3;
+          }
+          for (; t < len; t += PH) s += (g[t] * scl) * wc[(long)t * n];
+          s += s1;
+        }
         red[tid / CB][tid % CB] = s;
         __syncthreads();
         if (tid < CB && c0 + cb + tid < c1) {
@@ -182,9 +230,29 @@ __global__ void __launch_bounds__(RT) ralha_kernel(RalhaArgs A) {
           A.V[(long)i * n + c] = inva * w;
         }
       }
+      // this CTA's share of the next step's extra dots: w_{i+1}.v_i, v_i.v_i, w_{i+1}.w_{i+1}
+      __syncthreads();
+      if (tid < 32) {
+        double p0 = 0.0, p1 = 0.0, p2 = 0.0;
+        const double* v = A.V + (long)i * n;
+        for (int c = c0 + tid; c < c1; c += 32) {
+          const double w = A.nextw[c], vc = v[c];
+          p0 += w * vc;
+          p1 += vc * vc;
+          p2 += w * w;
+        }
+        p0 = warp_sum(p0);
+        p1 = warp_sum(p1);
+        p2 = warp_sum(p2);
+        if (tid == 0) {
+          pout[4 * blockIdx.x] = p0;
+          pout[4 * blockIdx.x + 1] = p1;
+          pout[4 * blockIdx.x + 2] = p2;
+        }
+      }
     }
     if (!grid_sync(A.bar, A.err)) return;
-    // ---- B2: rank-1 update of rows i+1.., next Gram row, next extras
+    // ---- B2: rank-1 update of rows i+1.., next Gram row
     {
       const int gw = blockIdx.x * RW + (tid >> 5), lane = tid & 31;
       const int nw = gridDim.x * RW;
@@ -192,30 +260,30 @@ __global__ void __launch_bounds__(RT) ralha_kernel(RalhaArgs A) {
         const int t = r - i - 1;
         const double h = (t == 0) ? 1.0 : g[t] * scl;
         double* row = A.W + (long)r * n;
-        double s = 0.0;
-        for (int c = lane; c < n; c += 32) {
+        double s = 0.0, s1 = 0.0;
+        int c = lane;
+        for (; c + 96 < n; c += 128) {   // four segments per iteration, loads in flight together
+          const double r0 = row[c], r1 = row[c + 32], r2 = row[c + 64], r3 = row[c + 96];
+          const double t0 = A.tv[c], t1 = A.tv[c + 32], t2 = A.tv[c + 64], t3 = A.tv[c + 96];
+          const double x0 = A.nextw[c], x1 = A.nextw[c + 32], x2 = A.nextw[c + 64], x3 = A.nextw[c + 96];
+          const double w0 = r0 + t0 * h, w1 = r1 + t1 * h, w2 = r2 + t2 * h, w3 = r3 + t3 * h;
+          row[c] = w0;
+          row[c + 32] = w1;
+          row[c + 64] = w2;
+          row[c + 96] = w3;
+          s += w0 * x0;
+          s1 += w1 * x1;
+          s += w2 * x2;
+          s1 += w3 * x3;
+        }
+        for (; c < n; c += 32) {
           const double w = row[c] + A.tv[c] * h;
           row[c] = w;
           s += w * A.nextw[c];
         }
-        s = warp_sum(s);
+        s = warp_sum(s + s1);
         // g for step i+1 has entries for rows >= i+2
         if (lane == 0 && r >= i + 2) gn[r - i - 2] = s;
-      }
-      if (blockIdx.x == 0) {
-        // extras for step i+1: w_{i+1}.v_i, v_i.v_i, w_{i+1}.w_{i+1}, v_i.w_{i+1}
-        double s0 = 0.0, s1 = 0.0, s2 = 0.0;
-        const double* v = A.V + (long)i * n;
-        for (int c = tid; c < n; c += RT) {
-          const double w = A.nextw[c];
-          s0 += w * v[c];
-          s1 += v[c] * v[c];
-          s2 += w * w;
-        }
-        s0 = block_sum(s0, sh);
-        s1 = block_sum(s1, sh);
-        s2 = block_sum(s2, sh);
-        if (tid == 0) { exn[0] = s0; exn[1] = s1; exn[2] = s2; exn[3] = s0; }
       }
     }
     if (!grid_sync(A.bar, A.err)) return;
@@ -291,7 +359,7 @@ bbt_status ralha(bbt_ctx* ctx, int m, int n, double* W, double* house, double* t
   A.beta = beta;
   A.V = V;
   A.g = ctx->ws.take<double>(2 * (size_t)m);
-  A.extra = ctx->ws.take<double>(8);
+  A.part = ctx->ws.take<double>(8 * (size_t)std::max(ctx->num_sms, 1));
   A.vt = ctx->ws.take<double>(n);
   A.tv = ctx->ws.take<double>(n);
   A.nextw = ctx->ws.take<double>(n);
