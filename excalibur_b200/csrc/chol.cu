@@ -7,6 +7,7 @@
 #include <algorithm>
 
 #include "internal.h"
+#include "sync.cuh"
 
 namespace bbt {
 namespace {
@@ -412,6 +413,241 @@ __global__ void apply_signs_kernel(int m, const double* __restrict__ d, double* 
   }
 }
 
+// ---- single-launch factorisations for square operands ---------------------
+// Cooperative launches (every CTA resident), phases separated by bounded grid
+// barriers (sync.cuh): a barrier that times out sets the tensor-core wait
+// flag, reported by check_tc_flags, and every CTA leaves.
+
+constexpr int CT = 256;   // threads of the cooperative Cholesky
+
+struct PotrfArgs {
+  int n;
+  double* G;
+  long ld;
+  int* flag;       // not-positive pivot
+  unsigned* bar;   // grid barrier
+  int* err;        // barrier timeout
+};
+
+// Right-looking blocked Cholesky G = R^T R (upper, 32 x 32 tiles), in place:
+// per block row k, (1) every CTA that needs it factors the diagonal tile in
+// shared memory (warp 0, lane c owning column c), CTA 0 stores it, and each
+// CTA solves its tiles of the row panel, R_kj = R_kk^-T G_kj, in shared
+// memory; (2) the trailing tiles G_ij -= R_ki^T R_kj, i <= j, one tile per
+// CTA at a time.  Only the upper triangle of G is read; the
+// strictly lower triangle is zeroed at the end.
+__global__ void __launch_bounds__(CT, 1) potrf_coop_kernel(PotrfArgs P) {
+  __shared__ double D[32][33], A1[32][33], B1[32][33];
+  const int n = P.n, nb = (n + 31) / 32;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = CT / 32;
+  for (int k = 0; k < nb; ++k) {
+    const int r0 = 32 * k, kb = min(32, n - r0);
+    if (blockIdx.x == 0 || k + 1 + (int)blockIdx.x < nb) {
+      for (int f = threadIdx.x; f < 1024; f += CT) {
+        const int i = f % 32, j = f / 32;
+        D[i][j] = (i < kb && j < kb && i <= j) ? P.G[(r0 + i) + (long)(r0 + j) * P.ld] : 0.0;
+      }
+      __syncthreads();
+      if (w == 0) {
+        for (int j = 0; j < kb; ++j) {
+          double d = D[j][j];
+          if (!(d > 0.0) || !isfinite(d)) {
+            if (lane == 0) atomicExch(P.flag, 1);
+            d = 1.0;
+          }
+          const double r = sqrt(d);
+          __syncwarp();
+          if (lane >= j && lane < kb) D[j][lane] = (lane == j) ? r : D[j][lane] / r;
+          __syncwarp();
+          if (lane > j && lane < kb) {
+            const double ajc = D[j][lane];
+            for (int i = j + 1; i <= lane; ++i) D[i][lane] -= D[j][i] * ajc;
+          }
+          __syncwarp();
+        }
+      }
+      __syncthreads();
+      if (blockIdx.x == 0)
+        for (int f = threadIdx.x; f < 1024; f += CT) {
+          const int i = f % 32, j = f / 32;
+          if (i < kb && j < kb && i <= j) P.G[(r0 + i) + (long)(r0 + j) * P.ld] = D[i][j];
+        }
+      for (int j = k + 1 + blockIdx.x; j < nb; j += gridDim.x) {   // R_kj = R_kk^-T G_kj in shared memory
+        const int c0 = 32 * j, jb = min(32, n - c0);
+        for (int f = threadIdx.x; f < 1024; f += CT) {
+          const int i = f % 32, c = f / 32;
+          A1[i][c] = (i < kb && c < jb) ? P.G[(r0 + i) + (long)(c0 + c) * P.ld] : 0.0;
+        }
+        __syncthreads();
+        for (int i = 0; i < kb; ++i) {   // row i final, then rows t > i lose D(i, t) x_i
+          if (threadIdx.x < 32) A1[i][threadIdx.x] /= D[i][i];
+          __syncthreads();
+          for (int f = threadIdx.x; f < (kb - 1 - i) * 32; f += CT) {
+            const int t = i + 1 + f / 32, c = f % 32;
+            A1[t][c] -= D[i][t] * A1[i][c];
+          }
+          __syncthreads();
+        }
+        for (int f = threadIdx.x; f < 1024; f += CT) {
+          const int i = f % 32, c = f / 32;
+          if (i < kb && c < jb) P.G[(r0 + i) + (long)(c0 + c) * P.ld] = A1[i][c];
+        }
+        __syncthreads();
+      }
+    }
+    if (!grid_sync(P.bar, P.err)) return;
+    const int T = nb - k - 1, count = T * (T + 1) / 2;
+    for (int q = blockIdx.x; q < count; q += gridDim.x) {
+      int a = 0, rem = q;   // q -> (a, b), 0 <= a <= b < T, row by row
+      while (rem >= T - a) {
+        rem -= T - a;
+        ++a;
+      }
+      const int bi = k + 1 + a, bj = k + 1 + a + rem;
+      const int i0 = 32 * bi, j0 = 32 * bj, ib = min(32, n - i0), jb = min(32, n - j0);
+      __syncthreads();
+      for (int f = threadIdx.x; f < 1024; f += CT) {
+        const int t = f % 32, c = f / 32;
+        A1[t][c] = (t < kb && c < ib) ? P.G[(r0 + t) + (long)(i0 + c) * P.ld] : 0.0;
+        B1[t][c] = (t < kb && c < jb) ? P.G[(r0 + t) + (long)(j0 + c) * P.ld] : 0.0;
+      }
+      __syncthreads();
+      const int ii = lane;
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int jj = w + nw * e;
+        double acc = 0.0;
+#pragma unroll 8
+        for (int t = 0; t < 32; ++t) acc = fma(A1[t][ii], B1[t][jj], acc);
+        if (ii < ib && jj < jb && (bi < bj || ii <= jj)) P.G[(i0 + ii) + (long)(j0 + jj) * P.ld] -= acc;
+      }
+    }
+    if (!grid_sync(P.bar, P.err)) return;
+  }
+  const long total = (long)n * n;
+  for (long f = blockIdx.x * (long)CT + threadIdx.x; f < total; f += (long)gridDim.x * CT) {
+    const int i = (int)(f % n), j = (int)(f / n);
+    if (i > j) P.G[i + (long)j * P.ld] = 0.0;
+  }
+}
+
+constexpr int LT = 1024;   // threads of the cooperative sign-recovery LU (one row each)
+
+struct LuArgs {
+  int rows, cols;
+  double* A;
+  long lda;
+  double* d;
+  unsigned* bar;
+  int* err;
+};
+
+// The sign-recovery elimination (lu_sign_leaf_reg) on the 16-column panel at
+// p0, rows p0.. in registers, one row per thread.
+__device__ void lu_panel(const LuArgs& P, int p0, double* rowj, double* sf) {
+  const int pb = min(LB, P.cols - p0);
+  const int i = p0 + threadIdx.x;
+  const bool live = i < P.rows;
+  double x[LB];
+#pragma unroll
+  for (int c = 0; c < LB; ++c) x[c] = (live && c < pb) ? P.A[i + (long)(p0 + c) * P.lda] : 0.0;
+#pragma unroll
+  for (int j = 0; j < LB; ++j) {
+    if (j < pb) {
+      if ((int)threadIdx.x == j) {
+#pragma unroll
+        for (int c = 0; c < LB; ++c) rowj[c] = x[c];
+        const double cj = x[j];
+        const double dj = cj < 0.0 ? 1.0 : -1.0;
+        P.d[p0 + j] = dj;
+        *sf = -dj / (1.0 + fabs(cj));
+      }
+      __syncthreads();
+      if ((int)threadIdx.x > j && live) {
+        const double l = *sf * x[j];
+        x[j] = l;
+#pragma unroll
+        for (int c = j + 1; c < LB; ++c) x[c] -= l * rowj[c];
+      }
+      __syncthreads();
+    }
+  }
+  if (live)
+#pragma unroll
+    for (int c = 0; c < LB; ++c)
+      if (c < pb) P.A[i + (long)(p0 + c) * P.lda] = x[c];
+}
+
+// Right-looking blocked elimination with 16-column panels: per panel, every
+// CTA takes 16-column chunks of the trailing columns, solves their panel rows
+// U12 = L11^-1 A12 and updates A22 -= L21 U12 (one row per thread); CTA 0
+// owns the chunk of the next panel and factors it right after updating it,
+// so one grid barrier per panel suffices.
+__global__ void __launch_bounds__(LT, 1) lu_sign_coop_kernel(LuArgs P) {
+  __shared__ double rowj[LB];
+  __shared__ double sf;
+  __shared__ double L11[LB][LB + 1];
+  __shared__ double U[LB][LB + 1];
+  const int np = (P.cols + LB - 1) / LB;
+  if (blockIdx.x == 0) lu_panel(P, 0, rowj, &sf);
+  if (!grid_sync(P.bar, P.err)) return;
+  for (int k = 0; k < np; ++k) {
+    const int p0 = k * LB, pb = min(LB, P.cols - p0);
+    const int nch = np - k - 1;   // trailing chunks
+    if (nch > 0 && (int)blockIdx.x < nch) {
+      for (int f = threadIdx.x; f < LB * LB; f += LT) {   // unit lower L11 of the panel
+        const int r = f % LB, c = f / LB;
+        L11[r][c] = (r > c && r < pb && c < pb) ? P.A[(p0 + r) + (long)(p0 + c) * P.lda] : 0.0;
+      }
+      // this thread's row of L21 (rows below the panel)
+      const int i = p0 + pb + threadIdx.x;
+      const bool live = i < P.rows;
+      double l[LB];
+#pragma unroll
+      for (int t = 0; t < LB; ++t) l[t] = (live && t < pb) ? P.A[i + (long)(p0 + t) * P.lda] : 0.0;
+      for (int q = blockIdx.x; q < nch; q += gridDim.x) {
+        const int c0 = p0 + LB * (q + 1), cw = min(LB, P.cols - c0);
+        __syncthreads();
+        for (int f = threadIdx.x; f < LB * LB; f += LT) {   // the panel rows of the chunk
+          const int r = f % LB, c = f / LB;
+          U[r][c] = (c < cw && r < pb) ? P.A[(p0 + r) + (long)(c0 + c) * P.lda] : 0.0;
+        }
+        __syncthreads();
+        if (threadIdx.x < LB) {   // U12 column c = L11^-1 A12 column c (unit lower, forward)
+          const int c = threadIdx.x;
+          for (int r = 1; r < pb; ++r) {
+            double acc = U[r][c];
+            for (int t = 0; t < r; ++t) acc -= L11[r][t] * U[t][c];
+            U[r][c] = acc;
+          }
+          if (c < cw)
+            for (int r = 0; r < pb; ++r) P.A[(p0 + r) + (long)(c0 + c) * P.lda] = U[r][c];
+        }
+        __syncthreads();
+        if (live)
+#pragma unroll 4
+          for (int c = 0; c < cw; ++c) {
+            double s = 0.0;
+#pragma unroll
+            for (int t = 0; t < LB; ++t) s = fma(l[t], U[t][c], s);
+            P.A[i + (long)(c0 + c) * P.lda] -= s;
+          }
+      }
+      __syncthreads();
+    }
+    if (blockIdx.x == 0 && k + 1 < np) lu_panel(P, p0 + LB, rowj, &sf);   // CTA 0 updated that chunk (q = 0)
+    if (!grid_sync(P.bar, P.err)) return;
+  }
+}
+
+// Co-resident CTAs of a cooperative kernel: at most one per SM, at most `want`.
+template <class K>
+int coop_grid(bbt_ctx* ctx, K kernel, int threads, int want) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0) != cudaSuccess || per_sm < 1) return 0;
+  return std::max(1, std::min(want, ctx->num_sms));
+}
+
 int split_point(int n) { return (n / 2 + TB - 1) / TB * TB; }
 
 bbt_status trsm_left_lower_unit(bbt_ctx* ctx, int n, long ncols, const double* L, long ldl, double* B, long ldb) {
@@ -437,6 +673,19 @@ bbt_status trsm_left_lower_unit(bbt_ctx* ctx, int n, long ncols, const double* L
 
 bbt_status householder_signs(bbt_ctx* ctx, int rows, int cols, double* A, long lda, double* d) {
   if (cols <= 0) return BBT_OK;
+  if (ctx->allow_coop && cols > LB && rows >= cols && rows <= LT) {   // one cooperative launch
+    const int grid = coop_grid(ctx, lu_sign_coop_kernel, LT, (cols + LB - 1) / LB - 1);
+    if (grid > 0) {
+      ProfScope prof(ctx, BBT_PROF_CHOL, (double)rows * cols * cols);
+      LuArgs P{rows, cols, A, lda, d, ctx->d_barrier, ctx->d_flag + FLAG_SKETCH};
+      BBT_CUDA(ctx, cudaMemsetAsync(ctx->d_barrier, 0, 2 * sizeof(unsigned), ctx->stream));
+      void* args[] = {&P};
+      BBT_CUDA(ctx, cudaLaunchCooperativeKernel((void*)lu_sign_coop_kernel, dim3(grid), dim3(LT), args, 0,
+                                                ctx->stream));
+      BBT_LAUNCHED(ctx);
+      return BBT_OK;
+    }
+  }
   if (cols <= LB) {
     ProfScope prof(ctx, BBT_PROF_CHOL, (double)rows * cols * cols);
     if (rows <= 1024)
@@ -491,6 +740,20 @@ bbt_status trsm_right_upper(bbt_ctx* ctx, long rows, int n, const double* R, lon
 
 bbt_status potrf_upper(bbt_ctx* ctx, int n, double* G, long ld, int* flag) {
   if (n <= 0) return BBT_OK;
+  if (ctx->allow_coop && n > PB && n <= 4096) {   // one cooperative launch
+    const int nb = (n + 31) / 32;
+    const int grid = coop_grid(ctx, potrf_coop_kernel, CT, nb * (nb - 1) / 2);
+    if (grid > 0) {
+      ProfScope prof(ctx, BBT_PROF_CHOL, (double)n * n * n / 3.0);
+      PotrfArgs P{n, G, ld, flag, ctx->d_barrier, ctx->d_flag + FLAG_SKETCH};
+      BBT_CUDA(ctx, cudaMemsetAsync(ctx->d_barrier, 0, 2 * sizeof(unsigned), ctx->stream));
+      void* args[] = {&P};
+      BBT_CUDA(ctx, cudaLaunchCooperativeKernel((void*)potrf_coop_kernel, dim3(grid), dim3(CT), args, 0,
+                                                ctx->stream));
+      BBT_LAUNCHED(ctx);
+      return BBT_OK;
+    }
+  }
   if (n <= PB) {
     ProfScope prof(ctx, BBT_PROF_CHOL, (double)n * n * n / 3.0);
     potrf_leaf<<<1, 32, 0, ctx->stream>>>(n, G, ld, flag);

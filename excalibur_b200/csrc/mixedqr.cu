@@ -41,7 +41,7 @@ bbt_status check_tc_flags(bbt_ctx* ctx, const char* what) {
   int h[2] = {0, 0};
   BBT_CUDA(ctx, cudaMemcpyAsync(h, ctx->d_flag + FLAG_SKETCH, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
   BBT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  if (h[0]) return fail(ctx, BBT_ERR_TIMEOUT, "%s: a tensor-core pipeline wait gave up (code %d)", what, h[0]);
+  if (h[0]) return fail(ctx, BBT_ERR_TIMEOUT, "%s: a device wait gave up (code %d)", what, h[0]);
   if (h[1]) return fail(ctx, BBT_ERR_NUMERIC, "%s: Cholesky pivot not positive (rank-deficient block?)", what);
   return BBT_OK;
 }
