@@ -339,6 +339,11 @@ struct CrtArgs {
   int* err;
 };
 
+// AMN: A's residue planes are MN-major (the row index i of A contiguous, K
+// along the planes' rows), as the Gram's planes of X serve the products
+// X_int^T Z: the TMA box and the K advance change, and the instruction
+// descriptor marks A as MN-major (valid for 8-bit integer operands).
+template <bool AMN>
 __global__ void __launch_bounds__(THREADS, 1)
 crt_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, CrtArgs P) {
   const int n0 = blockIdx.x * TN, m0 = blockIdx.y * TM;
@@ -388,7 +393,10 @@ crt_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUte
         mbar_expect_tx(fb, (uint32_t)STAGE_BYTES);
         const uint32_t st = smem_u32(smem + (size_t)s * STAGE_BYTES);
         const int kx = (kb0 + kb) * TK;
-        tma_load_3d(st, &tmA, fb, kx, m0, q);
+        if (AMN)
+          tma_load_3d(st, &tmA, fb, m0, kx, q);
+        else
+          tma_load_3d(st, &tmA, fb, kx, m0, q);
         tma_load_3d(st + A_TILE, &tmB, fb, kx, n0, q);
         ++issued;
       }
@@ -398,8 +406,9 @@ crt_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUte
     }
   } else if (warp == EPI_WARPS + 1) {
     if (lane == 0) {   // ---- MMA issuer: u8 x u8 -> int32, K-major, 128 x 256 x 32 per instruction
-      const uint32_t idesc =   // c_format S32, a/b unsigned 8-bit
-          (2u << 4) | (0u << 7) | (0u << 10) | ((uint32_t)(TN >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
+      const uint32_t idesc =   // c_format S32, a/b unsigned 8-bit, A K-major or MN-major (bit 15)
+          (2u << 4) | (0u << 7) | (0u << 10) | ((AMN ? 1u : 0u) << 15) | ((uint32_t)(TN >> 3) << 17) |
+          ((uint32_t)(TM >> 4) << 24);
       bool ok = true;
       for (int q = 0; q < P.n && ok; ++q) {
         const int buf = q & 1, use = q >> 1;
@@ -413,9 +422,11 @@ crt_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUte
           tc_fence_after();
           const uint32_t st = smem_u32(smem + (size_t)s * STAGE_BYTES);
           const uint64_t ad = sw128_desc(st), bd = sw128_desc(st + A_TILE);
+          // +32 along K: +32 bytes (K-major, +2 in the descriptor's address field) or
+          // +32 rows of 128 bytes (MN-major, +256)
 #pragma unroll
-          for (int kk = 0; kk < TK / 32; ++kk)   // +32 bytes along K = +2 in the descriptor's address field
-            mma_i8(d, ad + 2 * kk, bd + 2 * kk, idesc, (kb != 0 || kk != 0) ? 1u : 0u);
+          for (int kk = 0; kk < TK / 32; ++kk)
+            mma_i8(d, ad + (AMN ? 256 : 2) * kk, bd + 2 * kk, idesc, (kb != 0 || kk != 0) ? 1u : 0u);
           mma_commit(empty0 + 8 * s);
         }
         mma_commit(accf0 + 8 * buf);
@@ -485,40 +496,43 @@ __device__ __forceinline__ uint32_t mod_c(uint32_t x) {
 // LIMBS = 4: the fraction to 128 bits (double-double outputs); 3: to 96 bits
 // (FP64 outputs: the missing 32 bits are below 2^-75 of the largest |T|), the
 // limbs of floor(2^96 / p) being the top three of floor(2^128 / p).
-template <int Q, int NM, int LIMBS>
+// SPLIT: the product came in several K-splits, whose residues are summed
+// first; with one split every byte is already a residue in [0, p).
+template <int Q, int NM, int LIMBS, bool SPLIT>
 __device__ __forceinline__ void frac4_q(const CombArgs& A, long f, long total, uint64_t (&L)[4][4]) {
   using C = ModK<Q, NM>;
   uint32_t s[4];
   const uint32_t w = *reinterpret_cast<const uint32_t*>(A.R + (size_t)Q * total + f);
 #pragma unroll
   for (int e = 0; e < 4; ++e) s[e] = (w >> (8 * e)) & 0xFFu;
-  for (int z = 1; z < A.splits; ++z) {
-    const uint32_t v = *reinterpret_cast<const uint32_t*>(A.R + ((size_t)z * NM + Q) * total + f);
+  if (SPLIT)
+    for (int z = 1; z < A.splits; ++z) {
+      const uint32_t v = *reinterpret_cast<const uint32_t*>(A.R + ((size_t)z * NM + Q) * total + f);
 #pragma unroll
-    for (int e = 0; e < 4; ++e) s[e] += (v >> (8 * e)) & 0xFFu;
-  }
+      for (int e = 0; e < 4; ++e) s[e] += (v >> (8 * e)) & 0xFFu;
+    }
 #pragma unroll
   for (int e = 0; e < 4; ++e) {
-    const uint32_t y = mod_c<C>(mod_c<C>(s[e]) * C::inv);
+    const uint32_t y = mod_c<C>((SPLIT ? mod_c<C>(s[e]) : s[e]) * C::inv);
     if (LIMBS == 4) L[e][0] += (uint64_t)y * C::F0;   // 32 x 32 -> 64-bit products, < 2^40 each
     L[e][1] += (uint64_t)y * C::F1;
     L[e][2] += (uint64_t)y * C::F2;
     L[e][3] += (uint64_t)y * C::F3;
   }
 }
-template <int NM, int LIMBS, int... Q>
+template <int NM, int LIMBS, bool SPLIT, int... Q>
 __device__ __forceinline__ void frac4_all(const CombArgs& A, long f, long total, uint64_t (&L)[4][4],
                                           std::integer_sequence<int, Q...>) {
-  (frac4_q<Q, NM, LIMBS>(A, f, total, L), ...);
+  (frac4_q<Q, NM, LIMBS, SPLIT>(A, f, total, L), ...);
 }
 
 // The centred fractions T / M (mod 1) of four consecutive outputs as signed
 // 128-bit fixed-point numbers (two 64-bit halves each).
-template <int NM, int LIMBS>
+template <int NM, int LIMBS, bool SPLIT = true>
 __device__ __forceinline__ void crt_fraction4(const CombArgs& A, long f, long total, uint64_t (&hi)[4],
                                               uint64_t (&lo)[4]) {
   uint64_t L[4][4] = {};
-  frac4_all<NM, LIMBS>(A, f, total, L, std::make_integer_sequence<int, NM>{});
+  frac4_all<NM, LIMBS, SPLIT>(A, f, total, L, std::make_integer_sequence<int, NM>{});
 #pragma unroll
   for (int e = 0; e < 4; ++e) {
     L[e][1] += L[e][0] >> 32;
@@ -564,27 +578,53 @@ __device__ __forceinline__ void two_prod(double a, double b, double& p, double& 
   e = fma(a, b, -p);
 }
 
+// A signed 128-bit fraction (two's complement, hi:lo) as the nearest-ish
+// double times 2^128: magnitude first (no cancellation between the halves),
+// then hi 2^64 + lo converted in two roundings (within 2 ulps).
+__device__ __forceinline__ double fixed_to_double(uint64_t hi, uint64_t lo) {
+  const bool neg = (int64_t)hi < 0;
+  if (neg) {
+    lo = ~lo + 1;
+    hi = ~hi + (lo == 0 ? 1 : 0);
+  }
+  const double v = fma((double)hi, 18446744073709551616.0, (double)lo);   // 2^64
+  return neg ? -v : v;
+}
+
 // C (column-major, ldc) = alpha * sa_i sb_j 2^-shift T + beta * C; four
-// consecutive i per thread.
-template <int NM>
-__global__ void __launch_bounds__(256, 3)
-combine_kernel(CombArgs A, const double* __restrict__ sa, const double* __restrict__ sb, int shift, double alpha,
+// consecutive i per thread.  scale = M 2^(-128 - shift) (M the moduli's
+// product): the fraction T / M (mod 1) times M, back at the operands' scale.
+template <int NM, bool SPLIT>
+__global__ void __launch_bounds__(256, 4)
+combine_kernel(CombArgs A, const double* __restrict__ sa, const double* __restrict__ sb, double scale, double alpha,
                double beta, double* __restrict__ C, long ldc) {
   const long total = (long)A.Mp * A.N;
   for (int j = blockIdx.y; j < A.N; j += gridDim.y)
   for (int i = (blockIdx.x * blockDim.x + threadIdx.x) * 4; i < A.M; i += gridDim.x * blockDim.x * 4) {
     if (A.upper && (i / TM) * TM >= (j / TN) * TN + TN) continue;   // tile never computed
     uint64_t hi[4], lo[4];
-    crt_fraction4<NM, 3>(A, i + (long)j * A.Mp, total, hi, lo);
-    const double sbj = sb[j];
+    crt_fraction4<NM, 3, SPLIT>(A, i + (long)j * A.Mp, total, hi, lo);
+    const double sbj = sb[j] * scale;
+    double v[4];
 #pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      if (i + e >= A.M) break;
-      double dh, dl;
-      fixed_to_dd(hi[e], lo[e], dh, dl);
-      const double v = ldexp((dh + dl) * A.mod_hi, -128 - shift) * (sa ? sa[i + e] : 1.0) * sbj;
-      double* c = C + (i + e) + (long)j * ldc;
-      *c = (beta == 0.0) ? alpha * v : alpha * v + beta * (*c);
+    for (int e = 0; e < 4; ++e) v[e] = fixed_to_double(hi[e], lo[e]) * (sa ? sa[min(i + e, A.M - 1)] : 1.0) * sbj;
+    double* c = C + i + (long)j * ldc;
+    if (i + 4 <= A.M && ((reinterpret_cast<uintptr_t>(c) & 15) == 0)) {   // two 16-byte stores
+      double2* c2 = reinterpret_cast<double2*>(c);
+      if (beta == 0.0) {
+        c2[0] = make_double2(alpha * v[0], alpha * v[1]);
+        c2[1] = make_double2(alpha * v[2], alpha * v[3]);
+      } else {
+        const double2 o0 = c2[0], o1 = c2[1];
+        c2[0] = make_double2(alpha * v[0] + beta * o0.x, alpha * v[1] + beta * o0.y);
+        c2[1] = make_double2(alpha * v[2] + beta * o1.x, alpha * v[3] + beta * o1.y);
+      }
+    } else {
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        if (i + e >= A.M) break;
+        c[e] = (beta == 0.0) ? alpha * v[e] : alpha * v[e] + beta * c[e];
+      }
     }
   }
 }
@@ -808,10 +848,14 @@ size_t crt_product_bytes(const bbt_ctx* ctx, int M, int N, long K, int n, bool u
   return (size_t)pl.splits * n * (size_t)((M + 3) & ~3) * N + 4096;
 }
 
-bbt_status crt_product(bbt_ctx* ctx, int M, int N, long K, int n, const int8_t* RA, const int8_t* RB, long Kp,
-                       bool upper, uint8_t* R, int* splits_out) {
+namespace {
+// A: K-major planes [n][M][Kp] (lda = 0) or MN-major planes [n][K][lda] (A(i, k) at k lda + i).
+bbt_status crt_launch(bbt_ctx* ctx, int M, int N, long K, int n, const int8_t* RA, long lda, const int8_t* RB,
+                      long Kp, bool upper, uint8_t* R, int* splits_out) {
   if (n < 1 || n > MAXMOD) return fail(ctx, BBT_ERR_ARG, "crt: %d moduli", n);
   if (M < 1 || N < 1 || K < 1) return fail(ctx, BBT_ERR_ARG, "crt: M=%d N=%d K=%ld", M, N, K);
+  const bool amn = lda > 0;
+  if (amn && (lda < M || lda % 16 != 0 || upper)) return fail(ctx, BBT_ERR_ARG, "crt: MN-major A, pitch %ld", lda);
   const unsigned gy = (unsigned)((M + TM - 1) / TM);
   if (gy > 65535) return fail(ctx, BBT_ERR_ARG, "crt: M=%d too large", M);
   EncodeTiled enc = encode_fn();
@@ -819,9 +863,18 @@ bbt_status crt_product(bbt_ctx* ctx, int M, int N, long K, int n, const int8_t* 
   const Plan pl = plan(M, N, K, ctx->num_sms, upper);
   CUtensorMap ta, tb;
   {
-    const cuuint64_t dims[3] = {(cuuint64_t)K, (cuuint64_t)M, (cuuint64_t)n};
-    const cuuint64_t strides[2] = {(cuuint64_t)Kp, (cuuint64_t)Kp * M};
-    const cuuint32_t box[3] = {TK, TM, 1}, es[3] = {1, 1, 1};
+    cuuint64_t dims[3] = {(cuuint64_t)K, (cuuint64_t)M, (cuuint64_t)n};
+    cuuint64_t strides[2] = {(cuuint64_t)Kp, (cuuint64_t)Kp * M};
+    cuuint32_t box[3] = {TK, TM, 1};
+    if (amn) {   // i contiguous (TM bytes of it per box row), TK rows of K
+      dims[0] = (cuuint64_t)M;
+      dims[1] = (cuuint64_t)K;
+      strides[0] = (cuuint64_t)lda;
+      strides[1] = (cuuint64_t)lda * K;
+      box[0] = TM;
+      box[1] = TK;
+    }
+    const cuuint32_t es[3] = {1, 1, 1};
     if (enc(&ta, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<int8_t*>(RA), dims, strides, box, es,
             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
@@ -836,10 +889,11 @@ bbt_status crt_product(bbt_ctx* ctx, int M, int N, long K, int n, const int8_t* 
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
       return fail(ctx, BBT_ERR_CUDA, "crt: tensor map of B");
   }
-  static bool attr = false;
-  if (!attr) {
-    BBT_CUDA(ctx, cudaFuncSetAttribute(crt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
-    attr = true;
+  static bool attr[2] = {false, false};
+  if (!attr[amn]) {
+    BBT_CUDA(ctx, cudaFuncSetAttribute(amn ? crt_kernel<true> : crt_kernel<false>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+    attr[amn] = true;
   }
   const Mods md = make_mods(n);
   CrtArgs a;
@@ -859,10 +913,25 @@ bbt_status crt_product(bbt_ctx* ctx, int M, int N, long K, int n, const int8_t* 
   }
   a.err = ctx->d_flag + FLAG_SKETCH;
   ProfScope prof(ctx, BBT_PROF_CRT, (upper ? 1.0 : 2.0) * n * (double)M * N * K);   // int8 operations
-  crt_kernel<<<dim3((N + TN - 1) / TN, gy, pl.splits), THREADS, SMEM_BYTES, ctx->stream>>>(ta, tb, a);
+  const dim3 grid((N + TN - 1) / TN, gy, pl.splits);
+  if (amn)
+    crt_kernel<true><<<grid, THREADS, SMEM_BYTES, ctx->stream>>>(ta, tb, a);
+  else
+    crt_kernel<false><<<grid, THREADS, SMEM_BYTES, ctx->stream>>>(ta, tb, a);
   BBT_LAUNCHED(ctx);
   *splits_out = pl.splits;
   return BBT_OK;
+}
+}  // namespace
+
+bbt_status crt_product(bbt_ctx* ctx, int M, int N, long K, int n, const int8_t* RA, const int8_t* RB, long Kp,
+                       bool upper, uint8_t* R, int* splits_out) {
+  return crt_launch(ctx, M, N, K, n, RA, 0, RB, Kp, upper, R, splits_out);
+}
+
+bbt_status crt_product_amn(bbt_ctx* ctx, int M, int N, long K, int n, const int8_t* RA, long lda, const int8_t* RB,
+                           long Kp, uint8_t* R, int* splits_out) {
+  return crt_launch(ctx, M, N, K, n, RA, lda, RB, Kp, false, R, splits_out);
 }
 
 namespace {
@@ -885,11 +954,16 @@ bbt_status crt_combine(bbt_ctx* ctx, int M, int N, int n, int splits, const uint
                        const double* sb, int shift, double alpha, double beta, double* C, long ldc) {
   const dim3 g((unsigned)std::min((M + 1023) / 1024, 1024), (unsigned)std::min(N, 65535));   // 4 outputs a thread
   const CombArgs A = comb_args(R, M, N, n, splits, upper);
+  // M 2^(-128 - shift): a power of two times the moduli's product, normal for every shift used
+  const double scale = std::ldexp(A.mod_hi, -128 - shift);
   ProfScope prof(ctx, BBT_PROF_CRT_COMBINE, ((double)n * splits + 8.0) * (double)M * N);
   switch (n) {
 #define CASE(NM)                                                                                   \
   case NM:                                                                                         \
-    combine_kernel<NM><<<g, 256, 0, ctx->stream>>>(A, sa, sb, shift, alpha, beta, C, ldc);          \
+    if (splits > 1)                                                                                \
+      combine_kernel<NM, true><<<g, 256, 0, ctx->stream>>>(A, sa, sb, scale, alpha, beta, C, ldc);  \
+    else                                                                                           \
+      combine_kernel<NM, false><<<g, 256, 0, ctx->stream>>>(A, sa, sb, scale, alpha, beta, C, ldc); \
     break;
     CRT_NM_CASES(CASE)
 #undef CASE

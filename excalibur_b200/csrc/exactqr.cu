@@ -62,8 +62,18 @@ size_t exact_qr_workspace_bytes(const bbt_ctx* ctx, int m, long n) {
   return s + ((size_t)N * m + 6 * (size_t)m * m + 2 * m) * 8 + 16384;
 }
 
+int exact_keep_moduli(int m, long n) {
+  const int a = crt_moduli(GRAM_BITS, GRAM_BITS, n), b = crt_moduli(GRAM_BITS, Z_BITS, m);
+  return (a < 1 || b < 1) ? -1 : std::max(a, b);
+}
+
+size_t exact_keep_bytes(int m, long n) {
+  const int nk = exact_keep_moduli(m, n);
+  return nk < 1 ? 0 : (size_t)nk * m * crt_pitch(n) + 256;
+}
+
 bbt_status exact_local_qr(bbt_ctx* ctx, int m, long n, const double* X, const void* S, long spitch, double* R,
-                          double* W, double* Rp, double* scale) {
+                          double* W, double* Rp, double* scale, int8_t* keep) {
   if (n < m) return fail(ctx, BBT_ERR_ARG, "exact local QR: n=%ld < m=%d", n, m);
   const int nm = crt_moduli(GRAM_BITS, GRAM_BITS, n);
   if (nm < 1) return fail(ctx, BBT_ERR_ARG, "exact local QR: n=%ld too long", n);
@@ -87,13 +97,15 @@ bbt_status exact_local_qr(bbt_ctx* ctx, int m, long n, const double* X, const vo
   {
     const size_t m2 = ctx->ws.top;
     const long Kp = crt_pitch(n);
-    int8_t* RX = ctx->ws.take<int8_t>((size_t)nm * m * Kp);
+    // kept: every plane the later products with X_int^T need, the Gram using the first nm
+    const int nr = keep ? exact_keep_moduli(m, n) : nm;
+    int8_t* RX = keep ? keep : ctx->ws.take<int8_t>((size_t)nm * m * Kp);
     const size_t m3 = ctx->ws.top;
     BBT_TRY(crt_row_scales(ctx, m, n, X, n, scale));
     ctx->ws.top = m3;
     uint8_t* Rb = ctx->ws.take<uint8_t>(crt_product_bytes(ctx, m, m, n, nm, true));
-    if (!Rb) return fail(ctx, BBT_ERR_NOMEM, "exact local QR: Gram workspace");
-    BBT_TRY(crt_residues_rows(ctx, m, n, X, n, scale, GRAM_BITS, nm, RX, Kp));
+    if (!Rb || !RX) return fail(ctx, BBT_ERR_NOMEM, "exact local QR: Gram workspace");
+    BBT_TRY(crt_residues_rows(ctx, m, n, X, n, scale, GRAM_BITS, nr, RX, Kp));
     int splits = 1;
     BBT_TRY(crt_product(ctx, m, m, n, nm, RX, RX, Kp, true, Rb, &splits));
     BBT_TRY(crt_combine_dd(ctx, m, m, nm, splits, Rb, true, scale, scale, 2 * (GRAM_BITS - 1), Gh, Gl, m));
@@ -180,6 +192,24 @@ bbt_status exact_apply_rows(bbt_ctx* ctx, const ExactOperand& op, long rows, con
   BBT_TRY(crt_residues_cols(ctx, (int)rows, m, X, ldx, scale, GRAM_BITS, nm, RA, op.Kp));
   int splits = 1;
   BBT_TRY(crt_product(ctx, (int)rows, k, m, nm, RA, op.RB, op.Kp, false, Rb, &splits));
+  BBT_TRY(crt_combine(ctx, (int)rows, k, nm, splits, Rb, false, nullptr, op.t, (GRAM_BITS - 1) + (Z_BITS - 1), 1.0,
+                      0.0, C, ldc));
+  ctx->ws.top = mark;
+  return BBT_OK;
+}
+
+// The same from the planes exact_local_qr kept (A_int(j, i) = X_int(i, j),
+// planes [q][m][pitch], pitch = crt_pitch(rows)): X_int^T as an MN-major
+// operand, so the block is not read again.
+bbt_status exact_apply_planes(bbt_ctx* ctx, const ExactOperand& op, long rows, const int8_t* planes, long pitch,
+                              double* C, long ldc) {
+  if (rows > 0x7fffffffL) return fail(ctx, BBT_ERR_ARG, "exact apply: rows=%ld", rows);
+  const int m = op.m, k = op.k, nm = op.nm;
+  const size_t mark = ctx->ws.top;
+  uint8_t* Rb = ctx->ws.take<uint8_t>(crt_product_bytes(ctx, (int)rows, k, m, nm, false));
+  if (!Rb) return fail(ctx, BBT_ERR_NOMEM, "exact apply: workspace");
+  int splits = 1;
+  BBT_TRY(crt_product_amn(ctx, (int)rows, k, m, nm, planes, pitch, op.RB, op.Kp, Rb, &splits));
   BBT_TRY(crt_combine(ctx, (int)rows, k, nm, splits, Rb, false, nullptr, op.t, (GRAM_BITS - 1) + (Z_BITS - 1), 1.0,
                       0.0, C, ldc));
   ctx->ws.top = mark;

@@ -233,6 +233,7 @@ struct QrJob {
   long spitch = 0;
   std::vector<double*> RT, tau, T, W;
   std::vector<double*> Rp, scale;   // precision 2: the preconditioner and X's row scales
+  std::vector<int8_t*> planes;      // precision 2: X_int's residue planes kept for the V back-transform (or null)
   bool compute_v = false;
 };
 
@@ -271,7 +272,8 @@ bbt_status qr_one(bbt_ctx* c, int mi, double* X, long n, int p, const QrJob& job
   if (job.precision == 1)   // R (column-major) is R^T row-major: the same bytes as r_transpose's output
     return mixed_local_qr(c, mi, n, X, job.S, job.spitch, job.RT[p], job.compute_v ? job.W[p] : nullptr);
   if (job.precision == 2)   // X kept: Q = X_int^T Rp^-1 W is applied by exact products
-    return exact_local_qr(c, mi, n, X, job.S, job.spitch, job.RT[p], job.W[p], job.Rp[p], job.scale[p]);
+    return exact_local_qr(c, mi, n, X, job.S, job.spitch, job.RT[p], job.W[p], job.Rp[p], job.scale[p],
+                          job.planes.empty() ? nullptr : job.planes[p]);
   BBT_TRY(geqrf(c, n, mi, X, n, job.tau[p], job.T[p], qp));
   BBT_TRY(r_transpose(c, mi, X, n, job.RT[p]));
   if (job.compute_v) BBT_TRY(orgqr(c, n, mi, X, n, job.tau[p], job.T[p], qp));   // X_c <- Q (= local_v)
@@ -673,7 +675,18 @@ bbt_status fedsvd(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* X, 
   }
   const size_t need =
       persistent_bytes(L) + std::max(scratch_bytes(ctx, L), batched_scratch(ctx, L, streams, qp) + (64u << 20));
-  if (ctx->ws.cap < need) BBT_CUDA(ctx, ctx->ws.reserve(need));
+  // precision 2: X_int's residue planes serve the Gram and, kept, the V back-transform
+  // (no second pass over the blocks), where the device has room for them
+  size_t keep = 0;
+  if (L.precision == 2 && cfg->svd_mode != 2) {
+    for (int c = 0; c < P; ++c)
+      if (L.qr[c]) keep += exact_keep_bytes(mi, (long)L.n[c]);
+    size_t free_b = 0, total_b = 0;   // a larger arena replaces the current one: its bytes come back
+    if (ctx->ws.cap < need + keep &&
+        (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess || need + keep + ((size_t)4 << 30) > free_b + ctx->ws.cap))
+      keep = 0;
+  }
+  if (ctx->ws.cap < need + keep) BBT_CUDA(ctx, ctx->ws.reserve(need + keep));
   ctx->ws.reset();
   const size_t tq = ((m + qp.nb - 1) / qp.nb) * qp.nb * qp.nb;
   std::vector<double*> RT(P), tauc(P), Tc(P);
@@ -724,6 +737,14 @@ bbt_status fedsvd(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* X, 
     Rpg = ctx->ws.take<double>(m * m);
     scg = ctx->ws.take<double>(m);
     if (!scg) return fail(ctx, BBT_ERR_NOMEM, "fedsvd: workspace (exact Gram)");
+    if (keep) {
+      job.planes.assign(P, nullptr);
+      for (int c = 0; c < P; ++c)
+        if (L.qr[c]) {
+          job.planes[c] = ctx->ws.take<int8_t>(exact_keep_bytes(mi, (long)L.n[c]));
+          if (!job.planes[c]) return fail(ctx, BBT_ERR_NOMEM, "fedsvd: workspace (residue planes)");
+        }
+    }
   }
 
   cudaEvent_t ev[7];
@@ -845,7 +866,13 @@ bbt_status fedsvd(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* X, 
     if (L.qr[c] && L.precision == 2) {   // Q_c = X_int^T Rp_c^-1 W_c: FinalVT^T = X_int^T Rp_c^-1 (W_c tmp^T)
       BBT_TRY(dgemm(ctx, false, false, mi, k, m, 1.0, job.W[c], (long)m, tmp, rc, 0.0, Z, (long)m));
       const size_t mark = ctx->ws.top;
-      BBT_TRY(exact_apply_q(ctx, mi, n, X[c], n, job.scale[c], job.Rp[c], Z, k, VT[c], n));
+      if (!job.planes.empty() && job.planes[c]) {   // from the planes the local QR kept
+        ExactOperand op;
+        BBT_TRY(exact_operand(ctx, mi, job.scale[c], job.Rp[c], Z, k, op));
+        BBT_TRY(exact_apply_planes(ctx, op, n, job.planes[c], crt_pitch(n), VT[c], n));
+      } else {
+        BBT_TRY(exact_apply_q(ctx, mi, n, X[c], n, job.scale[c], job.Rp[c], Z, k, VT[c], n));
+      }
       ctx->ws.top = mark;
     } else if (L.qr[c] && L.precision == 1) {   // Q_c = Q_p W_c: FinalVT^T = Q_p (W_c tmp^T)
       BBT_TRY(dgemm(ctx, false, false, mi, k, m, 1.0, job.W[c], (long)m, tmp, rc, 0.0, Z, (long)m));

@@ -282,6 +282,10 @@ bbt_status crt_residues_dd(bbt_ctx* ctx, int rows, long K, const double* Xh, con
 size_t crt_product_bytes(const bbt_ctx* ctx, int M, int N, long K, int n, bool upper);
 bbt_status crt_product(bbt_ctx* ctx, int M, int N, long K, int n, const int8_t* RA, const int8_t* RB, long Kp,
                        bool upper, uint8_t* R, int* splits);
+// The same with A's planes MN-major: A(i, k) at RA[q][k lda + i] (lda >= M,
+// a multiple of 16), e.g. the Gram's planes of X for products with X^T.
+bbt_status crt_product_amn(bbt_ctx* ctx, int M, int N, long K, int n, const int8_t* RA, long lda, const int8_t* RB,
+                           long Kp, uint8_t* R, int* splits_out);
 bbt_status crt_combine(bbt_ctx* ctx, int M, int N, int n, int splits, const uint8_t* R, bool upper, const double* sa,
                        const double* sb, int shift, double alpha, double beta, double* C, long ldc);
 bbt_status crt_combine_dd(bbt_ctx* ctx, int M, int N, int n, int splits, const uint8_t* R, bool upper,
@@ -305,8 +309,13 @@ bbt_status dd_symmetrize_upper(bbt_ctx* ctx, int m, double* Gh, double* Gl, long
 // kept), R (m x m column-major, dgeqrf's row signs), W = R_3^-1 D, the
 // preconditioner Rp and the row scales of X's 53-bit integers; Q = A_int Rp^-1 W.
 size_t exact_qr_workspace_bytes(const bbt_ctx* ctx, int m, long n);
+// The residue planes of X_int that serve both the Gram and the later products
+// with X_int^T (exact_apply_planes): their count and bytes for an m x n block.
+int exact_keep_moduli(int m, long n);
+size_t exact_keep_bytes(int m, long n);
 bbt_status exact_local_qr(bbt_ctx* ctx, int m, long n, const double* X, const void* S, long spitch, double* R,
-                          double* W, double* Rp, double* scale);
+                          double* W, double* Rp, double* scale,
+                          int8_t* keep = nullptr);
 // C (rows x k column-major) = A_int Rp^-1 Z for A_int(j, i) the integers of X[i ldx + j];
 // the Z side can be prepared once (exact_operand, taken from the workspace)
 // and applied to several row blocks of A_int (exact_apply_rows).
@@ -321,6 +330,8 @@ bbt_status exact_operand(bbt_ctx* ctx, int m, const double* scale, const double*
                          ExactOperand& op);
 bbt_status exact_apply_rows(bbt_ctx* ctx, const ExactOperand& op, long rows, const double* X, long ldx,
                             const double* scale, double* C, long ldc);
+bbt_status exact_apply_planes(bbt_ctx* ctx, const ExactOperand& op, long rows, const int8_t* planes, long pitch,
+                              double* C, long ldc);
 size_t exact_apply_workspace_bytes(const bbt_ctx* ctx, long rows, int m, int k);
 bbt_status exact_apply_q(bbt_ctx* ctx, int m, long rows, const double* X, long ldx, const double* scale,
                          const double* Rp, const double* Z, int k, double* C, long ldc);
