@@ -97,7 +97,8 @@ constexpr int STAGES = 4;
 constexpr int A_TILE = TM * TK, B_TILE = TN * TK;
 constexpr int STAGE_BYTES = A_TILE + B_TILE;   // 48 KB
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
-constexpr int EPI_WARPS = 8;
+constexpr int EPI_WARPS = 16;   // four per TMEM lane quarter, each draining TN / 4 columns
+constexpr int EPI_COLS = TN / (EPI_WARPS / 4);
 constexpr int THREADS = (EPI_WARPS + 2) * 32;
 constexpr uint32_t TMEM_COLS = 2 * TN;          // two accumulators: modulus p+1 runs while p drains
 constexpr int MAX_KB_PER_SPLIT = 32768 / TK;    // T < 2^15 * 2^16 per split: no int32 overflow
@@ -434,10 +435,11 @@ crt_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUte
       if (!ok) atomicExch(P.err, 2);
     }
   } else {
-    // ---- epilogue: TMEM lanes 32 (warp % 4).., columns 128 (warp / 4).. of the accumulator;
-    //      T mod p as a byte per element, i (the TMEM lane) contiguous in memory
+    // ---- epilogue: TMEM lanes 32 (warp % 4).., columns EPI_COLS (warp / 4).. of the
+    //      accumulator; T mod p as a byte per element, i (the TMEM lane) contiguous in memory
     const int q4 = warp & 3, ch = warp >> 2;
     const int i = m0 + q4 * 32 + lane;
+    const bool row_ok = i < P.M;
     bool ok = true;
     for (int q = 0; q < P.n; ++q) {
       const int buf = q & 1, use = q >> 1;
@@ -445,12 +447,13 @@ crt_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUte
       tc_fence_after();
       const int p = P.p[q], c16 = P.c16[q];
       const uint32_t magic = P.magic[q], off = (uint32_t)P.off[q];
-      uint8_t* o = P.out + ((size_t)blockIdx.z * P.n + q) * (size_t)P.N * P.Mp;
+      uint8_t* o = P.out + ((size_t)blockIdx.z * P.n + q) * (size_t)P.N * P.Mp + i;
 #pragma unroll 1
-      for (int c = 0; c < TN / 2 / 16; ++c) {
+      for (int c = 0; c < EPI_COLS / 16; ++c) {
         uint32_t v[16];
-        tmem_ld16(tmem + ((uint32_t)(q4 * 32) << 16) + (uint32_t)(buf * TN + ch * (TN / 2) + c * 16), v);
-        const int j0 = n0 + ch * (TN / 2) + c * 16;
+        tmem_ld16(tmem + ((uint32_t)(q4 * 32) << 16) + (uint32_t)(buf * TN + ch * EPI_COLS + c * 16), v);
+        const int j0 = n0 + ch * EPI_COLS + c * 16;
+        uint8_t* oc = o + (size_t)j0 * P.Mp;
 #pragma unroll
         for (int e = 0; e < 16; ++e) {
           // a = (h - 2^15) 2^16 + lo with 0 <= h, lo < 2^16: h c16 + lo (< 2^24) is
@@ -460,8 +463,7 @@ crt_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUte
           const uint32_t x = (a >> 16) * (uint32_t)c16 + (a & 0xFFFFu);
           int r = (int)(x - __umulhi(x, magic) * (uint32_t)p) - (int)off;
           if (r < 0) r += p;
-          const int j = j0 + e;
-          if (i < P.M && j < P.N) o[(size_t)j * P.Mp + i] = (uint8_t)r;
+          if (row_ok && j0 + e < P.N) oc[(size_t)e * P.Mp] = (uint8_t)r;
         }
       }
       tc_fence_before();
