@@ -1,7 +1,15 @@
-// FP64 Cholesky factorisation and right-side triangular solve, recursive:
-// the diagonal leaves run as small SIMT kernels, everything above them as
-// FP64 tensor-core GEMMs (dgemm.cu).  Used by the mixed-precision local QR
-// (mixedqr.cu), whose R factor is built from Gram matrices.
+// FP64 Cholesky factorisation, triangular solves and the sign-recovery
+// elimination of the mixed-precision and exact-Gram local QRs (mixedqr.cu,
+// exactqr.cu), whose R factors are built from Gram matrices.
+//
+// Square operands (m x m, m up to a few thousand) take single launches: a
+// cooperative blocked Cholesky and sign-recovery LU with bounded grid
+// barriers, and triangular solves of independent rows or columns held in
+// shared memory.  Tall operands (the mixed mode's A R_p^-1 over the long
+// dimension), and the concurrent streams of the batched QR where cooperative
+// launches are not used, take the recursive forms: the diagonal leaves as
+// small SIMT kernels, everything above them as FP64 tensor-core GEMMs
+// (dgemm.cu).
 #include <cuda_runtime.h>
 
 #include <algorithm>

@@ -21,8 +21,10 @@
 // describe the same matrix: C = Q Z = A_int (R_p^-1 (W Z)) with R_p^-1 (W Z)
 // solved in double-double, rounded to 80-bit integers per column and
 // multiplied exactly by A_int (19 moduli at K = 1000).  No triangular solve
-// over the long dimension of A is left: the Gram and the back-transform are
-// the only passes over it.
+// over the long dimension of A is left.  The residue planes of A_int can be
+// formed once, with every modulus both products need, and kept: the Gram
+// reads them K-major, the products with Q MN-major (exact_apply_planes), and
+// X itself is then read only by the sketch, the row maxima and that one pass.
 #include <cuda_runtime.h>
 
 #include <algorithm>

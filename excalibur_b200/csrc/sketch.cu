@@ -191,23 +191,25 @@ sketch_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
   }
 }
 
-// X (m x n row-major, ld ldx) -> three bf16 pieces A[p][i][j] (row pitch `pitch`).
+// X (m x n row-major, ld ldx) -> three bf16 pieces A[p][i][j] (row pitch `pitch`);
+// rows over blockIdx.y, columns over the x grid (no index division).
 __global__ void split3_kernel(int m, long n, const double* __restrict__ X, long ldx, __nv_bfloat16* __restrict__ A,
                               long pitch) {
-  const long total = (long)m * n;
   const size_t plane = (size_t)m * pitch;
-  for (long f = blockIdx.x * (long)blockDim.x + threadIdx.x; f < total; f += (long)gridDim.x * blockDim.x) {
-    const long i = f / n, j = f - i * n;
-    const double x = X[i * ldx + j];
-    const __nv_bfloat16 b0 = __double2bfloat16(x);
-    const double r1 = x - (double)__bfloat162float(b0);
-    const __nv_bfloat16 b1 = __double2bfloat16(r1);
-    const double r2 = r1 - (double)__bfloat162float(b1);
-    const __nv_bfloat16 b2 = __double2bfloat16(r2);
-    const size_t o = (size_t)i * pitch + j;
-    A[o] = b0;
-    A[plane + o] = b1;
-    A[2 * plane + o] = b2;
+  for (int i = blockIdx.y; i < m; i += gridDim.y) {
+    const double* xr = X + (long)i * ldx;
+    __nv_bfloat16* ar = A + (size_t)i * pitch;
+    for (long j = blockIdx.x * (long)blockDim.x + threadIdx.x; j < n; j += (long)gridDim.x * blockDim.x) {
+      const double x = xr[j];
+      const __nv_bfloat16 b0 = __double2bfloat16(x);
+      const double r1 = x - (double)__bfloat162float(b0);
+      const __nv_bfloat16 b1 = __double2bfloat16(r1);
+      const double r2 = r1 - (double)__bfloat162float(b1);
+      const __nv_bfloat16 b2 = __double2bfloat16(r2);
+      ar[j] = b0;
+      ar[plane + j] = b1;
+      ar[2 * plane + j] = b2;
+    }
   }
 }
 
@@ -218,14 +220,30 @@ __device__ __forceinline__ uint64_t mix64(uint64_t z) {   // splitmix64 finalise
   return z ^ (z >> 31);
 }
 
-// S (N x n, row pitch `pitch`) with independent +-1 entries.
+// S (N x n, row pitch `pitch`, a multiple of 8) with independent +-1 entries,
+// entry (i, j) from the hash of i n + j; eight entries per 16-byte store.
 __global__ void rademacher_kernel(int N, long n, long pitch, __nv_bfloat16* __restrict__ S, uint64_t seed) {
-  const long total = (long)N * n;
-  const __nv_bfloat16_raw plus = {0x3F80}, minus = {0xBF80};
-  for (long f = blockIdx.x * (long)blockDim.x + threadIdx.x; f < total; f += (long)gridDim.x * blockDim.x) {
-    const long i = f / n, j = f - i * n;
-    S[(size_t)i * pitch + j] = (mix64(seed ^ (uint64_t)f * 0xD1B54A32D192ED03ull) & 1u) ? __nv_bfloat16(plus)
-                                                                                           : __nv_bfloat16(minus);
+  const uint16_t plus = 0x3F80, minus = 0xBF80;
+  for (int i = blockIdx.y; i < N; i += gridDim.y) {
+    uint16_t* row = reinterpret_cast<uint16_t*>(S) + (size_t)i * pitch;
+    for (long j0 = (blockIdx.x * (long)blockDim.x + threadIdx.x) * 8; j0 < n; j0 += (long)gridDim.x * blockDim.x * 8) {
+      uint16_t v[8];
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        const uint64_t f = (uint64_t)i * (uint64_t)n + (uint64_t)(j0 + e);
+        v[e] = (mix64(seed ^ f * 0xD1B54A32D192ED03ull) & 1u) ? plus : minus;
+      }
+      if (j0 + 8 <= n && (reinterpret_cast<uintptr_t>(row + j0) & 15) == 0) {
+        uint4 w;
+        w.x = v[0] | ((uint32_t)v[1] << 16);
+        w.y = v[2] | ((uint32_t)v[3] << 16);
+        w.z = v[4] | ((uint32_t)v[5] << 16);
+        w.w = v[6] | ((uint32_t)v[7] << 16);
+        *reinterpret_cast<uint4*>(row + j0) = w;
+      } else {
+        for (int e = 0; e < 8 && j0 + e < n; ++e) row[j0 + e] = v[e];
+      }
+    }
   }
 }
 
@@ -291,7 +309,10 @@ size_t sketch_workspace_bytes(const bbt_ctx* ctx, int m, long n, int N) {
 }
 
 bbt_status rademacher(bbt_ctx* ctx, int N, long n, void* S, uint64_t seed) {
-  rademacher_kernel<<<8 * ctx->num_sms, 256, 0, ctx->stream>>>(N, n, sketch_pitch(n), (__nv_bfloat16*)S, seed);
+  const long pitch = sketch_pitch(n);
+  if (pitch % 8 != 0) return fail(ctx, BBT_ERR_ARG, "rademacher: pitch %ld", pitch);
+  const dim3 g((unsigned)std::max(1L, std::min((n + 2047) / 2048, 64L)), (unsigned)std::min(N, 65535));
+  rademacher_kernel<<<g, 256, 0, ctx->stream>>>(N, n, pitch, (__nv_bfloat16*)S, seed);
   BBT_LAUNCHED(ctx);
   return BBT_OK;
 }
@@ -310,7 +331,8 @@ bbt_status sketch_bf16x3(bbt_ctx* ctx, int m, long n, const double* X, long ldx,
   __nv_bfloat16* A = ctx->ws.take<__nv_bfloat16>((size_t)PIECES * m * pitch);
   double* part = ctx->ws.take<double>((size_t)sp.splits * m * N);
   if (!part) return fail(ctx, BBT_ERR_NOMEM, "sketch: workspace");
-  split3_kernel<<<8 * ctx->num_sms, 256, 0, ctx->stream>>>(m, n, X, ldx, A, pitch);
+  split3_kernel<<<dim3((unsigned)std::max(1L, std::min((n + 255) / 256, 16L)), (unsigned)std::min(m, 65535)), 256, 0,
+                  ctx->stream>>>(m, n, X, ldx, A, pitch);
   BBT_LAUNCHED(ctx);
 
   CUtensorMap ta, tb;
