@@ -239,6 +239,16 @@ def cublas_dgemm_peak(torch, dev):
     return best
 
 
+def max_over_ranks(torch, value, device, world):
+    """The largest of every rank's value (a collective every rank calls in
+    the same order): the job-level time of replicas timed independently."""
+    if world <= 1:
+        return value
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t)
+
+
 def run_ours(args, rank, world):
     """Times the pipeline at each requested precision (plain FP64 first, then
     mixed); returns {precision: result} plus the end-to-end measurement of the
@@ -292,11 +302,7 @@ def run_ours(args, rank, world):
         launches = (ctx.launches() - l0) // args.steps
         torch.cuda.synchronize()
         # device time of a step = sum of its stage events (CUDA events on the stream)
-        sec = sum(stage.values()) / 1e3
-        if world > 1:
-            t = torch.tensor([sec], device=dev)
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            sec = float(t)
+        sec = max_over_ranks(torch, sum(stage.values()) / 1e3, dev, world)
         out_all[pname] = {"sec": sec, "host_sec": statistics.median(times), "stage_ms": stage, "acc": acc,
                           "tuned": tuned, "launches": launches, "prof": prof, "clocks": clk.summary()}
     res = {"runs": out_all, "head": precisions[-1]}
@@ -319,7 +325,8 @@ def run_ours(args, rank, world):
             sg, Ug, VTg = ctx.fedsvd_host(hb, pub, priv, precision=prec, out=outbuf)
             et.append(time.perf_counter() - t0)
         k = len(sg)
-        res["e2e"] = {"value": statistics.median(et), "unit": "s", "precision": res["head"],
+        res["e2e"] = {"value": max_over_ranks(torch, statistics.median(et), dev, world), "unit": "s",
+                      "precision": res["head"],
                       "h2d_bytes_per_step": int(sum(h.nbytes for h in hb)),
                       "d2h_bytes_per_step": int(8 * (k + m * k + k * sum(h.shape[1] for h in hb)))}
     return res
