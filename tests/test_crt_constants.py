@@ -1,0 +1,146 @@
+"""The arithmetic the CRT kernels (excalibur_b200/csrc/crt.cu) rely on,
+checked on the CPU from the same moduli list and the same formulas for their
+constants: the moduli are pairwise coprime bytes, the multiply-high
+quotients are exact over the ranges the kernels feed them, the residues of
+53-bit integers formed from 18-bit pieces stay in range, the epilogue's
+reduction of an int32 accumulator is the residue, the modulus count covers
+every product, and the fixed-point reconstruction recovers the integer."""
+import math
+import os
+import re
+
+import numpy as np
+import pytest
+
+SRC = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "excalibur_b200", "csrc", "crt.cu")
+
+
+def moduli():
+    text = open(SRC).read()
+    body = re.search(r"MODULI\[MAXMOD\]\s*=\s*\{([^}]*)\}", text).group(1)
+    return [int(v) for v in body.replace("\n", " ").split(",") if v.strip()]
+
+
+MOD = moduli()
+
+
+def crt_moduli(bits_a, bits_b, K):
+    """crt.cu's rule: the fewest moduli (at least 4) whose product holds
+    (bits_a - 2) + (bits_b - 2) + log2 K + 2 bits."""
+    need = (bits_a - 2) + (bits_b - 2) + math.log2(max(K, 1)) + 2.0
+    bits = 0.0
+    for n, p in enumerate(MOD):
+        bits += math.log2(p)
+        if bits >= need:
+            return max(n + 1, 4)
+    return -1
+
+
+def test_moduli_are_pairwise_coprime_bytes():
+    assert len(MOD) == 24 and MOD[0] == 256
+    assert all(2 <= p <= 256 for p in MOD)
+    for i, p in enumerate(MOD):
+        for q in MOD[i + 1:]:
+            assert math.gcd(p, q) == 1, (p, q)
+
+
+@pytest.mark.parametrize("p", MOD)
+def test_multiply_high_quotients_are_exact(p):
+    # magic32 = ceil(2^32 / p): exact quotients for 0 <= x < 2^24 (exhaustive)
+    magic32 = -(-(1 << 32) // p)
+    x = np.arange(1 << 24, dtype=np.uint64)
+    assert np.array_equal((x * np.uint64(magic32)) >> np.uint64(32), x // np.uint64(p))
+    # magic35 = ceil(2^35 / p) for x < 2^27: x (magic35 p - 2^35) < 2^35 is the
+    # exactness condition; checked at its worst case, and on random x
+    magic35 = -(-(1 << 35) // p)
+    assert ((1 << 27) - 1) * (magic35 * p - (1 << 35)) < (1 << 35)
+    rng = np.random.default_rng(p)
+    xs = rng.integers(0, 1 << 27, 1 << 20, dtype=np.uint64)
+    assert np.array_equal(((xs * np.uint64(magic35)) >> np.uint64(32)) >> np.uint64(3), xs // np.uint64(p))
+
+
+@pytest.mark.parametrize("p", MOD)
+def test_residues_from_pieces_stay_in_range(p):
+    """t = a 2^36 + b 2^18 + c (a = floor(t / 2^36), 0 <= b, c < 2^18) for
+    |t| <= 2^51, the 53-bit integers of the products: x = a c36 + b c18 + c +
+    off lies in [0, 2^27), and x mod p is t mod p."""
+    c36, c18 = (1 << 36) % p, (1 << 18) % p
+    off = p * (((1 << 23) + p - 1) // p)
+    lo = -(1 << 15) * c36 + off
+    hi = (1 << 15) * c36 + ((1 << 18) - 1) * (c18 + 1) + off
+    assert 0 <= lo and hi < (1 << 27)
+    rng = np.random.default_rng(p + 1)
+    for t in [-(1 << 51), (1 << 51), 0, -1, 1, *[int(v) for v in rng.integers(-(1 << 51), 1 << 51, 2000)]]:
+        a, rem = divmod(t, 1 << 36)
+        b, c = divmod(rem, 1 << 18)
+        x = a * c36 + b * c18 + c + off
+        assert 0 <= x < (1 << 27)
+        assert x % p == t % p
+
+
+@pytest.mark.parametrize("p", MOD)
+def test_epilogue_reduction_of_int32_accumulators(p):
+    """The GEMM epilogue's a = v xor 2^31, x = (a >> 16) c16 + (a & 0xFFFF)
+    (< 2^24), r = x mod p - (2^31 mod p), r += p if negative: r = v mod p."""
+    c16, off, magic = 65536 % p, (1 << 31) % p, -(-(1 << 32) // p)
+    rng = np.random.default_rng(p + 2)
+    vals = [-(1 << 31), (1 << 31) - 1, 0, -1, 1, *[int(v) for v in rng.integers(-(1 << 31), 1 << 31, 5000)]]
+    for v in vals:
+        a = (v & 0xFFFFFFFF) ^ 0x80000000
+        x = (a >> 16) * c16 + (a & 0xFFFF)
+        assert x < (1 << 24)
+        r = x - ((x * magic) >> 32) * p - off
+        if r < 0:
+            r += p
+        assert r == v % p
+
+
+@pytest.mark.parametrize("bits_a,bits_b,K,expect", [(53, 53, 500_000, 16), (50, 50, 500_000, 15),
+                                                    (53, 80, 1000, 19), (53, 80, 512, 18), (53, 53, 2000, 15)])
+def test_modulus_count_covers_the_product(bits_a, bits_b, K, expect):
+    n = crt_moduli(bits_a, bits_b, K)
+    assert n == expect
+    M = math.prod(MOD[:n])
+    # |t| <= 2^(b-2) per operand, so |T| <= 2^(ba-2) 2^(bb-2) K <= M / 4
+    assert 4 * (1 << (bits_a - 2)) * (1 << (bits_b - 2)) * K <= M
+
+
+def reconstruct(T, n, limbs):
+    """crt.cu's reconstruction: y_q = (T mod p_q) ((M / p_q)^-1 mod p_q) mod
+    p_q and the fraction S = sum_q y_q floor(2^128 / p_q) mod 2^128 (its low 32
+    bits dropped when limbs = 3), read as a signed 128-bit number: S M / 2^128
+    is T up to the floors' errors."""
+    ps = MOD[:n]
+    M = math.prod(ps)
+    S = 0
+    for p in ps:
+        inv = pow((M // p) % p, -1, p)
+        y = ((T % p) * inv) % p
+        F = ((1 << 128) - 1) // p + (1 if ((1 << 128) - 1) % p == p - 1 else 0)
+        if limbs == 3:
+            F = (F >> 32) << 32
+        S += y * F
+    S %= 1 << 128
+    if S >= 1 << 127:
+        S -= 1 << 128
+    return S, M
+
+
+@pytest.mark.parametrize("n", [4, 15, 16, 19, 24])
+@pytest.mark.parametrize("limbs", [3, 4])
+def test_fixed_point_reconstruction(n, limbs):
+    M = math.prod(MOD[:n])
+    rng = np.random.default_rng(n * 10 + limbs)
+    # the modulus count leaves M >= 4 max|T| (two bits of margin over the sign)
+    Ts = [0, 1, -1, M // 4, -(M // 4)]
+    Ts += [int(rng.integers(-(1 << 62), 1 << 62)) * int(rng.integers(1, 1 << 62)) % (M // 2) - M // 4
+           for _ in range(300)]
+    bits = 128 if limbs == 4 else 96
+    for T in Ts:
+        S, _ = reconstruct(T, n, limbs)
+        # every term y_q F_q is short of y_q 2^128 / p_q by less than y_q < 256
+        # units of 2^(128 - bits): |S M - T 2^128| < n 256 M 2^(128 - bits)
+        assert abs(S * M - T * (1 << 128)) < n * 256 * M * (1 << (128 - bits)), T
+    # relative to the largest |T| the kernels allow (M / 4): below 2^-100 with
+    # 128-bit fractions, 2^-70 with 96-bit ones
+    assert n * 256 * 4 / float(1 << bits) < (2.0 ** -100 if limbs == 4 else 2.0 ** -70)
