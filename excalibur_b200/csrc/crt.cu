@@ -546,9 +546,9 @@ __device__ __forceinline__ void crt_fraction4(const CombArgs& A, long f, long to
 }
 
 __device__ __forceinline__ void two_sum(double a, double b, double& s, double& e) {
-  s = a + b;
-  const double bb = s - a;
-  e = (a - (s - bb)) + (b - bb);
+  s = __dadd_rn(a, b);
+  const double bb = __dsub_rn(s, a);
+  e = __dadd_rn(__dsub_rn(a, __dsub_rn(s, bb)), __dsub_rn(b, bb));
 }
 
 // A signed 128-bit integer (two's complement, hi:lo) as a double-double: its
@@ -576,7 +576,7 @@ __device__ __forceinline__ void fixed_to_dd(uint64_t hi, uint64_t lo, double& dh
 }
 
 __device__ __forceinline__ void two_prod(double a, double b, double& p, double& e) {
-  p = a * b;
+  p = __dmul_rn(a, b);   // rounded on its own: never fused with a later sum
   e = fma(a, b, -p);
 }
 
@@ -651,8 +651,8 @@ combine_dd_kernel(CombArgs A, const double* __restrict__ sa, const double* __res
       double p, er;
       two_prod(fh, A.mod_hi, p, er);
       er += fh * A.mod_lo + fl * A.mod_hi;
-      const double s = p + er;
-      const double t = er - (s - p);
+      const double s = __dadd_rn(p, er);
+      const double t = __dsub_rn(er, __dsub_rn(s, p));
       const double sc = ldexp((sa ? sa[i + e] : 1.0) * sb[j], -128 - shift);
       Ch[(i + e) + (long)j * ldc] = s * sc;
       Cl[(i + e) + (long)j * ldc] = t * sc;

@@ -32,14 +32,16 @@ struct dd {
   double hi, lo;
 };
 
+// The error-free transformations need every sum and product rounded on its
+// own: the _rn intrinsics are never merged into a fused multiply-add.
 __device__ __forceinline__ dd two_sum(double a, double b) {
-  const double s = a + b;
-  const double bb = s - a;
-  return {s, (a - (s - bb)) + (b - bb)};
+  const double s = __dadd_rn(a, b);
+  const double bb = __dsub_rn(s, a);
+  return {s, __dadd_rn(__dsub_rn(a, __dsub_rn(s, bb)), __dsub_rn(b, bb))};
 }
 __device__ __forceinline__ dd quick_two_sum(double a, double b) {   // |a| >= |b|
-  const double s = a + b;
-  return {s, b - (s - a)};
+  const double s = __dadd_rn(a, b);
+  return {s, __dsub_rn(b, __dsub_rn(s, a))};
 }
 __device__ __forceinline__ dd dd_add(dd x, dd y) {
   dd s = two_sum(x.hi, y.hi);
@@ -51,7 +53,7 @@ __device__ __forceinline__ dd dd_add(dd x, dd y) {
 }
 // a (double) times x (double-double)
 __device__ __forceinline__ dd dd_mul_d(dd x, double a) {
-  const double p = x.hi * a;
+  const double p = __dmul_rn(x.hi, a);
   const double e = fma(x.hi, a, -p) + x.lo * a;
   return quick_two_sum(p, e);
 }
@@ -60,7 +62,7 @@ __device__ __forceinline__ dd dd_mul_d(dd x, double a) {
 // restores double-double accuracy without a division instruction)
 __device__ __forceinline__ dd dd_div_d(dd x, double a, double ia) {
   const double q1 = x.hi * ia;
-  const double p = q1 * a;
+  const double p = __dmul_rn(q1, a);
   const double pe = fma(q1, a, -p);
   const dd r = dd_add(x, {-p, -pe});
   const double q2 = r.hi * ia;
@@ -73,11 +75,11 @@ __device__ __forceinline__ dd dd_div_d(dd x, double a, double ia) {
 struct dot2 {
   double s = 0.0, c = 0.0;
   __device__ __forceinline__ void add(double a, dd x) {
-    const double p = a * x.hi;
+    const double p = __dmul_rn(a, x.hi);
     const double pe = fma(a, x.hi, -p);
-    const double t = s + p;
-    const double bb = t - s;
-    c += ((s - (t - bb)) + (p - bb)) + pe + a * x.lo;
+    const double t = __dadd_rn(s, p);
+    const double bb = __dsub_rn(t, s);
+    c += (__dsub_rn(s, __dsub_rn(t, bb)) + __dsub_rn(p, bb)) + pe + a * x.lo;
     s = t;
   }
   __device__ __forceinline__ dd value() const { return quick_two_sum(s, c); }
