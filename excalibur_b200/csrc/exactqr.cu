@@ -12,8 +12,10 @@
 //      the integer product computed exactly from int8 residues on the tensor
 //      cores (crt.cu) and kept as a double-double;
 //   3. G_Q = R_p^-T G R_p^-1 in double-double (ddsolve.cu): the Gram of
-//      Q_p = A_int R_p^-1 to ~2^-100 of its norm, well conditioned, so
-//      R_3 = chol(G_Q) in FP64 is as accurate as R_3 can be;
+//      Q_p = A_int R_p^-1 to ~2^-90 of its norm (compensated sums,
+//      renormalised every 32 terms, growing with cond(R_p)), far below FP64
+//      rounding; it is well conditioned, so R_3 = chol(G_Q) in FP64 is as
+//      accurate as R_3 can be;
 //   4. R = R_3 R_p, W = R_3^-1, Q = A_int R_p^-1 W (never formed), and
 //      dgeqrf's row signs recovered from Q's top block as mixedqr.cu does.
 //
