@@ -188,9 +188,9 @@ bbt_status bbt_gebrd(bbt_ctx* ctx, int n, double* d_A, double* d_d, double* d_e)
  * N must be a multiple of 128.
  * bbt_mixed_local_qr: the precision-1 local QR.  d_x (row-major m x
  * local_n, local_n > m) is overwritten by Q_p^T, d_r receives R (m x m
- * column-major, upper triangular, positive diagonal; equal as memory to the
- * row-major R^T of bbt_local_qr up to row signs), d_w (may be NULL) receives
- * W (m x m column-major) with Q = Q_p W orthonormal and A = X^T = Q R.
+ * column-major, upper triangular with dgeqrf's row signs; equal as memory to
+ * the row-major R^T of bbt_local_qr), d_w (may be NULL) receives W (m x m
+ * column-major) with Q = Q_p W orthonormal and A = X^T = Q R.
  * Additive: the reference has no split-precision path (its local QR is
  * client.cpp:417-445). */
 bbt_status bbt_rademacher(bbt_ctx* ctx, int N, size_t local_n, unsigned long long seed, void* d_S);
@@ -255,7 +255,9 @@ bbt_status bbt_gram_dd(bbt_ctx* ctx, int m, long n, const double* d_X, long ldx,
  * bbt_exact_local_qr: the R factor of A = X^T for a row-major m x local_n d_x
  * (local_n >= m; not modified) from the BF16x3 sketch's preconditioner R_p
  * and the exact Gram of X's 53-bit rows (bbt_gram_dd), preconditioned in
- * double-double: d_R (m x m, column-major, dgeqrf's row signs), d_W, d_Rp
+ * double-double: d_R (m x m, column-major, dgeqrf's row signs; with
+ * local_n == m the last row's sign can differ, LAPACK's last reflector being
+ * the identity there), d_W, d_Rp
  * (m x m column-major) and d_scale (m) describe Q = A_int R_p^-1 W, with
  * A_int X^T's rows rounded to 53-bit integers at the row scales d_scale.
  * bbt_exact_apply_q: d_C (rows x k column-major, ldc) = A_int R_p^-1 d_Z for
