@@ -360,22 +360,12 @@ bbt_status bbt_dgemm_crt(bbt_ctx* ctx, int M, int N, long K, double alpha, const
 bbt_status bbt_gram_dd(bbt_ctx* ctx, int m, long n, const double* X, long ldx, double* Gh, double* Gl) {
   if (!ctx) return BBT_ERR_ARG;
   if (m < 1 || n < 1 || bad(X) || bad(Gh) || bad(Gl) || ldx < n) return fail(ctx, BBT_ERR_ARG, "gram_dd: bad arguments");
-  const int nm = crt_moduli(53, 53, n);
-  if (nm < 1) return fail(ctx, BBT_ERR_ARG, "gram_dd: n=%ld too long", n);
-  const long Kp = crt_pitch(n);
-  BBT_TRY(ensure(ctx, (size_t)nm * m * Kp + crt_product_bytes(ctx, m, m, n, nm, true) + (size_t)m * 16 + (4 << 20)));
+  if (crt_moduli(53, 53, n) < 1) return fail(ctx, BBT_ERR_ARG, "gram_dd: n=%ld too long", n);
+  BBT_TRY(ensure(ctx, exact_gram_workspace_bytes(ctx, m, n) + (size_t)m * 16 + (4 << 20)));
   BBT_TRY(clear_tc_flags(ctx));
-  int8_t* RX = ctx->ws.take<int8_t>((size_t)nm * m * Kp);
   double* s = ctx->ws.take<double>(m);
-  const size_t mark = ctx->ws.top;
-  BBT_TRY(crt_row_scales(ctx, m, n, X, ldx, s));
-  ctx->ws.top = mark;
-  uint8_t* R = ctx->ws.take<uint8_t>(crt_product_bytes(ctx, m, m, n, nm, true));
-  if (!R) return fail(ctx, BBT_ERR_NOMEM, "gram_dd: workspace");
-  BBT_TRY(crt_residues_rows(ctx, m, n, X, ldx, s, 53, nm, RX, Kp));
-  int splits = 1;
-  BBT_TRY(crt_product(ctx, m, m, n, nm, RX, RX, Kp, true, R, &splits));
-  BBT_TRY(crt_combine_dd(ctx, m, m, nm, splits, R, true, s, s, 2 * 52, Gh, Gl, m));
+  if (!s) return fail(ctx, BBT_ERR_NOMEM, "gram_dd: workspace");
+  BBT_TRY(exact_gram_dd(ctx, m, n, X, ldx, s, nullptr, Gh, Gl));
   return check_tc_flags(ctx, "gram_dd");
 }
 

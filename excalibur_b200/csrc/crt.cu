@@ -995,12 +995,33 @@ bbt_status crt_combine_dd(bbt_ctx* ctx, int M, int N, int n, int splits, const u
   return BBT_OK;
 }
 
+namespace {
+// K-chunk of gemm_crt's residue planes: all of K when they fit the cap, else
+// equal chunks, multiples of 2^15 columns (one K-split each at most).
+constexpr size_t CRT_CHUNK_DEFAULT = (size_t)6 << 30;
+long crt_k_chunk(int rows, long K, int n) {
+  const size_t cap = long_chunk_bytes(CRT_CHUNK_DEFAULT);
+  const size_t full = (size_t)n * rows * crt_pitch(K);
+  if (full <= cap) return K;
+  long c = (long)(cap / ((size_t)n * rows)) / 32768 * 32768;
+  c = std::max(c, 32768L);
+  const long chunks = (K + c - 1) / c;
+  return ((K + chunks - 1) / chunks + 32767) / 32768 * 32768;
+}
+size_t chunked_product_bytes(const bbt_ctx* ctx, int M, int N, long K, int n, bool upper, long kc) {
+  size_t b = 0;
+  for (long k0 = 0; k0 < K; k0 += kc) b += crt_product_bytes(ctx, M, N, std::min(kc, K - k0), n, upper) - 4096;
+  return b + 4096;
+}
+}  // namespace
+
 size_t crt_gemm_workspace_bytes(const bbt_ctx* ctx, int M, int N, long K, int bits, bool same, bool upper) {
   const int n = crt_moduli(bits, bits, K);
   if (n < 1) return 0;
-  const long Kp = crt_pitch(K);
-  return (size_t)n * (same ? M : M + N) * Kp + crt_product_bytes(ctx, M, N, K, n, upper) + (size_t)(M + N) * 16 +
-         (size_t)std::max(M, N) * 8 + 8192;
+  const long kc = crt_k_chunk(same ? M : M + N, K, n);
+  const long Kp = crt_pitch(kc);
+  return (size_t)n * (same ? M : M + N) * Kp + chunked_product_bytes(ctx, M, N, K, n, upper, kc) +
+         (size_t)(M + N) * 16 + (size_t)std::max(M, N) * 8 + 8192;
 }
 
 // The Gram matrix of a long operand: K long enough for the CRT product (one
@@ -1014,30 +1035,36 @@ bbt_status gemm_crt(bbt_ctx* ctx, int M, int N, long K, double alpha, const doub
                     int bits) {
   const int n = crt_moduli(bits, bits, K);
   if (n < 1) return fail(ctx, BBT_ERR_ARG, "crt: %d bits over K=%ld needs too many moduli", bits, K);
-  const long Kp = crt_pitch(K);
+  if (csA != 1 || (!same && csB != 1))   // row scales need each row contiguous along K
+    return fail(ctx, BBT_ERR_ARG, "crt: operands must be contiguous along K");
+  // long K: residue planes in K-chunks (scales over all of K first), the
+  // chunks' K-splits side by side, summed by one reconstruction
+  const long kc = crt_k_chunk(same ? M : M + N, K, n);
+  const long Kp = crt_pitch(kc);
   const size_t mark = ctx->ws.top;
   int8_t* RA = ctx->ws.take<int8_t>((size_t)n * M * Kp);
   int8_t* RB = same ? RA : ctx->ws.take<int8_t>((size_t)n * N * Kp);
   double* sa = ctx->ws.take<double>(M);
   double* sb = same ? sa : ctx->ws.take<double>(N);
-  uint8_t* R = ctx->ws.take<uint8_t>(crt_product_bytes(ctx, M, N, K, n, upper));
+  uint8_t* R = ctx->ws.take<uint8_t>(chunked_product_bytes(ctx, M, N, K, n, upper, kc));
   if (!R) return fail(ctx, BBT_ERR_NOMEM, "crt: workspace");
-  auto prep = [&](int rows, const double* X, long rs, long cs, double* s, int8_t* planes) -> bbt_status {
-    if (cs == 1) {
-      const size_t m2 = ctx->ws.top;
-      BBT_TRY(crt_row_scales(ctx, rows, K, X, rs, s));
-      ctx->ws.top = m2;
-      return crt_residues_rows(ctx, rows, K, X, rs, s, bits, n, planes, Kp);
-    }
-    if (rs == 1) {   // scales of rows contiguous in i: the row maxima over K of the transposed view
-      return fail(ctx, BBT_ERR_ARG, "crt: row scales of a column-contiguous operand are not built");
-    }
-    return fail(ctx, BBT_ERR_ARG, "crt: operand needs a unit stride");
-  };
-  BBT_TRY(prep(M, A, rsA, csA, sa, RA));
-  if (!same) BBT_TRY(prep(N, B, rsB, csB, sb, RB));
-  int splits = 1;
-  BBT_TRY(crt_product(ctx, M, N, K, n, RA, RB, Kp, upper, R, &splits));
+  {
+    const size_t m2 = ctx->ws.top;
+    BBT_TRY(crt_row_scales(ctx, M, K, A, rsA, sa));
+    ctx->ws.top = m2;
+    if (!same) BBT_TRY(crt_row_scales(ctx, N, K, B, rsB, sb));
+    ctx->ws.top = m2;
+  }
+  const size_t split_bytes = (size_t)n * ((M + 3) & ~3) * N;
+  int splits = 0;
+  for (long k0 = 0; k0 < K; k0 += kc) {
+    const long Kc = std::min(kc, K - k0);
+    BBT_TRY(crt_residues_rows(ctx, M, Kc, A + k0, rsA, sa, bits, n, RA, Kp));
+    if (!same) BBT_TRY(crt_residues_rows(ctx, N, Kc, B + k0, rsB, sb, bits, n, RB, Kp));
+    int sp = 1;
+    BBT_TRY(crt_product(ctx, M, N, Kc, n, RA, RB, Kp, upper, R + (size_t)splits * split_bytes, &sp));
+    splits += sp;
+  }
   BBT_TRY(crt_combine(ctx, M, N, n, splits, R, upper, sa, sb, 2 * (bits - 1), alpha, beta, C, ldc));
   ctx->ws.top = mark;
   return BBT_OK;

@@ -38,6 +38,36 @@ namespace {
 
 constexpr int GRAM_BITS = 53;
 constexpr int Z_BITS = 80;
+// Scratch cap of one pass over the long dimension: the Gram's residue planes
+// (when they are not kept) and the products with Q (residues of the rows and
+// of the product) are formed in chunks of at most this many bytes, so a
+// participant of any length needs bounded workspace (2 x 10^9-element blocks
+// of 4 x 2000 x 10^6 included).
+constexpr size_t LONG_CHUNK_DEFAULT = (size_t)6 << 30;
+
+// K-chunk of the Gram's residue planes (nm planes of m rows): all of n when
+// the planes fit the cap, else equal chunks, a multiple of 2^15 columns.
+long gram_chunk(int m, long n, int nm) {
+  const size_t cap = long_chunk_bytes(LONG_CHUNK_DEFAULT);
+  const size_t full = (size_t)nm * m * crt_pitch(n);
+  if (full <= cap) return n;
+  long c = (long)(cap / ((size_t)nm * m)) / 32768 * 32768;
+  c = std::max(c, 32768L);
+  const long chunks = (n + c - 1) / c;
+  return ((n + chunks - 1) / chunks + 32767) / 32768 * 32768;
+}
+
+// Row chunk of a product with Q over `rows` rows: all rows when the residues
+// of A and of the product fit the cap, else equal chunks (multiples of 128).
+long apply_chunk(long rows, int nm, long Kp, int k) {
+  const size_t cap = long_chunk_bytes(LONG_CHUNK_DEFAULT);
+  const size_t per_row = (size_t)nm * (Kp + k) + 8;
+  if ((size_t)rows * per_row <= cap) return rows;
+  long c = (long)(cap / per_row) / 128 * 128;
+  c = std::max(c, 128L);
+  const long chunks = (rows + c - 1) / c;
+  return ((rows + chunks - 1) / chunks + 127) / 128 * 128;
+}
 
 __global__ void dd_scale_rows_kernel(int m, int k, const double* __restrict__ s, double* __restrict__ Zh,
                                      double* __restrict__ Zl, long ld) {
@@ -56,13 +86,25 @@ __global__ void zero_kernel(double* __restrict__ p, long n) {
 
 }  // namespace
 
+// Product residues of the chunked Gram: every chunk's K-splits side by side.
+size_t gram_product_bytes(const bbt_ctx* ctx, int m, long n, int nm, long kc, int* total_splits) {
+  size_t b = 0;
+  int sp = 0;
+  for (long k0 = 0; k0 < n; k0 += kc) {
+    const long K = std::min(kc, n - k0);
+    const size_t one = crt_product_bytes(ctx, m, m, K, nm, true) - 4096;
+    b += one;
+    sp += (int)(one / ((size_t)nm * ((m + 3) & ~3) * m));
+  }
+  if (total_splits) *total_splits = sp;
+  return b + 4096;
+}
+
 size_t exact_qr_workspace_bytes(const bbt_ctx* ctx, int m, long n) {
   const int N = sketch_rows(m);
-  const int nm = crt_moduli(GRAM_BITS, GRAM_BITS, n);
-  const long Kp = crt_pitch(n);
   size_t s = sketch_workspace_bytes(ctx, m, n, N);
   s = std::max(s, dgemm_workspace_bytes(ctx, m, m, N));
-  s = std::max(s, (size_t)nm * m * Kp + crt_product_bytes(ctx, m, m, n, nm, true) + (size_t)m * 8 + 4096);
+  s = std::max(s, exact_gram_workspace_bytes(ctx, m, n));
   return s + ((size_t)N * m + 6 * (size_t)m * m + 2 * m) * 8 + 16384;
 }
 
@@ -74,6 +116,47 @@ int exact_keep_moduli(int m, long n) {
 size_t exact_keep_bytes(int m, long n) {
   const int nk = exact_keep_moduli(m, n);
   return nk < 1 ? 0 : (size_t)nk * m * crt_pitch(n) + 256;
+}
+
+size_t exact_gram_workspace_bytes(const bbt_ctx* ctx, int m, long n) {
+  const int nm = crt_moduli(GRAM_BITS, GRAM_BITS, n);
+  if (nm < 1) return 0;
+  const long kc = gram_chunk(m, n, nm);
+  return (size_t)nm * m * crt_pitch(kc) + gram_product_bytes(ctx, m, n, nm, kc, nullptr) + (size_t)m * 8 + 4096;
+}
+
+// The upper triangle of G = X X^T for X's rows rounded to 53-bit integers at
+// the row scales (written to scale), exactly, as a double-double (column-major,
+// ld m).  Kept planes (every modulus the later products with X_int^T need)
+// cover all of K at once; otherwise the planes are formed in K-chunks (the row
+// scales over all of K first) whose products' K-splits sit side by side and
+// are summed by one reconstruction.
+bbt_status exact_gram_dd(bbt_ctx* ctx, int m, long n, const double* X, long ldx, double* scale, int8_t* keep,
+                         double* Gh, double* Gl) {
+  const int nm = crt_moduli(GRAM_BITS, GRAM_BITS, n);
+  if (nm < 1) return fail(ctx, BBT_ERR_ARG, "exact Gram: n=%ld too long", n);
+  const size_t m2 = ctx->ws.top;
+  const int nr = keep ? exact_keep_moduli(m, n) : nm;   // the Gram uses the first nm of the kept planes
+  const long kc = keep ? n : gram_chunk(m, n, nm);
+  const long Kp = crt_pitch(kc);
+  int8_t* RX = keep ? keep : ctx->ws.take<int8_t>((size_t)nm * m * Kp);
+  const size_t m3 = ctx->ws.top;
+  BBT_TRY(crt_row_scales(ctx, m, n, X, ldx, scale));
+  ctx->ws.top = m3;
+  uint8_t* Rb = ctx->ws.take<uint8_t>(gram_product_bytes(ctx, m, n, nm, kc, nullptr));
+  if (!Rb || !RX) return fail(ctx, BBT_ERR_NOMEM, "exact Gram: workspace");
+  const size_t split_bytes = (size_t)nm * ((m + 3) & ~3) * m;
+  int splits = 0;
+  for (long k0 = 0; k0 < n; k0 += kc) {
+    const long K = std::min(kc, n - k0);
+    BBT_TRY(crt_residues_rows(ctx, m, K, X + k0, ldx, scale, GRAM_BITS, nr, RX, Kp));
+    int sp = 1;
+    BBT_TRY(crt_product(ctx, m, m, K, nm, RX, RX, Kp, true, Rb + (size_t)splits * split_bytes, &sp));
+    splits += sp;
+  }
+  BBT_TRY(crt_combine_dd(ctx, m, m, nm, splits, Rb, true, scale, scale, 2 * (GRAM_BITS - 1), Gh, Gl, m));
+  ctx->ws.top = m2;
+  return BBT_OK;
 }
 
 bbt_status exact_local_qr(bbt_ctx* ctx, int m, long n, const double* X, const void* S, long spitch, double* R,
@@ -98,24 +181,8 @@ bbt_status exact_local_qr(bbt_ctx* ctx, int m, long n, const double* X, const vo
   BBT_TRY(shift_diag(ctx, m, Rp, m, 1e-14));
   BBT_TRY(potrf_upper(ctx, m, Rp, m, flag));
   // 2. the exact Gram of the 53-bit rows of X, as a double-double
-  {
-    const size_t m2 = ctx->ws.top;
-    const long Kp = crt_pitch(n);
-    // kept: every plane the later products with X_int^T need, the Gram using the first nm
-    const int nr = keep ? exact_keep_moduli(m, n) : nm;
-    int8_t* RX = keep ? keep : ctx->ws.take<int8_t>((size_t)nm * m * Kp);
-    const size_t m3 = ctx->ws.top;
-    BBT_TRY(crt_row_scales(ctx, m, n, X, n, scale));
-    ctx->ws.top = m3;
-    uint8_t* Rb = ctx->ws.take<uint8_t>(crt_product_bytes(ctx, m, m, n, nm, true));
-    if (!Rb || !RX) return fail(ctx, BBT_ERR_NOMEM, "exact local QR: Gram workspace");
-    BBT_TRY(crt_residues_rows(ctx, m, n, X, n, scale, GRAM_BITS, nr, RX, Kp));
-    int splits = 1;
-    BBT_TRY(crt_product(ctx, m, m, n, nm, RX, RX, Kp, true, Rb, &splits));
-    BBT_TRY(crt_combine_dd(ctx, m, m, nm, splits, Rb, true, scale, scale, 2 * (GRAM_BITS - 1), Gh, Gl, m));
-    BBT_TRY(dd_symmetrize_upper(ctx, m, Gh, Gl, m));
-    ctx->ws.top = m2;
-  }
+  BBT_TRY(exact_gram_dd(ctx, m, n, X, n, scale, keep, Gh, Gl));
+  BBT_TRY(dd_symmetrize_upper(ctx, m, Gh, Gl, m));
   // 3. G_Q = R_p^-T (R_p^-T G)^T in double-double (G symmetric)
   BBT_TRY(dd_trsm_left(ctx, true, m, m, Rp, m, Gh, Gl, m));
   BBT_TRY(dd_transpose(ctx, m, Gh, Gl, m, Th, Tl, m));
@@ -138,7 +205,8 @@ bbt_status exact_local_qr(bbt_ctx* ctx, int m, long n, const double* X, const vo
 size_t exact_apply_workspace_bytes(const bbt_ctx* ctx, long rows, int m, int k) {
   const int nm = crt_moduli(GRAM_BITS, Z_BITS, m);
   const long Kp = crt_pitch(m);
-  return (size_t)nm * (rows + k) * Kp + crt_product_bytes(ctx, (int)rows, k, m, nm, false) +
+  const long rc = apply_chunk(rows, nm, Kp, k);
+  return (size_t)nm * (rc + k) * Kp + crt_product_bytes(ctx, (int)rc, k, m, nm, false) +
          (4 * (size_t)m * k + 2 * (size_t)k) * 8 + 16384;
 }
 
@@ -190,14 +258,18 @@ bbt_status exact_apply_rows(bbt_ctx* ctx, const ExactOperand& op, long rows, con
   if (rows > 0x7fffffffL) return fail(ctx, BBT_ERR_ARG, "exact apply: rows=%ld", rows);
   const int m = op.m, k = op.k, nm = op.nm;
   const size_t mark = ctx->ws.top;
-  int8_t* RA = ctx->ws.take<int8_t>((size_t)nm * rows * op.Kp);
-  uint8_t* Rb = ctx->ws.take<uint8_t>(crt_product_bytes(ctx, (int)rows, k, m, nm, false));
+  const long rc = apply_chunk(rows, nm, op.Kp, k);   // rows are independent: chunks bound the scratch
+  int8_t* RA = ctx->ws.take<int8_t>((size_t)nm * rc * op.Kp);
+  uint8_t* Rb = ctx->ws.take<uint8_t>(crt_product_bytes(ctx, (int)rc, k, m, nm, false));
   if (!Rb) return fail(ctx, BBT_ERR_NOMEM, "exact apply: workspace");
-  BBT_TRY(crt_residues_cols(ctx, (int)rows, m, X, ldx, scale, GRAM_BITS, nm, RA, op.Kp));
-  int splits = 1;
-  BBT_TRY(crt_product(ctx, (int)rows, k, m, nm, RA, op.RB, op.Kp, false, Rb, &splits));
-  BBT_TRY(crt_combine(ctx, (int)rows, k, nm, splits, Rb, false, nullptr, op.t, (GRAM_BITS - 1) + (Z_BITS - 1), 1.0,
-                      0.0, C, ldc));
+  for (long r0 = 0; r0 < rows; r0 += rc) {
+    const int R = (int)std::min(rc, rows - r0);
+    BBT_TRY(crt_residues_cols(ctx, R, m, X + r0, ldx, scale, GRAM_BITS, nm, RA, op.Kp));
+    int splits = 1;
+    BBT_TRY(crt_product(ctx, R, k, m, nm, RA, op.RB, op.Kp, false, Rb, &splits));
+    BBT_TRY(crt_combine(ctx, R, k, nm, splits, Rb, false, nullptr, op.t, (GRAM_BITS - 1) + (Z_BITS - 1), 1.0, 0.0,
+                        C + r0, ldc));
+  }
   ctx->ws.top = mark;
   return BBT_OK;
 }
@@ -210,12 +282,16 @@ bbt_status exact_apply_planes(bbt_ctx* ctx, const ExactOperand& op, long rows, c
   if (rows > 0x7fffffffL) return fail(ctx, BBT_ERR_ARG, "exact apply: rows=%ld", rows);
   const int m = op.m, k = op.k, nm = op.nm;
   const size_t mark = ctx->ws.top;
-  uint8_t* Rb = ctx->ws.take<uint8_t>(crt_product_bytes(ctx, (int)rows, k, m, nm, false));
+  const long rc = apply_chunk(rows, nm, 0, k);   // only the product's residues are scratch here
+  uint8_t* Rb = ctx->ws.take<uint8_t>(crt_product_bytes(ctx, (int)rc, k, m, nm, false));
   if (!Rb) return fail(ctx, BBT_ERR_NOMEM, "exact apply: workspace");
-  int splits = 1;
-  BBT_TRY(crt_product_amn(ctx, (int)rows, k, m, nm, planes, pitch, op.RB, op.Kp, Rb, &splits));
-  BBT_TRY(crt_combine(ctx, (int)rows, k, nm, splits, Rb, false, nullptr, op.t, (GRAM_BITS - 1) + (Z_BITS - 1), 1.0,
-                      0.0, C, ldc));
+  for (long r0 = 0; r0 < rows; r0 += rc) {   // row chunks start at multiples of 128: 16-byte TMA offsets
+    const int R = (int)std::min(rc, rows - r0);
+    int splits = 1;
+    BBT_TRY(crt_product_amn(ctx, R, k, m, nm, planes + r0, pitch, op.RB, op.Kp, Rb, &splits));
+    BBT_TRY(crt_combine(ctx, R, k, nm, splits, Rb, false, nullptr, op.t, (GRAM_BITS - 1) + (Z_BITS - 1), 1.0, 0.0,
+                        C + r0, ldc));
+  }
   ctx->ws.top = mark;
   return BBT_OK;
 }

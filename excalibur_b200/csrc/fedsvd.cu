@@ -552,12 +552,15 @@ bbt_status fedsvd_tall(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, const Layout&
   int k = hc[0] - hc[1];
   if (cfg->top_k > 0) k = std::min(k, cfg->top_k);
   if (k < 1) return fail(ctx, BBT_ERR_COUNT, "fedsvd: no singular values in (0, bound]");
+  int ncl = 0;   // dbdsdc (modes 0, 4) keeps the vectors of tight clusters orthogonal: refine_clusters
   if ((mode == 0 || mode == 4) && k < gi) {
     BBT_TRY(bidiag_svd(ctx, k, alpha, beta, tmp, W, sigma, k, true));   // leading k x k (W is free)
+    BBT_TRY(refine_clusters(ctx, k, k, alpha, beta, sigma, tmp, W, &ncl));
     embed_leading<<<4 * ctx->num_sms, 256, 0, ctx->stream>>>(gi, k, tmp, W, Ub, Vb);
     BBT_LAUNCHED(ctx);
   } else {
     BBT_TRY(bidiag_svd(ctx, gi, alpha, beta, Ub, Vb, sigma, k, true));   // Ub g x k, Vb k x g
+    if (mode == 0 || mode == 4) BBT_TRY(refine_clusters(ctx, gi, k, alpha, beta, sigma, Ub, Vb, &ncl));
   }
   BBT_CUDA(ctx, cudaEventRecord(ev[5], ctx->stream));
   // 6) U (:1002-1015): part_c = V_b Vr_c (Q_c^T), k x m_part[c], at columns
@@ -816,15 +819,20 @@ bbt_status fedsvd(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* X, 
   int k = hc[0] - hc[1];
   if (cfg->top_k > 0) k = std::min(k, cfg->top_k);
   if (k < 1) return fail(ctx, BBT_ERR_COUNT, "fedsvd: no singular values in (0, bound]");
+  // dbdsdc (mode 0) keeps the vectors of tight clusters orthogonal where the
+  // twisted vectors collapse onto each other: refine_clusters after bidiag_svd
+  int ncl = 0;
   if (cfg->svd_mode == 0 && k < mi) {
     // dbdsdc on the leading k x k bidiagonal (client.cpp:975-980)
     double* Us = tmp;   // k x k each; the Ralha input W is free by now
     double* Vs = W;
     BBT_TRY(bidiag_svd(ctx, k, alpha, beta, Us, Vs, sigma, k, true));
+    BBT_TRY(refine_clusters(ctx, k, k, alpha, beta, sigma, Us, Vs, &ncl));
     embed_leading<<<4 * ctx->num_sms, 256, 0, ctx->stream>>>(mi, k, Us, Vs, Ub, Vb);
     BBT_LAUNCHED(ctx);
   } else {
     BBT_TRY(bidiag_svd(ctx, mi, alpha, beta, Ub, Vb, sigma, k, true));   // Ub m x k, Vb k x m
+    if (cfg->svd_mode == 0) BBT_TRY(refine_clusters(ctx, mi, k, alpha, beta, sigma, Ub, Vb, &ncl));
   }
   BBT_CUDA(ctx, cudaEventRecord(ev[5], ctx->stream));
   // 6) U: FinalU (m x k row-major) = (V_b Vr)^T, unmasked (client.cpp:1018, 1071-1115)

@@ -217,6 +217,10 @@ bbt_status ralha(bbt_ctx* ctx, int m, int n, double* W, double* house, double* t
                  double* beta, double* V, double* cs);
 
 // Small helpers (util.cu)
+// Scratch cap (bytes) of the chunked passes over a long dimension (the
+// sketch's bf16 pieces, the CRT residue planes, the Ozaki slices): dflt, or
+// the environment's EXCALIBUR_B200_CHUNK_BYTES (at least 1 MiB) when set.
+size_t long_chunk_bytes(size_t dflt);
 bbt_status transpose(bbt_ctx* ctx, int rows, int cols, const double* src, long lds, double* dst,
                      long ldd);   // dst (cols x rows, row-major) = src^T
 bbt_status copy2d(bbt_ctx* ctx, int rows, int cols, const double* src, long lds, double* dst,
@@ -313,6 +317,12 @@ size_t exact_qr_workspace_bytes(const bbt_ctx* ctx, int m, long n);
 // with X_int^T (exact_apply_planes): their count and bytes for an m x n block.
 int exact_keep_moduli(int m, long n);
 size_t exact_keep_bytes(int m, long n);
+// The exact Gram of X's 53-bit rows as a double-double (upper triangle, ld m),
+// the row scales written to scale; keep: residue planes to fill and keep (or
+// null: chunked scratch planes).
+size_t exact_gram_workspace_bytes(const bbt_ctx* ctx, int m, long n);
+bbt_status exact_gram_dd(bbt_ctx* ctx, int m, long n, const double* X, long ldx, double* scale, int8_t* keep,
+                         double* Gh, double* Gl);
 bbt_status exact_local_qr(bbt_ctx* ctx, int m, long n, const double* X, const void* S, long spitch, double* R,
                           double* W, double* Rp, double* scale,
                           int8_t* keep = nullptr);

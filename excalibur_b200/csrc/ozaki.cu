@@ -417,7 +417,20 @@ bbt_status slices(bbt_ctx* ctx, int rows, long K, const double* X, long rs, long
 
 }  // namespace
 
+// Row chunk of a product whose A slices exceed this many bytes (rows of C are
+// independent; B's slices are formed again per chunk).
+constexpr size_t OZ_CHUNK_DEFAULT = (size_t)6 << 30;
+int oz_row_chunk(int M, long K) {
+  const size_t cap = long_chunk_bytes(OZ_CHUNK_DEFAULT);
+  const size_t per_row = (size_t)OS * pitch16(K);
+  if ((size_t)M * per_row <= cap) return M;
+  const long c = std::max(128L, (long)(cap / per_row) / 128 * 128);
+  const long chunks = (M + c - 1) / c;
+  return (int)(((M + chunks - 1) / chunks + 127) / 128 * 128);
+}
+
 size_t oz_workspace_bytes(const bbt_ctx* ctx, int M, int N, long K, bool same) {
+  if (!same) M = oz_row_chunk(M, K);
   const long Kp = pitch16(K);
   const int sms = ctx->num_sms > 0 ? ctx->num_sms : 148;
   const int splits = std::max(plan(M, N, K, sms, false).splits, plan(M, N, K, sms, true).splits);
@@ -432,11 +445,31 @@ bool oz_worthwhile(int M, int N, long K) {
   return M >= 128 && N >= 64 && K >= 768 && (double)M * N * K >= 4e9;
 }
 
+namespace {
+bbt_status gemm_oz_one(bbt_ctx* ctx, int M, int N, long K, double alpha, const double* A, long rsA, long csA,
+                       const double* B, long rsB, long csB, double beta, double* C, long ldc, bool same, bool upper,
+                       int S);
+}  // namespace
+
 bbt_status gemm_oz(bbt_ctx* ctx, int M, int N, long K, double alpha, const double* A, long rsA, long csA,
                    const double* B, long rsB, long csB, double beta, double* C, long ldc, bool same, bool upper,
                    int S) {
   if (S < 4 || S > OS) return fail(ctx, BBT_ERR_ARG, "ozaki: %d slices (4..8)", S);
   if (M < 1 || N < 1 || K < 1 || K > (1L << 31) - TK) return fail(ctx, BBT_ERR_ARG, "ozaki: M=%d N=%d K=%ld", M, N, K);
+  if (!same && !upper) {   // a long A: row chunks of bounded slice scratch (rows of C are independent)
+    const int rc = oz_row_chunk(M, K);
+    for (long r0 = 0; r0 < M; r0 += rc)
+      BBT_TRY(gemm_oz_one(ctx, (int)std::min<long>(rc, M - r0), N, K, alpha, A + r0 * rsA, rsA, csA, B, rsB, csB,
+                          beta, C + r0, ldc, false, false, S));
+    return BBT_OK;
+  }
+  return gemm_oz_one(ctx, M, N, K, alpha, A, rsA, csA, B, rsB, csB, beta, C, ldc, same, upper, S);
+}
+
+namespace {
+bbt_status gemm_oz_one(bbt_ctx* ctx, int M, int N, long K, double alpha, const double* A, long rsA, long csA,
+                       const double* B, long rsB, long csB, double beta, double* C, long ldc, bool same, bool upper,
+                       int S) {
   EncodeTiled enc = encode_fn();
   if (!enc) return fail(ctx, BBT_ERR_CUDA, "ozaki: cuTensorMapEncodeTiled is not available");
   const long Kp = pitch16(K);
@@ -504,5 +537,6 @@ bbt_status gemm_oz(bbt_ctx* ctx, int M, int N, long K, double alpha, const doubl
   ctx->ws.top = mark;
   return BBT_OK;
 }
+}  // namespace
 
 }  // namespace bbt

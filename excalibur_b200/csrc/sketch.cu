@@ -247,11 +247,14 @@ __global__ void rademacher_kernel(int N, long n, long pitch, __nv_bfloat16* __re
   }
 }
 
-__global__ void sketch_reduce(long MN, int splits, const double* __restrict__ part, double* __restrict__ Y) {
+// Y = sum of the K-splits' partial products (accumulate: Y += the sum, for
+// every K-chunk after the first).
+__global__ void sketch_reduce(long MN, int splits, const double* __restrict__ part, double* __restrict__ Y,
+                              int accumulate) {
   for (long f = blockIdx.x * (long)blockDim.x + threadIdx.x; f < MN; f += (long)gridDim.x * blockDim.x) {
     double s = 0.0;
     for (int z = 0; z < splits; ++z) s += part[(size_t)z * MN + f];
-    Y[f] = s;
+    Y[f] = accumulate ? Y[f] + s : s;
   }
 }
 
@@ -303,9 +306,27 @@ long sketch_pitch(long n) { return (n + 7) / 8 * 8; }
 
 int sketch_rows(int m) { return (2 * m + TN - 1) / TN * TN; }
 
+namespace {
+// The bf16 pieces of X are staged in HBM; over a long dimension they are
+// formed in K-chunks of at most this many bytes (multiples of 2^15 columns),
+// each chunk's products added into Y, so a block of any length needs bounded
+// workspace.
+constexpr size_t PIECES_CHUNK_DEFAULT = (size_t)4 << 30;
+long sketch_chunk(int m, long n) {
+  const size_t cap = long_chunk_bytes(PIECES_CHUNK_DEFAULT);
+  const size_t full = (size_t)PIECES * m * sketch_pitch(n) * 2;
+  if (full <= cap) return n;
+  long c = (long)(cap / ((size_t)PIECES * m * 2)) / 32768 * 32768;
+  c = std::max(c, 32768L);
+  const long chunks = (n + c - 1) / c;
+  return ((n + chunks - 1) / chunks + 32767) / 32768 * 32768;
+}
+}  // namespace
+
 size_t sketch_workspace_bytes(const bbt_ctx* ctx, int m, long n, int N) {
-  const Split s = plan_split(m, n, N, ctx->num_sms > 0 ? ctx->num_sms : 148);
-  return (size_t)PIECES * m * sketch_pitch(n) * 2 + (size_t)s.splits * m * N * 8 + 4096;
+  const long kc = sketch_chunk(m, n);
+  const Split s = plan_split(m, kc, N, ctx->num_sms > 0 ? ctx->num_sms : 148);
+  return (size_t)PIECES * m * sketch_pitch(kc) * 2 + (size_t)s.splits * m * N * 8 + 4096;
 }
 
 bbt_status rademacher(bbt_ctx* ctx, int N, long n, void* S, uint64_t seed) {
@@ -317,6 +338,9 @@ bbt_status rademacher(bbt_ctx* ctx, int N, long n, void* S, uint64_t seed) {
   return BBT_OK;
 }
 
+bbt_status sketch_chunk_run(bbt_ctx* ctx, int m, long n, const double* X, long ldx, int N, const __nv_bfloat16* S,
+                            long spitch, double* Y, __nv_bfloat16* A, double* part, bool accumulate);
+
 // Stream-ordered; a pipeline wait that gave up leaves a nonzero code in
 // ctx->d_flag[FLAG_SKETCH] (cleared and read by the caller).
 bbt_status sketch_bf16x3(bbt_ctx* ctx, int m, long n, const double* X, long ldx, int N, const void* S, long spitch,
@@ -325,12 +349,26 @@ bbt_status sketch_bf16x3(bbt_ctx* ctx, int m, long n, const double* X, long ldx,
     return fail(ctx, BBT_ERR_ARG, "sketch: m=%d n=%ld N=%d", m, n, N);
   EncodeTiled enc = encode_fn();
   if (!enc) return fail(ctx, BBT_ERR_CUDA, "sketch: cuTensorMapEncodeTiled is not available");
+  const long kc = sketch_chunk(m, n);
+  const size_t mark = ctx->ws.top;
+  const long cpitch = sketch_pitch(kc);
+  __nv_bfloat16* A = ctx->ws.take<__nv_bfloat16>((size_t)PIECES * m * cpitch);
+  double* part = ctx->ws.take<double>((size_t)plan_split(m, kc, N, ctx->num_sms).splits * m * N);
+  if (!part) return fail(ctx, BBT_ERR_NOMEM, "sketch: workspace");
+  for (long k0 = 0; k0 < n; k0 += kc)   // chunk offsets are multiples of 2^15: 16-byte TMA bases in S
+    BBT_TRY(sketch_chunk_run(ctx, m, std::min(kc, n - k0), X + k0, ldx, N,
+                             static_cast<const __nv_bfloat16*>(S) + k0, spitch, Y, A, part, k0 > 0));
+  ctx->ws.top = mark;
+  return BBT_OK;
+}
+
+// One K-chunk of sketch_bf16x3: its bf16 pieces in A (pitch sketch_pitch(n)),
+// the products of its K-splits in part, summed into Y (added with accumulate).
+bbt_status sketch_chunk_run(bbt_ctx* ctx, int m, long n, const double* X, long ldx, int N, const __nv_bfloat16* S,
+                            long spitch, double* Y, __nv_bfloat16* A, double* part, bool accumulate) {
+  EncodeTiled enc = encode_fn();
   const long pitch = sketch_pitch(n);
   const Split sp = plan_split(m, n, N, ctx->num_sms);
-  const size_t mark = ctx->ws.top;
-  __nv_bfloat16* A = ctx->ws.take<__nv_bfloat16>((size_t)PIECES * m * pitch);
-  double* part = ctx->ws.take<double>((size_t)sp.splits * m * N);
-  if (!part) return fail(ctx, BBT_ERR_NOMEM, "sketch: workspace");
   split3_kernel<<<dim3((unsigned)std::max(1L, std::min((n + 255) / 256, 16L)), (unsigned)std::min(m, 65535)), 256, 0,
                   ctx->stream>>>(m, n, X, ldx, A, pitch);
   BBT_LAUNCHED(ctx);
@@ -349,7 +387,7 @@ bbt_status sketch_bf16x3(bbt_ctx* ctx, int m, long n, const double* X, long ldx,
     const cuuint64_t dims[2] = {(cuuint64_t)n, (cuuint64_t)N};
     const cuuint64_t strides[1] = {(cuuint64_t)spitch * 2};
     const cuuint32_t box[2] = {TK, TN}, es[2] = {1, 1};
-    if (enc(&tb, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(S), dims, strides, box, es,
+    if (enc(&tb, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<__nv_bfloat16*>(S), dims, strides, box, es,
             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
       return fail(ctx, BBT_ERR_CUDA, "sketch: tensor map of S");
@@ -372,9 +410,8 @@ bbt_status sketch_bf16x3(bbt_ctx* ctx, int m, long n, const double* X, long ldx,
     BBT_LAUNCHED(ctx);
   }
   const long MN = (long)m * N;
-  sketch_reduce<<<4 * ctx->num_sms, 256, 0, ctx->stream>>>(MN, sp.splits, part, Y);
+  sketch_reduce<<<4 * ctx->num_sms, 256, 0, ctx->stream>>>(MN, sp.splits, part, Y, accumulate ? 1 : 0);
   BBT_LAUNCHED(ctx);
-  ctx->ws.top = mark;
   return BBT_OK;
 }
 

@@ -254,7 +254,9 @@ bbt_status twisted(bbt_ctx* ctx, int n, int cnt, const double* sigma, const doub
   double* UPa = ctx->ws.take<double>(col);
   double* Vt = ctx->ws.take<double>((size_t)n * cnt);
   signed char* vs = ctx->ws.take<signed char>(cnt);
-  if (!vs) return fail(ctx, BBT_ERR_NOMEM, "twisted: workspace (%zu MB)", (col * 7 * 8) >> 20);
+  if (!vs)
+    return fail(ctx, BBT_ERR_NOMEM, "twisted: workspace (%zu MB)",
+                ((2 * (size_t)n + 6 * col + (size_t)n * cnt) * 8 + cnt) >> 20);
   ProfScope prof(ctx, BBT_PROF_TWISTED, 0.0);
   ldl_kernel<<<1, 1, 0, ctx->stream>>>(n, a, b, L, D);
   BBT_LAUNCHED(ctx);

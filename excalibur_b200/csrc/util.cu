@@ -1,9 +1,23 @@
 // Small layout kernels shared by the pipeline.
 #include <cuda_runtime.h>
 
+#include <cstdlib>
+
 #include "internal.h"
 
 namespace bbt {
+
+// Scratch cap of the passes over a long dimension.  EXCALIBUR_B200_CHUNK_BYTES
+// (bytes, read at every call) overrides the default, e.g. to bound the
+// workspace further on a device shared with other work.
+size_t long_chunk_bytes(size_t dflt) {
+  const char* v = std::getenv("EXCALIBUR_B200_CHUNK_BYTES");
+  if (!v || !*v) return dflt;
+  char* end = nullptr;
+  const unsigned long long b = std::strtoull(v, &end, 10);
+  return (end && *end == 0 && b >= ((size_t)1 << 20)) ? (size_t)b : dflt;
+}
+
 namespace {
 
 // dst (cols x rows, row-major, ld ldd) = src^T, src rows x cols row-major (ld lds).

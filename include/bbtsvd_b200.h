@@ -92,13 +92,16 @@ bbt_status bbt_bidiagonal_svd(bbt_ctx* ctx, int k, const double* d_alpha, const 
 /* bbt_twisted_vectors for callers that must not allocate device memory (an
  * allocation-free hot loop, memory handed in full to another allocator, a
  * zero allocation budget).  No counterpart in the reference: an addition.
- * Takes a cudaStream_t (as void*; NULL = the default stream) instead of a
- * context and keeps its work arrays in one static 64 MiB __device__ array
- * that every GPU loading the library holds until exit.  Needs about
- * 7*(n+1)*cnt + n*cnt doubles of it; larger shapes return BBT_ERR_ARG with a
- * message on stderr.  The first call on a device looks up the array's
- * device address (cudaGetSymbolAddress, with that device current); make
- * that first call before any stream capture.  All calls share the array and
+ * Takes a cudaStream_t (as void*; NULL = the default stream) of the current
+ * device (another device's stream returns BBT_ERR_ARG) instead of a context
+ * and keeps its work arrays in one static 64 MiB __device__ array that every
+ * GPU loading the library holds until exit.  Needs 2n + 6(n+1)cnt + n*cnt
+ * doubles of it (each of its arrays rounded up to 256 bytes; n = cnt = 1094
+ * fits, 1095 does not); larger shapes return BBT_ERR_ARG with a message on
+ * stderr.  The first call in each CUDA context looks up the array's device
+ * address (cudaGetSymbolAddress, with that device current), and again after
+ * the context is recreated (cudaDeviceReset); make that first call before
+ * any stream capture.  All calls share the array and
  * it keeps the last call's contents (every work array is written before it
  * is read, so nothing needs clearing); calls that overlap on the GPU race.
  * Same results as bbt_twisted_vectors. */

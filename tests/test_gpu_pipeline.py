@@ -136,3 +136,49 @@ def test_autotuned_batched_local_qr(ctx):
     s, U, VT = ctx.fedsvd([ctx._dev(b.copy()) for b in blocks], pub, priv)
     assert np.max(np.abs(s.cpu().numpy() - so) / so) < 1e-12
     assert np.max(np.abs(U.cpu().numpy() - Uo)) < 1e-9
+
+
+def _clustered_blocks(rng, m, n, P, clusters, size, gap=1e-10, lo=1e-3):
+    """X = Ux diag(s) Vx^T (m x P n) with `clusters` clusters of `size` values
+    at relative spacing `gap`, centres log-uniform in [lo, 1]; blocks X_c."""
+    c = np.exp(rng.uniform(np.log(lo), 0.0, clusters))
+    sv = np.sort(np.concatenate([ci * (1.0 + gap * np.arange(size)) for ci in c]))[::-1]
+    sv = np.concatenate([sv, np.geomspace(lo / 2, lo / 4, m - len(sv))]) if len(sv) < m else sv
+    Ux, _ = np.linalg.qr(rng.standard_normal((m, m)))
+    Vx, _ = np.linalg.qr(rng.standard_normal((P * n, m)))
+    X = (Ux * sv) @ Vx.T
+    return [X[:, c * n:(c + 1) * n].copy() for c in range(P)], sv
+
+
+@pytest.mark.parametrize("top_k", [-1, 40])
+def test_pipeline_mode0_clustered_orthogonal(ctx, top_k):
+    """svd_mode 0 stands in for the reference's dbdsdc (client.cpp:975-980),
+    which keeps singular vectors orthogonal inside tight clusters.  Clusters
+    of 16 values at relative spacing 1e-10: the vectors of every cluster are
+    orthonormal to 1e-12 (the twisted vectors alone collapse onto each
+    other), and each cluster's left and right subspaces match LAPACK's to the
+    gap-aware bar max(1e-8, 100 eps ||X|| / gap)."""
+    rng = np.random.default_rng(77)
+    m, n, P = 96, 700, 2
+    blocks, sv = _clustered_blocks(rng, m, n, P, clusters=5, size=16)
+    s, U, VT = run(ctx, blocks, 8, top_k=top_k, svd_mode=0)
+    X = np.concatenate(blocks, axis=1)
+    Ul, sl, Vl = np.linalg.svd(X, full_matrices=False)
+    k = len(s)
+    assert k == (m if top_k < 0 else top_k)
+    assert np.max(np.abs(s - sl[:k])) < 1e-12 * sl[0]
+    V = np.concatenate(VT, axis=1).T
+    assert np.all(np.isfinite(U[:, :k])) and np.all(np.isfinite(V[:, :k]))
+    eps = np.finfo(float).eps
+    groups = [g for g in gap_groups(sl[:k], rel_gap=1e-7)]
+    for g in groups:
+        if len(g) < 2 or g[-1] >= k:
+            continue
+        assert np.max(np.abs(U[:, g].T @ U[:, g] - np.eye(len(g)))) < 1e-12
+        assert np.max(np.abs(V[:, g].T @ V[:, g] - np.eye(len(g)))) < 1e-12
+        lo_gap = sl[g[-1]] - sl[g[-1] + 1] if g[-1] + 1 < len(sl) else sl[g[-1]]
+        hi_gap = sl[g[0] - 1] - sl[g[0]] if g[0] > 0 else np.inf
+        bar = max(1e-8, 100 * eps * sl[0] / min(lo_gap, hi_gap))
+        if g[-1] + 1 < k or top_k < 0:
+            assert subspace_angle(U[:, g], Ul[:, g]) < bar
+            assert subspace_angle(V[:, g], Vl[g].T) < bar
