@@ -102,6 +102,12 @@ class Context:
     def _pre(self):
         self.torch.cuda.synchronize(self.device)   # inputs written by torch are complete
 
+    def set_stream(self, stream=None):
+        """Launch on a borrowed CUDA stream (a torch.cuda.Stream or a raw
+        cudaStream_t handle); None returns to the context's own stream."""
+        h = None if stream is None else getattr(stream, "cuda_stream", stream)
+        self._check(self.L.bbt_set_stream(self.h, C.c_void_p(h) if h else None), "set_stream")
+
     # -- bbtsvd.hpp ---------------------------------------------------------
     def negative_count(self, alpha, beta, mu):
         """Sturm counts at every shift in mu (bbtsvd.cpp:7-17)."""

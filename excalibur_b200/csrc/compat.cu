@@ -6,11 +6,13 @@
 // The masks draw their random tables on the host with the same calls as the
 // reference, so glibc's rand() state after a call is the reference's.
 //
-// Functions the reference declares but never calls from client.cpp (the dead
-// mask variants and the opt_control 0/2 dense mask) abort with a message
-// instead of silently computing on the CPU.
+// Functions the reference declares but never calls from client.cpp with
+// opt_control 1/3 (the unused mask variants, the random orthogonal matrix
+// generators and the opt_control 0/2 dense mask) abort with a message instead
+// of silently computing on the CPU.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <mutex>
@@ -201,18 +203,188 @@ void find_best_convert(struct SquareMaskConvert* smc) {
   }
 }
 
-// ---- declared by bbtsvd.hpp, not on the run() path (see file comment) ----
-void ldl_decomposition(int, double*, double*, double*, double*) { not_provided("ldl_decomposition"); }
-void inverse_iteration(int, int, double*, double*, double*, int) { not_provided("inverse_iteration"); }
-void dstqds(int, double*, double*, double, double*, double*, double*) { not_provided("dstqds"); }
-void dpqds(int, double*, double*, double, double*, double*, double*) { not_provided("dpqds"); }
-void one_pair_singular_vector_twisted_factorization(int, int, double, double*, double*, double*, double*, double*,
-                                                    double*) {
-  not_provided("one_pair_singular_vector_twisted_factorization");
+// ---- the qd / twisted-factorisation steps and the small vector helpers ----
+// (bbtsvd.cpp:54-136, 149-164, 970-978).  Each is an O(n) recurrence or an
+// elementwise rotation, run on the device (one thread for a recurrence) in
+// the reference's order of operations, every product and sum rounded
+// separately; host arrays are staged as for the functions above.
+namespace {
+
+#define MUL __dmul_rn
+#define DIV __ddiv_rn
+#define ADD __dadd_rn
+#define SUB __dsub_rn
+
+// bbtsvd.cpp:73-81
+__global__ void dstqds_kernel(int n, const double* l, const double* d, double tau, double* lp, double* dp,
+                              double* s) {
+  if (blockIdx.x || threadIdx.x) return;
+  double si = -tau;
+  s[0] = si;
+  for (int i = 0; i + 1 < n; ++i) {
+    const double dpi = ADD(d[i], si);
+    dp[i] = dpi;
+    const double lpi = DIV(MUL(d[i], l[i]), dpi);
+    lp[i] = lpi;
+    si = SUB(MUL(MUL(lpi, l[i]), si), tau);
+    s[i + 1] = si;
+  }
+  dp[n - 1] = ADD(d[n - 1], si);
 }
-void generate_house(int, double*, int, double*) { not_provided("generate_house"); }
+
+// bbtsvd.cpp:83-91
+__global__ void dpqds_kernel(int n, const double* l, const double* d, double tau, double* up, double* rp,
+                             double* p) {
+  if (blockIdx.x || threadIdx.x) return;
+  double pi = SUB(d[n - 1], tau);
+  p[n - 1] = pi;
+  for (int i = n - 2; i >= 0; --i) {
+    const double r = ADD(MUL(d[i], MUL(l[i], l[i])), pi);
+    rp[i + 1] = r;
+    up[i] = DIV(MUL(l[i], d[i]), r);
+    pi = SUB(DIV(MUL(pi, d[i]), r), tau);
+    p[i] = pi;
+  }
+  rp[0] = pi;
+}
+
+// bbtsvd.cpp:149-164: x <- the Householder vector (x[0] = 1 after the
+// scaling), *beta its coefficient; sigma summed in index order.
+__global__ void house_kernel(int n, double* x, long inc, double* beta) {
+  if (blockIdx.x || threadIdx.x) return;
+  double sigma = 0.0;
+  for (int i = 1; i < n; ++i) sigma = ADD(sigma, MUL(x[i * inc], x[i * inc]));
+  const double x0 = x[0];
+  x[0] = 1.0;
+  if (sigma == 0.0 && x0 >= 0.0) {
+    *beta = 0.0;
+  } else if (sigma == 0.0 && x0 < 0.0) {
+    *beta = 2.0;
+  } else {
+    const double mu = sqrt(ADD(MUL(x0, x0), sigma));   // pow(., 0.5): the correctly rounded square root
+    const double h = (x0 <= 0.0) ? SUB(x0, mu) : DIV(-sigma, ADD(x0, mu));
+    x[0] = h;
+    const double h2 = MUL(h, h);
+    *beta = DIV(MUL(2.0, h2), ADD(sigma, h2));
+    const double r = DIV(1.0, h);   // cblas_dscal(n, 1 / x[0], x, incX)
+    for (int i = 0; i < n; ++i) x[i * inc] = MUL(x[i * inc], r);
+  }
+}
+
+// bbtsvd.cpp:970-978: (x, y) <- (x c + y s, x (-s) + y c), elementwise
+__global__ void drot_kernel(size_t n, double* x, size_t incx, double* y, size_t incy, double c, double s) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const double xi = x[i * incx], yi = y[i * incy];
+    x[i * incx] = ADD(MUL(xi, c), MUL(yi, s));
+    y[i * incy] = ADD(MUL(xi, -s), MUL(yi, c));
+  }
+}
+
+void launched(bbt_ctx* c, const char* what) {
+  c->launches++;
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) die(what, bbt::cuda_fail(c, e, "kernel launch"));
+}
+
+void sync(bbt_ctx* c, const char* what) {
+  const bbt_status s = bbt_synchronize(c);
+  if (s != BBT_OK) die(what, s);
+}
+
+#undef MUL
+#undef DIV
+#undef ADD
+#undef SUB
+
+}  // namespace
+
+void ldl_decomposition(int n, double* x_diagonal, double* x_upper_diagonal, double* l, double* d) {
+  bbt_ctx* c = ctx();
+  Dev da(x_diagonal, n), db(x_upper_diagonal, n > 1 ? n - 1 : 0), dl(nullptr, n > 1 ? n - 1 : 0), dd(nullptr, n);
+  bbt_status s = bbt::ldl_factor(c, n, da.p, db.p, dl.p, dd.p);
+  if (s != BBT_OK) die("ldl_decomposition", s);
+  sync(c, "ldl_decomposition");
+  dl.back(l, n > 1 ? n - 1 : 0);
+  dd.back(d, n);
+}
+
+// v (stride ldv) gets the normalised inverse-iteration vector twisted at k;
+// the reference normalises with BLAS dnrm2, this library with the scaled sum
+// of squares, so the two agree to rounding.
+void inverse_iteration(int n, int k, double* l, double* u, double* v, int ldv) {
+  bbt_ctx* c = ctx();
+  const size_t span = (size_t)(n - 1) * ldv + 1;
+  Dev dl(l, n > 1 ? n - 1 : 0), du(u, n > 1 ? n - 1 : 0), dv(v, span);
+  bbt_status s = bbt::inverse_iteration_dev(c, n, k, dl.p, du.p, dv.p, ldv);
+  if (s != BBT_OK) die("inverse_iteration", s);
+  sync(c, "inverse_iteration");
+  dv.back(v, span);
+}
+
+void dstqds(int n, double* l, double* d, double tau, double* l_plus, double* d_plus, double* s) {
+  bbt_ctx* c = ctx();
+  Dev dl(l, n > 1 ? n - 1 : 0), dd(d, n), lp(nullptr, n > 1 ? n - 1 : 0), dp(nullptr, n), ds(nullptr, n);
+  dstqds_kernel<<<1, 1, 0, c->stream>>>(n, dl.p, dd.p, tau, lp.p, dp.p, ds.p);
+  launched(c, "dstqds");
+  sync(c, "dstqds");
+  lp.back(l_plus, n > 1 ? n - 1 : 0);
+  dp.back(d_plus, n);
+  ds.back(s, n);
+}
+
+void dpqds(int n, double* l, double* d, double tau, double* u_plus, double* r_plus, double* p) {
+  bbt_ctx* c = ctx();
+  Dev dl(l, n > 1 ? n - 1 : 0), dd(d, n), up(nullptr, n > 1 ? n - 1 : 0), rp(nullptr, n), dp(nullptr, n);
+  dpqds_kernel<<<1, 1, 0, c->stream>>>(n, dl.p, dd.p, tau, up.p, rp.p, dp.p);
+  launched(c, "dpqds");
+  sync(c, "dpqds");
+  up.back(u_plus, n > 1 ? n - 1 : 0);
+  rp.back(r_plus, n);
+  dp.back(p, n);
+}
+
+// v (n, contiguous) and u (stride omege_count) of one singular value omega
+// from the LDL^T factors l, d of B^T B (bbtsvd.cpp:93-136).
+void one_pair_singular_vector_twisted_factorization(int n, int omege_count, double omega, double* l, double* d,
+                                                    double* x_diagonal, double* x_upper_diagonal, double* v,
+                                                    double* u) {
+  bbt_ctx* c = ctx();
+  const size_t uspan = (size_t)(n - 1) * omege_count + 1;
+  Dev dl(l, n > 1 ? n - 1 : 0), dd(d, n), da(x_diagonal, n), db(x_upper_diagonal, n > 1 ? n - 1 : 0);
+  Dev dom(&omega, 1), dv(nullptr, n), du(u, uspan), scr(nullptr, bbt::twisted_pair_scratch_doubles(n));
+  bbt_status s = bbt::twisted_pair(c, n, dom.p, dl.p, dd.p, da.p, db.p, dv.p, du.p, omege_count, scr.p);
+  if (s != BBT_OK) die("one_pair_singular_vector_twisted_factorization", s);
+  sync(c, "one_pair_singular_vector_twisted_factorization");
+  dv.back(v, n);
+  du.back(u, uspan);
+}
+
+void generate_house(int n, double* x, int incX, double* beta) {
+  bbt_ctx* c = ctx();
+  const size_t span = n > 0 ? (size_t)(n - 1) * incX + 1 : 0;
+  Dev dx(x, span), db(nullptr, 1);
+  house_kernel<<<1, 1, 0, c->stream>>>(n, dx.p, incX, db.p);
+  launched(c, "generate_house");
+  sync(c, "generate_house");
+  dx.back(x, span);
+  db.back(beta, 1);
+}
+
+void mmap_drot(size_t n, double* x, size_t incX, double* y, size_t incY, double c_, double s_) {
+  if (n == 0) return;
+  bbt_ctx* c = ctx();
+  const size_t sx = (n - 1) * incX + 1, sy = (n - 1) * incY + 1;
+  Dev dx(x, sx), dy(y, sy);
+  const unsigned g = (unsigned)std::min<size_t>((n + 255) / 256, 8 * (size_t)c->num_sms);
+  drot_kernel<<<g, 256, 0, c->stream>>>(n, dx.p, incX, dy.p, incY, c_, s_);
+  launched(c, "mmap_drot");
+  sync(c, "mmap_drot");
+  dx.back(x, sx);
+  dy.back(y, sy);
+}
+
+// ---- declared by bbtsvd.hpp, not on the run() path (see file comment) ----
 void house_mask(size_t, size_t, size_t, double*, bool, bool, unsigned int) { not_provided("house_mask"); }
-void mmap_drot(size_t, double*, size_t, double*, size_t, double, double) { not_provided("mmap_drot"); }
 void householder_reflector_mask(size_t, size_t, size_t, double*, bool, bool, unsigned int) {
   not_provided("householder_reflector_mask");
 }

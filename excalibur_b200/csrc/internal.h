@@ -160,6 +160,16 @@ bbt_status bidiag_svd(bbt_ctx* ctx, int k, const double* a, const double* b, dou
 size_t scratch_doubles_twisted(int n, int cnt);
 bbt_status twisted_scratch(bbt_ctx* ctx, int n, int cnt, const double* sigma, const double* a,
                            const double* b, double* U, int ldu, double* V, double* scratch);
+// The reference's per-step helpers on device arrays (bbtsvd.cpp:54-136):
+// LDL^T of B^T B (L n-1, D n), one inverse iteration (v[k ldv] = 1, backward
+// with l, forward with u, normalised), one singular pair at *omega (device)
+// from the given L, D: v contiguous (n), u with stride ldu; scratch holds
+// twisted_pair_scratch_doubles(n) doubles.
+bbt_status ldl_factor(bbt_ctx* ctx, int n, const double* a, const double* b, double* L, double* D);
+bbt_status inverse_iteration_dev(bbt_ctx* ctx, int n, int k, const double* l, const double* u, double* v, long ldv);
+size_t twisted_pair_scratch_doubles(int n);
+bbt_status twisted_pair(bbt_ctx* ctx, int n, const double* omega, const double* L, const double* D, const double* a,
+                        const double* b, double* v, double* u, int ldu, double* scratch);
 // d_out[0] = ||a||^2 + ||b||^2 (the bisection bound, bbtsvd.cpp:936)
 bbt_status bidiag_bound(bbt_ctx* ctx, int n, const double* a, const double* b, double* d_out);
 

@@ -236,7 +236,44 @@ __global__ void bound_kernel(int n, const double* __restrict__ a, const double* 
   out[0] = ADD(MUL(x, x), MUL(y, y));
 }
 
+// bbtsvd.cpp:65-71 (inverse_iteration) on one vector: twisted_solve.
+__global__ void inverse_iteration_kernel(int n, int k, const double* __restrict__ l, const double* __restrict__ u,
+                                         double* __restrict__ v, long ldv) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  twisted_solve(n, k, l, u, 1, v, ldv);
+}
+
 }  // namespace
+
+// The reference's per-step helpers on device arrays (the bbtsvd.hpp entry
+// points of the compatibility layer): LDL^T of B^T B, one inverse
+// iteration, and one singular pair by the twisted factorisation (no sign
+// rule: bbtsvd.cpp:93-136 leaves it to the driver).
+bbt_status ldl_factor(bbt_ctx* ctx, int n, const double* a, const double* b, double* L, double* D) {
+  ldl_kernel<<<1, 1, 0, ctx->stream>>>(n, a, b, L, D);
+  BBT_LAUNCHED(ctx);
+  return BBT_OK;
+}
+
+bbt_status inverse_iteration_dev(bbt_ctx* ctx, int n, int k, const double* l, const double* u, double* v, long ldv) {
+  if (n < 1 || k < 0 || k >= n) return fail(ctx, BBT_ERR_ARG, "inverse iteration: n=%d k=%d", n, k);
+  inverse_iteration_kernel<<<1, 1, 0, ctx->stream>>>(n, k, l, u, v, ldv);
+  BBT_LAUNCHED(ctx);
+  return BBT_OK;
+}
+
+size_t twisted_pair_scratch_doubles(int n) { return 6 * ((size_t)n + 1) + 1; }
+
+bbt_status twisted_pair(bbt_ctx* ctx, int n, const double* omega, const double* L, const double* D, const double* a,
+                        const double* b, double* v, double* u, int ldu, double* scratch) {
+  if (n < 1) return fail(ctx, BBT_ERR_ARG, "twisted pair: n=%d", n);
+  const size_t c = (size_t)n + 1;
+  double* p = scratch;
+  twisted_kernel<<<1, 32, 0, ctx->stream>>>(n, 1, omega, a, b, L, D, p, p + c, p + 2 * c, p + 3 * c, p + 4 * c,
+                                            p + 5 * c, v, u, ldu, reinterpret_cast<signed char*>(p + 6 * c), 0);
+  BBT_LAUNCHED(ctx);
+  return BBT_OK;
+}
 
 bbt_status twisted(bbt_ctx* ctx, int n, int cnt, const double* sigma, const double* a,
                    const double* b, double* U, int ldu, double* V, bool sign_fix) {

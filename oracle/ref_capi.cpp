@@ -25,5 +25,22 @@ void ref_givens_mask(size_t m, size_t n, size_t t, double* x, int mask, int is_l
 void ref_block_shift_mask(size_t m, size_t n, size_t t, double* x, int mask, int is_left, unsigned seed) {
   block_shift_mask(m, n, t, x, mask != 0, is_left != 0, seed);
 }
+void ref_ldl(int n, double* a, double* b, double* l, double* d) { ldl_decomposition(n, a, b, l, d); }
+void ref_inverse_iteration(int n, int k, double* l, double* u, double* v, int ldv) {
+  inverse_iteration(n, k, l, u, v, ldv);
+}
+void ref_dstqds(int n, double* l, double* d, double tau, double* lp, double* dp, double* s) {
+  dstqds(n, l, d, tau, lp, dp, s);
+}
+void ref_dpqds(int n, double* l, double* d, double tau, double* up, double* rp, double* p) {
+  dpqds(n, l, d, tau, up, rp, p);
+}
+void ref_one_pair(int n, int cnt, double omega, double* l, double* d, double* a, double* b, double* v, double* u) {
+  one_pair_singular_vector_twisted_factorization(n, cnt, omega, l, d, a, b, v, u);
+}
+void ref_generate_house(int n, double* x, int inc, double* beta) { generate_house(n, x, inc, beta); }
+void ref_mmap_drot(size_t n, double* x, size_t incx, double* y, size_t incy, double c, double s) {
+  mmap_drot(n, x, incx, y, incy, c, s);
+}
 void ref_set_threads(int n) { omp_set_num_threads(n); mkl_set_num_threads(n); }
 }

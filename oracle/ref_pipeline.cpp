@@ -14,7 +14,9 @@
 //                     k = min(m, global_n) (the bidiagonal's order, :805-814)
 //   <out>/time.txt    the reference's own run() timer (run_begin..run_finish)
 //                     followed by its phase timers
-// Usage: ref_pipeline cid nclient m local_n port dpath logdir seed mode topk out
+// Usage: ref_pipeline cid nclient m local_n port dpath logdir seed mode topk out [opt_control]
+// (opt_control defaults to 3, the masks run() applies with block_shift_mask;
+// 0 and 2 select the dense block_mask, client.cpp:549-555, 598-601)
 #include <algorithm>
 #include <cstdio>
 #include <string>
@@ -38,10 +40,11 @@ int main(int argc, char** argv) {
   int mode = atoi(argv[9]);
   int topk = atoi(argv[10]);
   std::string out = argv[11];
+  const int opt = argc > 12 ? atoi(argv[12]) : 3;
   mkl_set_num_threads(omp_get_max_threads());
   omp_set_num_threads(omp_get_max_threads());
   DecentralizedClient* c = new DecentralizedClient(cid, nc, mode, (size_t)topk, m, ln, port, "127.0.0.1",
-                                                   dpath, false, false, logdir, seed, 3);
+                                                   dpath, false, false, logdir, seed, opt);
   // Singular values: run() keeps them in a local; recompute them from the
   // final bidiagonal with the same bisection run() used (client.cpp:966-985).
   int k = (int)std::min(m, c->global_n);

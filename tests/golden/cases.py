@@ -115,3 +115,23 @@ def square_cases():
     U (client.cpp:795-798, 1129-1160)."""
     rng = np.random.default_rng(41)
     return {"sq80": ([rng.standard_normal((80, n)) for n in (30, 50)], 41)}
+
+
+def step_cases():
+    """name -> (alpha, beta, omega index, twist index k, house x, house inc,
+    drot (c, s)): inputs of the reference's per-step helpers
+    (ldl_decomposition, dstqds, dpqds, inverse_iteration,
+    one_pair_singular_vector_twisted_factorization, generate_house, mmap_drot,
+    bbtsvd.cpp:54-164, 970-978), taken from the bidiagonal cases."""
+    out = {}
+    rng = np.random.default_rng(99)
+    for name in ("rand_k100", "rand_k257", "graded_signed_k64", "rand_k5"):
+        a, b, _ = bidiagonal_cases()[name]
+        k = len(a)
+        x = rng.standard_normal(3 * k)
+        th = rng.uniform(0, 2 * np.pi)
+        out[name] = (a, b, min(3, k - 1), k // 2, x, 3, (np.cos(th), np.sin(th)))
+    a, b, _ = bidiagonal_cases()["rand_k31"]
+    out["house_zero_tail_neg"] = (a, b, 0, 0, np.array([-2.0] + [0.0] * 9), 1, (0.6, 0.8))
+    out["house_zero_tail_pos"] = (a, b, 0, 0, np.array([2.0] + [0.0] * 9), 1, (0.6, -0.8))
+    return out

@@ -189,17 +189,54 @@ def pipeline_fixtures():
     return out
 
 
+def step_fixtures(R):
+    """The reference's per-step helpers (bbtsvd.cpp:54-164, 970-978) on the
+    step cases, each exactly as the reference computes it."""
+    out = {}
+    for name, (a, b, oi, kt, hx, inc, (cr, sr)) in cases.step_cases().items():
+        n = len(a)
+        aa, bb = a.copy(), (b.copy() if n > 1 else np.zeros(1))
+        l, d = np.zeros(max(n - 1, 1)), np.zeros(n)
+        R.ref_ldl(C.c_int(n), p(aa), p(bb), p(l), p(d))
+        sig = np.linalg.svd(np.diag(a) + np.diag(b, 1), compute_uv=False)
+        omega = float(sig[oi])
+        tau = omega * omega
+        lp, dp, s = np.zeros(max(n - 1, 1)), np.zeros(n), np.zeros(n)
+        R.ref_dstqds(C.c_int(n), p(l), p(d), C.c_double(tau), p(lp), p(dp), p(s))
+        up, rp, pp = np.zeros(max(n - 1, 1)), np.zeros(n), np.zeros(n)
+        R.ref_dpqds(C.c_int(n), p(l), p(d), C.c_double(tau), p(up), p(rp), p(pp))
+        vi = np.zeros(2 * n)
+        R.ref_inverse_iteration(C.c_int(n), C.c_int(kt), p(lp), p(up), p(vi), C.c_int(2))
+        cnt = 3
+        v, u = np.zeros(n), np.zeros(n * cnt)
+        R.ref_one_pair(C.c_int(n), C.c_int(cnt), C.c_double(omega), p(l), p(d), p(aa), p(bb), p(v), p(u))
+        hxo = hx.copy()
+        beta = np.zeros(1)
+        R.ref_generate_house(C.c_int(len(hx) // inc), p(hxo), C.c_int(inc), p(beta))
+        x2, y2 = a.copy(), np.resize(b, n).copy()
+        R.ref_mmap_drot(C.c_size_t(n), p(x2), C.c_size_t(1), p(y2), C.c_size_t(1), C.c_double(cr), C.c_double(sr))
+        out[name] = dict(alpha=a, beta=b, omega=np.float64(omega), twist=np.int32(kt), l=l[:n - 1], d=d,
+                         lp=lp[:n - 1], dp=dp, s=s, up=up[:n - 1], rp=rp, p=pp, vi=vi, v=v, u=u, house_in=hx,
+                         house_inc=np.int32(inc), house_out=hxo, house_beta=beta, drot_c=np.float64(cr),
+                         drot_s=np.float64(sr), drot_x=x2, drot_y=y2)
+    return out
+
+
 def main():
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref", f"REF={REF}"], check=True)
     R = C.CDLL(os.path.join(REFDIR, "libref_capi.so"))
     R.ref_negative_count.restype = C.c_int
     R.ref_set_threads(1)
     fx = {}
-    for grp, d in (("bidiag", bidiagonal_fixtures(R)), ("mask", mask_fixtures(R)),
-                   ("pipe", pipeline_fixtures())):
+    groups = (("bidiag", bidiagonal_fixtures), ("mask", mask_fixtures), ("step", step_fixtures),
+              ("pipe", lambda R: pipeline_fixtures()))
+    keep = sys.argv[1:]
+    for grp, fn in groups:
+        if keep and not any(k.startswith(grp) for k in keep):
+            continue
+        d = fn(R)
         for name, arrs in d.items():
             fx[f"{grp}__{name}"] = arrs
-    keep = sys.argv[1:]
     fx = {k: v for k, v in fx.items() if not keep or any(k.startswith(p) for p in keep)}
     for key, arrs in fx.items():
         np.savez_compressed(os.path.join(HERE, f"{key}.npz"), **arrs)
