@@ -660,6 +660,225 @@ combine_dd_kernel(CombArgs A, const double* __restrict__ sa, const double* __res
   }
 }
 
+// ---- the product fused with its reconstruction --------------------------
+// For products with one K-split (K <= 2^15), one CTA owns a 128 x TNF output
+// tile over every modulus: the MMAs of modulus q run into one of two TMEM
+// accumulators while the epilogue warps reduce the other one mod p_q and add
+// y_q floor(2^96 / p_q) into a 96-bit fixed-point sum per output (three
+// 32-bit limbs, the carries propagated every modulus: the same value mod 2^96
+// as crt_combine's 64-bit limb sums).  The two low limbs live in TMEM beside
+// the accumulators (2 x 128 + 2 x 128 = 512 columns), the high limb in
+// registers.  After the last modulus the centred fraction is scaled as
+// crt_combine scales it and written as FP64: the product's residues never
+// leave the SM, and the result equals crt_product + crt_combine bit for bit.
+constexpr int TNF = 128;
+constexpr int FSTAGES = 6;
+constexpr int FB_TILE = TNF * TK;
+constexpr int FSTAGE_BYTES = A_TILE + FB_TILE;   // 32 KB
+constexpr int FSMEM_BYTES = FSTAGES * FSTAGE_BYTES + 1024 + 256;
+constexpr int FEPI_COLS = TNF / (EPI_WARPS / 4);   // 32 columns per epilogue warp
+constexpr uint32_t FTMEM_COLS = 512;               // accumulators [0, 2 TNF), limbs 0 and 1 [2 TNF, 4 TNF)
+constexpr uint32_t LIMB0 = 2 * TNF, LIMB1 = 3 * TNF;
+
+struct FusedArgs {
+  double* C;
+  long ldc;
+  int M, N, kblocks;
+  const double* sb;   // per-column scales of the product
+  double scale;       // M 2^(-128 - shift)
+  double alpha;
+  int* err;
+};
+
+// One 8-column batch of modulus Q: T mod p_Q from the int32 accumulator (as
+// the unfused epilogue reduces it), y = (T mod p) ((M / p)^-1 mod p) mod p,
+// S += y floor(2^96 / p) (mod 2^96).
+template <int Q, int NM>
+__device__ __forceinline__ void fused_add8(const uint32_t (&v)[8], uint32_t (&s0)[8], uint32_t (&s1)[8],
+                                           uint32_t* s2) {
+  using K = ModK<Q, NM>;
+  constexpr int p = MODULI[Q];
+  constexpr uint32_t c16 = 65536u % p;
+  constexpr uint32_t magic = (uint32_t)((((uint64_t)1 << 32) + p - 1) / p);
+  constexpr int off = (int)(((uint64_t)1 << 31) % p);
+#pragma unroll
+  for (int e = 0; e < 8; ++e) {
+    const uint32_t a = v[e] ^ 0x80000000u;
+    const uint32_t x = (a >> 16) * c16 + (a & 0xFFFFu);
+    int r = (int)(x - __umulhi(x, magic) * (uint32_t)p) - off;
+    if (r < 0) r += p;
+    const uint32_t y = mod_c<K>((uint32_t)r * K::inv);
+    uint64_t t = (uint64_t)y * K::F1 + s0[e];
+    s0[e] = (uint32_t)t;
+    t = (uint64_t)y * K::F2 + s1[e] + (t >> 32);
+    s1[e] = (uint32_t)t;
+    s2[e] += y * K::F3 + (uint32_t)(t >> 32);
+  }
+}
+
+// Modulus Q's accumulator (buffer Q % 2) folded into the state of this warp's
+// 32 lanes x FEPI_COLS columns; the buffer is handed back to the MMA warp.
+template <int NM, int Q>
+__device__ __forceinline__ void fused_drain(uint32_t tmem, uint32_t accf0, uint32_t acce0, int lane, uint32_t col,
+                                            uint32_t (&s2)[FEPI_COLS], bool& ok) {
+  constexpr int buf = Q & 1, use = Q >> 1;
+  if (!ok) return;
+  if (!mbar_wait(accf0 + 8 * buf, (uint32_t)use & 1u)) { ok = false; return; }
+  tc_fence_after();
+#pragma unroll
+  for (int b = 0; b < FEPI_COLS / 8; ++b) {
+    uint32_t v[8], s0[8], s1[8];
+    tmem_ld8_nowait(tmem + col + (uint32_t)(buf * TNF + 8 * b), v);
+    if (Q > 0) {
+      tmem_ld8_nowait(tmem + col + LIMB0 + (uint32_t)(8 * b), s0);
+      tmem_ld8_nowait(tmem + col + LIMB1 + (uint32_t)(8 * b), s1);
+    } else {
+#pragma unroll
+      for (int e = 0; e < 8; ++e) s0[e] = s1[e] = 0u;
+    }
+    tmem_wait_ld();
+    fused_add8<Q, NM>(v, s0, s1, s2 + 8 * b);
+    tmem_st8(tmem + col + LIMB0 + (uint32_t)(8 * b), s0);
+    tmem_st8(tmem + col + LIMB1 + (uint32_t)(8 * b), s1);
+  }
+  tmem_wait_st();
+  tc_fence_before();
+  __syncwarp();
+  if (lane == 0) mbar_arrive(acce0 + 8 * buf);
+}
+
+template <int NM, int... Q>
+__device__ __forceinline__ void fused_drain_all(uint32_t tmem, uint32_t accf0, uint32_t acce0, int lane, uint32_t col,
+                                                uint32_t (&s2)[FEPI_COLS], bool& ok,
+                                                std::integer_sequence<int, Q...>) {
+  (fused_drain<NM, Q>(tmem, accf0, acce0, lane, col, s2, ok), ...);
+}
+
+template <bool AMN, int NM>
+__global__ void __launch_bounds__(THREADS, 1)
+crt_fused_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, FusedArgs P) {
+  const int n0 = blockIdx.x * TNF, m0 = blockIdx.y * TM;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint64_t* bars = (uint64_t*)(smem + FSTAGES * FSTAGE_BYTES);
+  uint32_t* tmem_slot = (uint32_t*)(bars + 2 * FSTAGES + 4);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nk = P.kblocks;
+  const uint32_t full0 = smem_u32(bars), empty0 = smem_u32(bars + FSTAGES);
+  const uint32_t accf0 = smem_u32(bars + 2 * FSTAGES), acce0 = smem_u32(bars + 2 * FSTAGES + 2);
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < FSTAGES; ++s) {
+      mbar_init(full0 + 8 * s, 1);
+      mbar_init(empty0 + 8 * s, 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(accf0 + 8 * b, 1);
+      mbar_init(acce0 + 8 * b, EPI_WARPS);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(FTMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const int total = NM * nk;
+
+  if (warp == EPI_WARPS) {
+    if (lane == 0) {   // ---- TMA producer: modulus after modulus, K-block after K-block
+      int issued = 0;
+      bool ok = true;
+      for (int it = 0; it < total; ++it) {
+        const int q = it / nk, kb = it - q * nk;
+        const int s = it % FSTAGES;
+        const uint32_t ph = (uint32_t)(it / FSTAGES) & 1u;
+        if (!mbar_wait(empty0 + 8 * s, ph ^ 1u)) { ok = false; break; }
+        const uint32_t fb = full0 + 8 * s;
+        mbar_expect_tx(fb, (uint32_t)FSTAGE_BYTES);
+        const uint32_t st = smem_u32(smem + (size_t)s * FSTAGE_BYTES);
+        const int kx = kb * TK;
+        if (AMN)
+          tma_load_3d(st, &tmA, fb, m0, kx, q);
+        else
+          tma_load_3d(st, &tmA, fb, kx, m0, q);
+        tma_load_3d(st + A_TILE, &tmB, fb, kx, n0, q);
+        ++issued;
+      }
+      if (!ok) atomicExch(P.err, 1);
+      for (int it = max(0, issued - FSTAGES); it < issued; ++it)
+        if (!mbar_wait(full0 + 8 * (it % FSTAGES), (uint32_t)(it / FSTAGES) & 1u)) atomicExch(P.err, 4);
+    }
+  } else if (warp == EPI_WARPS + 1) {
+    if (lane == 0) {   // ---- MMA issuer: u8 x u8 -> int32, 128 x 128 x 32 per instruction
+      const uint32_t idesc = (2u << 4) | ((AMN ? 1u : 0u) << 15) | ((uint32_t)(TNF >> 3) << 17) |
+                             ((uint32_t)(TM >> 4) << 24);
+      bool ok = true;
+      for (int q = 0; q < NM && ok; ++q) {
+        const int buf = q & 1, use = q >> 1;
+        if (use > 0 && !mbar_wait(acce0 + 8 * buf, (uint32_t)(use - 1) & 1u)) { ok = false; break; }
+        tc_fence_after();
+        const uint32_t d = tmem + (uint32_t)(buf * TNF);
+        for (int kb = 0; kb < nk; ++kb) {
+          const int it = q * nk + kb;
+          const int s = it % FSTAGES;
+          if (!mbar_wait(full0 + 8 * s, (uint32_t)(it / FSTAGES) & 1u)) { ok = false; break; }
+          tc_fence_after();
+          const uint32_t st = smem_u32(smem + (size_t)s * FSTAGE_BYTES);
+          const uint64_t ad = sw128_desc(st), bd = sw128_desc(st + A_TILE);
+#pragma unroll
+          for (int kk = 0; kk < TK / 32; ++kk)
+            mma_i8(d, ad + (AMN ? 256 : 2) * kk, bd + 2 * kk, idesc, (kb != 0 || kk != 0) ? 1u : 0u);
+          mma_commit(empty0 + 8 * s);
+        }
+        mma_commit(accf0 + 8 * buf);
+      }
+      if (!ok) atomicExch(P.err, 2);
+    }
+  } else {
+    // ---- epilogue: TMEM lanes 32 (warp % 4).. (rows), columns FEPI_COLS (warp / 4).. of
+    //      the tile; the fraction of every output accumulates over the moduli
+    const int q4 = warp & 3, ch = warp >> 2;
+    uint32_t s2[FEPI_COLS];
+#pragma unroll
+    for (int e = 0; e < FEPI_COLS; ++e) s2[e] = 0u;
+    bool ok = true;
+    const uint32_t col = ((uint32_t)(q4 * 32) << 16) + (uint32_t)(ch * FEPI_COLS);
+    fused_drain_all<NM>(tmem, accf0, acce0, lane, col, s2, ok, std::make_integer_sequence<int, NM>{});
+    if (!ok) {
+      if (lane == 0) atomicExch(P.err, 3);
+    } else {
+      const int i = m0 + q4 * 32 + lane;
+#pragma unroll
+      for (int b = 0; b < FEPI_COLS / 8; ++b) {
+        uint32_t s0[8], s1[8];
+        tmem_ld8_nowait(tmem + col + LIMB0 + (uint32_t)(8 * b), s0);
+        tmem_ld8_nowait(tmem + col + LIMB1 + (uint32_t)(8 * b), s1);
+        tmem_wait_ld();
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+          const int j = n0 + ch * FEPI_COLS + 8 * b + e;
+          if (i < P.M && j < P.N) {
+            const uint64_t hi = (uint64_t)s1[e] | ((uint64_t)s2[8 * b + e] << 32), lo = (uint64_t)s0[e] << 32;
+            const double v = fixed_to_double(hi, lo) * (P.sb[j] * P.scale);
+            P.C[i + (long)j * P.ldc] = P.alpha * v;
+          }
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(FTMEM_COLS));
+  }
+}
+
 using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
@@ -925,6 +1144,89 @@ bbt_status crt_launch(bbt_ctx* ctx, int M, int N, long K, int n, const int8_t* R
   return BBT_OK;
 }
 }  // namespace
+
+namespace {
+// Tensor maps of the fused kernel: A as in crt_launch, B with TNF-row boxes.
+bbt_status fused_maps(bbt_ctx* ctx, int M, int N, long K, int n, const int8_t* RA, long lda, const int8_t* RB, long Kp,
+                      CUtensorMap* ta, CUtensorMap* tb) {
+  EncodeTiled enc = encode_fn();
+  if (!enc) return fail(ctx, BBT_ERR_CUDA, "crt: cuTensorMapEncodeTiled is not available");
+  const bool amn = lda > 0;
+  cuuint64_t dims[3] = {(cuuint64_t)K, (cuuint64_t)M, (cuuint64_t)n};
+  cuuint64_t strides[2] = {(cuuint64_t)Kp, (cuuint64_t)Kp * M};
+  cuuint32_t box[3] = {TK, TM, 1};
+  if (amn) {
+    dims[0] = (cuuint64_t)M;
+    dims[1] = (cuuint64_t)K;
+    strides[0] = (cuuint64_t)lda;
+    strides[1] = (cuuint64_t)lda * K;
+    box[0] = TM;
+    box[1] = TK;
+  }
+  const cuuint32_t es[3] = {1, 1, 1};
+  if (enc(ta, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<int8_t*>(RA), dims, strides, box, es,
+          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return fail(ctx, BBT_ERR_CUDA, "crt: tensor map of A (fused)");
+  const cuuint64_t bd[3] = {(cuuint64_t)K, (cuuint64_t)N, (cuuint64_t)n};
+  const cuuint64_t bs[2] = {(cuuint64_t)Kp, (cuuint64_t)Kp * N};
+  const cuuint32_t bb[3] = {TK, TNF, 1};
+  if (enc(tb, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<int8_t*>(RB), bd, bs, bb, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+          CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return fail(ctx, BBT_ERR_CUDA, "crt: tensor map of B (fused)");
+  return BBT_OK;
+}
+
+template <bool AMN, int NM>
+bbt_status fused_launch(bbt_ctx* ctx, const CUtensorMap& ta, const CUtensorMap& tb, const FusedArgs& a, dim3 grid) {
+  static bool attr = false;
+  if (!attr) {
+    BBT_CUDA(ctx, cudaFuncSetAttribute(crt_fused_kernel<AMN, NM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       FSMEM_BYTES));
+    attr = true;
+  }
+  crt_fused_kernel<AMN, NM><<<grid, THREADS, FSMEM_BYTES, ctx->stream>>>(ta, tb, a);
+  BBT_LAUNCHED(ctx);
+  return BBT_OK;
+}
+}  // namespace
+
+bool crt_fused_supported(long K, int n) { return K >= 1 && K <= (long)MAX_KB_PER_SPLIT * TK && n >= 16 && n <= 20; }
+
+bbt_status crt_product_fused(bbt_ctx* ctx, int M, int N, long K, int n, const int8_t* RA, long lda, const int8_t* RB,
+                             long Kp, const double* sb, int shift, double alpha, double* C, long ldc) {
+  if (!crt_fused_supported(K, n)) return fail(ctx, BBT_ERR_ARG, "crt: fused product with K=%ld, %d moduli", K, n);
+  if (M < 1 || N < 1) return fail(ctx, BBT_ERR_ARG, "crt: M=%d N=%d", M, N);
+  const bool amn = lda > 0;
+  if (amn && (lda < M || lda % 16 != 0)) return fail(ctx, BBT_ERR_ARG, "crt: MN-major A, pitch %ld", lda);
+  const unsigned gy = (unsigned)((M + TM - 1) / TM);
+  if (gy > 65535) return fail(ctx, BBT_ERR_ARG, "crt: M=%d too large", M);
+  CUtensorMap ta, tb;
+  BBT_TRY(fused_maps(ctx, M, N, K, n, RA, lda, RB, Kp, &ta, &tb));
+  const Mods md = make_mods(n);
+  FusedArgs a;
+  a.C = C;
+  a.ldc = ldc;
+  a.M = M;
+  a.N = N;
+  a.kblocks = (int)((K + TK - 1) / TK);
+  a.sb = sb;
+  a.scale = std::ldexp(md.mod_hi, -128 - shift);
+  a.alpha = alpha;
+  a.err = ctx->d_flag + FLAG_SKETCH;
+  const dim3 grid((N + TNF - 1) / TNF, gy);   // N-tiles fastest: CTAs sharing A's row block run together
+  ProfScope prof(ctx, BBT_PROF_CRT, 2.0 * n * (double)M * N * K);   // int8 operations
+  switch (n) {
+#define CASE(NM) \
+  case NM:       \
+    return amn ? fused_launch<true, NM>(ctx, ta, tb, a, grid) : fused_launch<false, NM>(ctx, ta, tb, a, grid);
+    CASE(16) CASE(17) CASE(18) CASE(19) CASE(20)
+#undef CASE
+    default:
+      return fail(ctx, BBT_ERR_ARG, "crt: fused product with %d moduli", n);
+  }
+}
 
 bbt_status crt_product(bbt_ctx* ctx, int M, int N, long K, int n, const int8_t* RA, const int8_t* RB, long Kp,
                        bool upper, uint8_t* R, int* splits_out) {

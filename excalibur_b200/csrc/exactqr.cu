@@ -30,6 +30,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 
 #include "internal.h"
 
@@ -57,11 +58,22 @@ long gram_chunk(int m, long n, int nm) {
   return ((n + chunks - 1) / chunks + 32767) / 32768 * 32768;
 }
 
+// Products with Q run the CRT product fused with its reconstruction (no
+// residues of the product in HBM) when the fused kernel supports the shape;
+// EXCALIBUR_B200_FUSED_APPLY=0 selects the two-pass product + reconstruction
+// instead (the same result bit for bit).
+bool apply_fused(int m, int nm) {
+  const char* v = std::getenv("EXCALIBUR_B200_FUSED_APPLY");
+  if (v && v[0] == '0') return false;
+  return crt_fused_supported(m, nm);
+}
+
 // Row chunk of a product with Q over `rows` rows: all rows when the residues
 // of A and of the product fit the cap, else equal chunks (multiples of 128).
-long apply_chunk(long rows, int nm, long Kp, int k) {
+// fused: the product's residues are not stored.
+long apply_chunk(long rows, int nm, long Kp, int k, bool fused) {
   const size_t cap = long_chunk_bytes(LONG_CHUNK_DEFAULT);
-  const size_t per_row = (size_t)nm * (Kp + k) + 8;
+  const size_t per_row = (size_t)nm * (Kp + (fused ? 0 : k)) + 8;
   if ((size_t)rows * per_row <= cap) return rows;
   long c = (long)(cap / per_row) / 128 * 128;
   c = std::max(c, 128L);
@@ -205,8 +217,9 @@ bbt_status exact_local_qr(bbt_ctx* ctx, int m, long n, const double* X, const vo
 size_t exact_apply_workspace_bytes(const bbt_ctx* ctx, long rows, int m, int k) {
   const int nm = crt_moduli(GRAM_BITS, Z_BITS, m);
   const long Kp = crt_pitch(m);
-  const long rc = apply_chunk(rows, nm, Kp, k);
-  return (size_t)nm * (rc + k) * Kp + crt_product_bytes(ctx, (int)rc, k, m, nm, false) +
+  const bool fused = apply_fused(m, nm);
+  const long rc = apply_chunk(rows, nm, Kp, k, fused);
+  return (size_t)nm * (rc + k) * Kp + (fused ? 0 : crt_product_bytes(ctx, (int)rc, k, m, nm, false)) +
          (4 * (size_t)m * k + 2 * (size_t)k) * 8 + 16384;
 }
 
@@ -258,17 +271,22 @@ bbt_status exact_apply_rows(bbt_ctx* ctx, const ExactOperand& op, long rows, con
   if (rows > 0x7fffffffL) return fail(ctx, BBT_ERR_ARG, "exact apply: rows=%ld", rows);
   const int m = op.m, k = op.k, nm = op.nm;
   const size_t mark = ctx->ws.top;
-  const long rc = apply_chunk(rows, nm, op.Kp, k);   // rows are independent: chunks bound the scratch
+  const bool fused = apply_fused(m, nm);
+  const long rc = apply_chunk(rows, nm, op.Kp, k, fused);   // rows are independent: chunks bound the scratch
   int8_t* RA = ctx->ws.take<int8_t>((size_t)nm * rc * op.Kp);
-  uint8_t* Rb = ctx->ws.take<uint8_t>(crt_product_bytes(ctx, (int)rc, k, m, nm, false));
-  if (!Rb) return fail(ctx, BBT_ERR_NOMEM, "exact apply: workspace");
+  uint8_t* Rb = fused ? nullptr : ctx->ws.take<uint8_t>(crt_product_bytes(ctx, (int)rc, k, m, nm, false));
+  if (!RA || (!fused && !Rb)) return fail(ctx, BBT_ERR_NOMEM, "exact apply: workspace");
+  const int shift = (GRAM_BITS - 1) + (Z_BITS - 1);
   for (long r0 = 0; r0 < rows; r0 += rc) {
     const int R = (int)std::min(rc, rows - r0);
     BBT_TRY(crt_residues_cols(ctx, R, m, X + r0, ldx, scale, GRAM_BITS, nm, RA, op.Kp));
+    if (fused) {
+      BBT_TRY(crt_product_fused(ctx, R, k, m, nm, RA, 0, op.RB, op.Kp, op.t, shift, 1.0, C + r0, ldc));
+      continue;
+    }
     int splits = 1;
     BBT_TRY(crt_product(ctx, R, k, m, nm, RA, op.RB, op.Kp, false, Rb, &splits));
-    BBT_TRY(crt_combine(ctx, R, k, nm, splits, Rb, false, nullptr, op.t, (GRAM_BITS - 1) + (Z_BITS - 1), 1.0, 0.0,
-                        C + r0, ldc));
+    BBT_TRY(crt_combine(ctx, R, k, nm, splits, Rb, false, nullptr, op.t, shift, 1.0, 0.0, C + r0, ldc));
   }
   ctx->ws.top = mark;
   return BBT_OK;
@@ -281,16 +299,18 @@ bbt_status exact_apply_planes(bbt_ctx* ctx, const ExactOperand& op, long rows, c
                               double* C, long ldc) {
   if (rows > 0x7fffffffL) return fail(ctx, BBT_ERR_ARG, "exact apply: rows=%ld", rows);
   const int m = op.m, k = op.k, nm = op.nm;
+  const int shift = (GRAM_BITS - 1) + (Z_BITS - 1);
+  if (apply_fused(m, nm))   // the kept planes in, FP64 out: no scratch at all
+    return crt_product_fused(ctx, (int)rows, k, m, nm, planes, pitch, op.RB, op.Kp, op.t, shift, 1.0, C, ldc);
   const size_t mark = ctx->ws.top;
-  const long rc = apply_chunk(rows, nm, 0, k);   // only the product's residues are scratch here
+  const long rc = apply_chunk(rows, nm, 0, k, false);   // only the product's residues are scratch here
   uint8_t* Rb = ctx->ws.take<uint8_t>(crt_product_bytes(ctx, (int)rc, k, m, nm, false));
   if (!Rb) return fail(ctx, BBT_ERR_NOMEM, "exact apply: workspace");
   for (long r0 = 0; r0 < rows; r0 += rc) {   // row chunks start at multiples of 128: 16-byte TMA offsets
     const int R = (int)std::min(rc, rows - r0);
     int splits = 1;
     BBT_TRY(crt_product_amn(ctx, R, k, m, nm, planes + r0, pitch, op.RB, op.Kp, Rb, &splits));
-    BBT_TRY(crt_combine(ctx, R, k, nm, splits, Rb, false, nullptr, op.t, (GRAM_BITS - 1) + (Z_BITS - 1), 1.0, 0.0,
-                        C + r0, ldc));
+    BBT_TRY(crt_combine(ctx, R, k, nm, splits, Rb, false, nullptr, op.t, shift, 1.0, 0.0, C + r0, ldc));
   }
   ctx->ws.top = mark;
   return BBT_OK;

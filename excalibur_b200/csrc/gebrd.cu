@@ -1,30 +1,41 @@
-// Two-sided Householder bidiagonalisation (LAPACK dgebd2 semantics) of a
-// dense n x n column-major matrix, as one persistent cooperative kernel.
+// Two-sided Householder bidiagonalisation A = Q B P^T of a dense n x n
+// column-major matrix (LAPACK dgebrd semantics and storage), blocked:
+// panels of NB columns and rows are reduced by one persistent cooperative
+// kernel each, and the rest of the matrix is brought up to date once per
+// panel by two rank-NB GEMMs on the FP64 tensor cores (dgemm.cu).
 //
 // Used for the dense-matrix SVD (the 8192^2 stress case), where the
 // reference's one-sided Ralha recurrence (client.cpp:829-910) is not
 // backward stable: on clustered spectra it loses ~1e-6 relative accuracy in
-// the small singular values.  A = Q B P^T with B upper bidiagonal; the
-// reflectors are stored as LAPACK's dgebrd stores them (v_i below the
-// diagonal of column i, u_i right of the superdiagonal of row i).
+// the small singular values.  B is upper bidiagonal; v_j is stored below the
+// diagonal of column j, u_j right of the superdiagonal of row j (the unit
+// entries implied), d and e hold B.
 //
-// Step i, with v the column reflector of A(i:, i) and u the row reflector
-// of the updated row i:
-//   phase 1 (every CTA): the reflector H_i from ||A(i+1:, i)||^2, summed
-//           from per-CTA partials left by the previous pass 2;
-//   pass 1  (column-partitioned): w_j = v^T A(i:, j) for j > i and the
-//           updated row i, r_j = A(i, j) - tauq w_j, with per-CTA partials
-//           of sum r_j^2 and sum w_j r_j;
-//   barrier;
-//   phase 2 (every CTA): the reflector G_i of r and w . u from the partials;
-//   pass 2  (row-partitioned, 8 rows x 4 column phases per warp): z_r = (A u)_r -
-//           tauq v_r (w . u), then A(r, j) -= tauq v_r w_j + taup z_r u_j
-//           and A(r, i) <- v_r; the partials of the next column's norm;
-//   barrier.
+// Within a panel (local indices; V, U the panel's column and row reflectors,
+// X, Y their companions) the matrix is never updated in place except for the
+// panel's own column j and row j: the current matrix is
+//   A_j = A - V(:, :j) Y(:, :j)^T - X(:, :j) U(:j, :),
+// and each column step needs the two matrix-vector products
+//   y_j = tauq_j (A^T v_j - Y (V^T v_j) - U^T (X^T v_j))    (gemv pass 1)
+//   x_j = taup_j (A u_j  - V (Y^T u_j)  - X (U u_j))         (gemv pass 2)
+// over the trailing part of the panel-start matrix.  Those two read-only
+// passes are the kernel's HBM traffic (16 bytes per trailing element and
+// column step, against 24 for the unblocked two-sided update); everything
+// else is O(n NB) per step.  After the panel, A(NB:, NB:) -= V Y^T + X U.
+//
+// Column step j, five phases separated by bounded grid barriers:
+//   B: column reflector of the updated column j (its norm from per-CTA
+//      partials), gemv pass 1 (one warp per column) and the partials of
+//      V^T v_j, X^T v_j;
+//   C: y_j, the updated row j (its norm's partials); v_j written to A;
+//   D: row reflector, gemv pass 2 (32-row x 512-column tiles, per-chunk
+//      partials) and the partials of Y^T u_j, U u_j; u_j written to A;
+//   E: x_j, and the update of column j+1 with the partials of its norm.
 // Every reduction is summed in a fixed order, so the result is deterministic.
-// Two grid barriers per step, bounded (sync.cuh).
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
+
+#include <algorithm>
 
 #include "internal.h"
 #include "sync.cuh"
@@ -32,21 +43,30 @@
 namespace bbt {
 namespace {
 
+constexpr int NB = 32;      // panel width
 constexpr int GT = 256;
 constexpr int GW = GT / 32;
+constexpr int CCH = 512;    // columns per gemv-2 partial
+constexpr int PG = 32;      // CTAs that form the panel-correction partials
 
-struct BrdArgs {
-  int n;
-  double* A;      // n x n column-major, lda = n
-  double* d;      // n
-  double* e;      // n-1
-  double* tauq;   // n
-  double* taup;   // n
-  double* w;      // n
-  double* rowb;   // n: updated row i
-  double* colp;   // 2 x grid: per-CTA ||A(i+1:, i)||^2, ping-pong between steps
-  double* rowp;   // grid: per-CTA sum_{j >= i+2} rowb_j^2
-  double* wup;    // grid: per-CTA sum_{j >= i+2} w_j rowb_j
+struct PanelArgs {
+  int M;           // trailing order at this panel
+  int nbp;         // columns (and rows) reduced by this panel
+  long ld;
+  double* A;       // panel origin, column-major, ld
+  double* d;       // at the panel origin
+  double* e;
+  double* tauq;
+  double* taup;
+  double* X;       // M x NB, ld M
+  double* Y;       // M x NB, ld M
+  double* g;       // M: gemv pass 1
+  double* rowb;    // M: the updated row j
+  double* hp;      // [ceil(M / CCH)][M]: gemv pass 2 partials
+  double* colp;    // [grid]
+  double* rowp;    // [grid]
+  double* pq;      // [PG][2 NB]
+  double* st;      // [PG][2 NB]
   unsigned* bar;
   int* err;
 };
@@ -80,151 +100,233 @@ __device__ void larfg(double alpha, double xx, double* beta, double* tau, double
   *scale = 1.0 / (alpha - b);
 }
 
-__global__ void __launch_bounds__(GT) gebrd_kernel(BrdArgs P) {
+// out[kk] (kk < cnt) = sum over the PG partial rows of part[b * 2NB + kk].
+__device__ void sum_partials(const double* part, int cnt, double* out) {
+  for (int kk = threadIdx.x; kk < cnt; kk += GT) {
+    double s = 0.0;
+    for (int b = 0; b < PG; ++b) s += part[b * 2 * NB + kk];
+    out[kk] = s;
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(GT) labrd_kernel(PanelArgs P) {
   __shared__ double sh[GW];
   __shared__ double sc[8];
-  const int n = P.n, tid = threadIdx.x, G = gridDim.x;
+  __shared__ double cor[2 * NB];
+  const int M = P.M, tid = threadIdx.x, G = gridDim.x;
+  const long ld = P.ld;
   double* A = P.A;
-  const long ld = n;
+  const double* X = P.X;
+  const double* Y = P.Y;
   const int lane = tid & 31, gw = blockIdx.x * GW + (tid >> 5), nwarps = G * GW;
-  // ---- set-up: per-CTA partials of ||A(1:, 0)||^2
+  const long gtid = (long)blockIdx.x * GT + tid, nthr = (long)G * GT;
+  // the panel's first column: its norm's partials (no pending updates)
   {
     double s = 0.0;
-    for (int r = 1 + blockIdx.x * GT + tid; r < n; r += G * GT) { const double x = A[r]; s += x * x; }
+    for (long r = 1 + gtid; r < M; r += nthr) { const double x = A[r]; s += x * x; }
     s = bsum(s, sh);
     if (tid == 0) P.colp[blockIdx.x] = s;
   }
   if (!grid_sync(P.bar, P.err)) return;
-  for (int i = 0; i < n; ++i) {
-    // ---- phase 1: column reflector of A(i:, i) from the partials of ||A(i+1:, i)||^2
+  for (int j = 0; j < P.nbp; ++j) {
+    double* cj = A + j * ld;
+    // ---- B: column reflector, gemv pass 1, partials of V^T v and X^T v
     {
-      const double s = psum(P.colp + (i & 1) * G, G, sh);
+      const double s = psum(P.colp, G, sh);
       if (tid == 0) {
         double be, ta, scl;
-        larfg(A[i + i * ld], s, &be, &ta, &scl);
+        larfg(cj[j], s, &be, &ta, &scl);
         sc[0] = be; sc[1] = ta; sc[2] = scl;
       }
       __syncthreads();
     }
     const double tq = sc[1], sq = sc[2];
-    if (blockIdx.x == 0 && tid == 0) { P.d[i] = sc[0]; P.tauq[i] = tq; }
-    if (i == n - 1) break;
-    // ---- pass 1: w_j = v^T A(i:, j), r_j = A(i,j) - tauq w_j, one warp per column;
-    //      per-CTA partials of sum r_j^2 and sum w_j r_j over j >= i+2
-    {
-      double prr = 0.0, pwr = 0.0;
-      for (int j = i + 1 + gw; j < n; j += nwarps) {
-        const double* col = A + j * ld;
-        const double* ci = A + i * ld;
-        double s = 0.0;
-        for (int r = i + lane; r < n; r += 32) {
-          const double vr = (r == i) ? 1.0 : ci[r] * sq;
-          s += vr * col[r];
-        }
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        const double rb = col[i] - tq * s;
-        if (lane == 0) {
-          P.w[j] = s;
-          P.rowb[j] = rb;
-          if (j >= i + 2) { prr += rb * rb; pwr += s * rb; }
-        }
+    if (blockIdx.x == 0 && tid == 0) { P.d[j] = sc[0]; P.tauq[j] = tq; }
+    if (j == M - 1) break;   // the last diagonal entry: no row reflector
+    for (int c = j + 1 + gw; c < M; c += nwarps) {   // g_c = v^T A(j:, c), v_j(j) = 1
+      const double* col = A + c * ld;
+      double s = 0.0;
+      int r = j + 1 + lane;
+      for (; r + 7 * 32 < M; r += 8 * 32) {   // eight loads in flight per lane
+        double a[8], v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) { a[u] = col[r + u * 32]; v[u] = cj[r + u * 32]; }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) s += a[u] * v[u];
       }
-      prr = bsum(prr, sh);
-      pwr = bsum(pwr, sh);
-      if (tid == 0) { P.rowp[blockIdx.x] = prr; P.wup[blockIdx.x] = pwr; }
+      for (; r < M; r += 32) s += col[r] * cj[r];
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+      // column j still holds the updated column a_j (scaled to v_j in phase C)
+      if (lane == 0) P.g[c] = col[j] + sq * s;
+    }
+    if (blockIdx.x < PG && j > 0) {   // rows split over PG CTAs: p_k = V(:, k)^T v, q_k = X(:, k)^T v
+      const int rows = M - j, per = (rows + PG - 1) / PG;
+      const int r0 = j + blockIdx.x * per, r1 = min(M, r0 + per);
+      for (int kk = tid >> 5; kk < 2 * j; kk += GW) {
+        const double* src = kk < j ? A + kk * ld : X + (long)(kk - j) * M;
+        double s = 0.0;
+        for (int r = r0 + lane; r < r1; r += 32) s += src[r] * (r == j ? 1.0 : cj[r] * sq);
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) P.pq[blockIdx.x * 2 * NB + kk] = s;
+      }
     }
     if (!grid_sync(P.bar, P.err)) return;
-    // ---- phase 2: row reflector of r = rowb(i+1:), and w . u
+    // ---- C: y_j, the updated row j and its norm's partials; v_j into A
+    if (j > 0) sum_partials(P.pq, 2 * j, cor);
+    {
+      double pr = 0.0;
+      for (long c = j + 1 + gtid; c < M; c += nthr) {
+        double y = P.g[c];
+        for (int k = 0; k < j; ++k) y -= Y[c + (long)k * M] * cor[k] + A[k + c * ld] * cor[j + k];
+        y *= tq;
+        P.Y[c + (long)j * M] = y;
+        double r = A[j + c * ld] - y;   // V(j, j) = 1
+        for (int k = 0; k < j; ++k) r -= A[j + k * ld] * Y[c + (long)k * M] + X[j + (long)k * M] * A[k + c * ld];
+        P.rowb[c] = r;
+        if (c >= j + 2) pr += r * r;
+      }
+      pr = bsum(pr, sh);
+      if (tid == 0) P.rowp[blockIdx.x] = pr;
+      for (long r = j + 1 + gtid; r < M; r += nthr) cj[r] *= sq;   // v_j
+      if (blockIdx.x == 0 && tid == 0) cj[j] = sc[0];
+    }
+    if (!grid_sync(P.bar, P.err)) return;
+    // ---- D: row reflector, gemv pass 2, partials of Y^T u and U u; u_j into A
     {
       const double s = psum(P.rowp, G, sh);
-      const double t = psum(P.wup, G, sh);
       if (tid == 0) {
         double be, ta, scl;
-        larfg(P.rowb[i + 1], s, &be, &ta, &scl);
+        larfg(P.rowb[j + 1], s, &be, &ta, &scl);
         sc[3] = be; sc[4] = ta; sc[5] = scl;
-        sc[6] = P.w[i + 1] + scl * t;   // w . u, u = (1, scl * rowb(i+2:))
       }
       __syncthreads();
     }
-    const double tp = sc[4], sp = sc[5], wu = sc[6];
-    if (blockIdx.x == 0 && tid == 0) { P.e[i] = sc[3]; P.taup[i] = tp; }
-    // ---- pass 2: rows r > i, 8 rows per warp; lane = (row r0 + lane % 8,
-    //      column phase lane / 8), so each load covers 8 consecutive rows of
-    //      4 columns: whole 32-byte sectors of the column-major matrix.  The
-    //      lanes of column i+1 also sum the next column norm's partial.
-    double cn = 0.0;
+    const double tp = sc[4], sp = sc[5];
+    if (blockIdx.x == 0 && tid == 0) { P.e[j] = sc[3]; P.taup[j] = tp; }
     {
-      const int ro = lane & 7, co = lane >> 3;
-      const int nblk8 = (n - i - 1 + 7) / 8;
-      for (int rb = gw; rb < nblk8; rb += nwarps) {
-        const int r = i + 1 + rb * 8 + ro;
-        const bool live = r < n;
-        const double vr = live ? A[r + i * ld] * sq : 0.0;
+      const int r0 = j + 1, c0 = j + 1;
+      const int nrb = (M - r0 + 31) / 32, ncc = (M - c0 + CCH - 1) / CCH;
+      for (int item = gw; item < nrb * ncc; item += nwarps) {
+        const int rb = item % nrb, cc = item / nrb;
+        const int r = r0 + rb * 32 + lane;
+        const int ca = c0 + cc * CCH, cb = min(M, ca + CCH);
         double s = 0.0;
-        if (live)
-          for (int j = i + 1 + co; j < n; j += 4) {
-            const double uj = (j == i + 1) ? 1.0 : P.rowb[j] * sp;
-            s += A[r + j * ld] * uj;
+        if (r < M) {
+          int c = ca;
+          for (; c + 7 < cb; c += 8) {
+            double a[8], u[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+              a[q] = A[r + (c + q) * ld];
+              u[q] = (c + q == j + 1) ? 1.0 : P.rowb[c + q] * sp;
+            }
+#pragma unroll
+            for (int q = 0; q < 8; ++q) s += a[q] * u[q];
           }
-        s += __shfl_xor_sync(0xffffffffu, s, 8);
-        s += __shfl_xor_sync(0xffffffffu, s, 16);
-        if (live) {
-          const double z = s - tq * vr * wu;
-          for (int j = i + 1 + co; j < n; j += 4) {
-            const double uj = (j == i + 1) ? 1.0 : P.rowb[j] * sp;
-            const double x = A[r + j * ld] - (tq * vr * P.w[j] + tp * z * uj);
-            A[r + j * ld] = x;
-            if (j == i + 1 && r > i + 1) cn += x * x;
-          }
-          if (co == 0) A[r + i * ld] = vr;   // the other lanes of this row read A(r, i) above
+          for (; c < cb; ++c) s += A[r + c * ld] * ((c == j + 1) ? 1.0 : P.rowb[c] * sp);
+          P.hp[(long)cc * M + r] = s;
         }
       }
     }
-    cn = bsum(cn, sh);
-    if (tid == 0) P.colp[((i + 1) & 1) * G + blockIdx.x] = cn;
-    if (blockIdx.x == 0) {   // pivot row: d_i on the diagonal, e_i then u to the right
-      for (int j = i + 1 + tid; j < n; j += GT)
-        A[i + j * ld] = (j == i + 1) ? sc[3] : P.rowb[j] * sp;
-      if (tid == 0) A[i + i * ld] = sc[0];
+    if (blockIdx.x < PG) {   // columns split over PG CTAs: s_k = Y(:, k)^T u (k <= j), t_k = U(k, :) u (k < j)
+      const int cols = M - (j + 1), per = (cols + PG - 1) / PG;
+      const int ca = j + 1 + blockIdx.x * per, cb = min(M, ca + per);
+      for (int kk = tid >> 5; kk < 2 * j + 1; kk += GW) {
+        double s = 0.0;
+        for (int c = ca + lane; c < cb; c += 32) {
+          const double u = (c == j + 1) ? 1.0 : P.rowb[c] * sp;
+          s += (kk <= j ? Y[c + (long)kk * M] : A[(kk - j - 1) + c * ld]) * u;
+        }
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) P.st[blockIdx.x * 2 * NB + kk] = s;
+      }
+    }
+    for (long c = j + 2 + gtid; c < M; c += nthr) A[j + c * ld] = P.rowb[c] * sp;   // u_j (row j is not read here)
+    if (blockIdx.x == 0 && tid == 0) A[j + (j + 1) * ld] = (j == P.nbp - 1 && j + 1 < M) ? 1.0 : sc[3];
+    if (!grid_sync(P.bar, P.err)) return;
+    // ---- E: x_j and the update of column j+1 (and its norm's partials)
+    sum_partials(P.st, 2 * j + 1, cor);
+    {
+      const int ncc = (M - (j + 1) + CCH - 1) / CCH;
+      const bool next = j + 1 < P.nbp;
+      double* cn = A + (j + 1) * ld;
+      double pn = 0.0;
+      for (long r = j + 1 + gtid; r < M; r += nthr) {
+        double h = 0.0;
+        for (int cc = 0; cc < ncc; ++cc) h += P.hp[(long)cc * M + r];
+        for (int k = 0; k <= j; ++k) h -= A[r + k * ld] * cor[k];
+        for (int k = 0; k < j; ++k) h -= X[r + (long)k * M] * cor[j + 1 + k];
+        const double x = tp * h;
+        P.X[r + (long)j * M] = x;
+        if (next) {   // column j+1 of A_{j+1}: U(k, j+1) = A(k, j+1) for k < j, U(j, j+1) = 1
+          double a = cn[r] - x;
+          for (int k = 0; k <= j; ++k) a -= A[r + k * ld] * Y[(j + 1) + (long)k * M];
+          for (int k = 0; k < j; ++k) a -= X[r + (long)k * M] * A[k + (j + 1) * ld];
+          cn[r] = a;
+          if (r >= j + 2) pn += a * a;
+        }
+      }
+      pn = bsum(pn, sh);
+      if (tid == 0) P.colp[blockIdx.x] = pn;
     }
     if (!grid_sync(P.bar, P.err)) return;
   }
 }
 
+// A(j, j+1) <- e_j after the trailing update used the unit entry there.
+__global__ void put_e_kernel(double* a, const double* e) { *a = *e; }
+
 }  // namespace
 
 bbt_status gebrd(bbt_ctx* ctx, int n, double* A, double* d, double* e, double* tauq, double* taup) {
   if (n < 2) return fail(ctx, BBT_ERR_ARG, "gebrd: n=%d", n);
-  size_t mark = ctx->ws.top;
-  BrdArgs P;
-  P.n = n;
-  P.A = A;
-  P.d = d;
-  P.e = e;
-  P.tauq = tauq;
-  P.taup = taup;
-  P.w = ctx->ws.take<double>(n);
+  const size_t mark = ctx->ws.top;
+  int per_sm = 0;
+  BBT_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, labrd_kernel, GT, 0));
+  if (per_sm < 1) return fail(ctx, BBT_ERR_CUDA, "gebrd: kernel does not fit an SM");
+  const int grid = std::max(PG, ctx->num_sms * std::min(per_sm, 2));
+  PanelArgs P;
+  P.ld = n;
+  P.X = ctx->ws.take<double>((size_t)n * NB);
+  P.Y = ctx->ws.take<double>((size_t)n * NB);
+  P.g = ctx->ws.take<double>(n);
   P.rowb = ctx->ws.take<double>(n);
-  P.colp = ctx->ws.take<double>(2 * 1024);
-  P.rowp = ctx->ws.take<double>(1024);
-  P.wup = ctx->ws.take<double>(1024);
-  if (!P.wup) return fail(ctx, BBT_ERR_NOMEM, "gebrd: workspace");
+  P.hp = ctx->ws.take<double>((size_t)((n + CCH - 1) / CCH) * n);
+  P.colp = ctx->ws.take<double>(grid);
+  P.rowp = ctx->ws.take<double>(grid);
+  P.pq = ctx->ws.take<double>(PG * 2 * NB);
+  P.st = ctx->ws.take<double>(PG * 2 * NB);
+  if (!P.st) return fail(ctx, BBT_ERR_NOMEM, "gebrd: workspace");
   P.bar = ctx->d_barrier;
   P.err = ctx->d_flag;
   BBT_CUDA(ctx, cudaMemsetAsync(taup, 0, (size_t)n * sizeof(double), ctx->stream));
   BBT_CUDA(ctx, cudaMemsetAsync(ctx->d_barrier, 0, 2 * sizeof(unsigned), ctx->stream));
   BBT_CUDA(ctx, cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), ctx->stream));
-  int per_sm = 0;
-  BBT_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gebrd_kernel, GT, 0));
-  if (per_sm < 1) return fail(ctx, BBT_ERR_CUDA, "gebrd: kernel does not fit an SM");
-  int grid = ctx->num_sms * (per_sm > 2 ? 2 : per_sm);
-  if (grid > 1024) grid = 1024;
-  if (grid < 1) grid = 1;
-  void* args[] = {&P};
+  const double traffic = 16.0 * (double)n * n * n / 3.0;   // the two gemv passes
   {
-    ProfScope prof(ctx, BBT_PROF_RALHA, 4.0 * 8.0 * (double)n * n * n / 3.0);
-    BBT_CUDA(ctx, cudaLaunchCooperativeKernel((void*)gebrd_kernel, dim3(grid), dim3(GT), args, 0, ctx->stream));
-    BBT_LAUNCHED(ctx);
+    ProfScope prof(ctx, BBT_PROF_RALHA, traffic);
+    for (int i0 = 0; i0 < n; i0 += NB) {
+      const int M = n - i0;
+      P.M = M;
+      P.nbp = std::min(NB, M);
+      P.A = A + i0 + (long)i0 * n;
+      P.d = d + i0;
+      P.e = e + i0;
+      P.tauq = tauq + i0;
+      P.taup = taup + i0;
+      void* args[] = {&P};
+      BBT_CUDA(ctx, cudaLaunchCooperativeKernel((void*)labrd_kernel, dim3(grid), dim3(GT), args, 0, ctx->stream));
+      BBT_LAUNCHED(ctx);
+      if (M > NB) {   // A(NB:, NB:) -= V Y^T + X U on the FP64 tensor cores
+        const int T = M - NB;
+        double* A22 = P.A + NB + (long)NB * n;
+        BBT_TRY(dgemm(ctx, false, true, T, T, NB, -1.0, P.A + NB, n, P.Y + NB, M, 1.0, A22, n));
+        BBT_TRY(dgemm(ctx, false, false, T, T, NB, -1.0, P.X + NB, M, P.A + (long)NB * n, n, 1.0, A22, n));
+        put_e_kernel<<<1, 1, 0, ctx->stream>>>(P.A + (NB - 1) + (long)NB * n, P.e + NB - 1);
+        BBT_LAUNCHED(ctx);
+      }
+    }
   }
   int herr = 0;
   BBT_CUDA(ctx, cudaMemcpyAsync(&herr, ctx->d_flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));

@@ -300,6 +300,13 @@ bbt_status crt_product(bbt_ctx* ctx, int M, int N, long K, int n, const int8_t* 
 // a multiple of 16), e.g. the Gram's planes of X for products with X^T.
 bbt_status crt_product_amn(bbt_ctx* ctx, int M, int N, long K, int n, const int8_t* RA, long lda, const int8_t* RB,
                            long Kp, uint8_t* R, int* splits_out);
+// The product fused with its reconstruction (one K-split, 16..20 moduli):
+// C (column-major, ldc) = alpha sb_j 2^-shift T, equal bit for bit to
+// crt_product + crt_combine with no row scales and beta = 0.  A as for
+// crt_product (lda = 0) or crt_product_amn (lda > 0).
+bool crt_fused_supported(long K, int n);
+bbt_status crt_product_fused(bbt_ctx* ctx, int M, int N, long K, int n, const int8_t* RA, long lda, const int8_t* RB,
+                             long Kp, const double* sb, int shift, double alpha, double* C, long ldc);
 bbt_status crt_combine(bbt_ctx* ctx, int M, int N, int n, int splits, const uint8_t* R, bool upper, const double* sa,
                        const double* sb, int shift, double alpha, double beta, double* C, long ldc);
 bbt_status crt_combine_dd(bbt_ctx* ctx, int M, int N, int n, int splits, const uint8_t* R, bool upper,

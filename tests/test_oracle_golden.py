@@ -193,3 +193,31 @@ def test_square_matches_reference(golden, mode):
     pub, priv = oracle.reference_seeds(seed, len(blocks))
     s, U, VT = pipeline.run(blocks, pub, priv, svd_mode=mode)
     _check_outputs(g, s, U, VT, mode)
+
+
+@pytest.mark.parametrize("name", sorted(cases.step_cases()))
+def test_oracle_steps_match_reference(golden, name):
+    """The per-step helpers (bbtsvd.cpp:54-164, 970-978) restated in
+    oracle/steps.py against the reference's own outputs: the qd recurrences,
+    the Householder vector and the rotation bit for bit, the normalised
+    inverse-iteration vector to rounding (the reference's dnrm2)."""
+    from oracle import steps
+    g = golden(f"step__{name}")
+    a, b = list(g["alpha"]), list(g["beta"])
+    l, d = steps.ldl_decomposition(a, b)
+    assert np.array_equal(l, g["l"]) and np.array_equal(d, g["d"])
+    tau = float(g["omega"]) ** 2
+    lp, dp, s = steps.dstqds(l, d, tau)
+    assert np.array_equal(lp, g["lp"]) and np.array_equal(dp, g["dp"]) and np.array_equal(s, g["s"])
+    up, rp, p = steps.dpqds(l, d, tau)
+    assert np.array_equal(up, g["up"]) and np.array_equal(rp, g["rp"]) and np.array_equal(p, g["p"])
+    n = len(a)
+    v = steps.inverse_iteration(n, int(g["twist"]), lp, up)
+    assert np.max(np.abs(np.array(v) - g["vi"][::2])) < 1e-15
+    inc = int(g["house_inc"])
+    hx, beta = steps.generate_house(list(g["house_in"][::inc]))
+    out = g["house_in"].copy()
+    out[::inc] = hx
+    assert np.array_equal(out, g["house_out"]) and beta == float(g["house_beta"][0])
+    x, y = steps.mmap_drot(a, list(np.resize(g["beta"], n)), float(g["drot_c"]), float(g["drot_s"]))
+    assert np.array_equal(x, g["drot_x"]) and np.array_equal(y, g["drot_y"])
