@@ -52,18 +52,21 @@ bbt_ctx* ctx() {
   abort();
 }
 
-// RAII device copy of a host array.
+// RAII device copy of a host array.  The copies run on the context's stream
+// (non-blocking), in order with the kernels: in, kernels, out, then a wait.
 struct Dev {
   double* p = nullptr;
   size_t n = 0;
   Dev(const double* h, size_t count) : n(count) {
     if (cudaMalloc(&p, (count ? count : 1) * sizeof(double)) != cudaSuccess) die("cudaMalloc", BBT_ERR_NOMEM);
-    if (h && count && cudaMemcpy(p, h, count * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
-      die("cudaMemcpy", BBT_ERR_CUDA);
+    if (h && count &&
+        cudaMemcpyAsync(p, h, count * sizeof(double), cudaMemcpyHostToDevice, g_ctx->stream) != cudaSuccess)
+      die("cudaMemcpyAsync", BBT_ERR_CUDA);
   }
   void back(double* h, size_t count) const {
-    if (count && cudaMemcpy(h, p, count * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
-      die("cudaMemcpy", BBT_ERR_CUDA);
+    if (count && (cudaMemcpyAsync(h, p, count * sizeof(double), cudaMemcpyDeviceToHost, g_ctx->stream) != cudaSuccess ||
+                  cudaStreamSynchronize(g_ctx->stream) != cudaSuccess))
+      die("cudaMemcpyAsync", BBT_ERR_CUDA);
   }
   ~Dev() { cudaFree(p); }
 };
@@ -89,7 +92,9 @@ int negative_count(int n, double* x_diagonal, double* x_upper_diagonal, double m
   bbt_status s = bbt_negative_count(c, n, a.p, b.p, m.p, 1, dc);
   if (s != BBT_OK) die("negative_count", s);
   int h = 0;
-  cudaMemcpy(&h, dc, sizeof(int), cudaMemcpyDeviceToHost);
+  if (cudaMemcpyAsync(&h, dc, sizeof(int), cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
+      cudaStreamSynchronize(c->stream) != cudaSuccess)
+    die("negative_count", BBT_ERR_CUDA);
   cudaFree(dc);
   return h;
 }

@@ -99,6 +99,9 @@ def tall_cases():
     rng = np.random.default_rng(33)
     # m_part = 51, 50, 50 against global_n = 50: only the first slab is reduced
     out["t_mixed"] = ([rng.standard_normal((n, 151)) for n in (10, 25, 15)], 33, rng.standard_normal(151))
+    rng = np.random.default_rng(34)
+    # one participant, m = 120 > global_n = 30: a slab QR of its whole block
+    out["t_p1"] = ([rng.standard_normal((30, 120))], 34, rng.standard_normal(120))
     return out
 
 
@@ -114,7 +117,11 @@ def square_cases():
     case without a global QR whose V comes from rows of the rotated bidiagonal
     U (client.cpp:795-798, 1129-1160)."""
     rng = np.random.default_rng(41)
-    return {"sq80": ([rng.standard_normal((80, n)) for n in (30, 50)], 41)}
+    out = {"sq80": ([rng.standard_normal((80, n)) for n in (30, 50)], 41)}
+    # one participant (the reference's -t 1), square: the shape its single-process run supports
+    rng = np.random.default_rng(10)
+    out["sq60_p1"] = ([rng.standard_normal((60, 60))], 10)
+    return out
 
 
 def step_cases():

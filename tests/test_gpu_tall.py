@@ -70,12 +70,13 @@ def test_tall_modes_match_reference(ctx, golden, name, precision):
     check(g, *run(ctx, blocks, seed, precision, top_k=topk, svd_mode=mode, y=y if mode == 4 else None), mode)
 
 
+@pytest.mark.parametrize("name", sorted(cases.square_cases()))
 @pytest.mark.parametrize("mode", [0, 1])
-def test_square_matches_reference(ctx, golden, mode):
+def test_square_matches_reference(ctx, golden, mode, name):
     """m == global_n: no global QR, FinalVT_c from rows of the rotated U_b
-    (client.cpp:795-798, 1129-1169)."""
-    g = golden(f"pipe__sq80_mode{mode}")
-    blocks, seed = cases.square_cases()["sq80"]
+    (client.cpp:795-798, 1129-1169); two participants and one."""
+    g = golden(f"pipe__{name}_mode{mode}")
+    blocks, seed = cases.square_cases()[name]
     for precision in (0, 1):
         check(g, *run(ctx, blocks, seed, precision, svd_mode=mode, tall=False), mode)
 

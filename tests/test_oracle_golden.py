@@ -32,7 +32,8 @@ def test_every_fixture_has_a_case():
     want = ({f"bidiag__{n}" for n in BIDIAG} | {f"mask__{n}" for n in MASKS}
             | {f"pipe__{n}" for n in PIPES} | {f"pipe__{n}" for n in cases.pipeline_mode_cases()}
             | {f"pipe__{n}" for n in cases.tall_cases()} | {f"pipe__{n}" for n in cases.tall_mode_cases()}
-            | {f"pipe__{n}_mode{m}" for n in cases.square_cases() for m in (0, 1)})
+            | {f"pipe__{n}_mode{m}" for n in cases.square_cases() for m in (0, 1)}
+            | {f"step__{n}" for n in cases.step_cases()})
     assert names == want
 
 
@@ -185,10 +186,11 @@ def test_tall_lr_is_least_squares():
     assert np.max(np.abs(np.concatenate(w) - np.linalg.lstsq(X, y, rcond=None)[0])) < 1e-12
 
 
+@pytest.mark.parametrize("name", sorted(cases.square_cases()))
 @pytest.mark.parametrize("mode", [0, 1])
-def test_square_matches_reference(golden, mode):
-    g = golden(f"pipe__sq80_mode{mode}")
-    blocks, seed = cases.square_cases()["sq80"]
+def test_square_matches_reference(golden, mode, name):
+    g = golden(f"pipe__{name}_mode{mode}")
+    blocks, seed = cases.square_cases()[name]
     assert sha(*blocks) == str(g["x_sha"])
     pub, priv = oracle.reference_seeds(seed, len(blocks))
     s, U, VT = pipeline.run(blocks, pub, priv, svd_mode=mode)
