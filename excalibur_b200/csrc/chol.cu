@@ -439,11 +439,39 @@ struct PotrfArgs {
 
 // Right-looking blocked Cholesky G = R^T R (upper, 32 x 32 tiles), in place:
 // per block row k, (1) every CTA that needs it factors the diagonal tile in
-// shared memory (warp 0, lane c owning column c), CTA 0 stores it, and each
-// CTA solves its tiles of the row panel, R_kj = R_kk^-T G_kj, in shared
-// memory; (2) the trailing tiles G_ij -= R_ki^T R_kj, i <= j, one tile per
-// CTA at a time.  Only the upper triangle of G is read; the
-// strictly lower triangle is zeroed at the end.
+// one warp, lane c holding column c in registers (step j broadcasts row j by
+// warp shuffles), CTA 0 stores it, and each warp of the CTA solves one tile
+// of the row panel, R_kj = R_kk^-T G_kj, lane c forward-substituting column c
+// in registers against the factor in shared memory; (2) the trailing tiles
+// G_ij -= R_ki^T R_kj, i <= j, one tile per CTA at a time.  Only the upper
+// triangle of G is read; the strictly lower triangle is zeroed at the end.
+__device__ __forceinline__ void chol_tile_warp(double (&D)[32][33], int kb, int lane, int* flag) {
+  double x[32];
+#pragma unroll
+  for (int i = 0; i < 32; ++i) x[i] = D[i][lane];   // column lane (rows past kb: zero)
+#pragma unroll
+  for (int j = 0; j < 32; ++j) {
+    if (j < kb) {
+      double d = __shfl_sync(0xffffffffu, x[j], j);
+      if (!(d > 0.0) || !isfinite(d)) {
+        if (lane == 0) atomicExch(flag, 1);
+        d = 1.0;
+      }
+      const double r = sqrt(d);
+      if (lane == j) x[j] = r;
+      else if (lane > j) x[j] = x[j] / r;   // R(j, lane)
+#pragma unroll
+      for (int i = j + 1; i < 32; ++i) {
+        const double rji = __shfl_sync(0xffffffffu, x[j], i);   // R(j, i) from lane i
+        if (lane >= i) x[i] -= rji * x[j];
+      }
+    }
+  }
+  __syncwarp();
+#pragma unroll
+  for (int i = 0; i < 32; ++i) D[i][lane] = (i <= lane && lane < kb) ? x[i] : 0.0;
+}
+
 __global__ void __launch_bounds__(CT, 1) potrf_coop_kernel(PotrfArgs P) {
   __shared__ double D[32][33], A1[32][33], B1[32][33];
   const int n = P.n, nb = (n + 31) / 32;
@@ -456,51 +484,33 @@ __global__ void __launch_bounds__(CT, 1) potrf_coop_kernel(PotrfArgs P) {
         D[i][j] = (i < kb && j < kb && i <= j) ? P.G[(r0 + i) + (long)(r0 + j) * P.ld] : 0.0;
       }
       __syncthreads();
-      if (w == 0) {
-        for (int j = 0; j < kb; ++j) {
-          double d = D[j][j];
-          if (!(d > 0.0) || !isfinite(d)) {
-            if (lane == 0) atomicExch(P.flag, 1);
-            d = 1.0;
-          }
-          const double r = sqrt(d);
-          __syncwarp();
-          if (lane >= j && lane < kb) D[j][lane] = (lane == j) ? r : D[j][lane] / r;
-          __syncwarp();
-          if (lane > j && lane < kb) {
-            const double ajc = D[j][lane];
-            for (int i = j + 1; i <= lane; ++i) D[i][lane] -= D[j][i] * ajc;
-          }
-          __syncwarp();
-        }
-      }
+      if (w == 0) chol_tile_warp(D, kb, lane, P.flag);
       __syncthreads();
       if (blockIdx.x == 0)
         for (int f = threadIdx.x; f < 1024; f += CT) {
           const int i = f % 32, j = f / 32;
           if (i < kb && j < kb && i <= j) P.G[(r0 + i) + (long)(r0 + j) * P.ld] = D[i][j];
         }
-      for (int j = k + 1 + blockIdx.x; j < nb; j += gridDim.x) {   // R_kj = R_kk^-T G_kj in shared memory
+      // R_kj = R_kk^-T G_kj: warp w takes every nw-th tile of this CTA's share, lane c column c
+      for (int j = k + 1 + blockIdx.x + w * gridDim.x; j < nb; j += nw * gridDim.x) {
         const int c0 = 32 * j, jb = min(32, n - c0);
-        for (int f = threadIdx.x; f < 1024; f += CT) {
-          const int i = f % 32, c = f / 32;
-          A1[i][c] = (i < kb && c < jb) ? P.G[(r0 + i) + (long)(c0 + c) * P.ld] : 0.0;
-        }
-        __syncthreads();
-        for (int i = 0; i < kb; ++i) {   // row i final, then rows t > i lose D(i, t) x_i
-          if (threadIdx.x < 32) A1[i][threadIdx.x] /= D[i][i];
-          __syncthreads();
-          for (int f = threadIdx.x; f < (kb - 1 - i) * 32; f += CT) {
-            const int t = i + 1 + f / 32, c = f % 32;
-            A1[t][c] -= D[i][t] * A1[i][c];
+        double* col = P.G + r0 + (long)(c0 + lane) * P.ld;
+        double x[32];
+#pragma unroll
+        for (int i = 0; i < 32; ++i) x[i] = (i < kb && lane < jb) ? col[i] : 0.0;
+#pragma unroll
+        for (int i = 0; i < 32; ++i) {
+          if (i < kb) {
+            double s = x[i];
+#pragma unroll
+            for (int t = 0; t < i; ++t) s -= D[t][i] * x[t];
+            x[i] = s / D[i][i];
           }
-          __syncthreads();
         }
-        for (int f = threadIdx.x; f < 1024; f += CT) {
-          const int i = f % 32, c = f / 32;
-          if (i < kb && c < jb) P.G[(r0 + i) + (long)(c0 + c) * P.ld] = A1[i][c];
-        }
-        __syncthreads();
+        if (lane < jb)
+#pragma unroll
+          for (int i = 0; i < 32; ++i)
+            if (i < kb) col[i] = x[i];
       }
     }
     if (!grid_sync(P.bar, P.err)) return;
