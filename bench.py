@@ -81,6 +81,9 @@ def parse():
     p.add_argument("--extras", default="all",
                    help="comma list of the other workloads timed after the headline (c1,c3,c4,c5), "
                         "'all' or 'none'")
+    p.add_argument("--only", default=None, choices=list(EXTRAS),
+                   help="run just this one of the other workloads (no headline line): for profiling")
+    p.add_argument("--c4-n", type=int, default=C4_N, help="order of the c4 dense matrix (smaller runs)")
     p.add_argument("--precision", default="all", choices=["both", "mixed", "plain", "exact", "all"],
                    help="all: plain FP64, mixed (mode 1) and exact Gram (mode 2), the JSON value is the last; "
                         "both: plain then mixed")
@@ -499,14 +502,13 @@ def clustered_spectrum(rng, clusters, size, gap=1e-10, lo=1e-8, hi=1.0):
     return np.sort(np.concatenate([ci * (1.0 + gap * np.arange(size)) for ci in c]))[::-1]
 
 
-def extra_c4(rank, world, warmup, steps):
+def extra_c4(rank, world, warmup, steps, n=C4_N):
     """c4: the dense SVD of one 8192^2 matrix X = Ux diag(s) Vx^T (Haar Ux, Vx)
     with 512 clusters of 16 values at relative spacing 1e-10.  Oracle: the
     singular values of the stored X by cuSOLVER (FP64); cluster subspaces
     against Ux / Vx at the gap-aware bar max(1e-8, 100 eps ||X|| / gap)."""
     import torch
     import excalibur_b200 as eb
-    n = C4_N
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     ctx = eb.Context(dev.index)
     rng = np.random.default_rng(4)
@@ -585,7 +587,7 @@ def extra_c4(rank, world, warmup, steps):
     ctx.close()
     del X, X0, Ux, Vx
     torch.cuda.empty_cache()
-    return {"workload": workload_name("c4"), "warmup": warmup, "steps": steps,
+    return {"workload": workload_name("c4", n), "warmup": warmup, "steps": steps,
             "value": max_over_ranks(torch, statistics.median(times), dev, world), "unit": "s",
             "accuracy": acc, "clocks": clk.summary(),
             "kernel_classes": {k: {"ms": v[0] / steps, "launches": v[1] // steps} for k, v in prof.items() if v[1]}}
@@ -701,9 +703,10 @@ def workload_name(name, n=None):
         return (f"c3: 64 participants, rows {min(rows)}..{max(rows)} (sum {sum(rows)}) x 512 FP64, "
                 f"entries N(0,1) x 10^U[-2,2] per participant")
     if name == "c4":
-        return (f"c4: dense {C4_N} x {C4_N} FP64, 512 clusters of 16 singular values at relative spacing 1e-10, "
+        n = n or C4_N
+        return (f"c4: dense {n} x {n} FP64, {n // 16} clusters of 16 singular values at relative spacing 1e-10, "
                 f"centres log-uniform in [1e-8, 1] (Householder bidiagonalisation, bisection + twisted vectors "
-                f"for all {C4_N} triplets, cluster refinement)")
+                f"for all {n} triplets, cluster refinement)")
     if name == "c5":
         return ("c5: 4 participants x 1000000 x 2000 FP64 (reference m=2000, local_n=1000000; 64 GB), rank 50 "
                 "with singular values 1e3..10 plus N(0, 1e-3) noise")
@@ -752,6 +755,19 @@ def main():
                           "e2e": {"value": val, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
         return
     import torch
+    if args.only:   # one of the other workloads alone (profiling and measurement runs)
+        dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+        torch.cuda.set_device(dev)
+        dp, ip = cublas_dgemm_peak(torch, dev), cublas_int8_peak(torch, dev)
+        if args.only == "c4":
+            e = extra_c4(rank, 1, 1, max(1, args.steps), n=args.c4_n)
+        elif args.only == "c5":
+            e = extra_c5(rank, 1, 1, max(1, args.steps), dp, ip)
+        else:
+            modes = ["plain", "mixed", "exact"] if args.only == "c3" else ["plain", "exact"]
+            e = extra_blocks(args, rank, 1, args.only, modes, args.warmup, args.steps, dp, ip)
+        print(json.dumps({args.only: e, "dgemm_peak_tflops": dp, "int8_peak_tops": ip}))
+        return
     if world > 1:
         torch.distributed.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
     res = run_ours(args, rank, world)

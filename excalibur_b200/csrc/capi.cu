@@ -115,6 +115,7 @@ bbt_status bbt_destroy(bbt_ctx* ctx) {
   if (ctx->d_barrier) cudaFree(ctx->d_barrier);
   if (ctx->bracket_theta) cudaFree(ctx->bracket_theta);
   if (ctx->io_ws.base) cudaFree(ctx->io_ws.base);
+  if (ctx->mask_pinned) cudaFreeHost(ctx->mask_pinned);
   if (ctx->copy_in) cudaStreamDestroy(ctx->copy_in);
   if (ctx->copy_out) cudaStreamDestroy(ctx->copy_out);
   for (auto e : ctx->in_ready) cudaEventDestroy(e);

@@ -693,6 +693,10 @@ struct FusedArgs {
 // One 8-column batch of modulus Q: T mod p_Q from the int32 accumulator (as
 // the unfused epilogue reduces it), y = (T mod p) ((M / p)^-1 mod p) mod p,
 // S += y floor(2^96 / p) (mod 2^96).
+// The accumulator of u8 x u8 products over at most 2^15 terms is a
+// non-negative int32 below 2^31: (a >> 16) c16 + (a & 0xFFFF) < 2^24 is
+// congruent to it, and its multiply-high quotient by p is exact, so r is
+// T mod p in [0, p) -- the residue the two-pass epilogue stores.
 template <int Q, int NM>
 __device__ __forceinline__ void fused_add8(const uint32_t (&v)[8], uint32_t (&s0)[8], uint32_t (&s1)[8],
                                            uint32_t* s2) {
@@ -700,14 +704,12 @@ __device__ __forceinline__ void fused_add8(const uint32_t (&v)[8], uint32_t (&s0
   constexpr int p = MODULI[Q];
   constexpr uint32_t c16 = 65536u % p;
   constexpr uint32_t magic = (uint32_t)((((uint64_t)1 << 32) + p - 1) / p);
-  constexpr int off = (int)(((uint64_t)1 << 31) % p);
 #pragma unroll
   for (int e = 0; e < 8; ++e) {
-    const uint32_t a = v[e] ^ 0x80000000u;
+    const uint32_t a = v[e];
     const uint32_t x = (a >> 16) * c16 + (a & 0xFFFFu);
-    int r = (int)(x - __umulhi(x, magic) * (uint32_t)p) - off;
-    if (r < 0) r += p;
-    const uint32_t y = mod_c<K>((uint32_t)r * K::inv);
+    const uint32_t r = x - __umulhi(x, magic) * (uint32_t)p;
+    const uint32_t y = mod_c<K>(r * K::inv);
     uint64_t t = (uint64_t)y * K::F1 + s0[e];
     s0[e] = (uint32_t)t;
     t = (uint64_t)y * K::F2 + s1[e] + (t >> 32);

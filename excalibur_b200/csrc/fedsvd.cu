@@ -19,6 +19,9 @@
 #include <algorithm>
 #include <vector>
 
+#include <cstring>
+#include <thread>
+
 #include "internal.h"
 
 namespace bbt {
@@ -221,6 +224,102 @@ size_t persistent_bytes(const Layout& L) {
   }
   if (L.precision == 2) b += (size_t)(L.P + 1) * ((m * m + m) * 8 + 512);   // R_p and the row scales
   return b;
+}
+
+// ---- the masks' random tables, drawn while the local QRs run -------------
+// Every mask of a short-and-wide call is known from the shapes and seeds
+// alone: the public row mask and each participant's private column mask
+// (client.cpp:593-596) and their inverses (:1109, :1182).  Their tables are
+// drawn with the reference's own calls (glibc rand() and
+// std::default_random_engine, so bit for bit the tables the reference draws)
+// on a host thread while the GPU runs the local QRs, then uploaded at once
+// through pinned memory; each mask is then a single launch with no host work.
+// Rotated lengths above 10000 (the virtual-matrix path) draw theirs in place.
+struct MaskPrefetch {
+  struct Key {
+    size_t k;
+    bool mask;
+    unsigned seed;
+  };
+  std::vector<Key> keys;
+  std::vector<GivensTables> tabs;
+  std::vector<GivensDev> dev;
+  std::thread th;
+  bool failed = false;
+
+  int find(size_t k, bool mask, unsigned seed) const {
+    for (size_t i = 0; i < keys.size(); ++i)
+      if (keys[i].k == k && keys[i].mask == mask && keys[i].seed == seed) return (int)i;
+    return -1;
+  }
+  void add(size_t k, bool mask, unsigned seed) {
+    if (k < 2 || k > 10000 || find(k, mask, seed) >= 0) return;
+    keys.push_back({k, mask, seed});
+  }
+  static size_t ops(size_t k) { return (k + (k & 1)) / 2; }
+  size_t bytes() const {
+    size_t b = 0;
+    for (const Key& key : keys) b += MASK_PASSES * ops(key.k) * (sizeof(int2) + sizeof(double2)) + 512;
+    return b;
+  }
+  void start() {
+    tabs.resize(keys.size());
+    th = std::thread([this] {
+      try {
+        for (size_t i = 0; i < keys.size(); ++i)
+          draw_givens_tables(keys[i].k, MASK_PASSES, keys[i].mask, keys[i].seed, tabs[i]);
+      } catch (...) {
+        failed = true;
+      }
+    });
+  }
+  // Joins the drawing thread and copies every table into the device slab.
+  bbt_status upload(bbt_ctx* ctx, char* slab) {
+    if (th.joinable()) th.join();
+    if (failed) return fail(ctx, BBT_ERR_NOMEM, "fedsvd: mask tables");
+    if (keys.empty()) return BBT_OK;
+    const size_t total = bytes();
+    if (ctx->mask_pinned_cap < total) {
+      if (ctx->mask_pinned) cudaFreeHost(ctx->mask_pinned);
+      ctx->mask_pinned = nullptr;
+      ctx->mask_pinned_cap = 0;
+      BBT_CUDA(ctx, cudaMallocHost(&ctx->mask_pinned, total));
+      ctx->mask_pinned_cap = total;
+    }
+    char* h = static_cast<char*>(ctx->mask_pinned);
+    size_t off = 0;
+    dev.resize(keys.size());
+    for (size_t i = 0; i < keys.size(); ++i) {
+      const GivensTables& T = tabs[i];
+      GivensDev& D = dev[i];
+      D.k = T.k;
+      D.passes = T.passes;
+      D.ops = T.ops;
+      D.b1 = T.b1;
+      D.b2 = T.b2;
+      off = (off + 255) & ~size_t(255);
+      std::memcpy(h + off, T.pairs.data(), T.pairs.size() * sizeof(int2));
+      D.pairs = reinterpret_cast<const int2*>(slab + off);
+      off += T.pairs.size() * sizeof(int2);
+      off = (off + 255) & ~size_t(255);
+      std::memcpy(h + off, T.cs.data(), T.cs.size() * sizeof(double2));
+      D.cs = reinterpret_cast<const double2*>(slab + off);
+      off += T.cs.size() * sizeof(double2);
+    }
+    BBT_CUDA(ctx, cudaMemcpyAsync(slab, h, off, cudaMemcpyHostToDevice, ctx->stream));
+    return BBT_OK;
+  }
+  ~MaskPrefetch() {
+    if (th.joinable()) th.join();
+  }
+};
+
+// A mask with its prefetched tables, or drawn in place.
+bbt_status apply_mask(bbt_ctx* ctx, const MaskPrefetch& pf, size_t m, size_t n, double* x, bool mask, bool is_left,
+                      unsigned seed) {
+  const int i = pf.find(is_left ? m : n, mask, seed);
+  if (i >= 0 && (size_t)i < pf.dev.size()) return apply_givens(ctx, pf.dev[i], m, n, x, is_left);
+  return block_shift_mask(ctx, m, n, MASK_PASSES, x, mask, is_left, seed);
 }
 
 // ---- batched local QR (all participants, concurrent streams, CUDA graph) --
@@ -676,8 +775,16 @@ bbt_status fedsvd(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* X, 
       streams = 8;
     }
   }
-  const size_t need =
-      persistent_bytes(L) + std::max(scratch_bytes(ctx, L), batched_scratch(ctx, L, streams, qp) + (64u << 20));
+  const bool compute_u = cfg->svd_mode != 3, compute_v = cfg->svd_mode != 2;   // client.cpp:491-492
+  MaskPrefetch pf;
+  for (int c = 0; c < P; ++c) {
+    pf.add(m, true, cfg->public_seed);                  // row mask, client.cpp:594
+    pf.add(L.r[c], true, cfg->private_seeds[c]);        // column mask, :595
+    if (compute_v) pf.add(L.r[c], false, cfg->private_seeds[c]);   // its inverse on FinalVT_c, :1182
+  }
+  if (compute_u) pf.add(m, false, cfg->public_seed);    // the row mask's inverse on FinalU, :1109
+  const size_t need = persistent_bytes(L) + pf.bytes() +
+                      std::max(scratch_bytes(ctx, L), batched_scratch(ctx, L, streams, qp) + (64u << 20));
   // precision 2: X_int's residue planes serve the Gram and, kept, the V back-transform
   // (no second pass over the blocks), where the device has room for them
   size_t keep = 0;
@@ -713,7 +820,9 @@ bbt_status fedsvd(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* X, 
   double* scal = ctx->ws.take<double>(8);
   int* cnt = ctx->ws.take<int>(8);
   double* tmp = ctx->ws.take<double>(m * std::max(m, rg));
-  if (!tmp) return fail(ctx, BBT_ERR_NOMEM, "fedsvd: workspace");
+  char* mask_slab = ctx->ws.take<char>(pf.bytes());
+  if (!tmp || !mask_slab) return fail(ctx, BBT_ERR_NOMEM, "fedsvd: workspace");
+  pf.start();   // the mask tables are drawn on the host while the GPU runs the local QRs
   QrJob job;
   job.precision = L.precision;
   job.RT = RT;
@@ -759,7 +868,6 @@ bbt_status fedsvd(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* X, 
   BBT_CUDA(ctx, cudaEventRecord(ev[0], ctx->stream));
 
   // 1) local QR (client.cpp:572-589): A = X_c^T column-major n x m, in place
-  const bool compute_u = cfg->svd_mode != 3, compute_v = cfg->svd_mode != 2;   // client.cpp:491-492
   job.compute_v = compute_v;
   std::vector<double*> masked(P);
   for (int c = 0; c < P; ++c) masked[c] = L.qr[c] ? RT[c] : X[c];
@@ -777,9 +885,10 @@ bbt_status fedsvd(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* X, 
     for (int c = 0; c < P; ++c) BBT_TRY(wait_input(ctx, c));
   BBT_CUDA(ctx, cudaEventRecord(ev[1], ctx->stream));
   // 2) masks (client.cpp:593-596)
+  BBT_TRY(pf.upload(ctx, mask_slab));
   for (int c = 0; c < P; ++c) {
-    BBT_TRY(block_shift_mask(ctx, m, L.r[c], MASK_PASSES, masked[c], true, true, cfg->public_seed));
-    BBT_TRY(block_shift_mask(ctx, m, L.r[c], MASK_PASSES, masked[c], true, false, cfg->private_seeds[c]));
+    BBT_TRY(apply_mask(ctx, pf, m, L.r[c], masked[c], true, true, cfg->public_seed));
+    BBT_TRY(apply_mask(ctx, pf, m, L.r[c], masked[c], true, false, cfg->private_seeds[c]));
   }
   BBT_CUDA(ctx, cudaEventRecord(ev[2], ctx->stream));
   // 3) repartition + global QR of M^T (client.cpp:681-794)
@@ -838,7 +947,7 @@ bbt_status fedsvd(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* X, 
   // 6) U: FinalU (m x k row-major) = (V_b Vr)^T, unmasked (client.cpp:1018, 1071-1115)
   if (compute_u) {
     BBT_TRY(dgemm(ctx, true, true, k, mi, m, 1.0, Vb, (long)m, Vr, (long)m, 0.0, Uout, k));
-    BBT_TRY(block_shift_mask(ctx, m, (size_t)k, MASK_PASSES, Uout, false, true, cfg->public_seed));
+    BBT_TRY(apply_mask(ctx, pf, m, (size_t)k, Uout, false, true, cfg->public_seed));
   }
   //    V: U2 = H (G^T U_b) (client.cpp:1127-1176)
   if (compute_v) {
@@ -853,7 +962,7 @@ bbt_status fedsvd(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* X, 
     const int rc = (int)L.r[c];
     if (rg == m) {   // m == global_n: FinalVT_c = U2[rows of c]^T, unmasked (client.cpp:1161-1166)
       BBT_TRY(transpose(ctx, rc, k, Ub + L.rpos[c] * k, k, VT[c], rc));
-      BBT_TRY(block_shift_mask(ctx, (size_t)k, (size_t)rc, MASK_PASSES, VT[c], false, false, cfg->private_seeds[c]));
+      BBT_TRY(apply_mask(ctx, pf, (size_t)k, (size_t)rc, VT[c], false, false, cfg->private_seeds[c]));
       if (ctx->io_on && ctx->vt_dst[c]) {
         BBT_CUDA(ctx, cudaEventRecord(ctx->vt_done[c], ctx->stream));
         BBT_CUDA(ctx, cudaStreamWaitEvent(ctx->copy_out, ctx->vt_done[c], 0));
@@ -869,7 +978,7 @@ bbt_status fedsvd(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* X, 
       BBT_TRY(dgemm(ctx, false, false, rc, k, m, 1.0, M + L.rpos[c], (long)rg, Rg, (long)m, 0.0, tmp, rc));
     else
       BBT_TRY(dgemm(ctx, false, true, rc, k, m, 1.0, M + L.rpos[c], (long)rg, Ub, k, 0.0, tmp, rc));
-    BBT_TRY(block_shift_mask(ctx, (size_t)k, (size_t)rc, MASK_PASSES, tmp, false, false, cfg->private_seeds[c]));
+    BBT_TRY(apply_mask(ctx, pf, (size_t)k, (size_t)rc, tmp, false, false, cfg->private_seeds[c]));
     const long n = (long)L.n[c];
     if (L.qr[c] && L.precision == 2) {   // Q_c = X_int^T Rp_c^-1 W_c: FinalVT^T = X_int^T Rp_c^-1 (W_c tmp^T)
       BBT_TRY(dgemm(ctx, false, false, mi, k, m, 1.0, job.W[c], (long)m, tmp, rc, 0.0, Z, (long)m));

@@ -27,12 +27,7 @@
 namespace bbt {
 namespace {
 
-struct Tables {
-  size_t k = 0, passes = 0, ops = 0;
-  int b1 = 0, b2 = 0;               // stages [0,b1), [b1,b2), [b2,ops)
-  std::vector<int2> pairs;          // [pass][op]
-  std::vector<double2> cs;          // (c, s) with s signed for the direction
-};
+using Tables = GivensTables;
 
 // bbtsvd.cpp:729-779.  Leaves glibc's rand() state exactly as the reference.
 void draw_tables(size_t k, size_t passes, bool mask, unsigned seed, Tables& T) {
@@ -153,7 +148,28 @@ __global__ void __launch_bounds__(512) givens_kernel(double* __restrict__ x, lon
 
 constexpr size_t SMEM_CAP = 200 * 1024;
 
+// The strip kernel for one block with the tables already on the device.
+bbt_status launch_tables(bbt_ctx* ctx, const GivensDev& T, size_t m, size_t n, double* x, bool is_left);
+
 bbt_status apply_tables(bbt_ctx* ctx, const Tables& T, size_t m, size_t n, double* x, bool is_left) {
+  if (T.ops == 0) return BBT_OK;
+  const long nvec = (long)(is_left ? n : m);
+  if (nvec == 0) return BBT_OK;
+  size_t mark = ctx->ws.top;
+  int2* dp = ctx->ws.take<int2>(T.pairs.size());
+  double2* dc = ctx->ws.take<double2>(T.cs.size());
+  if (!dc) return fail(ctx, BBT_ERR_NOMEM, "givens mask: workspace");
+  BBT_CUDA(ctx, cudaMemcpyAsync(dp, T.pairs.data(), T.pairs.size() * sizeof(int2),
+                                cudaMemcpyHostToDevice, ctx->stream));
+  BBT_CUDA(ctx, cudaMemcpyAsync(dc, T.cs.data(), T.cs.size() * sizeof(double2),
+                                cudaMemcpyHostToDevice, ctx->stream));
+  GivensDev D{T.k, T.passes, T.ops, T.b1, T.b2, dp, dc};
+  BBT_TRY(launch_tables(ctx, D, m, n, x, is_left));
+  ctx->ws.top = mark;   // stream order protects the tables until the kernel has run
+  return BBT_OK;
+}
+
+bbt_status launch_tables(bbt_ctx* ctx, const GivensDev& T, size_t m, size_t n, double* x, bool is_left) {
   if (T.ops == 0) return BBT_OK;
   const size_t k = T.k;
   const long nvec = (long)(is_left ? n : m);
@@ -171,14 +187,8 @@ bbt_status apply_tables(bbt_ctx* ctx, const Tables& T, size_t m, size_t n, doubl
     w = w2;
   }
   const size_t smem = k * (size_t)(w + 1) * 8;
-  size_t mark = ctx->ws.top;
-  int2* dp = ctx->ws.take<int2>(T.pairs.size());
-  double2* dc = ctx->ws.take<double2>(T.cs.size());
-  if (!dc) return fail(ctx, BBT_ERR_NOMEM, "givens mask: workspace");
-  BBT_CUDA(ctx, cudaMemcpyAsync(dp, T.pairs.data(), T.pairs.size() * sizeof(int2),
-                                cudaMemcpyHostToDevice, ctx->stream));
-  BBT_CUDA(ctx, cudaMemcpyAsync(dc, T.cs.data(), T.cs.size() * sizeof(double2),
-                                cudaMemcpyHostToDevice, ctx->stream));
+  const int2* dp = T.pairs;
+  const double2* dc = T.cs;
   const int blocks = (int)((nvec + w - 1) / w);
   const int threads = 512;
   ProfScope prof(ctx, BBT_PROF_MASK, 16.0 * (double)k * (double)nvec);
@@ -192,7 +202,6 @@ bbt_status apply_tables(bbt_ctx* ctx, const Tables& T, size_t m, size_t n, doubl
                                                                  (int)T.ops, T.b1, T.b2, dp, dc);
   }
   BBT_LAUNCHED(ctx);
-  ctx->ws.top = mark;   // stream order protects the tables until the kernel has run
   return BBT_OK;
 }
 
@@ -275,6 +284,15 @@ void square_convert(size_t k, size_t* rows, size_t* cols, size_t* remain) {
 }
 
 }  // namespace
+
+void draw_givens_tables(size_t k, size_t passes, bool mask, unsigned seed, GivensTables& T) {
+  draw_tables(k, passes, mask, seed, T);
+}
+
+bbt_status apply_givens(bbt_ctx* ctx, const GivensDev& T, size_t m, size_t n, double* x, bool is_left) {
+  if (T.k > 10000) return fail(ctx, BBT_ERR_ARG, "givens mask: prepared tables of the direct path only");
+  return launch_tables(ctx, T, m, n, x, is_left);
+}
 
 bbt_status givens_mask(bbt_ctx* ctx, size_t m, size_t n, size_t passes, double* x, bool mask,
                        bool is_left, unsigned seed) {

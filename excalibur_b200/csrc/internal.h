@@ -84,6 +84,9 @@ struct bbt_ctx {
   // file entry: two pinned staging buffers and their copy events; the gate
   // blocks until participant c's input has been read and its copy enqueued
   void* io_pinned = nullptr;
+  // pinned staging of the pipeline's prepared mask tables (grown on demand)
+  void* mask_pinned = nullptr;
+  size_t mask_pinned_cap = 0;
   cudaEvent_t io_stage_ev[2] = {nullptr, nullptr};
   bool (*io_gate)(void*, int) = nullptr;
   void* io_gate_arg = nullptr;
@@ -174,6 +177,24 @@ bbt_status twisted_pair(bbt_ctx* ctx, int n, const double* omega, const double* 
 bbt_status bidiag_bound(bbt_ctx* ctx, int n, const double* a, const double* b, double* d_out);
 
 // Givens masks (givens.cu)
+// The random tables of one mask (bbtsvd.cpp:729-779): pairs and (c, s) per
+// pass, drawn on the host with the reference's own calls (glibc rand(),
+// std::default_random_engine, std::shuffle), and the same on the device.
+struct GivensTables {
+  size_t k = 0, passes = 0, ops = 0;
+  int b1 = 0, b2 = 0;               // stages [0,b1), [b1,b2), [b2,ops)
+  std::vector<int2> pairs;          // [pass][op]
+  std::vector<double2> cs;          // (c, s) with s signed for the direction
+};
+struct GivensDev {
+  size_t k = 0, passes = 0, ops = 0;
+  int b1 = 0, b2 = 0;
+  const int2* pairs = nullptr;
+  const double2* cs = nullptr;
+};
+void draw_givens_tables(size_t k, size_t passes, bool mask, unsigned seed, GivensTables& T);
+// The mask of a rotated length k <= 10000 (the direct path) with device tables.
+bbt_status apply_givens(bbt_ctx* ctx, const GivensDev& T, size_t m, size_t n, double* x, bool is_left);
 bbt_status givens_mask(bbt_ctx* ctx, size_t m, size_t n, size_t passes, double* x, bool mask,
                        bool is_left, unsigned seed);
 bbt_status block_shift_mask(bbt_ctx* ctx, size_t m, size_t n, size_t passes, double* x, bool mask,

@@ -95,6 +95,27 @@ def test_epilogue_reduction_of_int32_accumulators(p):
         assert r == v % p
 
 
+@pytest.mark.parametrize("p", MOD)
+def test_fused_epilogue_reduction(p):
+    """The fused product's epilogue: the accumulator of u8 x u8 products over
+    at most 2^15 terms is 0 <= v < 2^31, x = (v >> 16) c16 + (v & 0xFFFF) <
+    2^24, r = x - floor(x ceil(2^32 / p) / 2^32) p = v mod p, and y =
+    (r inv) mod p by the same multiply-high quotient: the residues and the
+    CRT digits of the two-pass path, hence its output bit for bit."""
+    c16, magic = 65536 % p, -(-(1 << 32) // p)
+    rng = np.random.default_rng(p + 3)
+    top = (1 << 15) * 255 * 255
+    vals = [0, 1, p - 1, p, (1 << 16) - 1, 1 << 16, top, *[int(v) for v in rng.integers(0, top + 1, 5000)]]
+    for inv in (1, p - 1, (p // 2) | 1):
+        for v in vals:
+            x = (v >> 16) * c16 + (v & 0xFFFF)
+            assert x < (1 << 24)
+            r = x - ((x * magic) >> 32) * p
+            assert r == v % p
+            t = r * inv
+            assert t - ((t * magic) >> 32) * p == (v * inv) % p
+
+
 @pytest.mark.parametrize("bits_a,bits_b,K,expect", [(53, 53, 500_000, 16), (50, 50, 500_000, 15),
                                                     (53, 80, 1000, 19), (53, 80, 512, 18), (53, 53, 2000, 15)])
 def test_modulus_count_covers_the_product(bits_a, bits_b, K, expect):
