@@ -2,7 +2,7 @@
 the products with the implicit Q of the exact-Gram mode keep every modulus's
 accumulator on the SM and write FP64 directly.  It must equal the two-pass
 product (residues of the product in HBM) + reconstruction bit for bit:
-EXCALIBUR_B200_FUSED_APPLY=0 selects the two-pass path for the comparison.
+EXCALIBUR_B200_FUSED_APPLY=1 selects the fused path, =0 the two-pass path.
 Both operand layouts are covered: the recomputed residues of X's columns
 (K-major, bbt_exact_apply_q) and the Gram's kept residue planes read MN-major
 (the pipeline's V back-transform)."""
@@ -47,7 +47,7 @@ def test_fused_apply_equals_two_pass(ctx, m, n, k):
     _, _, Rpt, sc = ctx.exact_local_qr(Xd)
     Z = ctx._dev(rng.standard_normal((k, m)))
     two = with_env("0", lambda: ctx.exact_apply_q(Xd, sc, Rpt, Z).cpu().numpy())
-    one = with_env(None, lambda: ctx.exact_apply_q(Xd, sc, Rpt, Z).cpu().numpy())
+    one = with_env("1", lambda: ctx.exact_apply_q(Xd, sc, Rpt, Z).cpu().numpy())
     assert np.all(np.isfinite(one))
     assert np.array_equal(one, two)
 
@@ -65,7 +65,7 @@ def test_fused_pipeline_back_transform_bitwise(ctx, precision):
         return s.cpu().numpy(), U.cpu().numpy(), [v.cpu().numpy() for v in VT]
 
     s0, U0, V0 = with_env("0", run)
-    s1, U1, V1 = with_env(None, run)
+    s1, U1, V1 = with_env("1", run)
     assert np.array_equal(s0, s1) and np.array_equal(U0, U1)
     for a, b in zip(V0, V1):
         assert np.array_equal(a, b)
