@@ -1,11 +1,18 @@
 // Bounded grid-wide barrier for cooperative launches.
 //
-// Generation-counting barrier: thread 0 of every CTA arrives on bar[0]; the
-// last arrival resets it and bumps the generation bar[1].  The wait polls a
-// bounded number of times; on a timeout (or when another CTA has already
-// timed out) it sets *err and returns false, so every CTA can leave the
-// kernel instead of hanging the GPU.  Launch with cudaLaunchCooperativeKernel
-// so that all CTAs are co-resident.
+// A monotonic arrival count: thread 0 of every CTA makes the CTA's writes
+// visible at GPU scope and adds 1 to bar[0]; the value it gets back, divided
+// by the grid size, is the index of this barrier (every barrier adds exactly
+// gridDim.x), so the CTA waits until the count reaches the end of that
+// barrier's round.  No CTA resets anything, so the last arrival is not on
+// anyone's critical path twice, and a waiter polls one word with an acquire
+// load.  The count starts at 0 for each launch (the host clears it; kernels
+// launched back to back with the same grid may share one clearing) and
+// wraps only after 2^32 arrivals.  The wait polls a bounded number of times;
+// on a timeout (or when another CTA has already timed out) it sets *err and
+// returns false, so every CTA can leave the kernel instead of hanging the
+// GPU.  Launch with cudaLaunchCooperativeKernel so that all CTAs are
+// co-resident.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -13,29 +20,31 @@ namespace bbt {
 
 constexpr long GRID_SPIN_LIMIT = 20000000;   // ~seconds of polling before giving up
 
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
 __device__ __forceinline__ bool grid_sync(unsigned* bar, int* err) {
+  __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
-    volatile unsigned* gen = bar + 1;
-    const unsigned g0 = *gen;
-    __threadfence();
-    const unsigned arrived = atomicAdd(bar, 1u) + 1u;
-    if (arrived == gridDim.x) {
-      atomicExch(bar, 0u);
-      __threadfence();
-      atomicAdd(bar + 1, 1u);
-    } else {
-      long spins = 0;
-      while (*gen == g0) {
-        if (++spins > GRID_SPIN_LIMIT) { atomicExch(err, 1); break; }
-        if (*(volatile int*)err) break;
-        __nanosleep(64);
-      }
+    __threadfence();   // the CTA's writes (ordered before thread 0 by __syncthreads) at GPU scope
+    const unsigned old = atomicAdd(bar, 1u);
+    const unsigned target = (old / gridDim.x + 1u) * gridDim.x;
+    long spins = 0;
+    int ok = 1;
+    while ((int)(ld_acquire_gpu(bar) - target) < 0) {   // wrap-safe: count < target
+      if (++spins > GRID_SPIN_LIMIT) { atomicExch(err, 1); ok = 0; break; }
+      if ((spins & 63) == 0 && *(volatile int*)err) { ok = 0; break; }
     }
-    __threadfence();
+    __threadfence();   // the other CTAs' writes, seen through the acquire, ordered before the CTA's reads
+    if (ok && *(volatile int*)err) ok = 0;
+    s_ok = ok;
   }
   __syncthreads();
-  return *(volatile int*)err == 0;
+  return s_ok != 0;
 }
 
 }  // namespace bbt
