@@ -426,7 +426,22 @@ __global__ void apply_signs_kernel(int m, const double* __restrict__ d, double* 
 // barriers (sync.cuh): a barrier that times out sets the tensor-core wait
 // flag, reported by check_tc_flags, and every CTA leaves.
 
-constexpr int CT = 256;   // threads of the cooperative Cholesky
+// Right-looking blocked Cholesky G = R^T R (upper, 32 x 32 tiles), in place.
+// Per block row k: (1) every CTA that needs it factors the diagonal tile in
+// one warp (lane c holds column c in registers; step j broadcasts row j by
+// warp shuffles; the steps are unrolled at compile time so the column stays
+// in registers), keeps R_kk and the reciprocals of its diagonal in shared
+// memory, and solves its tile of the row panel, R_kj = R_kk^-T G_kj: the
+// tile is staged through shared memory with coalesced loads, lane c
+// forward-substitutes column c in registers; (2) the trailing tiles
+// G_ij -= R_ki^T R_kj, i <= j: four tiles per CTA at a time, one per pair of
+// warps, every load of the round (both panel tiles and the tile updated)
+// issued before any arithmetic.  Only the upper triangle of G is read; the
+// strictly lower triangle is zeroed at the end.
+constexpr int CT = 256;      // threads of the cooperative Cholesky
+constexpr int CGROUPS = 4;   // trailing tiles per CTA and round (two warps each)
+constexpr int TSTR = 33;     // padded row stride of a shared tile
+constexpr size_t POTRF_SMEM = (size_t)(1 + 2 * CGROUPS) * 32 * TSTR * sizeof(double) + 32 * sizeof(double);
 
 struct PotrfArgs {
   int n;
@@ -437,115 +452,172 @@ struct PotrfArgs {
   int* err;        // barrier timeout
 };
 
-// Right-looking blocked Cholesky G = R^T R (upper, 32 x 32 tiles), in place:
-// per block row k, (1) every CTA that needs it factors the diagonal tile in
-// one warp, lane c holding column c in registers (step j broadcasts row j by
-// warp shuffles), CTA 0 stores it, and each warp of the CTA solves one tile
-// of the row panel, R_kj = R_kk^-T G_kj, lane c forward-substituting column c
-// in registers against the factor in shared memory; (2) the trailing tiles
-// G_ij -= R_ki^T R_kj, i <= j, one tile per CTA at a time.  Only the upper
-// triangle of G is read; the strictly lower triangle is zeroed at the end.
-__device__ __forceinline__ void chol_tile_warp(double (&D)[32][33], int kb, int lane, int* flag) {
-  double x[32];
-#pragma unroll
-  for (int i = 0; i < 32; ++i) x[i] = D[i][lane];   // column lane (rows past kb: zero)
-#pragma unroll
-  for (int j = 0; j < 32; ++j) {
-    if (j < kb) {
-      double d = __shfl_sync(0xffffffffu, x[j], j);
+template <int J>
+__device__ __forceinline__ void chol_steps(double (&x)[32], int lane, int kb, int* flag) {
+  if constexpr (J < 32) {
+    if (J < kb) {
+      double d = __shfl_sync(0xffffffffu, x[J], J);
       if (!(d > 0.0) || !isfinite(d)) {
         if (lane == 0) atomicExch(flag, 1);
         d = 1.0;
       }
       const double r = sqrt(d);
-      if (lane == j) x[j] = r;
-      else if (lane > j) x[j] = x[j] / r;   // R(j, lane)
+      const double xj = x[J] / r;   // R(J, lane)
+      x[J] = lane == J ? r : (lane > J ? xj : x[J]);
 #pragma unroll
-      for (int i = j + 1; i < 32; ++i) {
-        const double rji = __shfl_sync(0xffffffffu, x[j], i);   // R(j, i) from lane i
-        if (lane >= i) x[i] -= rji * x[j];
+      for (int i = J + 1; i < 32; ++i) {
+        const double rji = __shfl_sync(0xffffffffu, x[J], i);   // R(J, i) from lane i
+        const double u = fma(-rji, x[J], x[i]);
+        x[i] = lane >= i ? u : x[i];
       }
     }
+    chol_steps<J + 1>(x, lane, kb, flag);
   }
+}
+
+// D (upper kb x kb, zero elsewhere) <- its Cholesky factor; rinv[i] = 1 / R(i, i).
+__device__ __forceinline__ void chol_tile_warp(double* D, double* rinv, int kb, int lane, int* flag) {
+  double x[32];
+#pragma unroll
+  for (int i = 0; i < 32; ++i) x[i] = D[i * TSTR + lane];   // column lane (rows past kb: zero)
+  chol_steps<0>(x, lane, kb, flag);
   __syncwarp();
 #pragma unroll
-  for (int i = 0; i < 32; ++i) D[i][lane] = (i <= lane && lane < kb) ? x[i] : 0.0;
+  for (int i = 0; i < 32; ++i) D[i * TSTR + lane] = (i <= lane && lane < kb) ? x[i] : 0.0;
+  __syncwarp();
+  if (lane < kb) rinv[lane] = 1.0 / D[lane * TSTR + lane];
+}
+
+// Column c of T (in shared memory) <- R_kk^-T column c: x_i = (t_i - sum_{s<i} R(s, i) x_s) / R(i, i).
+template <int I>
+__device__ __forceinline__ void trsm_steps(double (&x)[32], const double* D, const double* rinv, int kb) {
+  if constexpr (I < 32) {
+    if (I < kb) {
+      double s0 = x[I], s1 = 0.0;
+#pragma unroll
+      for (int t = 0; t < I; t += 2) {
+        s0 = fma(-D[t * TSTR + I], x[t], s0);
+        if (t + 1 < I) s1 = fma(-D[(t + 1) * TSTR + I], x[t + 1], s1);
+      }
+      x[I] = (s0 + s1) * rinv[I];
+    }
+    trsm_steps<I + 1>(x, D, rinv, kb);
+  }
 }
 
 __global__ void __launch_bounds__(CT, 1) potrf_coop_kernel(PotrfArgs P) {
-  __shared__ double D[32][33], A1[32][33], B1[32][33];
+  extern __shared__ double psm[];
+  double* D = psm;                          // R_kk
+  double* T = psm + 32 * TSTR;              // group tiles: [group][2][32][TSTR]
+  double* rinv = psm + (1 + 2 * CGROUPS) * 32 * TSTR;
   const int n = P.n, nb = (n + 31) / 32;
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = CT / 32;
+  const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
+  const long ld = P.ld;
   for (int k = 0; k < nb; ++k) {
     const int r0 = 32 * k, kb = min(32, n - r0);
-    if (blockIdx.x == 0 || k + 1 + (int)blockIdx.x < nb) {
-      for (int f = threadIdx.x; f < 1024; f += CT) {
-        const int i = f % 32, j = f / 32;
-        D[i][j] = (i < kb && j < kb && i <= j) ? P.G[(r0 + i) + (long)(r0 + j) * P.ld] : 0.0;
+    const int jt = k + 1 + blockIdx.x;   // this CTA's panel tile (at most one: nb <= 128 < 148)
+    if (blockIdx.x == 0 || jt < nb) {
+      for (int f = tid; f < 1024; f += CT) {
+        const int i = f & 31, j = f >> 5;
+        D[i * TSTR + j] = (i < kb && j < kb && i <= j) ? P.G[(r0 + i) + (long)(r0 + j) * ld] : 0.0;
+      }
+      // stage the panel tile G_kj (rows r0.., columns 32 jt..), coalesced along the rows
+      const int c0 = 32 * jt, jb = jt < nb ? min(32, n - c0) : 0;
+      for (int f = tid; f < 1024; f += CT) {
+        const int i = f & 31, c = f >> 5;
+        T[i * TSTR + c] = (i < kb && c < jb) ? P.G[(r0 + i) + (long)(c0 + c) * ld] : 0.0;
       }
       __syncthreads();
-      if (w == 0) chol_tile_warp(D, kb, lane, P.flag);
+      if (w == 0) chol_tile_warp(D, rinv, kb, lane, P.flag);
       __syncthreads();
       if (blockIdx.x == 0)
-        for (int f = threadIdx.x; f < 1024; f += CT) {
-          const int i = f % 32, j = f / 32;
-          if (i < kb && j < kb && i <= j) P.G[(r0 + i) + (long)(r0 + j) * P.ld] = D[i][j];
+        for (int f = tid; f < 1024; f += CT) {
+          const int i = f & 31, j = f >> 5;
+          if (i < kb && j < kb && i <= j) P.G[(r0 + i) + (long)(r0 + j) * ld] = D[i * TSTR + j];
         }
-      // R_kj = R_kk^-T G_kj: warp w takes every nw-th tile of this CTA's share, lane c column c
-      for (int j = k + 1 + blockIdx.x + w * gridDim.x; j < nb; j += nw * gridDim.x) {
-        const int c0 = 32 * j, jb = min(32, n - c0);
-        double* col = P.G + r0 + (long)(c0 + lane) * P.ld;
-        double x[32];
+      if (jb > 0) {
+        if (w == 0) {
+          double x[32];
 #pragma unroll
-        for (int i = 0; i < 32; ++i) x[i] = (i < kb && lane < jb) ? col[i] : 0.0;
+          for (int i = 0; i < 32; ++i) x[i] = T[i * TSTR + lane];
+          trsm_steps<0>(x, D, rinv, kb);
 #pragma unroll
-        for (int i = 0; i < 32; ++i) {
-          if (i < kb) {
-            double s = x[i];
-#pragma unroll
-            for (int t = 0; t < i; ++t) s -= D[t][i] * x[t];
-            x[i] = s / D[i][i];
-          }
+          for (int i = 0; i < 32; ++i) T[i * TSTR + lane] = x[i];
         }
-        if (lane < jb)
-#pragma unroll
-          for (int i = 0; i < 32; ++i)
-            if (i < kb) col[i] = x[i];
+        __syncthreads();
+        for (int f = tid; f < 1024; f += CT) {
+          const int i = f & 31, c = f >> 5;
+          if (i < kb && c < jb) P.G[(r0 + i) + (long)(c0 + c) * ld] = T[i * TSTR + c];
+        }
       }
     }
     if (!grid_sync(P.bar, P.err)) return;
-    const int T = nb - k - 1, count = T * (T + 1) / 2;
-    for (int q = blockIdx.x; q < count; q += gridDim.x) {
-      int a = 0, rem = q;   // q -> (a, b), 0 <= a <= b < T, row by row
-      while (rem >= T - a) {
-        rem -= T - a;
-        ++a;
+    // trailing tiles (bi, bj), k < bi <= bj, numbered row by row; group g of
+    // this CTA takes tiles blockIdx.x + (g + CGROUPS r) gridDim.x
+    const int Tn = nb - k - 1, count = Tn * (Tn + 1) / 2;
+    const int g = w >> 1, gt = tid & 63;
+    double* A1 = T + (size_t)g * 2 * 32 * TSTR;
+    double* B1 = A1 + 32 * TSTR;
+    for (int base = 0; base < count; base += CGROUPS * gridDim.x) {
+      const int q = base + blockIdx.x + g * gridDim.x;
+      const bool live = q < count;
+      int bi = 0, bj = 0;
+      if (live) {
+        int a = 0, rem = q;
+        while (rem >= Tn - a) {
+          rem -= Tn - a;
+          ++a;
+        }
+        bi = k + 1 + a;
+        bj = k + 1 + a + rem;
       }
-      const int bi = k + 1 + a, bj = k + 1 + a + rem;
-      const int i0 = 32 * bi, j0 = 32 * bj, ib = min(32, n - i0), jb = min(32, n - j0);
-      __syncthreads();
-      for (int f = threadIdx.x; f < 1024; f += CT) {
-        const int t = f % 32, c = f / 32;
-        A1[t][c] = (t < kb && c < ib) ? P.G[(r0 + t) + (long)(i0 + c) * P.ld] : 0.0;
-        B1[t][c] = (t < kb && c < jb) ? P.G[(r0 + t) + (long)(j0 + c) * P.ld] : 0.0;
-      }
-      __syncthreads();
-      const int ii = lane;
+      const int i0 = 32 * bi, j0 = 32 * bj, ib = live ? min(32, n - i0) : 0, jb = live ? min(32, n - j0) : 0;
+      const int ii = gt & 31, jh = gt >> 5;
+      // the tile's 16 outputs of this thread, loaded with the panel tiles
+      double c[16];
 #pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        const int jj = w + nw * e;
-        double acc = 0.0;
-#pragma unroll 8
-        for (int t = 0; t < 32; ++t) acc = fma(A1[t][ii], B1[t][jj], acc);
-        if (ii < ib && jj < jb && (bi < bj || ii <= jj)) P.G[(i0 + ii) + (long)(j0 + jj) * P.ld] -= acc;
+      for (int e = 0; e < 16; ++e) {
+        const int jj = jh + 2 * e;
+        c[e] = (ii < ib && jj < jb) ? P.G[(i0 + ii) + (long)(j0 + jj) * ld] : 0.0;
+      }
+      double av[16], bv[16];
+#pragma unroll
+      for (int e = 0; e < 16; ++e) {
+        const int f = gt + 64 * e, t = f & 31, cc = f >> 5;
+        av[e] = (t < kb && cc < ib) ? P.G[(r0 + t) + (long)(i0 + cc) * ld] : 0.0;
+        bv[e] = (t < kb && cc < jb) ? P.G[(r0 + t) + (long)(j0 + cc) * ld] : 0.0;
+      }
+      __syncthreads();   // the previous round's readers are done with A1, B1
+#pragma unroll
+      for (int e = 0; e < 16; ++e) {
+        const int f = gt + 64 * e, t = f & 31, cc = f >> 5;
+        A1[t * TSTR + cc] = av[e];
+        B1[t * TSTR + cc] = bv[e];
+      }
+      __syncthreads();
+      if (live) {
+        double acc[16];
+#pragma unroll
+        for (int e = 0; e < 16; ++e) acc[e] = 0.0;
+#pragma unroll 4
+        for (int t = 0; t < 32; ++t) {
+          const double a = A1[t * TSTR + ii];
+#pragma unroll
+          for (int e = 0; e < 16; ++e) acc[e] = fma(a, B1[t * TSTR + jh + 2 * e], acc[e]);
+        }
+#pragma unroll
+        for (int e = 0; e < 16; ++e) {
+          const int jj = jh + 2 * e;
+          if (ii < ib && jj < jb && (bi < bj || ii <= jj)) P.G[(i0 + ii) + (long)(j0 + jj) * ld] = c[e] - acc[e];
+        }
       }
     }
     if (!grid_sync(P.bar, P.err)) return;
   }
   const long total = (long)n * n;
-  for (long f = blockIdx.x * (long)CT + threadIdx.x; f < total; f += (long)gridDim.x * CT) {
+  for (long f = blockIdx.x * (long)CT + tid; f < total; f += (long)gridDim.x * CT) {
     const int i = (int)(f % n), j = (int)(f / n);
-    if (i > j) P.G[i + (long)j * P.ld] = 0.0;
+    if (i > j) P.G[i + (long)j * ld] = 0.0;
   }
 }
 
@@ -642,13 +714,19 @@ __global__ void __launch_bounds__(LT, 1) lu_sign_coop_kernel(LuArgs P) {
             for (int r = 0; r < pb; ++r) P.A[(p0 + r) + (long)(c0 + c) * P.lda] = U[r][c];
         }
         __syncthreads();
-        if (live)
-#pragma unroll 4
-          for (int c = 0; c < cw; ++c) {
-            double s = 0.0;
+        if (live)   // eight columns at a time: their loads issued before any store
 #pragma unroll
-            for (int t = 0; t < LB; ++t) s = fma(l[t], U[t][c], s);
-            P.A[i + (long)(c0 + c) * P.lda] -= s;
+          for (int h = 0; h < LB; h += 8) {
+            double a[8];
+#pragma unroll
+            for (int c = 0; c < 8; ++c) a[c] = (h + c < cw) ? P.A[i + (long)(c0 + h + c) * P.lda] : 0.0;
+#pragma unroll
+            for (int c = 0; c < 8; ++c) {
+              double s = 0.0;
+#pragma unroll
+              for (int t = 0; t < LB; ++t) s = fma(l[t], U[t][h + c], s);
+              if (h + c < cw) P.A[i + (long)(c0 + h + c) * P.lda] = a[c] - s;
+            }
           }
       }
       __syncthreads();
@@ -660,9 +738,10 @@ __global__ void __launch_bounds__(LT, 1) lu_sign_coop_kernel(LuArgs P) {
 
 // Co-resident CTAs of a cooperative kernel: at most one per SM, at most `want`.
 template <class K>
-int coop_grid(bbt_ctx* ctx, K kernel, int threads, int want) {
+int coop_grid(bbt_ctx* ctx, K kernel, int threads, int want, size_t smem = 0) {
   int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0) != cudaSuccess || per_sm < 1) return 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess || per_sm < 1)
+    return 0;
   return std::max(1, std::min(want, ctx->num_sms));
 }
 
@@ -760,13 +839,19 @@ bbt_status potrf_upper(bbt_ctx* ctx, int n, double* G, long ld, int* flag) {
   if (n <= 0) return BBT_OK;
   if (ctx->allow_coop && n > PB && n <= 4096) {   // one cooperative launch
     const int nb = (n + 31) / 32;
-    const int grid = coop_grid(ctx, potrf_coop_kernel, CT, nb * (nb - 1) / 2);
-    if (grid > 0) {
+    static bool attr = false;
+    if (!attr) {
+      BBT_CUDA(ctx, cudaFuncSetAttribute(potrf_coop_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)POTRF_SMEM));
+      attr = true;
+    }
+    const int grid = coop_grid(ctx, potrf_coop_kernel, CT, nb * (nb - 1) / 2, POTRF_SMEM);
+    if (grid >= nb - 1) {   // one CTA per tile of every row panel
       ProfScope prof(ctx, BBT_PROF_CHOL, (double)n * n * n / 3.0);
       PotrfArgs P{n, G, ld, flag, ctx->d_barrier, ctx->d_flag + FLAG_SKETCH};
       BBT_CUDA(ctx, cudaMemsetAsync(ctx->d_barrier, 0, 2 * sizeof(unsigned), ctx->stream));
       void* args[] = {&P};
-      BBT_CUDA(ctx, cudaLaunchCooperativeKernel((void*)potrf_coop_kernel, dim3(grid), dim3(CT), args, 0,
+      BBT_CUDA(ctx, cudaLaunchCooperativeKernel((void*)potrf_coop_kernel, dim3(grid), dim3(CT), args, POTRF_SMEM,
                                                 ctx->stream));
       BBT_LAUNCHED(ctx);
       return BBT_OK;

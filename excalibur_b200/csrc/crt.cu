@@ -11,9 +11,10 @@
 // one u8 x u8 -> int32 GEMM (tcgen05 kind::i8, 128 x 256 tiles, one TMEM
 // accumulator), exact for up to 2^15 terms per K-split.  The
 // residues of T are written as bytes and the integer is rebuilt from them
-// (crt_combine): with y_p = (T mod p) ((M/p)^-1 mod p) mod p, T/M = sum_p y_p / p
-// mod 1 (M = prod p), evaluated as a 128-bit fixed-point sum of y_p
-// floor(2^128 / p) whose wrap-around discards the integer part exactly.  n is
+// (crt_combine): T/M = sum_p (T mod p) ((M/p)^-1 mod p) / p mod 1 (M = prod p),
+// evaluated as a 128-bit fixed-point sum of (T mod p) G_p, G_p =
+// floor(2^128 ((M/p)^-1 mod p) / p), whose wrap-around discards the integer
+// part exactly (no reduction of the CRT digit mod p is needed).  n is
 // chosen so that |T| < M / 2, so the centred fraction times M is T itself, to
 // about 2^-110 of the largest possible |T|.
 //
@@ -77,6 +78,21 @@ constexpr uint32_t flimb_c(int p, int l) {   // 32-bit limb l of floor(2^128 / p
   }
   return q[4 - l];
 }
+// 32-bit limb l of G = floor(2^128 inv / p) (inv < p, so G < 2^128):
+// inv floor(2^128 / p) + floor(inv (2^128 mod p) / p), least significant limb first.
+constexpr uint32_t glimb_c(int p, int inv, int l) {
+  uint64_t limb[4] = {flimb_c(p, 0), flimb_c(p, 1), flimb_c(p, 2), flimb_c(p, 3)};
+  uint64_t rem = 1;   // 2^128 mod p, by doubling
+  for (int i = 0; i < 128; ++i) rem = (2 * rem) % (uint64_t)p;
+  uint64_t carry = ((uint64_t)inv * rem) / (uint64_t)p;
+  uint32_t out[4] = {0, 0, 0, 0};
+  for (int i = 0; i < 4; ++i) {
+    const uint64_t t = limb[i] * (uint64_t)inv + carry;
+    out[i] = (uint32_t)t;
+    carry = t >> 32;
+  }
+  return out[l];
+}
 template <int Q>
 struct ModR {   // residues of an integer t = a 2^36 + b 2^18 + c
   static constexpr int p = MODULI[Q];
@@ -90,6 +106,10 @@ struct ModK {   // reconstruction from the residues of an NM-modulus set
   static constexpr uint32_t magic32 = (uint32_t)((((uint64_t)1 << 32) + p - 1) / p);
   static constexpr uint32_t inv = (uint32_t)crt_inv_c(Q, NM);
   static constexpr uint32_t F0 = flimb_c(p, 0), F1 = flimb_c(p, 1), F2 = flimb_c(p, 2), F3 = flimb_c(p, 3);
+  // r G / 2^128 = r inv / p (mod 1) up to r units of 2^-128: the CRT digit's
+  // fraction straight from the residue r, with no reduction of r inv mod p
+  static constexpr uint32_t G0 = glimb_c(p, (int)inv, 0), G1 = glimb_c(p, (int)inv, 1),
+                            G2 = glimb_c(p, (int)inv, 2), G3 = glimb_c(p, (int)inv, 3);
 };
 
 constexpr int TM = 128, TN = 256, TK = 128;   // TK: bytes of K per stage row (SWIZZLE_128B)
@@ -495,9 +515,11 @@ __device__ __forceinline__ uint32_t mod_c(uint32_t x) {
 }
 
 // Four consecutive outputs: one 32-bit word of residues per modulus (and split).
-// LIMBS = 4: the fraction to 128 bits (double-double outputs); 3: to 96 bits
-// (FP64 outputs: the missing 32 bits are below 2^-75 of the largest |T|), the
-// limbs of floor(2^96 / p) being the top three of floor(2^128 / p).
+// The fraction T / M (mod 1) is sum_q r_q G_q / 2^128 (mod 1), r_q = T mod p_q
+// and G_q = floor(2^128 ((M / p_q)^-1 mod p_q) / p_q): each term is short by
+// less than r_q < 256 units of its last limb.  LIMBS = 4: the fraction to 128
+// bits (double-double outputs); 3: to 96 bits (FP64 outputs: the missing 32
+// bits are below 2^-75 of the largest |T|), the top three limbs of G_q.
 // SPLIT: the product came in several K-splits, whose residues are summed
 // first; with one split every byte is already a residue in [0, p).
 template <int Q, int NM, int LIMBS, bool SPLIT>
@@ -515,11 +537,11 @@ __device__ __forceinline__ void frac4_q(const CombArgs& A, long f, long total, u
     }
 #pragma unroll
   for (int e = 0; e < 4; ++e) {
-    const uint32_t y = mod_c<C>((SPLIT ? mod_c<C>(s[e]) : s[e]) * C::inv);
-    if (LIMBS == 4) L[e][0] += (uint64_t)y * C::F0;   // 32 x 32 -> 64-bit products, < 2^40 each
-    L[e][1] += (uint64_t)y * C::F1;
-    L[e][2] += (uint64_t)y * C::F2;
-    L[e][3] += (uint64_t)y * C::F3;
+    const uint32_t r = SPLIT ? mod_c<C>(s[e]) : s[e];
+    if (LIMBS == 4) L[e][0] += (uint64_t)r * C::G0;   // 32 x 32 -> 64-bit products, < 2^40 each
+    L[e][1] += (uint64_t)r * C::G1;
+    L[e][2] += (uint64_t)r * C::G2;
+    L[e][3] += (uint64_t)r * C::G3;
   }
 }
 template <int NM, int LIMBS, bool SPLIT, int... Q>
@@ -664,7 +686,7 @@ combine_dd_kernel(CombArgs A, const double* __restrict__ sa, const double* __res
 // For products with one K-split (K <= 2^15), one CTA owns a 128 x TNF output
 // tile over every modulus: the MMAs of modulus q run into one of two TMEM
 // accumulators while the epilogue warps reduce the other one mod p_q and add
-// y_q floor(2^96 / p_q) into a 96-bit fixed-point sum per output (three
+// (T mod p_q) G_q into a 96-bit fixed-point sum per output (three
 // 32-bit limbs, the carries propagated every modulus: the same value mod 2^96
 // as crt_combine's 64-bit limb sums).  The two low limbs live in TMEM beside
 // the accumulators (2 x 128 + 2 x 128 = 512 columns), the high limb in
@@ -690,9 +712,9 @@ struct FusedArgs {
   int* err;
 };
 
-// One 8-column batch of modulus Q: T mod p_Q from the int32 accumulator (as
-// the unfused epilogue reduces it), y = (T mod p) ((M / p)^-1 mod p) mod p,
-// S += y floor(2^96 / p) (mod 2^96).
+// One 8-column batch of modulus Q: r = T mod p_Q from the int32 accumulator
+// (as the unfused epilogue reduces it), S += r G_Q (mod 2^96, the top three
+// limbs of G_Q = floor(2^128 ((M / p)^-1 mod p) / p)).
 // The accumulator of u8 x u8 products over at most 2^15 terms is a
 // non-negative int32 below 2^31: (a >> 16) c16 + (a & 0xFFFF) < 2^24 is
 // congruent to it, and its multiply-high quotient by p is exact, so r is
@@ -709,12 +731,11 @@ __device__ __forceinline__ void fused_add8(const uint32_t (&v)[8], uint32_t (&s0
     const uint32_t a = v[e];
     const uint32_t x = (a >> 16) * c16 + (a & 0xFFFFu);
     const uint32_t r = x - __umulhi(x, magic) * (uint32_t)p;
-    const uint32_t y = mod_c<K>(r * K::inv);
-    uint64_t t = (uint64_t)y * K::F1 + s0[e];
+    uint64_t t = (uint64_t)r * K::G1 + s0[e];
     s0[e] = (uint32_t)t;
-    t = (uint64_t)y * K::F2 + s1[e] + (t >> 32);
+    t = (uint64_t)r * K::G2 + s1[e] + (t >> 32);
     s1[e] = (uint32_t)t;
-    s2[e] += y * K::F3 + (uint32_t)(t >> 32);
+    s2[e] += r * K::G3 + (uint32_t)(t >> 32);
   }
 }
 

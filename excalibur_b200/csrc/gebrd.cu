@@ -25,13 +25,18 @@
 //
 // Column step j, five phases separated by bounded grid barriers:
 //   B: column reflector of the updated column j (its norm from per-CTA
-//      partials), gemv pass 1 (one warp per column) and the partials of
-//      V^T v_j, X^T v_j;
+//      partials), gemv pass 1 (one warp per column and chunk of rows,
+//      per-chunk partials) and the partials of V^T v_j, X^T v_j;
 //   C: y_j, the updated row j (its norm's partials); v_j written to A;
-//   D: row reflector, gemv pass 2 (32-row x 512-column tiles, per-chunk
+//   D: row reflector, gemv pass 2 (32-row x cch-column tiles, per-chunk
 //      partials) and the partials of Y^T u_j, U u_j; u_j written to A;
 //   E: x_j, and the update of column j+1 with the partials of its norm.
 // Every reduction is summed in a fixed order, so the result is deterministic.
+// The gemv chunks are sized per panel to minimise the busiest warp's work
+// (its items times the chunk length): many short items while the trailing
+// matrix is small (the passes are latency-bound there), few long ones with
+// no ragged last round when it is large (bandwidth-bound); loads of a row or
+// column are issued before the stores that follow them.
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
@@ -46,7 +51,6 @@ namespace {
 constexpr int NB = 32;      // panel width
 constexpr int GT = 256;
 constexpr int GW = GT / 32;
-constexpr int CCH = 512;    // columns per gemv-2 partial
 constexpr int PG = 32;      // CTAs that form the panel-correction partials
 
 struct PanelArgs {
@@ -60,9 +64,11 @@ struct PanelArgs {
   double* taup;
   double* X;       // M x NB, ld M
   double* Y;       // M x NB, ld M
-  double* g;       // M: gemv pass 1
+  double* g;       // [nr1][M]: gemv pass 1 partials, by row chunk
   double* rowb;    // M: the updated row j
-  double* hp;      // [ceil(M / CCH)][M]: gemv pass 2 partials
+  double* hp;      // [ncc][M]: gemv pass 2 partials, by column chunk
+  int nr1, r1;     // gemv pass 1: row chunks (of r1 rows) per column
+  int ncc, cch;    // gemv pass 2: column chunks (of cch columns) per 32-row block
   double* colp;    // [grid]
   double* rowp;    // [grid]
   double* pq;      // [PG][2 NB]
@@ -144,21 +150,29 @@ __global__ void __launch_bounds__(GT) labrd_kernel(PanelArgs P) {
     const double tq = sc[1], sq = sc[2];
     if (blockIdx.x == 0 && tid == 0) { P.d[j] = sc[0]; P.tauq[j] = tq; }
     if (j == M - 1) break;   // the last diagonal entry: no row reflector
-    for (int c = j + 1 + gw; c < M; c += nwarps) {   // g_c = v^T A(j:, c), v_j(j) = 1
-      const double* col = A + c * ld;
-      double s = 0.0;
-      int r = j + 1 + lane;
-      for (; r + 7 * 32 < M; r += 8 * 32) {   // eight loads in flight per lane
-        double a[8], v[8];
+    {   // g_c = v^T A(j:, c), v_j(j) = 1: one warp per (column, chunk of r1 rows), partials by chunk
+      const int ncol = M - j - 1, items = ncol * P.nr1;
+      for (int it = gw; it < items; it += nwarps) {
+        const int c = j + 1 + it % ncol, rc = it / ncol;
+        const double* col = A + c * ld;
+        const int re = min(M, (rc + 1) * P.r1);
+        double s = 0.0, s1 = 0.0;
+        int r = max(j + 1, rc * P.r1) + lane;
+        for (; r + 7 * 32 < re; r += 8 * 32) {   // eight loads in flight per lane
+          double a[8], v[8];
 #pragma unroll
-        for (int u = 0; u < 8; ++u) { a[u] = col[r + u * 32]; v[u] = cj[r + u * 32]; }
+          for (int u = 0; u < 8; ++u) { a[u] = col[r + u * 32]; v[u] = cj[r + u * 32]; }
 #pragma unroll
-        for (int u = 0; u < 8; ++u) s += a[u] * v[u];
+          for (int u = 0; u < 8; u += 2) {
+            s += a[u] * v[u];
+            s1 += a[u + 1] * v[u + 1];
+          }
+        }
+        for (; r < re; r += 32) s += col[r] * cj[r];
+        s += s1;
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) P.g[(long)rc * M + c] = s;
       }
-      for (; r < M; r += 32) s += col[r] * cj[r];
-      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-      // column j still holds the updated column a_j (scaled to v_j in phase C)
-      if (lane == 0) P.g[c] = col[j] + sq * s;
     }
     if (blockIdx.x < PG && j > 0) {   // rows split over PG CTAs: p_k = V(:, k)^T v, q_k = X(:, k)^T v
       const int rows = M - j, per = (rows + PG - 1) / PG;
@@ -177,12 +191,15 @@ __global__ void __launch_bounds__(GT) labrd_kernel(PanelArgs P) {
     {
       double pr = 0.0;
       for (long c = j + 1 + gtid; c < M; c += nthr) {
-        double y = P.g[c];
-        for (int k = 0; k < j; ++k) y -= Y[c + (long)k * M] * cor[k] + A[k + c * ld] * cor[j + k];
-        y *= tq;
-        P.Y[c + (long)j * M] = y;
-        double r = A[j + c * ld] - y;   // V(j, j) = 1
+        // column j still holds the updated column a_j (scaled to v_j below)
+        double gs = 0.0;
+        for (int rc = 0; rc < P.nr1; ++rc) gs += P.g[(long)rc * M + c];
+        double gy = A[j + c * ld] + sq * gs;
+        for (int k = 0; k < j; ++k) gy -= Y[c + (long)k * M] * cor[k] + A[k + c * ld] * cor[j + k];
+        gy *= tq;
+        double r = A[j + c * ld] - gy;   // V(j, j) = 1
         for (int k = 0; k < j; ++k) r -= A[j + k * ld] * Y[c + (long)k * M] + X[j + (long)k * M] * A[k + c * ld];
+        P.Y[c + (long)j * M] = gy;   // stores after every load of the row
         P.rowb[c] = r;
         if (c >= j + 2) pr += r * r;
       }
@@ -205,13 +222,16 @@ __global__ void __launch_bounds__(GT) labrd_kernel(PanelArgs P) {
     const double tp = sc[4], sp = sc[5];
     if (blockIdx.x == 0 && tid == 0) { P.e[j] = sc[3]; P.taup[j] = tp; }
     {
-      const int r0 = j + 1, c0 = j + 1;
-      const int nrb = (M - r0 + 31) / 32, ncc = (M - c0 + CCH - 1) / CCH;
+      // (32-row block, column chunk cc of cch columns) per warp; the chunks are
+      // absolute (columns [cc cch, (cc + 1) cch) past j), so phase E sums the
+      // same ncc partials in the same order for every step of the panel
+      const int r0 = j + 1;
+      const int nrb = (M - r0 + 31) / 32, ncc = P.ncc;
       for (int item = gw; item < nrb * ncc; item += nwarps) {
         const int rb = item % nrb, cc = item / nrb;
         const int r = r0 + rb * 32 + lane;
-        const int ca = c0 + cc * CCH, cb = min(M, ca + CCH);
-        double s = 0.0;
+        const int ca = max(j + 1, cc * P.cch), cb = min(M, (cc + 1) * P.cch);
+        double s = 0.0, s1 = 0.0;
         if (r < M) {
           int c = ca;
           for (; c + 7 < cb; c += 8) {
@@ -222,10 +242,13 @@ __global__ void __launch_bounds__(GT) labrd_kernel(PanelArgs P) {
               u[q] = (c + q == j + 1) ? 1.0 : P.rowb[c + q] * sp;
             }
 #pragma unroll
-            for (int q = 0; q < 8; ++q) s += a[q] * u[q];
+            for (int q = 0; q < 8; q += 2) {
+              s += a[q] * u[q];
+              s1 += a[q + 1] * u[q + 1];
+            }
           }
           for (; c < cb; ++c) s += A[r + c * ld] * ((c == j + 1) ? 1.0 : P.rowb[c] * sp);
-          P.hp[(long)cc * M + r] = s;
+          P.hp[(long)cc * M + r] = s + s1;
         }
       }
     }
@@ -248,7 +271,7 @@ __global__ void __launch_bounds__(GT) labrd_kernel(PanelArgs P) {
     // ---- E: x_j and the update of column j+1 (and its norm's partials)
     sum_partials(P.st, 2 * j + 1, cor);
     {
-      const int ncc = (M - (j + 1) + CCH - 1) / CCH;
+      const int ncc = P.ncc;
       const bool next = j + 1 < P.nbp;
       double* cn = A + (j + 1) * ld;
       double pn = 0.0;
@@ -258,7 +281,6 @@ __global__ void __launch_bounds__(GT) labrd_kernel(PanelArgs P) {
         for (int k = 0; k <= j; ++k) h -= A[r + k * ld] * cor[k];
         for (int k = 0; k < j; ++k) h -= X[r + (long)k * M] * cor[j + 1 + k];
         const double x = tp * h;
-        P.X[r + (long)j * M] = x;
         if (next) {   // column j+1 of A_{j+1}: U(k, j+1) = A(k, j+1) for k < j, U(j, j+1) = 1
           double a = cn[r] - x;
           for (int k = 0; k <= j; ++k) a -= A[r + k * ld] * Y[(j + 1) + (long)k * M];
@@ -266,6 +288,7 @@ __global__ void __launch_bounds__(GT) labrd_kernel(PanelArgs P) {
           cn[r] = a;
           if (r >= j + 2) pn += a * a;
         }
+        P.X[r + (long)j * M] = x;   // after the loads of X above
       }
       pn = bsum(pn, sh);
       if (tid == 0) P.colp[blockIdx.x] = pn;
@@ -290,9 +313,11 @@ bbt_status gebrd(bbt_ctx* ctx, int n, double* A, double* d, double* e, double* t
   P.ld = n;
   P.X = ctx->ws.take<double>((size_t)n * NB);
   P.Y = ctx->ws.take<double>((size_t)n * NB);
-  P.g = ctx->ws.take<double>(n);
   P.rowb = ctx->ws.take<double>(n);
-  P.hp = ctx->ws.take<double>((size_t)((n + CCH - 1) / CCH) * n);
+  const int nwarps = grid * GW;
+  const int nr1_max = 16, ncc_max = (n + 63) / 64;
+  P.g = ctx->ws.take<double>((size_t)nr1_max * n);
+  P.hp = ctx->ws.take<double>((size_t)ncc_max * n);
   P.colp = ctx->ws.take<double>(grid);
   P.rowp = ctx->ws.take<double>(grid);
   P.pq = ctx->ws.take<double>(PG * 2 * NB);
@@ -315,6 +340,26 @@ bbt_status gebrd(bbt_ctx* ctx, int n, double* A, double* d, double* e, double* t
       P.e = e + i0;
       P.tauq = tauq + i0;
       P.taup = taup + i0;
+      // gemv chunking: the chunk count that minimises the busiest warp's work,
+      // (items per warp, rounded up) x (chunk length), so that neither a long
+      // tail round (large trailing matrix) nor long serial chunks (small one)
+      // set the step's time
+      auto best_chunks = [&](int units, int len, int cap, int align) {
+        int best = 1;
+        long cost = -1;
+        for (int c = 1; c <= cap; ++c) {
+          const long chunk = ((len + c - 1) / c + align - 1) / align * align;
+          const long rounds = ((long)units * c + nwarps - 1) / nwarps;
+          const long cst = rounds * chunk + 8L * c;   // + the partials summed per output
+          if (cost < 0 || cst < cost) { cost = cst; best = c; }
+        }
+        return best;
+      };
+      P.nr1 = best_chunks(M, M, nr1_max, 32);
+      P.r1 = ((M + P.nr1 - 1) / P.nr1 + 31) / 32 * 32;
+      const int nrb = (M + 31) / 32;
+      P.ncc = best_chunks(nrb, M, std::max(1, std::min(ncc_max, (M + 63) / 64)), 8);
+      P.cch = ((M + P.ncc - 1) / P.ncc + 7) / 8 * 8;
       void* args[] = {&P};
       BBT_CUDA(ctx, cudaLaunchCooperativeKernel((void*)labrd_kernel, dim3(grid), dim3(GT), args, 0, ctx->stream));
       BBT_LAUNCHED(ctx);

@@ -22,7 +22,9 @@
 //   B2 (row-partitioned, one warp per row): W[r] += (-tau vt) h_r for
 //      r > i, and, in the same pass, the next step's Gram row
 //      g'[r] = W[r] . W[i+1].
-// The passes over W keep four loads in flight per thread.
+// The passes over W keep sixteen loads in flight per thread; B2 reads the two
+// vectors every row needs (-tau vt and the updated row i+1) from shared
+// memory, staged once per CTA and step.
 //
 // Barriers spin a bounded number of times; on a timeout every CTA stops and
 // the host reports BBT_ERR_TIMEOUT.
@@ -39,6 +41,8 @@ namespace {
 constexpr int RT = 256;                 // threads per CTA
 constexpr int RW = RT / 32;             // warps per CTA
 constexpr int CB = 8;                   // columns per pass of B1
+constexpr int RB = 16;                  // loads in flight per thread in the passes over W
+constexpr size_t RALHA_STAGE_MAX = 200 * 1024;   // shared bytes for the staged vectors (n <= 12800)
 
 struct RalhaArgs {
   int m, n;
@@ -53,8 +57,9 @@ struct RalhaArgs {
   double* vt;      // n
   double* tv;      // n: -tau * vt
   double* nextw;   // n: row i+1 after the update
-  unsigned* bar;   // [0] arrivals, [1] generation
+  unsigned* bar;   // grid barrier
   int* err;
+  int stage;       // 1: B2 reads tv and nextw from shared memory (2n doubles)
 };
 
 __device__ double block_sum(double v, double* sh) {
@@ -108,12 +113,16 @@ __device__ void gram_rows(const RalhaArgs& A, int i, const double* piv, double* 
 }
 
 __global__ void __launch_bounds__(RT, 1) ralha_kernel(RalhaArgs A) {
+  extern __shared__ double st_dyn[];
   __shared__ double sh[RW];
   __shared__ double sh4[RW][4];
   __shared__ double scal[6];   // beta_{i-1}, alpha_i, tau, scale, 1/alpha_i
   __shared__ double red[RT / CB][CB + 1];
   const int m = A.m, n = A.n;
   const int tid = threadIdx.x;
+  const bool stage = A.stage != 0;   // tv and nextw copied to shared memory for B2
+  double* st_tv = st_dyn;
+  double* st_nw = st_dyn + n;
   // ---- step 0 set-up: alpha_0, v_0 (CTA 0); Gram row of w_0 (all)
   if (blockIdx.x == 0) {
     double s = 0.0;
@@ -188,7 +197,6 @@ __global__ void __launch_bounds__(RT, 1) ralha_kernel(RalhaArgs A) {
         const int c = c0 + cb + (tid % CB);
         double s = 0.0;
         if (c < c1) {
-          // four rows per iteration: their loads are in flight together
           constexpr int PH = RT / CB;
           const double* wc = A.W + (long)(i + 1) * n + c;
           double s1 = 0.0;
@@ -197,16 +205,20 @@ __global__ void __launch_bounds__(RT, 1) ralha_kernel(RalhaArgs A) {
             s = wc[0];   // h_0 = 1
             t += PH;
           }
-          for (; t + 3 * PH < len; t += 4 * PH) {
-            const double w0 = wc[(long)t * n], w1 = wc[(long)(t + PH) * n];
-            const double w2 = wc[(long)(t + 2 * PH) * n], w3 = wc[(long)(t + 3 * PH) * n];
-            const double h0 = g[t], h1 = g[t + PH], h2 = g[t + 2 * PH], h3 = g[t + 3 * PH];
-            s += (h0 * scl) * w0;
-            s1 += (h1 * scl) * w1;
-            s += (h2 * scl) * w2;
-            s1 += (h3 * scl) * w3;
+          for (; t < len; t += RB * PH) {   // RB rows' loads in flight, the last batch masked
+            double w[RB], hh[RB];
+#pragma unroll
+            for (int e = 0; e < RB; ++e) {
+              const bool in = t + e * PH < len;
+              w[e] = in ? wc[(long)(t + e * PH) * n] : 0.0;
+              hh[e] = in ? g[t + e * PH] : 0.0;
+            }
+#pragma unroll
+            for (int e = 0; e < RB; e += 2) {
+              s += (hh[e] * scl) * w[e];
+              s1 += (hh[e + 1] * scl) * w[e + 1];
+            }
           }
-          for (; t < len; t += PH) s += (g[t] * scl) * wc[(long)t * n];
           s += s1;
         }
         red[tid / CB][tid % CB] = s;
@@ -254,6 +266,18 @@ __global__ void __launch_bounds__(RT, 1) ralha_kernel(RalhaArgs A) {
     if (!grid_sync(A.bar, A.err)) return;
     // ---- B2: rank-1 update of rows i+1.., next Gram row
     {
+      // -tau vt and row i+1 after the update, read by every row: staged once per CTA
+      const double* tv = A.tv;
+      const double* nw_ = A.nextw;
+      if (stage) {
+        for (int c = tid; c < n; c += RT) {
+          st_tv[c] = A.tv[c];
+          st_nw[c] = A.nextw[c];
+        }
+        __syncthreads();
+        tv = st_tv;
+        nw_ = st_nw;
+      }
       const int gw = blockIdx.x * RW + (tid >> 5), lane = tid & 31;
       const int nw = gridDim.x * RW;
       for (int r = i + 1 + gw; r < m; r += nw) {
@@ -261,25 +285,21 @@ __global__ void __launch_bounds__(RT, 1) ralha_kernel(RalhaArgs A) {
         const double h = (t == 0) ? 1.0 : g[t] * scl;
         double* row = A.W + (long)r * n;
         double s = 0.0, s1 = 0.0;
-        int c = lane;
-        for (; c + 96 < n; c += 128) {   // four segments per iteration, loads in flight together
-          const double r0 = row[c], r1 = row[c + 32], r2 = row[c + 64], r3 = row[c + 96];
-          const double t0 = A.tv[c], t1 = A.tv[c + 32], t2 = A.tv[c + 64], t3 = A.tv[c + 96];
-          const double x0 = A.nextw[c], x1 = A.nextw[c + 32], x2 = A.nextw[c + 64], x3 = A.nextw[c + 96];
-          const double w0 = r0 + t0 * h, w1 = r1 + t1 * h, w2 = r2 + t2 * h, w3 = r3 + t3 * h;
-          row[c] = w0;
-          row[c + 32] = w1;
-          row[c + 64] = w2;
-          row[c + 96] = w3;
-          s += w0 * x0;
-          s1 += w1 * x1;
-          s += w2 * x2;
-          s1 += w3 * x3;
-        }
-        for (; c < n; c += 32) {
-          const double w = row[c] + A.tv[c] * h;
-          row[c] = w;
-          s += w * A.nextw[c];
+        // batches of RB segments: all loads of a batch issued before its stores
+        for (int c = lane; c < n; c += RB * 32) {
+          double w[RB];
+#pragma unroll
+          for (int e = 0; e < RB; ++e) w[e] = (c + 32 * e < n) ? row[c + 32 * e] : 0.0;
+#pragma unroll
+          for (int e = 0; e < RB; ++e)
+            if (c + 32 * e < n) {
+              w[e] = fma(tv[c + 32 * e], h, w[e]);
+              if (e & 1) s1 = fma(w[e], nw_[c + 32 * e], s1);
+              else s = fma(w[e], nw_[c + 32 * e], s);
+            }
+#pragma unroll
+          for (int e = 0; e < RB; ++e)
+            if (c + 32 * e < n) row[c + 32 * e] = w[e];
         }
         s = warp_sum(s + s1);
         // g for step i+1 has entries for rows >= i+2
@@ -366,13 +386,22 @@ bbt_status ralha(bbt_ctx* ctx, int m, int n, double* W, double* house, double* t
   if (!A.nextw) return fail(ctx, BBT_ERR_NOMEM, "ralha: workspace");
   A.bar = ctx->d_barrier;
   A.err = ctx->d_flag;
+  const size_t smem = 2 * (size_t)n * sizeof(double);
+  A.stage = smem <= RALHA_STAGE_MAX;
+  static bool attr = false;
+  if (A.stage && !attr) {
+    BBT_CUDA(ctx, cudaFuncSetAttribute(ralha_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)RALHA_STAGE_MAX));
+    attr = true;
+  }
+  const size_t dsmem = A.stage ? smem : 0;
   BBT_CUDA(ctx, cudaMemsetAsync(house, 0, (size_t)m * m * sizeof(double), ctx->stream));
   BBT_CUDA(ctx, cudaMemsetAsync(V, 0, (size_t)m * n * sizeof(double), ctx->stream));
   BBT_CUDA(ctx, cudaMemsetAsync(tau, 0, (size_t)m * sizeof(double), ctx->stream));
   BBT_CUDA(ctx, cudaMemsetAsync(ctx->d_barrier, 0, 2 * sizeof(unsigned), ctx->stream));
   BBT_CUDA(ctx, cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), ctx->stream));
   int per_sm = 0;
-  BBT_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ralha_kernel, RT, 0));
+  BBT_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ralha_kernel, RT, dsmem));
   if (per_sm < 1) return fail(ctx, BBT_ERR_CUDA, "ralha: kernel does not fit an SM");
   int grid = (n + CB - 1) / CB;             // at least CB columns per CTA in B1, one CTA per SM
   if (grid > ctx->num_sms * per_sm) grid = ctx->num_sms * per_sm;
@@ -380,7 +409,7 @@ bbt_status ralha(bbt_ctx* ctx, int m, int n, double* W, double* house, double* t
   if (grid < 1) grid = 1;
   void* args[] = {&A};
   ProfScope prof(ctx, BBT_PROF_RALHA, 16.0 * (double)m * m * n / 3.0);
-  BBT_CUDA(ctx, cudaLaunchCooperativeKernel((void*)ralha_kernel, dim3(grid), dim3(RT), args, 0, ctx->stream));
+  BBT_CUDA(ctx, cudaLaunchCooperativeKernel((void*)ralha_kernel, dim3(grid), dim3(RT), args, dsmem, ctx->stream));
   BBT_LAUNCHED(ctx);
   lower_to_upper_kernel<<<1, 1, 0, ctx->stream>>>(m, alpha, beta, cs);
   BBT_LAUNCHED(ctx);

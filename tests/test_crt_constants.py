@@ -99,21 +99,18 @@ def test_epilogue_reduction_of_int32_accumulators(p):
 def test_fused_epilogue_reduction(p):
     """The fused product's epilogue: the accumulator of u8 x u8 products over
     at most 2^15 terms is 0 <= v < 2^31, x = (v >> 16) c16 + (v & 0xFFFF) <
-    2^24, r = x - floor(x ceil(2^32 / p) / 2^32) p = v mod p, and y =
-    (r inv) mod p by the same multiply-high quotient: the residues and the
-    CRT digits of the two-pass path, hence its output bit for bit."""
+    2^24, r = x - floor(x ceil(2^32 / p) / 2^32) p = v mod p: the residue the
+    two-pass path stores, which both paths then multiply by the same G limbs,
+    so their outputs agree bit for bit."""
     c16, magic = 65536 % p, -(-(1 << 32) // p)
     rng = np.random.default_rng(p + 3)
     top = (1 << 15) * 255 * 255
     vals = [0, 1, p - 1, p, (1 << 16) - 1, 1 << 16, top, *[int(v) for v in rng.integers(0, top + 1, 5000)]]
-    for inv in (1, p - 1, (p // 2) | 1):
-        for v in vals:
-            x = (v >> 16) * c16 + (v & 0xFFFF)
-            assert x < (1 << 24)
-            r = x - ((x * magic) >> 32) * p
-            assert r == v % p
-            t = r * inv
-            assert t - ((t * magic) >> 32) * p == (v * inv) % p
+    for v in vals:
+        x = (v >> 16) * c16 + (v & 0xFFFF)
+        assert x < (1 << 24)
+        r = x - ((x * magic) >> 32) * p
+        assert r == v % p
 
 
 @pytest.mark.parametrize("bits_a,bits_b,K,expect", [(53, 53, 500_000, 16), (50, 50, 500_000, 15),
@@ -126,9 +123,26 @@ def test_modulus_count_covers_the_product(bits_a, bits_b, K, expect):
     assert 4 * (1 << (bits_a - 2)) * (1 << (bits_b - 2)) * K <= M
 
 
+def glimbs(p, inv):
+    """crt.cu's glimb_c: G = inv floor(2^128 / p) + floor(inv (2^128 mod p) / p)
+    as four 32-bit limbs, least significant first."""
+    F = (1 << 128) // p
+    G = inv * F + (inv * ((1 << 128) % p)) // p
+    return [(G >> (32 * l)) & 0xFFFFFFFF for l in range(4)]
+
+
+def test_g_limbs_are_the_scaled_crt_digit():
+    for n in (15, 16, 19, 24):
+        M = math.prod(MOD[:n])
+        for p in MOD[:n]:
+            inv = pow((M // p) % p, -1, p)
+            G = sum(v << (32 * l) for l, v in enumerate(glimbs(p, inv)))
+            assert G == ((inv << 128) // p)
+
+
 def reconstruct(T, n, limbs):
-    """crt.cu's reconstruction: y_q = (T mod p_q) ((M / p_q)^-1 mod p_q) mod
-    p_q and the fraction S = sum_q y_q floor(2^128 / p_q) mod 2^128 (its low 32
+    """crt.cu's reconstruction: r_q = T mod p_q and the fraction S = sum_q r_q
+    G_q mod 2^128, G_q = floor(2^128 ((M / p_q)^-1 mod p_q) / p_q) (its low 32
     bits dropped when limbs = 3), read as a signed 128-bit number: S M / 2^128
     is T up to the floors' errors."""
     ps = MOD[:n]
@@ -136,11 +150,10 @@ def reconstruct(T, n, limbs):
     S = 0
     for p in ps:
         inv = pow((M // p) % p, -1, p)
-        y = ((T % p) * inv) % p
-        F = ((1 << 128) - 1) // p + (1 if ((1 << 128) - 1) % p == p - 1 else 0)
+        G = sum(v << (32 * l) for l, v in enumerate(glimbs(p, inv)))
         if limbs == 3:
-            F = (F >> 32) << 32
-        S += y * F
+            G = (G >> 32) << 32
+        S += (T % p) * G
     S %= 1 << 128
     if S >= 1 << 127:
         S -= 1 << 128
@@ -159,8 +172,8 @@ def test_fixed_point_reconstruction(n, limbs):
     bits = 128 if limbs == 4 else 96
     for T in Ts:
         S, _ = reconstruct(T, n, limbs)
-        # every term y_q F_q is short of y_q 2^128 / p_q by less than y_q < 256
-        # units of 2^(128 - bits): |S M - T 2^128| < n 256 M 2^(128 - bits)
+        # every term r_q G_q is short of r_q inv_q 2^128 / p_q by less than
+        # r_q < 256 units of 2^(128 - bits): |S M - T 2^128| < n 256 M 2^(128 - bits)
         assert abs(S * M - T * (1 << 128)) < n * 256 * M * (1 << (128 - bits)), T
     # relative to the largest |T| the kernels allow (M / 4): below 2^-100 with
     # 128-bit fractions, 2^-70 with 96-bit ones
