@@ -427,13 +427,11 @@ __global__ void apply_signs_kernel(int m, const double* __restrict__ d, double* 
 // flag, reported by check_tc_flags, and every CTA leaves.
 
 // Right-looking blocked Cholesky G = R^T R (upper, 32 x 32 tiles), in place.
-// Per block row k: (1) every CTA that needs it factors the diagonal tile in
-// one warp (lane c holds column c in registers; step j broadcasts row j by
-// warp shuffles; the steps are unrolled at compile time so the column stays
-// in registers), keeps R_kk and the reciprocals of its diagonal in shared
+// Per block row k: (1) every CTA that needs it factors the diagonal tile
+// (chol_tile_cta), keeps R_kk and the reciprocals of its diagonal in shared
 // memory, and solves its tile of the row panel, R_kj = R_kk^-T G_kj: the
 // tile is staged through shared memory with coalesced loads, lane c
-// forward-substitutes column c in registers; (2) the trailing tiles
+// substitutes column c in registers (trsm_col_warp); (2) the trailing tiles
 // G_ij -= R_ki^T R_kj, i <= j: four tiles per CTA at a time, one per pair of
 // warps, every load of the round (both panel tiles and the tile updated)
 // issued before any arithmetic.  Only the upper triangle of G is read; the
@@ -452,56 +450,56 @@ struct PotrfArgs {
   int* err;        // barrier timeout
 };
 
-template <int J>
-__device__ __forceinline__ void chol_steps(double (&x)[32], int lane, int kb, int* flag) {
-  if constexpr (J < 32) {
-    if (J < kb) {
-      double d = __shfl_sync(0xffffffffu, x[J], J);
-      if (!(d > 0.0) || !isfinite(d)) {
-        if (lane == 0) atomicExch(flag, 1);
-        d = 1.0;
-      }
-      const double r = sqrt(d);
-      const double xj = x[J] / r;   // R(J, lane)
-      x[J] = lane == J ? r : (lane > J ? xj : x[J]);
-#pragma unroll
-      for (int i = J + 1; i < 32; ++i) {
-        const double rji = __shfl_sync(0xffffffffu, x[J], i);   // R(J, i) from lane i
-        const double u = fma(-rji, x[J], x[i]);
-        x[i] = lane >= i ? u : x[i];
-      }
+// D (upper kb x kb in a padded shared tile, zero elsewhere) <- its Cholesky
+// factor, by the whole CTA; rinv[j] = 1 / R(j, j).  Step j: every thread
+// forms R(j, j) and its reciprocal from D(j, j) (final since the previous
+// step's update), the first warp scales row j, and after a CTA barrier
+// thread j stores R(j, j) while every thread updates its share of the
+// trailing triangle (a second barrier).  The
+// loop stays rolled: the code is small enough to stay in the instruction
+// cache between the kernel's phases, which a fully unrolled register
+// version did not.
+__device__ __forceinline__ void chol_tile_cta(double* D, double* rinv, int kb, int* flag) {
+  const int tid = threadIdx.x;
+  for (int j = 0; j < kb; ++j) {
+    double d = D[j * TSTR + j];
+    if (!(d > 0.0) || !isfinite(d)) {
+      if (tid == 0) atomicExch(flag, 1);
+      d = 1.0;
     }
-    chol_steps<J + 1>(x, lane, kb, flag);
+    const double r = sqrt(d);
+    const double ri = 1.0 / r;
+    if (tid < 32 && tid > j && tid < kb) D[j * TSTR + tid] *= ri;
+    __syncthreads();   // every thread has read D(j, j); row j is scaled
+    if (tid == j) {    // R(j, j): not read again in this step or later ones
+      D[j * TSTR + j] = r;
+      rinv[j] = ri;
+    }
+    for (int e = tid; e < 1024; e += CT) {
+      const int a = e >> 5, b = e & 31;
+      if (a > j && a <= b && b < kb) D[a * TSTR + b] = fma(-D[j * TSTR + a], D[j * TSTR + b], D[a * TSTR + b]);
+    }
+    __syncthreads();
   }
 }
 
-// D (upper kb x kb, zero elsewhere) <- its Cholesky factor; rinv[i] = 1 / R(i, i).
-__device__ __forceinline__ void chol_tile_warp(double* D, double* rinv, int kb, int lane, int* flag) {
+// Column lane of the shared tile T <- R_kk^-T column lane, right-looking with
+// the column in registers: step i finishes x_i = x_i / R(i, i) and removes it
+// from the rows below.  The array is shifted down one place per step so its
+// indices stay compile-time constants in a rolled loop (row i is always x[0]).
+__device__ __forceinline__ void trsm_col_warp(double* T, const double* D, const double* rinv, int kb, int lane) {
   double x[32];
 #pragma unroll
-  for (int i = 0; i < 32; ++i) x[i] = D[i * TSTR + lane];   // column lane (rows past kb: zero)
-  chol_steps<0>(x, lane, kb, flag);
-  __syncwarp();
+  for (int i = 0; i < 32; ++i) x[i] = T[i * TSTR + lane];
+  for (int i = 0; i < kb; ++i) {
+    const double xi = x[0] * rinv[i];
+    T[i * TSTR + lane] = xi;
 #pragma unroll
-  for (int i = 0; i < 32; ++i) D[i * TSTR + lane] = (i <= lane && lane < kb) ? x[i] : 0.0;
-  __syncwarp();
-  if (lane < kb) rinv[lane] = 1.0 / D[lane * TSTR + lane];
-}
-
-// Column c of T (in shared memory) <- R_kk^-T column c: x_i = (t_i - sum_{s<i} R(s, i) x_s) / R(i, i).
-template <int I>
-__device__ __forceinline__ void trsm_steps(double (&x)[32], const double* D, const double* rinv, int kb) {
-  if constexpr (I < 32) {
-    if (I < kb) {
-      double s0 = x[I], s1 = 0.0;
-#pragma unroll
-      for (int t = 0; t < I; t += 2) {
-        s0 = fma(-D[t * TSTR + I], x[t], s0);
-        if (t + 1 < I) s1 = fma(-D[(t + 1) * TSTR + I], x[t + 1], s1);
-      }
-      x[I] = (s0 + s1) * rinv[I];
+    for (int u = 1; u < 32; ++u) {
+      const double rt = D[i * TSTR + min(i + u, 31)];   // R(i, i + u), clamped inside the tile
+      x[u - 1] = (i + u < kb) ? fma(-rt, xi, x[u]) : x[u];
     }
-    trsm_steps<I + 1>(x, D, rinv, kb);
+    x[31] = 0.0;
   }
 }
 
@@ -528,22 +526,14 @@ __global__ void __launch_bounds__(CT, 1) potrf_coop_kernel(PotrfArgs P) {
         T[i * TSTR + c] = (i < kb && c < jb) ? P.G[(r0 + i) + (long)(c0 + c) * ld] : 0.0;
       }
       __syncthreads();
-      if (w == 0) chol_tile_warp(D, rinv, kb, lane, P.flag);
-      __syncthreads();
+      chol_tile_cta(D, rinv, kb, P.flag);
       if (blockIdx.x == 0)
         for (int f = tid; f < 1024; f += CT) {
           const int i = f & 31, j = f >> 5;
           if (i < kb && j < kb && i <= j) P.G[(r0 + i) + (long)(r0 + j) * ld] = D[i * TSTR + j];
         }
       if (jb > 0) {
-        if (w == 0) {
-          double x[32];
-#pragma unroll
-          for (int i = 0; i < 32; ++i) x[i] = T[i * TSTR + lane];
-          trsm_steps<0>(x, D, rinv, kb);
-#pragma unroll
-          for (int i = 0; i < 32; ++i) T[i * TSTR + lane] = x[i];
-        }
+        if (w == 0) trsm_col_warp(T, D, rinv, kb, lane);
         __syncthreads();
         for (int f = tid; f < 1024; f += CT) {
           const int i = f & 31, c = f >> 5;
@@ -633,8 +623,11 @@ struct LuArgs {
 };
 
 // The sign-recovery elimination (lu_sign_leaf_reg) on the 16-column panel at
-// p0, rows p0.. in registers, one row per thread.
-__device__ void lu_panel(const LuArgs& P, int p0, double* rowj, double* sf) {
+// p0, rows p0.. in registers, one row per thread.  The pivot row and its
+// multiplier scale go through two shared buffers used alternately, so each
+// column needs one CTA barrier: the row written at step j + 1 goes to the
+// buffer read at step j - 1, which every thread left before step j's barrier.
+__device__ void lu_panel(const LuArgs& P, int p0, double (*rowj)[LB], double* sf) {
   const int pb = min(LB, P.cols - p0);
   const int i = p0 + threadIdx.x;
   const bool live = i < P.rows;
@@ -644,22 +637,22 @@ __device__ void lu_panel(const LuArgs& P, int p0, double* rowj, double* sf) {
 #pragma unroll
   for (int j = 0; j < LB; ++j) {
     if (j < pb) {
+      const int b = j & 1;
       if ((int)threadIdx.x == j) {
 #pragma unroll
-        for (int c = 0; c < LB; ++c) rowj[c] = x[c];
+        for (int c = 0; c < LB; ++c) rowj[b][c] = x[c];
         const double cj = x[j];
         const double dj = cj < 0.0 ? 1.0 : -1.0;
         P.d[p0 + j] = dj;
-        *sf = -dj / (1.0 + fabs(cj));
+        sf[b] = -dj / (1.0 + fabs(cj));
       }
       __syncthreads();
       if ((int)threadIdx.x > j && live) {
-        const double l = *sf * x[j];
+        const double l = sf[b] * x[j];
         x[j] = l;
 #pragma unroll
-        for (int c = j + 1; c < LB; ++c) x[c] -= l * rowj[c];
+        for (int c = j + 1; c < LB; ++c) x[c] -= l * rowj[b][c];
       }
-      __syncthreads();
     }
   }
   if (live)
@@ -674,12 +667,12 @@ __device__ void lu_panel(const LuArgs& P, int p0, double* rowj, double* sf) {
 // owns the chunk of the next panel and factors it right after updating it,
 // so one grid barrier per panel suffices.
 __global__ void __launch_bounds__(LT, 1) lu_sign_coop_kernel(LuArgs P) {
-  __shared__ double rowj[LB];
-  __shared__ double sf;
+  __shared__ double rowj[2][LB];
+  __shared__ double sf[2];
   __shared__ double L11[LB][LB + 1];
   __shared__ double U[LB][LB + 1];
   const int np = (P.cols + LB - 1) / LB;
-  if (blockIdx.x == 0) lu_panel(P, 0, rowj, &sf);
+  if (blockIdx.x == 0) lu_panel(P, 0, rowj, sf);
   if (!grid_sync(P.bar, P.err)) return;
   for (int k = 0; k < np; ++k) {
     const int p0 = k * LB, pb = min(LB, P.cols - p0);
@@ -731,7 +724,7 @@ __global__ void __launch_bounds__(LT, 1) lu_sign_coop_kernel(LuArgs P) {
       }
       __syncthreads();
     }
-    if (blockIdx.x == 0 && k + 1 < np) lu_panel(P, p0 + LB, rowj, &sf);   // CTA 0 updated that chunk (q = 0)
+    if (blockIdx.x == 0 && k + 1 < np) lu_panel(P, p0 + LB, rowj, sf);   // CTA 0 updated that chunk (q = 0)
     if (!grid_sync(P.bar, P.err)) return;
   }
 }

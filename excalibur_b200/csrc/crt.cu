@@ -105,7 +105,6 @@ struct ModK {   // reconstruction from the residues of an NM-modulus set
   static constexpr int p = MODULI[Q];
   static constexpr uint32_t magic32 = (uint32_t)((((uint64_t)1 << 32) + p - 1) / p);
   static constexpr uint32_t inv = (uint32_t)crt_inv_c(Q, NM);
-  static constexpr uint32_t F0 = flimb_c(p, 0), F1 = flimb_c(p, 1), F2 = flimb_c(p, 2), F3 = flimb_c(p, 3);
   // r G / 2^128 = r inv / p (mod 1) up to r units of 2^-128: the CRT digit's
   // fraction straight from the residue r, with no reduction of r inv mod p
   static constexpr uint32_t G0 = glimb_c(p, (int)inv, 0), G1 = glimb_c(p, (int)inv, 1),
@@ -356,7 +355,6 @@ struct CrtArgs {
   int upper;      // 1: skip tiles strictly below the diagonal
   int p[MAXMOD], c16[MAXMOD];
   uint32_t magic[MAXMOD];   // ceil(2^32 / p): exact quotients below 2^24
-  int off[MAXMOD];          // 2^31 mod p
   int* err;
 };
 
@@ -456,7 +454,10 @@ crt_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUte
     }
   } else {
     // ---- epilogue: TMEM lanes 32 (warp % 4).., columns EPI_COLS (warp / 4).. of the
-    //      accumulator; T mod p as a byte per element, i (the TMEM lane) contiguous in memory
+    //      accumulator; T mod p as a byte per element, i (the TMEM lane) contiguous in memory.
+    //      The accumulator sums at most 2^15 products of bytes, so 0 <= v < 2^31:
+    //      (v >> 16) c16 + (v & 0xFFFF) < 2^24 is congruent to it and its
+    //      multiply-high quotient by p is exact
     const int q4 = warp & 3, ch = warp >> 2;
     const int i = m0 + q4 * 32 + lane;
     const bool row_ok = i < P.M;
@@ -465,25 +466,20 @@ crt_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUte
       const int buf = q & 1, use = q >> 1;
       if (!mbar_wait(accf0 + 8 * buf, (uint32_t)use & 1u)) { ok = false; break; }
       tc_fence_after();
-      const int p = P.p[q], c16 = P.c16[q];
-      const uint32_t magic = P.magic[q], off = (uint32_t)P.off[q];
+      const uint32_t p = (uint32_t)P.p[q], c16 = (uint32_t)P.c16[q], magic = P.magic[q];
       uint8_t* o = P.out + ((size_t)blockIdx.z * P.n + q) * (size_t)P.N * P.Mp + i;
 #pragma unroll 1
       for (int c = 0; c < EPI_COLS / 16; ++c) {
         uint32_t v[16];
         tmem_ld16(tmem + ((uint32_t)(q4 * 32) << 16) + (uint32_t)(buf * TN + ch * EPI_COLS + c * 16), v);
         const int j0 = n0 + ch * EPI_COLS + c * 16;
+        const int jn = row_ok ? min(16, P.N - j0) : 0;   // columns of this chunk to store
         uint8_t* oc = o + (size_t)j0 * P.Mp;
 #pragma unroll
         for (int e = 0; e < 16; ++e) {
-          // a = (h - 2^15) 2^16 + lo with 0 <= h, lo < 2^16: h c16 + lo (< 2^24) is
-          // congruent to a + 2^31 mod p, reduced exactly by the multiply-high
-          // quotient; off = 2^31 mod p is taken back out
-          const uint32_t a = v[e] ^ 0x80000000u;
-          const uint32_t x = (a >> 16) * (uint32_t)c16 + (a & 0xFFFFu);
-          int r = (int)(x - __umulhi(x, magic) * (uint32_t)p) - (int)off;
-          if (r < 0) r += p;
-          if (row_ok && j0 + e < P.N) oc[(size_t)e * P.Mp] = (uint8_t)r;
+          const uint32_t x = (v[e] >> 16) * c16 + (v[e] & 0xFFFFu);
+          const uint32_t r = x - __umulhi(x, magic) * p;
+          if (e < jn) oc[(size_t)e * P.Mp] = (uint8_t)r;
         }
       }
       tc_fence_before();
@@ -679,6 +675,165 @@ combine_dd_kernel(CombArgs A, const double* __restrict__ sa, const double* __res
       Ch[(i + e) + (long)j * ldc] = s * sc;
       Cl[(i + e) + (long)j * ldc] = t * sc;
     }
+  }
+}
+
+// ---- products with a short K and an MN-major A: A kept in shared memory ----
+// The products with Q (C = X_int^T Z2, K = m <= 1024) read B (Z2's residues,
+// N x K per modulus, L2-resident) for every 128-row block of A.  Here one CTA
+// owns a 128-row block and every 256-column tile of it: per modulus, A's K
+// blocks (up to 8 x 16 KB) are loaded once into resident slots and each column
+// tile streams only its B blocks through a 3-stage ring, so the operand
+// traffic from L2 per tile falls from A + B to A / tiles + B (a quarter less at
+// N = 1000: the products are bound by that traffic).  A slot is refilled with
+// the next modulus as soon as the last tile's MMAs on it have completed
+// (tcgen05.commit on the slot's barrier), so the ring keeps running across
+// moduli.  The epilogue and the residue layout are crt_kernel's.
+constexpr int AR_SLOTS = 8;     // resident K blocks of A: K <= 1024
+constexpr int AR_BSTAGES = 3;
+constexpr int AR_SMEM = AR_SLOTS * A_TILE + AR_BSTAGES * B_TILE + 1024 + 256;
+
+__global__ void __launch_bounds__(THREADS, 1)
+crt_apply_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, CrtArgs P) {
+  const int m0 = blockIdx.x * TM;
+  const int nt = (P.N + TN - 1) / TN, nk = P.kblocks;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint8_t* aslots = smem;
+  uint8_t* bring = smem + AR_SLOTS * A_TILE;
+  uint64_t* bars = (uint64_t*)(bring + AR_BSTAGES * B_TILE);
+  // [0, 8) A full, [8, 16) A empty, [16, 19) B full, [19, 22) B empty, [22, 24) acc full, [24, 26) acc empty
+  uint32_t* tmem_slot = (uint32_t*)(bars + 26);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t afull0 = smem_u32(bars), aempty0 = smem_u32(bars + 8);
+  const uint32_t bfull0 = smem_u32(bars + 16), bempty0 = smem_u32(bars + 19);
+  const uint32_t accf0 = smem_u32(bars + 22), acce0 = smem_u32(bars + 24);
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < AR_SLOTS; ++k) {
+      mbar_init(afull0 + 8 * k, 1);
+      mbar_init(aempty0 + 8 * k, 1);
+    }
+    for (int s = 0; s < AR_BSTAGES; ++s) {
+      mbar_init(bfull0 + 8 * s, 1);
+      mbar_init(bempty0 + 8 * s, 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(accf0 + 8 * b, 1);
+      mbar_init(acce0 + 8 * b, EPI_WARPS);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == EPI_WARPS) {
+    if (lane == 0) {   // ---- TMA producer
+      bool ok = true;
+      int it = 0;      // B ring position
+      for (int q = 0; q < P.n && ok; ++q)
+        for (int t = 0; t < nt && ok; ++t)
+          for (int kb = 0; kb < nk; ++kb) {
+            const int kx = kb * TK;
+            if (t == 0) {   // A's block kb of modulus q, once its slot is free
+              const uint32_t fa = afull0 + 8 * kb;
+              if (q > 0 && !mbar_wait(aempty0 + 8 * kb, (uint32_t)(q - 1) & 1u)) { ok = false; break; }
+              mbar_expect_tx(fa, (uint32_t)A_TILE);
+              tma_load_3d(smem_u32(aslots + (size_t)kb * A_TILE), &tmA, fa, m0, kx, q);
+            }
+            const int s = it % AR_BSTAGES;
+            const uint32_t fb = bfull0 + 8 * s;
+            if (!mbar_wait(bempty0 + 8 * s, ((uint32_t)(it / AR_BSTAGES) & 1u) ^ 1u)) { ok = false; break; }
+            mbar_expect_tx(fb, (uint32_t)B_TILE);
+            tma_load_3d(smem_u32(bring + (size_t)s * B_TILE), &tmB, fb, kx, t * TN, q);
+            ++it;
+          }
+      if (!ok) atomicExch(P.err, 1);
+      // copies still in flight land before the CTA leaves (all consumed on success)
+      for (int k = max(0, it - AR_BSTAGES); k < it; ++k)
+        if (!mbar_wait(bfull0 + 8 * (k % AR_BSTAGES), (uint32_t)(k / AR_BSTAGES) & 1u)) atomicExch(P.err, 4);
+      if (it > 0) {
+        const int qlast = (it - 1) / (nt * nk);   // the last modulus whose A blocks were issued
+        for (int kb = 0; kb < nk; ++kb)
+          if (!mbar_wait(afull0 + 8 * kb, (uint32_t)qlast & 1u)) atomicExch(P.err, 4);
+      }
+    }
+  } else if (warp == EPI_WARPS + 1) {
+    if (lane == 0) {   // ---- MMA issuer: A MN-major (bit 15), u8 x u8 -> int32
+      const uint32_t idesc = (2u << 4) | (1u << 15) | ((uint32_t)(TN >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
+      bool ok = true;
+      int it = 0, tile = 0;
+      for (int q = 0; q < P.n && ok; ++q)
+        for (int t = 0; t < nt && ok; ++t, ++tile) {
+          const int buf = tile & 1, use = tile >> 1;
+          if (use > 0 && !mbar_wait(acce0 + 8 * buf, (uint32_t)(use - 1) & 1u)) { ok = false; break; }
+          tc_fence_after();
+          const uint32_t d = tmem + (uint32_t)(buf * TN);
+          for (int kb = 0; kb < nk; ++kb) {
+            if (t == 0 && !mbar_wait(afull0 + 8 * kb, (uint32_t)q & 1u)) { ok = false; break; }
+            const int s = it % AR_BSTAGES;
+            if (!mbar_wait(bfull0 + 8 * s, (uint32_t)(it / AR_BSTAGES) & 1u)) { ok = false; break; }
+            tc_fence_after();
+            const uint64_t ad = sw128_desc(smem_u32(aslots + (size_t)kb * A_TILE));
+            const uint64_t bd = sw128_desc(smem_u32(bring + (size_t)s * B_TILE));
+#pragma unroll
+            for (int kk = 0; kk < TK / 32; ++kk)
+              mma_i8(d, ad + 256 * kk, bd + 2 * kk, idesc, (kb != 0 || kk != 0) ? 1u : 0u);
+            mma_commit(bempty0 + 8 * s);
+            if (t == nt - 1) mma_commit(aempty0 + 8 * kb);   // slot kb free once these MMAs complete
+            ++it;
+          }
+          mma_commit(accf0 + 8 * buf);
+        }
+      if (!ok) atomicExch(P.err, 2);
+    }
+  } else {
+    // ---- epilogue: as crt_kernel's, tile after tile
+    const int q4 = warp & 3, ch = warp >> 2;
+    const int i = m0 + q4 * 32 + lane;
+    const bool row_ok = i < P.M;
+    bool ok = true;
+    int tile = 0;
+    for (int q = 0; q < P.n && ok; ++q) {
+      const uint32_t p = (uint32_t)P.p[q], c16 = (uint32_t)P.c16[q], magic = P.magic[q];
+      uint8_t* o = P.out + (size_t)q * (size_t)P.N * P.Mp + i;
+      for (int t = 0; t < nt; ++t, ++tile) {
+        const int buf = tile & 1, use = tile >> 1;
+        if (!mbar_wait(accf0 + 8 * buf, (uint32_t)use & 1u)) { ok = false; break; }
+        tc_fence_after();
+#pragma unroll 1
+        for (int c = 0; c < EPI_COLS / 16; ++c) {
+          uint32_t v[16];
+          tmem_ld16(tmem + ((uint32_t)(q4 * 32) << 16) + (uint32_t)(buf * TN + ch * EPI_COLS + c * 16), v);
+          const int j0 = t * TN + ch * EPI_COLS + c * 16;
+          const int jn = row_ok ? min(16, P.N - j0) : 0;
+          uint8_t* oc = o + (size_t)j0 * P.Mp;
+#pragma unroll
+          for (int e = 0; e < 16; ++e) {
+            const uint32_t x = (v[e] >> 16) * c16 + (v[e] & 0xFFFFu);
+            const uint32_t r = x - __umulhi(x, magic) * p;
+            if (e < jn) oc[(size_t)e * P.Mp] = (uint8_t)r;
+          }
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(acce0 + 8 * buf);
+      }
+    }
+    if (!ok && lane == 0) atomicExch(P.err, 3);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
   }
 }
 
@@ -1133,11 +1288,18 @@ bbt_status crt_launch(bbt_ctx* ctx, int M, int N, long K, int n, const int8_t* R
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
       return fail(ctx, BBT_ERR_CUDA, "crt: tensor map of B");
   }
-  static bool attr[2] = {false, false};
-  if (!attr[amn]) {
-    BBT_CUDA(ctx, cudaFuncSetAttribute(amn ? crt_kernel<true> : crt_kernel<false>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
-    attr[amn] = true;
+  // A kept in shared memory (crt_apply_kernel): MN-major A, one K-split of at
+  // most AR_SLOTS blocks, and enough 128-row blocks to occupy every SM
+  const bool resident = amn && pl.splits == 1 && pl.kblocks <= AR_SLOTS && (long)gy >= (long)ctx->num_sms;
+  static bool attr[3] = {false, false, false};
+  const int kind = resident ? 2 : (amn ? 1 : 0);
+  if (!attr[kind]) {
+    if (kind == 2)
+      BBT_CUDA(ctx, cudaFuncSetAttribute(crt_apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, AR_SMEM));
+    else
+      BBT_CUDA(ctx, cudaFuncSetAttribute(kind == 1 ? crt_kernel<true> : crt_kernel<false>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+    attr[kind] = true;
   }
   const Mods md = make_mods(n);
   CrtArgs a;
@@ -1153,12 +1315,13 @@ bbt_status crt_launch(bbt_ctx* ctx, int M, int N, long K, int n, const int8_t* R
     a.p[q] = md.p[q];
     a.c16[q] = md.c16[q];
     a.magic[q] = (uint32_t)((((uint64_t)1 << 32) + md.p[q] - 1) / md.p[q]);
-    a.off[q] = (int)(((uint64_t)1 << 31) % (uint64_t)md.p[q]);
   }
   a.err = ctx->d_flag + FLAG_SKETCH;
   ProfScope prof(ctx, BBT_PROF_CRT, (upper ? 1.0 : 2.0) * n * (double)M * N * K);   // int8 operations
   const dim3 grid((N + TN - 1) / TN, gy, pl.splits);
-  if (amn)
+  if (kind == 2)
+    crt_apply_kernel<<<dim3(gy), THREADS, AR_SMEM, ctx->stream>>>(ta, tb, a);
+  else if (kind == 1)
     crt_kernel<true><<<grid, THREADS, SMEM_BYTES, ctx->stream>>>(ta, tb, a);
   else
     crt_kernel<false><<<grid, THREADS, SMEM_BYTES, ctx->stream>>>(ta, tb, a);

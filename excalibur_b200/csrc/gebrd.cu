@@ -158,14 +158,25 @@ __global__ void __launch_bounds__(GT) labrd_kernel(PanelArgs P) {
         const int re = min(M, (rc + 1) * P.r1);
         double s = 0.0, s1 = 0.0;
         int r = max(j + 1, rc * P.r1) + lane;
-        for (; r + 7 * 32 < re; r += 8 * 32) {   // eight loads in flight per lane
+        if (r + 7 * 32 < re) {   // batches of eight loads per lane, the next batch issued first
           double a[8], v[8];
 #pragma unroll
           for (int u = 0; u < 8; ++u) { a[u] = col[r + u * 32]; v[u] = cj[r + u * 32]; }
+          for (; r + 7 * 32 < re; r += 8 * 32) {
+            const bool more = r + 8 * 32 + 7 * 32 < re;
+            double a2[8], v2[8];
 #pragma unroll
-          for (int u = 0; u < 8; u += 2) {
-            s += a[u] * v[u];
-            s1 += a[u + 1] * v[u + 1];
+            for (int u = 0; u < 8; ++u) {
+              a2[u] = more ? col[r + 256 + u * 32] : 0.0;
+              v2[u] = more ? cj[r + 256 + u * 32] : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < 8; u += 2) {
+              s += a[u] * v[u];
+              s1 += a[u + 1] * v[u + 1];
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u) { a[u] = a2[u]; v[u] = v2[u]; }
           }
         }
         for (; r < re; r += 32) s += col[r] * cj[r];
@@ -234,17 +245,25 @@ __global__ void __launch_bounds__(GT) labrd_kernel(PanelArgs P) {
         double s = 0.0, s1 = 0.0;
         if (r < M) {
           int c = ca;
-          for (; c + 7 < cb; c += 8) {
-            double a[8], u[8];
+          if (c + 7 < cb) {   // batches of eight columns, the next batch's loads issued first
+            double a[8];
 #pragma unroll
-            for (int q = 0; q < 8; ++q) {
-              a[q] = A[r + (c + q) * ld];
-              u[q] = (c + q == j + 1) ? 1.0 : P.rowb[c + q] * sp;
-            }
+            for (int q = 0; q < 8; ++q) a[q] = A[r + (c + q) * ld];
+            for (; c + 7 < cb; c += 8) {
+              const bool more = c + 15 < cb;
+              double a2[8];
 #pragma unroll
-            for (int q = 0; q < 8; q += 2) {
-              s += a[q] * u[q];
-              s1 += a[q + 1] * u[q + 1];
+              for (int q = 0; q < 8; ++q) a2[q] = more ? A[r + (c + 8 + q) * ld] : 0.0;
+              double u[8];
+#pragma unroll
+              for (int q = 0; q < 8; ++q) u[q] = (c + q == j + 1) ? 1.0 : P.rowb[c + q] * sp;
+#pragma unroll
+              for (int q = 0; q < 8; q += 2) {
+                s += a[q] * u[q];
+                s1 += a[q + 1] * u[q + 1];
+              }
+#pragma unroll
+              for (int q = 0; q < 8; ++q) a[q] = a2[q];
             }
           }
           for (; c < cb; ++c) s += A[r + c * ld] * ((c == j + 1) ? 1.0 : P.rowb[c] * sp);

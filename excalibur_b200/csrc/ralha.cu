@@ -22,7 +22,7 @@
 //   B2 (row-partitioned, one warp per row): W[r] += (-tau vt) h_r for
 //      r > i, and, in the same pass, the next step's Gram row
 //      g'[r] = W[r] . W[i+1].
-// The passes over W keep sixteen loads in flight per thread; B2 reads the two
+// The passes over W keep eight loads in flight per thread; B2 reads the two
 // vectors every row needs (-tau vt and the updated row i+1) from shared
 // memory, staged once per CTA and step.
 //
@@ -41,7 +41,7 @@ namespace {
 constexpr int RT = 256;                 // threads per CTA
 constexpr int RW = RT / 32;             // warps per CTA
 constexpr int CB = 8;                   // columns per pass of B1
-constexpr int RB = 16;                  // loads in flight per thread in the passes over W
+constexpr int RB = 8;                   // loads in flight per thread in the passes over W
 constexpr size_t RALHA_STAGE_MAX = 200 * 1024;   // shared bytes for the staged vectors (n <= 12800)
 
 struct RalhaArgs {
@@ -205,13 +205,12 @@ __global__ void __launch_bounds__(RT, 1) ralha_kernel(RalhaArgs A) {
             s = wc[0];   // h_0 = 1
             t += PH;
           }
-          for (; t < len; t += RB * PH) {   // RB rows' loads in flight, the last batch masked
+          for (; t + (RB - 1) * PH < len; t += RB * PH) {   // RB rows' loads in flight
             double w[RB], hh[RB];
 #pragma unroll
             for (int e = 0; e < RB; ++e) {
-              const bool in = t + e * PH < len;
-              w[e] = in ? wc[(long)(t + e * PH) * n] : 0.0;
-              hh[e] = in ? g[t + e * PH] : 0.0;
+              w[e] = wc[(long)(t + e * PH) * n];
+              hh[e] = g[t + e * PH];
             }
 #pragma unroll
             for (int e = 0; e < RB; e += 2) {
@@ -219,6 +218,7 @@ __global__ void __launch_bounds__(RT, 1) ralha_kernel(RalhaArgs A) {
               s1 += (hh[e + 1] * scl) * w[e + 1];
             }
           }
+          for (; t < len; t += PH) s += (g[t] * scl) * wc[(long)t * n];
           s += s1;
         }
         red[tid / CB][tid % CB] = s;
@@ -286,7 +286,21 @@ __global__ void __launch_bounds__(RT, 1) ralha_kernel(RalhaArgs A) {
         double* row = A.W + (long)r * n;
         double s = 0.0, s1 = 0.0;
         // batches of RB segments: all loads of a batch issued before its stores
-        for (int c = lane; c < n; c += RB * 32) {
+        int c = lane;
+        for (; c + (RB - 1) * 32 < n; c += RB * 32) {
+          double w[RB];
+#pragma unroll
+          for (int e = 0; e < RB; ++e) w[e] = row[c + 32 * e];
+#pragma unroll
+          for (int e = 0; e < RB; ++e) {
+            w[e] = fma(tv[c + 32 * e], h, w[e]);
+            if (e & 1) s1 = fma(w[e], nw_[c + 32 * e], s1);
+            else s = fma(w[e], nw_[c + 32 * e], s);
+          }
+#pragma unroll
+          for (int e = 0; e < RB; ++e) row[c + 32 * e] = w[e];
+        }
+        {
           double w[RB];
 #pragma unroll
           for (int e = 0; e < RB; ++e) w[e] = (c + 32 * e < n) ? row[c + 32 * e] : 0.0;
@@ -294,12 +308,9 @@ __global__ void __launch_bounds__(RT, 1) ralha_kernel(RalhaArgs A) {
           for (int e = 0; e < RB; ++e)
             if (c + 32 * e < n) {
               w[e] = fma(tv[c + 32 * e], h, w[e]);
-              if (e & 1) s1 = fma(w[e], nw_[c + 32 * e], s1);
-              else s = fma(w[e], nw_[c + 32 * e], s);
+              s = fma(w[e], nw_[c + 32 * e], s);
+              row[c + 32 * e] = w[e];
             }
-#pragma unroll
-          for (int e = 0; e < RB; ++e)
-            if (c + 32 * e < n) row[c + 32 * e] = w[e];
         }
         s = warp_sum(s + s1);
         // g for step i+1 has entries for rows >= i+2

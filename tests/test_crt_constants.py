@@ -80,18 +80,18 @@ def test_residues_from_pieces_stay_in_range(p):
 
 @pytest.mark.parametrize("p", MOD)
 def test_epilogue_reduction_of_int32_accumulators(p):
-    """The GEMM epilogue's a = v xor 2^31, x = (a >> 16) c16 + (a & 0xFFFF)
-    (< 2^24), r = x mod p - (2^31 mod p), r += p if negative: r = v mod p."""
-    c16, off, magic = 65536 % p, (1 << 31) % p, -(-(1 << 32) // p)
+    """The GEMM epilogue: an accumulator of at most 2^15 products of bytes in
+    [0, 256) is 0 <= v < 2^31; x = (v >> 16) c16 + (v & 0xFFFF) < 2^24 and
+    r = x - floor(x ceil(2^32 / p) / 2^32) p = v mod p."""
+    c16, magic = 65536 % p, -(-(1 << 32) // p)
+    top = (1 << 15) * 255 * 255
+    assert top < (1 << 31)
     rng = np.random.default_rng(p + 2)
-    vals = [-(1 << 31), (1 << 31) - 1, 0, -1, 1, *[int(v) for v in rng.integers(-(1 << 31), 1 << 31, 5000)]]
+    vals = [0, 1, p - 1, p, (1 << 16) - 1, 1 << 16, top, *[int(v) for v in rng.integers(0, top + 1, 5000)]]
     for v in vals:
-        a = (v & 0xFFFFFFFF) ^ 0x80000000
-        x = (a >> 16) * c16 + (a & 0xFFFF)
+        x = (v >> 16) * c16 + (v & 0xFFFF)
         assert x < (1 << 24)
-        r = x - ((x * magic) >> 32) * p - off
-        if r < 0:
-            r += p
+        r = x - ((x * magic) >> 32) * p
         assert r == v % p
 
 

@@ -5,7 +5,8 @@ product (residues of the product in HBM) + reconstruction bit for bit:
 EXCALIBUR_B200_FUSED_APPLY=1 selects the fused path, =0 the two-pass path.
 Both operand layouts are covered: the recomputed residues of X's columns
 (K-major, bbt_exact_apply_q) and the Gram's kept residue planes read MN-major
-(the pipeline's V back-transform)."""
+(the pipeline's V back-transform, by crt_kernel or, with enough row blocks,
+by crt_apply_kernel)."""
 import os
 
 import numpy as np
@@ -52,12 +53,14 @@ def test_fused_apply_equals_two_pass(ctx, m, n, k):
     assert np.array_equal(one, two)
 
 
-@pytest.mark.parametrize("precision", [2])
-def test_fused_pipeline_back_transform_bitwise(ctx, precision):
+# the second row set has more 128-row blocks than the B200 has SMs, so the
+# two-pass product runs the kernel that keeps A's blocks in shared memory
+@pytest.mark.parametrize("rows", [(5000, 3700), (20000, 19300)])
+def test_fused_pipeline_back_transform_bitwise(ctx, rows):
     """The V back-transform from the kept residue planes (MN-major A operand)."""
     rng = np.random.default_rng(12)
-    m, P = 300, 2
-    blocks = [rng.standard_normal((m, n)) for n in (5000, 3700)]
+    m, P, precision = 300, 2, 2
+    blocks = [rng.standard_normal((m, n)) for n in rows]
     pub, priv = oracle.reference_seeds(3, P)
 
     def run():
