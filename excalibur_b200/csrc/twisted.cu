@@ -59,30 +59,64 @@ struct Nrm {
 };
 
 // x[k] = 1, backward with lo, forward with up, normalise.  x has stride ld.
-// Returns the first index of max |x_i| after scaling.
+// Returns the first index of max |x_i| after scaling.  Every loop reads its
+// operands PF elements ahead into registers (the recurrences depend only on
+// the previous value, not on the loads), so the L2 latency of the work arrays
+// is paid once per PF elements; the arithmetic and its order are unchanged.
+constexpr int PF = 8;
+
 __device__ int twisted_solve(int n, int k, const double* lo, const double* up, long ldw, double* x,
                              long ld) {
   x[(long)k * ld] = 1.0;
   double prev = 1.0;
-  for (int i = k - 1; i >= 0; --i) {
-    prev = MUL(-lo[(long)i * ldw], prev);
-    x[(long)i * ld] = prev;
+  for (int i0 = k - 1; i0 >= 0; i0 -= PF) {
+    double v[PF];
+#pragma unroll
+    for (int u = 0; u < PF; ++u) v[u] = (i0 - u >= 0) ? lo[(long)(i0 - u) * ldw] : 0.0;
+#pragma unroll
+    for (int u = 0; u < PF; ++u)
+      if (i0 - u >= 0) {
+        prev = MUL(-v[u], prev);
+        x[(long)(i0 - u) * ld] = prev;
+      }
   }
   prev = 1.0;
-  for (int i = k + 1; i < n; ++i) {
-    prev = MUL(-up[(long)(i - 1) * ldw], prev);
-    x[(long)i * ld] = prev;
+  for (int i0 = k + 1; i0 < n; i0 += PF) {
+    double v[PF];
+#pragma unroll
+    for (int u = 0; u < PF; ++u) v[u] = (i0 + u < n) ? up[(long)(i0 + u - 1) * ldw] : 0.0;
+#pragma unroll
+    for (int u = 0; u < PF; ++u)
+      if (i0 + u < n) {
+        prev = MUL(-v[u], prev);
+        x[(long)(i0 + u) * ld] = prev;
+      }
   }
   Nrm nr;
-  for (int i = 0; i < n; ++i) nr.add(x[(long)i * ld]);
+  for (int i0 = 0; i0 < n; i0 += PF) {
+    double v[PF];
+#pragma unroll
+    for (int u = 0; u < PF; ++u) v[u] = (i0 + u < n) ? x[(long)(i0 + u) * ld] : 0.0;
+#pragma unroll
+    for (int u = 0; u < PF; ++u)
+      if (i0 + u < n) nr.add(v[u]);
+  }
   const double r = DIV(1.0, nr.get());
   int best = 0;
   double bv = 0.0;
-  for (int i = 0; i < n; ++i) {
-    const double v = MUL(x[(long)i * ld], r);
-    x[(long)i * ld] = v;
-    const double av = fabs(v);
-    if (i == 0 || av > bv) { bv = av; best = i; }   // first largest |x_i| (cblas_idamax)
+  for (int i0 = 0; i0 < n; i0 += PF) {
+    double v[PF];
+#pragma unroll
+    for (int u = 0; u < PF; ++u) v[u] = (i0 + u < n) ? x[(long)(i0 + u) * ld] : 0.0;
+#pragma unroll
+    for (int u = 0; u < PF; ++u)
+      if (i0 + u < n) {
+        const int i = i0 + u;
+        const double vs = MUL(v[u], r);
+        x[(long)i * ld] = vs;
+        const double av = fabs(vs);
+        if (i == 0 || av > bv) { bv = av; best = i; }   // first largest |x_i| (cblas_idamax)
+      }
   }
   return best;
 }
@@ -126,15 +160,24 @@ __global__ void __launch_bounds__(64) twisted_kernel(
   int k = n - 1;
   double gbest = fabs(ADD(ADD(s[(long)(n - 1) * w], pi), w2));
   double g0 = gbest;
-  for (int i = n - 2; i >= 0; --i) {
-    const double r = ADD(MUL(D[i], MUL(L[i], L[i])), pi);
-    rp[(long)(i + 1) * w] = r;
-    up[(long)i * w] = DIV(MUL(L[i], D[i]), r);
-    pi = SUB(DIV(MUL(pi, D[i]), r), w2);
-    p[(long)i * w] = pi;
-    const double g = fabs(ADD(ADD(s[(long)i * w], pi), w2));
-    if (g == g && (gbest != gbest || g <= gbest)) { gbest = g; k = i; }
-    g0 = g;
+  for (int i0 = n - 2; i0 >= 0; i0 -= PF) {
+    double sv[PF];
+#pragma unroll
+    for (int u = 0; u < PF; ++u) sv[u] = (i0 - u >= 0) ? s[(long)(i0 - u) * w] : 0.0;
+#pragma unroll
+    for (int u = 0; u < PF; ++u) {
+      const int i = i0 - u;
+      if (i >= 0) {
+        const double r = ADD(MUL(D[i], MUL(L[i], L[i])), pi);
+        rp[(long)(i + 1) * w] = r;
+        up[(long)i * w] = DIV(MUL(L[i], D[i]), r);
+        pi = SUB(DIV(MUL(pi, D[i]), r), w2);
+        p[(long)i * w] = pi;
+        const double g = fabs(ADD(ADD(sv[u], pi), w2));
+        if (g == g && (gbest != gbest || g <= gbest)) { gbest = g; k = i; }
+        g0 = g;
+      }
+    }
   }
   if (g0 != g0) k = 0;
   rp[0] = pi;
@@ -144,13 +187,27 @@ __global__ void __launch_bounds__(64) twisted_kernel(
   int k2 = 0;
   double g2best = 0.0;
   double dprev = 0.0;
-  for (int i = 0; i < n; ++i) {
-    const double s_i = s[(long)i * w];
-    const double s_n = (i + 1 < n) ? s[(long)(i + 1) * w] : -w2;
-    const double p_i = p[(long)i * w];
-    const double p_n = (i + 1 < n) ? p[(long)(i + 1) * w] : 1.0;
-    const double r_n = (i + 1 < n) ? rp[(long)(i + 1) * w] : 1.0;
-    const double d_new = MUL(DIV(s_n, s_i), dp[(long)i * w]);
+  for (int i0 = 0; i0 < n; i0 += PF) {
+    // s, p, rp at i0 .. i0 + PF (one past the batch), dp at i0 .. i0 + PF - 1
+    double sv[PF + 1], pv2[PF + 1], rv[PF + 1], dv[PF];
+#pragma unroll
+    for (int u = 0; u <= PF; ++u) {
+      const int i = i0 + u;
+      sv[u] = (i < n) ? s[(long)i * w] : -w2;
+      pv2[u] = (i < n) ? p[(long)i * w] : 1.0;
+      rv[u] = (i < n) ? rp[(long)i * w] : 1.0;
+      if (u < PF) dv[u] = (i < n) ? dp[(long)i * w] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < PF; ++u) {
+    const int i = i0 + u;
+    if (i >= n) break;
+    const double s_i = sv[u];
+    const double s_n = sv[u + 1];
+    const double p_i = pv2[u];
+    const double p_n = pv2[u + 1];
+    const double r_n = rv[u + 1];
+    const double d_new = MUL(DIV(s_n, s_i), dv[u]);
     const double g_old = ADD(ADD(s_i, p_i), w2);
     const double g_new = fabs(DIV(MUL(MUL(-w2, g_old), r_n), MUL(s_i, p_n)));
     if (i == 0 || g_new < g2best) { g2best = g_new; k2 = i; }
@@ -160,6 +217,7 @@ __global__ void __launch_bounds__(64) twisted_kernel(
       up[(long)(i - 1) * w] = MUL(DIV(a[i], r_new), b[i - 1]);
     }
     dprev = d_new;
+    }
   }
   // u (:126), column j of U
   twisted_solve(n, k2, lp, up, w, U + j, ldu);
