@@ -160,7 +160,7 @@ bbt_status bbt_bisection(bbt_ctx* ctx, int n, const double* a, const double* b, 
   *count = 0;
   if (n < 1 || bad(a) || (n > 1 && bad(b)) || (top_k > 0 && bad(sigma)))
     return fail(ctx, BBT_ERR_ARG, "bisection: bad arguments");
-  BBT_TRY(ensure(ctx, (size_t)(n + 2) * 48 * 18 + (1 << 20)));
+  BBT_TRY(ensure(ctx, bisect_workspace_bytes(n, top_k) + (1 << 20)));
   return bisect(ctx, n, a, b, lo, hi, tol, top_k, sigma, count);
 }
 
@@ -173,7 +173,7 @@ bbt_status bbt_bisection_bracketed(bbt_ctx* ctx, int n, const double* a, const d
   if (n < 1 || bad(a) || (n > 1 && bad(b)) || (top_k > 0 && (bad(sigma) || bad(brackets))))
     return fail(ctx, BBT_ERR_ARG, "bisection: bad arguments");
   const int tk = top_k < n ? top_k : n;
-  BBT_TRY(ensure(ctx, (size_t)(n + 2) * 48 * 18 + (size_t)tk * 64 + (1 << 20)));
+  BBT_TRY(ensure(ctx, bisect_workspace_bytes(n, tk) + (size_t)tk * 64 + (1 << 20)));
   long st[4];
   BBT_TRY(bisect(ctx, n, a, b, lo, hi, tol, top_k, sigma, count, brackets, st));
   if (stats) for (int i = 0; i < 4; ++i) stats[i] = st[i];
@@ -266,7 +266,7 @@ bbt_status bbt_bidiagonal_svd(bbt_ctx* ctx, int k, const double* a, const double
   if (!ctx) return BBT_ERR_ARG;
   if (k < 1 || top_k < 1 || top_k > k || bad(a) || (k > 1 && bad(b)) || bad(U) || bad(V) || bad(sigma))
     return fail(ctx, BBT_ERR_ARG, "bidiagonal_svd: bad arguments (k=%d top_k=%d)", k, top_k);
-  BBT_TRY(ensure(ctx, (size_t)(k + 1) * top_k * 8 * 8 + (size_t)(k + 2) * 48 * 18 + (2 << 20)));
+  BBT_TRY(ensure(ctx, (size_t)(k + 1) * top_k * 8 * 8 + bisect_workspace_bytes(k, top_k) + (2 << 20)));
   return bidiag_svd(ctx, k, a, b, U, V, sigma, top_k, false);
 }
 

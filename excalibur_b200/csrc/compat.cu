@@ -7,15 +7,21 @@
 // reference, so glibc's rand() state after a call is the reference's.
 //
 // Functions the reference declares but never calls from client.cpp with
-// opt_control 1/3 (the unused mask variants, the random orthogonal matrix
-// generators and the opt_control 0/2 dense mask) abort with a message instead
-// of silently computing on the CPU.
+// opt_control 1/3 (the unused mask variants and the opt_control 0/2 dense
+// masks) abort with a message instead of silently computing on the CPU.  The
+// random orthogonal matrix generators run the reference's LAPACK calls
+// through the LAPACK the process links (they are random-number generation,
+// not arithmetic this library accelerates).
 #include <cuda_runtime.h>
+
+#include <dlfcn.h>
 
 #include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <mutex>
+#include <random>
+#include <string>
 #include <vector>
 
 #include "internal.h"
@@ -399,13 +405,136 @@ void naive_givens_mask_parallel(size_t, size_t, size_t, double*, bool, bool, uns
 void givens_mask_cache_optimized_parallel(size_t, size_t, size_t, double*, bool, bool, unsigned int) {
   not_provided("givens_mask_cache_optimized_parallel");
 }
-void generate_random_orthogonal_matrix(int, size_t, double*, double*, unsigned int) {
-  not_provided("generate_random_orthogonal_matrix");
+
+// ---- random orthogonal matrices (bbtsvd.cpp:301-331, 370-395) -------------
+// Normal random entries from LAPACK's dlarnv (seeded from rand(), as the
+// reference seeds it) and Householder reflectors from dlarfg: the same
+// library calls in the same order, so the result is the reference's bit for
+// bit when the process links the same LAPACK.  This library bundles no
+// LAPACK; the functions are found in the process (the reference links MKL)
+// and the call aborts with a message when they are absent.
+namespace {
+using dlarnv_fn = int (*)(int, int*, int, double*);
+using dlarfg_fn = int (*)(int, double*, double*, int, double*);
+using dorgqr_fn = int (*)(int, int, int, int, double*, int, const double*);
+constexpr int ROW_MAJOR = 101, COL_MAJOR = 102;   // CblasRowMajor / LAPACK_ROW_MAJOR, column-major
+
+void* lapack_symbol(const char* name, const char* fn) {
+  void* f = dlsym(RTLD_DEFAULT, name);
+  if (!f) f = dlsym(RTLD_DEFAULT, (std::string("scipy_") + name).c_str());   // scipy's prefixed OpenBLAS
+  if (!f) {
+    fprintf(stderr, "libexcalibur_b200: %s needs %s from the LAPACK the process links; none is loaded\n", fn,
+            name);
+    abort();
+  }
+  return f;
 }
-void generate_random_orthogonal_matrix(size_t, size_t, double*, unsigned int) {
-  not_provided("generate_random_orthogonal_matrix");
+
+void random_seed4(int (&iseed)[4]) {
+  for (int r = 0; r < 4; ++r) iseed[r] = rand() % 4096;
+  if (iseed[3] % 2 == 0) iseed[3] = (iseed[3] + 1) % 4096;   // dlarnv wants an odd last seed
 }
-void shuffle_matrix(size_t, size_t, double*, unsigned int, bool, bool) { not_provided("shuffle_matrix"); }
+}  // namespace
+
+void generate_random_orthogonal_matrix(int matrix_layout, size_t m, double* house, double* tau, unsigned int seed) {
+  const auto dlarnv = (dlarnv_fn)lapack_symbol("LAPACKE_dlarnv", "generate_random_orthogonal_matrix");
+  const auto dlarfg = (dlarfg_fn)lapack_symbol("LAPACKE_dlarfg", "generate_random_orthogonal_matrix");
+  srand(seed);
+  int iseed[4];
+  std::vector<double> h(m);
+  const bool row = matrix_layout == ROW_MAJOR;
+  for (size_t i = 0; i < m; ++i) {   // row-major: row i holds i + 1 entries; else column i from its diagonal
+    random_seed4(iseed);
+    if (row) dlarnv(3, iseed, (int)(i + 1), house + i * m);
+    else dlarnv(3, iseed, (int)(m - i), house + i * m + i);
+  }
+  for (size_t i = 0; i + 1 < m; ++i) {   // reflector i from column i below the diagonal
+    const size_t step = row ? m : 1;
+    for (size_t j = 0; j < m - i; ++j) h[j] = house[i * m + i + j * step];
+    dlarfg((int)(m - i), h.data(), h.data() + 1, 1, tau + i);
+    for (size_t j = 0; j < m - i; ++j) house[i * m + i + j * step] = h[j];
+  }
+  if (m > 0) house[m * m - 1] = 1.0;
+}
+
+void generate_random_orthogonal_matrix(size_t m, size_t n, double* x, unsigned int seed) {
+  const auto dlarnv = (dlarnv_fn)lapack_symbol("LAPACKE_dlarnv", "generate_random_orthogonal_matrix");
+  const auto dlarfg = (dlarfg_fn)lapack_symbol("LAPACKE_dlarfg", "generate_random_orthogonal_matrix");
+  const auto dorgqr = (dorgqr_fn)lapack_symbol("LAPACKE_dorgqr", "generate_random_orthogonal_matrix");
+  srand(seed);
+  int iseed[4];
+  std::vector<double> tau(std::min(m, n));
+  if (m >= n) {   // m x n row-major with orthonormal columns
+    for (size_t i = 0; i < m; ++i) {
+      random_seed4(iseed);
+      dlarnv(3, iseed, (int)std::min(i + 1, n), x + i * n);
+    }
+    for (size_t i = 0; i + 1 < n; ++i) dlarfg((int)(m - i), x + i * n + i, x + i * n + i + n, (int)n, tau.data() + i);
+    dorgqr(ROW_MAJOR, (int)m, (int)n, (int)n, x, (int)n, tau.data());
+  } else {        // orthonormal rows: the transposed problem, column-major
+    for (size_t i = 0; i < m; ++i) {
+      random_seed4(iseed);
+      dlarnv(3, iseed, (int)(n - i), x + i * n + i);
+    }
+    for (size_t i = 0; i + 1 < m; ++i) dlarfg((int)(n - i), x + i * n + i, x + i * n + i + 1, 1, tau.data() + i);
+    dorgqr(COL_MAJOR, (int)n, (int)m, (int)m, x, (int)n, tau.data());
+  }
+}
+
+// ---- shuffle_matrix (bbtsvd.cpp:398-427) -----------------------------------
+// The permutation is drawn on the host with the reference's calls (srand,
+// default_random_engine, shuffle, rand), so rand()'s state afterwards is the
+// reference's; the swaps of rows (is_left) or columns run on the GPU: the
+// pairs are disjoint, and the extra swap of an odd count goes first when
+// unshuffling and last otherwise, as in the reference.
+namespace {
+__global__ void swap_lines_kernel(int npairs, const int2* __restrict__ pr, size_t len, size_t lstride,
+                                  size_t estride, double* __restrict__ x) {
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < (long)npairs * (long)len;
+       t += (long)gridDim.x * blockDim.x) {
+    const int2 q = pr[t / (long)len];
+    const size_t e = (size_t)(t % (long)len) * estride;
+    double* a = x + (size_t)q.x * lstride + e;
+    double* b = x + (size_t)q.y * lstride + e;
+    const double ta = *a;
+    *a = *b;
+    *b = ta;
+  }
+}
+}  // namespace
+
+void shuffle_matrix(size_t m, size_t n, double* x, unsigned int seed, bool is_left, bool unshuffle) {
+  srand(seed);
+  auto dre = std::default_random_engine(seed);
+  const size_t k = is_left ? m : n;
+  std::vector<int> idx(k);
+  for (size_t i = 0; i < k; ++i) idx[i] = (int)i;
+  std::shuffle(idx.begin(), idx.end(), dre);
+  size_t ri = 0;
+  if (k % 2 != 0) ri = k > 1 ? rand() % (k - 1) : 0;   // the reference divides by zero at k = 1
+  std::vector<int2> first, pairs, last;
+  if (k % 2 != 0 && unshuffle) first.push_back(make_int2((int)(k - 1), (int)ri));
+  for (size_t i = 0; i < k / 2; ++i) pairs.push_back(make_int2(idx[2 * i], idx[2 * i + 1]));
+  if (k % 2 != 0 && !unshuffle) last.push_back(make_int2((int)(k - 1), (int)ri));
+  if (m == 0 || n == 0) return;
+  bbt_ctx* c = ctx();
+  Dev dx(x, m * n);
+  const size_t len = is_left ? n : m, lstride = is_left ? n : 1, estride = is_left ? 1 : n;
+  for (const auto* v : {&first, &pairs, &last}) {
+    if (v->empty()) continue;
+    int2* dp = nullptr;
+    if (cudaMalloc(&dp, v->size() * sizeof(int2)) != cudaSuccess) die("cudaMalloc", BBT_ERR_NOMEM);
+    if (cudaMemcpyAsync(dp, v->data(), v->size() * sizeof(int2), cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
+      die("cudaMemcpyAsync", BBT_ERR_CUDA);
+    const long work = (long)v->size() * (long)len;
+    const unsigned g = (unsigned)std::min<long>((work + 255) / 256, 8L * c->num_sms);
+    swap_lines_kernel<<<g, 256, 0, c->stream>>>((int)v->size(), dp, len, lstride, estride, dx.p);
+    launched(c, "shuffle_matrix");
+    sync(c, "shuffle_matrix");
+    cudaFree(dp);
+  }
+  dx.back(x, m * n);
+}
 void block_mask(size_t, size_t, size_t, double*, bool, bool, unsigned int) { not_provided("block_mask"); }
 void shuffle_block_mask(size_t, size_t, size_t, int, double*, bool, bool, unsigned int) {
   not_provided("shuffle_block_mask");

@@ -199,7 +199,7 @@ size_t scratch_bytes(const bbt_ctx* ctx, const Layout& L) {
   s = std::max(s, qr_workspace_bytes((long)L.rg, (int)L.m, (int)L.m, qp));
   const size_t m = L.m;
   s = std::max(s, (7 * (m + 1) * m + 4 * m) * 8 + 4096);          // twisted
-  s = std::max(s, (m + 2) * (1 + 8 + 1 + 7) * 48 + 4096);         // bisection nodes
+  s = std::max(s, bisect_workspace_bytes((int)m, (int)m) + 16 * m);   // bisection nodes, brackets
   size_t mask = mask_workspace_bytes(m, m, MASK_PASSES, true);   // FinalU (m x k, k <= m)
   for (int c = 0; c < L.P; ++c)
     mask = std::max({mask, mask_workspace_bytes(m, L.r[c], MASK_PASSES, true),
@@ -507,7 +507,7 @@ size_t tall_scratch_bytes(const bbt_ctx* ctx, const Layout& L, const Layout& Q) 
     }
   s = std::max(s, qr_workspace_bytes((long)g, (int)g, (int)g, qp));   // the reflectors of Ralha on U_b
   s = std::max(s, (7 * (g + 1) * g + 4 * g) * 8 + 4096);              // twisted
-  s = std::max(s, (g + 2) * (1 + 8 + 1 + 7) * 48 + 4096);             // bisection nodes
+  s = std::max(s, bisect_workspace_bytes((int)g, (int)g) + 16 * g);       // bisection nodes, brackets
   size_t mask = std::max(mask_workspace_bytes(g, L.m, MASK_PASSES, false),    // FinalU (k x m, k <= g)
                          mask_workspace_bytes(1, L.m, MASK_PASSES, false));   // y
   for (int c = 0; c < L.P; ++c)
@@ -1132,7 +1132,7 @@ bbt_status svd_dense(bbt_ctx* ctx, int m, double* X, int top_k, double* sigma, d
   const size_t mm = (size_t)m * m;
   QrPlan qp;
   size_t scratch = std::max(qr_workspace_bytes(m, m, m, qp), (7 * ((size_t)m + 1) * m + 4 * (size_t)m) * 8 + 4096);
-  scratch = std::max(scratch, ((size_t)m + 2) * 17 * 48 + 4096) + (64u << 20);
+  scratch = std::max(scratch, bisect_workspace_bytes(m, m) + 16 * (size_t)m) + (64u << 20);
   const size_t need = (2 * mm + 8 * (size_t)m + 64) * 8 + 4096 + scratch;
   if (ctx->ws.cap < need) BBT_CUDA(ctx, ctx->ws.reserve(need));
   ctx->ws.reset();

@@ -152,6 +152,9 @@ bbt_status sturm_counts(bbt_ctx* ctx, int n, const double* a, const double* b, c
 // snapped to the reference's tree, verified by Sturm counts, used to skip
 // levels; stats (optional, 4): Sturm evaluations (verification included),
 // rounds, jumps taken, Sturm evaluations spent on verification.
+// Scratch of bisect for an order-n bidiagonal and top_k values (the node
+// tree, the candidates of a round, the learned-bracket table).
+size_t bisect_workspace_bytes(int n, int top_k);
 bbt_status bisect(bbt_ctx* ctx, int n, const double* a, const double* b, double lo, double hi,
                   double tol, int top_k, double* sigma, int* count, const double* brackets = nullptr,
                   long* stats = nullptr);

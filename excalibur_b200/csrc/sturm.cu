@@ -25,7 +25,7 @@
 namespace bbt {
 namespace {
 
-constexpr int DEPTH = 3;                 // tree levels resolved per round
+constexpr int DEPTH = 5;                 // tree levels resolved per round
 constexpr int NPTS = (1 << DEPTH) - 1;   // midpoints counted per live interval
 constexpr int FAN = 1 << DEPTH;          // max intervals one interval becomes
 constexpr int SMEM_PAIRS_MAX = 12288;    // stage (beta^2, alpha^2) in SMEM up to this n
@@ -272,6 +272,12 @@ bbt_status sturm_counts(bbt_ctx* ctx, int n, const double* a, const double* b, c
   BBT_LAUNCHED(ctx);
   ctx->ws.top = mark;
   return BBT_OK;
+}
+
+size_t bisect_workspace_bytes(int n, int top_k) {
+  const size_t cap = (size_t)std::max(n, 0) + 2;
+  const size_t tk = (size_t)std::max(top_k, 0);
+  return 16 * cap + cap * (sizeof(Node) * (1 + FAN) + sizeof(int) * (1 + NPTS)) + tk * sizeof(Node) + 16 * 256 + 4096;
 }
 
 bbt_status bisect(bbt_ctx* ctx, int n, const double* a, const double* b, double lo, double hi,

@@ -268,19 +268,34 @@ __global__ void check_none_kernel(int k, int top_k, const double* __restrict__ s
 
 // client.cpp:988-995: make the largest |entry| of each u positive, flipping
 // u and v together.  One thread per column of U (k x cnt row-major).
-__global__ void global_sign_kernel(int k, int cnt, double* __restrict__ U, double* __restrict__ V) {
+// client.cpp:987-995: each column of U (k x cnt, row-major) made positive at
+// its first largest |entry|, the matching row of V (cnt x k) flipped with it.
+// One thread per column finds the entry (loads read PF rows ahead) and flips
+// U's column, coalesced across the warp; the rows of V are flipped by
+// vflip_kernel, coalesced along each row.
+__global__ void global_sign_kernel(int k, int cnt, double* __restrict__ U, signed char* __restrict__ flip) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= cnt) return;
   int best = 0;
   double bv = fabs(U[j]);
-  for (int i = 1; i < k; ++i) {
-    const double v = fabs(U[(long)i * cnt + j]);
-    if (v > bv) { bv = v; best = i; }
+  for (int i0 = 1; i0 < k; i0 += PF) {
+    double v[PF];
+#pragma unroll
+    for (int u = 0; u < PF; ++u) v[u] = (i0 + u < k) ? fabs(U[(long)(i0 + u) * cnt + j]) : 0.0;
+#pragma unroll
+    for (int u = 0; u < PF; ++u)
+      if (i0 + u < k && v[u] > bv) { bv = v[u]; best = i0 + u; }
   }
-  if (U[(long)best * cnt + j] < 0) {
+  const bool neg = U[(long)best * cnt + j] < 0;
+  flip[j] = neg ? 1 : 0;
+  if (neg)
     for (int i = 0; i < k; ++i) U[(long)i * cnt + j] = -U[(long)i * cnt + j];
-    for (int i = 0; i < k; ++i) V[(long)j * k + i] = -V[(long)j * k + i];
-  }
+}
+
+__global__ void vflip_kernel(int k, int cnt, const signed char* __restrict__ flip, double* __restrict__ V) {
+  const long total = (long)k * cnt;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x)
+    if (flip[e / k]) V[e] = -V[e];
 }
 
 // ||a||^2 + ||b||^2 with the scaled norm (bbtsvd.cpp:936), one thread.
@@ -437,7 +452,11 @@ bbt_status bidiag_svd(bbt_ctx* ctx, int k, const double* a, const double* b, dou
   check_none_kernel<<<top_k, 128, 0, ctx->stream>>>(k, top_k, sigma, a, U, V);
   BBT_LAUNCHED(ctx);
   if (global_sign) {
-    global_sign_kernel<<<(top_k + 63) / 64, 64, 0, ctx->stream>>>(k, top_k, U, V);
+    signed char* flip = ctx->ws.take<signed char>(top_k);
+    if (!flip) return fail(ctx, BBT_ERR_NOMEM, "bidiagonal svd: sign workspace");
+    global_sign_kernel<<<(top_k + 63) / 64, 64, 0, ctx->stream>>>(k, top_k, U, flip);
+    BBT_LAUNCHED(ctx);
+    vflip_kernel<<<2 * ctx->num_sms, 256, 0, ctx->stream>>>(k, top_k, flip, V);
     BBT_LAUNCHED(ctx);
   }
   ctx->ws.top = mark;

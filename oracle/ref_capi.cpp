@@ -5,6 +5,7 @@
 // can call them through ctypes.  Built only where the reference sources are
 // present; nothing here is part of the product.
 #include <cstdint>
+#include <cstdlib>
 #include "bbtsvd.hpp"
 
 extern "C" {
@@ -42,5 +43,15 @@ void ref_generate_house(int n, double* x, int inc, double* beta) { generate_hous
 void ref_mmap_drot(size_t n, double* x, size_t incx, double* y, size_t incy, double c, double s) {
   mmap_drot(n, x, incx, y, incy, c, s);
 }
+void ref_random_orthogonal_house(int layout, size_t m, double* house, double* tau, unsigned seed) {
+  generate_random_orthogonal_matrix(layout, m, house, tau, seed);
+}
+void ref_random_orthogonal(size_t m, size_t n, double* x, unsigned seed) {
+  generate_random_orthogonal_matrix(m, n, x, seed);
+}
+void ref_shuffle_matrix(size_t m, size_t n, double* x, unsigned seed, int is_left, int unshuffle) {
+  shuffle_matrix(m, n, x, seed, is_left != 0, unshuffle != 0);
+}
+int ref_rand() { return rand(); }
 void ref_set_threads(int n) { omp_set_num_threads(n); mkl_set_num_threads(n); }
 }

@@ -142,3 +142,9 @@ def step_cases():
     out["house_zero_tail_neg"] = (a, b, 0, 0, np.array([-2.0] + [0.0] * 9), 1, (0.6, 0.8))
     out["house_zero_tail_pos"] = (a, b, 0, 0, np.array([2.0] + [0.0] * 9), 1, (0.6, -0.8))
     return out
+
+
+# Fixtures of the reference's random orthogonal matrix generators and
+# shuffle_matrix (make_golden.py generator_fixtures): name -> its test.
+GENERATOR_FIXTURES = ("house_row7", "house_col6", "orth_tall9x4", "orth_wide4x9", "shuffle_left7x5",
+                      "unshuffle_left7x5", "shuffle_right6x9", "unshuffle_right6x9", "shuffle_left8x3")

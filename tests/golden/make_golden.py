@@ -222,6 +222,33 @@ def step_fixtures(R):
     return out
 
 
+def generator_fixtures(R):
+    """The reference's random orthogonal matrix generators and shuffle_matrix
+    (bbtsvd.cpp:301-331, 370-427) on small shapes, each with the next rand()
+    value after the call (the glibc state the reference leaves behind)."""
+    R.ref_rand.restype = C.c_int
+    out = {}
+    for name, (layout, m, seed) in {"house_row7": (101, 7, 5), "house_col6": (102, 6, 9)}.items():
+        house, tau = np.zeros(m * m), np.zeros(max(m - 1, 1))
+        R.ref_random_orthogonal_house(C.c_int(layout), C.c_size_t(m), p(house), p(tau), C.c_uint(seed))
+        out[name] = dict(layout=np.int32(layout), m=np.int64(m), seed=np.uint32(seed), house=house, tau=tau,
+                         rand_after=np.int64(R.ref_rand()))
+    for name, (m, n, seed) in {"orth_tall9x4": (9, 4, 3), "orth_wide4x9": (4, 9, 11)}.items():
+        x = np.zeros(m * n)
+        R.ref_random_orthogonal(C.c_size_t(m), C.c_size_t(n), p(x), C.c_uint(seed))
+        out[name] = dict(m=np.int64(m), n=np.int64(n), seed=np.uint32(seed), x=x, rand_after=np.int64(R.ref_rand()))
+    rng = np.random.default_rng(17)
+    for name, (m, n, seed, left, unsh) in {"shuffle_left7x5": (7, 5, 21, 1, 0), "unshuffle_left7x5": (7, 5, 21, 1, 1),
+                                           "shuffle_right6x9": (6, 9, 8, 0, 0), "unshuffle_right6x9": (6, 9, 8, 0, 1),
+                                           "shuffle_left8x3": (8, 3, 2, 1, 0)}.items():
+        x0 = rng.standard_normal(m * n)
+        x = x0.copy()
+        R.ref_shuffle_matrix(C.c_size_t(m), C.c_size_t(n), p(x), C.c_uint(seed), C.c_int(left), C.c_int(unsh))
+        out[name] = dict(m=np.int64(m), n=np.int64(n), seed=np.uint32(seed), is_left=np.int32(left),
+                         unshuffle=np.int32(unsh), x_in=x0, x_out=x, rand_after=np.int64(R.ref_rand()))
+    return out
+
+
 def main():
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref", f"REF={REF}"], check=True)
     R = C.CDLL(os.path.join(REFDIR, "libref_capi.so"))
@@ -229,7 +256,7 @@ def main():
     R.ref_set_threads(1)
     fx = {}
     groups = (("bidiag", bidiagonal_fixtures), ("mask", mask_fixtures), ("step", step_fixtures),
-              ("pipe", lambda R: pipeline_fixtures()))
+              ("gen", generator_fixtures), ("pipe", lambda R: pipeline_fixtures()))
     keep = sys.argv[1:]
     for grp, fn in groups:
         if keep and not any(k.startswith(grp) for k in keep):

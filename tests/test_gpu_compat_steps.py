@@ -77,3 +77,19 @@ def test_step_helpers_match_reference(lib, golden, name):
     x, y = a.copy(), np.resize(b, n).copy()
     rot(n, p(x), 1, p(y), 1, float(g["drot_c"]), float(g["drot_s"]))
     assert np.array_equal(x, g["drot_x"]) and np.array_equal(y, g["drot_y"])
+
+
+@pytest.mark.parametrize("name", ["shuffle_left7x5", "unshuffle_left7x5", "shuffle_right6x9",
+                                  "unshuffle_right6x9", "shuffle_left8x3"])
+def test_shuffle_matrix(lib, golden, name):
+    """shuffle_matrix (bbtsvd.cpp:398-427): the permutation drawn on the host
+    with the reference's calls, the row or column swaps on the GPU; the
+    result and glibc's rand() state afterwards are the reference's."""
+    g = golden(f"gen__{name}")
+    m, n = int(g["m"]), int(g["n"])
+    x = g["x_in"].copy()
+    f = fn(lib, "_Z14shuffle_matrixmmPdjbb", [C.c_size_t, C.c_size_t, D, C.c_uint, C.c_bool, C.c_bool])
+    f(m, n, p(x), int(g["seed"]), bool(g["is_left"]), bool(g["unshuffle"]))
+    assert np.array_equal(x, g["x_out"])
+    libc = C.CDLL(None)
+    assert libc.rand() == int(g["rand_after"])
