@@ -467,8 +467,8 @@ __device__ __forceinline__ void chol_tile_cta(double* D, double* rinv, int kb, i
       if (tid == 0) atomicExch(flag, 1);
       d = 1.0;
     }
-    const double r = sqrt(d);
-    const double ri = 1.0 / r;
+    const double ri = rsqrt(d);   // 1 / R(j, j); R(j, j) = d / sqrt(d)
+    const double r = d * ri;
     if (tid < 32 && tid > j && tid < kb) D[j * TSTR + tid] *= ri;
     __syncthreads();   // every thread has read D(j, j); row j is scaled
     if (tid == j) {    // R(j, j): not read again in this step or later ones

@@ -299,14 +299,18 @@ bbt_status exact_apply_rows(bbt_ctx* ctx, const ExactOperand& op, long rows, con
 // planes [q][m][pitch], pitch = crt_pitch(rows)): X_int^T as an MN-major
 // operand, so the block is not read again.
 bbt_status exact_apply_planes(bbt_ctx* ctx, const ExactOperand& op, long rows, const int8_t* planes, long pitch,
-                              double* C, long ldc) {
+                              double* C, long ldc, const std::function<bbt_status(long, int)>* after,
+                              long chunk_rows) {
   if (rows > 0x7fffffffL) return fail(ctx, BBT_ERR_ARG, "exact apply: rows=%ld", rows);
   const int m = op.m, k = op.k, nm = op.nm;
   const int shift = (GRAM_BITS - 1) + (Z_BITS - 1);
-  if (apply_fused(m, nm))   // the kept planes in, FP64 out: no scratch at all
-    return crt_product_fused(ctx, (int)rows, k, m, nm, planes, pitch, op.RB, op.Kp, op.t, shift, 1.0, C, ldc);
+  if (apply_fused(m, nm)) {   // the kept planes in, FP64 out: no scratch at all
+    BBT_TRY(crt_product_fused(ctx, (int)rows, k, m, nm, planes, pitch, op.RB, op.Kp, op.t, shift, 1.0, C, ldc));
+    return after ? (*after)(0, (int)rows) : BBT_OK;
+  }
   const size_t mark = ctx->ws.top;
-  const long rc = apply_chunk(rows, nm, 0, k, false);   // only the product's residues are scratch here
+  long rc = apply_chunk(rows, nm, 0, k, false);   // only the product's residues are scratch here
+  if (chunk_rows > 0 && rc > chunk_rows) rc = std::max(128L, chunk_rows / 128 * 128);
   uint8_t* Rb = ctx->ws.take<uint8_t>(crt_product_bytes(ctx, (int)rc, k, m, nm, false));
   if (!Rb) return fail(ctx, BBT_ERR_NOMEM, "exact apply: workspace");
   for (long r0 = 0; r0 < rows; r0 += rc) {   // row chunks start at multiples of 128: 16-byte TMA offsets
@@ -314,6 +318,7 @@ bbt_status exact_apply_planes(bbt_ctx* ctx, const ExactOperand& op, long rows, c
     int splits = 1;
     BBT_TRY(crt_product_amn(ctx, R, k, m, nm, planes + r0, pitch, op.RB, op.Kp, Rb, &splits));
     BBT_TRY(crt_combine(ctx, R, k, nm, splits, Rb, false, nullptr, op.t, shift, 1.0, 0.0, C + r0, ldc));
+    if (after) BBT_TRY((*after)(r0, R));
   }
   ctx->ws.top = mark;
   return BBT_OK;

@@ -980,13 +980,34 @@ bbt_status fedsvd(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* X, 
       BBT_TRY(dgemm(ctx, false, true, rc, k, m, 1.0, M + L.rpos[c], (long)rg, Ub, k, 0.0, tmp, rc));
     BBT_TRY(apply_mask(ctx, pf, (size_t)k, (size_t)rc, tmp, false, false, cfg->private_seeds[c]));
     const long n = (long)L.n[c];
+    bool vt_sent = false;   // FinalVT_c already copied out chunk by chunk
     if (L.qr[c] && L.precision == 2) {   // Q_c = X_int^T Rp_c^-1 W_c: FinalVT^T = X_int^T Rp_c^-1 (W_c tmp^T)
       BBT_TRY(dgemm(ctx, false, false, mi, k, m, 1.0, job.W[c], (long)m, tmp, rc, 0.0, Z, (long)m));
       const size_t mark = ctx->ws.top;
       if (!job.planes.empty() && job.planes[c]) {   // from the planes the local QR kept
         ExactOperand op;
         BBT_TRY(exact_operand(ctx, mi, job.scale[c], job.Rp[c], Z, k, op));
-        BBT_TRY(exact_apply_planes(ctx, op, n, job.planes[c], crt_pitch(n), VT[c], n));
+        if (ctx->io_on && ctx->vt_dst[c]) {
+          // host output: each chunk of rows leaves as soon as it is computed
+          // (a 2D copy of its k row segments), eight chunks per participant
+          double* dst = ctx->vt_dst[c];
+          double* src = VT[c];
+          const std::function<bbt_status(long, int)> out = [&](long r0, int R) -> bbt_status {
+            cudaEvent_t ev;
+            BBT_CUDA(ctx, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+            BBT_CUDA(ctx, cudaEventRecord(ev, ctx->stream));
+            BBT_CUDA(ctx, cudaStreamWaitEvent(ctx->copy_out, ev, 0));
+            BBT_CUDA(ctx, cudaEventDestroy(ev));
+            BBT_CUDA(ctx, cudaMemcpy2DAsync(dst + r0, (size_t)n * sizeof(double), src + r0, (size_t)n * sizeof(double),
+                                            (size_t)R * sizeof(double), (size_t)k, cudaMemcpyDeviceToHost,
+                                            ctx->copy_out));
+            return BBT_OK;
+          };
+          BBT_TRY(exact_apply_planes(ctx, op, n, job.planes[c], crt_pitch(n), VT[c], n, &out, (n + 7) / 8));
+          vt_sent = true;
+        } else {
+          BBT_TRY(exact_apply_planes(ctx, op, n, job.planes[c], crt_pitch(n), VT[c], n));
+        }
       } else {
         BBT_TRY(exact_apply_q(ctx, mi, n, X[c], n, job.scale[c], job.Rp[c], Z, k, VT[c], n));
       }
@@ -1003,7 +1024,7 @@ bbt_status fedsvd(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* X, 
       BBT_CUDA(ctx, cudaMemcpyAsync(VT[c], tmp, (size_t)k * n * sizeof(double), cudaMemcpyDeviceToDevice,
                                     ctx->stream));
     }
-    if (ctx->io_on && ctx->vt_dst[c]) {   // FinalVT_c leaves while the next participant is computed
+    if (ctx->io_on && ctx->vt_dst[c] && !vt_sent) {   // FinalVT_c leaves while the next participant is computed
       BBT_CUDA(ctx, cudaEventRecord(ctx->vt_done[c], ctx->stream));
       BBT_CUDA(ctx, cudaStreamWaitEvent(ctx->copy_out, ctx->vt_done[c], 0));
       BBT_CUDA(ctx, cudaMemcpyAsync(ctx->vt_dst[c], VT[c], (size_t)k * n * sizeof(double), cudaMemcpyDeviceToHost,

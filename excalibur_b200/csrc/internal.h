@@ -4,6 +4,7 @@
 
 #include <cstdint>
 #include <cstdio>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -381,8 +382,12 @@ bbt_status exact_operand(bbt_ctx* ctx, int m, const double* scale, const double*
                          ExactOperand& op);
 bbt_status exact_apply_rows(bbt_ctx* ctx, const ExactOperand& op, long rows, const double* X, long ldx,
                             const double* scale, double* C, long ldc);
+// after(r0, R), when given, is called once the rows [r0, r0 + R) of C are
+// issued on the context's stream (the caller can copy them out while the
+// next rows are computed); chunk_rows (> 0) caps the rows per chunk.
 bbt_status exact_apply_planes(bbt_ctx* ctx, const ExactOperand& op, long rows, const int8_t* planes, long pitch,
-                              double* C, long ldc);
+                              double* C, long ldc, const std::function<bbt_status(long, int)>* after = nullptr,
+                              long chunk_rows = 0);
 size_t exact_apply_workspace_bytes(const bbt_ctx* ctx, long rows, int m, int k);
 bbt_status exact_apply_q(bbt_ctx* ctx, int m, long rows, const double* X, long ldx, const double* scale,
                          const double* Rp, const double* Z, int k, double* C, long ldc);
