@@ -93,12 +93,16 @@ constexpr uint32_t glimb_c(int p, int inv, int l) {
   }
   return out[l];
 }
+constexpr uint32_t byte_weight(int p, int j) { return (uint32_t)(((uint64_t)1 << (8 * j)) % (uint64_t)p); }
 template <int Q>
-struct ModR {   // residues of an integer t = a 2^36 + b 2^18 + c
+struct ModR {   // residues of an integer t from the bytes of u = t + 2^51
   static constexpr int p = MODULI[Q];
-  static constexpr int c36 = (int)((1LL << 36) % p), c18 = (1 << 18) % p;
-  static constexpr int off = p * (((1 << 23) + p - 1) / p);
-  static constexpr uint32_t magic35 = (uint32_t)((((uint64_t)1 << 35) + p - 1) / p);
+  // 256^j mod p for the bytes j = 0..3 of u's low word and 4..6 of its high word
+  static constexpr uint32_t W0 = byte_weight(p, 0) | byte_weight(p, 1) << 8 | byte_weight(p, 2) << 16 |
+                                 byte_weight(p, 3) << 24;
+  static constexpr uint32_t W1 = byte_weight(p, 4) | byte_weight(p, 5) << 8 | byte_weight(p, 6) << 16;
+  static constexpr uint32_t off = (uint32_t)p - (uint32_t)(((uint64_t)1 << 51) % (uint64_t)p);   // -2^51 mod p, in [1, p]
+  static constexpr uint32_t magic32 = (uint32_t)((((uint64_t)1 << 32) + p - 1) / p);
 };
 template <int Q, int NM>
 struct ModK {   // reconstruction from the residues of an NM-modulus set
@@ -221,38 +225,35 @@ struct ModTab {
   int n;
   int p[MAXMOD];
   double invp[MAXMOD];
-  int c36[MAXMOD], c18[MAXMOD];   // 2^36, 2^18 mod p
-  int off[MAXMOD];                // a multiple of p above 2^23
-  uint32_t magic35[MAXMOD];       // ceil(2^35 / p): exact quotients below 2^27
 };
 
-// t = a 2^36 + b 2^18 + c (|t| <= 2^51): |a| <= 2^15, 0 <= b, c < 2^18, exact.
-struct Pieces {
-  int a, b, c;
+// An integer-valued t with |t| <= 2^51 as u = t + 2^51 in [0, 2^52]:
+// y = t + 1.5 2^52 is exact (unit spacing below 2^53, and u = 2^52 gives
+// y = 2^53 exactly), y's low word is u's low 32 bits, and y's high word less
+// that of 2^52 is u >> 32 (at y = 2^53 the exponent step leaves 2^20 there,
+// which is 2^52 >> 32).
+struct U52 {
+  uint32_t lo, hi;
 };
-__device__ __forceinline__ Pieces pieces(double t) {
-  const double RND = 6755399441055744.0;
-  const double a = floor(t * 0x1p-36);
-  const double rem = fma(-a, 0x1p36, t);
-  const double b = floor(rem * 0x1p-18);
-  const double c = fma(-b, 0x1p18, rem);
-  return {__double2loint(a + RND), __double2loint(b + RND), __double2loint(c + RND)};
+__device__ __forceinline__ U52 offset_u52(double t) {
+  const double y = __dadd_rn(t, 0x1.8p52);
+  return {(uint32_t)__double2loint(y), (uint32_t)__double2hiint(y) - 0x43300000u};
 }
 
-// The residue in [0, p) of modulus Q from the pieces: x = a c36 + b c18 + c +
-// off lies in [0, 2^27) and its multiply-high quotient by p is exact.
+// The residue in [0, p) of modulus Q: u's seven bytes (the high word is at
+// most 2^20) weighted by 256^j mod p in two byte dot products, plus -2^51 mod
+// p: 0 < x < 2^19, so the multiply-high quotient by ceil(2^32 / p) is exact.
 template <int Q>
-__device__ __forceinline__ int res_q(const Pieces& t) {
+__device__ __forceinline__ uint32_t res_q(const U52& u) {
   using C = ModR<Q>;
-  const uint32_t x = (uint32_t)(t.a * C::c36 + t.b * C::c18 + t.c + C::off);
-  return (int)(x - (__umulhi(x, C::magic35) >> 3) * (uint32_t)C::p);
+  const uint32_t x = __dp4a(u.lo, C::W0, __dp4a(u.hi, C::W1, C::off));
+  return x - __umulhi(x, C::magic32) * (uint32_t)C::p;
 }
 
 template <int Q>
-__device__ __forceinline__ void store4_q(const Pieces (&t)[4], int8_t* o, int valid) {
-  uint32_t w = 0;
-#pragma unroll
-  for (int e = 0; e < 4; ++e) w |= (uint32_t)(uint8_t)(int8_t)res_q<Q>(t[e]) << (8 * e);
+__device__ __forceinline__ void store4_q(const U52 (&t)[4], int8_t* o, int valid) {
+  const uint32_t w = __byte_perm(__byte_perm(res_q<Q>(t[0]), res_q<Q>(t[1]), 0x0040),
+                                 __byte_perm(res_q<Q>(t[2]), res_q<Q>(t[3]), 0x0040), 0x5410);
   if (valid == 4) {
     *reinterpret_cast<uint32_t*>(o) = w;
   } else {
@@ -260,7 +261,7 @@ __device__ __forceinline__ void store4_q(const Pieces (&t)[4], int8_t* o, int va
   }
 }
 template <int... Q>
-__device__ __forceinline__ void store4_all(const Pieces (&t)[4], int8_t* o, size_t plane, int valid,
+__device__ __forceinline__ void store4_all(const U52 (&t)[4], int8_t* o, size_t plane, int valid,
                                            std::integer_sequence<int, Q...>) {
   (store4_q<Q>(t, o + (size_t)Q * plane, valid), ...);
 }
@@ -277,16 +278,11 @@ __global__ void residues_rows_kernel(int rows, long K, const double* __restrict_
     const long k = kk * 4;
     const double mul = pow2_ratio(b, scale[i]);   // a power of two: exact
     const double* x = X + (long)i * rs + k;
-    Pieces t[4];
+    U52 t[4];
 #pragma unroll
-    for (int e = 0; e < 4; ++e) t[e] = pieces((k + e < K) ? rint(x[e] * mul) : 0.0);
+    for (int e = 0; e < 4; ++e) t[e] = offset_u52((k + e < K) ? rint(x[e] * mul) : 0.0);
     store4_all(t, out + (size_t)i * Kp + k, plane, (int)min(4L, K - k), std::make_integer_sequence<int, NM>{});
   }
-}
-
-template <int... Q>
-__device__ __forceinline__ void store1_all(const Pieces& t, int8_t* o, size_t plane, std::integer_sequence<int, Q...>) {
-  ((o[(size_t)Q * plane] = (int8_t)res_q<Q>(t)), ...);
 }
 
 // Rows contiguous in i, K stride cs; the scale belongs to the K index
@@ -313,9 +309,9 @@ __global__ void __launch_bounds__(256) residues_cols_kernel(int rows, long K, co
   for (int r = ty; r < 32; r += 8) {
     const int i = i0 + r;
     if (i < rows && k < K) {
-      Pieces t[4];
+      U52 t[4];
 #pragma unroll
-      for (int e = 0; e < 4; ++e) t[e] = pieces(tile[4 * tx + e][r]);
+      for (int e = 0; e < 4; ++e) t[e] = offset_u52(tile[4 * tx + e][r]);
       store4_all(t, out + (size_t)i * Kp + k, plane, (int)min(4L, K - k), std::make_integer_sequence<int, NM>{});
     }
   }
@@ -1125,10 +1121,6 @@ ModTab mod_tab(int n) {
     const int p = MODULI[q];
     t.p[q] = p;
     t.invp[q] = 1.0 / p;
-    t.c36[q] = (int)(((uint64_t)1 << 36) % (uint64_t)p);
-    t.c18[q] = (1 << 18) % p;
-    t.off[q] = p * (((1 << 23) + p - 1) / p);
-    t.magic35[q] = (uint32_t)((((uint64_t)1 << 35) + p - 1) / p);
   }
   return t;
 }
@@ -1190,6 +1182,12 @@ bbt_status crt_row_scales(bbt_ctx* ctx, int rows, long K, const double* X, long 
   scale_kernel<<<(rows + 255) / 256, 256, 0, ctx->stream>>>(rows, mx, scale);
   BBT_LAUNCHED(ctx);
   return BBT_OK;   // mx stays taken until the caller releases its workspace mark
+}
+
+bbt_status crt_scales_from_max(bbt_ctx* ctx, int rows, const unsigned long long* mx, double* scale) {
+  scale_kernel<<<(rows + 255) / 256, 256, 0, ctx->stream>>>(rows, mx, scale);
+  BBT_LAUNCHED(ctx);
+  return BBT_OK;
 }
 
 bbt_status crt_residues_rows(bbt_ctx* ctx, int rows, long K, const double* X, long rs, const double* scale, int b,

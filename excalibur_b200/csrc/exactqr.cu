@@ -120,7 +120,7 @@ size_t exact_qr_workspace_bytes(const bbt_ctx* ctx, int m, long n) {
   size_t s = sketch_workspace_bytes(ctx, m, n, N);
   s = std::max(s, dgemm_workspace_bytes(ctx, m, m, N));
   s = std::max(s, exact_gram_workspace_bytes(ctx, m, n));
-  return s + ((size_t)N * m + 6 * (size_t)m * m + 2 * m) * 8 + 16384;
+  return s + ((size_t)N * m + 6 * (size_t)m * m + 3 * m) * 8 + 16384;
 }
 
 int exact_keep_moduli(int m, long n) {
@@ -147,7 +147,7 @@ size_t exact_gram_workspace_bytes(const bbt_ctx* ctx, int m, long n) {
 // scales over all of K first) whose products' K-splits sit side by side and
 // are summed by one reconstruction.
 bbt_status exact_gram_dd(bbt_ctx* ctx, int m, long n, const double* X, long ldx, double* scale, int8_t* keep,
-                         double* Gh, double* Gl) {
+                         double* Gh, double* Gl, const unsigned long long* rowmax) {
   const int nm = crt_moduli(GRAM_BITS, GRAM_BITS, n);
   if (nm < 1) return fail(ctx, BBT_ERR_ARG, "exact Gram: n=%ld too long", n);
   const size_t m2 = ctx->ws.top;
@@ -156,7 +156,10 @@ bbt_status exact_gram_dd(bbt_ctx* ctx, int m, long n, const double* X, long ldx,
   const long Kp = crt_pitch(kc);
   int8_t* RX = keep ? keep : ctx->ws.take<int8_t>((size_t)nm * m * Kp);
   const size_t m3 = ctx->ws.top;
-  BBT_TRY(crt_row_scales(ctx, m, n, X, ldx, scale));
+  if (rowmax)
+    BBT_TRY(crt_scales_from_max(ctx, m, rowmax, scale));
+  else
+    BBT_TRY(crt_row_scales(ctx, m, n, X, ldx, scale));
   ctx->ws.top = m3;
   uint8_t* Rb = ctx->ws.take<uint8_t>(gram_product_bytes(ctx, m, n, nm, kc, nullptr));
   if (!Rb || !RX) return fail(ctx, BBT_ERR_NOMEM, "exact Gram: workspace");
@@ -187,16 +190,19 @@ bbt_status exact_local_qr(bbt_ctx* ctx, int m, long n, const double* X, const vo
   double* Th = ctx->ws.take<double>((size_t)m * m);
   double* Tl = ctx->ws.take<double>((size_t)m * m);
   double* dsig = ctx->ws.take<double>(m);
-  if (!dsig) return fail(ctx, BBT_ERR_NOMEM, "exact local QR: workspace");
+  unsigned long long* rowmax = ctx->ws.take<unsigned long long>(m);
+  if (!rowmax) return fail(ctx, BBT_ERR_NOMEM, "exact local QR: workspace");
   int* flag = ctx->d_flag + FLAG_CHOL;
-  // 1. the preconditioner from the sketch
-  BBT_TRY(sketch_bf16x3(ctx, m, n, X, n, N, S, spitch, Y));
+  // 1. the preconditioner from the sketch (its pass over X also forms the row
+  //    maxima of the Gram's scales)
+  BBT_CUDA(ctx, cudaMemsetAsync(rowmax, 0, (size_t)m * 8, ctx->stream));
+  BBT_TRY(sketch_bf16x3(ctx, m, n, X, n, N, S, spitch, Y, rowmax));
   BBT_TRY(dgemm(ctx, true, false, m, m, N, 1.0, Y, N, Y, N, 0.0, Rp, m, 0, true));
   BBT_TRY(symmetrize_upper(ctx, m, Rp, m));
   BBT_TRY(shift_diag(ctx, m, Rp, m, 1e-14));
   BBT_TRY(potrf_upper(ctx, m, Rp, m, flag));
   // 2. the exact Gram of the 53-bit rows of X, as a double-double
-  BBT_TRY(exact_gram_dd(ctx, m, n, X, n, scale, keep, Gh, Gl));
+  BBT_TRY(exact_gram_dd(ctx, m, n, X, n, scale, keep, Gh, Gl, rowmax));
   BBT_TRY(dd_symmetrize_upper(ctx, m, Gh, Gl, m));
   // 3. G_Q = R_p^-T (R_p^-T G)^T in double-double (G symmetric)
   BBT_TRY(dd_trsm_left(ctx, true, m, m, Rp, m, Gh, Gl, m));

@@ -270,8 +270,10 @@ long sketch_pitch(long n);
 int sketch_rows(int m);   // N used by the mixed local QR: 2m rounded up to 128
 size_t sketch_workspace_bytes(const bbt_ctx* ctx, int m, long n, int N);
 bbt_status rademacher(bbt_ctx* ctx, int N, long n, void* S, uint64_t seed);
+// rowmax (optional, zeroed by the caller): each row's max |X| as its FP64 bit
+// pattern, from the same pass over X (the CRT row scales of X need them).
 bbt_status sketch_bf16x3(bbt_ctx* ctx, int m, long n, const double* X, long ldx, int N, const void* S,
-                         long spitch, double* Y);
+                         long spitch, double* Y, unsigned long long* rowmax = nullptr);
 
 // FP64 Cholesky / triangular solve (chol.cu), column-major.
 // A (rows x n) <- A R^{-1}, R upper n x n.
@@ -310,6 +312,8 @@ bbt_status gemm_oz(bbt_ctx* ctx, int M, int N, long K, double alpha, const doubl
 long crt_pitch(long K);
 int crt_moduli(int bits_a, int bits_b, long K);   // moduli for an exact product; -1 if too many
 bbt_status crt_row_scales(bbt_ctx* ctx, int rows, long K, const double* X, long rs, double* scale);
+// The same scales from row maxima already formed (max |x| as FP64 bit patterns).
+bbt_status crt_scales_from_max(bbt_ctx* ctx, int rows, const unsigned long long* mx, double* scale);
 bbt_status crt_residues_rows(bbt_ctx* ctx, int rows, long K, const double* X, long rs, const double* scale, int b,
                              int n, int8_t* planes, long Kp);
 // X(i, k) = X[i + k cs] with the scale of K index k (the transposed layout of
@@ -361,10 +365,10 @@ int exact_keep_moduli(int m, long n);
 size_t exact_keep_bytes(int m, long n);
 // The exact Gram of X's 53-bit rows as a double-double (upper triangle, ld m),
 // the row scales written to scale; keep: residue planes to fill and keep (or
-// null: chunked scratch planes).
+// null: chunked scratch planes); rowmax: X's row maxima when already formed.
 size_t exact_gram_workspace_bytes(const bbt_ctx* ctx, int m, long n);
 bbt_status exact_gram_dd(bbt_ctx* ctx, int m, long n, const double* X, long ldx, double* scale, int8_t* keep,
-                         double* Gh, double* Gl);
+                         double* Gh, double* Gl, const unsigned long long* rowmax = nullptr);
 bbt_status exact_local_qr(bbt_ctx* ctx, int m, long n, const double* X, const void* S, long spitch, double* R,
                           double* W, double* Rp, double* scale,
                           int8_t* keep = nullptr);

@@ -192,15 +192,20 @@ sketch_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
 }
 
 // X (m x n row-major, ld ldx) -> three bf16 pieces A[p][i][j] (row pitch `pitch`);
-// rows over blockIdx.y, columns over the x grid (no index division).
+// rows over blockIdx.y, columns over the x grid (no index division).  With
+// mx, also each row's max |x| (as its bit pattern: the maximum of
+// non-negative doubles is the maximum of their patterns) by atomicMax, the
+// row maxima the CRT scales of the same X need, from this pass over X.
 __global__ void split3_kernel(int m, long n, const double* __restrict__ X, long ldx, __nv_bfloat16* __restrict__ A,
-                              long pitch) {
+                              long pitch, unsigned long long* __restrict__ mx) {
   const size_t plane = (size_t)m * pitch;
   for (int i = blockIdx.y; i < m; i += gridDim.y) {
     const double* xr = X + (long)i * ldx;
     __nv_bfloat16* ar = A + (size_t)i * pitch;
+    double amax = 0.0;
     for (long j = blockIdx.x * (long)blockDim.x + threadIdx.x; j < n; j += (long)gridDim.x * blockDim.x) {
       const double x = xr[j];
+      amax = fmax(amax, fabs(x));
       const __nv_bfloat16 b0 = __double2bfloat16(x);
       const double r1 = x - (double)__bfloat162float(b0);
       const __nv_bfloat16 b1 = __double2bfloat16(r1);
@@ -209,6 +214,10 @@ __global__ void split3_kernel(int m, long n, const double* __restrict__ X, long 
       ar[j] = b0;
       ar[plane + j] = b1;
       ar[2 * plane + j] = b2;
+    }
+    if (mx) {   // uniform across the block
+      for (int o = 16; o > 0; o >>= 1) amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+      if ((threadIdx.x & 31) == 0) atomicMax(mx + i, (unsigned long long)__double_as_longlong(amax));
     }
   }
 }
@@ -220,28 +229,25 @@ __device__ __forceinline__ uint64_t mix64(uint64_t z) {   // splitmix64 finalise
   return z ^ (z >> 31);
 }
 
-// S (N x n, row pitch `pitch`, a multiple of 8) with independent +-1 entries,
-// entry (i, j) from the hash of i n + j; eight entries per 16-byte store.
+// S (N x n, row pitch `pitch`, a multiple of 8) with independent +-1 entries:
+// the eight entries (i, 8g .. 8g + 7) take their signs from bits 0..7 of one
+// splitmix64 hash of i ceil(n / 8) + g (a set bit gives -1: bf16 0x3F80 with
+// its sign bit set); eight entries per 16-byte store.
 __global__ void rademacher_kernel(int N, long n, long pitch, __nv_bfloat16* __restrict__ S, uint64_t seed) {
-  const uint16_t plus = 0x3F80, minus = 0xBF80;
+  const uint64_t groups = (uint64_t)((n + 7) / 8);
   for (int i = blockIdx.y; i < N; i += gridDim.y) {
     uint16_t* row = reinterpret_cast<uint16_t*>(S) + (size_t)i * pitch;
     for (long j0 = (blockIdx.x * (long)blockDim.x + threadIdx.x) * 8; j0 < n; j0 += (long)gridDim.x * blockDim.x * 8) {
-      uint16_t v[8];
+      const uint64_t g = (uint64_t)i * groups + (uint64_t)(j0 / 8);
+      const uint32_t bits = (uint32_t)mix64(seed ^ g * 0xD1B54A32D192ED03ull);
+      uint32_t w[4];
 #pragma unroll
-      for (int e = 0; e < 8; ++e) {
-        const uint64_t f = (uint64_t)i * (uint64_t)n + (uint64_t)(j0 + e);
-        v[e] = (mix64(seed ^ f * 0xD1B54A32D192ED03ull) & 1u) ? plus : minus;
-      }
+      for (int e = 0; e < 4; ++e)
+        w[e] = 0x3F803F80u | ((bits >> (2 * e)) & 1u) << 15 | ((bits >> (2 * e + 1)) & 1u) << 31;
       if (j0 + 8 <= n && (reinterpret_cast<uintptr_t>(row + j0) & 15) == 0) {
-        uint4 w;
-        w.x = v[0] | ((uint32_t)v[1] << 16);
-        w.y = v[2] | ((uint32_t)v[3] << 16);
-        w.z = v[4] | ((uint32_t)v[5] << 16);
-        w.w = v[6] | ((uint32_t)v[7] << 16);
-        *reinterpret_cast<uint4*>(row + j0) = w;
+        *reinterpret_cast<uint4*>(row + j0) = make_uint4(w[0], w[1], w[2], w[3]);
       } else {
-        for (int e = 0; e < 8 && j0 + e < n; ++e) row[j0 + e] = v[e];
+        for (int e = 0; e < 8 && j0 + e < n; ++e) row[j0 + e] = (uint16_t)(w[e / 2] >> (16 * (e % 2)));
       }
     }
   }
@@ -339,12 +345,13 @@ bbt_status rademacher(bbt_ctx* ctx, int N, long n, void* S, uint64_t seed) {
 }
 
 bbt_status sketch_chunk_run(bbt_ctx* ctx, int m, long n, const double* X, long ldx, int N, const __nv_bfloat16* S,
-                            long spitch, double* Y, __nv_bfloat16* A, double* part, bool accumulate);
+                            long spitch, double* Y, __nv_bfloat16* A, double* part, bool accumulate,
+                            unsigned long long* rowmax);
 
 // Stream-ordered; a pipeline wait that gave up leaves a nonzero code in
 // ctx->d_flag[FLAG_SKETCH] (cleared and read by the caller).
 bbt_status sketch_bf16x3(bbt_ctx* ctx, int m, long n, const double* X, long ldx, int N, const void* S, long spitch,
-                         double* Y) {
+                         double* Y, unsigned long long* rowmax) {
   if (m < 1 || n < 1 || N < TN || N % TN != 0 || n > (1L << 31) - TK || spitch < n || spitch % 8 != 0)
     return fail(ctx, BBT_ERR_ARG, "sketch: m=%d n=%ld N=%d", m, n, N);
   EncodeTiled enc = encode_fn();
@@ -357,20 +364,22 @@ bbt_status sketch_bf16x3(bbt_ctx* ctx, int m, long n, const double* X, long ldx,
   if (!part) return fail(ctx, BBT_ERR_NOMEM, "sketch: workspace");
   for (long k0 = 0; k0 < n; k0 += kc)   // chunk offsets are multiples of 2^15: 16-byte TMA bases in S
     BBT_TRY(sketch_chunk_run(ctx, m, std::min(kc, n - k0), X + k0, ldx, N,
-                             static_cast<const __nv_bfloat16*>(S) + k0, spitch, Y, A, part, k0 > 0));
+                             static_cast<const __nv_bfloat16*>(S) + k0, spitch, Y, A, part, k0 > 0, rowmax));
   ctx->ws.top = mark;
   return BBT_OK;
 }
 
 // One K-chunk of sketch_bf16x3: its bf16 pieces in A (pitch sketch_pitch(n)),
-// the products of its K-splits in part, summed into Y (added with accumulate).
+// the products of its K-splits in part, summed into Y (added with accumulate);
+// the chunk's row maxima of |X| merged into rowmax (when given).
 bbt_status sketch_chunk_run(bbt_ctx* ctx, int m, long n, const double* X, long ldx, int N, const __nv_bfloat16* S,
-                            long spitch, double* Y, __nv_bfloat16* A, double* part, bool accumulate) {
+                            long spitch, double* Y, __nv_bfloat16* A, double* part, bool accumulate,
+                            unsigned long long* rowmax) {
   EncodeTiled enc = encode_fn();
   const long pitch = sketch_pitch(n);
   const Split sp = plan_split(m, n, N, ctx->num_sms);
   split3_kernel<<<dim3((unsigned)std::max(1L, std::min((n + 255) / 256, 16L)), (unsigned)std::min(m, 65535)), 256, 0,
-                  ctx->stream>>>(m, n, X, ldx, A, pitch);
+                  ctx->stream>>>(m, n, X, ldx, A, pitch, rowmax);
   BBT_LAUNCHED(ctx);
 
   CUtensorMap ta, tb;

@@ -2,7 +2,8 @@
 checked on the CPU from the same moduli list and the same formulas for their
 constants: the moduli are pairwise coprime bytes, the multiply-high
 quotients are exact over the ranges the kernels feed them, the residues of
-53-bit integers formed from 18-bit pieces stay in range, the epilogue's
+53-bit integers formed from the bytes of their offset FP64 bit patterns are
+exact and stay in range, the epilogue's
 reduction of an int32 accumulator is the residue, the modulus count covers
 every product, and the fixed-point reconstruction recovers the integer."""
 import math
@@ -50,32 +51,39 @@ def test_multiply_high_quotients_are_exact(p):
     magic32 = -(-(1 << 32) // p)
     x = np.arange(1 << 24, dtype=np.uint64)
     assert np.array_equal((x * np.uint64(magic32)) >> np.uint64(32), x // np.uint64(p))
-    # magic35 = ceil(2^35 / p) for x < 2^27: x (magic35 p - 2^35) < 2^35 is the
-    # exactness condition; checked at its worst case, and on random x
-    magic35 = -(-(1 << 35) // p)
-    assert ((1 << 27) - 1) * (magic35 * p - (1 << 35)) < (1 << 35)
-    rng = np.random.default_rng(p)
-    xs = rng.integers(0, 1 << 27, 1 << 20, dtype=np.uint64)
-    assert np.array_equal(((xs * np.uint64(magic35)) >> np.uint64(32)) >> np.uint64(3), xs // np.uint64(p))
+
+
+def dp4a(a, b, c):
+    """Unsigned byte dot product of two 32-bit words plus c."""
+    return c + sum(((a >> (8 * j)) & 255) * ((b >> (8 * j)) & 255) for j in range(4))
 
 
 @pytest.mark.parametrize("p", MOD)
-def test_residues_from_pieces_stay_in_range(p):
-    """t = a 2^36 + b 2^18 + c (a = floor(t / 2^36), 0 <= b, c < 2^18) for
-    |t| <= 2^51, the 53-bit integers of the products: x = a c36 + b c18 + c +
-    off lies in [0, 2^27), and x mod p is t mod p."""
-    c36, c18 = (1 << 36) % p, (1 << 18) % p
-    off = p * (((1 << 23) + p - 1) // p)
-    lo = -(1 << 15) * c36 + off
-    hi = (1 << 15) * c36 + ((1 << 18) - 1) * (c18 + 1) + off
-    assert 0 <= lo and hi < (1 << 27)
+def test_residues_from_offset_bytes(p):
+    """residues_rows/cols: t (an integer, |t| <= 2^51) + 1.5 2^52 is exact in
+    FP64; its low word and its high word less 0x43300000 are the two words
+    of u = t + 2^51 (also at t = 2^51, where y = 2^53); x = dp4a(lo, W0,
+    dp4a(hi, W1, off)) with the byte weights 256^j mod p and off = -2^51 mod
+    p in [1, p] lies in (0, 2^19) and is t mod p; the multiply-high quotient
+    by ceil(2^32 / p) then gives the residue."""
+    w = [(1 << (8 * j)) % p for j in range(7)]
+    W0 = w[0] | w[1] << 8 | w[2] << 16 | w[3] << 24
+    W1 = w[4] | w[5] << 8 | w[6] << 16
+    off = p - (1 << 51) % p
+    magic32 = -(-(1 << 32) // p)
+    assert 1 <= off <= p
     rng = np.random.default_rng(p + 1)
-    for t in [-(1 << 51), (1 << 51), 0, -1, 1, *[int(v) for v in rng.integers(-(1 << 51), 1 << 51, 2000)]]:
-        a, rem = divmod(t, 1 << 36)
-        b, c = divmod(rem, 1 << 18)
-        x = a * c36 + b * c18 + c + off
-        assert 0 <= x < (1 << 27)
-        assert x % p == t % p
+    ts = [-(1 << 51), (1 << 51), (1 << 51) - 1, -(1 << 51) + 1, 0, -1, 1,
+          *[int(v) for v in rng.integers(-(1 << 51), 1 << 51, 3000)]]
+    y = np.array(ts, dtype=np.float64) + np.float64(1.5 * 2.0 ** 52)
+    bits = y.view(np.uint64)
+    for t, b in zip(ts, bits):
+        lo, hi = int(b) & 0xFFFFFFFF, ((int(b) >> 32) - 0x43300000) & 0xFFFFFFFF
+        u = t + (1 << 51)
+        assert lo == u & 0xFFFFFFFF and hi == u >> 32 and hi <= 1 << 20
+        x = dp4a(lo, W0, dp4a(hi, W1, off))
+        assert 0 < x < (1 << 19)
+        assert x - ((x * magic32) >> 32) * p == t % p
 
 
 @pytest.mark.parametrize("p", MOD)
