@@ -6,12 +6,13 @@
 // The masks draw their random tables on the host with the same calls as the
 // reference, so glibc's rand() state after a call is the reference's.
 //
-// Functions the reference declares but never calls from client.cpp with
-// opt_control 1/3 (the unused mask variants and the opt_control 0/2 dense
-// masks) abort with a message instead of silently computing on the CPU.  The
-// random orthogonal matrix generators run the reference's LAPACK calls
-// through the LAPACK the process links (they are random-number generation,
-// not arithmetic this library accelerates).
+// The masks off the opt_control 1/3 path (the dense masks of opt_control
+// 0/2 and the variants the reference declares but never calls) run on the
+// GPU as well; where a size is outside what they provide they abort with a
+// message instead of computing on the CPU.  The random orthogonal matrix
+// generators run the reference's LAPACK calls through the LAPACK the process
+// links (they are random-number generation, not arithmetic this library
+// accelerates).
 #include <cuda_runtime.h>
 
 #include <dlfcn.h>
@@ -47,14 +48,6 @@ bbt_ctx* ctx() {
 [[noreturn]] void die(const char* what, bbt_status s) {
   fprintf(stderr, "libexcalibur_b200: %s failed: %s (%s)\n", what, bbt_status_string(s),
           g_ctx ? bbt_last_error(g_ctx) : "");
-  abort();
-}
-
-[[noreturn]] void not_provided(const char* fn) {
-  fprintf(stderr,
-          "libexcalibur_b200: %s is not provided (declared by bbtsvd.hpp but not on the path "
-          "DecentralizedClient::run() takes with opt_control 1/3)\n",
-          fn);
   abort();
 }
 
@@ -394,17 +387,6 @@ void mmap_drot(size_t n, double* x, size_t incX, double* y, size_t incY, double 
   dy.back(y, sy);
 }
 
-// ---- declared by bbtsvd.hpp, not on the run() path (see file comment) ----
-void house_mask(size_t, size_t, size_t, double*, bool, bool, unsigned int) { not_provided("house_mask"); }
-void householder_reflector_mask(size_t, size_t, size_t, double*, bool, bool, unsigned int) {
-  not_provided("householder_reflector_mask");
-}
-void naive_givens_mask_parallel(size_t, size_t, size_t, double*, bool, bool, unsigned int) {
-  not_provided("naive_givens_mask_parallel");
-}
-void givens_mask_cache_optimized_parallel(size_t, size_t, size_t, double*, bool, bool, unsigned int) {
-  not_provided("givens_mask_cache_optimized_parallel");
-}
 
 // ---- random orthogonal matrices (bbtsvd.cpp:301-331, 370-395) -------------
 // Normal random entries from LAPACK's dlarnv (seeded from rand(), as the
@@ -503,7 +485,10 @@ __global__ void swap_lines_kernel(int npairs, const int2* __restrict__ pr, size_
 }
 }  // namespace
 
-void shuffle_matrix(size_t m, size_t n, double* x, unsigned int seed, bool is_left, bool unshuffle) {
+namespace {
+// The swaps of shuffle_matrix on a device copy of x (the draws on the host,
+// made even when x is empty, as the reference makes them).
+void shuffle_dev(size_t m, size_t n, double* dx, unsigned int seed, bool is_left, bool unshuffle) {
   srand(seed);
   auto dre = std::default_random_engine(seed);
   const size_t k = is_left ? m : n;
@@ -518,7 +503,6 @@ void shuffle_matrix(size_t m, size_t n, double* x, unsigned int seed, bool is_le
   if (k % 2 != 0 && !unshuffle) last.push_back(make_int2((int)(k - 1), (int)ri));
   if (m == 0 || n == 0) return;
   bbt_ctx* c = ctx();
-  Dev dx(x, m * n);
   const size_t len = is_left ? n : m, lstride = is_left ? n : 1, estride = is_left ? 1 : n;
   for (const auto* v : {&first, &pairs, &last}) {
     if (v->empty()) continue;
@@ -528,14 +512,352 @@ void shuffle_matrix(size_t m, size_t n, double* x, unsigned int seed, bool is_le
       die("cudaMemcpyAsync", BBT_ERR_CUDA);
     const long work = (long)v->size() * (long)len;
     const unsigned g = (unsigned)std::min<long>((work + 255) / 256, 8L * c->num_sms);
-    swap_lines_kernel<<<g, 256, 0, c->stream>>>((int)v->size(), dp, len, lstride, estride, dx.p);
+    swap_lines_kernel<<<g, 256, 0, c->stream>>>((int)v->size(), dp, len, lstride, estride, dx);
     launched(c, "shuffle_matrix");
     sync(c, "shuffle_matrix");
     cudaFree(dp);
   }
+}
+}  // namespace
+
+void shuffle_matrix(size_t m, size_t n, double* x, unsigned int seed, bool is_left, bool unshuffle) {
+  if (m == 0 || n == 0) {
+    shuffle_dev(m, n, nullptr, seed, is_left, unshuffle);   // the draws only
+    return;
+  }
+  ctx();
+  Dev dx(x, m * n);
+  shuffle_dev(m, n, dx.p, seed, is_left, unshuffle);
   dx.back(x, m * n);
 }
-void block_mask(size_t, size_t, size_t, double*, bool, bool, unsigned int) { not_provided("block_mask"); }
-void shuffle_block_mask(size_t, size_t, size_t, int, double*, bool, bool, unsigned int) {
-  not_provided("shuffle_block_mask");
+
+// ---- the other masks of bbtsvd.hpp (bbtsvd.cpp:190-299, 429-531, 670-726) ----
+// Not on the path DecentralizedClient::run() takes with opt_control 1/3
+// (client.cpp calls block_mask for opt_control 0/2; the rest are declared
+// only).  Their random tables and reflectors are drawn on the host with the
+// reference's own calls in the reference's order, so glibc's rand() state
+// afterwards is the reference's; every application to x runs on the GPU.
+// The Givens variants rotate with the strip kernel of the mask path, each
+// product and sum rounded on its own, as the reference's scalar loops do.
+// The Householder variants form the orthogonal factor Q = H_0 ... H_{k-1}
+// explicitly on the GPU (the blocked reflector application to an identity)
+// and multiply by it (FP64 GEMM), where the reference applies the
+// reflectors with LAPACK's dormqr: the same Q to rounding.
+namespace {
+
+template <class T>
+struct DevArr {   // device copy of a host array of T (freed at scope end)
+  T* p = nullptr;
+  explicit DevArr(const std::vector<T>& h) {
+    if (cudaMalloc(&p, (h.empty() ? 1 : h.size()) * sizeof(T)) != cudaSuccess) die("cudaMalloc", BBT_ERR_NOMEM);
+    if (!h.empty() &&
+        cudaMemcpyAsync(p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, g_ctx->stream) != cudaSuccess)
+      die("cudaMemcpyAsync", BBT_ERR_CUDA);
+  }
+  ~DevArr() { cudaFree(p); }
+};
+
+void ensure_ws(bbt_ctx* c, size_t bytes, const char* what) {
+  c->ws.reset();
+  if (c->ws.cap < bytes && c->ws.reserve(bytes) != cudaSuccess) die(what, BBT_ERR_NOMEM);
+}
+
+// Rotations of a Givens mask drawn on the host, applied on the GPU: passes of
+// disjoint pairs (one stage each), (c, s) with s already signed.
+void rotate_dev(size_t m, size_t n, double* dx, bool is_left, size_t k, size_t passes, size_t ops,
+                const std::vector<int2>& pairs, const std::vector<double2>& cs, const char* what) {
+  if (k > 10000) {
+    fprintf(stderr, "libexcalibur_b200: %s: rotated dimensions above 10,000 are not provided\n", what);
+    abort();
+  }
+  bbt_ctx* c = ctx();
+  DevArr<int2> dp(pairs);
+  DevArr<double2> dc(cs);
+  bbt::GivensDev T{k, passes, ops, 0, (int)ops, dp.p, dc.p};
+  bbt_status s = bbt::apply_givens(c, T, m, n, dx, is_left);
+  if (s == BBT_OK) s = bbt_synchronize(c);
+  if (s != BBT_OK) die(what, s);
+}
+
+// (c, s) normalised as the reference does: c / |(c, s)|, s / |(c, s)|.
+void normalise_cs(std::vector<double>& c, std::vector<double>& s) {
+  for (size_t i = 0; i < c.size(); ++i) {
+    const double r = pow(pow(c[i], 2) + pow(s[i], 2), 0.5);
+    c[i] /= r;
+    s[i] /= r;
+  }
+}
+
+double random_value_pm1() { return (rand() / (double)RAND_MAX) * 2.0 + -1.0; }   // utils.hpp random_value(-1, 1)
+
+// Q (k x k, column-major, device) = H_0 ... H_{nref-1}: reflector j is column
+// j of V from row j down (unit diagonal implied), V(r, c) at V[r*rs + c*cs].
+void form_q(bbt_ctx* c, int k, int nref, const double* dV, long rs, long cs, const double* dtau, double* dQ,
+            const char* what) {
+  bbt_status s = bbt::identity(c, k, dQ, k);
+  if (s == BBT_OK && nref > 0) {
+    bbt::QrPlan plan;
+    ensure_ws(c, bbt::qr_workspace_bytes(k, nref, k, plan) + (1 << 20), what);
+    s = bbt::ormqr_left_notrans(c, k, nref, dV, rs, cs, dtau, dQ, k, k, false, plan);
+  }
+  if (s == BBT_OK) s = bbt_synchronize(c);
+  if (s != BBT_OK) die(what, s);
+}
+
+// X (r x cc, column-major, ld) <- op(Q) X (left, Q r x r) or X op(Q) (right,
+// Q cc x cc), op(Q) = Q^T when trans; dT holds r*cc doubles of scratch.
+void apply_q(bbt_ctx* c, bool left, bool trans, int r, int cc, const double* dQ, double* dX, long ld, double* dT,
+             const char* what) {
+  if (r < 1 || cc < 1) return;
+  ensure_ws(c, bbt::dgemm_workspace_bytes(c, r, cc, left ? r : cc) + (1 << 20), what);
+  bbt_status s = bbt::copy2d(c, cc, r, dX, ld, dT, r);   // cc columns of r contiguous entries
+  if (s == BBT_OK)
+    s = left ? bbt::dgemm(c, trans, false, r, cc, r, 1.0, dQ, r, dT, r, 0.0, dX, ld)
+             : bbt::dgemm(c, false, trans, r, cc, cc, 1.0, dT, r, dQ, cc, 0.0, dX, ld);
+  if (s == BBT_OK) s = bbt_synchronize(c);
+  if (s != BBT_OK) die(what, s);
+}
+
+// x (m x n row-major, on the device) <- the blocks of the reference's
+// block_mask / shuffle_block_mask step: per diagonal block of `bs` rows
+// (is_left) or columns, the random orthogonal Q of the block's size from
+// generate_random_orthogonal_matrix(row-major, size, seed) (every block
+// draws from srand(seed) again), applied as op(Q) x_block (is_left) or
+// x_block op(Q), op(Q) = Q for mask and Q^T otherwise.  The last of the
+// block's reflectors is the identity: the reference reads its tau one past
+// the tau array (a zeroed or negligible value); here it is left out.  With
+// dx null only the draws are made (the reference's rand() calls on an empty x).
+void block_orthogonal_dev(size_t m, size_t n, size_t bs, double* dx, bool mask, bool is_left, unsigned seed,
+                          const char* what) {
+  bbt_ctx* c = dx ? ctx() : nullptr;
+  const size_t k = is_left ? m : n;
+  std::vector<double> house, tau;
+  size_t formed = 0;   // block size of the Q in dQ
+  double* dQ = nullptr;
+  double* dT = nullptr;
+  for (size_t i = 0; i < k; i += bs) {
+    const size_t rb = std::min(bs, k - i);
+    house.assign(rb * rb, 0.0);
+    tau.assign(rb > 1 ? rb - 1 : 1, 0.0);
+    generate_random_orthogonal_matrix(ROW_MAJOR, rb, house.data(), tau.data(), seed);
+    if (!dx) continue;   // an empty x: the draws only
+    if (rb != formed) {
+      cudaFree(dQ);
+      cudaFree(dT);
+      dQ = dT = nullptr;
+      if (cudaMalloc(&dQ, rb * rb * sizeof(double)) != cudaSuccess ||
+          cudaMalloc(&dT, rb * (is_left ? n : m) * sizeof(double)) != cudaSuccess)
+        die(what, BBT_ERR_NOMEM);
+      DevArr<double> dV(house), dtau(tau);
+      form_q(c, (int)rb, (int)rb - 1, dV.p, (long)rb, 1, dtau.p, dQ, what);
+      formed = rb;
+    }
+    // row-major x is the column-major n x m matrix x^T (ld n)
+    if (is_left)   // x_block (rb x n) <- op(Q) x_block  <=>  x_block^T <- x_block^T op(Q)^T
+      apply_q(c, false, mask, (int)n, (int)rb, dQ, dx + i * n, (long)n, dT, what);
+    else           // x_block (m x rb) <- x_block op(Q)  <=>  x_block^T <- op(Q)^T x_block^T
+      apply_q(c, true, mask, (int)rb, (int)m, dQ, dx + i, (long)n, dT, what);
+  }
+  cudaFree(dQ);
+  cudaFree(dT);
+}
+
+}  // namespace
+
+// bbtsvd.cpp:190-226.  The permutation is shuffled again for every pass
+// (each pass starts from the previous one's order); pairs rotate as BLAS drot
+// (x, y) <- (c x + s y, c y - s x), s negated when unmasking, which takes
+// the passes in reverse order but their (c, s) in the forward order.
+void naive_givens_mask_parallel(size_t m, size_t n, size_t mask_size, double* x, bool mask, bool is_left,
+                                unsigned int seed) {
+  srand(seed);
+  auto dre = std::default_random_engine(seed);
+  const int k = (int)(is_left ? m : n);
+  std::vector<std::vector<int>> pmi;
+  std::vector<int> tmp;
+  for (int i = 0; i < k; ++i) tmp.push_back(i);
+  for (int i = 0; i < (int)mask_size; ++i) {
+    std::shuffle(tmp.begin(), tmp.end(), dre);
+    pmi.push_back(tmp);
+  }
+  const int ops = (k - (k % 2)) / 2;
+  const size_t cs_size = mask_size * (size_t)ops;
+  std::vector<double> cc(cs_size), ss(cs_size);
+  for (auto& v : cc) v = random_value_pm1();
+  for (auto& v : ss) v = random_value_pm1();
+  normalise_cs(cc, ss);
+  if (ops == 0 || mask_size == 0 || m == 0 || n == 0) return;
+  std::vector<int2> pairs(cs_size);
+  std::vector<double2> cs(cs_size);
+  const double sg = mask ? 1.0 : -1.0;
+  for (size_t i = 0; i < mask_size; ++i) {
+    const size_t pi = mask ? i : mask_size - 1 - i;
+    for (int j = 0; j < ops; ++j) {
+      pairs[i * ops + j] = make_int2(pmi[pi][2 * j], pmi[pi][2 * j + 1]);
+      cs[i * ops + j] = make_double2(cc[i * ops + j], sg * ss[i * ops + j]);
+    }
+  }
+  ctx();
+  Dev dx(x, m * n);
+  rotate_dev(m, n, dx.p, is_left, (size_t)k, mask_size, (size_t)ops, pairs, cs, "naive_givens_mask_parallel");
+  dx.back(x, m * n);
+}
+
+// bbtsvd.cpp:228-299.  A fresh shuffle per pass; pairs ordered (low, high);
+// unmasking reverses the passes and their (c, s) together.
+void givens_mask_cache_optimized_parallel(size_t m, size_t n, size_t mask_times, double* x, bool mask,
+                                          bool is_left, unsigned int seed) {
+  srand(seed);
+  auto dre = std::default_random_engine(seed);
+  const int k = (int)(is_left ? m : n);
+  std::vector<std::vector<int>> pmi;
+  for (int i = 0; i < (int)mask_times; ++i) {
+    std::vector<int> t;
+    for (int j = 0; j < k; ++j) t.push_back(j);
+    std::shuffle(t.begin(), t.end(), dre);
+    pmi.push_back(t);
+  }
+  if (!mask) std::reverse(pmi.begin(), pmi.end());
+  const int ops = (k - (k % 2)) / 2;
+  const size_t cs_size = mask_times * (size_t)ops;
+  std::vector<double> cc(cs_size), ss(cs_size);
+  for (auto& v : cc) v = random_value_pm1();
+  for (auto& v : ss) v = random_value_pm1();
+  normalise_cs(cc, ss);
+  if (ops == 0 || mask_times == 0 || m == 0 || n == 0) return;
+  std::vector<int2> pairs(cs_size);
+  std::vector<double2> cs(cs_size);
+  const double sg = mask ? 1.0 : -1.0;
+  for (size_t i = 0; i < mask_times; ++i) {
+    const size_t ci = mask ? i : mask_times - 1 - i;
+    for (int j = 0; j < ops; ++j) {
+      const int a = pmi[i][2 * j], b = pmi[i][2 * j + 1];
+      pairs[i * ops + j] = make_int2(std::min(a, b), std::max(a, b));
+      cs[i * ops + j] = make_double2(cc[ci * ops + j], sg * ss[ci * ops + j]);
+    }
+  }
+  ctx();
+  Dev dx(x, m * n);
+  rotate_dev(m, n, dx.p, is_left, (size_t)k, mask_times, (size_t)ops, pairs, cs,
+             "givens_mask_cache_optimized_parallel");
+  dx.back(x, m * n);
+}
+
+// bbtsvd.cpp:429-487 (blocks below 10,000; the reference's batched branch
+// for larger blocks is not provided).
+void block_mask(size_t m, size_t n, size_t block_size, double* x, bool mask, bool is_left, unsigned int seed) {
+  if ((is_left && m <= 1) || (!is_left && n <= 1)) return;
+  if (block_size == 0 || std::min(block_size, is_left ? m : n) >= 10000) {
+    fprintf(stderr, "libexcalibur_b200: block_mask: block size %zu is not provided (1 .. 9,999)\n", block_size);
+    abort();
+  }
+  if (m == 0 || n == 0) {
+    block_orthogonal_dev(m, n, block_size, nullptr, mask, is_left, seed, "block_mask");
+    return;
+  }
+  ctx();
+  Dev dx(x, m * n);
+  block_orthogonal_dev(m, n, block_size, dx.p, mask, is_left, seed, "block_mask");
+  dx.back(x, m * n);
+}
+
+// bbtsvd.cpp:489-531: per round a shuffle (before the blocks when masking,
+// after them when unmasking) and the block step with that round's seed.
+void shuffle_block_mask(size_t m, size_t n, size_t block_size, int shuffle_times, double* x, bool mask,
+                        bool is_left, unsigned int seed) {
+  srand(seed);
+  std::vector<unsigned int> shuffle_seed, mask_seed;
+  for (int st = 0; st < shuffle_times; ++st) {
+    shuffle_seed.push_back(rand());
+    mask_seed.push_back(rand());
+  }
+  if (!mask) {
+    std::reverse(shuffle_seed.begin(), shuffle_seed.end());
+    std::reverse(mask_seed.begin(), mask_seed.end());
+  }
+  if (shuffle_times > 0 && block_size == 0) {
+    fprintf(stderr, "libexcalibur_b200: shuffle_block_mask: block size 0\n");
+    abort();
+  }
+  ctx();
+  Dev dx(x, m * n);
+  for (int st = 0; st < shuffle_times; ++st) {
+    if (mask) shuffle_dev(m, n, m * n ? dx.p : nullptr, shuffle_seed[st], is_left, true);
+    srand(mask_seed[st]);
+    block_orthogonal_dev(m, n, block_size, m * n ? dx.p : nullptr, mask, is_left, mask_seed[st], "shuffle_block_mask");
+    if (!mask) shuffle_dev(m, n, m * n ? dx.p : nullptr, shuffle_seed[st], is_left, false);
+  }
+  dx.back(x, m * n);
+}
+
+// bbtsvd.cpp:670-694: Q from the QR of a normal random mask_size x k matrix
+// (column-major k x mask_size), applied to x as a column-major m x n matrix
+// (ld m) from the left (Q m x m) or the right (Q n x n); op(Q) = Q when
+// is_left equals mask, else Q^T.  The QR runs on the GPU (the library's
+// Householder QR, LAPACK's sign convention).
+void house_mask(size_t m, size_t n, size_t mask_size, double* x, bool mask, bool is_left, unsigned int seed) {
+  const auto dlarnv = (dlarnv_fn)lapack_symbol("LAPACKE_dlarnv", "house_mask");
+  srand(seed);
+  const size_t k = is_left ? m : n;
+  if (mask_size > k) {
+    fprintf(stderr, "libexcalibur_b200: house_mask: mask size %zu above the masked dimension %zu\n", mask_size, k);
+    abort();
+  }
+  std::vector<double> house(k * mask_size);
+  int iseed[4];
+  for (size_t i = 0; i < mask_size; ++i) {   // utils.cpp random_normal_matrix(house, mask_size, k)
+    random_seed4(iseed);
+    dlarnv(3, iseed, (int)k, house.data() + i * k);
+  }
+  if (mask_size == 0 || m == 0 || n == 0) return;
+  bbt_ctx* c = ctx();
+  Dev dx(x, m * n), dQ(nullptr, k * k), dT(nullptr, m * n), dtau(nullptr, mask_size);
+  DevArr<double> dA(house);
+  bbt::QrPlan plan;
+  const size_t tb = (size_t)((mask_size + plan.nb - 1) / plan.nb) * plan.nb * plan.nb;
+  Dev dTf(nullptr, tb);
+  ensure_ws(c, bbt::qr_workspace_bytes((long)k, (int)mask_size, (int)mask_size, plan) + (1 << 20), "house_mask");
+  bbt_status s = bbt::geqrf(c, (long)k, (int)mask_size, dA.p, (long)k, dtau.p, dTf.p, plan);
+  if (s == BBT_OK) s = bbt_synchronize(c);
+  if (s != BBT_OK) die("house_mask", s);
+  form_q(c, (int)k, (int)mask_size, dA.p, 1, (long)k, dtau.p, dQ.p, "house_mask");
+  const bool trans = is_left != mask;
+  apply_q(c, is_left, trans, (int)m, (int)n, dQ.p, dx.p, (long)m, dT.p, "house_mask");
+  dx.back(x, m * n);
+}
+
+// bbtsvd.cpp:696-726: mask_size reflectors with uniform random entries below
+// a unit head, tau = 2 / ||v||^2 (the process's BLAS dnrm2, as the
+// reference); x is column-major m x n when m >= n (Q on the side of is_left)
+// and column-major n x m otherwise (Q on the other side).
+void householder_reflector_mask(size_t m, size_t n, size_t mask_size, double* x, bool mask, bool is_left,
+                                unsigned int seed) {
+  using dnrm2_fn = double (*)(int, const double*, int);
+  srand(seed);
+  const size_t k = is_left ? m : n;
+  if (mask_size > k) {
+    fprintf(stderr, "libexcalibur_b200: householder_reflector_mask: mask size %zu above the masked dimension %zu\n",
+            mask_size, k);
+    abort();
+  }
+  std::vector<double> house(k * mask_size, 0.0), tau(mask_size, 0.0);
+  if (mask_size > 0) {
+    const auto dnrm2 = (dnrm2_fn)lapack_symbol("cblas_dnrm2", "householder_reflector_mask");
+    for (size_t i = 0; i < mask_size; ++i) {
+      house[i * k + i] = 1.0;
+      for (size_t j = 0; j + i + 1 < k; ++j) house[i * k + i + 1 + j] = random_value_pm1();
+      tau[i] = 2 / pow(dnrm2((int)(k - i), house.data() + i * k + i, 1), 2);
+    }
+  }
+  if (mask_size == 0 || m == 0 || n == 0) return;
+  bbt_ctx* c = ctx();
+  Dev dx(x, m * n), dQ(nullptr, k * k), dT(nullptr, m * n);
+  DevArr<double> dV(house), dtau(tau);
+  form_q(c, (int)k, (int)mask_size, dV.p, 1, (long)k, dtau.p, dQ.p, "householder_reflector_mask");
+  if (m >= n)   // Q on the is_left side of the column-major m x n x
+    apply_q(c, is_left, is_left != mask, (int)m, (int)n, dQ.p, dx.p, (long)m, dT.p, "householder_reflector_mask");
+  else          // Q on the other side of the column-major n x m x
+    apply_q(c, !is_left, is_left == mask, (int)n, (int)m, dQ.p, dx.p, (long)n, dT.p,
+            "householder_reflector_mask");
+  dx.back(x, m * n);
 }

@@ -52,6 +52,25 @@ void ref_random_orthogonal(size_t m, size_t n, double* x, unsigned seed) {
 void ref_shuffle_matrix(size_t m, size_t n, double* x, unsigned seed, int is_left, int unshuffle) {
   shuffle_matrix(m, n, x, seed, is_left != 0, unshuffle != 0);
 }
+void ref_naive_givens(size_t m, size_t n, size_t t, double* x, int mask, int is_left, unsigned seed) {
+  naive_givens_mask_parallel(m, n, t, x, mask != 0, is_left != 0, seed);
+}
+void ref_givens_cached(size_t m, size_t n, size_t t, double* x, int mask, int is_left, unsigned seed) {
+  givens_mask_cache_optimized_parallel(m, n, t, x, mask != 0, is_left != 0, seed);
+}
+void ref_block_mask(size_t m, size_t n, size_t bs, double* x, int mask, int is_left, unsigned seed) {
+  block_mask(m, n, bs, x, mask != 0, is_left != 0, seed);
+}
+void ref_shuffle_block_mask(size_t m, size_t n, size_t bs, int times, double* x, int mask, int is_left,
+                            unsigned seed) {
+  shuffle_block_mask(m, n, bs, times, x, mask != 0, is_left != 0, seed);
+}
+void ref_house_mask(size_t m, size_t n, size_t k, double* x, int mask, int is_left, unsigned seed) {
+  house_mask(m, n, k, x, mask != 0, is_left != 0, seed);
+}
+void ref_householder_reflector_mask(size_t m, size_t n, size_t k, double* x, int mask, int is_left, unsigned seed) {
+  householder_reflector_mask(m, n, k, x, mask != 0, is_left != 0, seed);
+}
 int ref_rand() { return rand(); }
 void ref_set_threads(int n) { omp_set_num_threads(n); mkl_set_num_threads(n); }
 }

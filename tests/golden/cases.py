@@ -148,3 +148,29 @@ def step_cases():
 # shuffle_matrix (make_golden.py generator_fixtures): name -> its test.
 GENERATOR_FIXTURES = ("house_row7", "house_col6", "orth_tall9x4", "orth_wide4x9", "shuffle_left7x5",
                       "unshuffle_left7x5", "shuffle_right6x9", "unshuffle_right6x9", "shuffle_left8x3")
+
+
+# The other masks of bbtsvd.hpp (make_golden.py other_mask_fixtures): name ->
+# (function, m, n, size, rounds, mask, is_left, seed); size is the pass count,
+# block size or reflector count, rounds the shuffle_block_mask rounds.  The
+# block masks' cases use one block smaller than the block size: a full block
+# makes the reference read its tau array one past the end (bbtsvd.cpp:432,
+# 442), whose value is whatever the allocator left there.
+OTHER_MASK_CASES = {
+    "naive_left7x5": ("naive", 7, 5, 3, 0, 1, 1, 4),
+    "naive_right6x9": ("naive", 6, 9, 2, 0, 0, 0, 13),
+    "naive_left8x4": ("naive", 8, 4, 4, 0, 0, 1, 7),
+    "cached_left7x5": ("cached", 7, 5, 3, 0, 1, 1, 4),
+    "cached_right6x9": ("cached", 6, 9, 2, 0, 0, 0, 13),
+    "cached_left5x8": ("cached", 5, 8, 3, 0, 0, 1, 21),
+    "block_left7x5": ("block", 7, 5, 9, 0, 1, 1, 5),
+    "block_right6x9": ("block", 6, 9, 12, 0, 0, 0, 6),
+    "block_right8x6": ("block", 8, 6, 8, 0, 1, 0, 2),
+    "shufblock_left7x5": ("shufblock", 7, 5, 8, 2, 1, 1, 8),
+    "shufblock_right6x9": ("shufblock", 6, 9, 10, 2, 0, 0, 3),
+    "house_left6x4": ("house", 6, 4, 3, 0, 1, 1, 10),
+    "house_right5x7": ("house", 5, 7, 7, 0, 0, 0, 12),
+    "reflector_left6x4": ("reflector", 6, 4, 3, 0, 1, 1, 14),
+    "reflector_left4x7": ("reflector", 4, 7, 4, 0, 0, 1, 15),
+    "reflector_right5x8": ("reflector", 5, 8, 5, 0, 1, 0, 16),
+}

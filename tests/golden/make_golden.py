@@ -249,6 +249,34 @@ def generator_fixtures(R):
     return out
 
 
+def other_mask_fixtures(R):
+    """The masks of bbtsvd.hpp off the opt_control 1/3 path (bbtsvd.cpp:190-299,
+    429-531, 670-726) on small blocks, each with the next rand() value after
+    the call."""
+    R.ref_rand.restype = C.c_int
+    out = {}
+    rng = np.random.default_rng(29)
+    for name, (fn, m, n, size, rounds, mask, left, seed) in cases.OTHER_MASK_CASES.items():
+        x0 = rng.standard_normal(m * n)
+        x = x0.copy()
+        args = (C.c_size_t(m), C.c_size_t(n), C.c_size_t(size))
+        tail = (p(x), C.c_int(mask), C.c_int(left), C.c_uint(seed))
+        if fn == "naive":
+            R.ref_naive_givens(*args, *tail)
+        elif fn == "cached":
+            R.ref_givens_cached(*args, *tail)
+        elif fn == "block":
+            R.ref_block_mask(*args, *tail)
+        elif fn == "shufblock":
+            R.ref_shuffle_block_mask(*args, C.c_int(rounds), *tail)
+        elif fn == "house":
+            R.ref_house_mask(*args, *tail)
+        else:
+            R.ref_householder_reflector_mask(*args, *tail)
+        out[name] = dict(x_in=x0, x_out=x, rand_after=np.int64(R.ref_rand()))
+    return out
+
+
 def main():
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref", f"REF={REF}"], check=True)
     R = C.CDLL(os.path.join(REFDIR, "libref_capi.so"))
@@ -256,7 +284,7 @@ def main():
     R.ref_set_threads(1)
     fx = {}
     groups = (("bidiag", bidiagonal_fixtures), ("mask", mask_fixtures), ("step", step_fixtures),
-              ("gen", generator_fixtures), ("pipe", lambda R: pipeline_fixtures()))
+              ("gen", generator_fixtures), ("omask", other_mask_fixtures), ("pipe", lambda R: pipeline_fixtures()))
     keep = sys.argv[1:]
     for grp, fn in groups:
         if keep and not any(k.startswith(grp) for k in keep):

@@ -33,7 +33,8 @@ def test_every_fixture_has_a_case():
             | {f"pipe__{n}" for n in PIPES} | {f"pipe__{n}" for n in cases.pipeline_mode_cases()}
             | {f"pipe__{n}" for n in cases.tall_cases()} | {f"pipe__{n}" for n in cases.tall_mode_cases()}
             | {f"pipe__{n}_mode{m}" for n in cases.square_cases() for m in (0, 1)}
-            | {f"step__{n}" for n in cases.step_cases()} | {f"gen__{n}" for n in cases.GENERATOR_FIXTURES})
+            | {f"step__{n}" for n in cases.step_cases()} | {f"gen__{n}" for n in cases.GENERATOR_FIXTURES}
+            | {f"omask__{n}" for n in cases.OTHER_MASK_CASES})
     assert names == want
 
 
