@@ -154,8 +154,8 @@ GENERATOR_FIXTURES = ("house_row7", "house_col6", "orth_tall9x4", "orth_wide4x9"
 # (function, m, n, size, rounds, mask, is_left, seed); size is the pass count,
 # block size or reflector count, rounds the shuffle_block_mask rounds.  The
 # block masks' cases use one block smaller than the block size: a full block
-# makes the reference read its tau array one past the end (bbtsvd.cpp:432,
-# 442), whose value is whatever the allocator left there.
+# makes the reference read its tau array one past the end (bbtsvd.cpp:433,
+# 441, 503), whose value is whatever the allocator left there.
 OTHER_MASK_CASES = {
     "naive_left7x5": ("naive", 7, 5, 3, 0, 1, 1, 4),
     "naive_right6x9": ("naive", 6, 9, 2, 0, 0, 0, 13),
