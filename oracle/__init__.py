@@ -49,6 +49,8 @@ def lib():
         for f in (L.orc_givens_mask, L.orc_block_shift_mask):
             f.argtypes = [_C.c_size_t, _C.c_size_t, _C.c_size_t, _C.c_void_p, _C.c_int, _C.c_int,
                           _C.c_uint]
+        L.orc_givens_variant.argtypes = [_C.c_size_t, _C.c_size_t, _C.c_size_t, _C.c_void_p, _C.c_int, _C.c_int,
+                                         _C.c_uint, _C.c_int]
         L.orc_square_convert.argtypes = [_C.c_size_t, _C.c_void_p, _C.c_void_p, _C.c_void_p]
         L.orc_srand.argtypes = [_C.c_uint]
         L.orc_rand.restype = _C.c_int
@@ -116,6 +118,20 @@ def givens_mask(x, passes, mask, is_left, seed):
     m, n = y.shape
     lib().orc_givens_mask(m, n, passes, _p(y), int(bool(mask)), int(bool(is_left)), seed)
     return y
+
+
+def givens_variant(x, passes, mask, is_left, seed, cached):
+    """naive_givens_mask_parallel (cached=False) or
+    givens_mask_cache_optimized_parallel (cached=True) on a copy of x."""
+    y = _f64(x).copy()
+    m, n = y.shape
+    lib().orc_givens_variant(m, n, passes, _p(y), int(bool(mask)), int(bool(is_left)), seed, int(bool(cached)))
+    return y
+
+
+def rand():
+    """glibc's next rand() value (the state the restated masks leave behind)."""
+    return lib().orc_rand()
 
 
 def block_shift_mask(x, passes, mask, is_left, seed):

@@ -304,6 +304,70 @@ void orc_givens_mask(size_t m, size_t n, size_t passes, double* x, int mask, int
   }
 }
 
+// The two other Givens masks of bbtsvd.hpp (bbtsvd.cpp:190-299), restated:
+// floor(k / 2) pairs per pass (an odd k's last index stays put), c and s
+// drawn as two runs of random_value(-1, 1) after every shuffle, normalised
+// by |(c, s)|.  naive (cached = 0): the permutation is shuffled again for
+// every pass, pairs rotate unordered as BLAS drot (x, y) <- (c x + s y,
+// c y - s x) with s negated when unmasking, which takes the passes in
+// reverse order but their (c, s) forward.  cached (cached = 1): a fresh
+// shuffle per pass, pairs ordered (low, high), unmasking reverses the passes
+// and their (c, s) together.  Each product and sum rounded on its own.
+void orc_givens_variant(size_t m, size_t n, size_t passes, double* x, int mask, int is_left, unsigned seed,
+                        int cached) {
+  srand(seed);
+  std::default_random_engine eng(seed);
+  const int k = (int)(is_left ? m : n);
+  std::vector<std::vector<int>> perm;
+  std::vector<int> run;
+  for (int i = 0; i < k; ++i) run.push_back(i);
+  for (size_t t = 0; t < passes; ++t) {
+    if (cached) {
+      std::vector<int> idx;
+      for (int i = 0; i < k; ++i) idx.push_back(i);
+      std::shuffle(idx.begin(), idx.end(), eng);
+      perm.push_back(idx);
+    } else {
+      std::shuffle(run.begin(), run.end(), eng);
+      perm.push_back(run);
+    }
+  }
+  if (cached && !mask) std::reverse(perm.begin(), perm.end());
+  const size_t ops = (size_t)((k - (k % 2)) / 2);
+  std::vector<double> c(passes * ops), s(passes * ops);
+  for (auto& v : c) v = (rand() / (double)RAND_MAX) * 2.0 + -1.0;
+  for (auto& v : s) v = (rand() / (double)RAND_MAX) * 2.0 + -1.0;
+  for (size_t q = 0; q < c.size(); ++q) {
+    const double r = pow(pow(c[q], 2) + pow(s[q], 2), 0.5);
+    c[q] /= r;
+    s[q] /= r;
+  }
+  const double sg = mask ? 1.0 : -1.0;
+  const size_t other = is_left ? n : m;
+  std::vector<double> vec(k);
+  for (size_t col = 0; col < other; ++col) {
+    for (int i = 0; i < k; ++i) vec[i] = is_left ? x[i * n + col] : x[col * n + i];
+    for (size_t t = 0; t < passes; ++t) {
+      const std::vector<int>& pr = cached ? perm[t] : perm[mask ? t : passes - 1 - t];
+      const size_t cb = (cached && !mask ? passes - 1 - t : t) * ops;
+      for (size_t j = 0; j < ops; ++j) {
+        int a = pr[2 * j], b = pr[2 * j + 1];
+        if (cached && a > b) std::swap(a, b);
+        const double cq = c[cb + j], sq = sg * s[cb + j];
+        const double x1 = vec[a], x2 = vec[b];
+        const double n1 = x1 * cq + x2 * sq;
+        const double n2 = x1 * (-sq) + x2 * cq;
+        vec[a] = n1;
+        vec[b] = n2;
+      }
+    }
+    for (int i = 0; i < k; ++i) {
+      if (is_left) x[i * n + col] = vec[i];
+      else x[col * n + i] = vec[i];
+    }
+  }
+}
+
 // Near-square factorisation k - remain = rows * cols used by the large-k
 // mask path.  bbtsvd.cpp:166-188 (limit 10000, aspect ratio < 2).
 void orc_square_convert(size_t k, size_t* rows, size_t* cols, size_t* remain) {

@@ -198,6 +198,23 @@ def test_square_matches_reference(golden, mode, name):
     _check_outputs(g, s, U, VT, mode)
 
 
+@pytest.mark.parametrize("name", sorted(n for n, c in cases.OTHER_MASK_CASES.items() if c[0] in ("naive", "cached")))
+def test_givens_variants_match_reference(golden, name):
+    """The oracle's restatement of naive_givens_mask_parallel and
+    givens_mask_cache_optimized_parallel against the reference's build: the
+    cache-optimised mask to the last bit, the naive one to rounding (the
+    reference rotates with its BLAS drot); glibc's rand() state afterwards
+    exactly."""
+    key, m, n, passes, _, mask, left, seed = cases.OTHER_MASK_CASES[name]
+    g = golden(f"omask__{name}")
+    y = oracle.givens_variant(g["x_in"].reshape(m, n), passes, mask, left, seed, key == "cached").reshape(-1)
+    if key == "cached":
+        assert np.array_equal(y, g["x_out"])
+    else:
+        assert np.abs(y - g["x_out"]).max() <= 1e-14 * np.abs(g["x_out"]).max()
+    assert oracle.rand() == int(g["rand_after"])
+
+
 @pytest.mark.parametrize("name", sorted(cases.step_cases()))
 def test_oracle_steps_match_reference(golden, name):
     """The per-step helpers (bbtsvd.cpp:54-164, 970-978) restated in
