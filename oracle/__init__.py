@@ -51,6 +51,12 @@ def lib():
                           _C.c_uint]
         L.orc_givens_variant.argtypes = [_C.c_size_t, _C.c_size_t, _C.c_size_t, _C.c_void_p, _C.c_int, _C.c_int,
                                          _C.c_uint, _C.c_int]
+        for f in (L.orc_block_mask, L.orc_house_mask, L.orc_householder_reflector_mask):
+            f.restype = _C.c_int
+            f.argtypes = [_C.c_size_t, _C.c_size_t, _C.c_size_t, _C.c_void_p, _C.c_int, _C.c_int, _C.c_uint]
+        L.orc_shuffle_block_mask.restype = _C.c_int
+        L.orc_shuffle_block_mask.argtypes = [_C.c_size_t, _C.c_size_t, _C.c_size_t, _C.c_int, _C.c_void_p,
+                                             _C.c_int, _C.c_int, _C.c_uint]
         L.orc_square_convert.argtypes = [_C.c_size_t, _C.c_void_p, _C.c_void_p, _C.c_void_p]
         L.orc_srand.argtypes = [_C.c_uint]
         L.orc_rand.restype = _C.c_int
@@ -126,6 +132,25 @@ def givens_variant(x, passes, mask, is_left, seed, cached):
     y = _f64(x).copy()
     m, n = y.shape
     lib().orc_givens_variant(m, n, passes, _p(y), int(bool(mask)), int(bool(is_left)), seed, int(bool(cached)))
+    return y
+
+
+def dense_mask(kind, x, size, mask, is_left, seed, rounds=0):
+    """block_mask / shuffle_block_mask / house_mask / householder_reflector_mask
+    (kind "block", "shufblock", "house", "reflector") on a copy of x (m x n as
+    the reference's buffer), over the LAPACK the process has loaded."""
+    y = _f64(x).copy()
+    m, n = y.shape
+    L = lib()
+    a = (m, n, size)
+    t = (_p(y), int(bool(mask)), int(bool(is_left)), seed)
+    if kind == "shufblock":
+        rc = L.orc_shuffle_block_mask(*a, rounds, *t)
+    else:
+        rc = {"block": L.orc_block_mask, "house": L.orc_house_mask,
+              "reflector": L.orc_householder_reflector_mask}[kind](*a, *t)
+    if rc != 0:
+        raise RuntimeError("no LAPACK loaded in this process")
     return y
 
 

@@ -13,15 +13,130 @@
 // with -ffp-contract=off (no fused multiply-add), matching the reference's
 // `-O3 -mavx2` build in which pow(x, 2) is folded to x*x and AVX2 without
 // FMA rounds every product and every sum.
+#include <dlfcn.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <random>
+#include <string>
 #include <vector>
 
 namespace {
+
+// The LAPACK / BLAS routines the reference's dense masks call (MKL there),
+// resolved in the process at run time: the plain name, else scipy's
+// prefixed OpenBLAS.  Null when none is loaded.
+void* lapack(const char* name) {
+  void* f = dlsym(RTLD_DEFAULT, name);
+  if (!f) f = dlsym(RTLD_DEFAULT, (std::string("scipy_") + name).c_str());
+  return f;
+}
+using dlarnv_t = int (*)(int, int*, int, double*);
+using dlarfg_t = int (*)(int, double*, double*, int, double*);
+using dgeqrf_t = int (*)(int, int, int, double*, int, double*);
+using dnrm2_t = double (*)(int, const double*, int);
+
+void seed4(int (&iseed)[4]) {   // the reference's dlarnv seeding (bbtsvd.cpp:305-306)
+  for (int r = 0; r < 4; ++r) iseed[r] = rand() % 4096;
+  if (iseed[3] % 2 == 0) iseed[3] = (iseed[3] + 1) % 4096;
+}
+
+// generate_random_orthogonal_matrix(CblasRowMajor, m, house, tau, seed),
+// bbtsvd.cpp:301-331: row i of house gets i + 1 normal entries, then
+// reflector i from column i below the diagonal (dlarfg), house[m*m-1] = 1.
+bool orthogonal_house(size_t m, double* house, double* tau, unsigned seed) {
+  const auto dlarnv = (dlarnv_t)lapack("LAPACKE_dlarnv");
+  const auto dlarfg = (dlarfg_t)lapack("LAPACKE_dlarfg");
+  if (!dlarnv || !dlarfg) return false;
+  srand(seed);
+  int iseed[4];
+  std::vector<double> h(m);
+  for (size_t i = 0; i < m; ++i) {
+    seed4(iseed);
+    dlarnv(3, iseed, (int)(i + 1), house + i * m);
+  }
+  for (size_t i = 0; i + 1 < m; ++i) {
+    for (size_t j = 0; j < m - i; ++j) h[j] = house[i * m + i + j * m];
+    dlarfg((int)(m - i), h.data(), h.data() + 1, 1, tau + i);
+    for (size_t j = 0; j < m - i; ++j) house[i * m + i + j * m] = h[j];
+  }
+  if (m > 0) house[m * m - 1] = 1.0;
+  return true;
+}
+
+// dormqr's action, by its definition: Q = H_0 ... H_{k-1}, H_j = I - tau_j
+// v_j v_j^T, v_j unit at j with A(r, j) below it (A(r, c) = A[r*ars + c*acs]);
+// C (rows x cols, C(r, c) = C[r*crs + c*ccs]) <- op(Q) C (left) or C op(Q).
+void reflect(bool left, bool trans, size_t rows, size_t cols, size_t k, const double* A, long ars, long acs,
+             const double* tau, double* C, long crs, long ccs) {
+  const size_t nq = left ? rows : cols;
+  std::vector<double> v(nq);
+  // left N and right T apply H_{k-1} first; left T and right N apply H_0 first
+  const bool backward = left != trans;
+  for (size_t s = 0; s < k; ++s) {
+    const size_t j = backward ? k - 1 - s : s;
+    for (size_t r = 0; r < nq; ++r) v[r] = r < j ? 0.0 : (r == j ? 1.0 : A[r * ars + j * acs]);
+    if (left) {
+      for (size_t c = 0; c < cols; ++c) {   // C(:, c) -= tau v (v^T C(:, c))
+        double w = 0.0;
+        for (size_t r = j; r < rows; ++r) w += v[r] * C[r * crs + c * ccs];
+        for (size_t r = j; r < rows; ++r) C[r * crs + c * ccs] -= tau[j] * v[r] * w;
+      }
+    } else {
+      for (size_t r = 0; r < rows; ++r) {   // C(r, :) -= tau (C(r, :) v) v^T
+        double w = 0.0;
+        for (size_t c = j; c < cols; ++c) w += C[r * crs + c * ccs] * v[c];
+        for (size_t c = j; c < cols; ++c) C[r * crs + c * ccs] -= tau[j] * w * v[c];
+      }
+    }
+  }
+}
+
+// The block step of block_mask / shuffle_block_mask (bbtsvd.cpp:436-442,
+// 463-467, 511-523) on a row-major m x n x: each block of bs rows (is_left)
+// or columns gets op(Q) from its size and seed, op = Q masking and Q^T
+// unmasking.  A full block's last reflector is taken as the identity (the
+// reference reads its tau one past the end of the tau array).
+bool block_step(size_t m, size_t n, size_t bs, double* x, int mask, int is_left, unsigned seed) {
+  const size_t k = is_left ? m : n;
+  std::vector<double> house, tau;
+  for (size_t i = 0; i < k; i += bs) {
+    const size_t rb = std::min(bs, k - i);
+    house.assign(rb * rb, 0.0);
+    tau.assign(rb, 0.0);
+    if (!orthogonal_house(rb, house.data(), tau.data(), seed)) return false;
+    tau[rb - 1] = 0.0;
+    if (is_left)
+      reflect(true, !mask, rb, n, rb, house.data(), (long)rb, 1, tau.data(), x + i * n, (long)n, 1);
+    else
+      reflect(false, !mask, m, rb, rb, house.data(), (long)rb, 1, tau.data(), x + i, (long)n, 1);
+  }
+  return true;
+}
+
+// shuffle_matrix, bbtsvd.cpp:396-427 (k = 1 left alone: the reference divides by zero).
+void shuffle_rows(size_t m, size_t n, double* x, unsigned seed, int is_left, int unshuffle) {
+  srand(seed);
+  std::default_random_engine dre(seed);
+  const size_t k = is_left ? m : n;
+  std::vector<int> idx;
+  for (size_t i = 0; i < k; ++i) idx.push_back((int)i);
+  std::shuffle(idx.begin(), idx.end(), dre);
+  size_t ri = 0;
+  if (k % 2 != 0) ri = k > 1 ? rand() % (k - 1) : 0;
+  auto sw = [&](size_t a, size_t b) {
+    if (a == b) return;
+    if (is_left) for (size_t e = 0; e < n; ++e) std::swap(x[a * n + e], x[b * n + e]);
+    else for (size_t e = 0; e < m; ++e) std::swap(x[e * n + a], x[e * n + b]);
+  };
+  if (k % 2 != 0 && unshuffle) sw(k - 1, ri);
+  for (size_t i = 0; i < k / 2; ++i) sw((size_t)idx[2 * i], (size_t)idx[2 * i + 1]);
+  if (k % 2 != 0 && !unshuffle) sw(k - 1, ri);
+}
 
 // Stationary-qd Sturm count of B^T B - mu^2 I.  bbtsvd.cpp:7-17.
 int sturm_count(int n, const double* a, const double* b, double mu) {
@@ -455,6 +570,79 @@ void orc_block_shift_mask(size_t m, size_t n, size_t passes, double* x, int mask
       for (size_t i = 0; i < body; ++i) at(v, i) = blk[i];
     }
   }
+}
+
+// The dense masks of bbtsvd.hpp, restated over the process's LAPACK (each
+// returns 0, or -1 when no LAPACK is loaded).  block_mask, bbtsvd.cpp:429-487
+// (blocks below 10,000): every block draws its Q from srand(seed) again.
+int orc_block_mask(size_t m, size_t n, size_t bs, double* x, int mask, int is_left, unsigned seed) {
+  if ((is_left && m <= 1) || (!is_left && n <= 1)) return 0;
+  return block_step(m, n, bs, x, mask, is_left, seed) ? 0 : -1;
+}
+
+// shuffle_block_mask, bbtsvd.cpp:489-531: per round a shuffle (before the
+// blocks when masking, after them when unmasking) and the block step.
+int orc_shuffle_block_mask(size_t m, size_t n, size_t bs, int rounds, double* x, int mask, int is_left,
+                           unsigned seed) {
+  srand(seed);
+  std::vector<unsigned> ss, ms;
+  for (int st = 0; st < rounds; ++st) {
+    ss.push_back((unsigned)rand());
+    ms.push_back((unsigned)rand());
+  }
+  if (!mask) {
+    std::reverse(ss.begin(), ss.end());
+    std::reverse(ms.begin(), ms.end());
+  }
+  for (int st = 0; st < rounds; ++st) {
+    if (mask) shuffle_rows(m, n, x, ss[st], is_left, 1);
+    srand(ms[st]);
+    if (!block_step(m, n, bs, x, mask, is_left, ms[st])) return -1;
+    if (!mask) shuffle_rows(m, n, x, ss[st], is_left, 0);
+  }
+  return 0;
+}
+
+// house_mask, bbtsvd.cpp:670-694: Q from dgeqrf of a normal random
+// mask_size x k matrix (column-major k x mask_size), applied to x as a
+// column-major m x n matrix; op(Q) = Q when is_left equals mask.
+int orc_house_mask(size_t m, size_t n, size_t ms, double* x, int mask, int is_left, unsigned seed) {
+  const auto dlarnv = (dlarnv_t)lapack("LAPACKE_dlarnv");
+  const auto dgeqrf = (dgeqrf_t)lapack("LAPACKE_dgeqrf");
+  if (!dlarnv || !dgeqrf) return -1;
+  srand(seed);
+  const size_t k = is_left ? m : n;
+  std::vector<double> A(k * ms), tau(ms);
+  int iseed[4];
+  for (size_t i = 0; i < ms; ++i) {   // utils.cpp:214-223 random_normal_matrix
+    seed4(iseed);
+    dlarnv(3, iseed, (int)k, A.data() + i * k);
+  }
+  dgeqrf(102, (int)k, (int)ms, A.data(), (int)k, tau.data());
+  reflect(is_left, is_left != mask, m, n, ms, A.data(), 1, (long)k, tau.data(), x, 1, (long)m);
+  return 0;
+}
+
+// householder_reflector_mask, bbtsvd.cpp:696-726: unit-headed reflectors
+// with random_value(-1, 1) entries below, tau = 2 / dnrm2(v)^2; x column-major
+// m x n when m >= n (Q on the is_left side), else n x m (Q on the other side).
+int orc_householder_reflector_mask(size_t m, size_t n, size_t ms, double* x, int mask, int is_left,
+                                   unsigned seed) {
+  const auto dnrm2 = (dnrm2_t)lapack("cblas_dnrm2");
+  if (!dnrm2) return -1;
+  srand(seed);
+  const size_t k = is_left ? m : n;
+  std::vector<double> H(k * ms, 0.0), tau(ms, 0.0);
+  for (size_t i = 0; i < ms; ++i) {
+    H[i * k + i] = 1.0;
+    for (size_t j = 0; j + i + 1 < k; ++j) H[i * k + i + 1 + j] = (rand() / (double)RAND_MAX) * 2.0 + -1.0;
+    tau[i] = 2 / pow(dnrm2((int)(k - i), H.data() + i * k + i, 1), 2);
+  }
+  if (m >= n)
+    reflect(is_left, is_left != mask, m, n, ms, H.data(), 1, (long)k, tau.data(), x, 1, (long)m);
+  else
+    reflect(!is_left, is_left == mask, n, m, ms, H.data(), 1, (long)k, tau.data(), x, 1, (long)n);
+  return 0;
 }
 
 // glibc srand/rand passthrough so tests can derive seeds the way the

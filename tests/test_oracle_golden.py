@@ -215,6 +215,29 @@ def test_givens_variants_match_reference(golden, name):
     assert oracle.rand() == int(g["rand_after"])
 
 
+@pytest.fixture(scope="module")
+def lapack():
+    import ctypes
+    import site
+    hits = [h for d in site.getsitepackages() for h in glob.glob(os.path.join(d, "scipy.libs", "libscipy_openblas-*.so"))]
+    if not hits:
+        pytest.skip("no LAPACK library in this environment")
+    ctypes.CDLL(hits[0], mode=ctypes.RTLD_GLOBAL)   # found by the oracle at run time
+
+
+@pytest.mark.parametrize("name", sorted(n for n, c in cases.OTHER_MASK_CASES.items() if c[0] not in ("naive", "cached")))
+def test_dense_masks_match_reference(golden, lapack, name):
+    """The oracle's restatement of block_mask, shuffle_block_mask, house_mask
+    and householder_reflector_mask (reflectors applied one by one, as
+    dormqr defines them) against the reference's build, to rounding; glibc's
+    rand() state afterwards exactly."""
+    key, m, n, size, rounds, mask, left, seed = cases.OTHER_MASK_CASES[name]
+    g = golden(f"omask__{name}")
+    y = oracle.dense_mask(key, g["x_in"].reshape(m, n), size, mask, left, seed, rounds).reshape(-1)
+    assert np.abs(y - g["x_out"]).max() <= 1e-13 * np.abs(g["x_out"]).max()
+    assert oracle.rand() == int(g["rand_after"])
+
+
 @pytest.mark.parametrize("name", sorted(cases.step_cases()))
 def test_oracle_steps_match_reference(golden, name):
     """The per-step helpers (bbtsvd.cpp:54-164, 970-978) restated in
