@@ -15,6 +15,7 @@
 // The ring all-reduce / all-gather of the reference become reductions
 // inside the kernels (Ralha) or plain device-memory reads (U all-gather).
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <vector>
@@ -26,6 +27,25 @@
 
 namespace bbt {
 namespace {
+
+// Host-side NVTX ranges, one per phase of a pipeline call, named as the
+// reference's phase timers (client.hpp:83-84: local_qr, apply_mask,
+// global_qr, bi_diag, bsvd, combine_svd_remove_mask), each opened where the
+// phase's start event is recorded, so a trace lines up with the reference's
+// log lines.  Without a tool attached NVTX calls do nothing.
+struct PhaseRanges {
+  bool open = false;
+  void next(const char* name) {
+    if (open) nvtxRangePop();
+    nvtxRangePushA(name);
+    open = true;
+  }
+  void close() {
+    if (open) nvtxRangePop();
+    open = false;
+  }
+  ~PhaseRanges() { close(); }
+};
 
 constexpr int MASK_PASSES = 32;            // client.cpp:536
 constexpr size_t MASK_SCRATCH_CAP = (size_t)2 << 30;
@@ -602,7 +622,9 @@ bbt_status fedsvd_tall(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, const Layout&
     cudaEvent_t* e;
     ~EvGuard() { for (int i = 0; i < 7; ++i) cudaEventDestroy(e[i]); }
   } guard{ev};
+  PhaseRanges phases;
   BBT_CUDA(ctx, cudaEventRecord(ev[0], ctx->stream));
+  phases.next("apply_mask");
   // 1) masks: private on the left (rows of X_c^T), public on the right (:548-551)
   for (int c = 0; c < P; ++c) {
     if (ctx->io_on) BBT_TRY(wait_input(ctx, c));
@@ -610,6 +632,7 @@ bbt_status fedsvd_tall(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, const Layout&
     BBT_TRY(block_shift_mask(ctx, L.n[c], m, MASK_PASSES, X[c], true, false, cfg->public_seed));
   }
   BBT_CUDA(ctx, cudaEventRecord(ev[1], ctx->stream));
+  phases.next("global_qr");
   // 2) repartition (:627-659): slab c = rows n_pos.. of every masked block,
   //    columns m_part_pos[c].., global_n x m_part[c]; a slab that is not
   //    reduced goes straight into its columns of the Ralha matrix
@@ -620,6 +643,7 @@ bbt_status fedsvd_tall(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, const Layout&
       BBT_TRY(copy2d(ctx, (int)L.n[d], (int)L.part[c], X[d] + L.ppos[c], (long)m, dst + L.npos[d] * ldd, ldd));
   }
   BBT_CUDA(ctx, cudaEventRecord(ev[2], ctx->stream));
+  phases.next("local_qr");
   // 3) local QR of the slabs with m_part > global_n (:661-677): R^T replaces the slab
   if (L.precision == 1) {
     BBT_TRY(rademacher(ctx, sketch_rows(gi), (long)Q.nmax, S, 0x5EED5EEDull));
@@ -638,9 +662,11 @@ bbt_status fedsvd_tall(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, const Layout&
   for (int c = 0; c < P; ++c)
     if (Q.qr[c]) BBT_TRY(copy2d(ctx, gi, gi, RT[c], (long)g, W + L.wpos[c], (long)wn));
   BBT_CUDA(ctx, cudaEventRecord(ev[3], ctx->stream));
+  phases.next("bi_diag");
   // 4) Ralha of the global_n x wn matrix (:805-954)
   BBT_TRY(ralha(ctx, gi, (int)wn, W, house, tauh, alpha, beta, Vr, cs));
   BBT_CUDA(ctx, cudaEventRecord(ev[4], ctx->stream));
+  phases.next("bsvd");
   // 5) singular values / vectors (:963-995); svd_mode 4 takes dbdsdc's path as mode 0
   BBT_TRY(bidiag_bound(ctx, gi, alpha, beta, scal));
   BBT_CUDA(ctx, cudaMemsetAsync(scal + 1, 0, sizeof(double), ctx->stream));
@@ -662,6 +688,7 @@ bbt_status fedsvd_tall(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, const Layout&
     if (mode == 0 || mode == 4) BBT_TRY(refine_clusters(ctx, gi, k, alpha, beta, sigma, Ub, Vb, &ncl));
   }
   BBT_CUDA(ctx, cudaEventRecord(ev[5], ctx->stream));
+  phases.next("combine_svd_remove_mask");
   // 6) U (:1002-1015): part_c = V_b Vr_c (Q_c^T), k x m_part[c], at columns
   //    m_part_pos[c] of FinalU (k x m row-major = column-major m x k)
   if (compute_u) {
@@ -723,6 +750,7 @@ bbt_status fedsvd_tall(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, const Layout&
     }
   }
   BBT_CUDA(ctx, cudaEventRecord(ev[6], ctx->stream));
+  phases.close();
   BBT_CUDA(ctx, cudaEventSynchronize(ev[6]));
   if (L.precision >= 1) BBT_TRY(check_tc_flags(ctx, "fedsvd: tensor-core back-transform"));
   // stage order of the reference's timers: local_qr, apply_mask, global_qr
@@ -865,7 +893,9 @@ bbt_status fedsvd(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* X, 
     cudaEvent_t* e;
     ~EvGuard() { for (int i = 0; i < 7; ++i) cudaEventDestroy(e[i]); }
   } guard{ev};
+  PhaseRanges phases;
   BBT_CUDA(ctx, cudaEventRecord(ev[0], ctx->stream));
+  phases.next("local_qr");
 
   // 1) local QR (client.cpp:572-589): A = X_c^T column-major n x m, in place
   job.compute_v = compute_v;
@@ -884,6 +914,7 @@ bbt_status fedsvd(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* X, 
   if (ctx->io_on)
     for (int c = 0; c < P; ++c) BBT_TRY(wait_input(ctx, c));
   BBT_CUDA(ctx, cudaEventRecord(ev[1], ctx->stream));
+  phases.next("apply_mask");
   // 2) masks (client.cpp:593-596)
   BBT_TRY(pf.upload(ctx, mask_slab));
   for (int c = 0; c < P; ++c) {
@@ -891,6 +922,7 @@ bbt_status fedsvd(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* X, 
     BBT_TRY(apply_mask(ctx, pf, m, L.r[c], masked[c], true, false, cfg->private_seeds[c]));
   }
   BBT_CUDA(ctx, cudaEventRecord(ev[2], ctx->stream));
+  phases.next("global_qr");
   // 3) repartition + global QR of M^T (client.cpp:681-794)
   for (int c = 0; c < P; ++c)
     BBT_TRY(copy2d(ctx, mi, (int)L.r[c], masked[c], (long)L.r[c], M + L.rpos[c], (long)rg));
@@ -915,9 +947,11 @@ bbt_status fedsvd(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* X, 
     if (compute_v) BBT_TRY(orgqr(ctx, (long)rg, mi, M, (long)rg, taug, Tg, qp));   // M <- Q_g (rg x m)
   }
   BBT_CUDA(ctx, cudaEventRecord(ev[3], ctx->stream));
+  phases.next("bi_diag");
   // 4) Ralha bidiagonalisation, lower -> upper (client.cpp:801-954)
   BBT_TRY(ralha(ctx, mi, mi, W, house, tauh, alpha, beta, Vr, cs));
   BBT_CUDA(ctx, cudaEventRecord(ev[4], ctx->stream));
+  phases.next("bsvd");
   // 5) singular values / vectors (client.cpp:963-995)
   BBT_TRY(bidiag_bound(ctx, mi, alpha, beta, scal));
   BBT_CUDA(ctx, cudaMemsetAsync(scal + 1, 0, sizeof(double), ctx->stream));
@@ -944,6 +978,7 @@ bbt_status fedsvd(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* X, 
     if (cfg->svd_mode == 0) BBT_TRY(refine_clusters(ctx, mi, k, alpha, beta, sigma, Ub, Vb, &ncl));
   }
   BBT_CUDA(ctx, cudaEventRecord(ev[5], ctx->stream));
+  phases.next("combine_svd_remove_mask");
   // 6) U: FinalU (m x k row-major) = (V_b Vr)^T, unmasked (client.cpp:1018, 1071-1115)
   if (compute_u) {
     BBT_TRY(dgemm(ctx, true, true, k, mi, m, 1.0, Vb, (long)m, Vr, (long)m, 0.0, Uout, k));
@@ -1033,6 +1068,7 @@ bbt_status fedsvd(bbt_ctx* ctx, const bbt_fedsvd_config* cfg, double* const* X, 
   }
   }
   BBT_CUDA(ctx, cudaEventRecord(ev[6], ctx->stream));
+  phases.close();
   BBT_CUDA(ctx, cudaEventSynchronize(ev[6]));
   if (L.precision >= 1) BBT_TRY(check_tc_flags(ctx, "fedsvd: tensor-core back-transform"));
   for (int s = 0; s < 6; ++s) {
